@@ -1,0 +1,193 @@
+"""ctypes binding of include/gpudb_capi.h (the engine's C ABI).
+
+This is the reference-side binding a Python caller uses; the same structs and entry points
+are what a cgo / JNI / N-API stub binds. Loading fails loudly when lib/libgpudb.so is
+missing: there is no fallback implementation.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgpudb.so")
+
+# status codes
+OK = 0
+E_INVALID, E_CUDA, E_OOM, E_NODEVICE, E_CAPACITY, E_KEY_RANGE, E_TIMEOUT, E_BUSY, E_CLOSED, E_UNSUPPORTED = \
+    -1, -2, -3, -4, -5, -6, -7, -8, -9, -10
+ERROR_NAMES = {0: "OK", -1: "E_INVALID", -2: "E_CUDA", -3: "E_OOM", -4: "E_NODEVICE", -5: "E_CAPACITY",
+               -6: "E_KEY_RANGE", -7: "E_TIMEOUT", -8: "E_BUSY", -9: "E_CLOSED", -10: "E_UNSUPPORTED"}
+
+MEM_DEVICE, MEM_HOST = 0, 1
+OPT_CHUNK_ROWS = 1
+JOIN_GLOBAL, JOIN_RADIX = 0, 1
+ORDERS_NONE, ORDERS_CLUSTERED, ORDERS_UNIFORM = 0, 1, 2
+Q3_MAX_K = 64
+
+# column ids
+COL = dict(
+    LI_SHIP_DATE=1, LI_QUANTITY=2, LI_EXT_PRICE=3, LI_DISCOUNT=4, LI_TAX=5, LI_FLAG=6, LI_STATUS=7,
+    LI_ORDER_KEY=8, LI_PART_KEY=9, LI_SUPP_KEY=10,
+    CU_CUST_KEY=20, CU_SEGMENT=21,
+    OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32,
+    PA_PART_KEY=40, PA_FLAG=41,
+    SU_SUPP_KEY=50, SU_NATION=51,
+    PS_PART_KEY=60, PS_SUPP_KEY=61, PS_SUPPLY_COST=62,
+)
+
+vp = C.c_void_p
+
+
+class I128(C.Structure):
+    _fields_ = [("lo", C.c_uint64), ("hi", C.c_int64)]
+
+    def value(self):
+        return (self.hi << 64) + self.lo
+
+
+class Exec(C.Structure):
+    _fields_ = [("async_", C.c_int32), ("flags", C.c_int32), ("stream", vp)]
+
+
+class Timing(C.Structure):
+    _fields_ = [("gpu_ms", C.c_double), ("host_ms", C.c_double), ("h2d_bytes", C.c_uint64),
+                ("d2h_bytes", C.c_uint64), ("kernels", C.c_uint32), ("chunks", C.c_uint32)]
+
+
+class Lineitem(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("location", C.c_int32), ("order_key_max", C.c_int32),
+                ("ship_date", vp), ("quantity", vp), ("ext_price", vp), ("discount", vp), ("tax", vp),
+                ("flag", vp), ("status", vp), ("order_key", vp), ("part_key", vp), ("supp_key", vp)]
+
+
+class Customer(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("reserved", C.c_int32),
+                ("cust_key", vp), ("segment", vp)]
+
+
+class Orders(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("cust_key_max", C.c_int32),
+                ("order_key", vp), ("cust_key", vp), ("order_date", vp)]
+
+
+class Part(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("reserved", C.c_int32),
+                ("part_key", vp), ("flag", vp)]
+
+
+class Supplier(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("reserved", C.c_int32),
+                ("supp_key", vp), ("nation", vp)]
+
+
+class Partsupp(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("part_key", vp), ("supp_key", vp), ("supply_cost", vp)]
+
+
+class GenSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("row_offset", C.c_uint64), ("n_rows", C.c_uint64),
+                ("n_orders", C.c_int64), ("n_cust", C.c_int64), ("n_parts", C.c_int64),
+                ("n_supp", C.c_int64), ("order_mode", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Q6Params(C.Structure):
+    _fields_ = [("ship_lo", C.c_int32), ("ship_hi", C.c_int32), ("disc_lo", C.c_int32),
+                ("disc_hi", C.c_int32), ("qty_lt", C.c_int32)]
+
+
+class Q6Result(C.Structure):
+    _fields_ = [("revenue", C.c_int64), ("rows_matched", C.c_uint64)]
+
+
+class Q1Params(C.Structure):
+    _fields_ = [("ship_le", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Q1Group(C.Structure):
+    _fields_ = [("flag", C.c_uint8), ("status", C.c_uint8), ("reserved", C.c_uint8 * 6), ("count", C.c_uint64),
+                ("sum_qty", I128), ("sum_base_price", I128), ("sum_disc_price", I128), ("sum_charge", I128),
+                ("sum_discount", I128)]
+
+
+class Q1Result(C.Structure):
+    _fields_ = [("n_groups", C.c_uint32), ("reserved", C.c_uint32), ("groups", Q1Group * 6)]
+
+
+class Q3Params(C.Structure):
+    _fields_ = [("segment", C.c_int32), ("order_date_lt", C.c_int32), ("ship_date_gt", C.c_int32),
+                ("k", C.c_int32), ("join_mode", C.c_int32), ("radix_bits", C.c_int32)]
+
+
+class Q3Row(C.Structure):
+    _fields_ = [("order_key", C.c_int32), ("order_date", C.c_int32), ("revenue", C.c_int64)]
+
+
+class Q3Result(C.Structure):
+    _fields_ = [("n_groups", C.c_uint64), ("n_rows", C.c_uint32), ("reserved", C.c_uint32),
+                ("rows", Q3Row * Q3_MAX_K)]
+
+
+class Q9Params(C.Structure):
+    _fields_ = [("smem_slots", C.c_int32), ("global_slots", C.c_int32), ("chunk_rows", C.c_uint64)]
+
+
+class Q9Group(C.Structure):
+    _fields_ = [("nation", C.c_int32), ("year", C.c_int32), ("profit", C.c_int64)]
+
+
+P = C.POINTER
+ctx_p = vp
+# name: (restype, argtypes)
+PROTOTYPES = {
+    "gpudb_abi_version": (C.c_int, []),
+    "gpudb_create": (C.c_int, [C.c_int, P(vp)]),
+    "gpudb_destroy": (C.c_int, [ctx_p]),
+    "gpudb_last_error_string": (C.c_char_p, [ctx_p]),
+    "gpudb_sync": (C.c_int, [ctx_p]),
+    "gpudb_stream": (vp, [ctx_p]),
+    "gpudb_kernel_launches": (C.c_uint64, [ctx_p]),
+    "gpudb_set_option": (C.c_int, [ctx_p, C.c_int32, C.c_int64]),
+    "gpudb_device_alloc": (C.c_int, [ctx_p, C.c_size_t, P(vp)]),
+    "gpudb_device_free": (C.c_int, [ctx_p, vp]),
+    "gpudb_host_alloc": (C.c_int, [ctx_p, C.c_size_t, P(vp)]),
+    "gpudb_host_free": (C.c_int, [ctx_p, vp]),
+    "gpudb_copy": (C.c_int, [ctx_p, vp, vp, C.c_size_t]),
+    "gpudb_generate": (C.c_int, [ctx_p, P(GenSpec), C.c_int32, vp, C.c_int32]),
+    "gpudb_column_width": (C.c_int, [C.c_int32]),
+    "gpudb_q6_sum": (C.c_int, [ctx_p, P(Lineitem), P(Q6Params), P(Q6Result), P(Timing), P(Exec)]),
+    "gpudb_q1_group6": (C.c_int, [ctx_p, P(Lineitem), P(Q1Params), P(Q1Result), P(Timing), P(Exec)]),
+    "gpudb_q3_join_topk": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q3Params), P(Q3Result),
+                                     P(Timing), P(Exec)]),
+    "gpudb_q9_star": (C.c_int, [ctx_p, P(Part), P(Supplier), P(Partsupp), P(Orders), P(Lineitem), P(Q9Params),
+                                P(Q9Group), C.c_uint32, P(C.c_uint32), P(Timing), P(Exec)]),
+    "gpudb_select_lt": (C.c_int, [ctx_p, vp, C.c_uint64, C.c_int32, vp, vp, P(C.c_uint64), P(Timing), P(Exec)]),
+    "gpudb_sum_i32": (C.c_int, [ctx_p, vp, C.c_uint64, P(C.c_int64), P(Timing), P(Exec)]),
+    "gpudb_hash_join_count": (C.c_int, [ctx_p, vp, C.c_uint64, vp, C.c_uint64, C.c_int32, P(C.c_uint64),
+                                        P(Timing), P(Exec)]),
+    "gpudb_radix_partition": (C.c_int, [ctx_p, vp, vp, C.c_uint64, C.c_int32, vp, vp, vp, P(Timing), P(Exec)]),
+    "gpudb_radix_join_pairs": (C.c_int, [ctx_p, vp, C.c_uint64, vp, C.c_uint64, vp, vp, C.c_uint64,
+                                         P(C.c_uint64), P(Timing), P(Exec)]),
+}
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load libgpudb.so and declare every prototype. Raises if the library is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("the engine library %s is not built (run python -m gpudbmetalbenchmark_b200.build)" % path)
+    lib = C.CDLL(path)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class GpudbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERROR_NAMES.get(code, "?"), code, msg))
+        self.code = code

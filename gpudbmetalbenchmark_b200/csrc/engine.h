@@ -1,0 +1,134 @@
+// Engine internals: the context object behind gpudb_ctx*, call scopes, scratch memory,
+// result slots, launch accounting and the chunked host->HBM streaming loop.
+//
+// These replace the reference's host infrastructure (src/infra.h): createPipeline /
+// releaseAll / createFilledBuffer (src/infra.h:178-189, 519-531) become the scratch arena
+// and RAII buffers, ChunkConfig + chunkedStreamLoop (src/infra.h:42-57, 816-869) become
+// stream_lineitem(), and GPUStartTime/GPUEndTime timing becomes CUDA events per call.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <functional>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gpudb_capi.h"
+
+namespace gpudb {
+
+constexpr int kResultSlots = 1024;
+constexpr size_t kSlotHeader = 16;                  // status word + padding
+constexpr size_t kSlotBytes = 4096;                 // header + largest fixed-size result
+constexpr int kStreamSlots = 3;                     // device buffers of the streaming ring
+constexpr uint64_t kDefaultChunkRows = 64ull << 20; // 64M rows per streamed chunk
+
+struct Buffer {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+double now_ms();
+
+}  // namespace gpudb
+
+struct gpudb_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;       // compute stream
+  cudaStream_t copy_stream = nullptr;  // host->device copies of streamed chunks
+  std::string err;
+  uint64_t launches = 0;
+  uint64_t chunk_rows = gpudb::kDefaultChunkRows;
+  std::unordered_map<std::string, gpudb::Buffer> scratch;
+  uint8_t* d_slots = nullptr;          // result slots (device)
+  uint8_t* h_slots = nullptr;          // their pinned host mirror
+  bool slot_busy[gpudb::kResultSlots] = {};
+  int next_slot = 0;
+  std::vector<std::function<int()>> pending;
+  std::vector<cudaStream_t> pending_streams;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace gpudb {
+
+int fail(gpudb_ctx* ctx, int code, const char* fmt, ...);
+int cuda_fail(gpudb_ctx* ctx, cudaError_t e, const char* what);
+
+#define GPUDB_CUDA(ctx, expr)                                  \
+  do {                                                         \
+    cudaError_t e_ = (expr);                                   \
+    if (e_ != cudaSuccess) return gpudb::cuda_fail(ctx, e_, #expr); \
+  } while (0)
+
+// Grow-only named scratch buffer on the device (never shrinks; freed at gpudb_destroy).
+int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out);
+
+cudaEvent_t event_get(gpudb_ctx* ctx);
+void event_put(gpudb_ctx* ctx, cudaEvent_t e);
+
+// One API call: picks the stream, owns a result slot and the timing events, and finishes
+// synchronously or by deferring the completion to gpudb_sync().
+class Call {
+ public:
+  Call(gpudb_ctx* ctx, const gpudb_exec* ex, gpudb_timing* t);
+  ~Call();
+  int begin(size_t result_bytes);          // acquires a slot and zeroes header + payload
+  cudaStream_t stream() const { return s_; }
+  uint32_t* status() const { return reinterpret_cast<uint32_t*>(dslot_); }
+  template <class T> T* result() const { return reinterpret_cast<T*>(dslot_ + kSlotHeader); }
+  void count_launch() { kernels_++; ctx_->launches++; }
+  void add_h2d(uint64_t b) { h2d_ += b; }
+  void add_chunk() { chunks_++; }
+  // Copies the result back and converts it with `convert(host_payload)`.
+  int finish(size_t result_bytes, std::function<int(const uint8_t*)> convert);
+  gpudb_ctx* ctx() const { return ctx_; }
+  int check_launch(const char* name);
+
+ private:
+  gpudb_ctx* ctx_;
+  cudaStream_t s_;
+  bool async_;
+  gpudb_timing* t_;
+  cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+  double host0_;
+  int slot_ = -1;
+  uint8_t* dslot_ = nullptr;
+  uint8_t* hslot_ = nullptr;
+  uint32_t kernels_ = 0, chunks_ = 0;
+  uint64_t h2d_ = 0, d2h_ = 0;
+  bool handed_off_ = false;
+};
+
+// Launch helper: counts the launch on the call and checks the launch error.
+#define GPUDB_LAUNCH(call, kernel, grid, block, smem, ...)                          \
+  do {                                                                              \
+    kernel<<<(grid), (block), (smem), (call).stream()>>>(__VA_ARGS__);             \
+    (call).count_launch();                                                          \
+    int rc_ = (call).check_launch(#kernel);                                         \
+    if (rc_ != GPUDB_OK) return rc_;                                                \
+  } while (0)
+
+// Status word -> error code (0 if clean).
+int status_to_error(gpudb_ctx* ctx, uint32_t st);
+
+// Columns of a lineitem chunk that a pipeline reads.
+enum : uint32_t {
+  LI_SHIP = 1u << 0, LI_QTY = 1u << 1, LI_EXT = 1u << 2, LI_DISC = 1u << 3, LI_TAX = 1u << 4,
+  LI_FLAG = 1u << 5, LI_STATUS = 1u << 6, LI_ORDER = 1u << 7, LI_PART = 1u << 8, LI_SUPP = 1u << 9
+};
+uint64_t lineitem_row_bytes(uint32_t mask);
+int lineitem_check(gpudb_ctx* ctx, const gpudb_lineitem* li, uint32_t mask);
+
+// Runs `dispatch(chunk)` once per chunk of a lineitem table. Device-resident tables are
+// one chunk that points at the caller's columns. Host-resident tables are copied in
+// chunks of `chunk_rows` rows into a ring of kStreamSlots device buffers on the copy
+// stream while the compute stream runs the previous chunk (events order the two).
+int stream_lineitem(Call& call, const gpudb_lineitem* li, uint32_t mask, uint64_t chunk_rows,
+                    const std::function<int(const gpudb_lineitem&)>& dispatch);
+
+}  // namespace gpudb

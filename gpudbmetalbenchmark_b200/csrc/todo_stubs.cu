@@ -1,0 +1,27 @@
+// Entry points whose kernels are not written yet: they report GPUDB_E_UNSUPPORTED.
+#include "engine.h"
+using namespace gpudb;
+extern "C" {
+int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer*, const gpudb_orders*, const gpudb_lineitem*,
+                       const gpudb_q3_params*, gpudb_q3_result*, gpudb_timing*, const gpudb_exec*) {
+  return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet");
+}
+int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part*, const gpudb_supplier*, const gpudb_partsupp*,
+                  const gpudb_orders*, const gpudb_lineitem*, const gpudb_q9_params*, gpudb_q9_group*, uint32_t,
+                  uint32_t*, gpudb_timing*, const gpudb_exec*) {
+  return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet");
+}
+int gpudb_select_lt(gpudb_ctx* ctx, const int32_t*, uint64_t, int32_t, uint32_t*, uint32_t*, uint64_t*,
+                    gpudb_timing*, const gpudb_exec*) { return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet"); }
+int gpudb_sum_i32(gpudb_ctx* ctx, const int32_t*, uint64_t, int64_t*, gpudb_timing*, const gpudb_exec*) {
+  return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet");
+}
+int gpudb_hash_join_count(gpudb_ctx* ctx, const int32_t*, uint64_t, const int32_t*, uint64_t, int32_t, uint64_t*,
+                          gpudb_timing*, const gpudb_exec*) { return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet"); }
+int gpudb_radix_partition(gpudb_ctx* ctx, const int32_t*, const int32_t*, uint64_t, int32_t, int32_t*, int32_t*,
+                          uint32_t*, gpudb_timing*, const gpudb_exec*) { return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet"); }
+int gpudb_radix_join_pairs(gpudb_ctx* ctx, const int32_t*, uint64_t, const int32_t*, uint64_t, int32_t*, int32_t*,
+                           uint64_t, uint64_t*, gpudb_timing*, const gpudb_exec*) {
+  return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet");
+}
+}

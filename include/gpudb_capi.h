@@ -1,0 +1,292 @@
+/*
+ * gpudb_capi.h -- C ABI of the B200 columnar query engine.
+ *
+ * One call per operator pipeline of the reference benchmark (nd-tung/GPUDBMetalBenchmark),
+ * which exposes each pipeline as `void runQnBenchmark(MTL::Device*, MTL::CommandQueue*,
+ * MTL::Library*)` (declared at src/infra.h:874-922, registered by name at
+ * src/main.cpp:158-188) and binds kernel arguments by `[[buffer(i)]]` index. Here the
+ * driver-level surface is the same set of pipelines, but every argument is a plain pointer
+ * or a plain-old-data struct, so any FFI (ctypes, cgo, JNI, N-API) can bind it.
+ *
+ * Conventions
+ *  - Every function returns int: GPUDB_OK (0) or a negative GPUDB_E_* code. The message of
+ *    the last failure on a context is returned by gpudb_last_error_string(). (The reference
+ *    prints to stderr and returns void, e.g. src/infra.h:178-186.)
+ *  - Column pointers are device pointers unless a struct's `location` says
+ *    GPUDB_MEM_HOST. A fact table in host memory is streamed to the GPU in chunks
+ *    (the reference's chunkedStreamLoop, src/infra.h:816-869).
+ *  - All arithmetic is exact integer arithmetic: money is int64 hundredths, products are
+ *    accumulated in int64 and group totals in int128.
+ *  - A context is thread-compatible: one host thread at a time per context.
+ *  - Calls are synchronous unless gpudb_exec.async is set; async calls complete, and fill
+ *    their host result structs, at the next gpudb_sync() on the context.
+ */
+#ifndef GPUDB_CAPI_H
+#define GPUDB_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUDB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------- */
+enum {
+  GPUDB_OK = 0,
+  GPUDB_E_INVALID = -1,     /* bad argument (null pointer, size, alignment, parameter) */
+  GPUDB_E_CUDA = -2,        /* a CUDA runtime call failed */
+  GPUDB_E_OOM = -3,         /* device or pinned-host allocation failed */
+  GPUDB_E_NODEVICE = -4,    /* no CUDA device, or not an sm_100 device */
+  GPUDB_E_CAPACITY = -5,    /* a hash table or partition overflowed on the device */
+  GPUDB_E_KEY_RANGE = -6,   /* a key outside the declared key range was seen on the device */
+  GPUDB_E_TIMEOUT = -7,     /* a bounded device-side wait ran out */
+  GPUDB_E_BUSY = -8,        /* serving: the request does not fit the admission budget */
+  GPUDB_E_CLOSED = -9,      /* serving: the request loop is closed */
+  GPUDB_E_UNSUPPORTED = -10
+};
+
+enum { GPUDB_MEM_DEVICE = 0, GPUDB_MEM_HOST = 1 };
+enum { GPUDB_JOIN_GLOBAL = 0, GPUDB_JOIN_RADIX = 1 };
+
+typedef struct gpudb_ctx gpudb_ctx;
+
+/* Signed 128-bit integer as two 64-bit halves (value = hi * 2^64 + lo). */
+typedef struct gpudb_i128 { uint64_t lo; int64_t hi; } gpudb_i128;
+
+/* Per-call execution options (NULL = synchronous on the context's stream). */
+typedef struct gpudb_exec {
+  int32_t async;      /* 1: enqueue only; results land at the next gpudb_sync() */
+  int32_t flags;      /* reserved, 0 */
+  void* stream;       /* cudaStream_t to launch on; NULL = the context's stream */
+} gpudb_exec;
+
+/* Timing of one call, filled when the call completes. gpu_ms is measured with CUDA events
+ * on the launching stream around all of the call's device work (copies included). */
+typedef struct gpudb_timing {
+  double gpu_ms;
+  double host_ms;          /* wall time of the call on the host */
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  uint32_t kernels;        /* kernel launches issued by the call */
+  uint32_t chunks;         /* streamed chunks (0 for HBM-resident inputs) */
+} gpudb_timing;
+
+/* ---- lifecycle (replaces the device/queue/library setup of src/main.cpp:76-156) -------- */
+int gpudb_create(int device, gpudb_ctx** out);
+int gpudb_destroy(gpudb_ctx* ctx);
+const char* gpudb_last_error_string(const gpudb_ctx* ctx);
+int gpudb_abi_version(void);
+/* Waits for all work enqueued on the context and completes pending async results. */
+int gpudb_sync(gpudb_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
+void* gpudb_stream(gpudb_ctx* ctx);
+/* Number of kernels this context has launched since creation. */
+uint64_t gpudb_kernel_launches(const gpudb_ctx* ctx);
+/* Context options (replaces the fixed ChunkConfig sizing of src/infra.h:42-57). */
+enum {
+  GPUDB_OPT_CHUNK_ROWS = 1   /* rows per streamed chunk of a host-resident fact table (default 64M) */
+};
+int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value);
+
+/* ---- memory (replaces MTL::Device::newBuffer and createFilledBuffer, src/infra.h:527-531) */
+int gpudb_device_alloc(gpudb_ctx* ctx, size_t bytes, void** out);
+int gpudb_device_free(gpudb_ctx* ctx, void* p);
+int gpudb_host_alloc(gpudb_ctx* ctx, size_t bytes, void** out);     /* pinned host memory */
+int gpudb_host_free(gpudb_ctx* ctx, void* p);
+int gpudb_copy(gpudb_ctx* ctx, void* dst, const void* src, size_t bytes); /* any direction */
+
+/* ---- column sets ------------------------------------------------------------------------ */
+/* Fact table (the reference's lineitem columns). Unused columns may be NULL. key_max fields
+ * give the largest key value of a join key column, used to size bitmaps and direct maps. */
+typedef struct gpudb_lineitem {
+  uint64_t n_rows;
+  int32_t location;            /* GPUDB_MEM_DEVICE or GPUDB_MEM_HOST */
+  int32_t order_key_max;
+  const int32_t* ship_date;    /* day number, 0 = first day of the date domain */
+  const int32_t* quantity;
+  const int64_t* ext_price;    /* hundredths */
+  const int32_t* discount;     /* hundredths: 0..10 means 0.00..0.10 */
+  const int32_t* tax;          /* hundredths */
+  const uint8_t* flag;         /* 0..2 */
+  const uint8_t* status;       /* 0..1 */
+  const int32_t* order_key;
+  const int32_t* part_key;
+  const int32_t* supp_key;
+} gpudb_lineitem;
+
+typedef struct gpudb_customer {
+  uint64_t n_rows; int32_t key_max; int32_t reserved;
+  const int32_t* cust_key; const uint8_t* segment;
+} gpudb_customer;
+
+typedef struct gpudb_orders {
+  uint64_t n_rows; int32_t key_max; int32_t cust_key_max;
+  const int32_t* order_key; const int32_t* cust_key; const int32_t* order_date;
+} gpudb_orders;
+
+typedef struct gpudb_part {
+  uint64_t n_rows; int32_t key_max; int32_t reserved;
+  const int32_t* part_key; const uint8_t* flag;      /* flag != 0: the part passes the filter */
+} gpudb_part;
+
+typedef struct gpudb_supplier {
+  uint64_t n_rows; int32_t key_max; int32_t reserved;
+  const int32_t* supp_key; const uint8_t* nation;
+} gpudb_supplier;
+
+typedef struct gpudb_partsupp {
+  uint64_t n_rows;
+  const int32_t* part_key; const int32_t* supp_key; const int64_t* supply_cost;
+} gpudb_partsupp;
+
+/* ---- synthetic data (replaces the .tbl loaders, src/infra.h:262-409) -------------------- */
+enum gpudb_column_id {
+  GPUDB_COL_LI_SHIP_DATE = 1, GPUDB_COL_LI_QUANTITY, GPUDB_COL_LI_EXT_PRICE,
+  GPUDB_COL_LI_DISCOUNT, GPUDB_COL_LI_TAX, GPUDB_COL_LI_FLAG, GPUDB_COL_LI_STATUS,
+  GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_PART_KEY, GPUDB_COL_LI_SUPP_KEY,
+  GPUDB_COL_CU_CUST_KEY = 20, GPUDB_COL_CU_SEGMENT,
+  GPUDB_COL_OR_ORDER_KEY = 30, GPUDB_COL_OR_CUST_KEY, GPUDB_COL_OR_ORDER_DATE,
+  GPUDB_COL_PA_PART_KEY = 40, GPUDB_COL_PA_FLAG,
+  GPUDB_COL_SU_SUPP_KEY = 50, GPUDB_COL_SU_NATION,
+  GPUDB_COL_PS_PART_KEY = 60, GPUDB_COL_PS_SUPP_KEY, GPUDB_COL_PS_SUPPLY_COST
+};
+enum { GPUDB_ORDERS_NONE = 0, GPUDB_ORDERS_CLUSTERED = 1, GPUDB_ORDERS_UNIFORM = 2 };
+
+typedef struct gpudb_gen_spec {
+  uint64_t seed;
+  uint64_t row_offset;         /* first row to generate (chunks and shards) */
+  uint64_t n_rows;             /* rows to generate */
+  int64_t n_orders;            /* orders table size (lineitem order keys) */
+  int64_t n_cust;              /* customer table size (orders cust keys) */
+  int64_t n_parts;             /* part table size */
+  int64_t n_supp;              /* supplier table size (a multiple of 4) */
+  int32_t order_mode;          /* GPUDB_ORDERS_* for lineitem order keys */
+  int32_t reserved;
+} gpudb_gen_spec;
+
+/* Writes rows [row_offset, row_offset+n_rows) of one column to dst, which is device memory
+ * (location GPUDB_MEM_DEVICE, generated by a kernel) or host memory (GPUDB_MEM_HOST,
+ * generated on the host cores). Both produce identical bytes. */
+int gpudb_generate(gpudb_ctx* ctx, const gpudb_gen_spec* spec, int32_t column,
+                   void* dst, int32_t location);
+/* Element size in bytes of a generated column, or 0 for an unknown column. */
+int gpudb_column_width(int32_t column);
+
+/* ---- Q6-like filtered sum (replaces runQ6Benchmark src/q6.cpp:8-120 and kernels
+ *      q6_filter_and_sum_stage1/2 kernels/q6.metal:12-70; streamed form replaces
+ *      runQ6BenchmarkSF100 src/q6.cpp:124-214) --------------------------------------- */
+typedef struct gpudb_q6_params {
+  int32_t ship_lo, ship_hi;    /* ship_date in [ship_lo, ship_hi) */
+  int32_t disc_lo, disc_hi;    /* discount in [disc_lo, disc_hi] */
+  int32_t qty_lt;              /* quantity < qty_lt */
+} gpudb_q6_params;
+typedef struct gpudb_q6_result { int64_t revenue; uint64_t rows_matched; } gpudb_q6_result;
+/* revenue = sum(ext_price * discount) over matching rows, in hundredths^2. */
+int gpudb_q6_sum(gpudb_ctx* ctx, const gpudb_lineitem* li, const gpudb_q6_params* p,
+                 gpudb_q6_result* out, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- Q1-like filter + 6-group aggregate (replaces runQ1Benchmark src/q1.cpp:8-173 and
+ *      q1_fused_kernel kernels/q1.metal:39-121; streamed form replaces runQ1BenchmarkSF100
+ *      src/q1.cpp:177-376) ------------------------------------------------------------ */
+typedef struct gpudb_q1_params { int32_t ship_le; int32_t reserved; } gpudb_q1_params;
+typedef struct gpudb_q1_group {
+  uint8_t flag, status; uint8_t reserved[6];
+  uint64_t count;
+  gpudb_i128 sum_qty;
+  gpudb_i128 sum_base_price;   /* sum(ext_price), hundredths */
+  gpudb_i128 sum_disc_price;   /* sum(ext_price*(100-discount)), hundredths^2 */
+  gpudb_i128 sum_charge;       /* sum(ext_price*(100-discount)*(100+tax)), hundredths^3 */
+  gpudb_i128 sum_discount;     /* sum(discount), hundredths (for avg_disc) */
+} gpudb_q1_group;
+typedef struct gpudb_q1_result {
+  uint32_t n_groups; uint32_t reserved;
+  gpudb_q1_group groups[6];    /* non-empty groups in (flag, status) order */
+} gpudb_q1_result;
+int gpudb_q1_group6(gpudb_ctx* ctx, const gpudb_lineitem* li, const gpudb_q1_params* p,
+                    gpudb_q1_result* out, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- Q3-like bitmap semi-join + hash join + per-order aggregate + top-k (replaces
+ *      runQ3Benchmark src/q3.cpp:8-173, kernels q3_build_customer_bitmap_kernel,
+ *      q3_build_orders_map_kernel/_ht_kernel, q3_probe_and_aggregate_*_kernel,
+ *      q3_compact_results_kernel kernels/q3.metal:43-340, and sortAndPrintQ3
+ *      src/infra.h:538-564; streamed form replaces runQ3BenchmarkSF100 src/q3.cpp:177-538) */
+#define GPUDB_Q3_MAX_K 64
+typedef struct gpudb_q3_params {
+  int32_t segment;             /* customer.segment == segment */
+  int32_t order_date_lt;       /* orders.order_date < order_date_lt */
+  int32_t ship_date_gt;        /* lineitem.ship_date > ship_date_gt */
+  int32_t k;                   /* rows of the top-k, 1..GPUDB_Q3_MAX_K */
+  int32_t join_mode;           /* GPUDB_JOIN_GLOBAL or GPUDB_JOIN_RADIX */
+  int32_t radix_bits;          /* radix mode: partition bits, 0 = chosen from the build size */
+} gpudb_q3_params;
+typedef struct gpudb_q3_row { int32_t order_key; int32_t order_date; int64_t revenue; } gpudb_q3_row;
+/* Rows ordered by revenue desc, order_date asc, order_key asc. revenue is in hundredths^2. */
+typedef struct gpudb_q3_result {
+  uint64_t n_groups;           /* orders with at least one joined lineitem row */
+  uint32_t n_rows; uint32_t reserved;
+  gpudb_q3_row rows[GPUDB_Q3_MAX_K];
+} gpudb_q3_result;
+int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_orders* od,
+                       const gpudb_lineitem* li, const gpudb_q3_params* p,
+                       gpudb_q3_result* out, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- Q9-like star join + (nation, year) aggregate (replaces runQ9Benchmark
+ *      src/q9.cpp:8-241, kernels q9_build_*_kernel and q9_probe_and_global_agg_kernel
+ *      kernels/q9.metal:44-289, postProcessQ9 src/infra.h:743-776; streamed form replaces
+ *      runQ9BenchmarkSF100 src/q9.cpp:245-557 and q9_probe_directorders_kernel
+ *      kernels/q9.metal:308-394) ------------------------------------------------------ */
+typedef struct gpudb_q9_params {
+  int32_t smem_slots;          /* per-block aggregation slots, 0 = default (power of two) */
+  int32_t global_slots;        /* global aggregation table slots, 0 = default (power of two) */
+  uint64_t chunk_rows;         /* host-resident lineitem: rows per streamed chunk, 0 = default */
+} gpudb_q9_params;
+typedef struct gpudb_q9_group { int32_t nation; int32_t year; int64_t profit; } gpudb_q9_group;
+/* profit = sum(ext_price*(100-discount) - supply_cost*quantity*100), hundredths^2.
+ * Groups are ordered by nation asc, year desc; *n_groups is the total number of groups and
+ * at most `capacity` of them are written. */
+int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_supplier* su,
+                  const gpudb_partsupp* ps, const gpudb_orders* od, const gpudb_lineitem* li,
+                  const gpudb_q9_params* p, gpudb_q9_group* out, uint32_t capacity,
+                  uint32_t* n_groups, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- microbenchmarks (replace runSelectionBenchmark / runAggregationBenchmark /
+ *      runJoinBenchmark src/microbenchmarks.cpp:8-251 and their kernels
+ *      kernels/microbenchmarks.metal:160-294) ------------------------------------------ */
+/* Rows with col[i] < value. out_bits (nullable, (n+31)/32 device words) receives a row
+ * bitmask; out_rows (nullable, device, capacity n) receives matching row ids in order. */
+int gpudb_select_lt(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int32_t value,
+                    uint32_t* out_bits, uint32_t* out_rows, uint64_t* count,
+                    gpudb_timing* t, const gpudb_exec* ex);
+/* Exact int64 sum of an int32 column. */
+int gpudb_sum_i32(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int64_t* sum,
+                  gpudb_timing* t, const gpudb_exec* ex);
+/* Number of probe rows whose key occurs among the build keys (hash_join_probe counts a
+ * probe row once, at its first match). mode: GPUDB_JOIN_GLOBAL or GPUDB_JOIN_RADIX. */
+int gpudb_hash_join_count(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n_build,
+                          const int32_t* probe_keys, uint64_t n_probe, int32_t mode,
+                          uint64_t* matches, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- radix partitioning (replaces sf100_radix_histogram / _prefix_sum / _scatter /
+ *      sf100_partition_join kernels/microbenchmarks.metal:15-156) ---------------------- */
+/* Partition p of a key is hash(key) & (2^bits - 1) with the reference's key hash
+ * (sf100_hash_key, kernels/common.h:81-87). Rows keep their input order inside a
+ * partition. offsets receives 2^bits + 1 device words (exclusive prefix of the sizes). */
+int gpudb_radix_partition(gpudb_ctx* ctx, const int32_t* keys, const int32_t* payload,
+                          uint64_t n, int32_t bits, int32_t* keys_out, int32_t* payload_out,
+                          uint32_t* offsets, gpudb_timing* t, const gpudb_exec* ex);
+/* All (build row, probe row) pairs with equal keys, via radix partitioning and per-partition
+ * shared-memory hash tables. Pairs are written in (probe row, build row) order; *n_pairs is
+ * the total, at most `capacity` pairs are written (device arrays). */
+int gpudb_radix_join_pairs(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n_build,
+                           const int32_t* probe_keys, uint64_t n_probe,
+                           int32_t* out_build_rows, int32_t* out_probe_rows,
+                           uint64_t capacity, uint64_t* n_pairs,
+                           gpudb_timing* t, const gpudb_exec* ex);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUDB_CAPI_H */

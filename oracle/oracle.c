@@ -1,0 +1,437 @@
+/*
+ * oracle.c -- CPU oracle (test infrastructure only; see oracle.h). Parity status: the
+ * query logic is pinned against the reference's own kernels compiled for the CPU
+ * (oracle/ref_harness.cpp) within float32 tolerance, since the reference computes in
+ * float32; exact integer results are pinned against an independent big-integer Python
+ * restatement (tests/golden/make_golden.py). The reference ships no golden vectors.
+ */
+#define _GNU_SOURCE
+#include "oracle.h"
+
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef __int128 i128;
+typedef unsigned __int128 u128;
+
+/* ------------------------------------------------------------------------------------
+ * Generator restatement: value(seed, stream, row) = F(K(seed, stream) + (row+1)*G) with
+ * F the SplitMix64 output function, K(seed, s) = F(seed*G + (s+1)*0xD1B54A32D192ED03),
+ * G = 0x9E3779B97F4A7C15, and uniform(lo, hi) = lo + floor(value * (hi-lo+1) / 2^64).
+ * ------------------------------------------------------------------------------------ */
+static uint64_t mix64(uint64_t x) {
+  x ^= x >> 30; x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27; x *= 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return x;
+}
+static const uint64_t G = 0x9E3779B97F4A7C15ull;
+static uint64_t stream_of(uint64_t seed, uint32_t s) { return mix64(seed * G + (uint64_t)(s + 1) * 0xD1B54A32D192ED03ull); }
+static int64_t unif(uint64_t key, uint64_t row, int64_t lo, int64_t hi) {
+  uint64_t v = mix64(key + (row + 1) * G);
+  uint64_t span = (uint64_t)(hi - lo + 1);
+  return lo + (int64_t)(uint64_t)(((u128)v * span) >> 64);
+}
+
+/* random stream ids (table*16 + column) */
+enum { S_SHIP = 16, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG, S_STATUS, S_OPICK, S_PART, S_SSLOT, S_RUN,
+       S_SEG = 32, S_OCUST = 48, S_ODATE, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
+
+static int32_t supp_of(int64_t part, int64_t j, int64_t n_supp) { return (int32_t)((part + j * (n_supp / 4)) % n_supp); }
+
+int or_gen_column(const or_spec* sp, int32_t column, void* dst) {
+  const uint64_t seed = sp->seed, off = sp->row_offset, n = sp->n_rows;
+  int32_t* i32 = (int32_t*)dst; int64_t* i64 = (int64_t*)dst; uint8_t* u8 = (uint8_t*)dst;
+  uint64_t i;
+  switch (column) {
+  case 1: { uint64_t k = stream_of(seed, S_SHIP); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, 2526); return 0; }
+  case 2: { uint64_t k = stream_of(seed, S_QTY); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 1, 50); return 0; }
+  case 3: { uint64_t kq = stream_of(seed, S_QTY), kp = stream_of(seed, S_PRICE);
+            for (i = 0; i < n; i++) i64[i] = unif(kq, off + i, 1, 50) * unif(kp, off + i, 90000, 209900); return 0; }
+  case 4: { uint64_t k = stream_of(seed, S_DISC); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, 10); return 0; }
+  case 5: { uint64_t k = stream_of(seed, S_TAX); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, 8); return 0; }
+  case 6: { uint64_t k = stream_of(seed, S_FLAG); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 2); return 0; }
+  case 7: { uint64_t k = stream_of(seed, S_STATUS); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 1); return 0; }
+  case 8:
+    if (sp->n_orders <= 0) return -1;
+    if (sp->order_mode == 2) {
+      uint64_t k = stream_of(seed, S_OPICK);
+      for (i = 0; i < n; i++) i32[i] = (int32_t)(4 * unif(k, off + i, 0, sp->n_orders - 1) + 1);
+      return 0;
+    } else if (sp->order_mode == 1) {
+      /* runs of 1..7 rows; run s belongs to order s mod n_orders */
+      uint64_t k = stream_of(seed, S_RUN), row = 0, s = 0, end = off + n;
+      while (row < end) {
+        int64_t len = unif(k, s, 1, 7);
+        int32_t key = (int32_t)(4 * (int64_t)(s % (uint64_t)sp->n_orders) + 1);
+        for (int64_t j = 0; j < len && row < end; j++, row++)
+          if (row >= off) i32[row - off] = key;
+        s++;
+      }
+      return 0;
+    }
+    return -1;
+  case 9: { if (sp->n_parts <= 0) return -1; uint64_t k = stream_of(seed, S_PART);
+            for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, sp->n_parts - 1); return 0; }
+  case 10: { if (sp->n_parts <= 0 || sp->n_supp < 4) return -1;
+             uint64_t kp = stream_of(seed, S_PART), ks = stream_of(seed, S_SSLOT);
+             for (i = 0; i < n; i++) i32[i] = supp_of(unif(kp, off + i, 0, sp->n_parts - 1), unif(ks, off + i, 0, 3), sp->n_supp);
+             return 0; }
+  case 20: case 30: case 40: case 50:
+    for (i = 0; i < n; i++) i32[i] = (column == 30) ? (int32_t)(4 * (off + i) + 1) : (int32_t)(off + i);
+    return 0;
+  case 21: { uint64_t k = stream_of(seed, S_SEG); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 4); return 0; }
+  case 31: { if (sp->n_cust <= 0) return -1; uint64_t k = stream_of(seed, S_OCUST);
+             for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, sp->n_cust - 1); return 0; }
+  case 32: { uint64_t k = stream_of(seed, S_ODATE); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, 2405); return 0; }
+  case 41: { uint64_t k = stream_of(seed, S_PFLAG); for (i = 0; i < n; i++) u8[i] = unif(k, off + i, 0, 999) < 55; return 0; }
+  case 51: { uint64_t k = stream_of(seed, S_NATION); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 24); return 0; }
+  case 60: for (i = 0; i < n; i++) i32[i] = (int32_t)((off + i) / 4); return 0;
+  case 61: if (sp->n_supp < 4) return -1;
+           for (i = 0; i < n; i++) i32[i] = supp_of((int64_t)((off + i) / 4), (int64_t)((off + i) % 4), sp->n_supp);
+           return 0;
+  case 62: { uint64_t k = stream_of(seed, S_COST); for (i = 0; i < n; i++) i64[i] = unif(k, off + i, 100, 100000); return 0; }
+  default: return -1;
+  }
+}
+
+/* ---- Q6: predicate and measure of kernels/q6.metal:36-44 (short-circuit &&), exact ---- */
+void or_q6(uint64_t n, const int32_t* ship, const int32_t* disc, const int32_t* qty,
+           const int64_t* ext, int32_t lo, int32_t hi, int32_t dlo, int32_t dhi, int32_t qlt,
+           int64_t* revenue, uint64_t* matched) {
+  int64_t rev = 0; uint64_t m = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    if (ship[i] >= lo && ship[i] < hi && disc[i] >= dlo && disc[i] <= dhi && qty[i] < qlt) {
+      rev += ext[i] * (int64_t)disc[i];
+      m++;
+    }
+  }
+  *revenue = rev; *matched = m;
+}
+
+/* ---- Q1: filter and binning of kernels/q1.metal:73-94 (bin = flag*2 + status), with the
+ *      measures exact instead of rounded per row ---------------------------------------- */
+static void put128(uint64_t* dst, i128 v) { dst[0] = (uint64_t)(u128)v; dst[1] = (uint64_t)((u128)v >> 64); }
+
+typedef struct q1acc { uint64_t cnt; i128 qty, base, disc, charge, dsum; } q1acc;
+
+static void q1_range(uint64_t b, uint64_t e, const int32_t* ship, const int32_t* qty, const int64_t* ext,
+                     const int32_t* disc, const int32_t* tax, const uint8_t* flag, const uint8_t* status,
+                     int32_t ship_le, q1acc* acc) {
+  for (uint64_t i = b; i < e; i++) {
+    if (ship[i] > ship_le) continue;
+    if (flag[i] > 2 || status[i] > 1) continue;
+    q1acc* a = &acc[flag[i] * 2 + status[i]];
+    i128 dp = (i128)ext[i] * (100 - disc[i]);
+    a->cnt++;
+    a->qty += qty[i];
+    a->base += ext[i];
+    a->disc += dp;
+    a->charge += dp * (100 + tax[i]);
+    a->dsum += disc[i];
+  }
+}
+
+static void q1_emit(const q1acc* acc, uint64_t* out) {
+  for (int g = 0; g < 6; g++) {
+    uint64_t* o = out + g * 11;
+    o[0] = acc[g].cnt;
+    put128(o + 1, acc[g].qty); put128(o + 3, acc[g].base); put128(o + 5, acc[g].disc);
+    put128(o + 7, acc[g].charge); put128(o + 9, acc[g].dsum);
+  }
+}
+
+void or_q1(uint64_t n, const int32_t* ship, const int32_t* qty, const int64_t* ext,
+           const int32_t* disc, const int32_t* tax, const uint8_t* flag, const uint8_t* status,
+           int32_t ship_le, uint64_t* out) {
+  q1acc acc[6]; memset(acc, 0, sizeof acc);
+  q1_range(0, n, ship, qty, ext, disc, tax, flag, status, ship_le, acc);
+  q1_emit(acc, out);
+}
+
+/* ---- threaded drivers for the timed CPU baseline --------------------------------------- */
+typedef struct mt_job {
+  uint64_t b, e; const int32_t *ship, *qty, *disc, *tax; const int64_t* ext;
+  const uint8_t *flag, *status; int32_t a0, a1, a2, a3, a4;
+  int64_t rev; uint64_t matched; q1acc acc[6];
+} mt_job;
+
+static void* q6_worker(void* p) {
+  mt_job* j = (mt_job*)p;
+  or_q6(j->e - j->b, j->ship + j->b, j->disc + j->b, j->qty + j->b, j->ext + j->b,
+        j->a0, j->a1, j->a2, j->a3, j->a4, &j->rev, &j->matched);
+  return NULL;
+}
+static void* q1_worker(void* p) {
+  mt_job* j = (mt_job*)p;
+  memset(j->acc, 0, sizeof j->acc);
+  q1_range(j->b, j->e, j->ship, j->qty, j->ext, j->disc, j->tax, j->flag, j->status, j->a0, j->acc);
+  return NULL;
+}
+
+static void run_jobs(int threads, uint64_t n, mt_job* base, void* (*fn)(void*), mt_job** out_jobs) {
+  if (threads < 1) threads = 1;
+  mt_job* jobs = (mt_job*)calloc((size_t)threads, sizeof(mt_job));
+  pthread_t* th = (pthread_t*)calloc((size_t)threads, sizeof(pthread_t));
+  for (int t = 0; t < threads; t++) {
+    jobs[t] = *base;
+    jobs[t].b = n * (uint64_t)t / (uint64_t)threads;
+    jobs[t].e = n * (uint64_t)(t + 1) / (uint64_t)threads;
+    pthread_create(&th[t], NULL, fn, &jobs[t]);
+  }
+  for (int t = 0; t < threads; t++) pthread_join(th[t], NULL);
+  free(th);
+  *out_jobs = jobs;
+}
+
+void or_q6_mt(int threads, uint64_t n, const int32_t* ship, const int32_t* disc,
+              const int32_t* qty, const int64_t* ext, int32_t lo, int32_t hi, int32_t dlo,
+              int32_t dhi, int32_t qlt, int64_t* revenue, uint64_t* matched) {
+  mt_job base; memset(&base, 0, sizeof base);
+  base.ship = ship; base.disc = disc; base.qty = qty; base.ext = ext;
+  base.a0 = lo; base.a1 = hi; base.a2 = dlo; base.a3 = dhi; base.a4 = qlt;
+  mt_job* jobs; if (threads < 1) threads = 1;
+  run_jobs(threads, n, &base, q6_worker, &jobs);
+  int64_t r = 0; uint64_t m = 0;
+  for (int t = 0; t < threads; t++) { r += jobs[t].rev; m += jobs[t].matched; }
+  free(jobs);
+  *revenue = r; *matched = m;
+}
+
+void or_q1_mt(int threads, uint64_t n, const int32_t* ship, const int32_t* qty,
+              const int64_t* ext, const int32_t* disc, const int32_t* tax,
+              const uint8_t* flag, const uint8_t* status, int32_t ship_le, uint64_t* out) {
+  mt_job base; memset(&base, 0, sizeof base);
+  base.ship = ship; base.qty = qty; base.ext = ext; base.disc = disc; base.tax = tax;
+  base.flag = flag; base.status = status; base.a0 = ship_le;
+  mt_job* jobs; if (threads < 1) threads = 1;
+  run_jobs(threads, n, &base, q1_worker, &jobs);
+  q1acc acc[6]; memset(acc, 0, sizeof acc);
+  for (int t = 0; t < threads; t++)
+    for (int g = 0; g < 6; g++) {
+      acc[g].cnt += jobs[t].acc[g].cnt; acc[g].qty += jobs[t].acc[g].qty;
+      acc[g].base += jobs[t].acc[g].base; acc[g].disc += jobs[t].acc[g].disc;
+      acc[g].charge += jobs[t].acc[g].charge; acc[g].dsum += jobs[t].acc[g].dsum;
+    }
+  free(jobs);
+  q1_emit(acc, out);
+}
+
+/* ---- Q3: customer bitmap (kernels/q3.metal:43-55), orders filter + map
+ *      (kernels/q3.metal:59-78), probe + per-order revenue (kernels/q3.metal:145-211),
+ *      top-k order of sortAndPrintQ3 (src/infra.h:544-564) plus order_key as the last key -- */
+typedef struct q3grp { int32_t key, date; int64_t rev; } q3grp;
+
+static int q3_cmp(const void* a, const void* b) {
+  const q3grp* x = (const q3grp*)a; const q3grp* y = (const q3grp*)b;
+  if (x->rev != y->rev) return x->rev > y->rev ? -1 : 1;
+  if (x->date != y->date) return x->date < y->date ? -1 : 1;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return 0;
+}
+
+uint64_t or_q3(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_seg, int32_t cu_key_max,
+               uint64_t n_or, const int32_t* or_key, const int32_t* or_cust,
+               const int32_t* or_date, int32_t or_key_max,
+               uint64_t n_li, const int32_t* li_order, const int32_t* li_ship,
+               const int64_t* li_ext, const int32_t* li_disc,
+               int32_t segment, int32_t date_lt, int32_t ship_gt, int32_t k,
+               int32_t* top_key, int32_t* top_date, int64_t* top_rev) {
+  uint8_t* cust_ok = (uint8_t*)calloc((size_t)cu_key_max + 1, 1);
+  for (uint64_t i = 0; i < n_cu; i++)
+    if (cu_seg[i] == segment) cust_ok[cu_key[i]] = 1;
+  int64_t* order_row = (int64_t*)malloc(((size_t)or_key_max + 1) * sizeof(int64_t));
+  for (int64_t i = 0; i <= or_key_max; i++) order_row[i] = -1;
+  for (uint64_t i = 0; i < n_or; i++)
+    if (or_date[i] < date_lt && or_cust[i] >= 0 && or_cust[i] <= cu_key_max && cust_ok[or_cust[i]])
+      order_row[or_key[i]] = (int64_t)i;
+  int64_t* rev = (int64_t*)calloc(n_or ? n_or : 1, sizeof(int64_t));
+  uint8_t* hit = (uint8_t*)calloc(n_or ? n_or : 1, 1);
+  for (uint64_t i = 0; i < n_li; i++) {
+    if (li_ship[i] <= ship_gt) continue;
+    int32_t key = li_order[i];
+    if (key < 0 || key > or_key_max) continue;
+    int64_t r = order_row[key];
+    if (r < 0) continue;
+    rev[r] += li_ext[i] * (int64_t)(100 - li_disc[i]);
+    hit[r] = 1;
+  }
+  uint64_t groups = 0;
+  for (uint64_t i = 0; i < n_or; i++) groups += hit[i];
+  q3grp* g = (q3grp*)malloc((groups ? groups : 1) * sizeof(q3grp));
+  uint64_t m = 0;
+  for (uint64_t i = 0; i < n_or; i++)
+    if (hit[i]) { g[m].key = or_key[i]; g[m].date = or_date[i]; g[m].rev = rev[i]; m++; }
+  qsort(g, groups, sizeof(q3grp), q3_cmp);
+  for (uint64_t i = 0; i < groups && i < (uint64_t)k; i++) {
+    top_key[i] = g[i].key; top_date[i] = g[i].date; top_rev[i] = g[i].rev;
+  }
+  free(g); free(hit); free(rev); free(order_row); free(cust_ok);
+  return groups;
+}
+
+/* ---- Q9: part filter (kernels/q9.metal:44-88, a flag column here), supplier -> nation
+ *      (kernels/q9.metal:91-104), partsupp (part, supp) -> cost (kernels/q9.metal:109-162),
+ *      orders -> year (kernels/q9.metal:165-189), probe chain and (nation<<16 | year)
+ *      grouping (kernels/q9.metal:223-288), order of postProcessQ9 (src/infra.h:756-759) -- */
+typedef struct kv64 { uint64_t key; int64_t val; uint8_t used; } kv64;
+
+static uint64_t slot_of(uint64_t key, uint64_t mask) { return mix64(key) & mask; }
+
+typedef struct q9grp { int32_t nation, year; int64_t profit; } q9grp;
+static int q9_cmp(const void* a, const void* b) {
+  const q9grp* x = (const q9grp*)a; const q9grp* y = (const q9grp*)b;
+  if (x->nation != y->nation) return x->nation < y->nation ? -1 : 1;
+  if (x->year != y->year) return x->year > y->year ? -1 : 1;
+  return 0;
+}
+
+uint32_t or_q9(uint64_t n_pa, const int32_t* pa_key, const uint8_t* pa_flag, int32_t pa_key_max,
+               uint64_t n_su, const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max,
+               uint64_t n_ps, const int32_t* ps_part, const int32_t* ps_supp, const int64_t* ps_cost,
+               uint64_t n_or, const int32_t* or_key, const int32_t* or_date, int32_t or_key_max,
+               uint64_t n_li, const int32_t* li_part, const int32_t* li_supp, const int32_t* li_order,
+               const int64_t* li_ext, const int32_t* li_disc, const int32_t* li_qty,
+               uint32_t cap, int32_t* g_nation, int32_t* g_year, int64_t* g_profit) {
+  uint8_t* part_ok = (uint8_t*)calloc((size_t)pa_key_max + 1, 1);
+  for (uint64_t i = 0; i < n_pa; i++) if (pa_flag[i]) part_ok[pa_key[i]] = 1;
+  int32_t* nation = (int32_t*)malloc(((size_t)su_key_max + 1) * sizeof(int32_t));
+  for (int64_t i = 0; i <= su_key_max; i++) nation[i] = -1;
+  for (uint64_t i = 0; i < n_su; i++) nation[su_key[i]] = su_nation[i];
+  /* (part, supp) -> cost, open addressing */
+  uint64_t cap_ps = 16; while (cap_ps < 2 * n_ps + 2) cap_ps <<= 1;
+  kv64* ps = (kv64*)calloc(cap_ps, sizeof(kv64));
+  for (uint64_t i = 0; i < n_ps; i++) {
+    if (ps_part[i] < 0 || ps_part[i] > pa_key_max || !part_ok[ps_part[i]]) continue;
+    uint64_t key = ((uint64_t)(uint32_t)ps_part[i] << 32) | (uint32_t)ps_supp[i];
+    uint64_t s = slot_of(key, cap_ps - 1);
+    while (ps[s].used && ps[s].key != key) s = (s + 1) & (cap_ps - 1);
+    ps[s].used = 1; ps[s].key = key; ps[s].val = ps_cost[i];
+  }
+  int32_t* year = (int32_t*)malloc(((size_t)or_key_max + 1) * sizeof(int32_t));
+  for (int64_t i = 0; i <= or_key_max; i++) year[i] = -1;
+  for (uint64_t i = 0; i < n_or; i++) year[or_key[i]] = 1992 + or_date[i] / 365;
+  uint64_t cap_g = 1u << 16;
+  kv64* grp = (kv64*)calloc(cap_g, sizeof(kv64));
+  uint32_t ngroups = 0;
+  for (uint64_t i = 0; i < n_li; i++) {
+    int32_t p = li_part[i];
+    if (p < 0 || p > pa_key_max || !part_ok[p]) continue;
+    int32_t s = li_supp[i];
+    if (s < 0 || s > su_key_max || nation[s] < 0) continue;
+    uint64_t key = ((uint64_t)(uint32_t)p << 32) | (uint32_t)s;
+    uint64_t h = slot_of(key, cap_ps - 1);
+    while (ps[h].used && ps[h].key != key) h = (h + 1) & (cap_ps - 1);
+    if (!ps[h].used) continue;
+    int32_t o = li_order[i];
+    if (o < 0 || o > or_key_max || year[o] < 0) continue;
+    int64_t profit = li_ext[i] * (int64_t)(100 - li_disc[i]) - ps[h].val * (int64_t)li_qty[i] * 100;
+    uint64_t gk = ((uint64_t)(uint32_t)nation[s] << 16) | (uint32_t)year[o];
+    uint64_t g = slot_of(gk, cap_g - 1);
+    while (grp[g].used && grp[g].key != gk) g = (g + 1) & (cap_g - 1);
+    if (!grp[g].used) { grp[g].used = 1; grp[g].key = gk; ngroups++; }
+    grp[g].val += profit;
+  }
+  q9grp* out = (q9grp*)malloc((ngroups ? ngroups : 1) * sizeof(q9grp));
+  uint32_t m = 0;
+  for (uint64_t g = 0; g < cap_g; g++)
+    if (grp[g].used) { out[m].nation = (int32_t)(grp[g].key >> 16); out[m].year = (int32_t)(grp[g].key & 0xFFFF); out[m].profit = grp[g].val; m++; }
+  qsort(out, ngroups, sizeof(q9grp), q9_cmp);
+  for (uint32_t i = 0; i < ngroups && i < cap; i++) { g_nation[i] = out[i].nation; g_year[i] = out[i].year; g_profit[i] = out[i].profit; }
+  free(out); free(grp); free(year); free(ps); free(nation); free(part_ok);
+  return ngroups;
+}
+
+/* ---- microbenchmarks: selection (kernels/microbenchmarks.metal:160-171), sum
+ *      (:178-220), join count (:225-294), radix partition (:15-99), pairs (:104-156) ---- */
+uint64_t or_select_lt(uint64_t n, const int32_t* col, int32_t value, uint32_t* bits, uint32_t* rows) {
+  uint64_t c = 0;
+  if (bits) memset(bits, 0, ((n + 31) / 32) * sizeof(uint32_t));
+  for (uint64_t i = 0; i < n; i++)
+    if (col[i] < value) {
+      if (bits) bits[i / 32] |= 1u << (i % 32);
+      if (rows) rows[c] = (uint32_t)i;
+      c++;
+    }
+  return c;
+}
+
+int64_t or_sum_i32(uint64_t n, const int32_t* col) {
+  int64_t s = 0;
+  for (uint64_t i = 0; i < n; i++) s += col[i];
+  return s;
+}
+
+static int cmp_i32(const void* a, const void* b) {
+  int32_t x = *(const int32_t*)a, y = *(const int32_t*)b;
+  return x < y ? -1 : x > y;
+}
+
+uint64_t or_join_count(uint64_t nb, const int32_t* bkeys, uint64_t np, const int32_t* pkeys) {
+  int32_t* s = (int32_t*)malloc((nb ? nb : 1) * sizeof(int32_t));
+  memcpy(s, bkeys, nb * sizeof(int32_t));
+  qsort(s, nb, sizeof(int32_t), cmp_i32);
+  uint64_t c = 0;
+  for (uint64_t i = 0; i < np; i++)
+    if (nb && bsearch(&pkeys[i], s, nb, sizeof(int32_t), cmp_i32)) c++;
+  free(s);
+  return c;
+}
+
+uint32_t or_key_hash(int32_t key) {
+  uint32_t h = (uint32_t)key;
+  h ^= h >> 16; h *= 0x45d9f3bu; h ^= h >> 16;
+  return h;
+}
+
+void or_radix_histogram(uint64_t n, const int32_t* keys, int32_t bits, uint32_t* hist) {
+  uint32_t parts = 1u << bits;
+  memset(hist, 0, parts * sizeof(uint32_t));
+  for (uint64_t i = 0; i < n; i++) hist[or_key_hash(keys[i]) & (parts - 1)]++;
+}
+
+void or_radix_partition(uint64_t n, const int32_t* keys, const int32_t* payload, int32_t bits,
+                        int32_t* keys_out, int32_t* payload_out, uint32_t* offsets) {
+  uint32_t parts = 1u << bits;
+  uint32_t* hist = (uint32_t*)calloc(parts, sizeof(uint32_t));
+  or_radix_histogram(n, keys, bits, hist);
+  uint32_t run = 0;
+  for (uint32_t p = 0; p < parts; p++) { offsets[p] = run; run += hist[p]; }
+  offsets[parts] = run;
+  uint32_t* cur = (uint32_t*)malloc(parts * sizeof(uint32_t));
+  memcpy(cur, offsets, parts * sizeof(uint32_t));
+  for (uint64_t i = 0; i < n; i++) {
+    uint32_t p = or_key_hash(keys[i]) & (parts - 1);
+    keys_out[cur[p]] = keys[i];
+    if (payload && payload_out) payload_out[cur[p]] = payload[i];
+    cur[p]++;
+  }
+  free(cur); free(hist);
+}
+
+typedef struct kidx { int32_t key; int32_t row; } kidx;
+static int cmp_kidx(const void* a, const void* b) {
+  const kidx* x = (const kidx*)a; const kidx* y = (const kidx*)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->row < y->row ? -1 : x->row > y->row;
+}
+
+uint64_t or_join_pairs(uint64_t nb, const int32_t* bkeys, uint64_t np, const int32_t* pkeys,
+                       uint64_t cap, int32_t* out_b, int32_t* out_p) {
+  kidx* s = (kidx*)malloc((nb ? nb : 1) * sizeof(kidx));
+  for (uint64_t i = 0; i < nb; i++) { s[i].key = bkeys[i]; s[i].row = (int32_t)i; }
+  qsort(s, nb, sizeof(kidx), cmp_kidx);
+  uint64_t c = 0;
+  for (uint64_t i = 0; i < np; i++) {
+    /* lower bound of pkeys[i] */
+    uint64_t lo = 0, hi = nb;
+    while (lo < hi) { uint64_t mid = (lo + hi) / 2; if (s[mid].key < pkeys[i]) lo = mid + 1; else hi = mid; }
+    for (uint64_t j = lo; j < nb && s[j].key == pkeys[i]; j++) {
+      if (c < cap) { out_b[c] = s[j].row; out_p[c] = (int32_t)i; }
+      c++;
+    }
+  }
+  free(s);
+  return c;
+}

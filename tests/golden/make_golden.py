@@ -1,0 +1,166 @@
+"""Writes tests/golden/golden.json: small seeded cases computed by an independent
+pure-Python (big-integer) restatement of the synthetic generator and of each pipeline.
+The oracle (oracle/oracle.c) and the engine are checked against these values.
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+
+M64 = (1 << 64) - 1
+G = 0x9E3779B97F4A7C15
+
+
+def fin(z):
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+    return z ^ (z >> 31)
+
+
+def stream(seed, col):
+    return fin((seed * G + (col + 1) * 0xD1B54A32D192ED03) & M64)
+
+
+def uniform(key, row, lo, hi):
+    v = fin((key + (row + 1) * G) & M64)
+    return lo + ((v * (hi - lo + 1)) >> 64)
+
+
+def column(name, n, seed, off=0, n_orders=0, n_cust=0, n_parts=0, n_supp=0, mode=0):
+    k = lambda s: stream(seed, s)  # noqa: E731
+    rows = range(off, off + n)
+    if name == "ship_date":
+        return [uniform(k(16), r, 0, 2526) for r in rows]
+    if name == "quantity":
+        return [uniform(k(17), r, 1, 50) for r in rows]
+    if name == "ext_price":
+        return [uniform(k(17), r, 1, 50) * uniform(k(18), r, 90000, 209900) for r in rows]
+    if name == "discount":
+        return [uniform(k(19), r, 0, 10) for r in rows]
+    if name == "tax":
+        return [uniform(k(20), r, 0, 8) for r in rows]
+    if name == "flag":
+        return [uniform(k(21), r, 0, 2) for r in rows]
+    if name == "status":
+        return [uniform(k(22), r, 0, 1) for r in rows]
+    if name == "order_key":
+        if mode == 2:
+            return [4 * uniform(k(23), r, 0, n_orders - 1) + 1 for r in rows]
+        out, s = [], 0
+        while len(out) < off + n:
+            out += [4 * (s % n_orders) + 1] * uniform(k(26), s, 1, 7)
+            s += 1
+        return out[off:off + n]
+    if name == "part_key":
+        return [uniform(k(24), r, 0, n_parts - 1) for r in rows]
+    if name == "supp_key":
+        return [(uniform(k(24), r, 0, n_parts - 1) + uniform(k(25), r, 0, 3) * (n_supp // 4)) % n_supp for r in rows]
+    if name == "segment":
+        return [uniform(k(32), r, 0, 4) for r in rows]
+    if name == "o_cust":
+        return [uniform(k(48), r, 0, n_cust - 1) for r in rows]
+    if name == "o_date":
+        return [uniform(k(49), r, 0, 2405) for r in rows]
+    if name == "p_flag":
+        return [1 if uniform(k(64), r, 0, 999) < 55 else 0 for r in rows]
+    if name == "nation":
+        return [uniform(k(80), r, 0, 24) for r in rows]
+    if name == "ps_cost":
+        return [uniform(k(96), r, 100, 100000) for r in rows]
+    raise KeyError(name)
+
+
+def q6(li, lo=365, hi=730, dlo=5, dhi=7, qlt=24):
+    rev = cnt = 0
+    for s, d, q, e in zip(li["ship_date"], li["discount"], li["quantity"], li["ext_price"]):
+        if lo <= s < hi and dlo <= d <= dhi and q < qlt:
+            rev += e * d
+            cnt += 1
+    return [rev, cnt]
+
+
+def q1(li, ship_le=2436):
+    g = {}
+    for s, q, e, d, t, f, st in zip(*(li[c] for c in ("ship_date", "quantity", "ext_price", "discount", "tax",
+                                                       "flag", "status"))):
+        if s > ship_le:
+            continue
+        a = g.setdefault("%d%d" % (f, st), [0, 0, 0, 0, 0, 0])
+        a[0] += 1
+        a[1] += q
+        a[2] += e
+        a[3] += e * (100 - d)
+        a[4] += e * (100 - d) * (100 + t)
+        a[5] += d
+    return {k: [str(x) for x in v] for k, v in sorted(g.items())}
+
+
+def q3(n_cu, n_or, n_li, seed, segment=1, date_lt=1170, ship_gt=1170, k=10):
+    seg = column("segment", n_cu, seed)
+    ocust = column("o_cust", n_or, seed, n_cust=n_cu)
+    odate = column("o_date", n_or, seed)
+    okey = [4 * i + 1 for i in range(n_or)]
+    li = {c: column(c, n_li, seed, n_orders=n_or, mode=1) for c in ("order_key", "ship_date", "ext_price", "discount")}
+    good = {okey[i]: odate[i] for i in range(n_or) if odate[i] < date_lt and seg[ocust[i]] == segment}
+    rev = {}
+    for key, s, e, d in zip(li["order_key"], li["ship_date"], li["ext_price"], li["discount"]):
+        if s > ship_gt and key in good:
+            rev[key] = rev.get(key, 0) + e * (100 - d)
+    rows = sorted(((key, good[key], r) for key, r in rev.items()), key=lambda x: (-x[2], x[1], x[0]))
+    return {"groups": len(rows), "top": [[a, b, str(c)] for a, b, c in rows[:k]]}
+
+
+def q9(n_pa, n_su, n_or, n_li, seed):
+    pflag = column("p_flag", n_pa, seed)
+    nation = column("nation", n_su, seed)
+    cost = column("ps_cost", 4 * n_pa, seed)
+    pscost = {(r // 4, (r // 4 + (r % 4) * (n_su // 4)) % n_su): cost[r] for r in range(4 * n_pa)}
+    odate = column("o_date", n_or, seed)
+    year = {4 * i + 1: 1992 + odate[i] // 365 for i in range(n_or)}
+    li = {c: column(c, n_li, seed, n_orders=n_or, n_parts=n_pa, n_supp=n_su, mode=2)
+          for c in ("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity")}
+    g = {}
+    for p, s, o, e, d, q in zip(*(li[c] for c in ("part_key", "supp_key", "order_key", "ext_price", "discount",
+                                                   "quantity"))):
+        if not pflag[p] or (p, s) not in pscost or o not in year:
+            continue
+        key = (nation[s], year[o])
+        g[key] = g.get(key, 0) + e * (100 - d) - pscost[(p, s)] * q * 100
+    rows = sorted(g.items(), key=lambda kv: (kv[0][0], -kv[0][1]))
+    return [[a, b, str(v)] for (a, b), v in rows]
+
+
+def main():
+    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}}
+    # generator: first values and column sums for two seeds and a shifted window
+    for seed, off in ((42, 0), (7, 1000)):
+        cols = {}
+        for name in ("ship_date", "quantity", "ext_price", "discount", "tax", "flag", "status"):
+            v = column(name, 64, seed, off)
+            cols[name] = {"head": v[:8], "sum": sum(v)}
+        for name in ("order_key",):
+            v1 = column(name, 64, seed, off, n_orders=50, mode=1)
+            v2 = column(name, 64, seed, off, n_orders=50, mode=2)
+            cols["order_key_clustered"] = {"head": v1[:8], "sum": sum(v1)}
+            cols["order_key_uniform"] = {"head": v2[:8], "sum": sum(v2)}
+        v = column("supp_key", 64, seed, off, n_parts=1000, n_supp=100)
+        cols["supp_key"] = {"head": v[:8], "sum": sum(v)}
+        out["generator"]["%d_%d" % (seed, off)] = cols
+    for n, seed in ((3000, 42), (2500, 9)):
+        li = {c: column(c, n, seed) for c in ("ship_date", "quantity", "ext_price", "discount", "tax", "flag",
+                                              "status")}
+        out["q6"]["%d_%d" % (n, seed)] = q6(li)
+        out["q6"]["%d_%d_wide" % (n, seed)] = q6(li, 0, 2527, 0, 10, 51)
+        out["q1"]["%d_%d" % (n, seed)] = q1(li)
+        out["q1"]["%d_%d_cut100" % (n, seed)] = q1(li, 100)
+    out["q3"]["300_1200_4800_42"] = q3(300, 1200, 4800, 42)
+    out["q3"]["200_900_3000_5_seg3"] = q3(200, 900, 3000, 5, segment=3, date_lt=2000, ship_gt=300, k=20)
+    out["q9"]["400_40_1500_6000_42"] = q9(400, 40, 1500, 6000, 42)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(path)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,230 @@
+"""ctypes access to the CPU oracle (oracle/_build/liboracle.so) and to the reference's own
+kernels compiled for the CPU (oracle/_ref/libgpudbref.so). Test infrastructure only."""
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgpudbref.so")
+
+WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 20: 4, 21: 1, 30: 4, 31: 4, 32: 4,
+         40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
+DT = {1: np.uint8, 4: np.int32, 8: np.int64}
+
+
+class Spec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("row_offset", C.c_uint64), ("n_rows", C.c_uint64),
+                ("n_orders", C.c_int64), ("n_cust", C.c_int64), ("n_parts", C.c_int64),
+                ("n_supp", C.c_int64), ("order_mode", C.c_int32), ("reserved", C.c_int32)]
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+V, U64, I32, U32, I64 = C.c_void_p, C.c_uint64, C.c_int32, C.c_uint32, C.c_int64
+ORACLE_ARGS = {
+    "or_gen_column": [V, I32, V],
+    "or_q6": [U64, V, V, V, V, I32, I32, I32, I32, I32, V, V],
+    "or_q6_mt": [C.c_int, U64, V, V, V, V, I32, I32, I32, I32, I32, V, V],
+    "or_q1": [U64, V, V, V, V, V, V, V, I32, V],
+    "or_q1_mt": [C.c_int, U64, V, V, V, V, V, V, V, I32, V],
+    "or_q3": [U64, V, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, I32, I32, V, V, V],
+    "or_q9": [U64, V, V, I32, U64, V, V, I32, U64, V, V, V, U64, V, V, I32, U64, V, V, V, V, V, V, U32, V, V, V],
+    "or_select_lt": [U64, V, I32, V, V],
+    "or_sum_i32": [U64, V],
+    "or_join_count": [U64, V, U64, V],
+    "or_key_hash": [I32],
+    "or_radix_histogram": [U64, V, I32, V],
+    "or_radix_partition": [U64, V, V, I32, V, V, V],
+    "or_join_pairs": [U64, V, U64, V, U64, V, V],
+}
+REF_ARGS = {
+    "ref_q6": [U64, V, V, V, V, I32, I32, I32, I32, I32, C.c_int, C.c_int],
+    "ref_q1": [U64, V, V, V, V, V, V, V, I32, C.c_int, C.c_int, V],
+    "ref_q3": [U64, V, V, U64, V, V, V, U64, V, V, V, V, I32, I32, I32, C.c_int, C.c_int, V, V, V, U32],
+    "ref_q9": [U64, V, V, U64, V, V, U64, V, V, V, U64, V, V, U64, V, V, V, V, V, V, C.c_int, C.c_int, V, V, V, U32],
+    "ref_select_lt": [U64, V, I32, V],
+    "ref_sum": [U64, V, C.c_int, C.c_int],
+    "ref_join_count": [U64, V, U64, V],
+    "ref_radix_partition": [U64, V, V, V, V, V, V],
+    "ref_partition_join": [U64, V, U64, V, V, V, U32],
+}
+
+
+def build():
+    import subprocess
+    import sys
+    subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "build.py")], check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+_or = None
+_ref = None
+
+
+def oracle():
+    global _or
+    if _or is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        _or = C.CDLL(ORACLE_SO)
+        for name, args in ORACLE_ARGS.items():
+            getattr(_or, name).argtypes = args
+        _or.or_key_hash.restype = C.c_uint32
+        _or.or_q3.restype = C.c_uint64
+        _or.or_q9.restype = C.c_uint32
+        _or.or_select_lt.restype = C.c_uint64
+        _or.or_sum_i32.restype = C.c_int64
+        _or.or_join_count.restype = C.c_uint64
+        _or.or_join_pairs.restype = C.c_uint64
+    return _or
+
+
+def reference():
+    """The reference's kernels on the CPU, or None where they were never built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        _ref = C.CDLL(REF_SO)
+        for name, args in REF_ARGS.items():
+            getattr(_ref, name).argtypes = args
+        _ref.ref_q6.restype = C.c_float
+        _ref.ref_sum.restype = C.c_float
+        _ref.ref_q3.restype = C.c_uint32
+        _ref.ref_q9.restype = C.c_uint32
+        _ref.ref_join_count.restype = C.c_uint32
+        _ref.ref_partition_join.restype = C.c_uint32
+    return _ref
+
+
+# ---- generator ---------------------------------------------------------------------------
+def gen(column, n_rows, seed=42, row_offset=0, n_orders=0, n_cust=0, n_parts=0, n_supp=0, order_mode=0):
+    out = np.empty(n_rows, dtype=DT[WIDTH[column]])
+    spec = Spec(seed, row_offset, n_rows, n_orders, n_cust, n_parts, n_supp, order_mode, 0)
+    rc = oracle().or_gen_column(C.byref(spec), column, out.ctypes.data)
+    assert rc == 0, "oracle generator rejected column %d" % column
+    return out
+
+
+def lineitem(n, seed=42, n_orders=0, order_mode=0, n_parts=0, n_supp=0, row_offset=0,
+             cols=("ship_date", "quantity", "ext_price", "discount", "tax", "flag", "status")):
+    ids = dict(ship_date=1, quantity=2, ext_price=3, discount=4, tax=5, flag=6, status=7, order_key=8,
+               part_key=9, supp_key=10)
+    return {c: gen(ids[c], n, seed, row_offset, n_orders, 0, n_parts, n_supp, order_mode) for c in cols}
+
+
+def q3_tables(n_cu, n_or, n_li, seed=42):
+    cu = dict(cust_key=gen(20, n_cu, seed), segment=gen(21, n_cu, seed))
+    od = dict(order_key=gen(30, n_or, seed), cust_key=gen(31, n_or, seed, n_cust=n_cu), order_date=gen(32, n_or, seed))
+    li = lineitem(n_li, seed, n_orders=n_or, order_mode=1, cols=("order_key", "ship_date", "ext_price", "discount"))
+    return cu, od, li
+
+
+def q9_tables(n_pa, n_su, n_or, n_li, seed=42):
+    pa = dict(part_key=gen(40, n_pa, seed), flag=gen(41, n_pa, seed))
+    su = dict(supp_key=gen(50, n_su, seed), nation=gen(51, n_su, seed))
+    n_ps = 4 * n_pa
+    ps = dict(part_key=gen(60, n_ps, seed), supp_key=gen(61, n_ps, seed, n_supp=n_su),
+              supply_cost=gen(62, n_ps, seed))
+    od = dict(order_key=gen(30, n_or, seed), order_date=gen(32, n_or, seed))
+    li = lineitem(n_li, seed, n_orders=n_or, order_mode=2, n_parts=n_pa, n_supp=n_su,
+                  cols=("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity"))
+    return pa, su, ps, od, li
+
+
+# ---- pipelines ---------------------------------------------------------------------------
+def q6(li, lo=365, hi=730, dlo=5, dhi=7, qlt=24, threads=0):
+    rev, m = C.c_int64(), C.c_uint64()
+    n = len(li["ship_date"])
+    args = (n, _p(li["ship_date"]), _p(li["discount"]), _p(li["quantity"]), _p(li["ext_price"]),
+            lo, hi, dlo, dhi, qlt, C.byref(rev), C.byref(m))
+    if threads:
+        oracle().or_q6_mt(threads, *args)
+    else:
+        oracle().or_q6(*args)
+    return rev.value, m.value
+
+
+def _i128(lo, hi):
+    v = (int(hi) << 64) | int(lo)
+    return v - (1 << 128) if v >> 127 else v
+
+
+def q1(li, ship_le=2436, threads=0):
+    out = np.zeros(66, dtype=np.uint64)
+    n = len(li["ship_date"])
+    args = (n, _p(li["ship_date"]), _p(li["quantity"]), _p(li["ext_price"]), _p(li["discount"]), _p(li["tax"]),
+            _p(li["flag"]), _p(li["status"]), ship_le, out.ctypes.data)
+    if threads:
+        oracle().or_q1_mt(threads, *args)
+    else:
+        oracle().or_q1(*args)
+    res = {}
+    for g in range(6):
+        o = out[g * 11:(g + 1) * 11]
+        if o[0] == 0:
+            continue
+        res[(g // 2, g % 2)] = dict(count=int(o[0]), sum_qty=_i128(o[1], o[2]), sum_base_price=_i128(o[3], o[4]),
+                                    sum_disc_price=_i128(o[5], o[6]), sum_charge=_i128(o[7], o[8]),
+                                    sum_discount=_i128(o[9], o[10]))
+    return res
+
+
+def q3(cu, od, li, segment=1, date_lt=1170, ship_gt=1170, k=10, cu_key_max=None, or_key_max=None):
+    cu_key_max = int(cu["cust_key"].max()) if cu_key_max is None else cu_key_max
+    or_key_max = int(od["order_key"].max()) if or_key_max is None else or_key_max
+    k = max(k, 1)
+    tk, td, tr = np.zeros(k, np.int32), np.zeros(k, np.int32), np.zeros(k, np.int64)
+    n = oracle().or_q3(len(cu["cust_key"]), _p(cu["cust_key"]), _p(cu["segment"]), cu_key_max,
+                       len(od["order_key"]), _p(od["order_key"]), _p(od["cust_key"]), _p(od["order_date"]), or_key_max,
+                       len(li["order_key"]), _p(li["order_key"]), _p(li["ship_date"]), _p(li["ext_price"]),
+                       _p(li["discount"]), segment, date_lt, ship_gt, k, tk.ctypes.data, td.ctypes.data,
+                       tr.ctypes.data)
+    m = min(n, k)
+    return [(int(tk[i]), int(td[i]), int(tr[i])) for i in range(m)], int(n)
+
+
+def q9(pa, su, ps, od, li, cap=4096):
+    gn, gy, gp = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap, np.int64)
+    n = oracle().or_q9(len(pa["part_key"]), _p(pa["part_key"]), _p(pa["flag"]), int(pa["part_key"].max()),
+                       len(su["supp_key"]), _p(su["supp_key"]), _p(su["nation"]), int(su["supp_key"].max()),
+                       len(ps["part_key"]), _p(ps["part_key"]), _p(ps["supp_key"]), _p(ps["supply_cost"]),
+                       len(od["order_key"]), _p(od["order_key"]), _p(od["order_date"]), int(od["order_key"].max()),
+                       len(li["part_key"]), _p(li["part_key"]), _p(li["supp_key"]), _p(li["order_key"]),
+                       _p(li["ext_price"]), _p(li["discount"]), _p(li["quantity"]), cap, gn.ctypes.data,
+                       gy.ctypes.data, gp.ctypes.data)
+    m = min(n, cap)
+    return [(int(gn[i]), int(gy[i]), int(gp[i])) for i in range(m)], int(n)
+
+
+def select_lt(col, value):
+    n = len(col)
+    bits = np.zeros((n + 31) // 32, np.uint32)
+    rows = np.zeros(max(n, 1), np.uint32)
+    c = oracle().or_select_lt(n, _p(col), value, bits.ctypes.data, rows.ctypes.data)
+    return int(c), bits, rows[:c]
+
+
+def sum_i32(col):
+    return int(oracle().or_sum_i32(len(col), _p(col)))
+
+
+def join_count(b, p):
+    return int(oracle().or_join_count(len(b), _p(b), len(p), _p(p)))
+
+
+def radix_partition(keys, payload, bits):
+    n = len(keys)
+    ko, po = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    off = np.zeros((1 << bits) + 1, np.uint32)
+    oracle().or_radix_partition(n, _p(keys), _p(payload), bits, ko.ctypes.data, po.ctypes.data, off.ctypes.data)
+    return ko, po, off
+
+
+def join_pairs(b, p, cap=None):
+    cap = cap if cap is not None else len(p) * 8 + 16
+    ob, op = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+    n = int(oracle().or_join_pairs(len(b), _p(b), len(p), _p(p), cap, ob.ctypes.data, op.ctypes.data))
+    return ob[:min(n, cap)], op[:min(n, cap)], n

@@ -1,0 +1,204 @@
+"""Parity of the sm_100a generator and scan kernels (Q6-like, Q1-like) against the CPU
+oracle, bit-exact, through the C ABI. Edge cases follow the reference's inputs: empty and
+ragged tables, unaligned column starts, all/none/one row passing, maximum values, one
+group, streamed host tables with ragged chunks, and the full 60M-row configuration."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gpudbmetalbenchmark_b200 import capi
+from gpudbmetalbenchmark_b200.engine import Q1_COLS
+
+pytestmark = pytest.mark.gpu
+
+GEN_CASES = [  # column id, generator kwargs
+    (1, {}), (2, {}), (3, {}), (4, {}), (5, {}), (6, {}), (7, {}),
+    (8, dict(n_orders=1000, order_mode=1)), (8, dict(n_orders=1000, order_mode=2)),
+    (9, dict(n_parts=5000)), (10, dict(n_parts=5000, n_supp=400)),
+    (20, {}), (21, {}), (30, {}), (31, dict(n_cust=777)), (32, {}), (40, {}), (41, {}), (50, {}), (51, {}),
+    (60, {}), (61, dict(n_supp=400)), (62, {}),
+]
+
+
+@pytest.mark.parametrize("col,kw", GEN_CASES)
+@pytest.mark.parametrize("n,off", [(1, 0), (4099, 0), (100_000, 12_345)])
+def test_device_generator_matches_oracle(engine, orc, col, kw, n, off):
+    w = engine.lib.gpudb_column_width(col)
+    dptr = engine.device_array(n * w)
+    spec = capi.GenSpec(seed=17, row_offset=off, n_rows=n, order_mode=kw.get("order_mode", 0),
+                        n_orders=kw.get("n_orders", 0), n_cust=kw.get("n_cust", 0), n_parts=kw.get("n_parts", 0),
+                        n_supp=kw.get("n_supp", 0))
+    engine._check(engine.lib.gpudb_generate(engine.ctx, C.byref(spec), col, dptr, capi.MEM_DEVICE))
+    got = engine.to_host(dptr, n, orc.DT[w])
+    engine.device_free(dptr)
+    want = orc.gen(col, n, 17, off, **kw)
+    host = np.empty_like(want)
+    engine._check(engine.lib.gpudb_generate(None, C.byref(spec), col, host.ctypes.data, capi.MEM_HOST))
+    assert np.array_equal(got, want)
+    assert np.array_equal(host, want)
+
+
+def upload_li(engine, li):
+    return engine.upload("lineitem", li)
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 4, 5, 31, 33, 127, 129, 1000, 4097, 100_003])
+def test_q6_q1_small_sizes(engine, orc, n):
+    li = orc.lineitem(n, seed=n + 1)
+    t = upload_li(engine, li)
+    try:
+        assert engine.q6(t) == orc.q6(li)
+        assert engine.q6(t, 0, 2527, 0, 10, 51) == orc.q6(li, 0, 2527, 0, 10, 51)
+        assert engine.q1(t) == orc.q1(li)
+        assert engine.q1(t, 100) == orc.q1(li, 100)
+    finally:
+        engine.free(t)
+
+
+@pytest.mark.parametrize("off", [1, 2, 3, 5])
+def test_unaligned_column_starts(engine, orc, off):
+    n = 50_001
+    li = orc.lineitem(n, seed=5)
+    t = upload_li(engine, li)
+    try:
+        view = t.lineitem(n_rows=n - off, row_offset=off)
+        sub = {k: v[off:] for k, v in li.items()}
+        assert engine.q6(view) == orc.q6(sub)
+        assert engine.q1(view) == orc.q1(sub)
+    finally:
+        engine.free(t)
+
+
+def test_predicate_edges(engine, orc):
+    n = 70_000
+    li = orc.lineitem(n, seed=9)
+    t = upload_li(engine, li)
+    try:
+        # all rows pass / none pass / exactly one row passes
+        assert engine.q6(t, 0, 2527, 0, 10, 51) == orc.q6(li, 0, 2527, 0, 10, 51)
+        assert engine.q6(t, 5, 5, 0, 10, 51) == (0, 0)
+        r = int(np.argmax(li["ship_date"]))
+        s = int(li["ship_date"][r])
+        one = orc.q6(li, s, s + 1, 0, 10, 51)
+        assert engine.q6(t, s, s + 1, 0, 10, 51) == one
+        assert engine.q1(t, -1) == {}
+        assert engine.q1(t, 2526) == orc.q1(li, 2526)
+    finally:
+        engine.free(t)
+
+
+def test_max_values_and_single_group(engine, orc):
+    n = 40_000
+    li = orc.lineitem(n, seed=10)
+    li["ext_price"][:] = 50 * 209900
+    li["quantity"][:] = 50
+    li["discount"][:] = 0
+    li["tax"][:] = 8
+    li["flag"][:] = 2
+    li["status"][:] = 1
+    t = upload_li(engine, li)
+    try:
+        got = engine.q1(t)
+        assert list(got) == [(2, 1)]
+        assert got == orc.q1(li)
+    finally:
+        engine.free(t)
+    # the edge of the exact-arithmetic domain
+    li["ext_price"][:] = (1 << 36) - 1
+    li["discount"][:] = 100
+    li["tax"][:] = 100
+    li["quantity"][:] = 65535
+    t = upload_li(engine, li)
+    try:
+        assert engine.q1(t) == orc.q1(li)
+    finally:
+        engine.free(t)
+
+
+def test_domain_violation_is_reported(engine, orc):
+    li = orc.lineitem(1000, seed=3)
+    li["discount"][17] = 101
+    li["ship_date"][17] = 0
+    t = upload_li(engine, li)
+    try:
+        with pytest.raises(capi.GpudbError) as e:
+            engine.q1(t)
+        assert e.value.code == capi.E_INVALID
+        # rows outside the filter do not count
+        li["ship_date"][17] = 2500
+        t2 = upload_li(engine, li)
+        assert engine.q1(t2) == orc.q1(li)
+        engine.free(t2)
+    finally:
+        engine.free(t)
+
+
+def test_bad_arguments(engine):
+    li = capi.Lineitem()
+    li.n_rows = 10
+    li.location = capi.MEM_DEVICE
+    with pytest.raises(capi.GpudbError) as e:
+        engine.q6(li)
+    assert e.value.code == capi.E_INVALID
+    li.location = 7
+    with pytest.raises(capi.GpudbError):
+        engine.q1(li)
+
+
+@pytest.mark.parametrize("chunk", [16, 1000, 4096, 33_333])
+def test_streamed_host_table(engine, orc, chunk):
+    n = 100_003
+    li = orc.lineitem(n, seed=21)
+    t = engine.upload("lineitem", li, location=capi.MEM_HOST)
+    try:
+        engine.set_chunk_rows(chunk)
+        tm = capi.Timing()
+        assert engine.q6(t, timing=tm) == orc.q6(li)
+        assert tm.chunks == (n + ((chunk + 15) // 16 * 16) - 1) // ((chunk + 15) // 16 * 16)
+        assert tm.h2d_bytes == 20 * n
+        assert engine.q1(t) == orc.q1(li)
+    finally:
+        engine.set_chunk_rows(64 << 20)
+        engine.free(t)
+
+
+def test_async_calls_complete_at_sync(engine, orc):
+    n = 200_000
+    li = orc.lineitem(n, seed=4)
+    t = upload_li(engine, li)
+    try:
+        before = engine.launches()
+        outs6 = [capi.Q6Result() for _ in range(40)]
+        outs1 = [capi.Q1Result() for _ in range(40)]
+        tms = [capi.Timing() for _ in range(40)]
+        for i in range(40):
+            engine.q6(t, ship_lo=i * 50, ship_hi=i * 50 + 400, async_=True, out=outs6[i], timing=tms[i])
+            engine.q1(t, ship_le=i * 60, async_=True, out=outs1[i])
+        engine.sync()
+        assert engine.launches() - before >= 80
+        from gpudbmetalbenchmark_b200.engine import q1_to_dict
+        for i in range(40):
+            assert (outs6[i].revenue, outs6[i].rows_matched) == orc.q6(li, i * 50, i * 50 + 400)
+            assert q1_to_dict(outs1[i]) == orc.q1(li, i * 60)
+            assert tms[i].kernels == 1 and tms[i].gpu_ms > 0
+    finally:
+        engine.free(t)
+
+
+def test_full_size_60m_bit_exact(engine, orc):
+    """Config 1 at its full size: 60M rows generated on the device, both scans bit-exact
+    against the oracle run on the same rows generated on the host."""
+    n = 60_000_000
+    t = engine.generate("lineitem", n, seed=42, columns=Q1_COLS)
+    try:
+        li = orc.lineitem(n, seed=42)
+        assert engine.q6(t) == orc.q6(li, threads=8)
+        assert engine.q1(t) == orc.q1(li, threads=8)
+        # linearity: the two halves add up to the whole
+        h = n // 2 + 3
+        a = engine.q6(t.lineitem(n_rows=h))
+        b = engine.q6(t.lineitem(n_rows=n - h, row_offset=h))
+        assert (a[0] + b[0], a[1] + b[1]) == engine.q6(t)
+    finally:
+        engine.free(t)
