@@ -14,7 +14,8 @@ enum : uint32_t {
   ST_CAPACITY = 1u,    // a hash table / partition / output buffer would overflow
   ST_KEY_RANGE = 2u,   // a key outside the declared key range
   ST_DOMAIN = 4u,      // a value outside the exact-arithmetic domain of the pipeline
-  ST_TIMEOUT = 8u      // a bounded device wait ran out
+  ST_TIMEOUT = 8u,     // a bounded device wait ran out
+  ST_DUPLICATE = 16u   // a unique build side holds a key twice
 };
 
 __device__ __forceinline__ void set_status(uint32_t* status, uint32_t bits) {

@@ -70,6 +70,8 @@ int status_to_error(gpudb_ctx* ctx, uint32_t st) {
     return fail(ctx, GPUDB_E_KEY_RANGE, "device status 0x%x: a key is outside the declared key range", st);
   if (st & ST_DOMAIN)
     return fail(ctx, GPUDB_E_INVALID, "device status 0x%x: a value is outside the exact-arithmetic domain", st);
+  if (st & ST_DUPLICATE)
+    return fail(ctx, GPUDB_E_INVALID, "device status 0x%x: a key occurs twice on a unique build side", st);
   if (st & ST_TIMEOUT)
     return fail(ctx, GPUDB_E_TIMEOUT, "device status 0x%x: a bounded device wait ran out", st);
   return fail(ctx, GPUDB_E_CUDA, "device status 0x%x", st);

@@ -1,0 +1,149 @@
+// Building blocks shared by the join pipelines: bitmap semi-join filters, warp-ballot
+// compaction, open-addressing hash tables keyed by int32 with atomicCAS insertion, and
+// block top-k selection over 128-bit sortable composites.
+#pragma once
+#include "common.cuh"
+
+namespace gpudb {
+
+constexpr int32_t kEmptyKey = INT32_MIN;   // empty slot marker; INT32_MIN is not a valid key
+
+__device__ __forceinline__ uint32_t lanemask_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
+__device__ __forceinline__ uint32_t lanemask_le() { uint32_t m; asm("mov.u32 %0, %%lanemask_le;" : "=r"(m)); return m; }
+__device__ __forceinline__ uint32_t lanemask_gt() { uint32_t m; asm("mov.u32 %0, %%lanemask_gt;" : "=r"(m)); return m; }
+
+// Sets bit `key` for rows whose predicate column equals `value` (all rows if pred is null).
+// Lanes that hit the same 32-bit word are combined first, so a dense key run costs one
+// atomicOr per word instead of one per row.
+__global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, const uint8_t* __restrict__ pred, int32_t value,
+                                    uint64_t n, int32_t key_max, uint32_t* bitmap, uint32_t* status) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t end = (n + 31) & ~31ull;   // whole warps stay in the loop
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+    bool on = false;
+    int32_t key = 0;
+    if (i < n) {
+      key = keys[i];
+      on = pred ? (pred[i] == (uint8_t)value) : true;
+      if (on && (key < 0 || key > key_max)) { set_status(status, ST_KEY_RANGE); on = false; }
+    }
+    const uint32_t word = (uint32_t)key >> 5, bit = 1u << ((uint32_t)key & 31u);
+    uint32_t pending = __ballot_sync(FULL_MASK, on);
+    while (pending) {
+      const int leader = __ffs(pending) - 1;
+      const uint32_t lw = __shfl_sync(FULL_MASK, word, leader);
+      const bool mine = on && word == lw;
+      const uint32_t bits = __reduce_or_sync(FULL_MASK, mine ? bit : 0u);
+      const uint32_t same = __ballot_sync(FULL_MASK, mine);
+      if ((int)(threadIdx.x & 31) == leader) atomicOr(bitmap + lw, bits);
+      pending &= ~same;
+    }
+  }
+}
+
+// Warp-aggregated append: returns this lane's output position (valid where `take`).
+__device__ __forceinline__ uint32_t warp_append(bool take, uint32_t* counter) {
+  const uint32_t m = __ballot_sync(FULL_MASK, take);
+  uint32_t base = 0;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && m) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(FULL_MASK, base, 0);
+  return base + __popc(m & lanemask_lt());
+}
+
+// Open-addressing table capacity from a device-side count: the smallest power of two
+// >= 2*count (at most 50% load), at least `min_cap`, at most `max_cap`.
+__device__ __forceinline__ uint32_t table_capacity(uint32_t count, uint32_t min_cap, uint32_t max_cap) {
+  uint64_t want = 2ull * count;
+  uint32_t cap = min_cap;
+  while (cap < want && cap < max_cap) cap <<= 1;
+  return cap;
+}
+
+__device__ __forceinline__ uint32_t key_slot(int32_t key, uint32_t mask) {
+  return slot_hash64((uint32_t)key) & mask;
+}
+
+// ---- 128-bit sortable composites for top-k: larger composite = earlier in the output --
+// hi = revenue with the sign bit flipped (signed order as unsigned order), lo = (~date, ~key)
+// with flipped signs, so larger lo = smaller date, then smaller key.
+__host__ __device__ __forceinline__ u128 topk_compose(int64_t rev, int32_t date, int32_t key) {
+  const uint64_t hi = (uint64_t)rev ^ 0x8000000000000000ull;
+  const uint64_t lo = ((uint64_t)(~((uint32_t)date ^ 0x80000000u)) << 32) | (uint64_t)(~((uint32_t)key ^ 0x80000000u));
+  return ((u128)hi << 64) | lo;
+}
+__host__ __device__ __forceinline__ void topk_decompose(u128 c, int64_t* rev, int32_t* date, int32_t* key) {
+  const uint64_t hi = (uint64_t)(c >> 64), lo = (uint64_t)c;
+  *rev = (int64_t)(hi ^ 0x8000000000000000ull);
+  *date = (int32_t)((~(uint32_t)(lo >> 32)) ^ 0x80000000u);
+  *key = (int32_t)((~(uint32_t)lo) ^ 0x80000000u);
+}
+
+__device__ __forceinline__ u128 shfl_u128(u128 v, int src) {
+  uint64_t lo = __shfl_sync(FULL_MASK, (uint64_t)v, src);
+  uint64_t hi = __shfl_sync(FULL_MASK, (uint64_t)(v >> 64), src);
+  return ((u128)hi << 64) | lo;
+}
+
+constexpr int kTopkThreads = 256;
+constexpr int kTopkPerThread = 16;
+constexpr int kTopkTile = kTopkThreads * kTopkPerThread;   // 4096 candidates per block
+
+// Block top-k over a tile held as kTopkPerThread composites per thread (0 = no candidate).
+// k rounds of block arg-max; the winner removes its element and rescans its own 16. Writes
+// k composites (0-padded) to out.
+__device__ __forceinline__ void block_topk(u128 (&v)[kTopkPerThread], int k, u128* out) {
+  __shared__ u128 wbest[kTopkThreads / 32];
+  __shared__ int wowner[kTopkThreads / 32];
+  __shared__ int winner;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int bi = 0;
+  u128 best = 0;
+#pragma unroll
+  for (int j = 0; j < kTopkPerThread; j++)
+    if (v[j] > best) { best = v[j]; bi = j; }
+  for (int r = 0; r < k; r++) {
+    u128 m = best;
+    int owner = threadIdx.x;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      u128 o = shfl_u128(m, lane ^ d);
+      int oo = __shfl_xor_sync(FULL_MASK, owner, d);
+      if (o > m || (o == m && oo < owner)) { m = o; owner = oo; }
+    }
+    if (lane == 0) { wbest[warp] = m; wowner[warp] = owner; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u128 b = wbest[0];
+      int o = wowner[0];
+      for (int w = 1; w < kTopkThreads / 32; w++)
+        if (wbest[w] > b) { b = wbest[w]; o = wowner[w]; }
+      out[r] = b;
+      winner = (b == 0) ? -1 : o;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x == winner) {
+#pragma unroll
+      for (int j = 0; j < kTopkPerThread; j++)
+        if (j == bi) v[j] = 0;
+      best = 0;
+      bi = 0;
+#pragma unroll
+      for (int j = 0; j < kTopkPerThread; j++)
+        if (v[j] > best) { best = v[j]; bi = j; }
+    }
+    __syncthreads();
+  }
+}
+
+// Top-k of `n` composites (tiles of kTopkTile per block) -> k per block.
+__global__ void __launch_bounds__(kTopkThreads) topk_merge_kernel(const u128* __restrict__ in, uint64_t n, int k,
+                                                                  u128* __restrict__ out) {
+  u128 v[kTopkPerThread];
+  const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
+#pragma unroll
+  for (int j = 0; j < kTopkPerThread; j++) v[j] = (base + j < n) ? in[base + j] : (u128)0;
+  block_topk(v, k, out + (size_t)blockIdx.x * k);
+}
+
+}  // namespace gpudb

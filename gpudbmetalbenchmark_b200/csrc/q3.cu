@@ -1,0 +1,303 @@
+// Q3-like pipeline: bitmap semi-join filter on the dimension table, filtered hash build
+// on orders, probe + per-order aggregation of the fact table, and device top-k.
+// Reference: kernels/q3.metal:43-340 (bitmap, direct map / hash table build, fused probe
+// + CAS aggregation, compaction), src/q3.cpp:8-538 (driver), src/infra.h:538-564 (CPU
+// top-10).
+//
+// B200 design (global-table mode):
+//  1. bitmap_build_kernel: customers with segment == S -> bitmap (warp-combined atomicOr).
+//  2. orders_filter_kernel: orders with order_date < D and cust in the bitmap are compacted
+//     (warp ballot + one atomicAdd per warp) into a staging list; the qualifying count stays
+//     on the device.
+//  3. table_clear_kernel: sizes the hash table from that count on the device (power of two,
+//     <= 50% load) and clears only those slots, so no host round trip is needed.
+//  4. orders_insert_kernel: atomicCAS insertion; each slot is {key, date, revenue} and a
+//     parallel hit counter, so the orders table doubles as the per-order aggregation table
+//     (the group key equals the join key).
+//  5. q3_probe_kernel: one lane per fact row; runs of equal order keys (adjacent rows of one
+//     order) are found with a warp ballot, only the run head probes the table, and the run's
+//     revenue is summed with a warp prefix scan, so each run costs one 64-bit atomicAdd.
+//     ext_price and discount are loaded only for rows that passed the date filter and found
+//     their order (late materialisation).
+//  6. topk kernels: block top-k over the table slots, then over the block winners.
+// Radix mode partitions both sides by key hash and joins each partition in shared memory
+// (radix.cu).
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.h"
+#include "join_common.cuh"
+#include "q3.h"
+
+namespace gpudb {
+
+struct Q3Slot {
+  int32_t key;
+  int32_t date;
+  unsigned long long rev;
+};
+
+namespace {
+
+__global__ void orders_filter_kernel(const int32_t* __restrict__ okey, const int32_t* __restrict__ ocust,
+                                     const int32_t* __restrict__ odate, uint64_t n, int32_t date_lt,
+                                     const uint32_t* __restrict__ bitmap, int32_t cust_max, int32_t* out_key,
+                                     int32_t* out_date, uint32_t* count, uint32_t* status) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t end = (n + 31) & ~31ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+    bool take = false;
+    int32_t key = 0, date = 0;
+    if (i < n) {
+      date = odate[i];
+      if (date < date_lt) {
+        const int32_t c = ocust[i];
+        if (c >= 0 && c <= cust_max && bitmap_test(bitmap, c)) {
+          key = okey[i];
+          if (key == kEmptyKey) set_status(status, ST_KEY_RANGE);
+          else take = true;
+        }
+      }
+    }
+    const uint32_t pos = warp_append(take, count);
+    if (take) { out_key[pos] = key; out_date[pos] = date; }
+  }
+}
+
+__global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint32_t max_cap, uint32_t* cap_out,
+                                   Q3Slot* ht, uint32_t* hits) {
+  const uint32_t cap = table_capacity(*count, min_cap, max_cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *cap_out = cap;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
+    ht[i].key = kEmptyKey;
+    ht[i].date = 0;
+    ht[i].rev = 0;
+    hits[i] = 0;
+  }
+}
+
+__global__ void orders_insert_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ date,
+                                     const uint32_t* count, const uint32_t* cap_p, Q3Slot* ht, uint32_t* status) {
+  const uint32_t n = *count, cap = *cap_p, mask = cap - 1;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = key[i];
+    uint32_t s = key_slot(k, mask);
+    bool done = false;
+    for (uint32_t p = 0; p < cap && !done; p++, s = (s + 1) & mask) {
+      const int32_t prev = atomicCAS(&ht[s].key, kEmptyKey, k);
+      if (prev == kEmptyKey) { ht[s].date = date[i]; done = true; }
+      else if (prev == k) { set_status(status, ST_DUPLICATE); done = true; }
+    }
+    if (!done) set_status(status, ST_CAPACITY);
+  }
+}
+
+__device__ __forceinline__ int32_t ht_find(const Q3Slot* ht, uint32_t cap, int32_t key) {
+  const uint32_t mask = cap - 1;
+  uint32_t s = key_slot(key, mask);
+  for (uint32_t p = 0; p < cap; p++, s = (s + 1) & mask) {
+    const int32_t k = __ldg(&ht[s].key);
+    if (k == key) return (int32_t)s;
+    if (k == kEmptyKey) return -1;
+  }
+  return -1;
+}
+
+__global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict__ lkey, const int32_t* __restrict__ lship,
+                                                       const int64_t* __restrict__ lext, const int32_t* __restrict__ ldisc,
+                                                       uint64_t n, int32_t ship_gt, Q3Slot* ht, uint32_t* hits,
+                                                       const uint32_t* cap_p) {
+  const uint32_t cap = *cap_p;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n; base += warps * 32) {
+    const uint64_t row = base + lane;
+    const bool valid = row < n;
+    const int32_t key = valid ? ld_stream(lkey + row) : kEmptyKey;
+    const bool pass = valid && ld_stream(lship + row) > ship_gt;
+    const int32_t prev = __shfl_up_sync(FULL_MASK, key, 1);
+    const bool head = (lane == 0) || (key != prev);
+    const uint32_t heads = __ballot_sync(FULL_MASK, head);
+    const uint32_t passm = __ballot_sync(FULL_MASK, pass);
+    // run = [head lane, next head); `last` = last lane of this lane's run
+    const int my_head = 31 - __clz(heads & lanemask_le());
+    const uint32_t later = heads & lanemask_gt();
+    const int last = later ? (__ffs(later) - 2) : 31;
+    const uint32_t run_mask = (last == 31 ? 0xFFFFFFFFu : ((1u << (last + 1)) - 1u)) & ~((1u << my_head) - 1u);
+    int32_t slot = -1;
+    if (head && (passm & run_mask) && key != kEmptyKey) slot = ht_find(ht, cap, key);
+    slot = __shfl_sync(FULL_MASK, slot, my_head);
+    const bool hit = pass && slot >= 0;
+    int64_t v = 0;
+    if (hit) v = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
+    // inclusive prefix sum of v across the warp
+    int64_t inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      int64_t o = __shfl_up_sync(FULL_MASK, inc, d);
+      if (lane >= d) inc += o;
+    }
+    const int64_t run_end = __shfl_sync(FULL_MASK, inc, last);
+    const int64_t before = inc - v;   // exclusive prefix at this lane
+    const uint32_t hitm = __ballot_sync(FULL_MASK, hit);
+    if (head && slot >= 0) {
+      const uint32_t c = __popc(hitm & run_mask);
+      if (c) {
+        atomicAdd(&ht[slot].rev, (unsigned long long)(run_end - before));
+        atomicAdd(&hits[slot], c);
+      }
+    }
+  }
+}
+
+// Level 1 of the top-k: slots [blockIdx*4096, +4096) of the table; also counts groups.
+__global__ void __launch_bounds__(kTopkThreads) q3_topk_slots_kernel(const Q3Slot* __restrict__ ht,
+                                                                     const uint32_t* __restrict__ hits,
+                                                                     const uint32_t* cap_p, int k, u128* out,
+                                                                     unsigned long long* groups) {
+  const uint32_t cap = *cap_p;
+  u128 v[kTopkPerThread];
+  uint32_t cnt = 0;
+  const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
+#pragma unroll
+  for (int j = 0; j < kTopkPerThread; j++) {
+    v[j] = 0;
+    const uint64_t s = base + j;
+    if (s < cap && hits[s]) {
+      v[j] = topk_compose((int64_t)ht[s].rev, ht[s].date, ht[s].key);
+      cnt++;
+    }
+  }
+  cnt = __reduce_add_sync(FULL_MASK, cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(groups, (unsigned long long)cnt);
+  block_topk(v, k, out + (size_t)blockIdx.x * k);
+}
+
+}  // namespace
+
+int q3_topk_levels(Call& call, u128* cand, uint64_t n_cand, int k, u128* scratch_a, u128* scratch_b, u128* final_out) {
+  // reduce n_cand candidates (k per 4096-candidate tile) until one block remains
+  const u128* in = cand;
+  u128* bufs[2] = {scratch_a, scratch_b};
+  int flip = 0;
+  while (true) {
+    const uint64_t blocks = (n_cand + kTopkTile - 1) / kTopkTile;
+    u128* out = (blocks == 1) ? final_out : bufs[flip];
+    GPUDB_LAUNCH(call, topk_merge_kernel, (unsigned)std::max<uint64_t>(blocks, 1), kTopkThreads, 0, in, n_cand, k, out);
+    if (blocks <= 1) return GPUDB_OK;
+    in = out;
+    n_cand = blocks * (uint64_t)k;
+    flip ^= 1;
+  }
+}
+
+// Global-table Q3 (steps 1-6 above). Result payload: {u64 groups, u128 rows[k]}.
+int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_lineitem* li,
+              const gpudb_q3_params& p, uint8_t* result) {
+  gpudb_ctx* ctx = call.ctx();
+  cudaStream_t s = call.stream();
+  const uint32_t words = (uint32_t)(cu.key_max >> 5) + 1;
+  const uint64_t n_or = od.n_rows;
+  uint32_t max_cap = 2048;
+  while (max_cap < 2 * n_or && max_cap < (1u << 31)) max_cap <<= 1;
+  void *bitmap, *stage, *count, *ht, *hits, *cand;
+  int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
+  if (!rc) rc = scratch(ctx, "q3.stage", std::max<size_t>(n_or, 1) * 8, &stage);
+  if (!rc) rc = scratch(ctx, "q3.count", 256, &count);
+  if (!rc) rc = scratch(ctx, "q3.ht", (size_t)max_cap * sizeof(Q3Slot), &ht);
+  if (!rc) rc = scratch(ctx, "q3.hits", (size_t)max_cap * 4, &hits);
+  const uint64_t tiles = (max_cap + kTopkTile - 1) / kTopkTile;
+  const size_t cand_elems = tiles * (size_t)p.k;
+  if (!rc) rc = scratch(ctx, "q3.cand", (cand_elems * 2 + 64) * sizeof(u128), &cand);
+  if (rc) return rc;
+  uint32_t* cnt = static_cast<uint32_t*>(count);
+  uint32_t* cap = cnt + 1;
+  GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+  const int sms = ctx->sm_count;
+  auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
+  if (cu.n_rows)
+    GPUDB_LAUNCH(call, bitmap_build_kernel, grid(cu.n_rows), 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows,
+                 cu.key_max, (uint32_t*)bitmap, call.status());
+  int32_t* skey = static_cast<int32_t*>(stage);
+  int32_t* sdate = skey + std::max<uint64_t>(n_or, 1);
+  if (n_or)
+    GPUDB_LAUNCH(call, orders_filter_kernel, grid(n_or), 256, 0, od.order_key, od.cust_key, od.order_date, n_or,
+                 p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, skey, sdate, cnt, call.status());
+  GPUDB_LAUNCH(call, table_clear_kernel, grid(max_cap), 256, 0, (const uint32_t*)cnt, 2048u, max_cap, cap,
+               (Q3Slot*)ht, (uint32_t*)hits);
+  GPUDB_LAUNCH(call, orders_insert_kernel, grid(n_or), 256, 0, (const int32_t*)skey, (const int32_t*)sdate,
+               (const uint32_t*)cnt, (const uint32_t*)cap, (Q3Slot*)ht, call.status());
+  const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
+  rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
+    if (c.n_rows == 0) return (int)GPUDB_OK;
+    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows + 255) / 256, (uint64_t)sms * 8));
+    GPUDB_LAUNCH(call, q3_probe_kernel, g, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount, c.n_rows,
+                 p.ship_date_gt, (Q3Slot*)ht, (uint32_t*)hits, (const uint32_t*)cap);
+    return (int)GPUDB_OK;
+  });
+  if (rc) return rc;
+  u128* cbuf = static_cast<u128*>(cand);
+  unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
+  u128* rows = reinterpret_cast<u128*>(result + 16);
+  GPUDB_LAUNCH(call, q3_topk_slots_kernel, (unsigned)tiles, kTopkThreads, 0, (const Q3Slot*)ht, (const uint32_t*)hits,
+               (const uint32_t*)cap, p.k, cbuf, groups);
+  if (tiles == 1) {
+    GPUDB_CUDA(ctx, cudaMemcpyAsync(rows, cbuf, (size_t)p.k * sizeof(u128), cudaMemcpyDeviceToDevice, s));
+    return GPUDB_OK;
+  }
+  return q3_topk_levels(call, cbuf, tiles * (uint64_t)p.k, p.k, cbuf + cand_elems, cbuf + cand_elems + cand_elems / 2 + 32,
+                        rows);
+}
+
+}  // namespace gpudb
+
+using namespace gpudb;
+
+extern "C" int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_orders* od,
+                                  const gpudb_lineitem* li, const gpudb_q3_params* p, gpudb_q3_result* out,
+                                  gpudb_timing* t, const gpudb_exec* ex) {
+  if (!ctx) return GPUDB_E_INVALID;
+  if (!cu || !od || !p || !out) return fail(ctx, GPUDB_E_INVALID, "q3: tables, params and result are required");
+  if (p->k < 1 || p->k > GPUDB_Q3_MAX_K) return fail(ctx, GPUDB_E_INVALID, "q3: k must be in 1..%d", GPUDB_Q3_MAX_K);
+  if (p->join_mode != GPUDB_JOIN_GLOBAL && p->join_mode != GPUDB_JOIN_RADIX)
+    return fail(ctx, GPUDB_E_INVALID, "q3: unknown join mode %d", p->join_mode);
+  if (cu->n_rows && (!cu->cust_key || !cu->segment)) return fail(ctx, GPUDB_E_INVALID, "q3: customer columns are NULL");
+  if (cu->key_max < 0 && cu->n_rows) return fail(ctx, GPUDB_E_INVALID, "q3: customer.key_max is required");
+  if (od->n_rows && (!od->order_key || !od->cust_key || !od->order_date))
+    return fail(ctx, GPUDB_E_INVALID, "q3: orders columns are NULL");
+  if (od->n_rows > (1ull << 30)) return fail(ctx, GPUDB_E_INVALID, "q3: orders larger than 2^30 rows");
+  int rc = lineitem_check(ctx, li, LI_ORDER | LI_SHIP | LI_EXT | LI_DISC);
+  if (rc) return rc;
+  gpudb_customer c = *cu;
+  if (c.key_max < 0) c.key_max = 0;
+  const gpudb_orders o = *od;
+  const gpudb_q3_params pp = *p;
+  Call call(ctx, ex, t);
+  const size_t bytes = 16 + (size_t)GPUDB_Q3_MAX_K * sizeof(u128);
+  if ((rc = call.begin(bytes))) return rc;
+  uint8_t* res = call.result<uint8_t>();
+  rc = (pp.join_mode == GPUDB_JOIN_GLOBAL) ? q3_global(call, c, o, li, pp, res) : q3_radix(call, c, o, li, pp, res);
+  if (rc) return rc;
+  const int k = pp.k;
+  return call.finish(bytes, [out, k](const uint8_t* h) {
+    uint64_t groups;
+    std::memcpy(&groups, h, 8);
+    out->n_groups = groups;
+    out->n_rows = (uint32_t)std::min<uint64_t>(groups, (uint64_t)k);
+    for (uint32_t i = 0; i < out->n_rows; i++) {
+      u128 c;
+      std::memcpy(&c, h + 16 + i * sizeof(u128), sizeof c);
+      int64_t rev;
+      int32_t date, key;
+      topk_decompose(c, &rev, &date, &key);
+      out->rows[i].order_key = key;
+      out->rows[i].order_date = date;
+      out->rows[i].revenue = rev;
+    }
+    return GPUDB_OK;
+  });
+}

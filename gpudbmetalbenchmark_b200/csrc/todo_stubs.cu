@@ -1,11 +1,14 @@
 // Entry points whose kernels are not written yet: they report GPUDB_E_UNSUPPORTED.
 #include "engine.h"
+#include "q3.h"
+namespace gpudb {
+int q3_radix(Call& call, const gpudb_customer&, const gpudb_orders&, const gpudb_lineitem*, const gpudb_q3_params&,
+             uint8_t*) {
+  return fail(call.ctx(), GPUDB_E_UNSUPPORTED, "radix mode not built yet");
+}
+}  // namespace gpudb
 using namespace gpudb;
 extern "C" {
-int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer*, const gpudb_orders*, const gpudb_lineitem*,
-                       const gpudb_q3_params*, gpudb_q3_result*, gpudb_timing*, const gpudb_exec*) {
-  return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet");
-}
 int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part*, const gpudb_supplier*, const gpudb_partsupp*,
                   const gpudb_orders*, const gpudb_lineitem*, const gpudb_q9_params*, gpudb_q9_group*, uint32_t,
                   uint32_t*, gpudb_timing*, const gpudb_exec*) {

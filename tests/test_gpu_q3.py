@@ -1,0 +1,102 @@
+"""Q3-like join + top-k on the GPU against the CPU oracle, bit-exact: the default and 10x
+configurations, randomised predicate constants, k from 1 to 64, revenue ties broken by
+order date then order key, empty sides, duplicate build keys and streamed fact tables."""
+import numpy as np
+import pytest
+
+from gpudbmetalbenchmark_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+MODES = [capi.JOIN_GLOBAL]
+
+
+def run(engine, cu, od, li, mode=capi.JOIN_GLOBAL, location=capi.MEM_DEVICE, **kw):
+    tc, to = engine.upload("customer", cu), engine.upload("orders", od)
+    tl = engine.upload("lineitem", li, location=location)
+    try:
+        return engine.q3(tc, to, tl, join_mode=mode, **kw)
+    finally:
+        for t in (tc, to, tl):
+            engine.free(t)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("sizes,seed", [((150_000, 1_500_000, 6_000_000), 42), ((3000, 20000, 80000), 1),
+                                        ((10, 40, 100), 2), ((1, 1, 1), 3)])
+def test_q3_matches_oracle(engine, orc, mode, sizes, seed):
+    cu, od, li = orc.q3_tables(*sizes, seed)
+    assert run(engine, cu, od, li, mode) == orc.q3(cu, od, li)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_q3_random_constants_and_k(engine, orc, mode):
+    rng = np.random.default_rng(5)
+    cu, od, li = orc.q3_tables(20_000, 200_000, 800_000, 11)
+    tc, to, tl = engine.upload("customer", cu), engine.upload("orders", od), engine.upload("lineitem", li)
+    try:
+        for _ in range(12):
+            seg = int(rng.integers(0, 5))
+            d = int(rng.integers(0, 2406))
+            s = int(rng.integers(0, 2527))
+            k = int(rng.choice([1, 3, 10, 33, 64]))
+            got = engine.q3(tc, to, tl, segment=seg, order_date_lt=d, ship_date_gt=s, k=k, join_mode=mode)
+            assert got == orc.q3(cu, od, li, seg, d, s, k), (seg, d, s, k)
+    finally:
+        for t in (tc, to, tl):
+            engine.free(t)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_q3_ties_break_by_date_then_key(engine, orc, mode):
+    n_or = 5000
+    cu = dict(cust_key=np.arange(10, dtype=np.int32), segment=np.ones(10, np.uint8))
+    od = dict(order_key=(4 * np.arange(n_or) + 1).astype(np.int32),
+              cust_key=(np.arange(n_or) % 10).astype(np.int32),
+              order_date=(np.arange(n_or) % 3).astype(np.int32))
+    # every order gets one row with the same revenue: the order is date asc, key asc
+    li = dict(order_key=od["order_key"].copy(), ship_date=np.full(n_or, 2000, np.int32),
+              ext_price=np.full(n_or, 123456, np.int64), discount=np.full(n_or, 4, np.int32))
+    got = run(engine, cu, od, li, mode, k=64)
+    assert got == orc.q3(cu, od, li, k=64)
+    assert [r[0] for r in got[0][:3]] == [1, 13, 25]
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_q3_empty_sides(engine, orc, mode):
+    cu, od, li = orc.q3_tables(100, 1000, 4000, 4)
+    none = dict(order_key=li["order_key"][:0], ship_date=li["ship_date"][:0], ext_price=li["ext_price"][:0],
+                discount=li["discount"][:0])
+    assert run(engine, cu, od, none, mode) == ([], 0)
+    # no qualifying customer
+    assert run(engine, cu, od, li, mode, segment=9) == ([], 0)
+    # no qualifying order date
+    assert run(engine, cu, od, li, mode, order_date_lt=0) == ([], 0)
+
+
+def test_q3_duplicate_build_key_reported(engine, orc):
+    cu, od, li = orc.q3_tables(100, 1000, 4000, 4)
+    od["order_key"][7] = od["order_key"][8]
+    od["order_date"][7] = od["order_date"][8] = 0
+    od["cust_key"][7] = od["cust_key"][8]
+    cu["segment"][od["cust_key"][8]] = 1
+    with pytest.raises(capi.GpudbError) as e:
+        run(engine, cu, od, li)
+    assert e.value.code == capi.E_INVALID
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_q3_streamed_fact_table(engine, orc, mode):
+    cu, od, li = orc.q3_tables(5000, 50_000, 200_003, 8)
+    engine.set_chunk_rows(30_000)
+    try:
+        assert run(engine, cu, od, li, mode, location=capi.MEM_HOST) == orc.q3(cu, od, li)
+    finally:
+        engine.set_chunk_rows(64 << 20)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_q3_10x_configuration(engine, orc, mode):
+    """Config 2 at 10x rows: 1.5M customers, 15M orders, 60M lineitem rows."""
+    cu, od, li = orc.q3_tables(1_500_000, 15_000_000, 60_000_000, 42)
+    assert run(engine, cu, od, li, mode) == orc.q3(cu, od, li)
