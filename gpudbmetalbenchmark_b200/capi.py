@@ -154,6 +154,7 @@ PROTOTYPES = {
     "gpudb_generate": (C.c_int, [ctx_p, P(GenSpec), C.c_int32, vp, C.c_int32]),
     "gpudb_column_width": (C.c_int, [C.c_int32]),
     "gpudb_q6_sum": (C.c_int, [ctx_p, P(Lineitem), P(Q6Params), P(Q6Result), P(Timing), P(Exec)]),
+    "gpudb_q6_sum_noalloc": (C.c_int, [P(Lineitem), P(Q6Params), vp, vp]),
     "gpudb_q1_group6": (C.c_int, [ctx_p, P(Lineitem), P(Q1Params), P(Q1Result), P(Timing), P(Exec)]),
     "gpudb_q3_join_topk": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q3Params), P(Q3Result),
                                      P(Timing), P(Exec)]),

@@ -188,6 +188,20 @@ typedef struct gpudb_q6_result { int64_t revenue; uint64_t rows_matched; } gpudb
 int gpudb_q6_sum(gpudb_ctx* ctx, const gpudb_lineitem* li, const gpudb_q6_params* p,
                  gpudb_q6_result* out, gpudb_timing* t, const gpudb_exec* ex);
 
+/* Q6-like filtered sum that allocates nothing. No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- code running while a stream is captured into a
+ * CUDA graph, programs whose device memory is owned by another memory manager, and plugins
+ * that have no gpudb_ctx. It needs no context. li must be device-resident; `out` is a
+ * caller-owned device buffer of two int64 (revenue, rows matched) that the call overwrites;
+ * the work is enqueued on `stream` (a cudaStream_t, NULL = default stream) of the current
+ * device and the call does not wait for it. Scratch is a fixed 262,400-byte static device
+ * array that every GPU loading this library holds until exit, so li->n_rows is limited to
+ * 67,108,864 rows (GPUDB_E_CAPACITY beyond). The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. All calls on a device share the one array: calls that overlap on the GPU (for
+ * example on two streams at once) race and give wrong results. */
+int gpudb_q6_sum_noalloc(const gpudb_lineitem* li, const gpudb_q6_params* p, int64_t* out, void* stream);
+
 /* ---- Q1-like filter + 6-group aggregate (replaces runQ1Benchmark src/q1.cpp:8-173 and
  *      q1_fused_kernel kernels/q1.metal:39-121; streamed form replaces runQ1BenchmarkSF100
  *      src/q1.cpp:177-376) ------------------------------------------------------------ */
