@@ -89,19 +89,23 @@ Call::Call(gpudb_ctx* ctx, const gpudb_exec* ex, gpudb_timing* t)
 
 Call::~Call() {
   if (!handed_off_) {
-    if (slot_ >= 0) ctx_->slot_busy[slot_] = false;
+    if (slot_ >= 0) (big_ ? ctx_->big_busy : ctx_->slot_busy)[slot_] = false;
     event_put(ctx_, e0_);
     event_put(ctx_, e1_);
   }
 }
 
 int Call::begin(size_t result_bytes) {
-  if (kSlotHeader + result_bytes > kSlotBytes) return fail(ctx_, GPUDB_E_INVALID, "result too large");
+  big_ = kSlotHeader + result_bytes > kSlotBytes;
+  if (kSlotHeader + result_bytes > (big_ ? kBigSlotBytes : kSlotBytes))
+    return fail(ctx_, GPUDB_E_INVALID, "result too large");
+  const int n = big_ ? kBigSlots : kResultSlots;
+  bool* busy = big_ ? ctx_->big_busy : ctx_->slot_busy;
   // find a free slot; if all are waiting for completion, drain the pending calls
   for (int pass = 0; pass < 2 && slot_ < 0; pass++) {
-    for (int i = 0; i < kResultSlots; i++) {
-      int s = (ctx_->next_slot + i) % kResultSlots;
-      if (!ctx_->slot_busy[s]) { slot_ = s; break; }
+    for (int i = 0; i < n; i++) {
+      int s = big_ ? i : (ctx_->next_slot + i) % n;
+      if (!busy[s]) { slot_ = s; break; }
     }
     if (slot_ < 0) {
       int rc = gpudb_sync(ctx_);
@@ -109,10 +113,15 @@ int Call::begin(size_t result_bytes) {
     }
   }
   if (slot_ < 0) return fail(ctx_, GPUDB_E_CUDA, "no free result slot");
-  ctx_->slot_busy[slot_] = true;
-  ctx_->next_slot = (slot_ + 1) % kResultSlots;
-  dslot_ = ctx_->d_slots + (size_t)slot_ * kSlotBytes;
-  hslot_ = ctx_->h_slots + (size_t)slot_ * kSlotBytes;
+  busy[slot_] = true;
+  if (big_) {
+    dslot_ = ctx_->d_big + (size_t)slot_ * kBigSlotBytes;
+    hslot_ = ctx_->h_big + (size_t)slot_ * kBigSlotBytes;
+  } else {
+    ctx_->next_slot = (slot_ + 1) % kResultSlots;
+    dslot_ = ctx_->d_slots + (size_t)slot_ * kSlotBytes;
+    hslot_ = ctx_->h_slots + (size_t)slot_ * kSlotBytes;
+  }
   GPUDB_CUDA(ctx_, cudaMemsetAsync(dslot_, 0, kSlotHeader + result_bytes, s_));
   if (t_) {
     // the timed region starts after the result slot is cleared: kernels (and copies) only
@@ -137,6 +146,7 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
   d2h_ += bytes;
   gpudb_ctx* ctx = ctx_;
   int slot = slot_;
+  bool big = big_;
   uint8_t* hs = hslot_;
   gpudb_timing* t = t_;
   cudaEvent_t e0 = e0_, e1 = e1_;
@@ -158,7 +168,7 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
       t->kernels = kernels;
       t->chunks = chunks;
     }
-    ctx->slot_busy[slot] = false;
+    (big ? ctx->big_busy : ctx->slot_busy)[slot] = false;
     event_put(ctx, e0);
     event_put(ctx, e1);
     return rc;
@@ -313,6 +323,8 @@ int gpudb_create(int device, gpudb_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_slots, (size_t)kResultSlots * kSlotBytes);
   if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_slots, (size_t)kResultSlots * kSlotBytes, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_big, (size_t)kBigSlots * kBigSlotBytes);
+  if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_big, (size_t)kBigSlots * kBigSlotBytes, cudaHostAllocDefault);
   if (e != cudaSuccess) {
     gpudb_destroy(ctx);
     return e == cudaErrorMemoryAllocation ? GPUDB_E_OOM : GPUDB_E_CUDA;
@@ -330,6 +342,8 @@ int gpudb_destroy(gpudb_ctx* ctx) {
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->d_slots) cudaFree(ctx->d_slots);
   if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
+  if (ctx->d_big) cudaFree(ctx->d_big);
+  if (ctx->h_big) cudaFreeHost(ctx->h_big);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   delete ctx;

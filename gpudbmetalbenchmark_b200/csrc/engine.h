@@ -24,6 +24,8 @@ namespace gpudb {
 constexpr int kResultSlots = 1024;
 constexpr size_t kSlotHeader = 16;                  // status word + padding
 constexpr size_t kSlotBytes = 4096;                 // header + largest fixed-size result
+constexpr int kBigSlots = 8;                        // slots for variable-size results
+constexpr size_t kBigSlotBytes = 256 * 1024;
 constexpr int kStreamSlots = 3;                     // device buffers of the streaming ring
 constexpr uint64_t kDefaultChunkRows = 64ull << 20; // 64M rows per streamed chunk
 
@@ -49,6 +51,9 @@ struct gpudb_ctx {
   uint8_t* h_slots = nullptr;          // their pinned host mirror
   bool slot_busy[gpudb::kResultSlots] = {};
   int next_slot = 0;
+  uint8_t* d_big = nullptr;            // large result slots (device) and their pinned mirror
+  uint8_t* h_big = nullptr;
+  bool big_busy[gpudb::kBigSlots] = {};
   std::vector<std::function<int()>> pending;
   std::vector<cudaStream_t> pending_streams;
   std::vector<cudaEvent_t> event_pool;
@@ -97,6 +102,7 @@ class Call {
   cudaEvent_t e0_ = nullptr, e1_ = nullptr;
   double host0_;
   int slot_ = -1;
+  bool big_ = false;
   uint8_t* dslot_ = nullptr;
   uint8_t* hslot_ = nullptr;
   uint32_t kernels_ = 0, chunks_ = 0;

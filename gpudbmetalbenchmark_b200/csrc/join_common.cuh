@@ -12,10 +12,10 @@ __device__ __forceinline__ uint32_t lanemask_lt() { uint32_t m; asm("mov.u32 %0,
 __device__ __forceinline__ uint32_t lanemask_le() { uint32_t m; asm("mov.u32 %0, %%lanemask_le;" : "=r"(m)); return m; }
 __device__ __forceinline__ uint32_t lanemask_gt() { uint32_t m; asm("mov.u32 %0, %%lanemask_gt;" : "=r"(m)); return m; }
 
-// Sets bit `key` for rows whose predicate column equals `value` (all rows if pred is null).
-// Lanes that hit the same 32-bit word are combined first, so a dense key run costs one
-// atomicOr per word instead of one per row.
-__global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, const uint8_t* __restrict__ pred, int32_t value,
+// Sets bit `key` for rows whose predicate column equals `value` (value < 0: is nonzero;
+// all rows if pred is null). Lanes that hit the same 32-bit word are combined first, so a
+// dense key run costs one atomicOr per word instead of one per row.
+static __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, const uint8_t* __restrict__ pred, int32_t value,
                                     uint64_t n, int32_t key_max, uint32_t* bitmap, uint32_t* status) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t end = (n + 31) & ~31ull;   // whole warps stay in the loop
@@ -24,7 +24,7 @@ __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, const uint
     int32_t key = 0;
     if (i < n) {
       key = keys[i];
-      on = pred ? (pred[i] == (uint8_t)value) : true;
+      on = pred ? (value >= 0 ? pred[i] == (uint8_t)value : pred[i] != 0) : true;
       if (on && (key < 0 || key > key_max)) { set_status(status, ST_KEY_RANGE); on = false; }
     }
     const uint32_t word = (uint32_t)key >> 5, bit = 1u << ((uint32_t)key & 31u);
@@ -137,7 +137,7 @@ __device__ __forceinline__ void block_topk(u128 (&v)[kTopkPerThread], int k, u12
 }
 
 // Top-k of `n` composites (tiles of kTopkTile per block) -> k per block.
-__global__ void __launch_bounds__(kTopkThreads) topk_merge_kernel(const u128* __restrict__ in, uint64_t n, int k,
+static __global__ void __launch_bounds__(kTopkThreads) topk_merge_kernel(const u128* __restrict__ in, uint64_t n, int k,
                                                                   u128* __restrict__ out) {
   u128 v[kTopkPerThread];
   const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;

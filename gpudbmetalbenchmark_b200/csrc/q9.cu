@@ -1,0 +1,353 @@
+// Q9-like star join + (nation, year) aggregate.
+// Reference: kernels/q9.metal:44-394 (part filter, supplier direct map, partsupp hash
+// table, orders hash table / year map, probe + global CAS aggregation), src/q9.cpp:8-557
+// (driver, SF100 streaming), src/infra.h:743-776 (post-processing order).
+//
+// B200 design:
+//  - part filter -> bitmap (bitmap_build_kernel); supplier -> nation and order -> year as
+//    uint8 direct maps (100 KB and max_order_key+1 bytes: 60 MB for 15M orders, mostly L2);
+//  - partsupp rows whose part passes the bitmap are compacted, then inserted into an
+//    open-addressing table keyed by the 64-bit (part, supp) composite with a 64-bit
+//    atomicCAS; the table is sized on the device from the qualifying count;
+//  - the probe reads part_key for every fact row (128-bit loads) and touches the other five
+//    columns only for rows whose part passes (late materialisation, ~5.5%);
+//  - aggregation goes to a per-block shared-memory hash table keyed by (nation<<16 | year)
+//    (CAS + 64-bit shared atomics); a group that finds no shared slot spills straight to the
+//    global open-addressing table, and each block merges its shared table into the global
+//    one once at the end (global atomics ~ blocks x groups, not rows);
+//  - one block compacts the global table and sorts it by nation asc, year desc.
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.h"
+#include "join_common.cuh"
+
+namespace gpudb {
+namespace {
+
+constexpr uint32_t kGroupEmpty = 0xFFFFFFFFu;
+constexpr unsigned long long kPsEmpty = ~0ull;
+constexpr uint8_t kNoValue = 0xFF;
+
+struct PsSlot {
+  unsigned long long key;   // (uint32 part << 32) | uint32 supp
+  long long cost;
+};
+
+__device__ __forceinline__ unsigned long long ps_key(int32_t part, int32_t supp) {
+  return ((unsigned long long)(uint32_t)part << 32) | (uint32_t)supp;
+}
+
+__global__ void map_u8_kernel(const int32_t* __restrict__ keys, const uint8_t* __restrict__ vals, uint64_t n,
+                              int32_t key_max, uint8_t* map, uint32_t* status) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = keys[i];
+    const uint8_t v = vals[i];
+    if (k < 0 || k > key_max) { set_status(status, ST_KEY_RANGE); continue; }
+    if (v == kNoValue) { set_status(status, ST_DOMAIN); continue; }
+    map[k] = v;
+  }
+}
+
+// order key -> year - 1992, where year = 1992 + order_date / 365.
+__global__ void year_map_kernel(const int32_t* __restrict__ keys, const int32_t* __restrict__ dates, uint64_t n,
+                                int32_t key_max, uint8_t* map, uint32_t* status) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = keys[i];
+    const int32_t d = dates[i];
+    if (k < 0 || k > key_max) { set_status(status, ST_KEY_RANGE); continue; }
+    if (d < 0 || d / 365 >= kNoValue) { set_status(status, ST_DOMAIN); continue; }
+    map[k] = (uint8_t)(d / 365);
+  }
+}
+
+__global__ void ps_filter_kernel(const int32_t* __restrict__ part, uint64_t n, const uint32_t* __restrict__ bits,
+                                 int32_t part_max, uint32_t* stage, uint32_t* count) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t end = (n + 31) & ~31ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+    bool take = false;
+    if (i < n) {
+      const int32_t p = part[i];
+      take = p >= 0 && p <= part_max && bitmap_test(bits, p);
+    }
+    const uint32_t pos = warp_append(take, count);
+    if (take) stage[pos] = (uint32_t)i;
+  }
+}
+
+__global__ void ps_clear_kernel(const uint32_t* count, uint32_t max_cap, uint32_t* cap_out, PsSlot* ht) {
+  const uint32_t cap = table_capacity(*count, 1024, max_cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *cap_out = cap;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
+    ht[i].key = kPsEmpty;
+    ht[i].cost = 0;
+  }
+}
+
+__global__ void ps_insert_kernel(const int32_t* __restrict__ part, const int32_t* __restrict__ supp,
+                                 const int64_t* __restrict__ cost, const uint32_t* __restrict__ stage,
+                                 const uint32_t* count, const uint32_t* cap_p, PsSlot* ht, uint32_t* status) {
+  const uint32_t n = *count, cap = *cap_p, mask = cap - 1;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t r = stage[i];
+    const int64_t c = cost[r];
+    if (c < 0 || c >= (1ll << 32)) { set_status(status, ST_DOMAIN); continue; }
+    const unsigned long long k = ps_key(part[r], supp[r]);
+    uint32_t s = slot_hash64(k) & mask;
+    bool done = false;
+    for (uint32_t p = 0; p < cap && !done; p++, s = (s + 1) & mask) {
+      const unsigned long long prev = atomicCAS(&ht[s].key, kPsEmpty, k);
+      if (prev == kPsEmpty) { ht[s].cost = c; done = true; }
+      else if (prev == k) { set_status(status, ST_DUPLICATE); done = true; }
+    }
+    if (!done) set_status(status, ST_CAPACITY);
+  }
+}
+
+__device__ __forceinline__ bool ps_find(const PsSlot* ht, uint32_t cap, unsigned long long k, long long* cost) {
+  const uint32_t mask = cap - 1;
+  uint32_t s = slot_hash64(k) & mask;
+  for (uint32_t p = 0; p < cap; p++, s = (s + 1) & mask) {
+    const unsigned long long key = __ldg(&ht[s].key);
+    if (key == k) { *cost = __ldg(&ht[s].cost); return true; }
+    if (key == kPsEmpty) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void global_group_add(uint32_t* gkeys, unsigned long long* gvals, uint32_t gcap,
+                                                 uint32_t key, unsigned long long v, uint32_t* status) {
+  const uint32_t mask = gcap - 1;
+  uint32_t s = slot_hash64(key) & mask;
+  for (uint32_t p = 0; p < gcap; p++, s = (s + 1) & mask) {
+    const uint32_t prev = atomicCAS(&gkeys[s], kGroupEmpty, key);
+    if (prev == kGroupEmpty || prev == key) { atomicAdd(&gvals[s], v); return; }
+  }
+  set_status(status, ST_CAPACITY);
+}
+
+struct Q9Maps {
+  const uint32_t* part_bits; int32_t part_max;
+  const uint8_t* nation; int32_t supp_max;
+  const PsSlot* ps; const uint32_t* ps_cap;
+  const uint8_t* year; int32_t order_max;
+};
+
+__global__ void __launch_bounds__(256) q9_probe_kernel(const int32_t* __restrict__ part, const int32_t* __restrict__ supp,
+                                                       const int32_t* __restrict__ order, const int64_t* __restrict__ ext,
+                                                       const int32_t* __restrict__ disc, const int32_t* __restrict__ qty,
+                                                       uint64_t n, Q9Maps m, uint32_t* gkeys, unsigned long long* gvals,
+                                                       uint32_t gcap, uint32_t scap, uint32_t* status) {
+  extern __shared__ unsigned long long q9_smem[];
+  unsigned long long* svals = q9_smem;
+  uint32_t* skeys = reinterpret_cast<uint32_t*>(svals + scap);
+  for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x) { skeys[i] = kGroupEmpty; svals[i] = 0; }
+  __syncthreads();
+  const uint32_t ps_cap = *m.ps_cap, smask = scap - 1;
+  uint32_t bad = 0;
+  auto row = [&](uint64_t r, int32_t p) {
+    if (p < 0 || p > m.part_max || !bitmap_test(m.part_bits, p)) return;
+    const int32_t s = supp[r];
+    if (s < 0 || s > m.supp_max) return;
+    const uint8_t nat = __ldg(m.nation + s);
+    if (nat == kNoValue) return;
+    long long cost;
+    if (!ps_find(m.ps, ps_cap, ps_key(p, s), &cost)) return;
+    const int32_t o = order[r];
+    if (o < 0 || o > m.order_max) return;
+    const uint8_t yoff = __ldg(m.year + o);
+    if (yoff == kNoValue) return;
+    const int64_t e = ext[r];
+    const int32_t d = disc[r], q = qty[r];
+    bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
+    const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
+    const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
+    uint32_t h = slot_hash64(key) & smask;
+    for (uint32_t t = 0; t < scap; t++, h = (h + 1) & smask) {
+      const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
+      if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); return; }
+    }
+    global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
+  };
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((reinterpret_cast<uintptr_t>(part) & 15u) == 0) {
+    const uint64_t nq = n >> 2;
+    const int4* p4 = reinterpret_cast<const int4*>(part);
+    for (uint64_t q = tid; q < nq; q += stride) {
+      const int4 v = ld_stream(p4 + q);
+      row(4 * q + 0, v.x);
+      row(4 * q + 1, v.y);
+      row(4 * q + 2, v.z);
+      row(4 * q + 3, v.w);
+    }
+    const uint64_t r = (nq << 2) + tid;
+    if (r < n) row(r, part[r]);
+  } else {
+    for (uint64_t r = tid; r < n; r += stride) row(r, part[r]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) set_status(status, ST_DOMAIN);
+  for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x)
+    if (skeys[i] != kGroupEmpty) global_group_add(gkeys, gvals, gcap, skeys[i], svals[i], status);
+}
+
+// One block: compact the global table and sort by nation asc, year desc (bitonic, in
+// shared memory). out = {u32 n, pad, u64 pad, groups[n] of (nation, year, profit)}.
+__global__ void __launch_bounds__(1024) q9_sort_kernel(const uint32_t* __restrict__ gkeys,
+                                                       const unsigned long long* __restrict__ gvals, uint32_t gcap,
+                                                       uint8_t* out) {
+  extern __shared__ unsigned long long sort_smem[];
+  unsigned long long* vals = sort_smem;                       // gcap
+  uint32_t* keys = reinterpret_cast<uint32_t*>(vals + gcap);  // gcap
+  __shared__ uint32_t count;
+  if (threadIdx.x == 0) count = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < gcap; i += blockDim.x) {
+    const uint32_t k = gkeys[i];
+    if (k != kGroupEmpty) {
+      const uint32_t pos = atomicAdd(&count, 1u);
+      keys[pos] = ((k >> 16) << 16) | (0xFFFFu - (k & 0xFFFFu));   // nation asc, year desc
+      vals[pos] = gvals[i];
+    }
+  }
+  __syncthreads();
+  const uint32_t n = count;
+  uint32_t size = 1;
+  while (size < n) size <<= 1;
+  for (uint32_t i = n + threadIdx.x; i < size; i += blockDim.x) { keys[i] = 0xFFFFFFFFu; vals[i] = 0; }
+  __syncthreads();
+  for (uint32_t k = 2; k <= size; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < size; i += blockDim.x) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          if ((keys[i] > keys[l]) == up) {
+            uint32_t tk = keys[i]; keys[i] = keys[l]; keys[l] = tk;
+            unsigned long long tv = vals[i]; vals[i] = vals[l]; vals[l] = tv;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) *reinterpret_cast<uint32_t*>(out) = n;
+  int32_t* g = reinterpret_cast<int32_t*>(out + 16);
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    g[4 * i + 0] = (int32_t)(keys[i] >> 16);
+    g[4 * i + 1] = (int32_t)(0xFFFFu - (keys[i] & 0xFFFFu));
+    *reinterpret_cast<long long*>(g + 4 * i + 2) = (long long)vals[i];
+  }
+}
+
+uint32_t pow2_at_least(uint32_t v, uint32_t lo) {
+  uint32_t p = lo;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+}  // namespace
+}  // namespace gpudb
+
+using namespace gpudb;
+
+extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_supplier* su, const gpudb_partsupp* ps,
+                             const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q9_params* p,
+                             gpudb_q9_group* out, uint32_t capacity, uint32_t* n_groups, gpudb_timing* t,
+                             const gpudb_exec* ex) {
+  if (!ctx) return GPUDB_E_INVALID;
+  if (!pa || !su || !ps || !od || !n_groups || (!out && capacity))
+    return fail(ctx, GPUDB_E_INVALID, "q9: tables, n_groups and the output are required");
+  if (pa->n_rows && (!pa->part_key || !pa->flag || pa->key_max < 0)) return fail(ctx, GPUDB_E_INVALID, "q9: part columns / key_max");
+  if (su->n_rows && (!su->supp_key || !su->nation || su->key_max < 0)) return fail(ctx, GPUDB_E_INVALID, "q9: supplier columns / key_max");
+  if (ps->n_rows && (!ps->part_key || !ps->supp_key || !ps->supply_cost)) return fail(ctx, GPUDB_E_INVALID, "q9: partsupp columns");
+  if (od->n_rows && (!od->order_key || !od->order_date || od->key_max < 0)) return fail(ctx, GPUDB_E_INVALID, "q9: orders columns / key_max");
+  if (ps->n_rows > (1ull << 30)) return fail(ctx, GPUDB_E_INVALID, "q9: partsupp larger than 2^30 rows");
+  const uint32_t mask = LI_PART | LI_SUPP | LI_ORDER | LI_EXT | LI_DISC | LI_QTY;
+  int rc = lineitem_check(ctx, li, mask);
+  if (rc) return rc;
+  gpudb_q9_params pp{};
+  if (p) pp = *p;
+  const uint32_t scap = pp.smem_slots ? (uint32_t)pp.smem_slots : 1024u;
+  const uint32_t gcap = pp.global_slots ? (uint32_t)pp.global_slots : 4096u;
+  if ((scap & (scap - 1)) || scap < 32 || scap > 8192) return fail(ctx, GPUDB_E_INVALID, "q9: smem_slots must be a power of two in 32..8192");
+  if ((gcap & (gcap - 1)) || gcap < 32 || gcap > 8192) return fail(ctx, GPUDB_E_INVALID, "q9: global_slots must be a power of two in 32..8192");
+
+  Call call(ctx, ex, t);
+  const size_t bytes = 16 + (size_t)gcap * 16;
+  if ((rc = call.begin(bytes))) return rc;
+  cudaStream_t s = call.stream();
+  const int32_t part_max = pa->n_rows ? pa->key_max : 0, supp_max = su->n_rows ? su->key_max : 0;
+  const int32_t order_max = od->n_rows ? od->key_max : 0;
+  const uint32_t words = (uint32_t)(part_max >> 5) + 1;
+  const uint32_t ps_max_cap = pow2_at_least((uint32_t)std::min<uint64_t>(2 * ps->n_rows, 1u << 31), 1024);
+  void *bits, *nation, *year, *stage, *count, *pst, *groups;
+  rc = scratch(ctx, "q9.bits", (size_t)words * 4, &bits);
+  if (!rc) rc = scratch(ctx, "q9.nation", (size_t)supp_max + 1, &nation);
+  if (!rc) rc = scratch(ctx, "q9.year", (size_t)order_max + 1, &year);
+  if (!rc) rc = scratch(ctx, "q9.stage", std::max<size_t>(ps->n_rows, 1) * 4, &stage);
+  if (!rc) rc = scratch(ctx, "q9.count", 256, &count);
+  if (!rc) rc = scratch(ctx, "q9.ps", (size_t)ps_max_cap * sizeof(PsSlot), &pst);
+  if (!rc) rc = scratch(ctx, "q9.groups", (size_t)gcap * 12, &groups);
+  if (rc) return rc;
+  uint32_t* cnt = static_cast<uint32_t*>(count);
+  uint32_t* cap = cnt + 1;
+  uint32_t* gkeys = reinterpret_cast<uint32_t*>(static_cast<unsigned long long*>(groups) + gcap);
+  unsigned long long* gvals = static_cast<unsigned long long*>(groups);
+  GPUDB_CUDA(ctx, cudaMemsetAsync(bits, 0, (size_t)words * 4, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(gvals, 0, (size_t)gcap * 8, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(gkeys, 0xFF, (size_t)gcap * 4, s));
+  const int sms = ctx->sm_count;
+  auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
+  if (pa->n_rows)
+    GPUDB_LAUNCH(call, bitmap_build_kernel, grid(pa->n_rows), 256, 0, pa->part_key, pa->flag, -1, pa->n_rows,
+                 part_max, (uint32_t*)bits, call.status());
+  if (su->n_rows)
+    GPUDB_LAUNCH(call, map_u8_kernel, grid(su->n_rows), 256, 0, su->supp_key, su->nation, su->n_rows, supp_max,
+                 (uint8_t*)nation, call.status());
+  if (od->n_rows)
+    GPUDB_LAUNCH(call, year_map_kernel, grid(od->n_rows), 256, 0, od->order_key, od->order_date, od->n_rows,
+                 order_max, (uint8_t*)year, call.status());
+  if (ps->n_rows)
+    GPUDB_LAUNCH(call, ps_filter_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->n_rows, (const uint32_t*)bits,
+                 part_max, (uint32_t*)stage, cnt);
+  GPUDB_LAUNCH(call, ps_clear_kernel, grid(ps_max_cap), 256, 0, (const uint32_t*)cnt, ps_max_cap, cap, (PsSlot*)pst);
+  GPUDB_LAUNCH(call, ps_insert_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->supp_key, ps->supply_cost,
+               (const uint32_t*)stage, (const uint32_t*)cnt, (const uint32_t*)cap, (PsSlot*)pst, call.status());
+  const Q9Maps maps{(const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,
+                    (const uint32_t*)cap, (const uint8_t*)year, order_max};
+  const size_t probe_smem = (size_t)scap * 12;
+  // dynamic + static shared memory may pass the 48 KB default: always opt in
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
+  rc = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
+    if (c.n_rows == 0) return (int)GPUDB_OK;
+    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows / 4 + 255) / 256, (uint64_t)sms * 8));
+    GPUDB_LAUNCH(call, q9_probe_kernel, g, 256, probe_smem, c.part_key, c.supp_key, c.order_key, c.ext_price, c.discount,
+                 c.quantity, c.n_rows, maps, gkeys, gvals, gcap, scap, call.status());
+    return (int)GPUDB_OK;
+  });
+  if (rc) return rc;
+  const size_t sort_smem = (size_t)gcap * 12;
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
+  GPUDB_LAUNCH(call, q9_sort_kernel, 1, 1024, sort_smem, (const uint32_t*)gkeys, (const unsigned long long*)gvals, gcap,
+               call.result<uint8_t>());
+  const uint32_t cap_out = capacity;
+  const size_t copy = 16 + (size_t)std::min(gcap, capacity) * 16;
+  return call.finish(copy, [out, cap_out, n_groups](const uint8_t* h) {
+    uint32_t n;
+    std::memcpy(&n, h, 4);
+    *n_groups = n;
+    const uint32_t m = std::min(n, cap_out);
+    if (m) std::memcpy(out, h + 16, (size_t)m * sizeof(gpudb_q9_group));
+    return GPUDB_OK;
+  });
+}

@@ -9,11 +9,6 @@ int q3_radix(Call& call, const gpudb_customer&, const gpudb_orders&, const gpudb
 }  // namespace gpudb
 using namespace gpudb;
 extern "C" {
-int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part*, const gpudb_supplier*, const gpudb_partsupp*,
-                  const gpudb_orders*, const gpudb_lineitem*, const gpudb_q9_params*, gpudb_q9_group*, uint32_t,
-                  uint32_t*, gpudb_timing*, const gpudb_exec*) {
-  return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet");
-}
 int gpudb_select_lt(gpudb_ctx* ctx, const int32_t*, uint64_t, int32_t, uint32_t*, uint32_t*, uint64_t*,
                     gpudb_timing*, const gpudb_exec*) { return fail(ctx, GPUDB_E_UNSUPPORTED, "not built yet"); }
 int gpudb_sum_i32(gpudb_ctx* ctx, const int32_t*, uint64_t, int64_t*, gpudb_timing*, const gpudb_exec*) {

@@ -186,7 +186,8 @@ class Engine:
                 t.key_max["order_key"] = int(arrays["order_key"].max()) if n else -1
             elif kind == "orders":
                 t.key_max["order_key"] = int(arrays["order_key"].max()) if n else -1
-                t.key_max["cust_key"] = int(arrays["cust_key"].max()) if n else -1
+                if "cust_key" in arrays:
+                    t.key_max["cust_key"] = int(arrays["cust_key"].max()) if n else -1
             elif kind in ("customer", "part", "supplier"):
                 k = {"customer": "cust_key", "part": "part_key", "supplier": "supp_key"}[kind]
                 t.key_max["key"] = int(arrays[k].max()) if n else -1

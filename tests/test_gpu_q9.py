@@ -1,0 +1,87 @@
+"""Q9-like star join + (nation, year) aggregate on the GPU against the CPU oracle, bit-exact:
+the full config 3 sizes, small tables, the shared-memory spill path, global-table overflow
+reporting, a streamed fact table with ragged chunks and truncated outputs."""
+import numpy as np
+import pytest
+
+from gpudbmetalbenchmark_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def upload_all(engine, tabs, location=capi.MEM_DEVICE):
+    pa, su, ps, od, li = tabs
+    return [engine.upload("part", pa), engine.upload("supplier", su), engine.upload("partsupp", ps),
+            engine.upload("orders", od), engine.upload("lineitem", li, location=location)]
+
+
+def free_all(engine, ts):
+    for t in ts:
+        engine.free(t)
+
+
+@pytest.mark.parametrize("sizes,seed", [((2_000_000, 100_000, 15_000_000, 60_000_000), 42),
+                                        ((20_000, 1_000, 100_000, 500_000), 3), ((40, 8, 30, 100), 4)])
+def test_q9_matches_oracle(engine, orc, sizes, seed):
+    tabs = orc.q9_tables(*sizes, seed)
+    ts = upload_all(engine, tabs)
+    try:
+        assert engine.q9(*ts) == orc.q9(*tabs)
+    finally:
+        free_all(engine, ts)
+
+
+def test_q9_shared_table_spill_and_small_global_table(engine, orc):
+    tabs = orc.q9_tables(20_000, 1_000, 100_000, 400_000, 8)
+    ts = upload_all(engine, tabs)
+    try:
+        want = orc.q9(*tabs)
+        assert want[1] > 100
+        assert engine.q9(*ts, smem_slots=32) == want        # most groups spill to the global table
+        assert engine.q9(*ts, global_slots=256) == want
+        with pytest.raises(capi.GpudbError) as e:
+            engine.q9(*ts, global_slots=64)                  # fewer slots than groups
+        assert e.value.code == capi.E_CAPACITY
+        with pytest.raises(capi.GpudbError) as e:
+            engine.q9(*ts, smem_slots=100)                   # not a power of two
+        assert e.value.code == capi.E_INVALID
+        rows, n = engine.q9(*ts, capacity=10)
+        assert n == want[1] and rows == want[0][:10]
+    finally:
+        free_all(engine, ts)
+
+
+def test_q9_streamed_fact_table(engine, orc):
+    tabs = orc.q9_tables(20_000, 1_000, 100_000, 300_001, 9)
+    ts = upload_all(engine, tabs, location=capi.MEM_HOST)
+    try:
+        assert engine.q9(*ts, chunk_rows=40_000) == orc.q9(*tabs)
+    finally:
+        free_all(engine, ts)
+
+
+def test_q9_no_flagged_part(engine, orc):
+    tabs = orc.q9_tables(2_000, 100, 3_000, 10_000, 5)
+    tabs[0]["flag"][:] = 0
+    ts = upload_all(engine, tabs)
+    try:
+        assert engine.q9(*ts) == ([], 0)
+    finally:
+        free_all(engine, ts)
+
+
+def test_q9_key_out_of_range_reported(engine, orc):
+    tabs = orc.q9_tables(2_000, 100, 3_000, 10_000, 5)
+    ts = upload_all(engine, tabs)
+    try:
+        s = ts[1].struct()
+        s.key_max = 50   # suppliers 51..99 fall outside the declared range
+        import ctypes as C
+        groups = (capi.Q9Group * 64)()
+        n = C.c_uint32()
+        rc = engine.lib.gpudb_q9_star(engine.ctx, C.byref(ts[0].struct()), C.byref(s), C.byref(ts[2].struct()),
+                                      C.byref(ts[3].struct()), C.byref(ts[4].lineitem()), None, groups, 64,
+                                      C.byref(n), None, None)
+        assert rc == capi.E_KEY_RANGE
+    finally:
+        free_all(engine, ts)
