@@ -1,0 +1,286 @@
+// Microbenchmark operators: selection, column sum and hash-join match count.
+// Reference: runSelectionBenchmark / runAggregationBenchmark / runJoinBenchmark
+// (src/microbenchmarks.cpp:8-251) and selection_kernel, sum_kernel_stage1/2,
+// hash_join_build/probe (kernels/microbenchmarks.metal:160-294).
+//
+// B200 design:
+//  - selection: one ballot per 32 rows gives a 32-bit word of the row bitmask directly
+//    (the reference writes one 32-bit 0/1 word per row); row ids are compacted in input
+//    order with per-tile counts, a device scan and a second pass;
+//  - sum: 128-bit loads, int64 per thread, warp shuffle + last-block fold (one launch);
+//  - join count: build keys go into an open-addressing set (atomicCAS, power of two,
+//    <= 50% load); probe rows count once per row at the first match (semi-join count,
+//    as hash_join_probe does). Radix mode lives in radix.cu.
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.h"
+#include "join_common.cuh"
+#include "micro.h"
+#include "scan.cuh"
+
+namespace gpudb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSelTile = kThreads * 16;     // rows per block in the selection kernels
+
+// Bits and per-tile counts. Each warp handles 32-row words of its block's tile.
+__global__ void __launch_bounds__(kThreads) select_count_kernel(const int32_t* __restrict__ col, uint64_t n,
+                                                                int32_t value, uint32_t* bits, uint32_t* tile_counts) {
+  __shared__ uint32_t wc[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * kSelTile;
+  uint32_t c = 0;
+  for (int w = warp; w < kSelTile / 32; w += kThreads / 32) {
+    const uint64_t r = base + (uint64_t)w * 32 + lane;
+    const bool hit = r < n && ld_stream(col + r) < value;
+    const uint32_t m = __ballot_sync(FULL_MASK, hit);
+    if (lane == 0) {
+      if (bits && base + (uint64_t)w * 32 < n) bits[(base >> 5) + w] = m;
+      c += __popc(m);
+    }
+  }
+  if (lane == 0) wc[warp] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kThreads / 32; w++) t += wc[w];
+    tile_counts[blockIdx.x] = t;
+  }
+}
+
+// Row ids in input order: tile offset + rank inside the tile.
+__global__ void __launch_bounds__(kThreads) select_rows_kernel(const int32_t* __restrict__ col, uint64_t n, int32_t value,
+                                                               const uint64_t* __restrict__ tile_offsets, uint32_t* rows) {
+  __shared__ uint32_t wc[kSelTile / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * kSelTile;
+  uint32_t masks[kSelTile / 32 / (kThreads / 32)];
+#pragma unroll
+  for (int j = 0; j < kSelTile / kThreads; j++) {
+    const int w = warp + j * (kThreads / 32);
+    const uint64_t r = base + (uint64_t)w * 32 + lane;
+    const bool hit = r < n && col[r] < value;
+    masks[j] = __ballot_sync(FULL_MASK, hit);
+    if (lane == 0) wc[w] = __popc(masks[j]);
+  }
+  __syncthreads();
+  // exclusive scan of the 128 word counts (one warp)
+  if (warp == 0) {
+    uint32_t v[4], s = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) { v[i] = wc[lane * 4 + i]; s += v[i]; }
+    uint32_t inc = s;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t o = __shfl_up_sync(FULL_MASK, inc, d);
+      if (lane >= d) inc += o;
+    }
+    uint32_t run = inc - s;
+#pragma unroll
+    for (int i = 0; i < 4; i++) { wc[lane * 4 + i] = run; run += v[i]; }
+  }
+  __syncthreads();
+  const uint64_t off = tile_offsets[blockIdx.x];
+#pragma unroll
+  for (int j = 0; j < kSelTile / kThreads; j++) {
+    const int w = warp + j * (kThreads / 32);
+    const uint32_t m = masks[j];
+    if ((m >> lane) & 1u) rows[off + wc[w] + __popc(m & lanemask_lt())] = (uint32_t)(base + (uint64_t)w * 32 + lane);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) sum_i32_kernel(const int32_t* __restrict__ col, uint64_t n, bool vec,
+                                                           int64_t* partials, unsigned* ticket, int64_t* out) {
+  const uint64_t T = (uint64_t)gridDim.x * kThreads;
+  const uint64_t tid = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+  int64_t s = 0;
+  if (vec) {
+    const uint64_t nq = n >> 2;
+    const int4* c4 = reinterpret_cast<const int4*>(col);
+    for (uint64_t q = tid; q < nq; q += T) {
+      const int4 v = ld_stream(c4 + q);
+      s += (int64_t)v.x + v.y + (int64_t)v.z + v.w;
+    }
+    const uint64_t r = (nq << 2) + tid;
+    if (r < n) s += col[r];
+  } else {
+    for (uint64_t r = tid; r < n; r += T) s += col[r];
+  }
+  __shared__ uint64_t sw[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t v = warp_sum_u64((uint64_t)s);
+  if (lane == 0) sw[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < kThreads / 32; w++) t += sw[w];
+    partials[blockIdx.x] = (int64_t)t;
+  }
+  if (!grid_last_block(ticket)) return;
+  uint64_t a = 0;
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += kThreads) a += (uint64_t)__ldcg(partials + i);
+  a = warp_sum_u64(a);
+  __syncthreads();
+  if (lane == 0) sw[warp] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < kThreads / 32; w++) t += sw[w];
+    *out += (int64_t)t;
+  }
+}
+
+__global__ void set_clear_kernel(int32_t* set, uint32_t cap) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) set[i] = kEmptyKey;
+}
+
+__global__ void set_insert_kernel(const int32_t* __restrict__ keys, uint64_t n, int32_t* set, uint32_t cap,
+                                  uint32_t* status) {
+  const uint32_t mask = cap - 1;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = keys[i];
+    if (k == kEmptyKey) { set_status(status, ST_KEY_RANGE); continue; }
+    uint32_t s = key_slot(k, mask);
+    bool done = false;
+    for (uint32_t p = 0; p < cap && !done; p++, s = (s + 1) & mask) {
+      const int32_t prev = atomicCAS(&set[s], kEmptyKey, k);
+      done = (prev == kEmptyKey || prev == k);   // duplicates keep one entry (set semantics)
+    }
+    if (!done) set_status(status, ST_CAPACITY);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) set_probe_count_kernel(const int32_t* __restrict__ keys, uint64_t n,
+                                                                   const int32_t* __restrict__ set, uint32_t cap,
+                                                                   unsigned long long* count) {
+  const uint32_t mask = cap - 1;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint32_t c = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = ld_stream(keys + i);
+    if (k == kEmptyKey) continue;
+    uint32_t s = key_slot(k, mask);
+    for (uint32_t p = 0; p < cap; p++, s = (s + 1) & mask) {
+      const int32_t v = __ldg(set + s);
+      if (v == k) { c++; break; }
+      if (v == kEmptyKey) break;
+    }
+  }
+  c = __reduce_add_sync(FULL_MASK, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+unsigned grid_of(gpudb_ctx* ctx, uint64_t items, int per_sm) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + kThreads - 1) / kThreads, (uint64_t)ctx->sm_count * per_sm));
+}
+
+}  // namespace
+
+// Open-addressing set of the build keys (capacity a power of two, <= 50% load).
+int build_key_set(Call& call, const int32_t* keys, uint64_t n, int32_t** set_out, uint32_t* cap_out) {
+  gpudb_ctx* ctx = call.ctx();
+  uint32_t cap = 1024;
+  while (cap < 2 * n && cap < (1u << 31)) cap <<= 1;
+  void* set = nullptr;
+  int rc = scratch(ctx, "join.set", (size_t)cap * 4, &set);
+  if (rc) return rc;
+  GPUDB_LAUNCH(call, set_clear_kernel, grid_of(ctx, cap, 16), kThreads, 0, (int32_t*)set, cap);
+  if (n) GPUDB_LAUNCH(call, set_insert_kernel, grid_of(ctx, n, 16), kThreads, 0, keys, n, (int32_t*)set, cap, call.status());
+  *set_out = (int32_t*)set;
+  *cap_out = cap;
+  return GPUDB_OK;
+}
+
+}  // namespace gpudb
+
+using namespace gpudb;
+
+extern "C" int gpudb_select_lt(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int32_t value, uint32_t* out_bits,
+                               uint32_t* out_rows, uint64_t* count, gpudb_timing* t, const gpudb_exec* ex) {
+  if (!ctx) return GPUDB_E_INVALID;
+  if (!count || (n && !col)) return fail(ctx, GPUDB_E_INVALID, "select: col and count are required");
+  if (n >= (1ull << 32)) return fail(ctx, GPUDB_E_INVALID, "select: at most 2^32-1 rows (32-bit row ids)");
+  Call call(ctx, ex, t);
+  int rc = call.begin(16);
+  if (rc) return rc;
+  const uint64_t tiles = (n + kSelTile - 1) / kSelTile;
+  void* tmp = nullptr;
+  rc = scratch(ctx, "select.tiles", (tiles + 1) * 4 + (tiles + 2) * 8 * 2 + 64, &tmp);
+  if (rc) return rc;
+  uint32_t* tile_counts = static_cast<uint32_t*>(tmp);
+  uint64_t* tile_off = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(tmp) + ((tiles + 1) * 4 + 15) / 16 * 16);
+  uint64_t* scan_tmp = tile_off + tiles + 2;
+  uint64_t* total = call.result<uint64_t>();
+  if (n) {
+    GPUDB_LAUNCH(call, select_count_kernel, (unsigned)tiles, kThreads, 0, col, n, value, out_bits, tile_counts);
+    rc = exclusive_scan<uint32_t, uint64_t>(call, tile_counts, tiles, tile_off, scan_tmp, total);
+    if (rc) return rc;
+    if (out_rows)
+      GPUDB_LAUNCH(call, select_rows_kernel, (unsigned)tiles, kThreads, 0, col, n, value, (const uint64_t*)tile_off,
+                   out_rows);
+  }
+  return call.finish(16, [count](const uint8_t* h) {
+    std::memcpy(count, h, 8);
+    return GPUDB_OK;
+  });
+}
+
+extern "C" int gpudb_sum_i32(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int64_t* sum, gpudb_timing* t,
+                             const gpudb_exec* ex) {
+  if (!ctx) return GPUDB_E_INVALID;
+  if (!sum || (n && !col)) return fail(ctx, GPUDB_E_INVALID, "sum: col and sum are required");
+  Call call(ctx, ex, t);
+  int rc = call.begin(16);
+  if (rc) return rc;
+  if (n) {
+    const unsigned grid = grid_of(ctx, n / 4 + 1, 8);
+    void* p = nullptr;
+    Buffer& b = ctx->scratch["sum.partials"];
+    const bool fresh = b.bytes < (size_t)grid * 8 + 256;
+    rc = scratch(ctx, "sum.partials", (size_t)grid * 8 + 256, &p);
+    if (rc) return rc;
+    if (fresh) GPUDB_CUDA(ctx, cudaMemset(p, 0, (size_t)grid * 8 + 256));
+    const bool vec = (reinterpret_cast<uintptr_t>(col) & 15u) == 0;
+    GPUDB_LAUNCH(call, sum_i32_kernel, grid, kThreads, 0, col, n, vec, (int64_t*)((uint8_t*)p + 256), (unsigned*)p,
+                 call.result<int64_t>());
+  }
+  return call.finish(16, [sum](const uint8_t* h) {
+    std::memcpy(sum, h, 8);
+    return GPUDB_OK;
+  });
+}
+
+extern "C" int gpudb_hash_join_count(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n_build,
+                                     const int32_t* probe_keys, uint64_t n_probe, int32_t mode, uint64_t* matches,
+                                     gpudb_timing* t, const gpudb_exec* ex) {
+  if (!ctx) return GPUDB_E_INVALID;
+  if (!matches || (n_build && !build_keys) || (n_probe && !probe_keys))
+    return fail(ctx, GPUDB_E_INVALID, "join: keys and matches are required");
+  if (mode != GPUDB_JOIN_GLOBAL && mode != GPUDB_JOIN_RADIX) return fail(ctx, GPUDB_E_INVALID, "join: unknown mode");
+  if (n_build > (1ull << 30)) return fail(ctx, GPUDB_E_INVALID, "join: build side larger than 2^30 rows");
+  Call call(ctx, ex, t);
+  int rc = call.begin(16);
+  if (rc) return rc;
+  unsigned long long* cnt = call.result<unsigned long long>();
+  if (mode == GPUDB_JOIN_GLOBAL) {
+    int32_t* set = nullptr;
+    uint32_t cap = 0;
+    rc = build_key_set(call, build_keys, n_build, &set, &cap);
+    if (rc) return rc;
+    if (n_probe)
+      GPUDB_LAUNCH(call, set_probe_count_kernel, grid_of(ctx, n_probe, 8), kThreads, 0, probe_keys, n_probe,
+                   (const int32_t*)set, cap, cnt);
+  } else {
+    rc = radix_join_count(call, build_keys, n_build, probe_keys, n_probe, cnt);
+    if (rc) return rc;
+  }
+  return call.finish(16, [matches](const uint8_t* h) {
+    std::memcpy(matches, h, 8);
+    return GPUDB_OK;
+  });
+}

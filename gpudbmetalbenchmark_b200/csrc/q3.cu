@@ -29,6 +29,7 @@
 #include "engine.h"
 #include "join_common.cuh"
 #include "q3.h"
+#include "radix.cuh"
 
 namespace gpudb {
 
@@ -176,7 +177,152 @@ __global__ void __launch_bounds__(kTopkThreads) q3_topk_slots_kernel(const Q3Slo
   block_topk(v, k, out + (size_t)blockIdx.x * k);
 }
 
+// ---- radix mode ----------------------------------------------------------------------
+// Fact rows with ship_date > cutoff, compacted to (order_key, ext*(100-disc)).
+__global__ void q3_fact_filter_kernel(const int32_t* __restrict__ lkey, const int32_t* __restrict__ lship,
+                                      const int64_t* __restrict__ lext, const int32_t* __restrict__ ldisc, uint64_t n,
+                                      int32_t ship_gt, int32_t* out_key, int64_t* out_val, uint32_t* count) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t end = (n + 31) & ~31ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+    const bool take = i < n && ld_stream(lship + i) > ship_gt;
+    const uint32_t pos = warp_append(take, count);
+    if (take) {
+      out_key[pos] = lkey[i];
+      out_val[pos] = lext[i] * (int64_t)(100 - ldisc[i]);
+    }
+  }
+}
+
+constexpr uint32_t kQ3PartCap = 2048;               // shared slots per partition table
+constexpr uint32_t kQ3PartChunk = kQ3PartCap / 2;   // build rows per chunk
+
+// One block per partition: shared table of the partition's orders (in chunks), probe of its
+// fact rows with shared 64-bit atomics, then a block top-k carried across chunks.
+__global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
+    const int32_t* __restrict__ bk, const int32_t* __restrict__ bdate, const uint32_t* __restrict__ boff,
+    const int32_t* __restrict__ pk, const int64_t* __restrict__ pval, const uint32_t* __restrict__ poff, int k,
+    u128* cand, unsigned long long* groups, uint32_t* status) {
+  __shared__ int32_t hkey[kQ3PartCap], hdate[kQ3PartCap];
+  __shared__ unsigned long long hrev[kQ3PartCap];
+  __shared__ uint32_t hhit[kQ3PartCap];
+  __shared__ u128 carry[GPUDB_Q3_MAX_K];
+  const uint32_t part = blockIdx.x, mask = kQ3PartCap - 1;
+  const uint32_t b0 = boff[part], b1 = boff[part + 1], p0 = poff[part], p1 = poff[part + 1];
+  for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
+  uint32_t ngroups = 0;
+  for (uint32_t c0 = b0; c0 < b1; c0 += kQ3PartChunk) {
+    const uint32_t c1 = min(c0 + kQ3PartChunk, b1);
+    for (uint32_t i = threadIdx.x; i < kQ3PartCap; i += kTopkThreads) { hkey[i] = kEmptyKey; hrev[i] = 0; hhit[i] = 0; }
+    __syncthreads();
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += kTopkThreads) {
+      const int32_t key = bk[i];
+      uint32_t s = key_slot(key, mask);
+      for (uint32_t t = 0; t < kQ3PartCap; t++, s = (s + 1) & mask) {
+        const int32_t prev = atomicCAS(&hkey[s], kEmptyKey, key);
+        if (prev == kEmptyKey) { hdate[s] = bdate[i]; break; }
+        if (prev == key) { set_status(status, ST_DUPLICATE); break; }
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kTopkThreads) {
+      const int32_t key = pk[i];
+      if (key == kEmptyKey) continue;
+      uint32_t s = key_slot(key, mask);
+      for (uint32_t t = 0; t < kQ3PartCap; t++, s = (s + 1) & mask) {
+        const int32_t hk = hkey[s];
+        if (hk == key) { atomicAdd(&hrev[s], (unsigned long long)pval[i]); atomicAdd(&hhit[s], 1u); break; }
+        if (hk == kEmptyKey) break;
+      }
+    }
+    __syncthreads();
+    u128 v[kTopkPerThread];
+#pragma unroll
+    for (int j = 0; j < kTopkPerThread; j++) v[j] = 0;
+#pragma unroll
+    for (int j = 0; j < (int)(kQ3PartCap / kTopkThreads); j++) {
+      const uint32_t s = threadIdx.x * (kQ3PartCap / kTopkThreads) + j;
+      if (hhit[s]) { v[j] = topk_compose((int64_t)hrev[s], hdate[s], hkey[s]); ngroups++; }
+    }
+    if ((int)threadIdx.x < k) v[kTopkPerThread - 1] = carry[threadIdx.x];
+    __syncthreads();
+    block_topk(v, k, carry);
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < k; i += kTopkThreads) cand[(size_t)part * k + i] = carry[i];
+  ngroups = __reduce_add_sync(FULL_MASK, ngroups);
+  if ((threadIdx.x & 31) == 0 && ngroups) atomicAdd(groups, (unsigned long long)ngroups);
+}
+
 }  // namespace
+
+int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_lineitem* li,
+             const gpudb_q3_params& p, uint8_t* result) {
+  gpudb_ctx* ctx = call.ctx();
+  cudaStream_t s = call.stream();
+  const uint32_t words = (uint32_t)(cu.key_max >> 5) + 1;
+  const uint64_t n_or = std::max<uint64_t>(od.n_rows, 1), n_li = std::max<uint64_t>(li->n_rows, 1);
+  const int bits = p.radix_bits > 0 ? std::min(p.radix_bits, (int)kRadixMaxBits) : radix_bits_for(od.n_rows, 512);
+  const uint64_t parts = 1ull << bits;
+  void *bitmap, *bstage, *fstage, *count, *bpart, *fpart, *offs, *cand;
+  int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
+  if (!rc) rc = scratch(ctx, "q3r.build", n_or * 4 * 4 + 256, &bstage);          // key, date, tmp key, tmp date
+  if (!rc) rc = scratch(ctx, "q3r.fact", n_li * 12 * 2 + 1024, &fstage);           // key, value, tmp
+  if (!rc) rc = scratch(ctx, "q3.count", 256, &count);
+  if (!rc) rc = scratch(ctx, "q3r.bpart", n_or * 8 + 256, &bpart);
+  if (!rc) rc = scratch(ctx, "q3r.fpart", n_li * 12 + 1024, &fpart);
+  if (!rc) rc = scratch(ctx, "q3r.offs", (2 * (parts + 1) + 64) * 4, &offs);
+  const size_t cand_elems = (size_t)parts * p.k;
+  if (!rc) rc = scratch(ctx, "q3.cand", (cand_elems * 2 + 64) * sizeof(u128), &cand);
+  if (rc) return rc;
+  uint32_t* cnt = static_cast<uint32_t*>(count);   // [0] orders, [1] fact rows
+  GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+  const int sms = ctx->sm_count;
+  auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
+  int32_t* bkey = static_cast<int32_t*>(bstage);
+  int32_t* bdate = bkey + n_or;
+  int32_t* bkey_t = bdate + n_or;
+  int32_t* bdate_t = bkey_t + n_or;
+  int32_t* fkey = static_cast<int32_t*>(fstage);
+  int64_t* fval = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(fstage) + ((n_li * 4 + 255) / 256) * 256);
+  int32_t* fkey_t = reinterpret_cast<int32_t*>(fval + n_li);
+  int64_t* fval_t = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(static_cast<void*>(fkey_t)) + ((n_li * 4 + 255) / 256) * 256);
+  int32_t* bk = static_cast<int32_t*>(bpart);
+  int32_t* bd = bk + n_or;
+  int32_t* pk = static_cast<int32_t*>(fpart);
+  int64_t* pv = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(fpart) + ((n_li * 4 + 255) / 256) * 256);
+  uint32_t* boff = static_cast<uint32_t*>(offs);
+  uint32_t* poff = boff + parts + 16;
+  if (cu.n_rows)
+    GPUDB_LAUNCH(call, bitmap_build_kernel, grid(cu.n_rows), 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows,
+                 cu.key_max, (uint32_t*)bitmap, call.status());
+  if (od.n_rows)
+    GPUDB_LAUNCH(call, orders_filter_kernel, grid(od.n_rows), 256, 0, od.order_key, od.cust_key, od.order_date, od.n_rows,
+                 p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, bkey, bdate, cnt, call.status());
+  const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
+  rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
+    if (c.n_rows == 0) return (int)GPUDB_OK;
+    GPUDB_LAUNCH(call, q3_fact_filter_kernel, grid(c.n_rows), 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount,
+                 c.n_rows, p.ship_date_gt, fkey, fval, cnt + 1);
+    return (int)GPUDB_OK;
+  });
+  if (rc) return rc;
+  rc = radix_partition_run<int32_t>(call, bkey, bdate, n_or, cnt, bits, bk, bd, boff, bkey_t, bdate_t);
+  if (!rc) rc = radix_partition_run<int64_t>(call, fkey, fval, n_li, cnt + 1, bits, pk, pv, poff, fkey_t, fval_t);
+  if (rc) return rc;
+  u128* cbuf = static_cast<u128*>(cand);
+  unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
+  u128* rows = reinterpret_cast<u128*>(result + 16);
+  GPUDB_LAUNCH(call, q3_partition_kernel, (unsigned)parts, kTopkThreads, 0, (const int32_t*)bk, (const int32_t*)bd,
+               (const uint32_t*)boff, (const int32_t*)pk, (const int64_t*)pv, (const uint32_t*)poff, p.k, cbuf, groups,
+               call.status());
+  if (parts == 1) {
+    GPUDB_CUDA(ctx, cudaMemcpyAsync(rows, cbuf, (size_t)p.k * sizeof(u128), cudaMemcpyDeviceToDevice, s));
+    return GPUDB_OK;
+  }
+  return q3_topk_levels(call, cbuf, cand_elems, p.k, cbuf + cand_elems, cbuf + cand_elems + cand_elems / 2 + 32, rows);
+}
 
 int q3_topk_levels(Call& call, u128* cand, uint64_t n_cand, int k, u128* scratch_a, u128* scratch_b, u128* final_out) {
   // reduce n_cand candidates (k per 4096-candidate tile) until one block remains

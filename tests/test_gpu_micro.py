@@ -1,0 +1,133 @@
+"""Microbenchmark operators and the radix partitioner on the GPU against the CPU oracle:
+selection (bitmask + ordered row ids), exact column sum, hash-join match count (global and
+radix), stable radix partitioning (identical to the oracle's, whose partition numbers are
+pinned to the reference's own sf100_radix_* kernels), and all-pairs radix join."""
+import numpy as np
+import pytest
+
+from gpudbmetalbenchmark_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [0, 1, 31, 32, 33, 4095, 4097, 1_000_003])
+@pytest.mark.parametrize("value", [0, 1000, 2527, 5000])
+def test_select_lt(engine, orc, n, value):
+    col = orc.gen(1, n, seed=n + 7)
+    dcol = engine.to_device(col) if n else None
+    bits = engine.device_array(((n + 31) // 32) * 4 + 4)
+    rows = engine.device_array(n * 4 + 4)
+    try:
+        c = engine.select_lt(dcol, n, value, bits, rows)
+        wc, wbits, wrows = orc.select_lt(col, value)
+        assert c == wc
+        assert np.array_equal(engine.to_host(bits, (n + 31) // 32, np.uint32), wbits)
+        assert np.array_equal(engine.to_host(rows, c, np.uint32), wrows)
+        assert engine.select_lt(dcol, n, value) == wc   # count only
+    finally:
+        for p in (dcol, bits, rows):
+            if p:
+                engine.device_free(p)
+
+
+@pytest.mark.parametrize("n,off", [(0, 0), (1, 0), (5, 1), (1_000_001, 0), (1_000_001, 3), (60_000_000, 0)])
+def test_sum_i32(engine, orc, n, off):
+    col = orc.gen(2, n + off, seed=3)
+    d = engine.to_device(col) if n + off else None
+    try:
+        got = engine.sum_i32(d + 4 * off if d else None, n)
+        assert got == orc.sum_i32(col[off:])
+    finally:
+        if d:
+            engine.device_free(d)
+
+
+def test_sum_i32_extreme_values(engine, orc):
+    col = np.full(3_000_001, np.iinfo(np.int32).max, np.int32)
+    col[::2] = np.iinfo(np.int32).min
+    d = engine.to_device(col)
+    try:
+        assert engine.sum_i32(d, len(col)) == int(col.astype(np.int64).sum())
+    finally:
+        engine.device_free(d)
+
+
+@pytest.mark.parametrize("mode", [capi.JOIN_GLOBAL, capi.JOIN_RADIX])
+@pytest.mark.parametrize("nb,np_,orders", [(1_500_000, 6_000_000, 1_500_000), (1000, 5000, 700), (1, 1, 1),
+                                           (0, 100, 10), (100, 0, 10), (200_000, 300_000, 50_000)])
+def test_hash_join_count(engine, orc, mode, nb, np_, orders):
+    b = orc.gen(30, nb, seed=1) if orders >= nb else orc.gen(8, nb, seed=1, n_orders=orders, order_mode=2)
+    p = orc.gen(8, np_, seed=2, n_orders=max(orders, 1) * 2, order_mode=2)
+    db = engine.to_device(b) if nb else None
+    dp = engine.to_device(p) if np_ else None
+    try:
+        assert engine.hash_join_count(db, nb, dp, np_, mode) == orc.join_count(b, p)
+    finally:
+        for x in (db, dp):
+            if x:
+                engine.device_free(x)
+
+
+@pytest.mark.parametrize("bits", [0, 1, 3, 8, 9, 10, 12, 16])
+@pytest.mark.parametrize("n", [1, 4096, 4097, 300_001])
+def test_radix_partition_is_the_oracle_partition(engine, orc, bits, n):
+    keys = orc.gen(8, n, seed=bits + 5, n_orders=max(n // 3, 1), order_mode=2)
+    pay = np.arange(n, dtype=np.int32) * 7 + 3
+    dk, dp = engine.to_device(keys), engine.to_device(pay)
+    ko, po, off = (engine.device_array(n * 4), engine.device_array(n * 4), engine.device_array(((1 << bits) + 1) * 4))
+    try:
+        engine.radix_partition(dk, dp, n, bits, ko, po, off)
+        wk, wp, woff = orc.radix_partition(keys, pay, bits)
+        assert np.array_equal(engine.to_host(off, (1 << bits) + 1, np.uint32), woff)
+        assert np.array_equal(engine.to_host(ko, n, np.int32), wk)
+        assert np.array_equal(engine.to_host(po, n, np.int32), wp)
+        engine.radix_partition(dk, None, n, bits, ko, po, off)   # payload = row ids
+        _, rows, _ = orc.radix_partition(keys, np.arange(n, dtype=np.int32), bits)
+        assert np.array_equal(engine.to_host(po, n, np.int32), rows)
+    finally:
+        for x in (dk, dp, ko, po, off):
+            engine.device_free(x)
+
+
+def test_radix_partition_bad_bits(engine):
+    with pytest.raises(capi.GpudbError) as e:
+        engine.radix_partition(None, None, 0, 17, 1, 1, 1)
+    assert e.value.code == capi.E_INVALID
+
+
+@pytest.mark.parametrize("nb,np_,orders", [(15_000, 60_000, 20_000), (3000, 9000, 4000), (1, 5, 1)])
+def test_radix_join_pairs(engine, orc, nb, np_, orders):
+    b = orc.gen(8, nb, seed=2, n_orders=orders, order_mode=2)   # duplicates on both sides
+    p = orc.gen(8, np_, seed=3, n_orders=orders, order_mode=2)
+    _, _, total = orc.join_pairs(b, p, 0)
+    db, dp = engine.to_device(b), engine.to_device(p)
+    ob, op = engine.device_array(total * 4 + 4), engine.device_array(total * 4 + 4)
+    try:
+        n = engine.radix_join_pairs(db, nb, dp, np_, ob, op, total)
+        assert n == total
+        got = sorted(zip(engine.to_host(op, n, np.int32).tolist(), engine.to_host(ob, n, np.int32).tolist()))
+        wb, wp, _ = orc.join_pairs(b, p, total)
+        assert got == sorted(zip(wp.tolist(), wb.tolist()))
+        # a short output buffer: the total is still reported, nothing is written past it
+        assert engine.radix_join_pairs(db, nb, dp, np_, ob, op, total // 2) == total
+    finally:
+        for x in (db, dp, ob, op):
+            engine.device_free(x)
+
+
+def test_radix_join_skewed_partition(engine, orc):
+    """One key repeated 5000 times on the build side: its partition needs several chunks."""
+    b = np.concatenate([np.full(5000, 77, np.int32), np.arange(1000, 3000, dtype=np.int32)])
+    p = np.concatenate([np.full(3, 77, np.int32), np.arange(0, 4000, 7, dtype=np.int32)])
+    db, dp = engine.to_device(b), engine.to_device(p)
+    _, _, total = orc.join_pairs(b, p, 0)
+    ob, op = engine.device_array(total * 4), engine.device_array(total * 4)
+    try:
+        assert engine.radix_join_pairs(db, len(b), dp, len(p), ob, op, total) == total
+        got = sorted(zip(engine.to_host(op, total, np.int32).tolist(), engine.to_host(ob, total, np.int32).tolist()))
+        wb, wp, _ = orc.join_pairs(b, p, total)
+        assert got == sorted(zip(wp.tolist(), wb.tolist()))
+        assert engine.hash_join_count(db, len(b), dp, len(p), capi.JOIN_RADIX) == orc.join_count(b, p)
+    finally:
+        for x in (db, dp, ob, op):
+            engine.device_free(x)

@@ -8,7 +8,7 @@ from gpudbmetalbenchmark_b200 import capi
 
 pytestmark = pytest.mark.gpu
 
-MODES = [capi.JOIN_GLOBAL]
+MODES = [capi.JOIN_GLOBAL, capi.JOIN_RADIX]
 
 
 def run(engine, cu, od, li, mode=capi.JOIN_GLOBAL, location=capi.MEM_DEVICE, **kw):
