@@ -19,6 +19,7 @@ ERROR_NAMES = {0: "OK", -1: "E_INVALID", -2: "E_CUDA", -3: "E_OOM", -4: "E_NODEV
 
 MEM_DEVICE, MEM_HOST = 0, 1
 OPT_CHUNK_ROWS = 1
+OPT_SCAN_VARIANT = 2
 JOIN_GLOBAL, JOIN_RADIX = 0, 1
 ORDERS_NONE, ORDERS_CLUSTERED, ORDERS_UNIFORM = 0, 1, 2
 Q3_MAX_K = 64

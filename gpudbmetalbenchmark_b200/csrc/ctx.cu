@@ -382,6 +382,10 @@ int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value) {
       if (value < 16) return fail(ctx, GPUDB_E_INVALID, "chunk rows must be >= 16");
       ctx->chunk_rows = (uint64_t)value;
       return GPUDB_OK;
+    case GPUDB_OPT_SCAN_VARIANT:
+      if (value < 0 || value > 7) return fail(ctx, GPUDB_E_INVALID, "scan variant must be 0..7");
+      ctx->scan_variant = (int)value;
+      return GPUDB_OK;
     default:
       return fail(ctx, GPUDB_E_INVALID, "unknown option %d", option);
   }

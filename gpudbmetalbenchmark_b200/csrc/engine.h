@@ -46,6 +46,7 @@ struct gpudb_ctx {
   std::string err;
   uint64_t launches = 0;
   uint64_t chunk_rows = gpudb::kDefaultChunkRows;
+  int scan_variant = 0;                // scan kernel choice (GPUDB_OPT_SCAN_VARIANT)
   std::unordered_map<std::string, gpudb::Buffer> scratch;
   uint8_t* d_slots = nullptr;          // result slots (device)
   uint8_t* h_slots = nullptr;          // their pinned host mirror

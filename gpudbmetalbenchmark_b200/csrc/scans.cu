@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "tma.cuh"
 
 namespace gpudb {
 namespace {
@@ -153,19 +154,24 @@ __device__ __forceinline__ void q1_row(Q1Acc& a, int32_t s, int32_t qt, int64_t 
   const uint64_t ed = (uint64_t)e * (uint32_t)d;
   const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)t;
   const uint64_t pk = ((uint64_t)(uint32_t)qt << 32) | ((uint64_t)(uint32_t)d << 13) | 1u;
+  // Exactly one group takes the row. Predicated adds (no branch): a data-dependent `if`
+  // per group compiles to divergent branches that stall on branch resolution.
 #pragma unroll
   for (int k = 0; k < 6; k++) {
-    if (g == (uint32_t)k) {
-      a.P[k] += pk;
-      a.E[k] += (uint64_t)e;
-      a.ED[k] += ed;
-      a.EDT[k] += edt;
-    }
+    asm("{\n\t.reg .pred p;\n\t"
+        "setp.eq.u32 p, %4, %5;\n\t"
+        "@p add.u64 %0, %0, %6;\n\t"
+        "@p add.u64 %1, %1, %7;\n\t"
+        "@p add.u64 %2, %2, %8;\n\t"
+        "@p add.u64 %3, %3, %9;\n\t}"
+        : "+l"(a.P[k]), "+l"(a.E[k]), "+l"(a.ED[k]), "+l"(a.EDT[k])
+        : "r"(g), "r"((uint32_t)k), "l"(pk), "l"((uint64_t)e), "l"(ed), "l"(edt));
   }
 }
 
+template <int T>
 __device__ __forceinline__ void q1_fold(Q1Acc& a, u128* partials, unsigned* ticket, u128* out, uint32_t* status) {
-  __shared__ u128 red[kThreads / 32][6 * kQ1Raw];
+  __shared__ u128 red[T / 32][6 * kQ1Raw];
   __shared__ u128 tot[6 * kQ1Raw];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (__syncthreads_or(a.bad) && threadIdx.x == 0) set_status(status, ST_DOMAIN);
@@ -181,7 +187,7 @@ __device__ __forceinline__ void q1_fold(Q1Acc& a, u128* partials, unsigned* tick
   __syncthreads();
   if (threadIdx.x < 6 * kQ1Raw) {
     u128 s = 0;
-    for (int w = 0; w < kThreads / 32; w++) s += red[w][threadIdx.x];
+    for (int w = 0; w < T / 32; w++) s += red[w][threadIdx.x];
     partials[(size_t)blockIdx.x * 6 * kQ1Raw + threadIdx.x] = s;
   }
   if (!grid_last_block(ticket)) return;
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 2) q1_vec_kernel(const int4* __restr
     const uint8_t* stat = reinterpret_cast<const uint8_t*>(stat4);
     q1_row(a, ship[r], qty[r], ext[r], disc[r], tax[r], flag[r], stat[r], ship_le);
   }
-  q1_fold(a, partials, ticket, out, status);
+  q1_fold<kThreads>(a, partials, ticket, out, status);
 }
 
 __global__ void __launch_bounds__(kThreads, 2) q1_row_kernel(const int32_t* ship, const int32_t* qty, const int64_t* ext,
@@ -255,7 +261,358 @@ __global__ void __launch_bounds__(kThreads, 2) q1_row_kernel(const int32_t* ship
   const uint64_t T = (uint64_t)gridDim.x * kThreads;
   for (uint64_t r = (uint64_t)blockIdx.x * kThreads + threadIdx.x; r < n; r += T)
     q1_row(a, ship[r], qty[r], ext[r], disc[r], tax[r], flag[r], stat[r], ship_le);
-  q1_fold(a, partials, ticket, out, status);
+  q1_fold<kThreads>(a, partials, ticket, out, status);
+}
+
+// ---- Q1 with TMA-staged column tiles ----------------------------------------------------
+// Persistent: one 512-thread block per SM walks tiles blockIdx, blockIdx+grid, ... of
+// R = 2048*QPT rows. Thread 0 keeps STAGES tiles in flight: for each tile it posts the
+// stage's byte count (26 R) on the stage's mbarrier and issues one bulk copy per column;
+// all threads wait on the barrier (bounded), read their 4*QPT rows from shared memory with
+// 128-bit loads, and a block barrier frees the stage for the next copy. Memory parallelism
+// therefore costs shared memory instead of registers, which the 24 accumulators need.
+// Shapes: QPT=1, STAGES=4 (2048-row tiles) and QPT=2, STAGES=2 (4096-row tiles, half the
+// block barriers per row); both use 212,992 bytes of shared memory.
+constexpr int kQ1TmaThreads = 512;
+
+template <int QPT, int STAGES>
+__global__ void __launch_bounds__(kQ1TmaThreads, 1) q1_tma_kernel(const int32_t* __restrict__ ship, const int32_t* __restrict__ qty,
+                                                                  const int64_t* __restrict__ ext, const int32_t* __restrict__ disc,
+                                                                  const int32_t* __restrict__ tax, const uint8_t* __restrict__ flag,
+                                                                  const uint8_t* __restrict__ stat, uint64_t n, int32_t ship_le,
+                                                                  u128* partials, unsigned* ticket, u128* out, uint32_t* status) {
+  constexpr uint32_t R = 2048u * QPT;            // rows per tile
+  constexpr uint32_t kStage = 26u * R;           // bytes per stage
+  constexpr uint32_t oShip = 0, oQty = 4 * R, oExt = 8 * R, oDisc = 16 * R, oTax = 20 * R, oFlag = 24 * R,
+                     oStat = 25 * R;
+  extern __shared__ __align__(128) uint8_t q1_stage[];
+  __shared__ __align__(8) uint64_t full[STAGES];
+  Q1Acc a;
+#pragma unroll
+  for (int g = 0; g < 6; g++) a.P[g] = a.E[g] = a.ED[g] = a.EDT[g] = 0;
+  a.bad = 0;
+  const uint64_t tiles = n / R;
+  const uint64_t mine = tiles > blockIdx.x ? (tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) mbar_init(&full[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](uint64_t j) {
+    const int s = (int)(j % STAGES);
+    const uint64_t r0 = (blockIdx.x + j * gridDim.x) * (uint64_t)R;
+    uint8_t* st = q1_stage + (size_t)s * kStage;
+    mbar_arrive_expect_tx(&full[s], kStage);
+    bulk_copy_g2s(st + oShip, ship + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oQty, qty + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oExt, ext + r0, R * 8, &full[s]);
+    bulk_copy_g2s(st + oDisc, disc + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oTax, tax + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oFlag, flag + r0, R, &full[s]);
+    bulk_copy_g2s(st + oStat, stat + r0, R, &full[s]);
+  };
+  if (threadIdx.x == 0)
+    for (uint64_t j = 0; j < mine && j < (uint64_t)STAGES; j++) issue(j);
+  uint64_t j = 0;
+  for (; j < mine; j++) {
+    const int s = (int)(j % STAGES);
+    const bool ok = mbar_wait(&full[s], (uint32_t)((j / STAGES) & 1), kMbarPollLimit);
+    if (__syncthreads_or(!ok)) break;
+    const uint8_t* st = q1_stage + (size_t)s * kStage;
+#pragma unroll
+    for (int q = 0; q < QPT; q++) {
+      const int t = threadIdx.x + q * kQ1TmaThreads;   // quad of the tile
+      const int4 sv = *reinterpret_cast<const int4*>(st + oShip + 16 * t);
+      const int4 kv = *reinterpret_cast<const int4*>(st + oQty + 16 * t);
+      const longlong2 e01 = *reinterpret_cast<const longlong2*>(st + oExt + 32 * t);
+      const longlong2 e23 = *reinterpret_cast<const longlong2*>(st + oExt + 32 * t + 16);
+      const int4 dv = *reinterpret_cast<const int4*>(st + oDisc + 16 * t);
+      const int4 tv = *reinterpret_cast<const int4*>(st + oTax + 16 * t);
+      const uint32_t f = *reinterpret_cast<const uint32_t*>(st + oFlag + 4 * t);
+      const uint32_t g = *reinterpret_cast<const uint32_t*>(st + oStat + 4 * t);
+      q1_row(a, sv.x, kv.x, e01.x, dv.x, tv.x, f & 0xFF, g & 0xFF, ship_le);
+      q1_row(a, sv.y, kv.y, e01.y, dv.y, tv.y, (f >> 8) & 0xFF, (g >> 8) & 0xFF, ship_le);
+      q1_row(a, sv.z, kv.z, e23.x, dv.z, tv.z, (f >> 16) & 0xFF, (g >> 16) & 0xFF, ship_le);
+      q1_row(a, sv.w, kv.w, e23.y, dv.w, tv.w, f >> 24, g >> 24, ship_le);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && j + STAGES < mine) issue(j + STAGES);
+  }
+  if (j < mine && threadIdx.x == 0) {
+    // a wait ran out: report it, and let the copies already issued land before leaving
+    set_status(status, ST_TIMEOUT);
+    for (uint64_t k = j; k < mine && k < j + STAGES; k++)
+      mbar_wait(&full[k % STAGES], (uint32_t)((k / STAGES) & 1), kMbarPollLimit);
+  }
+  // rows after the last whole tile
+  if (blockIdx.x == gridDim.x - 1)
+    for (uint64_t r = tiles * R + threadIdx.x; r < n; r += kQ1TmaThreads)
+      q1_row(a, ship[r], qty[r], ext[r], disc[r], tax[r], flag[r], stat[r], ship_le);
+  q1_fold<kQ1TmaThreads>(a, partials, ticket, out, status);
+}
+
+// Same tiles through a producer/consumer ring: `full[s]` completes when a stage's bytes have
+// landed, `empty[s]` when all 16 warps have read it. Warps release stages on their own (no
+// block-wide barrier per tile) and thread 0 refills a stage as soon as it is released, so
+// STAGES-1 tiles stay in flight while the warps compute.
+template <int QPT, int STAGES>
+__global__ void __launch_bounds__(kQ1TmaThreads, 1) q1_ring_kernel(const int32_t* __restrict__ ship, const int32_t* __restrict__ qty,
+                                                                   const int64_t* __restrict__ ext, const int32_t* __restrict__ disc,
+                                                                   const int32_t* __restrict__ tax, const uint8_t* __restrict__ flag,
+                                                                   const uint8_t* __restrict__ stat, uint64_t n, int32_t ship_le,
+                                                                   u128* partials, unsigned* ticket, u128* out, uint32_t* status) {
+  constexpr uint32_t R = 2048u * QPT;
+  constexpr uint32_t kStage = 26u * R;
+  constexpr uint32_t oShip = 0, oQty = 4 * R, oExt = 8 * R, oDisc = 16 * R, oTax = 20 * R, oFlag = 24 * R,
+                     oStat = 25 * R;
+  constexpr uint32_t kWarps = kQ1TmaThreads / 32;
+  extern __shared__ __align__(128) uint8_t q1_ring[];
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+  Q1Acc a;
+#pragma unroll
+  for (int g = 0; g < 6; g++) a.P[g] = a.E[g] = a.ED[g] = a.EDT[g] = 0;
+  a.bad = 0;
+  const uint64_t tiles = n / R;
+  const uint64_t mine = tiles > blockIdx.x ? (tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], kWarps); }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  uint64_t issued = 0;       // thread 0: tiles whose copies were issued
+  bool timed_out = false;
+  auto issue = [&](uint64_t j) {
+    const int s = (int)(j % STAGES);
+    const uint64_t r0 = (blockIdx.x + j * gridDim.x) * (uint64_t)R;
+    uint8_t* st = q1_ring + (size_t)s * kStage;
+    mbar_arrive_expect_tx(&full[s], kStage);
+    bulk_copy_g2s(st + oShip, ship + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oQty, qty + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oExt, ext + r0, R * 8, &full[s]);
+    bulk_copy_g2s(st + oDisc, disc + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oTax, tax + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oFlag, flag + r0, R, &full[s]);
+    bulk_copy_g2s(st + oStat, stat + r0, R, &full[s]);
+  };
+  uint64_t j = 0;
+  for (; j < mine; j++) {
+    if (threadIdx.x == 0) {
+      // keep the ring full: reuse a stage only after every warp has released it
+      while (issued < mine && issued < j + STAGES) {
+        if (issued >= (uint64_t)STAGES &&
+            !mbar_wait(&empty[issued % STAGES], (uint32_t)(((issued / STAGES) - 1) & 1), kMbarPollLimit)) {
+          timed_out = true;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    const int s = (int)(j % STAGES);
+    if (timed_out || !mbar_wait(&full[s], (uint32_t)((j / STAGES) & 1), kMbarPollLimit)) { timed_out = true; break; }
+    const uint8_t* st = q1_ring + (size_t)s * kStage;
+#pragma unroll
+    for (int q = 0; q < QPT; q++) {
+      const int t = threadIdx.x + q * kQ1TmaThreads;
+      const int4 sv = *reinterpret_cast<const int4*>(st + oShip + 16 * t);
+      const int4 kv = *reinterpret_cast<const int4*>(st + oQty + 16 * t);
+      const longlong2 e01 = *reinterpret_cast<const longlong2*>(st + oExt + 32 * t);
+      const longlong2 e23 = *reinterpret_cast<const longlong2*>(st + oExt + 32 * t + 16);
+      const int4 dv = *reinterpret_cast<const int4*>(st + oDisc + 16 * t);
+      const int4 tv = *reinterpret_cast<const int4*>(st + oTax + 16 * t);
+      const uint32_t f = *reinterpret_cast<const uint32_t*>(st + oFlag + 4 * t);
+      const uint32_t g = *reinterpret_cast<const uint32_t*>(st + oStat + 4 * t);
+      q1_row(a, sv.x, kv.x, e01.x, dv.x, tv.x, f & 0xFF, g & 0xFF, ship_le);
+      q1_row(a, sv.y, kv.y, e01.y, dv.y, tv.y, (f >> 8) & 0xFF, (g >> 8) & 0xFF, ship_le);
+      q1_row(a, sv.z, kv.z, e23.x, dv.z, tv.z, (f >> 16) & 0xFF, (g >> 16) & 0xFF, ship_le);
+      q1_row(a, sv.w, kv.w, e23.y, dv.w, tv.w, f >> 24, g >> 24, ship_le);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (timed_out) set_status(status, ST_TIMEOUT);
+  if (threadIdx.x == 0)
+    // copies this thread issued but never consumed must land before the block exits
+    for (uint64_t k = j; k < issued; k++) mbar_wait(&full[k % STAGES], (uint32_t)((k / STAGES) & 1), kMbarPollLimit);
+  if (blockIdx.x == gridDim.x - 1)
+    for (uint64_t r = tiles * R + threadIdx.x; r < n; r += kQ1TmaThreads)
+      q1_row(a, ship[r], qty[r], ext[r], disc[r], tax[r], flag[r], stat[r], ship_le);
+  q1_fold<kQ1TmaThreads>(a, partials, ticket, out, status);
+}
+
+// Ring of TMA tiles as above, but each thread's 6 x 4 group accumulators live in shared
+// memory ([metric][group][thread], conflict-free for a warp) and a row updates only its own
+// group: 4 load-add-store per row instead of 24 predicated 64-bit adds.
+template <int THREADS, int STAGES>
+__global__ void __launch_bounds__(THREADS, 1) q1_ring_smem_kernel(const int32_t* __restrict__ ship, const int32_t* __restrict__ qty,
+                                                                  const int64_t* __restrict__ ext, const int32_t* __restrict__ disc,
+                                                                  const int32_t* __restrict__ tax, const uint8_t* __restrict__ flag,
+                                                                  const uint8_t* __restrict__ stat, uint64_t n, int32_t ship_le,
+                                                                  u128* partials, unsigned* ticket, u128* out, uint32_t* status) {
+  constexpr uint32_t R = THREADS * 4u;            // one quad per thread per tile
+  constexpr uint32_t kStage = 26u * R;
+  constexpr uint32_t oShip = 0, oQty = 4 * R, oExt = 8 * R, oDisc = 16 * R, oTax = 20 * R, oFlag = 24 * R,
+                     oStat = 25 * R;
+  constexpr uint32_t kWarps = THREADS / 32;
+  extern __shared__ __align__(128) uint8_t q1_dyn[];
+  uint64_t* acc = reinterpret_cast<uint64_t*>(q1_dyn + (size_t)STAGES * kStage);   // [4][6][THREADS]
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+  const int t = threadIdx.x, lane = t & 31;
+#pragma unroll
+  for (int i = 0; i < 24; i++) acc[i * THREADS + t] = 0;
+  uint32_t bad = 0;
+  const uint64_t tiles = n / R;
+  const uint64_t mine = tiles > blockIdx.x ? (tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  if (t == 0) {
+    for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], kWarps); }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto row = [&](int32_t s, int32_t qt, int64_t e, int32_t d, int32_t tx, uint32_t f, uint32_t st) {
+    if (!((s <= ship_le) & (f <= 2u) & (st <= 1u))) return;
+    bad |= ((uint32_t)qt >= 65536u) | ((uint32_t)d > 100u) | ((uint32_t)tx > 100u) | ((uint64_t)e >= (1ull << 36));
+    const uint64_t ed = (uint64_t)e * (uint32_t)d;
+    const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)tx;
+    const uint64_t pk = ((uint64_t)(uint32_t)qt << 32) | ((uint64_t)(uint32_t)d << 13) | 1u;
+    uint64_t* p = acc + (f * 2u + st) * THREADS + t;
+    p[0] += pk;
+    p[6 * THREADS] += (uint64_t)e;
+    p[12 * THREADS] += ed;
+    p[18 * THREADS] += edt;
+  };
+  uint64_t issued = 0;
+  bool timed_out = false;
+  auto issue = [&](uint64_t j) {
+    const int s = (int)(j % STAGES);
+    const uint64_t r0 = (blockIdx.x + j * gridDim.x) * (uint64_t)R;
+    uint8_t* st = q1_dyn + (size_t)s * kStage;
+    mbar_arrive_expect_tx(&full[s], kStage);
+    bulk_copy_g2s(st + oShip, ship + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oQty, qty + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oExt, ext + r0, R * 8, &full[s]);
+    bulk_copy_g2s(st + oDisc, disc + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oTax, tax + r0, R * 4, &full[s]);
+    bulk_copy_g2s(st + oFlag, flag + r0, R, &full[s]);
+    bulk_copy_g2s(st + oStat, stat + r0, R, &full[s]);
+  };
+  uint64_t j = 0;
+  for (; j < mine; j++) {
+    if (t == 0) {
+      while (issued < mine && issued < j + STAGES) {
+        if (issued >= (uint64_t)STAGES &&
+            !mbar_wait(&empty[issued % STAGES], (uint32_t)(((issued / STAGES) - 1) & 1), kMbarPollLimit)) {
+          timed_out = true;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    const int s = (int)(j % STAGES);
+    if (timed_out || !mbar_wait(&full[s], (uint32_t)((j / STAGES) & 1), kMbarPollLimit)) { timed_out = true; break; }
+    const uint8_t* stg = q1_dyn + (size_t)s * kStage;
+    const int4 sv = *reinterpret_cast<const int4*>(stg + oShip + 16 * t);
+    const int4 kv = *reinterpret_cast<const int4*>(stg + oQty + 16 * t);
+    const longlong2 e01 = *reinterpret_cast<const longlong2*>(stg + oExt + 32 * t);
+    const longlong2 e23 = *reinterpret_cast<const longlong2*>(stg + oExt + 32 * t + 16);
+    const int4 dv = *reinterpret_cast<const int4*>(stg + oDisc + 16 * t);
+    const int4 tv = *reinterpret_cast<const int4*>(stg + oTax + 16 * t);
+    const uint32_t f = *reinterpret_cast<const uint32_t*>(stg + oFlag + 4 * t);
+    const uint32_t g = *reinterpret_cast<const uint32_t*>(stg + oStat + 4 * t);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);   // the tile is in registers: release the stage
+    row(sv.x, kv.x, e01.x, dv.x, tv.x, f & 0xFF, g & 0xFF);
+    row(sv.y, kv.y, e01.y, dv.y, tv.y, (f >> 8) & 0xFF, (g >> 8) & 0xFF);
+    row(sv.z, kv.z, e23.x, dv.z, tv.z, (f >> 16) & 0xFF, (g >> 16) & 0xFF);
+    row(sv.w, kv.w, e23.y, dv.w, tv.w, f >> 24, g >> 24);
+  }
+  if (timed_out) set_status(status, ST_TIMEOUT);
+  if (t == 0)
+    for (uint64_t k = j; k < issued; k++) mbar_wait(&full[k % STAGES], (uint32_t)((k / STAGES) & 1), kMbarPollLimit);
+  if (blockIdx.x == gridDim.x - 1)
+    for (uint64_t r = tiles * R + t; r < n; r += THREADS) row(ship[r], qty[r], ext[r], disc[r], tax[r], flag[r], stat[r]);
+  Q1Acc a;
+#pragma unroll
+  for (int gi = 0; gi < 6; gi++) {
+    a.P[gi] = acc[(0 * 6 + gi) * THREADS + t];
+    a.E[gi] = acc[(1 * 6 + gi) * THREADS + t];
+    a.ED[gi] = acc[(2 * 6 + gi) * THREADS + t];
+    a.EDT[gi] = acc[(3 * 6 + gi) * THREADS + t];
+  }
+  a.bad = bad;
+  q1_fold<THREADS>(a, partials, ticket, out, status);
+}
+
+// 128-bit loads straight from HBM with the accumulators in shared memory: registers stay low
+// (several blocks per SM), and each thread keeps two quads (208 bytes) of loads in flight.
+constexpr int kQ1SmemThreads = 256;
+constexpr size_t kQ1AccBytes = (size_t)4 * 6 * kQ1SmemThreads * 8;   // 49,152
+
+__global__ void __launch_bounds__(kQ1SmemThreads) q1_vec_smem_kernel(const int4* __restrict__ ship4, const int4* __restrict__ qty4,
+                                                                     const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
+                                                                     const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
+                                                                     const uint32_t* __restrict__ stat4, uint64_t n, int32_t ship_le,
+                                                                     u128* partials, unsigned* ticket, u128* out, uint32_t* status) {
+  constexpr int T = kQ1SmemThreads;
+  extern __shared__ __align__(16) uint64_t q1_acc[];   // [4 metrics][6 groups][T]
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 24; i++) q1_acc[i * T + t] = 0;
+  uint32_t bad = 0;
+  auto row = [&](int32_t s, int32_t qt, int64_t e, int32_t d, int32_t tx, uint32_t f, uint32_t st) {
+    if (!((s <= ship_le) & (f <= 2u) & (st <= 1u))) return;
+    bad |= ((uint32_t)qt >= 65536u) | ((uint32_t)d > 100u) | ((uint32_t)tx > 100u) | ((uint64_t)e >= (1ull << 36));
+    const uint64_t ed = (uint64_t)e * (uint32_t)d;
+    const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)tx;
+    const uint64_t pk = ((uint64_t)(uint32_t)qt << 32) | ((uint64_t)(uint32_t)d << 13) | 1u;
+    uint64_t* p = q1_acc + (f * 2u + st) * T + t;
+    p[0] += pk;
+    p[6 * T] += (uint64_t)e;
+    p[12 * T] += ed;
+    p[18 * T] += edt;
+  };
+  auto quad = [&](const int4& s, const int4& k, const longlong2& e01, const longlong2& e23, const int4& d, const int4& x,
+                  uint32_t f, uint32_t g) {
+    row(s.x, k.x, e01.x, d.x, x.x, f & 0xFF, g & 0xFF);
+    row(s.y, k.y, e01.y, d.y, x.y, (f >> 8) & 0xFF, (g >> 8) & 0xFF);
+    row(s.z, k.z, e23.x, d.z, x.z, (f >> 16) & 0xFF, (g >> 16) & 0xFF);
+    row(s.w, k.w, e23.y, d.w, x.w, f >> 24, g >> 24);
+  };
+  const uint64_t nq = n >> 2;
+  const uint64_t S = (uint64_t)gridDim.x * T;
+  uint64_t q = (uint64_t)blockIdx.x * T + t;
+  for (; q + S < nq; q += 2 * S) {
+    const uint64_t q2 = q + S;
+    const int4 s0 = ld_stream(ship4 + q), s1 = ld_stream(ship4 + q2);
+    const int4 k0 = ld_stream(qty4 + q), k1 = ld_stream(qty4 + q2);
+    const longlong2 a0 = ld_stream(ext2 + 2 * q), b0 = ld_stream(ext2 + 2 * q + 1);
+    const longlong2 a1 = ld_stream(ext2 + 2 * q2), b1 = ld_stream(ext2 + 2 * q2 + 1);
+    const int4 d0 = ld_stream(disc4 + q), d1 = ld_stream(disc4 + q2);
+    const int4 x0 = ld_stream(tax4 + q), x1 = ld_stream(tax4 + q2);
+    const uint32_t f0 = ld_stream(flag4 + q), f1 = ld_stream(flag4 + q2);
+    const uint32_t g0 = ld_stream(stat4 + q), g1 = ld_stream(stat4 + q2);
+    quad(s0, k0, a0, b0, d0, x0, f0, g0);
+    quad(s1, k1, a1, b1, d1, x1, f1, g1);
+  }
+  for (; q < nq; q += S)
+    quad(ld_stream(ship4 + q), ld_stream(qty4 + q), ld_stream(ext2 + 2 * q), ld_stream(ext2 + 2 * q + 1),
+         ld_stream(disc4 + q), ld_stream(tax4 + q), ld_stream(flag4 + q), ld_stream(stat4 + q));
+  const uint64_t r = (nq << 2) + (uint64_t)blockIdx.x * T + t;
+  if (r < n) {
+    row(reinterpret_cast<const int32_t*>(ship4)[r], reinterpret_cast<const int32_t*>(qty4)[r],
+        reinterpret_cast<const int64_t*>(ext2)[r], reinterpret_cast<const int32_t*>(disc4)[r],
+        reinterpret_cast<const int32_t*>(tax4)[r], reinterpret_cast<const uint8_t*>(flag4)[r],
+        reinterpret_cast<const uint8_t*>(stat4)[r]);
+  }
+  Q1Acc a;
+#pragma unroll
+  for (int gi = 0; gi < 6; gi++) {
+    a.P[gi] = q1_acc[(0 * 6 + gi) * T + t];
+    a.E[gi] = q1_acc[(1 * 6 + gi) * T + t];
+    a.ED[gi] = q1_acc[(2 * 6 + gi) * T + t];
+    a.EDT[gi] = q1_acc[(3 * 6 + gi) * T + t];
+  }
+  a.bad = bad;
+  q1_fold<T>(a, partials, ticket, out, status);
 }
 
 bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
@@ -316,14 +673,69 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
   if (c.n_rows == 0) return GPUDB_OK;
   const bool vec = aligned(c.ship_date, 16) && aligned(c.quantity, 16) && aligned(c.ext_price, 16) &&
                    aligned(c.discount, 16) && aligned(c.tax, 16) && aligned(c.flag, 4) && aligned(c.status, 4);
+  const bool tma_ok = vec && aligned(c.flag, 16) && aligned(c.status, 16) && c.n_rows >= 4096;
+  // 0 auto, 1 TMA 2048-row tiles x 4 stages, 2 vector loads, 3 one row per thread,
+  // 4 TMA 4096-row tiles x 2 stages
+  int variant = ctx->scan_variant;
+  if (variant == 0) variant = vec ? 7 : 3;
+  if (variant == 7 && !vec) variant = 3;
+  if (variant == 7) {
+    const size_t smem = kQ1AccBytes;
+    GPUDB_CUDA(ctx, cudaFuncSetAttribute(q1_vec_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, q1_vec_smem_kernel, kQ1SmemThreads, smem) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    const uint64_t min_blocks = (c.n_rows + (uint64_t)kQ1SmemThreads * kQ1RowsPerThread - 1) /
+                                ((uint64_t)kQ1SmemThreads * kQ1RowsPerThread);
+    const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
+    const int grid = (int)std::max<uint64_t>(
+        1, std::max(min_blocks, std::min<uint64_t>(want, (uint64_t)ctx->sm_count * per_sm)));
+    void* part = nullptr;
+    unsigned* ticket = nullptr;
+    int rc = scan_scratch(ctx, "q1.partials", (size_t)grid * 6 * kQ1Raw * sizeof(u128), &part, &ticket);
+    if (rc) return rc;
+    GPUDB_LAUNCH(call, q1_vec_smem_kernel, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
+                 (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
+                 (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, call.status());
+    return GPUDB_OK;
+  }
+  if ((variant == 1 || variant >= 4) && !tma_ok) variant = vec ? 2 : 3;
+  if (variant == 2 && !vec) variant = 3;
+  if (variant == 1 || variant >= 4) {
+    const uint32_t R = (variant == 1 || variant == 5) ? 2048u : variant == 6 ? 1024u : 4096u;
+    const int threads = variant == 6 ? 256 : kQ1TmaThreads;
+    auto kernel = variant == 1 ? q1_tma_kernel<1, 4>
+                  : variant == 4 ? q1_tma_kernel<2, 2>
+                  : variant == 5 ? q1_ring_kernel<1, 4>
+                                 : q1_ring_smem_kernel<256, 6>;
+    const uint64_t tiles = c.n_rows / R;
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ctx->sm_count, tiles));
+    // 212,992 bytes of tiles; the shared-accumulator ring: 6 x 26,624 tiles + 49,152 accumulators
+    const size_t smem = variant == 6 ? (size_t)6 * 26 * 1024 + 4 * 6 * 256 * 8 : (size_t)26 * 2048 * 4;
+    GPUDB_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void* part = nullptr;
+    unsigned* ticket = nullptr;
+    int rc = scan_scratch(ctx, "q1.partials", (size_t)grid * 6 * kQ1Raw * sizeof(u128), &part, &ticket);
+    if (rc) return rc;
+    // keep every thread under kQ1RowsPerThread rows: split very large tables into launches
+    const uint64_t per_launch = ((uint64_t)grid * threads * (kQ1RowsPerThread - 8) / R) * R;
+    for (uint64_t r0 = 0; r0 < c.n_rows; r0 += per_launch) {
+      const uint64_t rows = std::min<uint64_t>(per_launch, c.n_rows - r0);
+      GPUDB_LAUNCH(call, kernel, grid, threads, smem, c.ship_date + r0, c.quantity + r0, c.ext_price + r0,
+                   c.discount + r0, c.tax + r0, c.flag + r0, c.status + r0, rows, p.ship_le, (u128*)part, ticket,
+                   (u128*)out, call.status());
+    }
+    return GPUDB_OK;
+  }
   const int min_blocks = (int)((c.n_rows + (uint64_t)kThreads * kQ1RowsPerThread - 1) / ((uint64_t)kThreads * kQ1RowsPerThread));
-  const int grid = vec ? grid_for(ctx, (const void*)q1_vec_kernel, c.n_rows / 4 + 1, min_blocks)
-                       : grid_for(ctx, (const void*)q1_row_kernel, c.n_rows, min_blocks);
+  const int grid = variant == 2 ? grid_for(ctx, (const void*)q1_vec_kernel, c.n_rows / 4 + 1, min_blocks)
+                                : grid_for(ctx, (const void*)q1_row_kernel, c.n_rows, min_blocks);
   void* part = nullptr;
   unsigned* ticket = nullptr;
   int rc = scan_scratch(ctx, "q1.partials", (size_t)grid * 6 * kQ1Raw * sizeof(u128), &part, &ticket);
   if (rc) return rc;
-  if (vec) {
+  if (variant == 2) {
     GPUDB_LAUNCH(call, q1_vec_kernel, grid, kThreads, 0, (const int4*)c.ship_date, (const int4*)c.quantity,
                  (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
                  (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, call.status());

@@ -134,6 +134,10 @@ class Engine:
         """Rows per streamed chunk when a lineitem table lives in host memory."""
         return self._check(self.lib.gpudb_set_option(self.ctx, capi.OPT_CHUNK_ROWS, int(rows)))
 
+    def set_scan_variant(self, variant):
+        """Scan kernel choice: 0 auto, 1 TMA-staged tiles, 2 128-bit loads, 3 one row per thread."""
+        return self._check(self.lib.gpudb_set_option(self.ctx, capi.OPT_SCAN_VARIANT, int(variant)))
+
     def sync(self):
         return self._check(self.lib.gpudb_sync(self.ctx))
 

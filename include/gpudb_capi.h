@@ -87,7 +87,10 @@ void* gpudb_stream(gpudb_ctx* ctx);
 uint64_t gpudb_kernel_launches(const gpudb_ctx* ctx);
 /* Context options (replaces the fixed ChunkConfig sizing of src/infra.h:42-57). */
 enum {
-  GPUDB_OPT_CHUNK_ROWS = 1   /* rows per streamed chunk of a host-resident fact table (default 64M) */
+  GPUDB_OPT_CHUNK_ROWS = 1,  /* rows per streamed chunk of a host-resident fact table (default 64M) */
+  GPUDB_OPT_SCAN_VARIANT = 2 /* Q1 scan kernel: 0 auto (7), 1 TMA 2048-row tiles x 4 stages, 2 128-bit loads,
+                                3 one row per thread, 4 TMA 4096-row tiles x 2 stages, 5 TMA ring,
+                                6 TMA ring + shared accumulators, 7 128-bit loads + shared accumulators */
 };
 int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value);
 

@@ -56,6 +56,22 @@ def test_q6_q1_small_sizes(engine, orc, n):
         engine.free(t)
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("n", [2047, 2048, 2049, 3 * 4096 + 5, 1_000_003])
+def test_q1_every_kernel_variant(engine, orc, variant, n):
+    """TMA-staged tiles (1), 128-bit loads (2) and one row per thread (3) agree exactly."""
+    li = orc.lineitem(n, seed=n)
+    t = upload_li(engine, li)
+    try:
+        engine.set_scan_variant(variant)
+        assert engine.q1(t) == orc.q1(li)
+        assert engine.q1(t, 700) == orc.q1(li, 700)
+        assert engine.q1(t.lineitem(n_rows=n - 1, row_offset=1)) == orc.q1({k: v[1:] for k, v in li.items()})
+    finally:
+        engine.set_scan_variant(0)
+        engine.free(t)
+
+
 @pytest.mark.parametrize("off", [1, 2, 3, 5])
 def test_unaligned_column_starts(engine, orc, off):
     n = 50_001
@@ -194,7 +210,11 @@ def test_full_size_60m_bit_exact(engine, orc):
     try:
         li = orc.lineitem(n, seed=42)
         assert engine.q6(t) == orc.q6(li, threads=8)
-        assert engine.q1(t) == orc.q1(li, threads=8)
+        want = orc.q1(li, threads=8)
+        for variant in (1, 2, 3, 4, 5, 6, 7):
+            engine.set_scan_variant(variant)
+            assert engine.q1(t) == want
+        engine.set_scan_variant(0)
         # linearity: the two halves add up to the whole
         h = n // 2 + 3
         a = engine.q6(t.lineitem(n_rows=h))
