@@ -1,0 +1,81 @@
+"""The multi-GPU form of the scans on CPU: world size 2 over gloo. Each rank generates its
+row shard [rank*rows, (rank+1)*rows) of one seeded table (bench.py's weak-scaling layout),
+computes its exact partial results, and the gathered partials must equal the result over
+the whole table. Also covers the max-over-ranks timing reduction used by bench.py."""
+import os
+import socket
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, rows, out):
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.dirname(here))
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from gpudbmetalbenchmark_b200 import capi
+    import oracle_py as orc
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    lib = capi.load()
+    cols = {}
+    for name, cid in (("ship_date", 1), ("quantity", 2), ("ext_price", 3), ("discount", 4), ("tax", 5),
+                      ("flag", 6), ("status", 7)):
+        spec = capi.GenSpec(seed=42, row_offset=rank * rows, n_rows=rows)
+        a = np.empty(rows, dtype=orc.DT[lib.gpudb_column_width(cid)])
+        assert lib.gpudb_generate(None, C.byref(spec), cid, a.ctypes.data, capi.MEM_HOST) == capi.OK
+        cols[name] = a
+    part6 = orc.q6(cols)
+    part1 = orc.q1(cols)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, (part6, part1))
+    # the bench's timing reduction: max over ranks
+    t = torch.tensor([float(rank + 1)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        out.put((gathered, float(t.item())))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_shards_add_up_to_the_whole_table(orc):
+    world, rows = 2, 60_000
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, rows, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    gathered, tmax = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert tmax == 2.0
+    whole = orc.lineitem(world * rows, seed=42)
+    rev = sum(g[0][0] for g in gathered)
+    matched = sum(g[0][1] for g in gathered)
+    assert (rev, matched) == orc.q6(whole)
+    merged = {}
+    for _, q1 in gathered:
+        for k, v in q1.items():
+            m = merged.setdefault(k, dict.fromkeys(v, 0))
+            for f, x in v.items():
+                m[f] += x
+    assert merged == orc.q1(whole)
