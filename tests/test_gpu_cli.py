@@ -1,0 +1,101 @@
+"""The `gpudb <size> <pipeline>` command line (C++ drivers over the C ABI): each pipeline's
+printed exact result equals the oracle's, and the output keeps the reference's header and
+timing lines (the lines scripts/benchmark_gpu.sh greps)."""
+import os
+import re
+import subprocess
+from decimal import Decimal
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "gpudbmetalbenchmark_b200", "lib", "gpudb")
+TIMING = ["CPU Parsing (.tbl):", "GPU Execution:", "CPU Post Process:", "Total Execution:"]
+
+
+def run(*args):
+    r = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return r.stdout
+
+
+def scaled(v, digits):
+    return int(Decimal(v) * (10 ** digits))
+
+
+def timing_ok(out, q, rows):
+    assert re.search(r"^%s \| %d rows" % (q, rows), out, re.M), out
+    for t in TIMING:
+        assert t in out
+
+
+def test_cli_q6_and_q1(orc):
+    n = 60_000
+    li = orc.lineitem(n, seed=42)
+    out = run("sf1", "q6", "--scale", "0.01")
+    rev = scaled(re.search(r"Total Revenue: \$(\S+)", out).group(1), 4)
+    matched = int(re.search(r"Rows matched: (\d+)", out).group(1))
+    assert (rev, matched) == orc.q6(li)
+    timing_ok(out, "Q6", n)
+    out = run("sf1", "q1", "--scale", "0.01")
+    want = orc.q1(li)
+    rows = re.findall(r"^\|\s+([ANR])\s+\|\s+([FO])\s+\|\s+(\d+)\s+\|\s+(\S+)\s+\|\s+(\S+)\s+\|\s+(\S+)\s+\|.*\|\s+(\d+)\s+\|$",
+                      out, re.M)
+    assert len(rows) == len(want)
+    for f, s, qty, base, disc, charge, cnt in rows:
+        g = want[("ANR".index(f), "FO".index(s))]
+        assert (int(qty), scaled(base, 2), scaled(disc, 4), scaled(charge, 6), int(cnt)) == \
+            (g["sum_qty"], g["sum_base_price"], g["sum_disc_price"], g["sum_charge"], g["count"])
+    timing_ok(out, "Q1", n)
+
+
+def test_cli_q3_both_join_modes(orc):
+    cu, od, li = orc.q3_tables(1500, 15000, 60000, 42)
+    top, groups = orc.q3(cu, od, li)
+    out = run("sf1", "q3", "--scale", "0.01")
+    blocks = out.split("TPC-H Q3 Results")[1:]
+    assert len(blocks) == 2
+    for b in blocks:
+        rows = re.findall(r"^\|\s+(\d+) \| \$\s*(\S+) \|\s+(\d+) \|", b, re.M)
+        assert [(int(k), int(d), scaled(r, 4)) for k, r, d in rows] == top
+        assert int(re.search(r"Total results found: (\d+)", b).group(1)) == groups
+    timing_ok(out, "Q3", 60000)
+
+
+def test_cli_q9(orc):
+    pa, su, ps, od, li = orc.q9_tables(2000, 100, 15000, 60000, 42)
+    want, n = orc.q9(pa, su, ps, od, li)
+    out = run("sf1", "q9", "--scale", "0.01")
+    rows = re.findall(r"^\|\s+(\d+) \|\s+(\d+) \| \$\s*(\S+) \|$", out, re.M)
+    assert [(int(a), int(b), scaled(c, 4)) for a, b, c in rows] == want[:15]
+    assert int(re.search(r"Total results found: (\d+)", out).group(1)) == n
+    timing_ok(out, "Q9", 60000)
+
+
+def test_cli_microbenchmarks(orc):
+    out = run("sf1", "selection", "--scale", "0.01")
+    col = orc.gen(1, 60000, 42)
+    counts = [int(x) for x in re.findall(r"\((\d+) rows matched\)", out)]
+    assert counts == [orc.select_lt(col, v)[0] for v in (100, 1000, 2000)]
+    out = run("sf1", "aggregation", "--scale", "0.01")
+    assert int(re.search(r"SUM\(l_quantity\): (-?\d+)", out).group(1)) == orc.sum_i32(orc.gen(2, 60000, 42))
+    out = run("sf1", "join", "--scale", "0.01")
+    b = orc.gen(30, 15000, 42)
+    p = orc.gen(8, 60000, 42, n_orders=15000, order_mode=1)
+    assert [int(x) for x in re.findall(r"Found (\d+) total matches", out)] == [orc.join_count(b, p)] * 2
+
+
+def test_cli_sf100_streams_the_fact_table(orc):
+    n = 600_000   # sf100 x 0.001
+    li = orc.lineitem(n, seed=42)
+    out = run("sf100", "q6", "--scale", "0.001")
+    rev = scaled(re.search(r"Total Revenue: \$(\S+)", out).group(1), 4)
+    assert (rev, int(re.search(r"Rows matched: (\d+)", out).group(1))) == orc.q6(li)
+    assert re.search(r"^SF100 Q6 \| 1 chunks \| %d rows" % n, out, re.M)
+
+
+def test_cli_unknown_query_exits_1():
+    r = subprocess.run([CLI, "sf1", "q42"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Unknown query" in r.stderr
