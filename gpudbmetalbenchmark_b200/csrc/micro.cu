@@ -26,22 +26,37 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kSelTile = kThreads * 16;     // rows per block in the selection kernels
 
-// Bits and per-tile counts. Each warp handles 32-row words of its block's tile.
+// Bits and per-tile counts. Each warp step covers 128 rows: a lane loads 4 rows with one
+// 128-bit load (scalar loads on a ragged or unaligned tail), forms a 4-bit nibble, and an
+// OR-butterfly over 8 lanes assembles each 32-row word of the bitmask.
 __global__ void __launch_bounds__(kThreads) select_count_kernel(const int32_t* __restrict__ col, uint64_t n,
                                                                 int32_t value, uint32_t* bits, uint32_t* tile_counts) {
   __shared__ uint32_t wc[kThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t base = (uint64_t)blockIdx.x * kSelTile;
+  const bool vec = (reinterpret_cast<uintptr_t>(col) & 15u) == 0;
   uint32_t c = 0;
-  for (int w = warp; w < kSelTile / 32; w += kThreads / 32) {
-    const uint64_t r = base + (uint64_t)w * 32 + lane;
-    const bool hit = r < n && ld_stream(col + r) < value;
-    const uint32_t m = __ballot_sync(FULL_MASK, hit);
-    if (lane == 0) {
-      if (bits && base + (uint64_t)w * 32 < n) bits[(base >> 5) + w] = m;
-      c += __popc(m);
+#pragma unroll 2
+  for (int w = warp; w < kSelTile / 128; w += kThreads / 32) {
+    const uint64_t r = base + (uint64_t)w * 128 + 4 * lane;
+    uint32_t nib = 0;
+    if (vec && r + 4 <= n) {
+      const int4 v = ld_stream(reinterpret_cast<const int4*>(col + r));
+      nib = (uint32_t)(v.x < value) | ((uint32_t)(v.y < value) << 1) | ((uint32_t)(v.z < value) << 2) |
+            ((uint32_t)(v.w < value) << 3);
+    } else {
+      for (int i = 0; i < 4; i++)
+        if (r + i < n && col[r + i] < value) nib |= 1u << i;
     }
+    c += __popc(nib);
+    uint32_t word = nib << (4 * (lane & 7));
+    word |= __shfl_xor_sync(FULL_MASK, word, 1);
+    word |= __shfl_xor_sync(FULL_MASK, word, 2);
+    word |= __shfl_xor_sync(FULL_MASK, word, 4);
+    const uint64_t wr = base + (uint64_t)w * 128 + 32 * (lane >> 3);   // first row of this word
+    if (bits && (lane & 7) == 0 && wr < n) bits[wr >> 5] = word;
   }
+  c = __reduce_add_sync(FULL_MASK, c);
   if (lane == 0) wc[warp] = c;
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -160,6 +160,10 @@ __global__ void __launch_bounds__(kTopkThreads) q3_topk_slots_kernel(const Q3Slo
                                                                      const uint32_t* cap_p, int k, u128* out,
                                                                      unsigned long long* groups) {
   const uint32_t cap = *cap_p;
+  if ((uint64_t)blockIdx.x * kTopkTile >= cap) {   // past the live table: no candidates
+    for (int i = threadIdx.x; i < k; i += kTopkThreads) out[(size_t)blockIdx.x * k + i] = 0;
+    return;
+  }
   u128 v[kTopkPerThread];
   uint32_t cnt = 0;
   const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;

@@ -1,0 +1,141 @@
+"""Per-pipeline throughput of every hot-path pipeline on one GPU, against the HBM roofline.
+
+    python -m gpudbmetalbenchmark_b200.pipebench [--only NAME ...] [--reps N] [--stream600m]
+
+Prints one JSON line per measurement: pipeline, configuration, rows, median device time
+(CUDA events on the launching stream, recorded by the library around the pipeline's
+kernels), rows/s, algorithmic GB/s and the fraction of the measured HBM copy peak. Inputs
+are generated on the device (seeded); every input is larger than L2 except where noted.
+Streamed cases keep the fact table in pinned host memory and are bounded by the host link.
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+
+from . import capi
+from .engine import Engine, Q1_COLS
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def timed(fn, reps):
+    fn(None)   # warm-up (and scratch allocation)
+    ts = []
+    for _ in range(reps):
+        t = capi.Timing()
+        fn(t)
+        ts.append(t)
+    return statistics.median(t.gpu_ms for t in ts), ts[-1]
+
+
+def emit(name, config, rows, ms, alg_bytes, extra=None):
+    pk, kind = peak()
+    gbs = alg_bytes / (ms * 1e-3) / 1e9
+    line = {"pipeline": name, "config": config, "rows": rows, "ms": round(ms, 4),
+            "rows_per_s": rows / (ms * 1e-3), "algorithmic_bytes": alg_bytes, "gbs_algorithmic": round(gbs, 1),
+            "frac_of_%s_peak" % kind: round(gbs / pk, 3)}
+    if extra:
+        line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def q3_case(eng, n_cu, n_or, n_li, reps, label):
+    cu = eng.generate("customer", n_cu, seed=42)
+    od = eng.generate("orders", n_or, seed=42, n_cust=n_cu)
+    li = eng.generate("lineitem", n_li, seed=42, columns=("order_key", "ship_date", "ext_price", "discount"),
+                      n_orders=n_or, order_mode=capi.ORDERS_CLUSTERED)
+    alg = n_cu * 5 + n_or * 12 + n_li * 20
+    for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix")):
+        ms, t = timed(lambda tm: eng.q3(cu, od, li, join_mode=mode, timing=tm), reps)
+        emit("q3_join_topk", "%s, %s table" % (label, mname), n_li, ms, alg, {"kernels": t.kernels})
+    for x in (cu, od, li):
+        eng.free(x)
+
+
+def q9_tables(eng, n_pa, n_su, n_or):
+    pa = eng.generate("part", n_pa, seed=42)
+    su = eng.generate("supplier", n_su, seed=42)
+    ps = eng.generate("partsupp", 4 * n_pa, seed=42, n_supp=n_su)
+    od = eng.generate("orders", n_or, seed=42, columns=("order_key", "order_date"))
+    return pa, su, ps, od
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*")
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--stream600m", action="store_true", help="config 3 streamed at 600M fact rows (16.8 GB pinned)")
+    a = ap.parse_args(argv)
+    want = set(a.only) if a.only else None
+    eng = Engine(0)
+    on = lambda name: want is None or name in want  # noqa: E731
+
+    if on("scans"):
+        for rows in (6_000_000, 60_000_000):
+            t = eng.generate("lineitem", rows, seed=42, columns=Q1_COLS)
+            ms, _ = timed(lambda tm: eng.q6(t, timing=tm), a.reps)
+            emit("q6_sum", "config %s" % ("1a" if rows > 6e6 else "1a at 6M"), rows, ms, 20 * rows,
+                 {"note": "6M rows = 120 MB, inside L2" if rows == 6_000_000 else ""})
+            ms, _ = timed(lambda tm: eng.q1(t, timing=tm), a.reps)
+            emit("q1_group6", "config %s" % ("1b" if rows > 6e6 else "0"), rows, ms, 26 * rows,
+                 {"note": "6M rows = 156 MB" if rows == 6_000_000 else ""})
+            eng.free(t)
+    if on("q3"):
+        q3_case(eng, 150_000, 1_500_000, 6_000_000, a.reps, "config 2 (1x)")
+        q3_case(eng, 1_500_000, 15_000_000, 60_000_000, max(3, a.reps // 4), "config 2 (10x)")
+    if on("q9"):
+        pa, su, ps, od = q9_tables(eng, 2_000_000, 100_000, 15_000_000)
+        li = eng.generate("lineitem", 60_000_000, seed=42,
+                          columns=("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity"),
+                          n_orders=15_000_000, n_parts=2_000_000, n_supp=100_000, order_mode=capi.ORDERS_UNIFORM)
+        ms, t = timed(lambda tm: eng.q9(pa, su, ps, od, li, timing=tm), a.reps)
+        emit("q9_star", "config 3 (HBM-resident)", 60_000_000, ms, 60_000_000 * 28 + 8_000_000 * 16 + 15_000_000 * 8
+             + 2_000_000 + 100_000, {"kernels": t.kernels})
+        eng.free(li)
+        if a.stream600m:
+            rows = 600_000_000
+            lh = eng.generate("lineitem", rows, seed=42,
+                              columns=("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity"),
+                              n_orders=15_000_000, n_parts=2_000_000, n_supp=100_000, order_mode=capi.ORDERS_UNIFORM,
+                              location=capi.MEM_HOST)
+            ms, t = timed(lambda tm: eng.q9(pa, su, ps, od, lh, chunk_rows=64 << 20, timing=tm), max(2, a.reps // 10))
+            emit("q9_star", "config 3 streamed (600M rows, 64M-row chunks, pinned host)", rows, ms, rows * 28,
+                 {"chunks": t.chunks, "h2d_gbs": t.h2d_bytes / (ms * 1e-3) / 1e9, "bound": "host link"})
+            eng.free(lh)
+        for x in (pa, su, ps, od):
+            eng.free(x)
+    if on("micro"):
+        rows = 60_000_000
+        t = eng.generate("lineitem", rows, seed=42, columns=("ship_date", "quantity"))
+        bits = eng.device_array((rows + 31) // 32 * 4)
+        ms, _ = timed(lambda tm: eng.select_lt(t.ptr("ship_date"), rows, 1000, bits, timing=tm), a.reps)
+        emit("select_lt", "selection, bitmask output", rows, ms, rows * 4 + rows // 8)
+        ms, _ = timed(lambda tm: eng.sum_i32(t.ptr("quantity"), rows, timing=tm), a.reps)
+        emit("sum_i32", "aggregation", rows, ms, rows * 4)
+        eng.device_free(bits)
+        eng.free(t)
+        b = eng.generate("orders", 15_000_000, seed=42, columns=("order_key",))
+        p = eng.generate("lineitem", 60_000_000, seed=42, columns=("order_key",), n_orders=15_000_000,
+                         order_mode=capi.ORDERS_CLUSTERED)
+        for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix")):
+            ms, _ = timed(lambda tm: eng.hash_join_count(b.ptr("order_key"), 15_000_000, p.ptr("order_key"),
+                                                         60_000_000, mode, timing=tm), max(3, a.reps // 4))
+            emit("hash_join_count", "15M build x 60M probe, %s" % mname, 60_000_000, ms, 75_000_000 * 4)
+        eng.free(b)
+        eng.free(p)
+    eng.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
