@@ -135,6 +135,35 @@ class Q9Group(C.Structure):
     _fields_ = [("nation", C.c_int32), ("year", C.c_int32), ("profit", C.c_int64)]
 
 
+PIPE_Q6, PIPE_Q1, PIPE_Q3, PIPE_Q9 = 1, 2, 3, 4
+
+
+class Q3Tables(C.Structure):
+    _fields_ = [("cu", Customer), ("od", Orders), ("li", Lineitem)]
+
+
+class Q9Tables(C.Structure):
+    _fields_ = [("pa", Part), ("su", Supplier), ("ps", Partsupp), ("od", Orders), ("li", Lineitem)]
+
+
+class Request(C.Structure):
+    _fields_ = [("pipeline", C.c_int32), ("status", C.c_int32), ("row_begin", C.c_uint64), ("row_end", C.c_uint64),
+                ("li", C.POINTER(Lineitem)), ("q3", C.POINTER(Q3Tables)), ("q9", C.POINTER(Q9Tables)),
+                ("q6", Q6Params), ("q1", Q1Params), ("q3p", Q3Params), ("q9p", Q9Params),
+                ("q6_out", C.POINTER(Q6Result)), ("q1_out", C.POINTER(Q1Result)), ("q3_out", C.POINTER(Q3Result)),
+                ("q9_out", C.POINTER(Q9Group)), ("q9_capacity", C.c_uint32), ("q9_groups", C.c_uint32)]
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("lanes", C.c_uint32), ("max_batch", C.c_uint32), ("reserved", C.c_uint32),
+                ("memory_budget", C.c_uint64)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("max_batch_seen", C.c_uint64), ("peak_admitted_bytes", C.c_uint64)]
+
+
 P = C.POINTER
 ctx_p = vp
 # name: (restype, argtypes)
@@ -168,6 +197,13 @@ PROTOTYPES = {
     "gpudb_radix_partition": (C.c_int, [ctx_p, vp, vp, C.c_uint64, C.c_int32, vp, vp, vp, P(Timing), P(Exec)]),
     "gpudb_radix_join_pairs": (C.c_int, [ctx_p, vp, C.c_uint64, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          P(C.c_uint64), P(Timing), P(Exec)]),
+    "gpudb_batch_run": (C.c_int, [ctx_p, P(Request), C.c_uint32, P(Timing), P(Exec)]),
+    "gpudb_serve_open": (C.c_int, [P(ServeConfig), P(vp)]),
+    "gpudb_serve_submit": (C.c_int, [vp, P(Request), P(C.c_uint64)]),
+    "gpudb_serve_wait": (C.c_int, [vp, C.c_uint64, C.c_double, P(C.c_double)]),
+    "gpudb_serve_stats_get": (C.c_int, [vp, P(ServeStats)]),
+    "gpudb_request_footprint": (C.c_uint64, [P(Request)]),
+    "gpudb_serve_close": (C.c_int, [vp]),
 }
 
 _lib = None

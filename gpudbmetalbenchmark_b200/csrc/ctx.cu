@@ -81,6 +81,7 @@ int status_to_error(gpudb_ctx* ctx, uint32_t st) {
 Call::Call(gpudb_ctx* ctx, const gpudb_exec* ex, gpudb_timing* t)
     : ctx_(ctx), s_(ctx->stream), async_(false), t_(t), host0_(now_ms()) {
   cudaSetDevice(ctx->device);
+  status_sink_ = ctx->status_sink;
   if (ex) {
     async_ = ex->async != 0;
     if (ex->stream) s_ = static_cast<cudaStream_t>(ex->stream);
@@ -153,11 +154,13 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
   double host0 = host0_;
   uint32_t kernels = kernels_, chunks = chunks_;
   uint64_t h2d = h2d_, d2h = d2h_;
+  int32_t* sink = status_sink_;
   auto done = [=]() -> int {
     uint32_t st;
     std::memcpy(&st, hs, sizeof st);
     int rc = status_to_error(ctx, st);
     if (rc == GPUDB_OK) rc = convert(hs + kSlotHeader);
+    if (sink) *sink = rc;
     if (t) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = -1.f;

@@ -55,6 +55,7 @@ struct gpudb_ctx {
   uint8_t* d_big = nullptr;            // large result slots (device) and their pinned mirror
   uint8_t* h_big = nullptr;
   bool big_busy[gpudb::kBigSlots] = {};
+  int32_t* status_sink = nullptr;      // batch: where the next call reports its final status
   std::vector<std::function<int()>> pending;
   std::vector<cudaStream_t> pending_streams;
   std::vector<cudaEvent_t> event_pool;
@@ -109,6 +110,7 @@ class Call {
   uint32_t kernels_ = 0, chunks_ = 0;
   uint64_t h2d_ = 0, d2h_ = 0;
   bool handed_off_ = false;
+  int32_t* status_sink_ = nullptr;
 };
 
 // Launch helper: counts the launch on the call and checks the launch error.

@@ -1,0 +1,194 @@
+// Serving loop: lanes of (context, worker thread) over a shared FIFO with admission by
+// predicted device footprint. See gpudb_serve_* in include/gpudb_capi.h.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.h"
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+uint64_t pow2_at_least(uint64_t v, uint64_t lo) {
+  uint64_t p = lo;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+struct Ticket {
+  gpudb_request* req = nullptr;
+  double t_submit = 0, t_done = 0;
+  uint64_t footprint = 0;
+  bool done = false;
+};
+
+}  // namespace
+
+extern "C" uint64_t gpudb_request_footprint(const gpudb_request* r) {
+  if (!r) return 0;
+  switch (r->pipeline) {
+    case GPUDB_PIPE_Q6: return 256;
+    case GPUDB_PIPE_Q1: return 2048;
+    case GPUDB_PIPE_Q3: {
+      if (!r->q3) return 0;
+      const uint64_t n_or = r->q3->od.n_rows, cap = pow2_at_least(2 * n_or, 2048);
+      // bitmap + orders staging + hash table (16 B) + hit counters + top-k candidates
+      return (uint64_t)(r->q3->cu.key_max / 8 + 64) + n_or * 8 + cap * 20 + (cap / 4096 + 1) * 64 * 16 * 2;
+    }
+    case GPUDB_PIPE_Q9: {
+      if (!r->q9) return 0;
+      const uint64_t ps = r->q9->ps.n_rows, cap = pow2_at_least(2 * ps, 1024);
+      // part bitmap + supplier and year maps + partsupp staging + partsupp table + groups
+      return (uint64_t)(r->q9->pa.key_max / 8 + 64) + (uint64_t)r->q9->su.key_max + (uint64_t)r->q9->od.key_max +
+             ps * 4 + cap * 16 + 4096 * 12;
+    }
+    default: return 0;
+  }
+}
+
+struct gpudb_server {
+  gpudb_serve_config cfg{};
+  std::vector<gpudb_ctx*> lanes;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<uint64_t> queue;
+  std::unordered_map<uint64_t, Ticket> tickets;
+  uint64_t next_ticket = 1;
+  uint64_t admitted_bytes = 0;
+  bool closing = false;
+  gpudb_serve_stats stats{};
+
+  void work(size_t lane) {
+    gpudb_ctx* ctx = lanes[lane];
+    std::vector<gpudb_request> batch;
+    std::vector<uint64_t> ids;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return closing || (!queue.empty() && fits(tickets[queue.front()].footprint)); });
+        if (queue.empty() && closing) return;
+        if (queue.empty() || !fits(tickets[queue.front()].footprint)) continue;
+        ids.clear();
+        uint64_t bytes = 0;
+        while (!queue.empty() && ids.size() < cfg.max_batch) {
+          const uint64_t fp = tickets[queue.front()].footprint;
+          if (!ids.empty() && !fits(bytes + fp)) break;   // keep arrival order: stop at the first misfit
+          bytes += fp;
+          ids.push_back(queue.front());
+          queue.pop_front();
+        }
+        admitted_bytes += bytes;
+        stats.peak_admitted_bytes = std::max(stats.peak_admitted_bytes, admitted_bytes);
+        stats.batches++;
+        stats.max_batch_seen = std::max<uint64_t>(stats.max_batch_seen, ids.size());
+        batch.clear();
+        for (uint64_t id : ids) batch.push_back(*tickets[id].req);
+      }
+      gpudb_batch_run(ctx, batch.data(), (uint32_t)batch.size(), nullptr, nullptr);
+      const double t = now_ms();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        for (size_t i = 0; i < ids.size(); i++) {
+          Ticket& tk = tickets[ids[i]];
+          tk.req->status = batch[i].status;
+          tk.req->q9_groups = batch[i].q9_groups;
+          tk.t_done = t;
+          tk.done = true;
+          admitted_bytes -= tk.footprint;
+          stats.completed++;
+          if (batch[i].status != GPUDB_OK) stats.failed++;
+        }
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+
+  bool fits(uint64_t bytes) const {
+    return cfg.memory_budget == 0 || admitted_bytes + bytes <= cfg.memory_budget;
+  }
+};
+
+extern "C" int gpudb_serve_open(const gpudb_serve_config* cfg, gpudb_server** out) {
+  if (!cfg || !out || cfg->lanes < 1 || cfg->lanes > 16 || cfg->max_batch < 1) return GPUDB_E_INVALID;
+  *out = nullptr;
+  gpudb_server* s = new gpudb_server();
+  s->cfg = *cfg;
+  for (uint32_t i = 0; i < cfg->lanes; i++) {
+    gpudb_ctx* c = nullptr;
+    int rc = gpudb_create(cfg->device, &c);
+    if (rc != GPUDB_OK) {
+      for (auto* l : s->lanes) gpudb_destroy(l);
+      delete s;
+      return rc;
+    }
+    s->lanes.push_back(c);
+  }
+  for (size_t i = 0; i < s->lanes.size(); i++) s->workers.emplace_back(&gpudb_server::work, s, i);
+  *out = s;
+  return GPUDB_OK;
+}
+
+extern "C" int gpudb_serve_submit(gpudb_server* s, gpudb_request* req, uint64_t* ticket) {
+  if (!s || !req || !ticket) return GPUDB_E_INVALID;
+  const uint64_t fp = gpudb_request_footprint(req);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->closing) return GPUDB_E_CLOSED;
+    if (s->cfg.memory_budget && fp > s->cfg.memory_budget) return GPUDB_E_BUSY;
+    const uint64_t id = s->next_ticket++;
+    Ticket& t = s->tickets[id];
+    t.req = req;
+    t.t_submit = now_ms();
+    t.footprint = fp;
+    s->queue.push_back(id);
+    s->stats.submitted++;
+    *ticket = id;
+  }
+  s->cv_work.notify_one();
+  return GPUDB_OK;
+}
+
+extern "C" int gpudb_serve_wait(gpudb_server* s, uint64_t ticket, double timeout_ms, double* latency_ms) {
+  if (!s) return GPUDB_E_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return GPUDB_E_INVALID;
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms),
+                                      [&] { return s->tickets[ticket].done; });
+  if (!ok) return GPUDB_E_TIMEOUT;
+  Ticket t = s->tickets[ticket];
+  s->tickets.erase(ticket);
+  if (latency_ms) *latency_ms = t.t_done - t.t_submit;
+  return t.req->status;
+}
+
+extern "C" int gpudb_serve_stats_get(gpudb_server* s, gpudb_serve_stats* out) {
+  if (!s || !out) return GPUDB_E_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
+  return GPUDB_OK;
+}
+
+extern "C" int gpudb_serve_close(gpudb_server* s) {
+  if (!s) return GPUDB_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->closing = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& w : s->workers) w.join();
+  for (auto* l : s->lanes) gpudb_destroy(l);
+  delete s;
+  return GPUDB_OK;
+}

@@ -303,6 +303,76 @@ int gpudb_radix_join_pairs(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n
                            uint64_t capacity, uint64_t* n_pairs,
                            gpudb_timing* t, const gpudb_exec* ex);
 
+/* ---- batched execution (no reference counterpart: the reference runs one query per
+ *      command buffer, src/q1.cpp:59-106) ---------------------------------------------
+ * One call runs many requests. All Q6/Q1 requests over device-resident tables share one
+ * persistent kernel launch that pulls (request, row range) tiles from a device work queue,
+ * so small requests and uneven row ranges cost one launch in total; each request keeps
+ * its own exact result and status. Q3/Q9 requests run their pipelines behind it on the
+ * same stream without host synchronisation. */
+enum { GPUDB_PIPE_Q6 = 1, GPUDB_PIPE_Q1 = 2, GPUDB_PIPE_Q3 = 3, GPUDB_PIPE_Q9 = 4 };
+
+typedef struct gpudb_q3_tables { gpudb_customer cu; gpudb_orders od; gpudb_lineitem li; } gpudb_q3_tables;
+typedef struct gpudb_q9_tables {
+  gpudb_part pa; gpudb_supplier su; gpudb_partsupp ps; gpudb_orders od; gpudb_lineitem li;
+} gpudb_q9_tables;
+
+typedef struct gpudb_request {
+  int32_t pipeline;                 /* GPUDB_PIPE_* */
+  int32_t status;                   /* set when the request completes: GPUDB_OK or GPUDB_E_* */
+  uint64_t row_begin, row_end;      /* Q6/Q1: rows [row_begin, row_end) of li; row_end 0 = all rows */
+  const gpudb_lineitem* li;         /* Q6/Q1 input */
+  const gpudb_q3_tables* q3;        /* Q3 input */
+  const gpudb_q9_tables* q9;        /* Q9 input */
+  gpudb_q6_params q6;
+  gpudb_q1_params q1;
+  gpudb_q3_params q3p;
+  gpudb_q9_params q9p;
+  gpudb_q6_result* q6_out;          /* caller-owned results, filled at completion */
+  gpudb_q1_result* q1_out;
+  gpudb_q3_result* q3_out;
+  gpudb_q9_group* q9_out; uint32_t q9_capacity; uint32_t q9_groups;
+} gpudb_request;
+
+/* Runs n requests; with ex->async the requests complete (status and results filled) at the
+ * next gpudb_sync(). Returns GPUDB_OK when the batch was accepted; per-request failures
+ * are reported in each request's status. */
+int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- serving (no reference counterpart) ---------------------------------------------
+ * A request loop over HBM-resident tables. `lanes` worker threads each own a context
+ * (CUDA stream + scratch memory); a free lane takes the queued requests in arrival order,
+ * up to max_batch, while their predicted device footprint fits in memory_budget minus what
+ * running batches hold, and runs them as one gpudb_batch_run. Requests that arrive while
+ * other batches are on the GPU are admitted by the next free lane, so work of different
+ * batches overlaps on the device. max_batch = 1 and lanes = 1 is the plain
+ * one-query-at-a-time form. */
+typedef struct gpudb_server gpudb_server;
+typedef struct gpudb_serve_config {
+  int32_t device;
+  uint32_t lanes;            /* worker lanes (contexts), 1..16 */
+  uint32_t max_batch;        /* requests per batch, >= 1 */
+  uint32_t reserved;
+  uint64_t memory_budget;    /* bytes of predicted device footprint admitted at once; 0 = no limit */
+} gpudb_serve_config;
+typedef struct gpudb_serve_stats {
+  uint64_t submitted, completed, failed, batches, max_batch_seen;
+  uint64_t peak_admitted_bytes;
+} gpudb_serve_stats;
+
+int gpudb_serve_open(const gpudb_serve_config* cfg, gpudb_server** out);
+/* Queues a request (caller-owned until it completes). GPUDB_E_BUSY if its predicted
+ * footprint alone exceeds the budget, GPUDB_E_CLOSED after close. */
+int gpudb_serve_submit(gpudb_server* s, gpudb_request* req, uint64_t* ticket);
+/* Waits up to timeout_ms for a ticket; returns the request's status (GPUDB_E_TIMEOUT if it
+ * is still running) and its submit-to-completion latency in milliseconds. */
+int gpudb_serve_wait(gpudb_server* s, uint64_t ticket, double timeout_ms, double* latency_ms);
+int gpudb_serve_stats_get(gpudb_server* s, gpudb_serve_stats* out);
+/* Predicted device footprint of a request, in bytes (the admission estimate). */
+uint64_t gpudb_request_footprint(const gpudb_request* req);
+/* Stops accepting requests, finishes the queued ones, and frees the lanes. */
+int gpudb_serve_close(gpudb_server* s);
+
 #ifdef __cplusplus
 }
 #endif

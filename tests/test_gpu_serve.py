@@ -1,0 +1,134 @@
+"""Batched execution and the serving loop on the GPU: every request of a mixed batch equals
+its oracle result and its solo execution; a request that fails reports only its own status;
+served results are the same alone and in the mix under continuous batching; admission by
+predicted footprint rejects what can never fit and serialises what does not fit now."""
+import ctypes as C
+
+import pytest
+
+from gpudbmetalbenchmark_b200 import capi
+from gpudbmetalbenchmark_b200.engine import q1_to_dict, q3_to_list
+from gpudbmetalbenchmark_b200.serve import Server, Workload, open_loop
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small(engine):
+    return Workload(engine, scan_rows=(100_003, 1_000_003), q3=(3000, 30_000, 120_000), q9=(4000, 400, 20_000, 100_000))
+
+
+def test_mixed_batch_matches_oracle(engine, orc):
+    li = orc.lineitem(200_003, seed=5)
+    t = engine.upload("lineitem", li)
+    s = t.lineitem()
+    cu_, od_, l3 = orc.q3_tables(3000, 30_000, 120_000, 6)
+    q3t = capi.Q3Tables(engine.upload("customer", cu_).struct(), engine.upload("orders", od_).struct(),
+                        engine.upload("lineitem", l3).lineitem())
+    reqs = (capi.Request * 7)()
+    outs = []
+    # Q6 over uneven row ranges, Q1 over all rows and a range, Q3 global and radix, a bad request
+    ranges = [(0, 0), (17, 150_000), (150_000, 200_003)]
+    for i, (b, e) in enumerate(ranges):
+        reqs[i].pipeline = capi.PIPE_Q6
+        reqs[i].li = C.pointer(s)
+        reqs[i].row_begin, reqs[i].row_end = b, e
+        reqs[i].q6 = capi.Q6Params(300 + 100 * i, 900, 2, 8, 40)
+        o = capi.Q6Result()
+        outs.append(o)
+        reqs[i].q6_out = C.pointer(o)
+    o1 = capi.Q1Result()
+    reqs[3].pipeline, reqs[3].li, reqs[3].q1, reqs[3].q1_out = capi.PIPE_Q1, C.pointer(s), capi.Q1Params(2000, 0), C.pointer(o1)
+    o3a, o3b = capi.Q3Result(), capi.Q3Result()
+    for j, (o, mode) in enumerate(((o3a, capi.JOIN_GLOBAL), (o3b, capi.JOIN_RADIX))):
+        r = reqs[4 + j]
+        r.pipeline, r.q3, r.q3_out = capi.PIPE_Q3, C.pointer(q3t), C.pointer(o)
+        r.q3p = capi.Q3Params(2, 1500, 800, 12, mode, 0)
+    reqs[6].pipeline = 77
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, 7, None, None))
+    for i, (b, e) in enumerate(ranges):
+        e = e or 200_003
+        sub = {k: v[b:e] for k, v in li.items()}
+        assert reqs[i].status == capi.OK
+        assert (outs[i].revenue, outs[i].rows_matched) == orc.q6(sub, 300 + 100 * i, 900, 2, 8, 40)
+    assert reqs[3].status == capi.OK and q1_to_dict(o1) == orc.q1(li, 2000)
+    want3 = orc.q3(cu_, od_, l3, 2, 1500, 800, 12)
+    assert q3_to_list(o3a) == want3 and q3_to_list(o3b) == want3
+    assert reqs[6].status == capi.E_INVALID
+
+
+def test_failing_request_does_not_fail_its_batch(engine, orc):
+    li = orc.lineitem(50_000, seed=8)
+    li["discount"][10] = 500          # outside the exact-arithmetic domain of Q1
+    li["ship_date"][10] = 0
+    t = engine.upload("lineitem", li)
+    s = t.lineitem()
+    reqs = (capi.Request * 2)()
+    o1, o6 = capi.Q1Result(), capi.Q6Result()
+    reqs[0].pipeline, reqs[0].li, reqs[0].q1, reqs[0].q1_out = capi.PIPE_Q1, C.pointer(s), capi.Q1Params(2436, 0), C.pointer(o1)
+    reqs[1].pipeline, reqs[1].li, reqs[1].q6, reqs[1].q6_out = (capi.PIPE_Q6, C.pointer(s), capi.Q6Params(0, 2527, 0, 1000, 99),
+                                                                C.pointer(o6))
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, 2, None, None))
+    assert reqs[0].status == capi.E_INVALID
+    assert reqs[1].status == capi.OK and (o6.revenue, o6.rows_matched) == orc.q6(li, 0, 2527, 0, 1000, 99)
+
+
+def test_many_scans_in_one_batch(engine, small):
+    jobs = [j for j in small.jobs(1500, seed=3) if j.kind in (capi.PIPE_Q6, capi.PIPE_Q1)]
+    solo = small.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()   # clear results
+    arr = (capi.Request * len(jobs))(*[j.req for j in jobs])
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, arr, len(jobs), None, None))
+    for k, j in enumerate(jobs):
+        assert arr[k].status == capi.OK
+        assert j.result() == solo[k]
+
+
+@pytest.mark.parametrize("lanes,max_batch,rate", [(1, 1, 3000.0), (4, 64, 20000.0), (2, 8, 50000.0)])
+def test_served_results_same_alone_and_in_the_mix(engine, small, lanes, max_batch, rate):
+    jobs = small.jobs(1200, seed=int(rate))
+    solo = small.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()
+        j.req.q9_groups = 0
+    srv = Server(lanes=lanes, max_batch=max_batch)
+    try:
+        lat, status, wall = open_loop(srv, jobs, rate, seed=1)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert all(s == capi.OK for s in status)
+    assert [j.result() for j in jobs] == solo
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    if max_batch > 1:
+        assert st["max_batch_seen"] > 1   # arrivals during running batches were batched
+
+
+def test_admission_by_footprint(engine, small):
+    jobs = small.jobs(300, seed=11)
+    q3 = next(j for j in jobs if j.kind == capi.PIPE_Q3)
+    fp = engine.lib.gpudb_request_footprint(C.byref(q3.req))
+    assert fp > 1 << 20
+    srv = Server(lanes=2, max_batch=16, memory_budget=fp // 2)
+    try:
+        with pytest.raises(capi.GpudbError) as e:
+            srv.submit(q3.req)
+        assert e.value.code == capi.E_BUSY
+    finally:
+        srv.close()
+    # a budget that admits one join at a time still completes everything, exactly
+    solo = small.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()
+        j.req.q9_groups = 0
+    big = max(engine.lib.gpudb_request_footprint(C.byref(j.req)) for j in jobs)
+    srv = Server(lanes=3, max_batch=32, memory_budget=big)
+    try:
+        lat, status, wall = open_loop(srv, jobs, 20000.0, seed=2)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert all(s == capi.OK for s in status)
+    assert [j.result() for j in jobs] == solo
+    assert st["peak_admitted_bytes"] <= big
