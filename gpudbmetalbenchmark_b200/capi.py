@@ -204,6 +204,7 @@ PROTOTYPES = {
     "gpudb_serve_stats_get": (C.c_int, [vp, P(ServeStats)]),
     "gpudb_request_footprint": (C.c_uint64, [P(Request)]),
     "gpudb_serve_close": (C.c_int, [vp]),
+    "gpudb_serve_warmup": (C.c_int, [vp, P(Request), C.c_uint32]),
 }
 
 _lib = None

@@ -1,14 +1,24 @@
 // Batched execution: many requests per call (gpudb_batch_run).
 //
-// All Q6/Q1 requests over device-resident tables become tiles of at most kTileRows rows
-// (request, row range) in one work list; a persistent grid pulls tiles from a device queue
-// (one atomicAdd per tile), so a batch of small requests, or of uneven row ranges over
-// different tables, is a single launch. A tile's block reduces its partial sums and adds
-// them into the request's own result words with integer atomics (exact, order-independent).
-// Q3/Q9 requests are enqueued behind it on the same stream as ordinary async pipeline calls,
-// so the whole batch needs one host synchronisation.
+// Shared scans. Q6/Q1 requests over device-resident tables are grouped by (table, row
+// range); each group is read from HBM once per pass, and every request of the group is
+// evaluated on the rows while they are in registers:
+//  - Q6 requests (up to kMaxQ6 per pass) keep per-thread register sums;
+//  - Q1 requests (up to kMaxQ1 per pass) differ only in their ship_date cutoff, so the
+//    cutoffs are sorted and a row falls in bucket j = number of cutoffs below its ship
+//    date; it counts for every request whose sorted position is >= j. Rows are aggregated
+//    per (bucket, group) with shared-memory atomics, and each request's totals are the
+//    prefix sums over buckets 0..position. The per-row cost does not grow with the number
+//    of Q1 requests.
+// All groups' row tiles form one work list; a persistent grid pulls tiles from a device
+// queue (one atomicAdd per tile), so a batch of many requests over several tables is one
+// launch. Partial sums reach the requests' result words through integer atomics (exact and
+// order-independent). Q3/Q9 requests are enqueued behind it on the same stream as ordinary
+// async pipeline calls, so the whole batch needs one host synchronisation.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -18,21 +28,38 @@ namespace gpudb {
 namespace {
 
 constexpr int kBT = 256;
-constexpr uint64_t kTileRows = 16384;     // per-tile block sums stay below 2^64 (Q1 domain)
+constexpr int kBW = kBT / 32;
+constexpr uint64_t kTileRows = 8192;      // per warp per tile <= 1024 rows: packed Q1 fields cannot carry
+constexpr int kMaxQ6 = 16;                // Q6 requests per pass (register sums)
+constexpr int kMaxQ1 = 15;                // Q1 requests per pass (16 buckets incl. padding)
+constexpr int kQ1Keys = (kMaxQ1 + 1) * 6; // (bucket, flag*2+status)
 constexpr int kQ6Words = 2;               // revenue, rows matched
 constexpr int kQ1Words = 72;              // 6 groups x 6 raw metrics x u128
 
-struct ScanReq {
-  int32_t kind, a, b, c, d, e;            // Q6: ship_lo, ship_hi, disc_lo, disc_hi, qty_lt; Q1: ship_le
+struct ScanGroup {
   const int32_t *ship, *qty, *disc, *tax;
   const int64_t* ext;
   const uint8_t *flag, *stat;
-  uint32_t res;                           // first result word
-  uint32_t idx;                           // index among the scan requests (status word)
+  uint64_t begin, end;
+  uint32_t n_q6, n_q1, vec, pad;
+  int32_t q6p[kMaxQ6][5];                 // ship_lo, ship_hi, disc_lo, disc_hi, qty_lt
+  uint32_t q6_res[kMaxQ6];                // first result word
+  int32_t q1_cut[kMaxQ1 + 1];             // ascending; padded with INT32_MAX
+  uint32_t q1_res[kMaxQ1];                // in cutoff order
+  uint32_t q1_idx[kMaxQ1];                // status word of the request
 };
 struct ScanTile {
-  uint32_t req, pad;
+  uint32_t group, pad;
   uint64_t begin, end;
+};
+
+struct ScanSmem {
+  ScanGroup g;
+  unsigned long long wacc[kBW][kQ1Keys][4];   // per warp: packed (qty<<32|disc<<13|1), ext, ext*disc, (ext*100-ext*disc)*tax
+  u128 bacc[kQ1Keys][6];                      // per block: count, qty, ext, ext*disc, ext*(100-disc)*tax, disc
+  uint32_t bad[kMaxQ1 + 1];
+  unsigned long long red[kBW][2];
+  uint32_t tile;
 };
 
 __device__ __forceinline__ void atomic_add_u128(unsigned long long* p, u128 v) {
@@ -43,80 +70,182 @@ __device__ __forceinline__ void atomic_add_u128(unsigned long long* p, u128 v) {
   if (hi) atomicAdd(p + 1, hi);
 }
 
-__global__ void __launch_bounds__(kBT) scan_batch_kernel(const ScanReq* __restrict__ reqs,
-                                                         const ScanTile* __restrict__ tiles, uint32_t n_tiles,
-                                                         unsigned* queue, unsigned long long* res, uint32_t* req_status) {
-  extern __shared__ unsigned long long acc[];   // [24][kBT] Q1 group accumulators
-  __shared__ uint32_t tile_i;
-  __shared__ unsigned long long red[kBT / 32][36];
+// Adds the block's sums for the current group to the requests' result words.
+__device__ void flush_group(ScanSmem& S, const int64_t (&rev)[kMaxQ6], const uint32_t (&cnt)[kMaxQ6],
+                            unsigned long long* res, uint32_t* req_status) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  for (;;) {
-    if (t == 0) tile_i = atomicAdd(queue, 1u);
+  const ScanGroup& g = S.g;
+#pragma unroll
+  for (int r = 0; r < kMaxQ6; r++) {
+    if (r >= (int)g.n_q6) break;
+    const unsigned long long a = warp_sum_u64((unsigned long long)rev[r]), b = warp_sum_u64(cnt[r]);
+    if (lane == 0) { S.red[warp][0] = a; S.red[warp][1] = b; }
     __syncthreads();
-    const uint32_t i = tile_i;
-    __syncthreads();
-    if (i >= n_tiles) break;
-    const ScanTile T = tiles[i];
-    const ScanReq R = reqs[T.req];
-    if (R.kind == GPUDB_PIPE_Q6) {
-      int64_t rev = 0;
-      unsigned long long cnt = 0;
-      for (uint64_t r = T.begin + t; r < T.end; r += kBT) {
-        const int32_t s = R.ship[r], dd = R.disc[r], q = R.qty[r];
-        if ((s >= R.a) & (s < R.b) & (dd >= R.c) & (dd <= R.d) & (q < R.e)) { rev += R.ext[r] * (int64_t)dd; cnt++; }
-      }
-      const unsigned long long a = warp_sum_u64((unsigned long long)rev), b = warp_sum_u64(cnt);
-      if (lane == 0) { red[warp][0] = a; red[warp][1] = b; }
-      __syncthreads();
-      if (t < 2) {
-        unsigned long long s = 0;
-        for (int w = 0; w < kBT / 32; w++) s += red[w][t];
-        if (s) atomicAdd(res + R.res + t, s);
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 24; k++) acc[k * kBT + t] = 0;
-      uint32_t bad = 0;
-      for (uint64_t r = T.begin + t; r < T.end; r += kBT) {
-        const uint32_t f = R.flag[r], st = R.stat[r];
-        if (!((R.ship[r] <= R.a) & (f <= 2u) & (st <= 1u))) continue;
-        const int32_t qt = R.qty[r], dd = R.disc[r], tx = R.tax[r];
-        const int64_t e = R.ext[r];
-        bad |= ((uint32_t)qt >= 65536u) | ((uint32_t)dd > 100u) | ((uint32_t)tx > 100u) | ((uint64_t)e >= (1ull << 36));
-        const uint64_t ed = (uint64_t)e * (uint32_t)dd;
-        const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)tx;
-        unsigned long long* p = acc + (f * 2u + st) * kBT + t;
-        p[0] += ((uint64_t)(uint32_t)qt << 32) | ((uint64_t)(uint32_t)dd << 13) | 1u;
-        p[6 * kBT] += (uint64_t)e;
-        p[12 * kBT] += ed;
-        p[18 * kBT] += edt;
-      }
-      if (__syncthreads_or(bad) && t == 0) atomicOr(req_status + R.idx, ST_DOMAIN);
-#pragma unroll
-      for (int g = 0; g < 6; g++) {
-        const unsigned long long P = acc[g * kBT + t];
-        const unsigned long long v[6] = {P & 0x1FFFu, P >> 32, acc[(6 + g) * kBT + t], acc[(12 + g) * kBT + t],
-                                         acc[(18 + g) * kBT + t], (P >> 13) & 0x7FFFFu};
-#pragma unroll
-        for (int m = 0; m < 6; m++) {
-          const unsigned long long w = warp_sum_u64(v[m]);
-          if (lane == 0) red[warp][g * 6 + m] = w;
-        }
-      }
-      __syncthreads();
-      if (t < 36) {
-        u128 s = 0;
-        for (int w = 0; w < kBT / 32; w++) s += red[w][t];
-        if (s) atomic_add_u128(res + R.res + 2 * t, s);
-      }
+    if (t < 2) {
+      unsigned long long v = 0;
+      for (int w = 0; w < kBW; w++) v += S.red[w][t];
+      if (v) atomicAdd(res + g.q6_res[r] + t, v);
     }
     __syncthreads();
   }
+  // Q1: request at sorted position p = prefix over buckets 0..p
+  for (uint32_t i = t; i < g.n_q1 * 36; i += kBT) {
+    const uint32_t p = i / 36, gm = i % 36, grp = gm / 6, m = gm % 6;
+    u128 v = 0;
+    for (uint32_t j = 0; j <= p; j++) v += S.bacc[j * 6 + grp][m];
+    if (v) atomic_add_u128(res + g.q1_res[p] + 2 * gm, v);
+  }
+  for (uint32_t p = t; p < g.n_q1; p += kBT) {
+    uint32_t b = 0;
+    for (uint32_t j = 0; j <= p; j++) b |= S.bad[j];
+    if (b) atomicOr(req_status + g.q1_idx[p], ST_DOMAIN);
+  }
+  __syncthreads();
 }
 
-unsigned scan_grid(gpudb_ctx* ctx, uint32_t tiles, size_t smem) {
+__global__ void __launch_bounds__(kBT) scan_batch_kernel(const ScanGroup* __restrict__ groups,
+                                                         const ScanTile* __restrict__ tiles, uint32_t n_tiles,
+                                                         unsigned* queue, unsigned long long* res, uint32_t* req_status) {
+  extern __shared__ __align__(16) unsigned char scan_smem[];
+  ScanSmem& S = *reinterpret_cast<ScanSmem*>(scan_smem);
+  const int t = threadIdx.x, warp = t >> 5;
+  int64_t rev[kMaxQ6];
+  uint32_t cnt[kMaxQ6];
+  uint32_t cur = 0xFFFFFFFFu;
+  for (;;) {
+    if (t == 0) S.tile = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t i = S.tile;
+    const uint32_t gi = i < n_tiles ? tiles[i].group : 0xFFFFFFFFu;
+    if (gi != cur) {   // block-uniform
+      if (cur != 0xFFFFFFFFu) flush_group(S, rev, cnt, res, req_status);
+      if (i >= n_tiles) break;
+      for (uint32_t w = t; w < sizeof(ScanGroup) / 4; w += kBT)
+        reinterpret_cast<uint32_t*>(&S.g)[w] = reinterpret_cast<const uint32_t*>(groups + gi)[w];
+      for (uint32_t w = t; w < kQ1Keys * 6; w += kBT) (&S.bacc[0][0])[w] = 0;
+      if (t <= kMaxQ1) S.bad[t] = 0;
+#pragma unroll
+      for (int r = 0; r < kMaxQ6; r++) { rev[r] = 0; cnt[r] = 0; }
+      cur = gi;
+      __syncthreads();   // the descriptor and cleared sums are visible to every thread
+    }
+    if (i >= n_tiles) break;   // a block that never got a tile
+    const uint32_t nq6 = S.g.n_q6, nq1 = S.g.n_q1;
+    if (nq1)
+      for (uint32_t w = t; w < (uint32_t)kBW * (nq1 * 6) * 4; w += kBT) {
+        const uint32_t wp = w / ((nq1 * 6) * 4), rest = w % ((nq1 * 6) * 4);
+        S.wacc[wp][rest / 4][rest % 4] = 0;
+      }
+    __syncthreads();
+    const ScanTile T = tiles[i];
+    const bool vec = S.g.vec != 0;
+    uint32_t bad = 0;
+    for (uint64_t q = (T.begin >> 2) + t; q < ((T.end + 3) >> 2); q += kBT) {
+      const uint64_t r0 = q << 2;
+      int32_t sh[4], ds[4], qt[4], tx[4] = {0, 0, 0, 0};
+      int64_t ex[4];
+      uint32_t fl = 0xFFFFFFFFu, st = 0xFFFFFFFFu;
+      bool ok[4];
+      if (vec && r0 >= T.begin && r0 + 4 <= T.end) {
+        const int4 a = ld_stream(reinterpret_cast<const int4*>(S.g.ship) + q);
+        const int4 d = ld_stream(reinterpret_cast<const int4*>(S.g.disc) + q);
+        const int4 b = ld_stream(reinterpret_cast<const int4*>(S.g.qty) + q);
+        const longlong2 e0 = ld_stream(reinterpret_cast<const longlong2*>(S.g.ext) + 2 * q);
+        const longlong2 e1 = ld_stream(reinterpret_cast<const longlong2*>(S.g.ext) + 2 * q + 1);
+        sh[0] = a.x; sh[1] = a.y; sh[2] = a.z; sh[3] = a.w;
+        ds[0] = d.x; ds[1] = d.y; ds[2] = d.z; ds[3] = d.w;
+        qt[0] = b.x; qt[1] = b.y; qt[2] = b.z; qt[3] = b.w;
+        ex[0] = e0.x; ex[1] = e0.y; ex[2] = e1.x; ex[3] = e1.y;
+        if (nq1) {
+          const int4 x = ld_stream(reinterpret_cast<const int4*>(S.g.tax) + q);
+          tx[0] = x.x; tx[1] = x.y; tx[2] = x.z; tx[3] = x.w;
+          fl = ld_stream(reinterpret_cast<const uint32_t*>(S.g.flag) + q);
+          st = ld_stream(reinterpret_cast<const uint32_t*>(S.g.stat) + q);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) ok[k] = true;
+      } else {
+        fl = 0; st = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint64_t r = r0 + k;
+          ok[k] = r >= T.begin && r < T.end;
+          sh[k] = ok[k] ? S.g.ship[r] : 0;
+          ds[k] = ok[k] ? S.g.disc[r] : 0;
+          qt[k] = ok[k] ? S.g.qty[r] : 0;
+          ex[k] = ok[k] ? S.g.ext[r] : 0;
+          if (nq1) {
+            tx[k] = ok[k] ? S.g.tax[r] : 0;
+            fl |= (ok[k] ? (uint32_t)S.g.flag[r] : 0xFFu) << (8 * k);
+            st |= (ok[k] ? (uint32_t)S.g.stat[r] : 0xFFu) << (8 * k);
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kMaxQ6; r++) {
+        if (r >= (int)nq6) break;
+        const int32_t lo = S.g.q6p[r][0], hi = S.g.q6p[r][1], dlo = S.g.q6p[r][2], dhi = S.g.q6p[r][3], qlt = S.g.q6p[r][4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const bool m = ok[k] & (sh[k] >= lo) & (sh[k] < hi) & (ds[k] >= dlo) & (ds[k] <= dhi) & (qt[k] < qlt);
+          rev[r] += m ? ex[k] * (int64_t)ds[k] : 0;
+          cnt[r] += m;
+        }
+      }
+      if (nq1) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint32_t f = (fl >> (8 * k)) & 0xFFu, s = (st >> (8 * k)) & 0xFFu;
+          if (!ok[k] || f > 2u || s > 1u) continue;
+          // bucket = number of cutoffs below the ship date (cutoffs padded with INT32_MAX)
+          uint32_t j = 0;
+#pragma unroll
+          for (uint32_t step = 8; step > 0; step >>= 1)
+            if (S.g.q1_cut[j + step - 1] < sh[k]) j += step;
+          if (j >= nq1) continue;
+          const int32_t qv = qt[k], dv = ds[k], tv = tx[k];
+          const int64_t e = ex[k];
+          const uint32_t viol = ((uint32_t)qv >= 65536u) | ((uint32_t)dv > 100u) | ((uint32_t)tv > 100u) |
+                                ((uint64_t)e >= (1ull << 36));
+          if (viol) { atomicOr(&S.bad[j], 1u); continue; }
+          const uint64_t ed = (uint64_t)e * (uint32_t)dv;
+          const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)tv;
+          unsigned long long* a = S.wacc[warp][j * 6 + f * 2 + s];
+          atomicAdd(a + 0, ((uint64_t)(uint32_t)qv << 32) | ((uint64_t)(uint32_t)dv << 13) | 1u);
+          atomicAdd(a + 1, (unsigned long long)e);
+          atomicAdd(a + 2, (unsigned long long)ed);
+          atomicAdd(a + 3, (unsigned long long)edt);
+        }
+      }
+    }
+    (void)bad;
+    __syncthreads();
+    if (nq1) {   // fold the warps' tile sums into the block's u128 sums
+      for (uint32_t k = t; k < nq1 * 6; k += kBT) {
+        u128 c = 0, qs = 0, ds = 0, e = 0, ed = 0, edt = 0;
+        for (int w = 0; w < kBW; w++) {
+          const unsigned long long P = S.wacc[w][k][0];
+          c += P & 0x1FFFu;
+          ds += (P >> 13) & 0x7FFFFu;
+          qs += P >> 32;
+          e += S.wacc[w][k][1];
+          ed += S.wacc[w][k][2];
+          edt += S.wacc[w][k][3];
+        }
+        S.bacc[k][0] += c; S.bacc[k][1] += qs; S.bacc[k][2] += e;
+        S.bacc[k][3] += ed; S.bacc[k][4] += edt; S.bacc[k][5] += ds;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+size_t scan_smem_bytes() { return (sizeof(ScanSmem) + 15) / 16 * 16; }
+
+unsigned scan_grid(gpudb_ctx* ctx, uint32_t tiles) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_batch_kernel, kBT, smem) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_batch_kernel, kBT, scan_smem_bytes()) != cudaSuccess ||
+      per_sm < 1)
     per_sm = 1;
   return std::max<unsigned>(1, std::min<unsigned>(tiles, (unsigned)(ctx->sm_count * per_sm)));
 }
@@ -128,31 +257,79 @@ bool scan_columns_ok(const gpudb_request& r) {
   return li->ship_date && li->quantity && li->ext_price && li->discount && li->tax && li->flag && li->status;
 }
 
-// Runs one scan batch (fits one result slot): requests `ids` of `reqs`.
+bool aligned(const void* p, uintptr_t a) { return !p || (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+// Runs the scan requests `ids` of `reqs` as shared scans (fits one result slot).
 int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t>& ids, gpudb_timing* t,
                    const gpudb_exec* ex) {
-  std::vector<ScanReq> sr;
-  std::vector<ScanTile> tiles;
+  // group by (scan columns, row range); within a group, Q1 requests also share their
+  // tax/flag/status columns, so they are sub-grouped by those
+  using Key = std::tuple<const void*, const void*, const void*, const void*, uint64_t, uint64_t>;
+  using Q1Cols = std::tuple<const void*, const void*, const void*>;
+  struct Members {
+    std::vector<uint32_t> q6;
+    std::map<Q1Cols, std::vector<uint32_t>> q1;
+  };
+  std::map<Key, Members> by_table;   // -> positions in ids
   uint32_t words = 0;
+  std::vector<uint32_t> offs(ids.size());
   for (uint32_t k = 0; k < ids.size(); k++) {
-    gpudb_request& q = reqs[ids[k]];
+    const gpudb_request& q = reqs[ids[k]];
     const gpudb_lineitem* li = q.li;
-    ScanReq d{};
-    d.kind = q.pipeline;
-    if (q.pipeline == GPUDB_PIPE_Q6) {
-      d.a = q.q6.ship_lo; d.b = q.q6.ship_hi; d.c = q.q6.disc_lo; d.d = q.q6.disc_hi; d.e = q.q6.qty_lt;
-    } else {
-      d.a = q.q1.ship_le;
-    }
-    d.ship = li->ship_date; d.qty = li->quantity; d.disc = li->discount; d.tax = li->tax; d.ext = li->ext_price;
-    d.flag = li->flag; d.stat = li->status;
-    d.res = words;
-    d.idx = k;
-    words += q.pipeline == GPUDB_PIPE_Q6 ? kQ6Words : kQ1Words;
     const uint64_t end = q.row_end ? std::min<uint64_t>(q.row_end, li->n_rows) : li->n_rows;
-    for (uint64_t b = q.row_begin; b < end; b += kTileRows)
-      tiles.push_back(ScanTile{(uint32_t)sr.size(), 0, b, std::min(b + kTileRows, end)});
-    sr.push_back(d);
+    const uint64_t begin = std::min<uint64_t>(q.row_begin, end);
+    Members& m = by_table[Key(li->ship_date, li->quantity, li->discount, li->ext_price, begin, end)];
+    if (q.pipeline == GPUDB_PIPE_Q6) m.q6.push_back(k);
+    else m.q1[Q1Cols(li->tax, li->flag, li->status)].push_back(k);
+    offs[k] = words;
+    words += q.pipeline == GPUDB_PIPE_Q6 ? kQ6Words : kQ1Words;
+  }
+  std::vector<ScanGroup> groups;
+  std::vector<ScanTile> tiles;
+  for (auto& kv : by_table) {
+    Members& mb = kv.second;
+    for (auto& c : mb.q1)
+      std::sort(c.second.begin(), c.second.end(),
+                [&](uint32_t a, uint32_t b) { return reqs[ids[a]].q1.ship_le < reqs[ids[b]].q1.ship_le; });
+    auto q1it = mb.q1.begin();
+    size_t i6 = 0, i1 = 0;
+    while (i6 < mb.q6.size() || q1it != mb.q1.end()) {
+      ScanGroup g{};
+      g.ship = static_cast<const int32_t*>(std::get<0>(kv.first));
+      g.qty = static_cast<const int32_t*>(std::get<1>(kv.first));
+      g.disc = static_cast<const int32_t*>(std::get<2>(kv.first));
+      g.ext = static_cast<const int64_t*>(std::get<3>(kv.first));
+      g.begin = std::get<4>(kv.first);
+      g.end = std::get<5>(kv.first);
+      for (; i6 < mb.q6.size() && g.n_q6 < (uint32_t)kMaxQ6; i6++, g.n_q6++) {
+        const gpudb_q6_params& p = reqs[ids[mb.q6[i6]]].q6;
+        const int32_t v[5] = {p.ship_lo, p.ship_hi, p.disc_lo, p.disc_hi, p.qty_lt};
+        std::memcpy(g.q6p[g.n_q6], v, sizeof v);
+        g.q6_res[g.n_q6] = offs[mb.q6[i6]];
+      }
+      if (q1it != mb.q1.end()) {
+        g.tax = static_cast<const int32_t*>(std::get<0>(q1it->first));
+        g.flag = static_cast<const uint8_t*>(std::get<1>(q1it->first));
+        g.stat = static_cast<const uint8_t*>(std::get<2>(q1it->first));
+        const std::vector<uint32_t>& l = q1it->second;
+        for (; i1 < l.size() && g.n_q1 < (uint32_t)kMaxQ1; i1++, g.n_q1++) {
+          g.q1_cut[g.n_q1] = reqs[ids[l[i1]]].q1.ship_le;
+          g.q1_res[g.n_q1] = offs[l[i1]];
+          g.q1_idx[g.n_q1] = l[i1];
+        }
+        if (i1 == l.size()) { ++q1it; i1 = 0; }
+      }
+      for (uint32_t j = g.n_q1; j <= (uint32_t)kMaxQ1; j++) g.q1_cut[j] = INT32_MAX;
+      g.vec = aligned(g.ship, 16) && aligned(g.qty, 16) && aligned(g.disc, 16) && aligned(g.ext, 16) &&
+              aligned(g.tax, 16) && aligned(g.flag, 4) && aligned(g.stat, 4);
+      const uint32_t gi = (uint32_t)groups.size();
+      groups.push_back(g);
+      for (uint64_t b = g.begin; b < g.end;) {
+        const uint64_t e = std::min<uint64_t>(g.end, (b / kTileRows + 1) * kTileRows);
+        tiles.push_back(ScanTile{gi, 0, b, e});
+        b = e;
+      }
+    }
   }
   const size_t status_bytes = ((ids.size() * 4 + 15) / 16) * 16;
   const size_t bytes = status_bytes + (size_t)words * 8;
@@ -162,27 +339,25 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
   uint8_t* dres = call.result<uint8_t>();
   if (!tiles.empty()) {
     void* desc = nullptr;
-    const size_t qbytes = 256, rbytes = sr.size() * sizeof(ScanReq), tbytes = tiles.size() * sizeof(ScanTile);
-    rc = scratch(ctx, "batch.desc", qbytes + rbytes + tbytes + 256, &desc);
+    const size_t qbytes = 256, gbytes = groups.size() * sizeof(ScanGroup), tbytes = tiles.size() * sizeof(ScanTile);
+    rc = scratch(ctx, "batch.desc", qbytes + gbytes + tbytes + 256, &desc);
     if (rc) return rc;
     uint8_t* base = static_cast<uint8_t*>(desc);
     unsigned* queue = reinterpret_cast<unsigned*>(base);
-    ScanReq* dreq = reinterpret_cast<ScanReq*>(base + qbytes);
-    ScanTile* dtile = reinterpret_cast<ScanTile*>(base + qbytes + ((rbytes + 15) / 16) * 16);
+    ScanGroup* dgrp = reinterpret_cast<ScanGroup*>(base + qbytes);
+    ScanTile* dtile = reinterpret_cast<ScanTile*>(base + qbytes + ((gbytes + 15) / 16) * 16);
     // pageable sources: the copies stage the descriptors before returning
     GPUDB_CUDA(ctx, cudaMemsetAsync(queue, 0, 4, call.stream()));
-    GPUDB_CUDA(ctx, cudaMemcpyAsync(dreq, sr.data(), rbytes, cudaMemcpyHostToDevice, call.stream()));
+    GPUDB_CUDA(ctx, cudaMemcpyAsync(dgrp, groups.data(), gbytes, cudaMemcpyHostToDevice, call.stream()));
     GPUDB_CUDA(ctx, cudaMemcpyAsync(dtile, tiles.data(), tbytes, cudaMemcpyHostToDevice, call.stream()));
-    const size_t smem = (size_t)24 * kBT * 8;
+    const size_t smem = scan_smem_bytes();
     GPUDB_CUDA(ctx, cudaFuncSetAttribute(scan_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const unsigned grid = scan_grid(ctx, (uint32_t)tiles.size(), smem);
-    GPUDB_LAUNCH(call, scan_batch_kernel, grid, kBT, smem, (const ScanReq*)dreq, (const ScanTile*)dtile,
+    const unsigned grid = scan_grid(ctx, (uint32_t)tiles.size());
+    GPUDB_LAUNCH(call, scan_batch_kernel, grid, kBT, smem, (const ScanGroup*)dgrp, (const ScanTile*)dtile,
                  (uint32_t)tiles.size(), queue, reinterpret_cast<unsigned long long*>(dres + status_bytes),
                  reinterpret_cast<uint32_t*>(dres));
   }
   std::vector<uint32_t> ids_copy = ids;
-  std::vector<uint32_t> offs;
-  for (auto& d : sr) offs.push_back(d.res);
   return call.finish(bytes, [reqs, ids_copy, offs, status_bytes, ctx](const uint8_t* h) {
     for (size_t k = 0; k < ids_copy.size(); k++) {
       gpudb_request& q = reqs[ids_copy[k]];

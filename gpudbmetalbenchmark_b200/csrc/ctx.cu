@@ -33,18 +33,30 @@ int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out) {
   Buffer& b = ctx->scratch[name];
   if (b.bytes < bytes) {
     if (b.p) {
-      // the old buffer may still be read by queued work
-      GPUDB_CUDA(ctx, cudaDeviceSynchronize());
-      cudaFree(b.p);
+      // queued work may still read the old buffer: retire it until the context is idle
+      ctx->retired.push_back(b.p);
       b.p = nullptr;
       b.bytes = 0;
     }
     size_t sz = std::max<size_t>(bytes, 256);
-    GPUDB_CUDA(ctx, cudaMalloc(&b.p, sz));
+    cudaError_t e = cudaMallocAsync(&b.p, sz, ctx->stream);
+    // complete the allocation before any stream of this context (or a caller's) uses it
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      b.p = nullptr;
+      return e == cudaErrorMemoryAllocation ? fail(ctx, GPUDB_E_OOM, "scratch %s: %zu bytes", name, sz)
+                                            : cuda_fail(ctx, e, "cudaMallocAsync");
+    }
     b.bytes = sz;
   }
   *out = b.p;
   return GPUDB_OK;
+}
+
+// Frees outgrown scratch; only when no work of the context can still be queued.
+void release_retired(gpudb_ctx* ctx) {
+  for (void* p : ctx->retired) cudaFreeAsync(p, ctx->stream);
+  ctx->retired.clear();
 }
 
 cudaEvent_t event_get(gpudb_ctx* ctx) {
@@ -188,6 +200,7 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
     done();
     return cuda_fail(ctx_, e, "cudaStreamSynchronize");
   }
+  if (ctx_->pending.empty() && s_ == ctx_->stream) release_retired(ctx_);
   return done();
 }
 
@@ -339,9 +352,14 @@ int gpudb_create(int device, gpudb_ctx** out) {
 int gpudb_destroy(gpudb_ctx* ctx) {
   if (!ctx) return GPUDB_OK;
   cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
-  for (auto& kv : ctx->scratch) cudaFree(kv.second.p);
+  if (ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    release_retired(ctx);
+    for (auto& kv : ctx->scratch)
+      if (kv.second.p) cudaFreeAsync(kv.second.p, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+  }
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->d_slots) cudaFree(ctx->d_slots);
   if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
@@ -367,6 +385,7 @@ int gpudb_sync(gpudb_ctx* ctx) {
   std::vector<std::function<int()>> work;
   work.swap(ctx->pending);
   ctx->pending_streams.clear();
+  if (rc == GPUDB_OK) release_retired(ctx);
   for (auto& f : work) {
     int r = f();
     if (r != GPUDB_OK && rc == GPUDB_OK) rc = r;

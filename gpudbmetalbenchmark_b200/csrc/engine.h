@@ -48,6 +48,7 @@ struct gpudb_ctx {
   uint64_t chunk_rows = gpudb::kDefaultChunkRows;
   int scan_variant = 0;                // scan kernel choice (GPUDB_OPT_SCAN_VARIANT)
   std::unordered_map<std::string, gpudb::Buffer> scratch;
+  std::vector<void*> retired;          // outgrown scratch, freed once the context is idle
   uint8_t* d_slots = nullptr;          // result slots (device)
   uint8_t* h_slots = nullptr;          // their pinned host mirror
   bool slot_busy[gpudb::kResultSlots] = {};
@@ -73,6 +74,9 @@ int cuda_fail(gpudb_ctx* ctx, cudaError_t e, const char* what);
   } while (0)
 
 // Grow-only named scratch buffer on the device (never shrinks; freed at gpudb_destroy).
+// Stream-ordered allocation: growing one context's buffer waits for that context's compute
+// stream only, never for the whole device, and the outgrown buffer is freed in stream order
+// once the context is idle (gpudb_sync, or a synchronous call with nothing pending).
 int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out);
 
 cudaEvent_t event_get(gpudb_ctx* ctx);

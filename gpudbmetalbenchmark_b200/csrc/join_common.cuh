@@ -51,6 +51,31 @@ __device__ __forceinline__ uint32_t warp_append(bool take, uint32_t* counter) {
   return base + __popc(m & lanemask_lt());
 }
 
+// Block-aggregated reservation: each thread asks for `mine` output positions and gets the
+// first of them; the block takes one atomicAdd on `counter`. Every thread of the block must
+// call it the same number of times. `sh` needs 33 words of shared memory.
+template <int T>
+__device__ __forceinline__ uint32_t block_reserve(uint32_t mine, uint32_t* counter, uint32_t* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = mine;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(FULL_MASK, inc, d);
+    if (lane >= d) inc += o;
+  }
+  if (lane == 31) sh[warp] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int w = 0; w < T / 32; w++) { const uint32_t c = sh[w]; sh[w] = run; run += c; }
+    sh[32] = run ? atomicAdd(counter, run) : 0u;
+  }
+  __syncthreads();
+  const uint32_t pos = sh[32] + sh[warp] + inc - mine;
+  __syncthreads();
+  return pos;
+}
+
 // Open-addressing table capacity from a device-side count: the smallest power of two
 // >= 2*count (at most 50% load), at least `min_cap`, at most `max_cap`.
 __device__ __forceinline__ uint32_t table_capacity(uint32_t count, uint32_t min_cap, uint32_t max_cap) {
@@ -89,61 +114,65 @@ constexpr int kTopkThreads = 256;
 constexpr int kTopkPerThread = 16;
 constexpr int kTopkTile = kTopkThreads * kTopkPerThread;   // 4096 candidates per block
 
-// Block top-k over a tile held as kTopkPerThread composites per thread (0 = no candidate).
-// k rounds of block arg-max; the winner removes its element and rescans its own 16. Writes
-// k composites (0-padded) to out.
-__device__ __forceinline__ void block_topk(u128 (&v)[kTopkPerThread], int k, u128* out) {
-  __shared__ u128 wbest[kTopkThreads / 32];
-  __shared__ int wowner[kTopkThreads / 32];
-  __shared__ int winner;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int bi = 0;
-  u128 best = 0;
+// Block top-k over a tile held as kTopkPerThread composites per thread (0 = no candidate),
+// k <= GPUDB_Q3_MAX_K. Writes the k largest composites in descending order (0-padded) to
+// out. Method: rank the 256 per-thread maxima; only the k threads whose maxima rank below
+// k can hold a top-k element, and only their values >= T (the maximum of rank k-1) can, so
+// at most kTopkPerThread*k candidates remain; each candidate's rank among them is its
+// output position. Composites of one tile are distinct apart from 0; ties are broken by
+// position all the same, so every rank is unique. `sm` is shared scratch of kTopkScratch
+// composites.
+constexpr int kTopkScratch = kTopkThreads + kTopkPerThread * 64;
+__device__ __forceinline__ void block_topk(const u128 (&v)[kTopkPerThread], int k, u128* out, u128* sm) {
+  __shared__ uint32_t ncand;
+  __shared__ u128 thr;
+  u128* mx = sm;
+  u128* cand = sm + kTopkThreads;
+  const int t = threadIdx.x;
+  u128 m = v[0];
 #pragma unroll
-  for (int j = 0; j < kTopkPerThread; j++)
-    if (v[j] > best) { best = v[j]; bi = j; }
-  for (int r = 0; r < k; r++) {
-    u128 m = best;
-    int owner = threadIdx.x;
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) {
-      u128 o = shfl_u128(m, lane ^ d);
-      int oo = __shfl_xor_sync(FULL_MASK, owner, d);
-      if (o > m || (o == m && oo < owner)) { m = o; owner = oo; }
-    }
-    if (lane == 0) { wbest[warp] = m; wowner[warp] = owner; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      u128 b = wbest[0];
-      int o = wowner[0];
-      for (int w = 1; w < kTopkThreads / 32; w++)
-        if (wbest[w] > b) { b = wbest[w]; o = wowner[w]; }
-      out[r] = b;
-      winner = (b == 0) ? -1 : o;
-    }
-    __syncthreads();
-    if ((int)threadIdx.x == winner) {
-#pragma unroll
-      for (int j = 0; j < kTopkPerThread; j++)
-        if (j == bi) v[j] = 0;
-      best = 0;
-      bi = 0;
-#pragma unroll
-      for (int j = 0; j < kTopkPerThread; j++)
-        if (v[j] > best) { best = v[j]; bi = j; }
-    }
-    __syncthreads();
+  for (int j = 1; j < kTopkPerThread; j++) m = v[j] > m ? v[j] : m;
+  mx[t] = m;
+  if (t == 0) ncand = 0;
+  __syncthreads();
+  int rank = 0;
+#pragma unroll 8
+  for (int u = 0; u < kTopkThreads; u++) {
+    const u128 o = mx[u];
+    rank += (o > m) | ((o == m) & (u < t));
   }
+  if (rank == k - 1) thr = m;
+  __syncthreads();
+  if (rank < k) {
+    const u128 T = thr;
+#pragma unroll
+    for (int j = 0; j < kTopkPerThread; j++)
+      if (v[j] != 0 && v[j] >= T) cand[atomicAdd(&ncand, 1u)] = v[j];
+  }
+  __syncthreads();
+  const int C = (int)ncand;
+  for (int i = t; i < C; i += kTopkThreads) {
+    const u128 c = cand[i];
+    int r = 0;
+    for (int j = 0; j < C; j++) {
+      const u128 o = cand[j];
+      r += (o > c) | ((o == c) & (j < i));
+    }
+    if (r < k) out[r] = c;
+  }
+  for (int i = C + t; i < k; i += kTopkThreads) out[i] = 0;
+  __syncthreads();
 }
 
 // Top-k of `n` composites (tiles of kTopkTile per block) -> k per block.
 static __global__ void __launch_bounds__(kTopkThreads) topk_merge_kernel(const u128* __restrict__ in, uint64_t n, int k,
                                                                   u128* __restrict__ out) {
+  __shared__ u128 wtop[kTopkScratch];
   u128 v[kTopkPerThread];
   const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
 #pragma unroll
   for (int j = 0; j < kTopkPerThread; j++) v[j] = (base + j < n) ? in[base + j] : (u128)0;
-  block_topk(v, k, out + (size_t)blockIdx.x * k);
+  block_topk(v, k, out + (size_t)blockIdx.x * k, wtop);
 }
 
 }  // namespace gpudb

@@ -7,19 +7,21 @@
 // B200 design (global-table mode):
 //  1. bitmap_build_kernel: customers with segment == S -> bitmap (warp-combined atomicOr).
 //  2. orders_filter_kernel: orders with order_date < D and cust in the bitmap are compacted
-//     (warp ballot + one atomicAdd per warp) into a staging list; the qualifying count stays
-//     on the device.
+//     (block prefix sum + one atomicAdd per 1024 rows) into a staging list; the qualifying
+//     count stays on the device.
 //  3. table_clear_kernel: sizes the hash table from that count on the device (power of two,
 //     <= 50% load) and clears only those slots, so no host round trip is needed.
 //  4. orders_insert_kernel: atomicCAS insertion; each slot is {key, date, revenue} and a
 //     parallel hit counter, so the orders table doubles as the per-order aggregation table
 //     (the group key equals the join key).
 //  5. q3_probe_kernel: one lane per fact row; runs of equal order keys (adjacent rows of one
-//     order) are found with a warp ballot, only the run head probes the table, and the run's
+//     order) are found with a warp ballot, only the run head probes the table (after a test
+//     of the order-key bitmap that step 4 sets, which turns away most misses), and the run's
 //     revenue is summed with a warp prefix scan, so each run costs one 64-bit atomicAdd.
 //     ext_price and discount are loaded only for rows that passed the date filter and found
 //     their order (late materialisation).
-//  6. topk kernels: block top-k over the table slots, then over the block winners.
+//  6. q3_topk_slots_kernel: block top-k over each 4096-slot tile of the live table, then the
+//     last block to finish merges the tiles' winners (one launch).
 // Radix mode partitions both sides by key hash and joins each partition in shared memory
 // (radix.cu).
 #include <algorithm>
@@ -41,28 +43,39 @@ struct Q3Slot {
 
 namespace {
 
-__global__ void orders_filter_kernel(const int32_t* __restrict__ okey, const int32_t* __restrict__ ocust,
+constexpr int kFilterRows = 4;   // rows per thread per block step of orders_filter_kernel
+
+__global__ void __launch_bounds__(256) orders_filter_kernel(const int32_t* __restrict__ okey, const int32_t* __restrict__ ocust,
                                      const int32_t* __restrict__ odate, uint64_t n, int32_t date_lt,
                                      const uint32_t* __restrict__ bitmap, int32_t cust_max, int32_t* out_key,
                                      int32_t* out_date, uint32_t* count, uint32_t* status) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t end = (n + 31) & ~31ull;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
-    bool take = false;
-    int32_t key = 0, date = 0;
-    if (i < n) {
-      date = odate[i];
-      if (date < date_lt) {
-        const int32_t c = ocust[i];
-        if (c >= 0 && c <= cust_max && bitmap_test(bitmap, c)) {
-          key = okey[i];
-          if (key == kEmptyKey) set_status(status, ST_KEY_RANGE);
-          else take = true;
+  __shared__ uint32_t sh[33];
+  const uint64_t step = (uint64_t)gridDim.x * 256 * kFilterRows;
+  // whole blocks stay in the loop: block_reserve needs every thread of the block
+  for (uint64_t b = (uint64_t)blockIdx.x * 256 * kFilterRows; b < n; b += step) {
+    int32_t key[kFilterRows], date[kFilterRows];
+    uint32_t take = 0;
+#pragma unroll
+    for (int j = 0; j < kFilterRows; j++) {
+      const uint64_t i = b + (uint64_t)j * 256 + threadIdx.x;
+      key[j] = 0;
+      date[j] = 0;
+      if (i < n) {
+        date[j] = odate[i];
+        if (date[j] < date_lt) {
+          const int32_t c = ocust[i];
+          if (c >= 0 && c <= cust_max && bitmap_test(bitmap, c)) {
+            key[j] = okey[i];
+            if (key[j] == kEmptyKey) set_status(status, ST_KEY_RANGE);
+            else take |= 1u << j;
+          }
         }
       }
     }
-    const uint32_t pos = warp_append(take, count);
-    if (take) { out_key[pos] = key; out_date[pos] = date; }
+    uint32_t pos = block_reserve<256>(__popc(take), count, sh);
+#pragma unroll
+    for (int j = 0; j < kFilterRows; j++)
+      if (take & (1u << j)) { out_key[pos] = key[j]; out_date[pos] = date[j]; pos++; }
   }
 }
 
@@ -79,12 +92,20 @@ __global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint
   }
 }
 
+// Also sets bit `key` of the order-key bitmap `okbm` (keys in [0, key_max]); a key outside
+// that range turns the bitmap off for this query (okbm_off), so the probe then walks the
+// table for every run.
 __global__ void orders_insert_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ date,
-                                     const uint32_t* count, const uint32_t* cap_p, Q3Slot* ht, uint32_t* status) {
+                                     const uint32_t* count, const uint32_t* cap_p, Q3Slot* ht, uint32_t* okbm,
+                                     int32_t key_max, uint32_t* okbm_off, uint32_t* status) {
   const uint32_t n = *count, cap = *cap_p, mask = cap - 1;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const int32_t k = key[i];
+    if (okbm) {
+      if (k >= 0 && k <= key_max) atomicOr(okbm + ((uint32_t)k >> 5), 1u << ((uint32_t)k & 31u));
+      else *okbm_off = 1u;
+    }
     uint32_t s = key_slot(k, mask);
     bool done = false;
     for (uint32_t p = 0; p < cap && !done; p++, s = (s + 1) & mask) {
@@ -107,78 +128,134 @@ __device__ __forceinline__ int32_t ht_find(const Q3Slot* ht, uint32_t cap, int32
   return -1;
 }
 
+constexpr int kProbeBatches = 4;   // independent 32-row batches per warp step (memory-level parallelism)
+
 __global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict__ lkey, const int32_t* __restrict__ lship,
                                                        const int64_t* __restrict__ lext, const int32_t* __restrict__ ldisc,
                                                        uint64_t n, int32_t ship_gt, Q3Slot* ht, uint32_t* hits,
-                                                       const uint32_t* cap_p) {
+                                                       const uint32_t* cap_p, const uint32_t* __restrict__ okbm,
+                                                       int32_t key_max, const uint32_t* okbm_off) {
   const uint32_t cap = *cap_p;
+  // order-key bitmap: a run whose key is not in it cannot join (skips the table walk)
+  const uint32_t* bm = (okbm && *okbm_off == 0u) ? okbm : nullptr;
   const int lane = threadIdx.x & 31;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n; base += warps * 32) {
-    const uint64_t row = base + lane;
-    const bool valid = row < n;
-    const int32_t key = valid ? ld_stream(lkey + row) : kEmptyKey;
-    const bool pass = valid && ld_stream(lship + row) > ship_gt;
-    const int32_t prev = __shfl_up_sync(FULL_MASK, key, 1);
-    const bool head = (lane == 0) || (key != prev);
-    const uint32_t heads = __ballot_sync(FULL_MASK, head);
-    const uint32_t passm = __ballot_sync(FULL_MASK, pass);
-    // run = [head lane, next head); `last` = last lane of this lane's run
-    const int my_head = 31 - __clz(heads & lanemask_le());
-    const uint32_t later = heads & lanemask_gt();
-    const int last = later ? (__ffs(later) - 2) : 31;
-    const uint32_t run_mask = (last == 31 ? 0xFFFFFFFFu : ((1u << (last + 1)) - 1u)) & ~((1u << my_head) - 1u);
-    int32_t slot = -1;
-    if (head && (passm & run_mask) && key != kEmptyKey) slot = ht_find(ht, cap, key);
-    slot = __shfl_sync(FULL_MASK, slot, my_head);
-    const bool hit = pass && slot >= 0;
-    int64_t v = 0;
-    if (hit) v = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
-    // inclusive prefix sum of v across the warp
-    int64_t inc = v;
+  constexpr int U = kProbeBatches;
+  for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U; base < n;
+       base += warps * 32 * U) {
+    int32_t key[U];
+    bool pass[U];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      int64_t o = __shfl_up_sync(FULL_MASK, inc, d);
-      if (lane >= d) inc += o;
+    for (int u = 0; u < U; u++) {
+      const uint64_t row = base + u * 32 + lane;
+      const bool valid = row < n;
+      key[u] = valid ? ld_stream(lkey + row) : kEmptyKey;
+      pass[u] = valid && ld_stream(lship + row) > ship_gt;
     }
-    const int64_t run_end = __shfl_sync(FULL_MASK, inc, last);
-    const int64_t before = inc - v;   // exclusive prefix at this lane
-    const uint32_t hitm = __ballot_sync(FULL_MASK, hit);
-    if (head && slot >= 0) {
-      const uint32_t c = __popc(hitm & run_mask);
-      if (c) {
-        atomicAdd(&ht[slot].rev, (unsigned long long)(run_end - before));
-        atomicAdd(&hits[slot], c);
+    int32_t slot[U];
+    uint32_t run_mask[U];
+    int my_head[U], last[U];
+    bool head[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int32_t prev = __shfl_up_sync(FULL_MASK, key[u], 1);
+      head[u] = (lane == 0) || (key[u] != prev);
+      const uint32_t heads = __ballot_sync(FULL_MASK, head[u]);
+      const uint32_t passm = __ballot_sync(FULL_MASK, pass[u]);
+      // run = [head lane, next head); `last` = last lane of this lane's run
+      my_head[u] = 31 - __clz(heads & lanemask_le());
+      const uint32_t later = heads & lanemask_gt();
+      last[u] = later ? (__ffs(later) - 2) : 31;
+      run_mask[u] = (last[u] == 31 ? 0xFFFFFFFFu : ((1u << (last[u] + 1)) - 1u)) & ~((1u << my_head[u]) - 1u);
+      slot[u] = -1;
+      if (head[u] && (passm & run_mask[u]) && key[u] != kEmptyKey) {
+        const bool maybe = !bm || (key[u] >= 0 && key[u] <= key_max && bitmap_test(bm, key[u]));
+        if (maybe) slot[u] = ht_find(ht, cap, key[u]);
+      }
+    }
+    int64_t v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      slot[u] = __shfl_sync(FULL_MASK, slot[u], my_head[u]);
+      const uint64_t row = base + u * 32 + lane;
+      v[u] = 0;
+      if (pass[u] && slot[u] >= 0) v[u] = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool hit = pass[u] && slot[u] >= 0;
+      // inclusive prefix sum of v across the warp
+      int64_t inc = v[u];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int64_t o = __shfl_up_sync(FULL_MASK, inc, d);
+        if (lane >= d) inc += o;
+      }
+      const int64_t run_end = __shfl_sync(FULL_MASK, inc, last[u]);
+      const int64_t before = inc - v[u];   // exclusive prefix at this lane
+      const uint32_t hitm = __ballot_sync(FULL_MASK, hit);
+      if (head[u] && slot[u] >= 0) {
+        const uint32_t c = __popc(hitm & run_mask[u]);
+        if (c) {
+          atomicAdd(&ht[slot[u]].rev, (unsigned long long)(run_end - before));
+          atomicAdd(&hits[slot[u]], c);
+        }
       }
     }
   }
 }
 
-// Level 1 of the top-k: slots [blockIdx*4096, +4096) of the table; also counts groups.
+// Other blocks' candidates, read past L1.
+__device__ __forceinline__ u128 ld_cg_u128(const u128* p) {
+  const ulonglong2 q = __ldcg(reinterpret_cast<const ulonglong2*>(p));
+  return ((u128)q.y << 64) | q.x;
+}
+
+// Top-k of the table: block b takes slots [b*4096, +4096) (and counts groups), writes its
+// k best to cand[b*k..]; the last block to finish then merges the candidates of the live
+// tiles (the table holds *cap_p slots) in chunks, carrying the running top-k, into out.
 __global__ void __launch_bounds__(kTopkThreads) q3_topk_slots_kernel(const Q3Slot* __restrict__ ht,
                                                                      const uint32_t* __restrict__ hits,
-                                                                     const uint32_t* cap_p, int k, u128* out,
-                                                                     unsigned long long* groups) {
+                                                                     const uint32_t* cap_p, int k, u128* cand,
+                                                                     unsigned long long* groups, unsigned* ticket,
+                                                                     u128* out) {
+  __shared__ u128 sm[kTopkScratch];
+  __shared__ u128 carry[GPUDB_Q3_MAX_K];
   const uint32_t cap = *cap_p;
-  if ((uint64_t)blockIdx.x * kTopkTile >= cap) {   // past the live table: no candidates
-    for (int i = threadIdx.x; i < k; i += kTopkThreads) out[(size_t)blockIdx.x * k + i] = 0;
-    return;
-  }
   u128 v[kTopkPerThread];
-  uint32_t cnt = 0;
-  const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
+  if ((uint64_t)blockIdx.x * kTopkTile < cap) {   // blocks past the live table have no work
+    uint32_t cnt = 0;
+    const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
 #pragma unroll
-  for (int j = 0; j < kTopkPerThread; j++) {
-    v[j] = 0;
-    const uint64_t s = base + j;
-    if (s < cap && hits[s]) {
-      v[j] = topk_compose((int64_t)ht[s].rev, ht[s].date, ht[s].key);
-      cnt++;
+    for (int j = 0; j < kTopkPerThread; j++) {
+      v[j] = 0;
+      const uint64_t s = base + j;
+      if (s < cap && hits[s]) {
+        v[j] = topk_compose((int64_t)ht[s].rev, ht[s].date, ht[s].key);
+        cnt++;
+      }
     }
+    cnt = __reduce_add_sync(FULL_MASK, cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(groups, (unsigned long long)cnt);
+    block_topk(v, k, cand + (size_t)blockIdx.x * k, sm);
   }
-  cnt = __reduce_add_sync(FULL_MASK, cnt);
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(groups, (unsigned long long)cnt);
-  block_topk(v, k, out + (size_t)blockIdx.x * k);
+  if (!grid_last_block(ticket)) return;
+  // merge: live tiles' candidates, kTopkTile - k per chunk plus the carried top-k
+  const uint64_t n = ((uint64_t)cap + kTopkTile - 1) / kTopkTile * k;
+  const uint64_t per = (uint64_t)kTopkTile - k;
+  for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
+  __syncthreads();
+  for (uint64_t c0 = 0; c0 < n; c0 += per) {
+#pragma unroll
+    for (int j = 0; j < kTopkPerThread; j++) {
+      const uint64_t idx = (uint64_t)threadIdx.x * kTopkPerThread + j;   // position in this chunk
+      if (idx < (uint64_t)k) v[j] = carry[idx];
+      else v[j] = (c0 + idx - k < n) ? ld_cg_u128(cand + c0 + idx - k) : (u128)0;
+    }
+    __syncthreads();
+    block_topk(v, k, carry, sm);
+  }
+  for (int i = threadIdx.x; i < k; i += kTopkThreads) out[i] = carry[i];
 }
 
 // ---- radix mode ----------------------------------------------------------------------
@@ -207,10 +284,15 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
     const int32_t* __restrict__ bk, const int32_t* __restrict__ bdate, const uint32_t* __restrict__ boff,
     const int32_t* __restrict__ pk, const int64_t* __restrict__ pval, const uint32_t* __restrict__ poff, int k,
     u128* cand, unsigned long long* groups, uint32_t* status) {
-  __shared__ int32_t hkey[kQ3PartCap], hdate[kQ3PartCap];
-  __shared__ unsigned long long hrev[kQ3PartCap];
-  __shared__ uint32_t hhit[kQ3PartCap];
+  // one pool: the partition's table {rev, key, date, hits}, reused as the top-k scratch
+  constexpr size_t kPool = (size_t)kQ3PartCap * (8 + 4 + 4 + 4);
+  static_assert(kPool >= kTopkScratch * sizeof(u128), "top-k scratch");
+  __shared__ __align__(16) unsigned char pool[kPool];
   __shared__ u128 carry[GPUDB_Q3_MAX_K];
+  unsigned long long* hrev = reinterpret_cast<unsigned long long*>(pool);
+  int32_t* hkey = reinterpret_cast<int32_t*>(hrev + kQ3PartCap);
+  int32_t* hdate = hkey + kQ3PartCap;
+  uint32_t* hhit = reinterpret_cast<uint32_t*>(hdate + kQ3PartCap);
   const uint32_t part = blockIdx.x, mask = kQ3PartCap - 1;
   const uint32_t b0 = boff[part], b1 = boff[part + 1], p0 = poff[part], p1 = poff[part + 1];
   for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
@@ -250,7 +332,7 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
     }
     if ((int)threadIdx.x < k) v[kTopkPerThread - 1] = carry[threadIdx.x];
     __syncthreads();
-    block_topk(v, k, carry);
+    block_topk(v, k, carry, reinterpret_cast<u128*>(pool));
     __syncthreads();
   }
   for (int i = threadIdx.x; i < k; i += kTopkThreads) cand[(size_t)part * k + i] = carry[i];
@@ -302,7 +384,7 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
     GPUDB_LAUNCH(call, bitmap_build_kernel, grid(cu.n_rows), 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows,
                  cu.key_max, (uint32_t*)bitmap, call.status());
   if (od.n_rows)
-    GPUDB_LAUNCH(call, orders_filter_kernel, grid(od.n_rows), 256, 0, od.order_key, od.cust_key, od.order_date, od.n_rows,
+    GPUDB_LAUNCH(call, orders_filter_kernel, grid((od.n_rows + kFilterRows - 1) / kFilterRows), 256, 0, od.order_key, od.cust_key, od.order_date, od.n_rows,
                  p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, bkey, bdate, cnt, call.status());
   const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
   rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
@@ -353,8 +435,12 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   const uint64_t n_or = od.n_rows;
   uint32_t max_cap = 2048;
   while (max_cap < 2 * n_or && max_cap < (1u << 31)) max_cap <<= 1;
-  void *bitmap, *stage, *count, *ht, *hits, *cand;
+  void *bitmap, *stage, *count, *ht, *hits, *cand, *okbm = nullptr;
+  // order-key bitmap for the probe's miss test when the orders carry a key bound
+  const bool use_okbm = n_or && od.key_max >= 0;
+  const size_t okbm_bytes = use_okbm ? ((size_t)((uint32_t)od.key_max >> 5) + 1) * 4 : 0;
   int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
+  if (!rc && use_okbm) rc = scratch(ctx, "q3.okbm", okbm_bytes, &okbm);
   if (!rc) rc = scratch(ctx, "q3.stage", std::max<size_t>(n_or, 1) * 8, &stage);
   if (!rc) rc = scratch(ctx, "q3.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q3.ht", (size_t)max_cap * sizeof(Q3Slot), &ht);
@@ -366,7 +452,8 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   uint32_t* cnt = static_cast<uint32_t*>(count);
   uint32_t* cap = cnt + 1;
   GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
-  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));   // [0] count, [1] capacity, [2] okbm off, [3] ticket
+  if (use_okbm) GPUDB_CUDA(ctx, cudaMemsetAsync(okbm, 0, okbm_bytes, s));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
   if (cu.n_rows)
@@ -375,18 +462,21 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   int32_t* skey = static_cast<int32_t*>(stage);
   int32_t* sdate = skey + std::max<uint64_t>(n_or, 1);
   if (n_or)
-    GPUDB_LAUNCH(call, orders_filter_kernel, grid(n_or), 256, 0, od.order_key, od.cust_key, od.order_date, n_or,
+    GPUDB_LAUNCH(call, orders_filter_kernel, grid((n_or + kFilterRows - 1) / kFilterRows), 256, 0, od.order_key, od.cust_key, od.order_date, n_or,
                  p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, skey, sdate, cnt, call.status());
   GPUDB_LAUNCH(call, table_clear_kernel, grid(max_cap), 256, 0, (const uint32_t*)cnt, 2048u, max_cap, cap,
                (Q3Slot*)ht, (uint32_t*)hits);
-  GPUDB_LAUNCH(call, orders_insert_kernel, grid(n_or), 256, 0, (const int32_t*)skey, (const int32_t*)sdate,
-               (const uint32_t*)cnt, (const uint32_t*)cap, (Q3Slot*)ht, call.status());
+  GPUDB_LAUNCH(call, orders_insert_kernel, grid(n_or / 4), 256, 0, (const int32_t*)skey, (const int32_t*)sdate,
+               (const uint32_t*)cnt, (const uint32_t*)cap, (Q3Slot*)ht, (uint32_t*)okbm, od.key_max, cnt + 2,
+               call.status());
   const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
   rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
     if (c.n_rows == 0) return (int)GPUDB_OK;
-    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows + 255) / 256, (uint64_t)sms * 8));
+    const unsigned g = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((c.n_rows + 256 * kProbeBatches - 1) / (256 * kProbeBatches), (uint64_t)sms * 8));
     GPUDB_LAUNCH(call, q3_probe_kernel, g, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount, c.n_rows,
-                 p.ship_date_gt, (Q3Slot*)ht, (uint32_t*)hits, (const uint32_t*)cap);
+                 p.ship_date_gt, (Q3Slot*)ht, (uint32_t*)hits, (const uint32_t*)cap, (const uint32_t*)okbm, od.key_max,
+                 (const uint32_t*)(cnt + 2));
     return (int)GPUDB_OK;
   });
   if (rc) return rc;
@@ -394,13 +484,8 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
   u128* rows = reinterpret_cast<u128*>(result + 16);
   GPUDB_LAUNCH(call, q3_topk_slots_kernel, (unsigned)tiles, kTopkThreads, 0, (const Q3Slot*)ht, (const uint32_t*)hits,
-               (const uint32_t*)cap, p.k, cbuf, groups);
-  if (tiles == 1) {
-    GPUDB_CUDA(ctx, cudaMemcpyAsync(rows, cbuf, (size_t)p.k * sizeof(u128), cudaMemcpyDeviceToDevice, s));
-    return GPUDB_OK;
-  }
-  return q3_topk_levels(call, cbuf, tiles * (uint64_t)p.k, p.k, cbuf + cand_elems, cbuf + cand_elems + cand_elems / 2 + 32,
-                        rows);
+               (const uint32_t*)cap, p.k, cbuf, groups, (unsigned*)(cnt + 3), rows);
+  return GPUDB_OK;
 }
 
 }  // namespace gpudb

@@ -139,59 +139,103 @@ struct Q9Maps {
   const uint8_t* year; int32_t order_max;
 };
 
-__global__ void __launch_bounds__(256) q9_probe_kernel(const int32_t* __restrict__ part, const int32_t* __restrict__ supp,
+constexpr int kQ9Threads = 256;
+constexpr int kQ9Warps = kQ9Threads / 32;
+
+// Fact rows that passed the part bitmap wait in a per-warp queue until 32 are there; then
+// every lane resolves one of them (supplier -> nation, (part, supp) -> cost, order -> year,
+// the row's measures), so the dependent lookups of 32 rows are in flight together instead
+// of a few lanes at a time. Groups are aggregated in a shared table that spills to the
+// global table.
+__global__ void __launch_bounds__(kQ9Threads) q9_probe_kernel(const int32_t* __restrict__ part, const int32_t* __restrict__ supp,
                                                        const int32_t* __restrict__ order, const int64_t* __restrict__ ext,
                                                        const int32_t* __restrict__ disc, const int32_t* __restrict__ qty,
                                                        uint64_t n, Q9Maps m, uint32_t* gkeys, unsigned long long* gvals,
                                                        uint32_t gcap, uint32_t scap, uint32_t* status) {
   extern __shared__ unsigned long long q9_smem[];
+  __shared__ uint64_t qrow[kQ9Warps][64];
+  __shared__ int32_t qpart[kQ9Warps][64];
   unsigned long long* svals = q9_smem;
   uint32_t* skeys = reinterpret_cast<uint32_t*>(svals + scap);
   for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x) { skeys[i] = kGroupEmpty; svals[i] = 0; }
   __syncthreads();
   const uint32_t ps_cap = *m.ps_cap, smask = scap - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t bad = 0;
-  auto row = [&](uint64_t r, int32_t p) {
-    if (p < 0 || p > m.part_max || !bitmap_test(m.part_bits, p)) return;
-    const int32_t s = supp[r];
-    if (s < 0 || s > m.supp_max) return;
-    const uint8_t nat = __ldg(m.nation + s);
-    if (nat == kNoValue) return;
-    long long cost;
-    if (!ps_find(m.ps, ps_cap, ps_key(p, s), &cost)) return;
-    const int32_t o = order[r];
-    if (o < 0 || o > m.order_max) return;
-    const uint8_t yoff = __ldg(m.year + o);
-    if (yoff == kNoValue) return;
-    const int64_t e = ext[r];
-    const int32_t d = disc[r], q = qty[r];
-    bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
-    const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
-    const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
-    uint32_t h = slot_hash64(key) & smask;
-    for (uint32_t t = 0; t < scap; t++, h = (h + 1) & smask) {
-      const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
-      if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); return; }
+  // resolves queue entries [0, cnt) of this warp, one per lane
+  auto resolve = [&](int cnt) {
+    if (lane < cnt) {
+      const uint64_t r = qrow[warp][lane];
+      const int32_t p = qpart[warp][lane];
+      const int32_t s = supp[r], o = order[r];
+      const int64_t e = ext[r];
+      const int32_t d = disc[r], q = qty[r];
+      const bool s_ok = s >= 0 && s <= m.supp_max, o_ok = o >= 0 && o <= m.order_max;
+      const uint8_t nat = s_ok ? __ldg(m.nation + s) : kNoValue;
+      const uint8_t yoff = o_ok ? __ldg(m.year + o) : kNoValue;
+      long long cost = 0;
+      const bool found = s_ok && ps_find(m.ps, ps_cap, ps_key(p, s), &cost);
+      if (found && nat != kNoValue && yoff != kNoValue) {
+        bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
+        const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
+        const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
+        uint32_t h = slot_hash64(key) & smask;
+        bool done = false;
+        for (uint32_t t = 0; t < scap && !done; t++, h = (h + 1) & smask) {
+          const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
+          if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); done = true; }
+        }
+        if (!done) global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
+      }
     }
-    global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
+    __syncwarp();
   };
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int queued = 0;   // warp-uniform
+  auto offer = [&](bool take, uint64_t r, int32_t p) {
+    const uint32_t bal = __ballot_sync(FULL_MASK, take);
+    if (take) {
+      const int at = queued + __popc(bal & lanemask_lt());
+      qrow[warp][at] = r;
+      qpart[warp][at] = p;
+    }
+    queued += __popc(bal);
+    __syncwarp();
+    if (queued >= 32) {
+      resolve(32);
+      if (lane < queued - 32) { qrow[warp][lane] = qrow[warp][lane + 32]; qpart[warp][lane] = qpart[warp][lane + 32]; }
+      queued -= 32;
+      __syncwarp();
+    }
+  };
+  auto passes = [&](int32_t p) { return p >= 0 && p <= m.part_max && bitmap_test(m.part_bits, p); };
+  const uint64_t warps = (uint64_t)gridDim.x * kQ9Warps;
+  const uint64_t gwarp = (uint64_t)blockIdx.x * kQ9Warps + warp;
   if ((reinterpret_cast<uintptr_t>(part) & 15u) == 0) {
     const uint64_t nq = n >> 2;
     const int4* p4 = reinterpret_cast<const int4*>(part);
-    for (uint64_t q = tid; q < nq; q += stride) {
-      const int4 v = ld_stream(p4 + q);
-      row(4 * q + 0, v.x);
-      row(4 * q + 1, v.y);
-      row(4 * q + 2, v.z);
-      row(4 * q + 3, v.w);
+    for (uint64_t qb = gwarp * 32; qb < nq; qb += warps * 32) {   // warp-uniform trip count
+      const uint64_t q = qb + lane;
+      int4 v = make_int4(-1, -1, -1, -1);
+      if (q < nq) v = ld_stream(p4 + q);
+      const bool t0 = passes(v.x), t1 = passes(v.y), t2 = passes(v.z), t3 = passes(v.w);
+      offer(t0, 4 * q + 0, v.x);
+      offer(t1, 4 * q + 1, v.y);
+      offer(t2, 4 * q + 2, v.z);
+      offer(t3, 4 * q + 3, v.w);
     }
-    const uint64_t r = (nq << 2) + tid;
-    if (r < n) row(r, part[r]);
+    if (gwarp == 0) {   // the last n % 4 rows
+      const uint64_t r = (nq << 2) + lane;
+      const int32_t p = r < n ? part[r] : -1;
+      offer(r < n && passes(p), r, p);
+    }
   } else {
-    for (uint64_t r = tid; r < n; r += stride) row(r, part[r]);
+    for (uint64_t rb = gwarp * 32; rb < n; rb += warps * 32) {
+      const uint64_t r = rb + lane;
+      const int32_t p = r < n ? part[r] : -1;
+      offer(r < n && passes(p), r, p);
+    }
   }
+  resolve(queued);
   if (__syncthreads_or(bad) && threadIdx.x == 0) set_status(status, ST_DOMAIN);
   for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x)
     if (skeys[i] != kGroupEmpty) global_group_add(gkeys, gvals, gcap, skeys[i], svals[i], status);
@@ -331,7 +375,7 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   rc = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
     if (c.n_rows == 0) return (int)GPUDB_OK;
     const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows / 4 + 255) / 256, (uint64_t)sms * 8));
-    GPUDB_LAUNCH(call, q9_probe_kernel, g, 256, probe_smem, c.part_key, c.supp_key, c.order_key, c.ext_price, c.discount,
+    GPUDB_LAUNCH(call, q9_probe_kernel, g, kQ9Threads, probe_smem, c.part_key, c.supp_key, c.order_key, c.ext_price, c.discount,
                  c.quantity, c.n_rows, maps, gkeys, gvals, gcap, scap, call.status());
     return (int)GPUDB_OK;
   });

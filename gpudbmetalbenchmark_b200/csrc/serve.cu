@@ -66,6 +66,7 @@ struct gpudb_server {
   uint64_t next_ticket = 1;
   uint64_t admitted_bytes = 0;
   bool closing = false;
+  bool warming = false;
   gpudb_serve_stats stats{};
 
   void work(size_t lane) {
@@ -75,9 +76,11 @@ struct gpudb_server {
     for (;;) {
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return closing || (!queue.empty() && fits(tickets[queue.front()].footprint)); });
+        cv_work.wait(lk, [&] {
+          return closing || (!warming && !queue.empty() && fits(tickets[queue.front()].footprint));
+        });
         if (queue.empty() && closing) return;
-        if (queue.empty() || !fits(tickets[queue.front()].footprint)) continue;
+        if (warming || queue.empty() || !fits(tickets[queue.front()].footprint)) continue;
         ids.clear();
         uint64_t bytes = 0;
         while (!queue.empty() && ids.size() < cfg.max_batch) {
@@ -136,6 +139,33 @@ extern "C" int gpudb_serve_open(const gpudb_serve_config* cfg, gpudb_server** ou
   }
   for (size_t i = 0; i < s->lanes.size(); i++) s->workers.emplace_back(&gpudb_server::work, s, i);
   *out = s;
+  return GPUDB_OK;
+}
+
+extern "C" int gpudb_serve_warmup(gpudb_server* s, gpudb_request* reqs, uint32_t n) {
+  if (!s || (n && !reqs)) return GPUDB_E_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (!s->queue.empty() || s->admitted_bytes) return GPUDB_E_BUSY;   // only before traffic
+  s->warming = true;   // workers leave their contexts alone meanwhile
+  lk.unlock();
+  std::vector<int> rcs(s->lanes.size(), GPUDB_OK);
+  std::vector<std::thread> th;
+  for (size_t i = 0; i < s->lanes.size(); i++)
+    th.emplace_back([&, i] {
+      std::vector<gpudb_request> copy(reqs, reqs + n);
+      rcs[i] = gpudb_batch_run(s->lanes[i], copy.data(), n, nullptr, nullptr);
+      for (uint32_t k = 0; k < n && rcs[i] == GPUDB_OK; k++)
+        if (copy[k].status != GPUDB_OK) rcs[i] = copy[k].status;
+      if (i == 0)
+        for (uint32_t k = 0; k < n; k++) { reqs[k].status = copy[k].status; reqs[k].q9_groups = copy[k].q9_groups; }
+    });
+  for (auto& t : th) t.join();
+  lk.lock();
+  s->warming = false;
+  lk.unlock();
+  s->cv_work.notify_all();
+  for (int rc : rcs)
+    if (rc != GPUDB_OK) return rc;
   return GPUDB_OK;
 }
 

@@ -368,6 +368,10 @@ int gpudb_serve_submit(gpudb_server* s, gpudb_request* req, uint64_t* ticket);
  * is still running) and its submit-to-completion latency in milliseconds. */
 int gpudb_serve_wait(gpudb_server* s, uint64_t ticket, double timeout_ms, double* latency_ms);
 int gpudb_serve_stats_get(gpudb_server* s, gpudb_serve_stats* out);
+/* Runs `reqs` once on every lane (lanes in parallel, each a synchronous batch) so that
+ * the lanes' scratch memory is sized before traffic arrives; results are written to the
+ * requests' outputs. Call it before submitting; it returns the first failing status. */
+int gpudb_serve_warmup(gpudb_server* s, gpudb_request* reqs, uint32_t n);
 /* Predicted device footprint of a request, in bytes (the admission estimate). */
 uint64_t gpudb_request_footprint(const gpudb_request* req);
 /* Stops accepting requests, finishes the queued ones, and frees the lanes. */

@@ -85,6 +85,48 @@ def test_many_scans_in_one_batch(engine, small):
         assert j.result() == solo[k]
 
 
+def test_shared_scan_q1_cutoffs_and_q6_mix(engine, orc):
+    """One shared pass: Q1 cutoffs that tie, select nothing and select everything, with
+    more than one pass's worth of Q6 and Q1 requests over the same rows."""
+    li = orc.lineitem(70_001, seed=21)
+    s = engine.upload("lineitem", li).lineitem()
+    cuts = [-1, 0, 1200, 1200, 2526, 2**31 - 1] + [100 * i for i in range(14)]
+    q6s = [(100 * i, 100 * i + 400, i % 11, min(10, i % 11 + 2), 10 + i) for i in range(20)]
+    reqs = (capi.Request * (len(cuts) + len(q6s)))()
+    o1 = [capi.Q1Result() for _ in cuts]
+    o6 = [capi.Q6Result() for _ in q6s]
+    for i, c in enumerate(cuts):
+        r = reqs[2 * i if i < len(q6s) else len(q6s) + i]
+        r.pipeline, r.li, r.q1, r.q1_out = capi.PIPE_Q1, C.pointer(s), capi.Q1Params(c, 0), C.pointer(o1[i])
+    taken = {2 * i if i < len(q6s) else len(q6s) + i for i in range(len(cuts))}
+    free = [k for k in range(len(reqs)) if k not in taken]
+    for i, p in enumerate(q6s):
+        r = reqs[free[i]]
+        r.pipeline, r.li, r.q6, r.q6_out = capi.PIPE_Q6, C.pointer(s), capi.Q6Params(*p), C.pointer(o6[i])
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, len(reqs), None, None))
+    assert all(r.status == capi.OK for r in reqs)
+    for c, o in zip(cuts, o1):
+        assert q1_to_dict(o) == orc.q1(li, c), c
+    for p, o in zip(q6s, o6):
+        assert (o.revenue, o.rows_matched) == orc.q6(li, *p), p
+
+
+def test_serve_warmup(engine, small):
+    jobs = small.jobs(40, seed=17)
+    solo = small.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()
+        j.req.q9_groups = 0
+    srv = Server(lanes=3, max_batch=16)
+    try:
+        srv.warmup(jobs)
+        assert [j.result() for j in jobs] == solo
+        lat, status, wall = open_loop(srv, small.jobs(100, seed=18), 5000.0, seed=3)
+    finally:
+        srv.close()
+    assert all(s == capi.OK for s in status)
+
+
 @pytest.mark.parametrize("lanes,max_batch,rate", [(1, 1, 3000.0), (4, 64, 20000.0), (2, 8, 50000.0)])
 def test_served_results_same_alone_and_in_the_mix(engine, small, lanes, max_batch, rate):
     jobs = small.jobs(1200, seed=int(rate))
