@@ -3,13 +3,14 @@
 // Shared scans. Q6/Q1 requests over device-resident tables are grouped by (table, row
 // range); each group is read from HBM once per pass, and every request of the group is
 // evaluated on the rows while they are in registers:
+//  - a quad of rows whose ship dates no request can accept skips its other columns;
 //  - Q6 requests (up to kMaxQ6 per pass) keep per-thread register sums;
 //  - Q1 requests (up to kMaxQ1 per pass) differ only in their ship_date cutoff, so the
 //    cutoffs are sorted and a row falls in bucket j = number of cutoffs below its ship
-//    date; it counts for every request whose sorted position is >= j. Rows are aggregated
-//    per (bucket, group) with shared-memory atomics, and each request's totals are the
-//    prefix sums over buckets 0..position. The per-row cost does not grow with the number
-//    of Q1 requests.
+//    date; it counts for every request whose sorted position is >= j. Each thread keeps
+//    private shared-memory sums per (bucket, flag, status) (no atomics; shared memory
+//    bounds the buckets of one pass), and each request's totals are the prefix sums over
+//    buckets 0..position.
 // All groups' row tiles form one work list; a persistent grid pulls tiles from a device
 // queue (one atomicAdd per tile), so a batch of many requests over several tables is one
 // launch. Partial sums reach the requests' result words through integer atomics (exact and
@@ -29,10 +30,12 @@ namespace {
 
 constexpr int kBT = 256;
 constexpr int kBW = kBT / 32;
-constexpr uint64_t kTileRows = 8192;      // per warp per tile <= 1024 rows: packed Q1 fields cannot carry
-constexpr int kMaxQ6 = 16;                // Q6 requests per pass (register sums)
-constexpr int kMaxQ1 = 15;                // Q1 requests per pass (16 buckets incl. padding)
-constexpr int kQ1Keys = (kMaxQ1 + 1) * 6; // (bucket, flag*2+status)
+constexpr uint64_t kTileRows = 8192;      // 32 rows per thread per tile
+constexpr int kFoldTiles = 16;            // per-thread Q1 sums fold into the block's every 16 tiles (<= 512
+                                          // rows): the packed count/discount fields and u64 sums cannot carry
+constexpr int kMaxQ6 = 8;                 // Q6 requests per Q6 pass (register sums)
+constexpr int kMaxQ6WithQ1 = 4;           // Q6 requests riding along a Q1 pass
+constexpr int kMaxQ1 = 2;                 // Q1 requests per pass (one bucket of per-thread sums each)
 constexpr int kQ6Words = 2;               // revenue, rows matched
 constexpr int kQ1Words = 72;              // 6 groups x 6 raw metrics x u128
 
@@ -42,9 +45,10 @@ struct ScanGroup {
   const uint8_t *flag, *stat;
   uint64_t begin, end;
   uint32_t n_q6, n_q1, vec, pad;
+  int32_t ship_lo, ship_hi;               // union of the Q6 ship ranges, [lo, hi)
   int32_t q6p[kMaxQ6][5];                 // ship_lo, ship_hi, disc_lo, disc_hi, qty_lt
   uint32_t q6_res[kMaxQ6];                // first result word
-  int32_t q1_cut[kMaxQ1 + 1];             // ascending; padded with INT32_MAX
+  int32_t q1_cut[kMaxQ1];                 // ascending
   uint32_t q1_res[kMaxQ1];                // in cutoff order
   uint32_t q1_idx[kMaxQ1];                // status word of the request
 };
@@ -53,11 +57,15 @@ struct ScanTile {
   uint64_t begin, end;
 };
 
+template <int NB>
 struct ScanSmem {
+  static constexpr int kKeys = NB > 0 ? NB * 6 : 1;   // (bucket, flag*2+status)
+  // per-thread Q1 sums, [metric][key][thread]: packed (qty<<32|disc<<13|1), ext, ext*disc,
+  // (ext*100-ext*disc)*tax
+  unsigned long long acc[NB > 0 ? 4 : 1][kKeys][NB > 0 ? kBT : 1];
+  u128 bacc[kKeys][6];                    // per block: count, qty, ext, ext*disc, ext*(100-disc)*tax, disc
   ScanGroup g;
-  unsigned long long wacc[kBW][kQ1Keys][4];   // per warp: packed (qty<<32|disc<<13|1), ext, ext*disc, (ext*100-ext*disc)*tax
-  u128 bacc[kQ1Keys][6];                      // per block: count, qty, ext, ext*disc, ext*(100-disc)*tax, disc
-  uint32_t bad[kMaxQ1 + 1];
+  uint32_t bad[NB > 0 ? NB : 1];
   unsigned long long red[kBW][2];
   uint32_t tile;
 };
@@ -70,13 +78,43 @@ __device__ __forceinline__ void atomic_add_u128(unsigned long long* p, u128 v) {
   if (hi) atomicAdd(p + 1, hi);
 }
 
+// Folds the per-thread Q1 sums into the block's u128 sums and clears them.
+template <int NB>
+__device__ void fold_q1(ScanSmem<NB>& S, uint32_t nq1) {
+  __syncthreads();
+  const uint32_t keys = nq1 * 6;
+  for (uint32_t k = threadIdx.x; k < keys * 4; k += kBT) {
+    const uint32_t key = k / 4, m = k % 4;
+    const unsigned long long* row = S.acc[m][key];
+    if (m == 0) {
+      u128 c = 0, qs = 0, ds = 0;
+      for (int t = 0; t < kBT; t++) {
+        const unsigned long long P = row[t];
+        c += P & 0x1FFFu;
+        ds += (P >> 13) & 0x7FFFFu;
+        qs += P >> 32;
+      }
+      S.bacc[key][0] += c; S.bacc[key][1] += qs; S.bacc[key][5] += ds;
+    } else {
+      u128 v = 0;
+      for (int t = 0; t < kBT; t++) v += row[t];
+      S.bacc[key][1 + m] += v;   // ext -> 2, ext*disc -> 3, charge -> 4
+    }
+  }
+  __syncthreads();
+  for (uint32_t m = 0; m < 4; m++)
+    for (uint32_t key = 0; key < keys; key++) S.acc[m][key][threadIdx.x] = 0;
+}
+
 // Adds the block's sums for the current group to the requests' result words.
-__device__ void flush_group(ScanSmem& S, const int64_t (&rev)[kMaxQ6], const uint32_t (&cnt)[kMaxQ6],
+template <int NB, int Q6>
+__device__ void flush_group(ScanSmem<NB>& S, const int64_t (&rev)[Q6], const uint32_t (&cnt)[Q6],
                             unsigned long long* res, uint32_t* req_status) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const ScanGroup& g = S.g;
+  if (NB > 0 && g.n_q1) fold_q1<NB>(S, g.n_q1);
 #pragma unroll
-  for (int r = 0; r < kMaxQ6; r++) {
+  for (int r = 0; r < Q6; r++) {
     if (r >= (int)g.n_q6) break;
     const unsigned long long a = warp_sum_u64((unsigned long long)rev[r]), b = warp_sum_u64(cnt[r]);
     if (lane == 0) { S.red[warp][0] = a; S.red[warp][1] = b; }
@@ -88,7 +126,9 @@ __device__ void flush_group(ScanSmem& S, const int64_t (&rev)[kMaxQ6], const uin
     }
     __syncthreads();
   }
-  // Q1: request at sorted position p = prefix over buckets 0..p
+  if (NB == 0) return;
+  // Q1: bucket j holds the rows whose ship date is above cutoffs 0..j-1 and at most cutoff j,
+  // so the request at sorted position p takes buckets 0..p
   for (uint32_t i = t; i < g.n_q1 * 36; i += kBT) {
     const uint32_t p = i / 36, gm = i % 36, grp = gm / 6, m = gm % 6;
     u128 v = 0;
@@ -103,151 +143,196 @@ __device__ void flush_group(ScanSmem& S, const int64_t (&rev)[kMaxQ6], const uin
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBT) scan_batch_kernel(const ScanGroup* __restrict__ groups,
-                                                         const ScanTile* __restrict__ tiles, uint32_t n_tiles,
-                                                         unsigned* queue, unsigned long long* res, uint32_t* req_status) {
+// One quad (4 consecutive rows) of the columns a pass needs.
+struct Quad {
+  int32_t sh[4], ds[4], qt[4], tx[4];
+  int64_t ex[4];
+  uint32_t fl, st;   // 4 packed bytes; 0xFF = no row
+  bool ok[4];
+  bool need;         // some row may pass some request
+};
+
+__device__ __forceinline__ bool full_quad(bool vec, uint64_t q, uint64_t b, uint64_t e) {
+  return vec && (q << 2) >= b && (q << 2) + 4 <= e;
+}
+
+// Ship dates of quad q (rows 4q..4q+3 within [b, e)), and whether some row can pass a
+// Q6 request of the group (only then are the other columns of a Q6 pass loaded).
+__device__ __forceinline__ void load_ship(const ScanGroup& g, uint64_t q, uint64_t b, uint64_t e, bool vec, Quad& d) {
+  if (full_quad(vec, q, b, e)) {
+    const int4 a = ld_stream(reinterpret_cast<const int4*>(g.ship) + q);
+    d.sh[0] = a.x; d.sh[1] = a.y; d.sh[2] = a.z; d.sh[3] = a.w;
+#pragma unroll
+    for (int k = 0; k < 4; k++) d.ok[k] = true;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint64_t r = (q << 2) + k;
+      d.ok[k] = r >= b && r < e;
+      d.sh[k] = d.ok[k] ? g.ship[r] : 0;
+    }
+  }
+  bool need = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) need |= d.ok[k] & (d.sh[k] >= g.ship_lo) & (d.sh[k] < g.ship_hi);
+  d.need = need;
+}
+
+// The other columns of quad q (Q1 columns when Q1).
+template <bool Q1>
+__device__ __forceinline__ void load_rest(const ScanGroup& g, uint64_t q, bool vec, Quad& d) {
+  if (vec && d.ok[0] && d.ok[3]) {
+    const int4 dd = ld_stream(reinterpret_cast<const int4*>(g.disc) + q);
+    const int4 b = ld_stream(reinterpret_cast<const int4*>(g.qty) + q);
+    const longlong2 e0 = ld_stream(reinterpret_cast<const longlong2*>(g.ext) + 2 * q);
+    const longlong2 e1 = ld_stream(reinterpret_cast<const longlong2*>(g.ext) + 2 * q + 1);
+    d.ds[0] = dd.x; d.ds[1] = dd.y; d.ds[2] = dd.z; d.ds[3] = dd.w;
+    d.qt[0] = b.x; d.qt[1] = b.y; d.qt[2] = b.z; d.qt[3] = b.w;
+    d.ex[0] = e0.x; d.ex[1] = e0.y; d.ex[2] = e1.x; d.ex[3] = e1.y;
+    if (Q1) {
+      const int4 x = ld_stream(reinterpret_cast<const int4*>(g.tax) + q);
+      d.tx[0] = x.x; d.tx[1] = x.y; d.tx[2] = x.z; d.tx[3] = x.w;
+      d.fl = ld_stream(reinterpret_cast<const uint32_t*>(g.flag) + q);
+      d.st = ld_stream(reinterpret_cast<const uint32_t*>(g.stat) + q);
+    }
+  } else {
+    d.fl = 0;
+    d.st = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint64_t r = (q << 2) + k;
+      const bool ok = d.ok[k];
+      d.ds[k] = ok ? g.disc[r] : 0;
+      d.qt[k] = ok ? g.qty[r] : 0;
+      d.ex[k] = ok ? g.ext[r] : 0;
+      if (Q1) {
+        d.tx[k] = ok ? g.tax[r] : 0;
+        d.fl |= (ok ? (uint32_t)g.flag[r] : 0xFFu) << (8 * k);
+        d.st |= (ok ? (uint32_t)g.stat[r] : 0xFFu) << (8 * k);
+      }
+    }
+  }
+}
+
+template <int NB, int Q6>
+__device__ __forceinline__ void eval_quad(ScanSmem<NB>& S, const Quad& d, int64_t (&rev)[Q6], uint32_t (&cnt)[Q6],
+                                          uint32_t nq6, uint32_t nq1) {
+#pragma unroll
+  for (int r = 0; r < Q6; r++) {
+    if (r >= (int)nq6) break;
+    const int32_t lo = S.g.q6p[r][0], hi = S.g.q6p[r][1], dlo = S.g.q6p[r][2], dhi = S.g.q6p[r][3], qlt = S.g.q6p[r][4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const bool m = d.ok[k] & (d.sh[k] >= lo) & (d.sh[k] < hi) & (d.ds[k] >= dlo) & (d.ds[k] <= dhi) & (d.qt[k] < qlt);
+      rev[r] += m ? d.ex[k] * (int64_t)d.ds[k] : 0;
+      cnt[r] += m;
+    }
+  }
+  if (NB == 0) return;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t f = (d.fl >> (8 * k)) & 0xFFu, s = (d.st >> (8 * k)) & 0xFFu;
+    uint32_t j = 0;   // bucket = number of cutoffs below the ship date
+#pragma unroll
+    for (int c = 0; c < (NB > 0 ? NB : 1); c++) j += (uint32_t)(c < (int)nq1) & (uint32_t)(S.g.q1_cut[c] < d.sh[k]);
+    if (!d.ok[k] || f > 2u || s > 1u || j >= nq1) continue;
+    const int32_t qv = d.qt[k], dv = d.ds[k], tv = d.tx[k];
+    const int64_t e = d.ex[k];
+    const uint32_t viol = ((uint32_t)qv >= 65536u) | ((uint32_t)dv > 100u) | ((uint32_t)tv > 100u) |
+                          ((uint64_t)e >= (1ull << 36));
+    if (viol) { atomicOr(&S.bad[j], 1u); continue; }
+    const uint64_t ed = (uint64_t)e * (uint32_t)dv;
+    const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)tv;
+    const uint32_t key = j * 6 + f * 2 + s;
+    S.acc[0][key][t] += ((uint64_t)(uint32_t)qv << 32) | ((uint64_t)(uint32_t)dv << 13) | 1u;
+    S.acc[1][key][t] += (uint64_t)e;
+    S.acc[2][key][t] += ed;
+    S.acc[3][key][t] += edt;
+  }
+}
+
+// Persistent pass over the tiles of a set of groups. NB = 0: Q6 groups (ship dates first,
+// the other columns only where a request's date range can match); NB > 0: groups with up
+// to NB Q1 requests (and Q6 requests riding along), every column loaded at once.
+template <int NB, int Q6>
+__global__ void __launch_bounds__(kBT) scan_pass_kernel(const ScanGroup* __restrict__ groups,
+                                                        const ScanTile* __restrict__ tiles, uint32_t n_tiles,
+                                                        unsigned* queue, unsigned long long* res, uint32_t* req_status) {
   extern __shared__ __align__(16) unsigned char scan_smem[];
-  ScanSmem& S = *reinterpret_cast<ScanSmem*>(scan_smem);
-  const int t = threadIdx.x, warp = t >> 5;
-  int64_t rev[kMaxQ6];
-  uint32_t cnt[kMaxQ6];
+  ScanSmem<NB>& S = *reinterpret_cast<ScanSmem<NB>*>(scan_smem);
+  const int t = threadIdx.x;
+  int64_t rev[Q6];
+  uint32_t cnt[Q6];
   uint32_t cur = 0xFFFFFFFFu;
+  int since_fold = 0;
   for (;;) {
     if (t == 0) S.tile = atomicAdd(queue, 1u);
     __syncthreads();
     const uint32_t i = S.tile;
     const uint32_t gi = i < n_tiles ? tiles[i].group : 0xFFFFFFFFu;
     if (gi != cur) {   // block-uniform
-      if (cur != 0xFFFFFFFFu) flush_group(S, rev, cnt, res, req_status);
+      if (cur != 0xFFFFFFFFu) flush_group<NB, Q6>(S, rev, cnt, res, req_status);
       if (i >= n_tiles) break;
       for (uint32_t w = t; w < sizeof(ScanGroup) / 4; w += kBT)
         reinterpret_cast<uint32_t*>(&S.g)[w] = reinterpret_cast<const uint32_t*>(groups + gi)[w];
-      for (uint32_t w = t; w < kQ1Keys * 6; w += kBT) (&S.bacc[0][0])[w] = 0;
-      if (t <= kMaxQ1) S.bad[t] = 0;
+      if (NB > 0) {
+        for (uint32_t w = t; w < ScanSmem<NB>::kKeys * 6; w += kBT) (&S.bacc[0][0])[w] = 0;
+        if (t < NB) S.bad[t] = 0;
+        for (int m = 0; m < 4; m++)
+          for (int key = 0; key < ScanSmem<NB>::kKeys; key++) S.acc[m][key][t] = 0;
+      }
 #pragma unroll
-      for (int r = 0; r < kMaxQ6; r++) { rev[r] = 0; cnt[r] = 0; }
+      for (int r = 0; r < Q6; r++) { rev[r] = 0; cnt[r] = 0; }
       cur = gi;
+      since_fold = 0;
       __syncthreads();   // the descriptor and cleared sums are visible to every thread
     }
     if (i >= n_tiles) break;   // a block that never got a tile
     const uint32_t nq6 = S.g.n_q6, nq1 = S.g.n_q1;
-    if (nq1)
-      for (uint32_t w = t; w < (uint32_t)kBW * (nq1 * 6) * 4; w += kBT) {
-        const uint32_t wp = w / ((nq1 * 6) * 4), rest = w % ((nq1 * 6) * 4);
-        S.wacc[wp][rest / 4][rest % 4] = 0;
-      }
-    __syncthreads();
+    if (NB > 0) {
+      if (since_fold == kFoldTiles) { fold_q1<NB>(S, nq1); since_fold = 0; }
+      since_fold++;
+    }
     const ScanTile T = tiles[i];
     const bool vec = S.g.vec != 0;
-    uint32_t bad = 0;
-    for (uint64_t q = (T.begin >> 2) + t; q < ((T.end + 3) >> 2); q += kBT) {
-      const uint64_t r0 = q << 2;
-      int32_t sh[4], ds[4], qt[4], tx[4] = {0, 0, 0, 0};
-      int64_t ex[4];
-      uint32_t fl = 0xFFFFFFFFu, st = 0xFFFFFFFFu;
-      bool ok[4];
-      if (vec && r0 >= T.begin && r0 + 4 <= T.end) {
-        const int4 a = ld_stream(reinterpret_cast<const int4*>(S.g.ship) + q);
-        const int4 d = ld_stream(reinterpret_cast<const int4*>(S.g.disc) + q);
-        const int4 b = ld_stream(reinterpret_cast<const int4*>(S.g.qty) + q);
-        const longlong2 e0 = ld_stream(reinterpret_cast<const longlong2*>(S.g.ext) + 2 * q);
-        const longlong2 e1 = ld_stream(reinterpret_cast<const longlong2*>(S.g.ext) + 2 * q + 1);
-        sh[0] = a.x; sh[1] = a.y; sh[2] = a.z; sh[3] = a.w;
-        ds[0] = d.x; ds[1] = d.y; ds[2] = d.z; ds[3] = d.w;
-        qt[0] = b.x; qt[1] = b.y; qt[2] = b.z; qt[3] = b.w;
-        ex[0] = e0.x; ex[1] = e0.y; ex[2] = e1.x; ex[3] = e1.y;
-        if (nq1) {
-          const int4 x = ld_stream(reinterpret_cast<const int4*>(S.g.tax) + q);
-          tx[0] = x.x; tx[1] = x.y; tx[2] = x.z; tx[3] = x.w;
-          fl = ld_stream(reinterpret_cast<const uint32_t*>(S.g.flag) + q);
-          st = ld_stream(reinterpret_cast<const uint32_t*>(S.g.stat) + q);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) ok[k] = true;
-      } else {
-        fl = 0; st = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const uint64_t r = r0 + k;
-          ok[k] = r >= T.begin && r < T.end;
-          sh[k] = ok[k] ? S.g.ship[r] : 0;
-          ds[k] = ok[k] ? S.g.disc[r] : 0;
-          qt[k] = ok[k] ? S.g.qty[r] : 0;
-          ex[k] = ok[k] ? S.g.ext[r] : 0;
-          if (nq1) {
-            tx[k] = ok[k] ? S.g.tax[r] : 0;
-            fl |= (ok[k] ? (uint32_t)S.g.flag[r] : 0xFFu) << (8 * k);
-            st |= (ok[k] ? (uint32_t)S.g.stat[r] : 0xFFu) << (8 * k);
-          }
-        }
+    const uint64_t q_end = (T.end + 3) >> 2;
+    for (uint64_t q = (T.begin >> 2) + t; q < q_end; q += 2 * kBT) {   // two quads in flight per thread
+      Quad a, b;
+      const bool has_b = q + kBT < q_end;
+      load_ship(S.g, q, T.begin, T.end, vec, a);
+      if (has_b) load_ship(S.g, q + kBT, T.begin, T.end, vec, b);
+      if (NB > 0) {
+        a.need = true;
+        b.need = has_b;
+      } else if (!has_b) {
+        b.need = false;
       }
-#pragma unroll
-      for (int r = 0; r < kMaxQ6; r++) {
-        if (r >= (int)nq6) break;
-        const int32_t lo = S.g.q6p[r][0], hi = S.g.q6p[r][1], dlo = S.g.q6p[r][2], dhi = S.g.q6p[r][3], qlt = S.g.q6p[r][4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const bool m = ok[k] & (sh[k] >= lo) & (sh[k] < hi) & (ds[k] >= dlo) & (ds[k] <= dhi) & (qt[k] < qlt);
-          rev[r] += m ? ex[k] * (int64_t)ds[k] : 0;
-          cnt[r] += m;
-        }
-      }
-      if (nq1) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const uint32_t f = (fl >> (8 * k)) & 0xFFu, s = (st >> (8 * k)) & 0xFFu;
-          if (!ok[k] || f > 2u || s > 1u) continue;
-          // bucket = number of cutoffs below the ship date (cutoffs padded with INT32_MAX)
-          uint32_t j = 0;
-#pragma unroll
-          for (uint32_t step = 8; step > 0; step >>= 1)
-            if (S.g.q1_cut[j + step - 1] < sh[k]) j += step;
-          if (j >= nq1) continue;
-          const int32_t qv = qt[k], dv = ds[k], tv = tx[k];
-          const int64_t e = ex[k];
-          const uint32_t viol = ((uint32_t)qv >= 65536u) | ((uint32_t)dv > 100u) | ((uint32_t)tv > 100u) |
-                                ((uint64_t)e >= (1ull << 36));
-          if (viol) { atomicOr(&S.bad[j], 1u); continue; }
-          const uint64_t ed = (uint64_t)e * (uint32_t)dv;
-          const uint64_t edt = ((uint64_t)e * 100u - ed) * (uint32_t)tv;
-          unsigned long long* a = S.wacc[warp][j * 6 + f * 2 + s];
-          atomicAdd(a + 0, ((uint64_t)(uint32_t)qv << 32) | ((uint64_t)(uint32_t)dv << 13) | 1u);
-          atomicAdd(a + 1, (unsigned long long)e);
-          atomicAdd(a + 2, (unsigned long long)ed);
-          atomicAdd(a + 3, (unsigned long long)edt);
-        }
-      }
+      if (a.need) load_rest<(NB > 0)>(S.g, q, vec, a);
+      if (b.need) load_rest<(NB > 0)>(S.g, q + kBT, vec, b);
+      if (a.need) eval_quad<NB, Q6>(S, a, rev, cnt, nq6, nq1);
+      if (b.need) eval_quad<NB, Q6>(S, b, rev, cnt, nq6, nq1);
     }
-    (void)bad;
     __syncthreads();
-    if (nq1) {   // fold the warps' tile sums into the block's u128 sums
-      for (uint32_t k = t; k < nq1 * 6; k += kBT) {
-        u128 c = 0, qs = 0, ds = 0, e = 0, ed = 0, edt = 0;
-        for (int w = 0; w < kBW; w++) {
-          const unsigned long long P = S.wacc[w][k][0];
-          c += P & 0x1FFFu;
-          ds += (P >> 13) & 0x7FFFFu;
-          qs += P >> 32;
-          e += S.wacc[w][k][1];
-          ed += S.wacc[w][k][2];
-          edt += S.wacc[w][k][3];
-        }
-        S.bacc[k][0] += c; S.bacc[k][1] += qs; S.bacc[k][2] += e;
-        S.bacc[k][3] += ed; S.bacc[k][4] += edt; S.bacc[k][5] += ds;
-      }
-      __syncthreads();
-    }
   }
 }
 
-size_t scan_smem_bytes() { return (sizeof(ScanSmem) + 15) / 16 * 16; }
+template <int NB, int Q6>
+size_t pass_smem() { return (sizeof(ScanSmem<NB>) + 15) / 16 * 16; }
 
-unsigned scan_grid(gpudb_ctx* ctx, uint32_t tiles) {
+template <int NB, int Q6>
+int launch_pass(gpudb_ctx* ctx, Call& call, const ScanGroup* dgrp, const std::vector<ScanTile>& tiles, ScanTile* dtile,
+                unsigned* queue, unsigned long long* res, uint32_t* status) {
+  if (tiles.empty()) return GPUDB_OK;
+  auto kern = scan_pass_kernel<NB, Q6>;
+  const size_t smem = pass_smem<NB, Q6>();
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_batch_kernel, kBT, scan_smem_bytes()) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  return std::max<unsigned>(1, std::min<unsigned>(tiles, (unsigned)(ctx->sm_count * per_sm)));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  const unsigned grid = std::max<unsigned>(1, std::min<unsigned>((unsigned)tiles.size(), (unsigned)(ctx->sm_count * per_sm)));
+  GPUDB_CUDA(ctx, cudaMemcpyAsync(dtile, tiles.data(), tiles.size() * sizeof(ScanTile), cudaMemcpyHostToDevice, call.stream()));
+  GPUDB_LAUNCH(call, kern, grid, kBT, smem, dgrp, (const ScanTile*)dtile, (uint32_t)tiles.size(), queue, res, status);
+  return GPUDB_OK;
 }
 
 bool scan_columns_ok(const gpudb_request& r) {
@@ -258,6 +343,26 @@ bool scan_columns_ok(const gpudb_request& r) {
 }
 
 bool aligned(const void* p, uintptr_t a) { return !p || (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+// Q1 result from the raw words of one request: 6 groups x {count, qty, ext, ext*disc,
+// ext*(100-disc)*tax, disc} as u128.
+void q1_from_words(const uint8_t* w, gpudb_q1_result& o) {
+  std::memset(&o, 0, sizeof o);
+  for (int g = 0; g < 6; g++) {
+    u128 m[6];
+    std::memcpy(m, w + (size_t)g * 6 * 16, sizeof m);
+    if (m[0] == 0) continue;
+    const u128 disc_price = (u128)100 * m[2] - m[3];
+    const u128 charge = (u128)100 * disc_price + m[4];
+    gpudb_q1_group& G = o.groups[o.n_groups++];
+    G.flag = (uint8_t)(g / 2);
+    G.status = (uint8_t)(g % 2);
+    G.count = (uint64_t)m[0];
+    const u128 vals[5] = {m[1], m[2], disc_price, charge, m[5]};
+    gpudb_i128* f[5] = {&G.sum_qty, &G.sum_base_price, &G.sum_disc_price, &G.sum_charge, &G.sum_discount};
+    for (int j = 0; j < 5; j++) { f[j]->lo = (uint64_t)vals[j]; f[j]->hi = (int64_t)(uint64_t)(vals[j] >> 64); }
+  }
+}
 
 // Runs the scan requests `ids` of `reqs` as shared scans (fits one result slot).
 int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t>& ids, gpudb_timing* t,
@@ -285,7 +390,7 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
     words += q.pipeline == GPUDB_PIPE_Q6 ? kQ6Words : kQ1Words;
   }
   std::vector<ScanGroup> groups;
-  std::vector<ScanTile> tiles;
+  std::vector<ScanTile> tiles6, tiles1;   // Q6 passes, Q1 passes
   for (auto& kv : by_table) {
     Members& mb = kv.second;
     for (auto& c : mb.q1)
@@ -301,13 +406,8 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
       g.ext = static_cast<const int64_t*>(std::get<3>(kv.first));
       g.begin = std::get<4>(kv.first);
       g.end = std::get<5>(kv.first);
-      for (; i6 < mb.q6.size() && g.n_q6 < (uint32_t)kMaxQ6; i6++, g.n_q6++) {
-        const gpudb_q6_params& p = reqs[ids[mb.q6[i6]]].q6;
-        const int32_t v[5] = {p.ship_lo, p.ship_hi, p.disc_lo, p.disc_hi, p.qty_lt};
-        std::memcpy(g.q6p[g.n_q6], v, sizeof v);
-        g.q6_res[g.n_q6] = offs[mb.q6[i6]];
-      }
-      if (q1it != mb.q1.end()) {
+      const bool q1pass = q1it != mb.q1.end();
+      if (q1pass) {   // up to kMaxQ1 Q1 requests of one column set, Q6 requests riding along
         g.tax = static_cast<const int32_t*>(std::get<0>(q1it->first));
         g.flag = static_cast<const uint8_t*>(std::get<1>(q1it->first));
         g.stat = static_cast<const uint8_t*>(std::get<2>(q1it->first));
@@ -319,14 +419,27 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
         }
         if (i1 == l.size()) { ++q1it; i1 = 0; }
       }
-      for (uint32_t j = g.n_q1; j <= (uint32_t)kMaxQ1; j++) g.q1_cut[j] = INT32_MAX;
+      g.ship_lo = INT32_MAX;
+      g.ship_hi = INT32_MIN;
+      const uint32_t max6 = q1pass ? kMaxQ6WithQ1 : kMaxQ6;
+      for (; i6 < mb.q6.size() && g.n_q6 < max6; i6++, g.n_q6++) {
+        const gpudb_q6_params& p = reqs[ids[mb.q6[i6]]].q6;
+        if (p.ship_lo < p.ship_hi) {
+          g.ship_lo = std::min(g.ship_lo, p.ship_lo);
+          g.ship_hi = std::max(g.ship_hi, p.ship_hi);
+        }
+        const int32_t v[5] = {p.ship_lo, p.ship_hi, p.disc_lo, p.disc_hi, p.qty_lt};
+        std::memcpy(g.q6p[g.n_q6], v, sizeof v);
+        g.q6_res[g.n_q6] = offs[mb.q6[i6]];
+      }
       g.vec = aligned(g.ship, 16) && aligned(g.qty, 16) && aligned(g.disc, 16) && aligned(g.ext, 16) &&
               aligned(g.tax, 16) && aligned(g.flag, 4) && aligned(g.stat, 4);
       const uint32_t gi = (uint32_t)groups.size();
       groups.push_back(g);
+      std::vector<ScanTile>& tl = q1pass ? tiles1 : tiles6;
       for (uint64_t b = g.begin; b < g.end;) {
         const uint64_t e = std::min<uint64_t>(g.end, (b / kTileRows + 1) * kTileRows);
-        tiles.push_back(ScanTile{gi, 0, b, e});
+        tl.push_back(ScanTile{gi, 0, b, e});
         b = e;
       }
     }
@@ -337,25 +450,26 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
   int rc = call.begin(bytes);
   if (rc) return rc;
   uint8_t* dres = call.result<uint8_t>();
-  if (!tiles.empty()) {
+  if (!groups.empty()) {
     void* desc = nullptr;
-    const size_t qbytes = 256, gbytes = groups.size() * sizeof(ScanGroup), tbytes = tiles.size() * sizeof(ScanTile);
-    rc = scratch(ctx, "batch.desc", qbytes + gbytes + tbytes + 256, &desc);
+    const size_t qbytes = 256, gbytes = ((groups.size() * sizeof(ScanGroup) + 15) / 16) * 16;
+    const size_t t6 = ((tiles6.size() * sizeof(ScanTile) + 15) / 16) * 16, t1 = tiles1.size() * sizeof(ScanTile);
+    rc = scratch(ctx, "batch.desc", qbytes + gbytes + t6 + t1 + 256, &desc);
     if (rc) return rc;
     uint8_t* base = static_cast<uint8_t*>(desc);
-    unsigned* queue = reinterpret_cast<unsigned*>(base);
+    unsigned* queue = reinterpret_cast<unsigned*>(base);   // [0] Q6 passes, [1] Q1 passes
     ScanGroup* dgrp = reinterpret_cast<ScanGroup*>(base + qbytes);
-    ScanTile* dtile = reinterpret_cast<ScanTile*>(base + qbytes + ((gbytes + 15) / 16) * 16);
+    ScanTile* dt6 = reinterpret_cast<ScanTile*>(base + qbytes + gbytes);
+    ScanTile* dt1 = reinterpret_cast<ScanTile*>(base + qbytes + gbytes + t6);
     // pageable sources: the copies stage the descriptors before returning
-    GPUDB_CUDA(ctx, cudaMemsetAsync(queue, 0, 4, call.stream()));
-    GPUDB_CUDA(ctx, cudaMemcpyAsync(dgrp, groups.data(), gbytes, cudaMemcpyHostToDevice, call.stream()));
-    GPUDB_CUDA(ctx, cudaMemcpyAsync(dtile, tiles.data(), tbytes, cudaMemcpyHostToDevice, call.stream()));
-    const size_t smem = scan_smem_bytes();
-    GPUDB_CUDA(ctx, cudaFuncSetAttribute(scan_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const unsigned grid = scan_grid(ctx, (uint32_t)tiles.size());
-    GPUDB_LAUNCH(call, scan_batch_kernel, grid, kBT, smem, (const ScanGroup*)dgrp, (const ScanTile*)dtile,
-                 (uint32_t)tiles.size(), queue, reinterpret_cast<unsigned long long*>(dres + status_bytes),
-                 reinterpret_cast<uint32_t*>(dres));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(queue, 0, 8, call.stream()));
+    GPUDB_CUDA(ctx, cudaMemcpyAsync(dgrp, groups.data(), groups.size() * sizeof(ScanGroup), cudaMemcpyHostToDevice,
+                                    call.stream()));
+    unsigned long long* res = reinterpret_cast<unsigned long long*>(dres + status_bytes);
+    uint32_t* st = reinterpret_cast<uint32_t*>(dres);
+    rc = launch_pass<0, kMaxQ6>(ctx, call, dgrp, tiles6, dt6, queue, res, st);
+    if (!rc) rc = launch_pass<kMaxQ1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles1, dt1, queue + 1, res, st);
+    if (rc) return rc;
   }
   std::vector<uint32_t> ids_copy = ids;
   return call.finish(bytes, [reqs, ids_copy, offs, status_bytes, ctx](const uint8_t* h) {
@@ -367,39 +481,93 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
       const uint8_t* w = h + status_bytes + (size_t)offs[k] * 8;
       if (q.pipeline == GPUDB_PIPE_Q6) {
         if (q.q6_out) { std::memcpy(&q.q6_out->revenue, w, 8); std::memcpy(&q.q6_out->rows_matched, w + 8, 8); }
-        continue;
+      } else if (q.q1_out) {
+        q1_from_words(w, *q.q1_out);
       }
-      if (!q.q1_out) continue;
-      gpudb_q1_result& o = *q.q1_out;
-      std::memset(&o, 0, sizeof o);
-      for (int g = 0; g < 6; g++) {
-        u128 m[6];
-        std::memcpy(m, w + (size_t)g * 6 * 16, sizeof m);
-        if (m[0] == 0) continue;
-        const u128 disc_price = (u128)100 * m[2] - m[3];
-        const u128 charge = (u128)100 * disc_price + m[4];
-        gpudb_q1_group& G = o.groups[o.n_groups++];
-        G.flag = (uint8_t)(g / 2);
-        G.status = (uint8_t)(g % 2);
-        G.count = (uint64_t)m[0];
-        const u128 vals[5] = {m[1], m[2], disc_price, charge, m[5]};
-        gpudb_i128* f[5] = {&G.sum_qty, &G.sum_base_price, &G.sum_disc_price, &G.sum_charge, &G.sum_discount};
-        for (int j = 0; j < 5; j++) { f[j]->lo = (uint64_t)vals[j]; f[j]->hi = (int64_t)(uint64_t)(vals[j] >> 64); }
-      }
+      if (ctx->on_done) ctx->on_done(ctx->on_done_arg, &q.status);
     }
     return GPUDB_OK;
   });
 }
+
 
 }  // namespace
 }  // namespace gpudb
 
 using namespace gpudb;
 
+namespace {
+
+bool same_q3(const gpudb_request& a, const gpudb_request& b) {
+  return a.q3 && b.q3 && std::memcmp(a.q3, b.q3, sizeof *a.q3) == 0 &&
+         std::memcmp(&a.q3p, &b.q3p, sizeof a.q3p) == 0;
+}
+bool same_q9(const gpudb_request& a, const gpudb_request& b) {
+  return a.q9 && b.q9 && std::memcmp(a.q9, b.q9, sizeof *a.q9) == 0 &&
+         std::memcmp(&a.q9p, &b.q9p, sizeof a.q9p) == 0 && a.q9_capacity == b.q9_capacity;
+}
+
+// Completion hook of a synchronous batch: copies a coalesced request's result to its
+// duplicates, then passes every completion on to the previous hook.
+struct BatchHook {
+  void (*prev)(void*, int32_t*);
+  void* prev_arg;
+  gpudb_request* reqs;
+  uint32_t n;
+  std::vector<std::vector<uint32_t>> dups;   // per request: identical later requests
+
+  static void on_done(void* arg, int32_t* sink) {
+    BatchHook* h = static_cast<BatchHook*>(arg);
+    const uintptr_t base = reinterpret_cast<uintptr_t>(&h->reqs[0].status), at = reinterpret_cast<uintptr_t>(sink);
+    if (at >= base && (at - base) % sizeof(gpudb_request) == 0 && (at - base) / sizeof(gpudb_request) < h->n) {
+      const uint32_t i = (uint32_t)((at - base) / sizeof(gpudb_request));
+      const gpudb_request& o = h->reqs[i];
+      if (h->prev) h->prev(h->prev_arg, sink);
+      for (uint32_t d : h->dups[i]) {
+        gpudb_request& q = h->reqs[d];
+        q.status = o.status;
+        if (q.pipeline == GPUDB_PIPE_Q3) {
+          *q.q3_out = *o.q3_out;
+        } else {
+          q.q9_groups = o.q9_groups;
+          if (q.q9_capacity) std::memcpy(q.q9_out, o.q9_out, (size_t)std::min(o.q9_groups, q.q9_capacity) * sizeof(gpudb_q9_group));
+        }
+        if (h->prev) h->prev(h->prev_arg, &q.status);
+      }
+      return;
+    }
+    if (h->prev) h->prev(h->prev_arg, sink);
+  }
+};
+
+}  // namespace
+
 extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timing* t, const gpudb_exec* ex) {
   if (!ctx) return GPUDB_E_INVALID;
   if (n && !reqs) return fail(ctx, GPUDB_E_INVALID, "batch: requests are NULL");
+  const bool async = ex && ex->async;
   gpudb_exec aex{1, 0, ex ? ex->stream : nullptr};
+  // synchronous batches coalesce identical join requests: the first runs, the others copy
+  BatchHook hook{ctx->on_done, ctx->on_done_arg, reqs, n, {}};
+  std::vector<char> skip(n, 0);
+  if (!async) {
+    hook.dups.resize(n);
+    for (uint32_t i = 0; i < n; i++) {
+      const gpudb_request& q = reqs[i];
+      if (q.pipeline != GPUDB_PIPE_Q3 && q.pipeline != GPUDB_PIPE_Q9) continue;
+      if (q.pipeline == GPUDB_PIPE_Q3 ? !q.q3_out : (!q.q9_out && q.q9_capacity)) continue;
+      for (uint32_t j = 0; j < i; j++) {
+        if (skip[j] || reqs[j].pipeline != q.pipeline) continue;
+        if (q.pipeline == GPUDB_PIPE_Q3 ? (reqs[j].q3_out && same_q3(reqs[j], q)) : same_q9(reqs[j], q)) {
+          hook.dups[j].push_back(i);
+          skip[i] = 1;
+          break;
+        }
+      }
+    }
+    ctx->on_done = &BatchHook::on_done;
+    ctx->on_done_arg = &hook;
+  }
   std::vector<uint32_t> scans;
   size_t scan_bytes = 0;
   auto flush_scans = [&]() -> int {
@@ -413,6 +581,7 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
   for (uint32_t i = 0; i < n; i++) {
     gpudb_request& q = reqs[i];
     q.status = GPUDB_OK;
+    if (skip[i]) continue;
     int rc = GPUDB_OK;
     switch (q.pipeline) {
       case GPUDB_PIPE_Q6:
@@ -421,14 +590,14 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
           rc = fail(ctx, GPUDB_E_INVALID, "batch: request %u has no result struct", i);
           break;
         }
-        if (scan_columns_ok(q)) {
+        // a lone scan runs through its own pipeline (the plain form); several share passes
+        if (n > 1 && scan_columns_ok(q)) {
           const size_t b = (q.pipeline == GPUDB_PIPE_Q6 ? kQ6Words : kQ1Words) * 8 + 4;
           if (scan_bytes + b + 64 > kBigSlotBytes - kSlotHeader) flush_scans();
           scans.push_back(i);
           scan_bytes += b;
           break;
         }
-        // host-resident or incomplete columns: the single-request path reports or streams it
         gpudb_lineitem view = q.li ? *q.li : gpudb_lineitem{};
         if (q.li && (q.row_begin || q.row_end)) {
           const uint64_t end = q.row_end ? std::min<uint64_t>(q.row_end, view.n_rows) : view.n_rows;
@@ -462,10 +631,15 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
       default:
         rc = fail(ctx, GPUDB_E_INVALID, "batch: request %u has unknown pipeline %d", i, q.pipeline);
     }
-    if (rc != GPUDB_OK) q.status = rc;
+    if (rc != GPUDB_OK) {
+      q.status = rc;
+      for (uint32_t d : async ? std::vector<uint32_t>{} : hook.dups[i]) reqs[d].status = rc;
+    }
   }
   flush_scans();
-  if (ex && ex->async) return GPUDB_OK;
+  if (async) return GPUDB_OK;
   gpudb_sync(ctx);   // per-request outcomes are in each status
+  ctx->on_done = hook.prev;
+  ctx->on_done_arg = hook.prev_arg;
   return GPUDB_OK;
 }

@@ -172,7 +172,10 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
     std::memcpy(&st, hs, sizeof st);
     int rc = status_to_error(ctx, st);
     if (rc == GPUDB_OK) rc = convert(hs + kSlotHeader);
-    if (sink) *sink = rc;
+    if (sink) {
+      *sink = rc;
+      if (ctx->on_done) ctx->on_done(ctx->on_done_arg, sink);
+    }
     if (t) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = -1.f;
@@ -190,7 +193,9 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
   };
   handed_off_ = true;
   if (async_) {
-    ctx_->pending.push_back(done);
+    cudaEvent_t ev = event_get(ctx_);
+    GPUDB_CUDA(ctx_, cudaEventRecord(ev, s_));
+    ctx_->pending.push_back(gpudb_ctx::Pending{ev, done});
     if (std::find(ctx_->pending_streams.begin(), ctx_->pending_streams.end(), s_) == ctx_->pending_streams.end())
       ctx_->pending_streams.push_back(s_);
     return GPUDB_OK;
@@ -376,20 +381,24 @@ const char* gpudb_last_error_string(const gpudb_ctx* ctx) { return ctx ? ctx->er
 int gpudb_sync(gpudb_ctx* ctx) {
   if (!ctx) return GPUDB_E_INVALID;
   int rc = GPUDB_OK;
+  // finish the calls in issue order, each as soon as its own result has arrived
+  std::vector<gpudb_ctx::Pending> work;
+  work.swap(ctx->pending);
+  for (auto& w : work) {
+    cudaError_t e = cudaEventSynchronize(w.done);
+    if (e != cudaSuccess && rc == GPUDB_OK) rc = cuda_fail(ctx, e, "cudaEventSynchronize");
+    event_put(ctx, w.done);
+    const int r = w.finish();
+    if (r != GPUDB_OK && rc == GPUDB_OK) rc = r;
+  }
   for (cudaStream_t s : ctx->pending_streams) {
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess && rc == GPUDB_OK) rc = cuda_fail(ctx, e, "cudaStreamSynchronize");
   }
+  ctx->pending_streams.clear();
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess && rc == GPUDB_OK) rc = cuda_fail(ctx, e, "cudaStreamSynchronize");
-  std::vector<std::function<int()>> work;
-  work.swap(ctx->pending);
-  ctx->pending_streams.clear();
-  if (rc == GPUDB_OK) release_retired(ctx);
-  for (auto& f : work) {
-    int r = f();
-    if (r != GPUDB_OK && rc == GPUDB_OK) rc = r;
-  }
+  if (rc == GPUDB_OK && ctx->pending.empty()) release_retired(ctx);
   return rc;
 }
 

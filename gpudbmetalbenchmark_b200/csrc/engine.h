@@ -57,7 +57,14 @@ struct gpudb_ctx {
   uint8_t* h_big = nullptr;
   bool big_busy[gpudb::kBigSlots] = {};
   int32_t* status_sink = nullptr;      // batch: where the next call reports its final status
-  std::vector<std::function<int()>> pending;
+  // called after a call's final status is written to its status sink (batches, serving)
+  void (*on_done)(void* arg, int32_t* sink) = nullptr;
+  void* on_done_arg = nullptr;
+  struct Pending {
+    cudaEvent_t done;                  // recorded after the call's result copy
+    std::function<int()> finish;       // converts the result, writes the outputs
+  };
+  std::vector<Pending> pending;        // async calls in issue order
   std::vector<cudaStream_t> pending_streams;
   std::vector<cudaEvent_t> event_pool;
 };

@@ -69,10 +69,46 @@ struct gpudb_server {
   bool warming = false;
   gpudb_serve_stats stats{};
 
+  // Completion of request `i` of the lane's running batch (under no lock).
+  struct LaneRun {
+    gpudb_server* s;
+    std::vector<gpudb_request>* batch;
+    std::vector<uint64_t>* ids;
+    std::vector<char>* done;
+  };
+  static void on_done(void* arg, int32_t* sink) {
+    LaneRun* r = static_cast<LaneRun*>(arg);
+    const uintptr_t base = reinterpret_cast<uintptr_t>(&(*r->batch)[0].status), at = reinterpret_cast<uintptr_t>(sink);
+    if (at < base || (at - base) % sizeof(gpudb_request)) return;
+    const size_t i = (at - base) / sizeof(gpudb_request);
+    if (i >= r->batch->size() || (*r->done)[i]) return;
+    (*r->done)[i] = 1;
+    r->s->complete((*r->ids)[i], (*r->batch)[i]);
+  }
+
+  void complete(uint64_t id, const gpudb_request& q) {
+    const double t = now_ms();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      Ticket& tk = tickets[id];
+      tk.req->status = q.status;
+      tk.req->q9_groups = q.q9_groups;
+      tk.t_done = t;
+      tk.done = true;
+      admitted_bytes -= tk.footprint;
+      stats.completed++;
+      if (q.status != GPUDB_OK) stats.failed++;
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+  }
+
   void work(size_t lane) {
     gpudb_ctx* ctx = lanes[lane];
     std::vector<gpudb_request> batch;
     std::vector<uint64_t> ids;
+    std::vector<char> done;
+    LaneRun run{this, &batch, &ids, &done};
     for (;;) {
       {
         std::unique_lock<std::mutex> lk(mu);
@@ -97,23 +133,15 @@ struct gpudb_server {
         batch.clear();
         for (uint64_t id : ids) batch.push_back(*tickets[id].req);
       }
+      done.assign(batch.size(), 0);
+      // each request completes as soon as its own work has finished (hook), not at batch end
+      ctx->on_done = &gpudb_server::on_done;
+      ctx->on_done_arg = &run;
       gpudb_batch_run(ctx, batch.data(), (uint32_t)batch.size(), nullptr, nullptr);
-      const double t = now_ms();
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        for (size_t i = 0; i < ids.size(); i++) {
-          Ticket& tk = tickets[ids[i]];
-          tk.req->status = batch[i].status;
-          tk.req->q9_groups = batch[i].q9_groups;
-          tk.t_done = t;
-          tk.done = true;
-          admitted_bytes -= tk.footprint;
-          stats.completed++;
-          if (batch[i].status != GPUDB_OK) stats.failed++;
-        }
-      }
-      cv_done.notify_all();
-      cv_work.notify_all();
+      ctx->on_done = nullptr;
+      ctx->on_done_arg = nullptr;
+      for (size_t i = 0; i < batch.size(); i++)   // requests that failed before reaching the GPU
+        if (!done[i]) { done[i] = 1; complete(ids[i], batch[i]); }
     }
   }
 

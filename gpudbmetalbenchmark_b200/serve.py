@@ -137,6 +137,24 @@ class Workload:
             r.q9_capacity = 256
         return Job(kind, r, out)
 
+    def make_like(self, job):
+        """A new job with the same request as `job` and its own result storage."""
+        r = capi.Request()
+        C.pointer(r)[0] = job.req
+        if job.kind == capi.PIPE_Q6:
+            out = capi.Q6Result()
+            r.q6_out = C.pointer(out)
+        elif job.kind == capi.PIPE_Q1:
+            out = capi.Q1Result()
+            r.q1_out = C.pointer(out)
+        elif job.kind == capi.PIPE_Q3:
+            out = capi.Q3Result()
+            r.q3_out = C.pointer(out)
+        else:
+            out = (capi.Q9Group * job.req.q9_capacity)()
+            r.q9_out = C.cast(out, C.POINTER(capi.Q9Group))
+        return Job(job.kind, r, out)
+
     def jobs(self, n, seed):
         rng = random.Random(seed)
         return [self.make(rng) for _ in range(n)]

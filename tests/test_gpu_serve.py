@@ -85,6 +85,25 @@ def test_many_scans_in_one_batch(engine, small):
         assert j.result() == solo[k]
 
 
+def test_identical_joins_in_one_batch(engine, small):
+    """Identical Q3/Q9 requests of one batch run once; every copy gets the full result."""
+    base = [j for j in small.jobs(200, seed=23) if j.kind in (capi.PIPE_Q3, capi.PIPE_Q9)][:4]
+    jobs = []
+    for j in base:   # each request three times, plus a different Q3
+        for _ in range(3):
+            jobs.append(small.make_like(j))
+    solo = small.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()
+        j.req.q9_groups = 0
+    arr = (capi.Request * len(jobs))(*[j.req for j in jobs])
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, arr, len(jobs), None, None))
+    for k, j in enumerate(jobs):
+        assert arr[k].status == capi.OK
+        j.req.q9_groups = arr[k].q9_groups
+        assert j.result() == solo[k]
+
+
 def test_shared_scan_q1_cutoffs_and_q6_mix(engine, orc):
     """One shared pass: Q1 cutoffs that tie, select nothing and select everything, with
     more than one pass's worth of Q6 and Q1 requests over the same rows."""
