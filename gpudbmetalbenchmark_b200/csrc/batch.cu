@@ -14,16 +14,19 @@
 // All groups' row tiles form one work list; a persistent grid pulls tiles from a device
 // queue (one atomicAdd per tile), so a batch of many requests over several tables is one
 // launch. Partial sums reach the requests' result words through integer atomics (exact and
-// order-independent). Q3/Q9 requests are enqueued behind it on the same stream as ordinary
-// async pipeline calls, so the whole batch needs one host synchronisation.
+// order-independent). Q3 requests over the same tables run as batched Q3 launches (q3batch.cu),
+// and the other joins are enqueued behind them on the same stream as ordinary async
+// pipeline calls, so the whole batch needs one host synchronisation.
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <string>
 #include <tuple>
 #include <vector>
 
 #include "common.cuh"
 #include "engine.h"
+#include "q3.h"
 
 namespace gpudb {
 namespace {
@@ -578,10 +581,20 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     scan_bytes = 0;
     return GPUDB_OK;
   };
+  // order on the stream: shared scan passes, then batched Q3 groups, then the other joins
+  std::map<std::string, std::vector<uint32_t>> q3_groups;   // batchable Q3 by identical tables
+  std::vector<uint32_t> joins;
   for (uint32_t i = 0; i < n; i++) {
     gpudb_request& q = reqs[i];
     q.status = GPUDB_OK;
     if (skip[i]) continue;
+    if (q.pipeline == GPUDB_PIPE_Q3 || q.pipeline == GPUDB_PIPE_Q9) {
+      if (n > 1 && q3_batchable(q))
+        q3_groups[std::string(reinterpret_cast<const char*>(q.q3), sizeof *q.q3)].push_back(i);
+      else
+        joins.push_back(i);
+      continue;
+    }
     int rc = GPUDB_OK;
     switch (q.pipeline) {
       case GPUDB_PIPE_Q6:
@@ -615,6 +628,33 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
         ctx->status_sink = nullptr;
         break;
       }
+      default:
+        rc = fail(ctx, GPUDB_E_INVALID, "batch: request %u has unknown pipeline %d", i, q.pipeline);
+    }
+    if (rc != GPUDB_OK) q.status = rc;
+  }
+  flush_scans();
+  auto set_failed = [&](uint32_t i, int rc) {
+    reqs[i].status = rc;
+    if (!async)
+      for (uint32_t d : hook.dups[i]) reqs[d].status = rc;
+  };
+  for (auto& kv : q3_groups) {
+    std::vector<uint32_t>& l = kv.second;
+    for (size_t a = 0; a < l.size(); a += kQ3Batch) {
+      const size_t b = std::min(l.size(), a + (size_t)kQ3Batch);
+      if (b - a == 1) { joins.push_back(l[a]); continue; }
+      const std::vector<uint32_t> part(l.begin() + a, l.begin() + b);
+      const int rc = q3_batch_run(ctx, reqs, part, &aex);
+      if (rc != GPUDB_OK)
+        for (uint32_t i : part) set_failed(i, rc);
+    }
+  }
+  std::sort(joins.begin(), joins.end());
+  for (uint32_t i : joins) {
+    gpudb_request& q = reqs[i];
+    int rc = GPUDB_OK;
+    switch (q.pipeline) {
       case GPUDB_PIPE_Q3:
         if (!q.q3 || !q.q3_out) { rc = fail(ctx, GPUDB_E_INVALID, "batch: Q3 request %u lacks tables/result", i); break; }
         ctx->status_sink = &q.status;
@@ -629,14 +669,10 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
         ctx->status_sink = nullptr;
         break;
       default:
-        rc = fail(ctx, GPUDB_E_INVALID, "batch: request %u has unknown pipeline %d", i, q.pipeline);
+        break;
     }
-    if (rc != GPUDB_OK) {
-      q.status = rc;
-      for (uint32_t d : async ? std::vector<uint32_t>{} : hook.dups[i]) reqs[d].status = rc;
-    }
+    if (rc != GPUDB_OK) set_failed(i, rc);
   }
-  flush_scans();
   if (async) return GPUDB_OK;
   gpudb_sync(ctx);   // per-request outcomes are in each status
   ctx->on_done = hook.prev;

@@ -14,12 +14,13 @@ __device__ __forceinline__ uint32_t lanemask_gt() { uint32_t m; asm("mov.u32 %0,
 
 // Sets bit `key` for rows whose predicate column equals `value` (value < 0: is nonzero;
 // all rows if pred is null). Lanes that hit the same 32-bit word are combined first, so a
-// dense key run costs one atomicOr per word instead of one per row.
-static __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, const uint8_t* __restrict__ pred, int32_t value,
-                                    uint64_t n, int32_t key_max, uint32_t* bitmap, uint32_t* status) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+// dense key run costs one atomicOr per word instead of one per row. Rows first, first +
+// stride, ... (whole warps).
+__device__ __forceinline__ void bitmap_build_rows(const int32_t* __restrict__ keys, const uint8_t* __restrict__ pred,
+                                                  int32_t value, uint64_t n, int32_t key_max, uint32_t* bitmap,
+                                                  uint32_t* status, uint64_t first, uint64_t stride) {
   const uint64_t end = (n + 31) & ~31ull;   // whole warps stay in the loop
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+  for (uint64_t i = first; i < end; i += stride) {
     bool on = false;
     int32_t key = 0;
     if (i < n) {
@@ -39,6 +40,12 @@ static __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, con
       pending &= ~same;
     }
   }
+}
+
+static __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, const uint8_t* __restrict__ pred, int32_t value,
+                                           uint64_t n, int32_t key_max, uint32_t* bitmap, uint32_t* status) {
+  bitmap_build_rows(keys, pred, value, n, key_max, bitmap, status, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                    (uint64_t)gridDim.x * blockDim.x);
 }
 
 // Warp-aggregated append: returns this lane's output position (valid where `take`).

@@ -35,12 +35,6 @@
 
 namespace gpudb {
 
-struct Q3Slot {
-  int32_t key;
-  int32_t date;
-  unsigned long long rev;
-};
-
 namespace {
 
 constexpr int kFilterRows = 4;   // rows per thread per block step of orders_filter_kernel
@@ -117,16 +111,6 @@ __global__ void orders_insert_kernel(const int32_t* __restrict__ key, const int3
   }
 }
 
-__device__ __forceinline__ int32_t ht_find(const Q3Slot* ht, uint32_t cap, int32_t key) {
-  const uint32_t mask = cap - 1;
-  uint32_t s = key_slot(key, mask);
-  for (uint32_t p = 0; p < cap; p++, s = (s + 1) & mask) {
-    const int32_t k = __ldg(&ht[s].key);
-    if (k == key) return (int32_t)s;
-    if (k == kEmptyKey) return -1;
-  }
-  return -1;
-}
 
 constexpr int kProbeBatches = 4;   // independent 32-row batches per warp step (memory-level parallelism)
 
@@ -203,12 +187,6 @@ __global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict
       }
     }
   }
-}
-
-// Other blocks' candidates, read past L1.
-__device__ __forceinline__ u128 ld_cg_u128(const u128* p) {
-  const ulonglong2 q = __ldcg(reinterpret_cast<const ulonglong2*>(p));
-  return ((u128)q.y << 64) | q.x;
 }
 
 // Top-k of the table: block b takes slots [b*4096, +4096) (and counts groups), writes its
@@ -519,20 +497,28 @@ extern "C" int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, cons
   if (rc) return rc;
   const int k = pp.k;
   return call.finish(bytes, [out, k](const uint8_t* h) {
-    uint64_t groups;
-    std::memcpy(&groups, h, 8);
-    out->n_groups = groups;
-    out->n_rows = (uint32_t)std::min<uint64_t>(groups, (uint64_t)k);
-    for (uint32_t i = 0; i < out->n_rows; i++) {
-      u128 c;
-      std::memcpy(&c, h + 16 + i * sizeof(u128), sizeof c);
-      int64_t rev;
-      int32_t date, key;
-      topk_decompose(c, &rev, &date, &key);
-      out->rows[i].order_key = key;
-      out->rows[i].order_date = date;
-      out->rows[i].revenue = rev;
-    }
+    q3_result_from(h, k, out);
     return GPUDB_OK;
   });
 }
+
+namespace gpudb {
+
+void q3_result_from(const uint8_t* h, int k, gpudb_q3_result* out) {
+  uint64_t groups;
+  std::memcpy(&groups, h, 8);
+  out->n_groups = groups;
+  out->n_rows = (uint32_t)std::min<uint64_t>(groups, (uint64_t)k);
+  for (uint32_t i = 0; i < out->n_rows; i++) {
+    u128 c;
+    std::memcpy(&c, h + 16 + i * sizeof(u128), sizeof c);
+    int64_t rev;
+    int32_t date, key;
+    topk_decompose(c, &rev, &date, &key);
+    out->rows[i].order_key = key;
+    out->rows[i].order_date = date;
+    out->rows[i].revenue = rev;
+  }
+}
+
+}  // namespace gpudb

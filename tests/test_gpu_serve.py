@@ -85,6 +85,39 @@ def test_many_scans_in_one_batch(engine, small):
         assert j.result() == solo[k]
 
 
+@pytest.mark.parametrize("no_key_bound", [False, True])
+def test_batched_q3_matches_solo(engine, small, no_key_bound):
+    """Q3 requests over the same tables run as batched launches (groups of up to 8, so 19
+    requests make three groups): each equals the request run alone, for any segment, date
+    bounds and k, with and without the orders key bound (order-key bitmaps off)."""
+    import random
+    rng = random.Random(31 + no_key_bound)
+    tables = small.q3
+    if no_key_bound:
+        od = capi.Orders.from_buffer_copy(tables.od)
+        od.key_max = -1
+        tables = capi.Q3Tables(tables.cu, od, tables.li)
+    jobs = []
+    for i in range(19):
+        r = capi.Request(pipeline=capi.PIPE_Q3)
+        r.q3 = C.pointer(tables)
+        seg = rng.choice([0, 1, 1, 4, 7])             # 7: no customer has it
+        r.q3p = capi.Q3Params(seg, rng.randrange(-1, 2500), rng.randrange(-1, 2600), rng.choice([1, 3, 10, 64]),
+                              capi.JOIN_GLOBAL, 0)
+        out = capi.Q3Result()
+        r.q3_out = C.pointer(out)
+        from gpudbmetalbenchmark_b200.serve import Job
+        jobs.append(Job(capi.PIPE_Q3, r, out))
+    solo = small.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()
+    arr = (capi.Request * len(jobs))(*[j.req for j in jobs])
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, arr, len(jobs), None, None))
+    for k, j in enumerate(jobs):
+        assert arr[k].status == capi.OK
+        assert j.result() == solo[k], k
+
+
 def test_identical_joins_in_one_batch(engine, small):
     """Identical Q3/Q9 requests of one batch run once; every copy gets the full result."""
     base = [j for j in small.jobs(200, seed=23) if j.kind in (capi.PIPE_Q3, capi.PIPE_Q9)][:4]
