@@ -45,11 +45,12 @@ __device__ __forceinline__ u128 warp_sum_u128(u128 v) {
 // the next launch starts clean without a memset.
 __device__ __forceinline__ bool grid_last_block(unsigned* ticket) {
   __shared__ bool last;
+  __threadfence();   // every thread's partial results are visible device-wide before the ticket
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned t = atomicAdd(ticket, 1u);
+    const unsigned t = atomicAdd(ticket, 1u);
     last = (t == gridDim.x - 1);
+    if (last) __threadfence();   // the last block then reads every block's partials
   }
   __syncthreads();
   if (last && threadIdx.x == 0) *ticket = 0u;

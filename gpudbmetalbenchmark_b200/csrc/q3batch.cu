@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(256) q3m_orders_kernel(const int32_t* __restri
   __shared__ uint32_t sh[33];
   __shared__ uint32_t scount[kB];
   if (threadIdx.x < kB) scount[threadIdx.x] = 0;
+  __syncthreads();
   uint32_t mycnt[kB];
 #pragma unroll
   for (int r = 0; r < kB; r++) mycnt[r] = 0;

@@ -177,17 +177,34 @@ extern "C" int gpudb_serve_warmup(gpudb_server* s, gpudb_request* reqs, uint32_t
   s->warming = true;   // workers leave their contexts alone meanwhile
   lk.unlock();
   std::vector<int> rcs(s->lanes.size(), GPUDB_OK);
+  // every lane runs its own copy of the requests (copied before any lane starts)
+  std::vector<std::vector<gpudb_request>> copies(s->lanes.size(), std::vector<gpudb_request>(reqs, reqs + n));
   std::vector<std::thread> th;
   for (size_t i = 0; i < s->lanes.size(); i++)
     th.emplace_back([&, i] {
-      std::vector<gpudb_request> copy(reqs, reqs + n);
+      std::vector<gpudb_request>& copy = copies[i];
+      // lanes other than the first write into outputs of their own: results are converted
+      // in place, so two lanes must never share a result struct
+      std::vector<gpudb_q6_result> o6(i ? n : 0);
+      std::vector<gpudb_q1_result> o1(i ? n : 0);
+      std::vector<gpudb_q3_result> o3(i ? n : 0);
+      std::vector<std::vector<gpudb_q9_group>> o9(i ? n : 0);
+      for (uint32_t k = 0; i && k < n; k++) {
+        gpudb_request& q = copy[k];
+        if (q.q6_out) q.q6_out = &o6[k];
+        if (q.q1_out) q.q1_out = &o1[k];
+        if (q.q3_out) q.q3_out = &o3[k];
+        if (q.q9_out) {
+          o9[k].resize(q.q9_capacity);
+          q.q9_out = o9[k].data();
+        }
+      }
       rcs[i] = gpudb_batch_run(s->lanes[i], copy.data(), n, nullptr, nullptr);
       for (uint32_t k = 0; k < n && rcs[i] == GPUDB_OK; k++)
         if (copy[k].status != GPUDB_OK) rcs[i] = copy[k].status;
-      if (i == 0)
-        for (uint32_t k = 0; k < n; k++) { reqs[k].status = copy[k].status; reqs[k].q9_groups = copy[k].q9_groups; }
     });
   for (auto& t : th) t.join();
+  for (uint32_t k = 0; k < n; k++) { reqs[k].status = copies[0][k].status; reqs[k].q9_groups = copies[0][k].q9_groups; }
   lk.lock();
   s->warming = false;
   lk.unlock();

@@ -229,6 +229,7 @@ def main(argv=None):
     ap.add_argument("--seconds", type=float, default=2.0)
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--max-batch", type=int, default=64)
+    ap.add_argument("--modes", nargs="*", default=["plain", "served"], choices=["plain", "served"])
     a = ap.parse_args(argv)
     eng = Engine(0)
     wl = Workload(eng)
@@ -237,6 +238,8 @@ def main(argv=None):
         seed = int(rate)
         solo = wl.solo_results(wl.jobs(n, seed))
         for name, lanes, mb in (("plain", 1, 1), ("served", a.lanes, a.max_batch)):
+            if name not in a.modes:
+                continue
             res = run_mode(eng, wl, name, lanes, mb, rate, n, seed, check=solo)
             print(json.dumps(res), flush=True)
     eng.close()
