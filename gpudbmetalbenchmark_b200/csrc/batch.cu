@@ -571,11 +571,21 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     ctx->on_done = &BatchHook::on_done;
     ctx->on_done_arg = &hook;
   }
+  // synchronous batches time the whole batch: events around everything it enqueues
+  cudaStream_t bs = (ex && ex->stream) ? static_cast<cudaStream_t>(ex->stream) : ctx->stream;
+  cudaEvent_t te0 = nullptr, te1 = nullptr;
+  const uint64_t launches0 = ctx->launches;
+  const double host0 = now_ms();
+  if (t && !async) {
+    te0 = event_get(ctx);
+    te1 = event_get(ctx);
+    if (te0) cudaEventRecord(te0, bs);
+  }
   std::vector<uint32_t> scans;
   size_t scan_bytes = 0;
   auto flush_scans = [&]() -> int {
     if (scans.empty()) return GPUDB_OK;
-    int rc = run_scan_batch(ctx, reqs, scans, t, &aex);
+    int rc = run_scan_batch(ctx, reqs, scans, async ? t : nullptr, &aex);
     if (rc) for (uint32_t i : scans) reqs[i].status = rc;
     scans.clear();
     scan_bytes = 0;
@@ -674,8 +684,20 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     if (rc != GPUDB_OK) set_failed(i, rc);
   }
   if (async) return GPUDB_OK;
+  if (te1) cudaEventRecord(te1, bs);
   gpudb_sync(ctx);   // per-request outcomes are in each status
   ctx->on_done = hook.prev;
   ctx->on_done_arg = hook.prev_arg;
+  if (t && te0 && te1) {
+    float ms = -1.f;
+    if (cudaEventSynchronize(te1) != cudaSuccess || cudaEventElapsedTime(&ms, te0, te1) != cudaSuccess) ms = -1.f;
+    t->gpu_ms = ms;
+    t->host_ms = now_ms() - host0;
+    t->kernels = (uint32_t)(ctx->launches - launches0);
+    t->h2d_bytes = t->d2h_bytes = 0;
+    t->chunks = 0;
+  }
+  event_put(ctx, te0);
+  event_put(ctx, te1);
   return GPUDB_OK;
 }

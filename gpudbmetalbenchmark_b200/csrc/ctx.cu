@@ -40,7 +40,10 @@ int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out) {
     }
     size_t sz = std::max<size_t>(bytes, 256);
     cudaError_t e = cudaMallocAsync(&b.p, sz, ctx->stream);
-    // complete the allocation before any stream of this context (or a caller's) uses it
+    // pool memory holds whatever its last owner left: new scratch starts zeroed (last-block
+    // tickets and counters rely on it), and the allocation and the fill complete before any
+    // stream of this context (or a caller's) uses the buffer
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.p, 0, sz, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
       b.p = nullptr;

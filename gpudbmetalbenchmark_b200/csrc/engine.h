@@ -80,7 +80,8 @@ int cuda_fail(gpudb_ctx* ctx, cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return gpudb::cuda_fail(ctx, e_, #expr); \
   } while (0)
 
-// Grow-only named scratch buffer on the device (never shrinks; freed at gpudb_destroy).
+// Grow-only named scratch buffer on the device (never shrinks; freed at gpudb_destroy);
+// a new buffer is zero-filled before the call returns.
 // Stream-ordered allocation: growing one context's buffer waits for that context's compute
 // stream only, never for the whole device, and the outgrown buffer is freed in stream order
 // once the context is idle (gpudb_sync, or a synchronous call with nothing pending).

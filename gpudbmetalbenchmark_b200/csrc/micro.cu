@@ -254,12 +254,9 @@ extern "C" int gpudb_sum_i32(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int
   if (rc) return rc;
   if (n) {
     const unsigned grid = grid_of(ctx, n / 4 + 1, 8);
-    void* p = nullptr;
-    Buffer& b = ctx->scratch["sum.partials"];
-    const bool fresh = b.bytes < (size_t)grid * 8 + 256;
+    void* p = nullptr;   // new scratch is zeroed (the ticket); each launch's last block resets it
     rc = scratch(ctx, "sum.partials", (size_t)grid * 8 + 256, &p);
     if (rc) return rc;
-    if (fresh) GPUDB_CUDA(ctx, cudaMemset(p, 0, (size_t)grid * 8 + 256));
     const bool vec = (reinterpret_cast<uintptr_t>(col) & 15u) == 0;
     GPUDB_LAUNCH(call, sum_i32_kernel, grid, kThreads, 0, col, n, vec, (int64_t*)((uint8_t*)p + 256), (unsigned*)p,
                  call.result<int64_t>());

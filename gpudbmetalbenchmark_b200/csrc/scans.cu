@@ -627,15 +627,13 @@ int grid_for(gpudb_ctx* ctx, const void* kernel, uint64_t work_items, int min_bl
   return (int)std::max<uint64_t>(g, 1);
 }
 
-// Per-launch scratch: partials of every block + the last-block ticket (zeroed once).
+// Per-launch scratch: partials of every block + the last-block ticket (new scratch is
+// zeroed; each launch's last block resets the ticket).
 int scan_scratch(gpudb_ctx* ctx, const char* name, size_t partial_bytes, void** partials, unsigned** ticket) {
   void* p = nullptr;
   const size_t need = partial_bytes + 256;
-  Buffer& b = ctx->scratch[name];
-  const bool fresh = b.bytes < need;
   int rc = scratch(ctx, name, need, &p);
   if (rc) return rc;
-  if (fresh) GPUDB_CUDA(ctx, cudaMemset(p, 0, need));
   *ticket = reinterpret_cast<unsigned*>(p);
   *partials = static_cast<uint8_t*>(p) + 256;
   return GPUDB_OK;

@@ -70,6 +70,87 @@ def q9_tables(eng, n_pa, n_su, n_or):
     return pa, su, ps, od
 
 
+def batch_cases(eng, reps):
+    """Batched forms beside the same requests run one by one (gpudb_batch_run with one
+    request each): the device time of the whole batch and the per-request share."""
+    import ctypes as C
+    import random
+    from .serve import Job, Workload
+    wl = Workload(eng)
+    rng = random.Random(5)
+
+    def run(jobs, tm):
+        arr = (capi.Request * len(jobs))(*[j.req for j in jobs])
+        eng._check(eng.lib.gpudb_batch_run(eng.ctx, arr, len(jobs), tm, None))
+
+    def alone(jobs):
+        # one request per call; the sum of the calls' device times
+        total = []
+        for _ in range(3):
+            s = 0.0
+            for j in jobs:
+                t = capi.Timing()
+                if j.kind == capi.PIPE_Q3:
+                    eng._check(eng.lib.gpudb_q3_join_topk(eng.ctx, C.byref(wl.q3.cu), C.byref(wl.q3.od), C.byref(wl.q3.li),
+                                                          C.byref(j.req.q3p), j.req.q3_out, C.byref(t), None))
+                elif j.kind == capi.PIPE_Q6:
+                    eng._check(eng.lib.gpudb_q6_sum(eng.ctx, j.req.li, C.byref(j.req.q6), j.req.q6_out, C.byref(t), None))
+                elif j.kind == capi.PIPE_Q1:
+                    eng._check(eng.lib.gpudb_q1_group6(eng.ctx, j.req.li, C.byref(j.req.q1), j.req.q1_out, C.byref(t),
+                                                       None))
+                s += t.gpu_ms
+            total.append(s)
+        return statistics.median(total)
+
+    # 8 Q3 requests over the config-2 tables (1x) with random segment/date bounds
+    q3 = []
+    for _ in range(8):
+        r = capi.Request(pipeline=capi.PIPE_Q3)
+        r.q3 = C.pointer(wl.q3)
+        r.q3p = capi.Q3Params(rng.randrange(0, 5), rng.randrange(0, 2406), rng.randrange(0, 2527), 10,
+                              capi.JOIN_GLOBAL, 0)
+        out = capi.Q3Result()
+        r.q3_out = C.pointer(out)
+        q3.append(Job(capi.PIPE_Q3, r, out))
+    ms, t = timed(lambda tm: run(q3, tm), reps)
+    emit("q3_batched", "8 requests, config 2 (1x), one launch per stage", 8 * 6_000_000, ms,
+         8 * (150_000 * 5 + 1_500_000 * 12 + 6_000_000 * 20),
+         {"kernels": t.kernels, "ms_per_request": round(ms / 8, 4), "ms_alone_sum": round(alone(q3), 4)})
+    # shared scans over the 60M-row table: 8 Q6 + 2 Q1 requests in one pass each
+    big = wl.scan_structs[-1]
+    scans = []
+    for i in range(10):
+        r = capi.Request(pipeline=capi.PIPE_Q6 if i < 8 else capi.PIPE_Q1)
+        r.li = C.pointer(big)
+        if i < 8:
+            lo = rng.randrange(0, 2527)
+            r.q6 = capi.Q6Params(lo, lo + rng.randrange(1, 731), 2, 8, rng.randrange(1, 52))
+            out = capi.Q6Result()
+            r.q6_out = C.pointer(out)
+        else:
+            r.q1 = capi.Q1Params(rng.randrange(1500, 2527), 0)
+            out = capi.Q1Result()
+            r.q1_out = C.pointer(out)
+        scans.append(Job(r.pipeline, r, out))
+    ms, t = timed(lambda tm: run(scans, tm), reps)
+    emit("shared_scans", "8 Q6 + 2 Q1 over 60M rows, one pass per kind", 10 * 60_000_000, ms,
+         60_000_000 * 20 + 60_000_000 * 26, {"kernels": t.kernels, "ms_per_request": round(ms / 10, 4),
+                                             "ms_alone_sum": round(alone(scans), 4)})
+    # 8 identical Q9 requests at serving scale (6M fact rows): coalesced into one execution
+    q9 = []
+    for _ in range(8):
+        r = capi.Request(pipeline=capi.PIPE_Q9)
+        r.q9 = C.pointer(wl.q9)
+        out = (capi.Q9Group * 256)()
+        r.q9_out = C.cast(out, C.POINTER(capi.Q9Group))
+        r.q9_capacity = 256
+        q9.append(Job(capi.PIPE_Q9, r, out))
+    ms, t = timed(lambda tm: run(q9, tm), reps)
+    one, _ = timed(lambda tm: eng._check(eng.lib.gpudb_batch_run(eng.ctx, C.byref(q9[0].req), 1, tm, None)), reps)
+    emit("q9_coalesced", "8 identical requests, 6M fact rows", 8 * 6_000_000, ms, 8 * 6_000_000 * 28,
+         {"kernels": t.kernels, "ms_per_request": round(ms / 8, 4), "ms_alone": round(one, 4)})
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
@@ -114,6 +195,8 @@ def main(argv=None):
             eng.free(lh)
         for x in (pa, su, ps, od):
             eng.free(x)
+    if on("batch"):
+        batch_cases(eng, a.reps)
     if on("micro"):
         rows = 60_000_000
         t = eng.generate("lineitem", rows, seed=42, columns=("ship_date", "quantity"))

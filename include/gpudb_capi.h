@@ -56,7 +56,10 @@ typedef struct gpudb_ctx gpudb_ctx;
 /* Signed 128-bit integer as two 64-bit halves (value = hi * 2^64 + lo). */
 typedef struct gpudb_i128 { uint64_t lo; int64_t hi; } gpudb_i128;
 
-/* Per-call execution options (NULL = synchronous on the context's stream). */
+/* Per-call execution options (NULL = synchronous on the context's stream). A context's
+ * calls share its scratch memory, so async calls of one context on DIFFERENT streams must
+ * not overlap on the device; use one context per concurrent stream (as the serving lanes
+ * do). Calls on one stream are ordered by the stream. */
 typedef struct gpudb_exec {
   int32_t async;      /* 1: enqueue only; results land at the next gpudb_sync() */
   int32_t flags;      /* reserved, 0 */
@@ -305,11 +308,17 @@ int gpudb_radix_join_pairs(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n
 
 /* ---- batched execution (no reference counterpart: the reference runs one query per
  *      command buffer, src/q1.cpp:59-106) ---------------------------------------------
- * One call runs many requests. All Q6/Q1 requests over device-resident tables share one
- * persistent kernel launch that pulls (request, row range) tiles from a device work queue,
- * so small requests and uneven row ranges cost one launch in total; each request keeps
- * its own exact result and status. Q3/Q9 requests run their pipelines behind it on the
- * same stream without host synchronisation. */
+ * One call runs many requests, each with its own exact result and status:
+ *  - Q6/Q1 requests over device-resident tables are grouped by (table, row range) and
+ *    evaluated in shared passes that read the rows once (up to 8 Q6 per pass; up to 2 Q1
+ *    per pass, with 4 Q6 riding along); all passes are persistent launches that pull row
+ *    tiles from a device queue, so many small requests cost a few launches in total;
+ *  - Q3 requests (global mode) over the same tables run in groups of up to 8 that share
+ *    every stage's launch and one probe pass over the fact table;
+ *  - in a synchronous call, identical Q3/Q9 requests run once and the others get copies;
+ *  - a lone request runs through its own pipeline, exactly as the single-request call.
+ * Everything is enqueued on one stream; a synchronous call finishes the requests in issue
+ * order and times the whole batch in `t`. */
 enum { GPUDB_PIPE_Q6 = 1, GPUDB_PIPE_Q1 = 2, GPUDB_PIPE_Q3 = 3, GPUDB_PIPE_Q9 = 4 };
 
 typedef struct gpudb_q3_tables { gpudb_customer cu; gpudb_orders od; gpudb_lineitem li; } gpudb_q3_tables;
