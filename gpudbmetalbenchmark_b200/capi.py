@@ -20,6 +20,13 @@ ERROR_NAMES = {0: "OK", -1: "E_INVALID", -2: "E_CUDA", -3: "E_OOM", -4: "E_NODEV
 MEM_DEVICE, MEM_HOST = 0, 1
 OPT_CHUNK_ROWS = 1
 OPT_SCAN_VARIANT = 2
+OPT_Q6_VARIANT = 3
+OPT_HT_LOAD = 4
+OPT_RADIX_BITS = 5
+OPT_Q9_SMEM_SLOTS = 6
+OPT_Q9_GLOBAL_SLOTS = 7
+OPT_NAMES = {1: "chunk_rows", 2: "q1_variant", 3: "q6_variant", 4: "ht_load_pct", 5: "radix_bits",
+             6: "q9_smem_slots", 7: "q9_global_slots"}
 JOIN_GLOBAL, JOIN_RADIX = 0, 1
 ORDERS_NONE, ORDERS_CLUSTERED, ORDERS_UNIFORM = 0, 1, 2
 Q3_MAX_K = 64
@@ -164,6 +171,12 @@ class ServeStats(C.Structure):
                 ("batches", C.c_uint64), ("max_batch_seen", C.c_uint64), ("peak_admitted_bytes", C.c_uint64)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("pipeline", C.c_int32), ("candidates", C.c_uint32), ("dropped", C.c_uint32), ("option", C.c_int32),
+                ("value", C.c_int64), ("option2", C.c_int32), ("reserved", C.c_int32), ("value2", C.c_int64),
+                ("best_ms", C.c_double), ("default_ms", C.c_double)]
+
+
 P = C.POINTER
 ctx_p = vp
 # name: (restype, argtypes)
@@ -204,6 +217,10 @@ PROTOTYPES = {
     "gpudb_serve_stats_get": (C.c_int, [vp, P(ServeStats)]),
     "gpudb_request_footprint": (C.c_uint64, [P(Request)]),
     "gpudb_serve_close": (C.c_int, [vp]),
+    "gpudb_get_option": (C.c_int, [ctx_p, C.c_int32, P(C.c_int64)]),
+    "gpudb_autotune": (C.c_int, [ctx_p, P(Request), C.c_uint32, P(TuneResult)]),
+    "gpudb_tune_save": (C.c_int, [ctx_p, C.c_char_p]),
+    "gpudb_tune_load": (C.c_int, [ctx_p, C.c_char_p, P(C.c_uint32)]),
     "gpudb_serve_warmup": (C.c_int, [vp, P(Request), C.c_uint32]),
 }
 

@@ -39,6 +39,8 @@ __device__ __forceinline__ u128 warp_sum_u128(u128 v) {
   return v;
 }
 
+constexpr int kRadixMaxBits = 16;   // radix partitioning: largest fan-out, in bits
+
 // ---- last-block-done grid reduction ---------------------------------------------------
 // Each block publishes its partials, then takes a ticket; the block that draws the last
 // ticket sees every partial (fence before the ticket) and resets the ticket to zero so

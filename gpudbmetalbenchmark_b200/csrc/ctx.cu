@@ -420,8 +420,41 @@ int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value) {
       if (value < 0 || value > 7) return fail(ctx, GPUDB_E_INVALID, "scan variant must be 0..7");
       ctx->scan_variant = (int)value;
       return GPUDB_OK;
+    case GPUDB_OPT_Q6_VARIANT:
+      if (value < 0 || value > 4) return fail(ctx, GPUDB_E_INVALID, "Q6 variant must be 0..4");
+      ctx->q6_variant = (int)value;
+      return GPUDB_OK;
+    case GPUDB_OPT_HT_LOAD:
+      if (value != 50 && value != 25) return fail(ctx, GPUDB_E_INVALID, "hash-table load must be 50 or 25");
+      ctx->ht_shift = value == 50 ? 1 : 2;
+      return GPUDB_OK;
+    case GPUDB_OPT_RADIX_BITS:
+      if (value != 0 && (value < 1 || value > kRadixMaxBits))
+        return fail(ctx, GPUDB_E_INVALID, "radix bits must be 0 or 1..%d", (int)kRadixMaxBits);
+      ctx->radix_bits = (int)value;
+      return GPUDB_OK;
+    case GPUDB_OPT_Q9_SMEM_SLOTS:
+    case GPUDB_OPT_Q9_GLOBAL_SLOTS:
+      if (value < 32 || value > 8192 || (value & (value - 1)))
+        return fail(ctx, GPUDB_E_INVALID, "Q9 slots must be a power of two in 32..8192");
+      (option == GPUDB_OPT_Q9_SMEM_SLOTS ? ctx->q9_smem_slots : ctx->q9_global_slots) = (int)value;
+      return GPUDB_OK;
     default:
       return fail(ctx, GPUDB_E_INVALID, "unknown option %d", option);
+  }
+}
+
+int gpudb_get_option(const gpudb_ctx* ctx, int32_t option, int64_t* value) {
+  if (!ctx || !value) return GPUDB_E_INVALID;
+  switch (option) {
+    case GPUDB_OPT_CHUNK_ROWS: *value = (int64_t)ctx->chunk_rows; return GPUDB_OK;
+    case GPUDB_OPT_SCAN_VARIANT: *value = ctx->scan_variant; return GPUDB_OK;
+    case GPUDB_OPT_Q6_VARIANT: *value = ctx->q6_variant; return GPUDB_OK;
+    case GPUDB_OPT_HT_LOAD: *value = ctx->ht_shift == 1 ? 50 : 25; return GPUDB_OK;
+    case GPUDB_OPT_RADIX_BITS: *value = ctx->radix_bits; return GPUDB_OK;
+    case GPUDB_OPT_Q9_SMEM_SLOTS: *value = ctx->q9_smem_slots; return GPUDB_OK;
+    case GPUDB_OPT_Q9_GLOBAL_SLOTS: *value = ctx->q9_global_slots; return GPUDB_OK;
+    default: return GPUDB_E_INVALID;
   }
 }
 

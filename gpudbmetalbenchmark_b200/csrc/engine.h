@@ -46,7 +46,17 @@ struct gpudb_ctx {
   std::string err;
   uint64_t launches = 0;
   uint64_t chunk_rows = gpudb::kDefaultChunkRows;
-  int scan_variant = 0;                // scan kernel choice (GPUDB_OPT_SCAN_VARIANT)
+  int scan_variant = 0;                // Q1 scan kernel choice (GPUDB_OPT_SCAN_VARIANT)
+  int q6_variant = 0;                  // Q6 scan kernel choice (GPUDB_OPT_Q6_VARIANT)
+  int ht_shift = 1;                    // hash tables hold <= 1/2^ht_shift load (GPUDB_OPT_HT_LOAD)
+  int radix_bits = 0;                  // Q3 radix fan-out when a call leaves it 0 (GPUDB_OPT_RADIX_BITS)
+  int q9_smem_slots = 1024;            // Q9 aggregation slots when a call leaves them 0
+  int q9_global_slots = 4096;
+  struct Tuned {                       // autotuner choices (gpudb_autotune), for gpudb_tune_save
+    int32_t pipeline, rows_log2, option;
+    int64_t value;
+  };
+  std::vector<Tuned> tuned;
   std::unordered_map<std::string, gpudb::Buffer> scratch;
   std::vector<void*> retired;          // outgrown scratch, freed once the context is idle
   uint8_t* d_slots = nullptr;          // result slots (device)

@@ -84,9 +84,9 @@ __device__ __forceinline__ uint32_t block_reserve(uint32_t mine, uint32_t* count
 }
 
 // Open-addressing table capacity from a device-side count: the smallest power of two
-// >= 2*count (at most 50% load), at least `min_cap`, at most `max_cap`.
-__device__ __forceinline__ uint32_t table_capacity(uint32_t count, uint32_t min_cap, uint32_t max_cap) {
-  uint64_t want = 2ull * count;
+// >= count << shift (load at most 1/2^shift), at least `min_cap`, at most `max_cap`.
+__device__ __forceinline__ uint32_t table_capacity(uint32_t count, uint32_t min_cap, uint32_t max_cap, int shift = 1) {
+  uint64_t want = (uint64_t)count << shift;
   uint32_t cap = min_cap;
   while (cap < want && cap < max_cap) cap <<= 1;
   return cap;

@@ -73,9 +73,9 @@ __global__ void __launch_bounds__(256) orders_filter_kernel(const int32_t* __res
   }
 }
 
-__global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint32_t max_cap, uint32_t* cap_out,
+__global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint32_t max_cap, int shift, uint32_t* cap_out,
                                    Q3Slot* ht, uint32_t* hits) {
-  const uint32_t cap = table_capacity(*count, min_cap, max_cap);
+  const uint32_t cap = table_capacity(*count, min_cap, max_cap, shift);
   if (blockIdx.x == 0 && threadIdx.x == 0) *cap_out = cap;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
@@ -326,7 +326,8 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   cudaStream_t s = call.stream();
   const uint32_t words = (uint32_t)(cu.key_max >> 5) + 1;
   const uint64_t n_or = std::max<uint64_t>(od.n_rows, 1), n_li = std::max<uint64_t>(li->n_rows, 1);
-  const int bits = p.radix_bits > 0 ? std::min(p.radix_bits, (int)kRadixMaxBits) : radix_bits_for(od.n_rows, 512);
+  const int bits = p.radix_bits > 0 ? std::min(p.radix_bits, (int)kRadixMaxBits)
+                 : ctx->radix_bits > 0 ? ctx->radix_bits : radix_bits_for(od.n_rows, 4096);
   const uint64_t parts = 1ull << bits;
   void *bitmap, *bstage, *fstage, *count, *bpart, *fpart, *offs, *cand;
   int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
@@ -412,7 +413,7 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   const uint32_t words = (uint32_t)(cu.key_max >> 5) + 1;
   const uint64_t n_or = od.n_rows;
   uint32_t max_cap = 2048;
-  while (max_cap < 2 * n_or && max_cap < (1u << 31)) max_cap <<= 1;
+  while (max_cap < (n_or << ctx->ht_shift) && max_cap < (1u << 31)) max_cap <<= 1;
   void *bitmap, *stage, *count, *ht, *hits, *cand, *okbm = nullptr;
   // order-key bitmap for the probe's miss test when the orders carry a key bound
   const bool use_okbm = n_or && od.key_max >= 0;
@@ -442,7 +443,7 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   if (n_or)
     GPUDB_LAUNCH(call, orders_filter_kernel, grid((n_or + kFilterRows - 1) / kFilterRows), 256, 0, od.order_key, od.cust_key, od.order_date, n_or,
                  p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, skey, sdate, cnt, call.status());
-  GPUDB_LAUNCH(call, table_clear_kernel, grid(max_cap), 256, 0, (const uint32_t*)cnt, 2048u, max_cap, cap,
+  GPUDB_LAUNCH(call, table_clear_kernel, grid(max_cap), 256, 0, (const uint32_t*)cnt, 2048u, max_cap, ctx->ht_shift, cap,
                (Q3Slot*)ht, (uint32_t*)hits);
   GPUDB_LAUNCH(call, orders_insert_kernel, grid(n_or / 4), 256, 0, (const int32_t*)skey, (const int32_t*)sdate,
                (const uint32_t*)cnt, (const uint32_t*)cap, (Q3Slot*)ht, (uint32_t*)okbm, od.key_max, cnt + 2,

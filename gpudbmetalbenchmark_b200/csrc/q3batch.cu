@@ -46,6 +46,7 @@ struct Q3Multi {
   Q3Slot* ht;                                 // K tables of max_cap slots
   uint32_t* hits;
   uint32_t max_cap;
+  int shift;                                  // table load <= 1/2^shift
   uint32_t* cnt;                              // per request: count, capacity, okbm off, ticket
   int32_t* skey;                              // staged orders
   int32_t* sdate;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) q3m_orders_kernel(const int32_t* __restri
 
 __global__ void q3m_clear_kernel(Q3Multi m) {
   const int r = blockIdx.y;
-  const uint32_t cap = table_capacity(m.cnt[4 * r], 2048, m.max_cap);
+  const uint32_t cap = table_capacity(m.cnt[4 * r], 2048, m.max_cap, m.shift);
   if (blockIdx.x == 0 && threadIdx.x == 0) m.cnt[4 * r + 1] = cap;
   Q3Slot* ht = m.ht + (size_t)r * m.max_cap;
   uint32_t* hits = m.hits + (size_t)r * m.max_cap;
@@ -315,8 +316,9 @@ int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t
   for (int d = 0; d < m.D; d++) m.seg[d] = segs[d];
   const uint64_t n_or = od.n_rows;
   uint32_t max_cap = 2048;
-  while (max_cap < 2 * n_or && max_cap < (1u << 31)) max_cap <<= 1;
+  while (max_cap < (n_or << ctx->ht_shift) && max_cap < (1u << 31)) max_cap <<= 1;
   m.max_cap = max_cap;
+  m.shift = ctx->ht_shift;
   m.tiles = (max_cap + kTopkTile - 1) / kTopkTile;
   m.words = (uint32_t)((uint32_t)cu.key_max >> 5) + 1;
   const bool use_okbm = od.key_max >= 0;

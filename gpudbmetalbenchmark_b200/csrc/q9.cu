@@ -79,8 +79,8 @@ __global__ void ps_filter_kernel(const int32_t* __restrict__ part, uint64_t n, c
   }
 }
 
-__global__ void ps_clear_kernel(const uint32_t* count, uint32_t max_cap, uint32_t* cap_out, PsSlot* ht) {
-  const uint32_t cap = table_capacity(*count, 1024, max_cap);
+__global__ void ps_clear_kernel(const uint32_t* count, uint32_t max_cap, int shift, uint32_t* cap_out, PsSlot* ht) {
+  const uint32_t cap = table_capacity(*count, 1024, max_cap, shift);
   if (blockIdx.x == 0 && threadIdx.x == 0) *cap_out = cap;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
@@ -318,8 +318,8 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (rc) return rc;
   gpudb_q9_params pp{};
   if (p) pp = *p;
-  const uint32_t scap = pp.smem_slots ? (uint32_t)pp.smem_slots : 1024u;
-  const uint32_t gcap = pp.global_slots ? (uint32_t)pp.global_slots : 4096u;
+  const uint32_t scap = pp.smem_slots ? (uint32_t)pp.smem_slots : (uint32_t)ctx->q9_smem_slots;
+  const uint32_t gcap = pp.global_slots ? (uint32_t)pp.global_slots : (uint32_t)ctx->q9_global_slots;
   if ((scap & (scap - 1)) || scap < 32 || scap > 8192) return fail(ctx, GPUDB_E_INVALID, "q9: smem_slots must be a power of two in 32..8192");
   if ((gcap & (gcap - 1)) || gcap < 32 || gcap > 8192) return fail(ctx, GPUDB_E_INVALID, "q9: global_slots must be a power of two in 32..8192");
 
@@ -330,7 +330,8 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   const int32_t part_max = pa->n_rows ? pa->key_max : 0, supp_max = su->n_rows ? su->key_max : 0;
   const int32_t order_max = od->n_rows ? od->key_max : 0;
   const uint32_t words = (uint32_t)(part_max >> 5) + 1;
-  const uint32_t ps_max_cap = pow2_at_least((uint32_t)std::min<uint64_t>(2 * ps->n_rows, 1u << 31), 1024);
+  const uint32_t ps_max_cap =
+      pow2_at_least((uint32_t)std::min<uint64_t>(ps->n_rows << ctx->ht_shift, 1u << 31), 1024);
   void *bits, *nation, *year, *stage, *count, *pst, *groups;
   rc = scratch(ctx, "q9.bits", (size_t)words * 4, &bits);
   if (!rc) rc = scratch(ctx, "q9.nation", (size_t)supp_max + 1, &nation);
@@ -364,7 +365,8 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (ps->n_rows)
     GPUDB_LAUNCH(call, ps_filter_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->n_rows, (const uint32_t*)bits,
                  part_max, (uint32_t*)stage, cnt);
-  GPUDB_LAUNCH(call, ps_clear_kernel, grid(ps_max_cap), 256, 0, (const uint32_t*)cnt, ps_max_cap, cap, (PsSlot*)pst);
+  GPUDB_LAUNCH(call, ps_clear_kernel, grid(ps_max_cap), 256, 0, (const uint32_t*)cnt, ps_max_cap, ctx->ht_shift, cap,
+               (PsSlot*)pst);
   GPUDB_LAUNCH(call, ps_insert_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->supp_key, ps->supply_cost,
                (const uint32_t*)stage, (const uint32_t*)cnt, (const uint32_t*)cap, (PsSlot*)pst, call.status());
   const Q9Maps maps{(const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,

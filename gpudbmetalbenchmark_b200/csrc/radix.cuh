@@ -28,7 +28,6 @@ constexpr int kRadixThreads = 256;
 constexpr int kRadixItems = 16;
 constexpr int kRadixTile = kRadixThreads * kRadixItems;   // 4096 rows per block
 constexpr int kRadixPassBits = 8;                          // fan-out 256 per pass
-constexpr int kRadixMaxBits = 16;
 
 __device__ __forceinline__ uint32_t radix_digit(int32_t key, int shift, uint32_t dmask) {
   return (key_hash32(key) >> shift) & dmask;

@@ -647,16 +647,25 @@ int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, voi
   if (c.n_rows == 0) return GPUDB_OK;
   const Q6P pp{p.ship_lo, p.ship_hi, p.disc_lo, p.disc_hi, p.qty_lt};
   const bool vec = aligned(c.ship_date, 16) && aligned(c.discount, 16) && aligned(c.quantity, 16) && aligned(c.ext_price, 8);
-  const int grid = vec ? grid_for(ctx, (const void*)q6_vec_kernel<2>, (c.n_rows / 4 + 1) / 2, 1)
-                       : grid_for(ctx, (const void*)q6_row_kernel, c.n_rows, 1);
+  // 1 one row per thread; 2/3/4: 128-bit loads, 1/2/4 quads per thread per step. Auto (0):
+  // the autotuner's choice on B200 -- one row per thread below 2^24 rows (the columns stay
+  // in L2 across calls), one quad per step above
+  int variant = ctx->q6_variant ? ctx->q6_variant : (c.n_rows < (1u << 24) ? 1 : 2);
+  if (!vec) variant = 1;
+  const int unroll = variant == 2 ? 1 : variant == 4 ? 4 : 2;
+  const void* kfn = variant == 1 ? (const void*)q6_row_kernel
+                    : unroll == 1 ? (const void*)q6_vec_kernel<1>
+                    : unroll == 4 ? (const void*)q6_vec_kernel<4> : (const void*)q6_vec_kernel<2>;
+  const int grid = variant == 1 ? grid_for(ctx, kfn, c.n_rows, 1) : grid_for(ctx, kfn, (c.n_rows / 4 + 1) / unroll, 1);
   void* part = nullptr;
   unsigned* ticket = nullptr;
   int rc = scan_scratch(ctx, "q6.partials", (size_t)grid * 16, &part, &ticket);
   if (rc) return rc;
   int64_t* prev = static_cast<int64_t*>(part);
   uint64_t* pcnt = reinterpret_cast<uint64_t*>(prev + grid);
-  if (vec) {
-    GPUDB_LAUNCH(call, q6_vec_kernel<2>, grid, kThreads, 0, (const int4*)c.ship_date, (const int4*)c.discount,
+  if (variant != 1) {
+    auto k = unroll == 1 ? q6_vec_kernel<1> : unroll == 4 ? q6_vec_kernel<4> : q6_vec_kernel<2>;
+    GPUDB_LAUNCH(call, k, grid, kThreads, 0, (const int4*)c.ship_date, (const int4*)c.discount,
                  (const int4*)c.quantity, c.ext_price, c.n_rows, pp, prev, pcnt, ticket, (Q6Out*)out);
   } else {
     GPUDB_LAUNCH(call, q6_row_kernel, grid, kThreads, 0, c.ship_date, c.discount, c.quantity, c.ext_price, c.n_rows,

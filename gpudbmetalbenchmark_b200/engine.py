@@ -8,6 +8,7 @@ pipeline returns the exact result as Python integers. Every method calls the CUD
 library; a missing library or GPU is an error, never a CPU fallback.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -135,8 +136,35 @@ class Engine:
         return self._check(self.lib.gpudb_set_option(self.ctx, capi.OPT_CHUNK_ROWS, int(rows)))
 
     def set_scan_variant(self, variant):
-        """Scan kernel choice: 0 auto, 1 TMA-staged tiles, 2 128-bit loads, 3 one row per thread."""
+        """Q1 scan kernel choice (GPUDB_OPT_SCAN_VARIANT): 0 auto, 1..7 (see gpudb_capi.h)."""
         return self._check(self.lib.gpudb_set_option(self.ctx, capi.OPT_SCAN_VARIANT, int(variant)))
+
+    def set_option(self, option, value):
+        return self._check(self.lib.gpudb_set_option(self.ctx, int(option), int(value)))
+
+    def get_option(self, option):
+        v = C.c_int64()
+        self._check(self.lib.gpudb_get_option(self.ctx, int(option), C.byref(v)))
+        return v.value
+
+    def autotune(self, req, reps=10):
+        """Times the candidate settings of one request's pipeline (a capi.Request) on its own
+        tables and keeps the fastest on this context; returns what was chosen."""
+        r = capi.TuneResult()
+        self._check(self.lib.gpudb_autotune(self.ctx, C.byref(req), int(reps), C.byref(r)))
+        out = {"pipeline": r.pipeline, "candidates": r.candidates, "dropped": r.dropped,
+               capi.OPT_NAMES[r.option]: r.value, "best_ms": r.best_ms, "default_ms": r.default_ms}
+        if r.option2:
+            out[capi.OPT_NAMES[r.option2]] = r.value2
+        return out
+
+    def tune_save(self, path):
+        return self._check(self.lib.gpudb_tune_save(self.ctx, os.fsencode(path)))
+
+    def tune_load(self, path):
+        n = C.c_uint32()
+        self._check(self.lib.gpudb_tune_load(self.ctx, os.fsencode(path), C.byref(n)))
+        return n.value
 
     def sync(self):
         return self._check(self.lib.gpudb_sync(self.ctx))

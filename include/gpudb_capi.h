@@ -91,11 +91,19 @@ uint64_t gpudb_kernel_launches(const gpudb_ctx* ctx);
 /* Context options (replaces the fixed ChunkConfig sizing of src/infra.h:42-57). */
 enum {
   GPUDB_OPT_CHUNK_ROWS = 1,  /* rows per streamed chunk of a host-resident fact table (default 64M) */
-  GPUDB_OPT_SCAN_VARIANT = 2 /* Q1 scan kernel: 0 auto (7), 1 TMA 2048-row tiles x 4 stages, 2 128-bit loads,
-                                3 one row per thread, 4 TMA 4096-row tiles x 2 stages, 5 TMA ring,
-                                6 TMA ring + shared accumulators, 7 128-bit loads + shared accumulators */
+  GPUDB_OPT_SCAN_VARIANT = 2, /* Q1 scan kernel: 0 auto (7), 1 TMA 2048-row tiles x 4 stages, 2 128-bit loads,
+                                 3 one row per thread, 4 TMA 4096-row tiles x 2 stages, 5 TMA ring,
+                                 6 TMA ring + shared accumulators, 7 128-bit loads + shared accumulators */
+  GPUDB_OPT_Q6_VARIANT = 3,   /* Q6 scan kernel: 0 auto (1 below 2^24 rows, else 2), 1 one row per thread,
+                                 2/3/4 128-bit loads with 1/2/4 quads (4/8/16 rows) per thread per step */
+  GPUDB_OPT_HT_LOAD = 4,      /* largest load of the Q3/Q9 build hash tables, percent: 50 (default) or 25 */
+  GPUDB_OPT_RADIX_BITS = 5,   /* Q3 radix mode fan-out (bits) when a call's radix_bits is 0; 0 = from the
+                                 build size, ~4096 build rows per partition (default) */
+  GPUDB_OPT_Q9_SMEM_SLOTS = 6,   /* Q9 per-block aggregation slots when a call's smem_slots is 0 (1024) */
+  GPUDB_OPT_Q9_GLOBAL_SLOTS = 7  /* Q9 global aggregation slots when a call's global_slots is 0 (4096) */
 };
 int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value);
+int gpudb_get_option(const gpudb_ctx* ctx, int32_t option, int64_t* value);
 
 /* ---- memory (replaces MTL::Device::newBuffer and createFilledBuffer, src/infra.h:527-531) */
 int gpudb_device_alloc(gpudb_ctx* ctx, size_t bytes, void** out);
@@ -347,6 +355,33 @@ typedef struct gpudb_request {
  * next gpudb_sync(). Returns GPUDB_OK when the batch was accepted; per-request failures
  * are reported in each request's status. */
 int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- autotuner (no reference counterpart) --------------------------------------------
+ * gpudb_autotune times the candidate settings of one request's pipeline on the request's
+ * own tables (reps runs each, median device time) and sets the fastest on the context:
+ *   Q1: GPUDB_OPT_SCAN_VARIANT 1..7 (block size, rows per thread, 128-bit loads, TMA
+ *       staging, shared-memory accumulators); Q6: GPUDB_OPT_Q6_VARIANT 1..4 (row kernel or
+ *       128-bit loads with 1/2/4 quads per thread per step); Q3 global mode:
+ *       GPUDB_OPT_HT_LOAD 50/25; Q3 radix mode: GPUDB_OPT_RADIX_BITS; Q9:
+ *       GPUDB_OPT_Q9_SMEM_SLOTS x GPUDB_OPT_Q9_GLOBAL_SLOTS.
+ * A candidate whose result differs from the default setting's is dropped. The choices of a
+ * context are written by gpudb_tune_save as lines "device|pipeline|rows_log2|option|value"
+ * (other devices' lines are kept) and applied by gpudb_tune_load (this device's lines). */
+typedef struct gpudb_tune_result {
+  int32_t pipeline;          /* GPUDB_PIPE_* tuned */
+  uint32_t candidates;       /* settings timed, the default included */
+  uint32_t dropped;          /* candidates rejected: unsupported, failing or a different result */
+  int32_t option;            /* the chosen setting, now set on the context */
+  int64_t value;
+  int32_t option2;           /* a second option of the same choice (0 = none) */
+  int32_t reserved;
+  int64_t value2;
+  double best_ms;            /* median device time with the chosen setting */
+  double default_ms;         /* median device time with the default setting */
+} gpudb_tune_result;
+int gpudb_autotune(gpudb_ctx* ctx, const gpudb_request* req, uint32_t reps, gpudb_tune_result* out);
+int gpudb_tune_save(gpudb_ctx* ctx, const char* path);
+int gpudb_tune_load(gpudb_ctx* ctx, const char* path, uint32_t* applied);
 
 /* ---- serving (no reference counterpart) ---------------------------------------------
  * A request loop over HBM-resident tables. `lanes` worker threads each own a context
