@@ -25,8 +25,9 @@ OPT_HT_LOAD = 4
 OPT_RADIX_BITS = 5
 OPT_Q9_SMEM_SLOTS = 6
 OPT_Q9_GLOBAL_SLOTS = 7
+OPT_GRAPHS = 8
 OPT_NAMES = {1: "chunk_rows", 2: "q1_variant", 3: "q6_variant", 4: "ht_load_pct", 5: "radix_bits",
-             6: "q9_smem_slots", 7: "q9_global_slots"}
+             6: "q9_smem_slots", 7: "q9_global_slots", 8: "graphs"}
 JOIN_GLOBAL, JOIN_RADIX = 0, 1
 ORDERS_NONE, ORDERS_CLUSTERED, ORDERS_UNIFORM = 0, 1, 2
 Q3_MAX_K = 64

@@ -45,6 +45,7 @@ int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out) {
     // stream of this context (or a caller's) uses the buffer
     if (e == cudaSuccess) e = cudaMemsetAsync(b.p, 0, sz, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    ctx->scratch_gen++;   // captured graphs hold scratch pointers
     if (e != cudaSuccess) {
       b.p = nullptr;
       return e == cudaErrorMemoryAllocation ? fail(ctx, GPUDB_E_OOM, "scratch %s: %zu bytes", name, sz)
@@ -54,6 +55,32 @@ int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out) {
   }
   *out = b.p;
   return GPUDB_OK;
+}
+
+gpudb_ctx::Graph* graph_find(gpudb_ctx* ctx, const std::string& key) {
+  for (auto& g : ctx->graphs)
+    if (g.key == key) {
+      if (g.scratch_gen != ctx->scratch_gen) return nullptr;
+      g.last_use = ++ctx->graph_clock;
+      return &g;
+    }
+  return nullptr;
+}
+
+void graph_store(gpudb_ctx* ctx, const std::string& key, cudaGraphExec_t exec, uint32_t kernels) {
+  for (auto it = ctx->graphs.begin(); it != ctx->graphs.end(); ++it)
+    if (it->key == key) {   // stale (a scratch buffer moved): replace
+      cudaGraphExecDestroy(it->exec);
+      ctx->graphs.erase(it);
+      break;
+    }
+  if (ctx->graphs.size() >= kMaxGraphs) {
+    auto lru = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                [](const gpudb_ctx::Graph& a, const gpudb_ctx::Graph& b) { return a.last_use < b.last_use; });
+    cudaGraphExecDestroy(lru->exec);
+    ctx->graphs.erase(lru);
+  }
+  ctx->graphs.push_back({key, exec, ctx->scratch_gen, kernels, ++ctx->graph_clock});
 }
 
 // Frees outgrown scratch; only when no work of the context can still be queued.
@@ -368,6 +395,7 @@ int gpudb_destroy(gpudb_ctx* ctx) {
       if (kv.second.p) cudaFreeAsync(kv.second.p, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
   }
+  for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->d_slots) cudaFree(ctx->d_slots);
   if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
@@ -433,6 +461,10 @@ int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value) {
         return fail(ctx, GPUDB_E_INVALID, "radix bits must be 0 or 1..%d", (int)kRadixMaxBits);
       ctx->radix_bits = (int)value;
       return GPUDB_OK;
+    case GPUDB_OPT_GRAPHS:
+      if (value != 0 && value != 1) return fail(ctx, GPUDB_E_INVALID, "graphs option must be 0 or 1");
+      ctx->use_graphs = value != 0;
+      return GPUDB_OK;
     case GPUDB_OPT_Q9_SMEM_SLOTS:
     case GPUDB_OPT_Q9_GLOBAL_SLOTS:
       if (value < 32 || value > 8192 || (value & (value - 1)))
@@ -454,6 +486,7 @@ int gpudb_get_option(const gpudb_ctx* ctx, int32_t option, int64_t* value) {
     case GPUDB_OPT_RADIX_BITS: *value = ctx->radix_bits; return GPUDB_OK;
     case GPUDB_OPT_Q9_SMEM_SLOTS: *value = ctx->q9_smem_slots; return GPUDB_OK;
     case GPUDB_OPT_Q9_GLOBAL_SLOTS: *value = ctx->q9_global_slots; return GPUDB_OK;
+    case GPUDB_OPT_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return GPUDB_OK;
     default: return GPUDB_E_INVALID;
   }
 }

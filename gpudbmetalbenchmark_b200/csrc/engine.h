@@ -57,6 +57,18 @@ struct gpudb_ctx {
     int64_t value;
   };
   std::vector<Tuned> tuned;
+  // captured pipelines (CUDA graphs), replayed while the key and the scratch layout hold
+  struct Graph {
+    std::string key;
+    cudaGraphExec_t exec;
+    uint64_t scratch_gen;
+    uint32_t kernels;
+    uint64_t last_use;
+  };
+  std::vector<Graph> graphs;
+  bool use_graphs = true;              // GPUDB_OPT_GRAPHS
+  uint64_t scratch_gen = 0;            // bumped whenever a scratch buffer is (re)allocated
+  uint64_t graph_clock = 0;
   std::unordered_map<std::string, gpudb::Buffer> scratch;
   std::vector<void*> retired;          // outgrown scratch, freed once the context is idle
   uint8_t* d_slots = nullptr;          // result slots (device)
@@ -97,6 +109,13 @@ int cuda_fail(gpudb_ctx* ctx, cudaError_t e, const char* what);
 // once the context is idle (gpudb_sync, or a synchronous call with nothing pending).
 int scratch(gpudb_ctx* ctx, const char* name, size_t bytes, void** out);
 
+// Captured pipelines: the cached graph of `key` (null if none, or if a scratch buffer was
+// reallocated since it was captured), and storing a newly instantiated one (the cache keeps
+// kMaxGraphs, least recently used out).
+constexpr size_t kMaxGraphs = 16;
+gpudb_ctx::Graph* graph_find(gpudb_ctx* ctx, const std::string& key);
+void graph_store(gpudb_ctx* ctx, const std::string& key, cudaGraphExec_t exec, uint32_t kernels);
+
 cudaEvent_t event_get(gpudb_ctx* ctx);
 void event_put(gpudb_ctx* ctx, cudaEvent_t e);
 
@@ -108,9 +127,17 @@ class Call {
   ~Call();
   int begin(size_t result_bytes);          // acquires a slot and zeroes header + payload
   cudaStream_t stream() const { return s_; }
-  uint32_t* status() const { return reinterpret_cast<uint32_t*>(dslot_); }
-  template <class T> T* result() const { return reinterpret_cast<T*>(dslot_ + kSlotHeader); }
+  uint32_t* status() const { return reinterpret_cast<uint32_t*>(dwork_ ? dwork_ : dslot_); }
+  template <class T> T* result() const { return reinterpret_cast<T*>((dwork_ ? dwork_ : dslot_) + kSlotHeader); }
+  // Kernels write status and result into `base` (slot layout: header, payload) instead of the
+  // call's slot: a captured graph needs fixed pointers; the caller copies base into the slot.
+  void redirect(uint8_t* base) { dwork_ = base; }
+  uint8_t* slot_device() const { return dslot_; }
+  uint32_t kernels() const { return kernels_; }
   void count_launch() { kernels_++; ctx_->launches++; }
+  // launches recorded into a graph are not launches; a replay counts the graph's kernels
+  void uncount_launches(uint32_t n) { kernels_ -= n; ctx_->launches -= n; }
+  void count_launches(uint32_t n) { kernels_ += n; ctx_->launches += n; }
   void add_h2d(uint64_t b) { h2d_ += b; }
   void add_chunk() { chunks_++; }
   // Copies the result back and converts it with `convert(host_payload)`.
@@ -129,6 +156,7 @@ class Call {
   bool big_ = false;
   uint8_t* dslot_ = nullptr;
   uint8_t* hslot_ = nullptr;
+  uint8_t* dwork_ = nullptr;
   uint32_t kernels_ = 0, chunks_ = 0;
   uint64_t h2d_ = 0, d2h_ = 0;
   bool handed_off_ = false;

@@ -18,6 +18,7 @@
 //  - one block compacts the global table and sorts it by nation asc, year desc.
 #include <algorithm>
 #include <cstring>
+#include <string>
 
 #include "common.cuh"
 #include "engine.h"
@@ -345,47 +346,92 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   uint32_t* cap = cnt + 1;
   uint32_t* gkeys = reinterpret_cast<uint32_t*>(static_cast<unsigned long long*>(groups) + gcap);
   unsigned long long* gvals = static_cast<unsigned long long*>(groups);
-  GPUDB_CUDA(ctx, cudaMemsetAsync(bits, 0, (size_t)words * 4, s));
-  GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, s));
-  GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, s));
-  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
-  GPUDB_CUDA(ctx, cudaMemsetAsync(gvals, 0, (size_t)gcap * 8, s));
-  GPUDB_CUDA(ctx, cudaMemsetAsync(gkeys, 0xFF, (size_t)gcap * 4, s));
+  const size_t probe_smem = (size_t)scap * 12, sort_smem = (size_t)gcap * 12;
+  // dynamic + static shared memory may pass the 48 KB default: always opt in (before any capture)
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
-  if (pa->n_rows)
-    GPUDB_LAUNCH(call, bitmap_build_kernel, grid(pa->n_rows), 256, 0, pa->part_key, pa->flag, -1, pa->n_rows,
-                 part_max, (uint32_t*)bits, call.status());
-  if (su->n_rows)
-    GPUDB_LAUNCH(call, map_u8_kernel, grid(su->n_rows), 256, 0, su->supp_key, su->nation, su->n_rows, supp_max,
-                 (uint8_t*)nation, call.status());
-  if (od->n_rows)
-    GPUDB_LAUNCH(call, year_map_kernel, grid(od->n_rows), 256, 0, od->order_key, od->order_date, od->n_rows,
-                 order_max, (uint8_t*)year, call.status());
-  if (ps->n_rows)
-    GPUDB_LAUNCH(call, ps_filter_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->n_rows, (const uint32_t*)bits,
-                 part_max, (uint32_t*)stage, cnt);
-  GPUDB_LAUNCH(call, ps_clear_kernel, grid(ps_max_cap), 256, 0, (const uint32_t*)cnt, ps_max_cap, ctx->ht_shift, cap,
-               (PsSlot*)pst);
-  GPUDB_LAUNCH(call, ps_insert_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->supp_key, ps->supply_cost,
-               (const uint32_t*)stage, (const uint32_t*)cnt, (const uint32_t*)cap, (PsSlot*)pst, call.status());
-  const Q9Maps maps{(const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,
-                    (const uint32_t*)cap, (const uint8_t*)year, order_max};
-  const size_t probe_smem = (size_t)scap * 12;
-  // dynamic + static shared memory may pass the 48 KB default: always opt in
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
-  rc = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
-    if (c.n_rows == 0) return (int)GPUDB_OK;
-    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows / 4 + 255) / 256, (uint64_t)sms * 8));
-    GPUDB_LAUNCH(call, q9_probe_kernel, g, kQ9Threads, probe_smem, c.part_key, c.supp_key, c.order_key, c.ext_price, c.discount,
-                 c.quantity, c.n_rows, maps, gkeys, gvals, gcap, scap, call.status());
-    return (int)GPUDB_OK;
-  });
-  if (rc) return rc;
-  const size_t sort_smem = (size_t)gcap * 12;
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
-  GPUDB_LAUNCH(call, q9_sort_kernel, 1, 1024, sort_smem, (const uint32_t*)gkeys, (const unsigned long long*)gvals, gcap,
-               call.result<uint8_t>());
+  // Every device operation of the pipeline, in stream order (status and result through
+  // call.status()/call.result()).
+  auto enqueue = [&]() -> int {
+    GPUDB_CUDA(ctx, cudaMemsetAsync(bits, 0, (size_t)words * 4, s));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, s));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, s));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(gvals, 0, (size_t)gcap * 8, s));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(gkeys, 0xFF, (size_t)gcap * 4, s));
+    if (pa->n_rows)
+      GPUDB_LAUNCH(call, bitmap_build_kernel, grid(pa->n_rows), 256, 0, pa->part_key, pa->flag, -1, pa->n_rows,
+                   part_max, (uint32_t*)bits, call.status());
+    if (su->n_rows)
+      GPUDB_LAUNCH(call, map_u8_kernel, grid(su->n_rows), 256, 0, su->supp_key, su->nation, su->n_rows, supp_max,
+                   (uint8_t*)nation, call.status());
+    if (od->n_rows)
+      GPUDB_LAUNCH(call, year_map_kernel, grid(od->n_rows), 256, 0, od->order_key, od->order_date, od->n_rows,
+                   order_max, (uint8_t*)year, call.status());
+    if (ps->n_rows)
+      GPUDB_LAUNCH(call, ps_filter_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->n_rows, (const uint32_t*)bits,
+                   part_max, (uint32_t*)stage, cnt);
+    GPUDB_LAUNCH(call, ps_clear_kernel, grid(ps_max_cap), 256, 0, (const uint32_t*)cnt, ps_max_cap, ctx->ht_shift, cap,
+                 (PsSlot*)pst);
+    GPUDB_LAUNCH(call, ps_insert_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->supp_key, ps->supply_cost,
+                 (const uint32_t*)stage, (const uint32_t*)cnt, (const uint32_t*)cap, (PsSlot*)pst, call.status());
+    const Q9Maps maps{(const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,
+                      (const uint32_t*)cap, (const uint8_t*)year, order_max};
+    int r = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
+      if (c.n_rows == 0) return (int)GPUDB_OK;
+      const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows / 4 + 255) / 256, (uint64_t)sms * 8));
+      GPUDB_LAUNCH(call, q9_probe_kernel, g, kQ9Threads, probe_smem, c.part_key, c.supp_key, c.order_key, c.ext_price,
+                   c.discount, c.quantity, c.n_rows, maps, gkeys, gvals, gcap, scap, call.status());
+      return (int)GPUDB_OK;
+    });
+    if (r) return r;
+    GPUDB_LAUNCH(call, q9_sort_kernel, 1, 1024, sort_smem, (const uint32_t*)gkeys, (const unsigned long long*)gvals,
+                 gcap, call.result<uint8_t>());
+    return GPUDB_OK;
+  };
+  // A device-resident call on the context's stream runs as a CUDA graph: captured the first
+  // time its tables and parameters are seen (and again after a scratch buffer moves), then
+  // replayed. The graph writes status and groups into a fixed scratch buffer; one copy moves
+  // them into this call's result slot.
+  const bool graph = ctx->use_graphs && li->location == GPUDB_MEM_DEVICE && s == ctx->stream;
+  if (!graph) {
+    if ((rc = enqueue())) return rc;
+  } else {
+    void* gout = nullptr;
+    if ((rc = scratch(ctx, "q9.graph_out", kSlotHeader + bytes, &gout))) return rc;
+    std::string key = "q9|";
+    auto add = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
+    add(pa, sizeof *pa); add(su, sizeof *su); add(ps, sizeof *ps); add(od, sizeof *od); add(li, sizeof *li);
+    add(&scap, sizeof scap); add(&gcap, sizeof gcap); add(&ctx->ht_shift, sizeof ctx->ht_shift);
+    gpudb_ctx::Graph* g = graph_find(ctx, key);
+    if (!g) {
+      call.redirect(static_cast<uint8_t*>(gout));
+      const uint32_t k0 = call.kernels();
+      GPUDB_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      cudaError_t me = cudaMemsetAsync(gout, 0, kSlotHeader + bytes, s);
+      int er = me == cudaSuccess ? enqueue() : cuda_fail(ctx, me, "cudaMemsetAsync");
+      cudaGraph_t cg = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(s, &cg);
+      const uint32_t captured = call.kernels() - k0;
+      call.uncount_launches(captured);
+      cudaGraphExec_t exec = nullptr;
+      if (er == GPUDB_OK && ee != cudaSuccess) er = cuda_fail(ctx, ee, "cudaStreamEndCapture");
+      if (er == GPUDB_OK) {
+        const cudaError_t ie = cudaGraphInstantiate(&exec, cg, 0);
+        if (ie != cudaSuccess) er = cuda_fail(ctx, ie, "cudaGraphInstantiate");
+      }
+      if (cg) cudaGraphDestroy(cg);
+      if (er != GPUDB_OK) return er;
+      graph_store(ctx, key, exec, captured);
+      g = graph_find(ctx, key);
+      call.redirect(nullptr);
+    }
+    GPUDB_CUDA(ctx, cudaGraphLaunch(g->exec, s));
+    call.count_launches(g->kernels);
+    GPUDB_CUDA(ctx, cudaMemcpyAsync(call.slot_device(), gout, kSlotHeader + bytes, cudaMemcpyDeviceToDevice, s));
+  }
   const uint32_t cap_out = capacity;
   const size_t copy = 16 + (size_t)std::min(gcap, capacity) * 16;
   return call.finish(copy, [out, cap_out, n_groups](const uint8_t* h) {

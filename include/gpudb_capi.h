@@ -100,7 +100,10 @@ enum {
   GPUDB_OPT_RADIX_BITS = 5,   /* Q3 radix mode fan-out (bits) when a call's radix_bits is 0; 0 = from the
                                  build size, ~4096 build rows per partition (default) */
   GPUDB_OPT_Q9_SMEM_SLOTS = 6,   /* Q9 per-block aggregation slots when a call's smem_slots is 0 (1024) */
-  GPUDB_OPT_Q9_GLOBAL_SLOTS = 7  /* Q9 global aggregation slots when a call's global_slots is 0 (4096) */
+  GPUDB_OPT_Q9_GLOBAL_SLOTS = 7, /* Q9 global aggregation slots when a call's global_slots is 0 (4096) */
+  GPUDB_OPT_GRAPHS = 8           /* 1 (default): a Q9 call over device-resident tables on the context's
+                                    stream is captured into a CUDA graph once per (tables, parameters)
+                                    and replayed after; 0: its kernels are launched one by one */
 };
 int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value);
 int gpudb_get_option(const gpudb_ctx* ctx, int32_t option, int64_t* value);

@@ -85,3 +85,32 @@ def test_q9_key_out_of_range_reported(engine, orc):
         assert rc == capi.E_KEY_RANGE
     finally:
         free_all(engine, ts)
+
+
+def test_q9_graph_capture_and_replay(orc):
+    """A device-resident Q9 call is captured into a CUDA graph once and replayed: the first
+    (capturing) call, replays, a changed parameter (a new capture) and graphs switched off all
+    give the oracle's groups; replays count the graph's kernels as launches."""
+    from gpudbmetalbenchmark_b200.engine import Engine
+    tabs = orc.q9_tables(20_000, 1_000, 100_000, 400_000, 11)
+    want = orc.q9(*tabs)
+    with Engine(0) as e:
+        assert e.get_option(capi.OPT_GRAPHS) == 1
+        ts = upload_all(e, tabs)
+        kernels = []
+        for _ in range(3):
+            t = capi.Timing()
+            assert e.q9(*ts, timing=t) == want
+            kernels.append(t.kernels)
+        assert kernels[0] == kernels[1] == kernels[2] == 8
+        before = e.launches()
+        assert e.q9(*ts, smem_slots=64) == want          # another key: captured anew
+        assert e.q9(*ts, smem_slots=64) == want
+        assert e.launches() - before == 16
+        with pytest.raises(capi.GpudbError) as err:       # device status still reported from a graph
+            e.q9(*ts, global_slots=64)
+        assert err.value.code == capi.E_CAPACITY
+        e.set_option(capi.OPT_GRAPHS, 0)
+        assert e.q9(*ts) == want
+        e.set_option(capi.OPT_GRAPHS, 1)
+        assert e.q9(*ts) == want
