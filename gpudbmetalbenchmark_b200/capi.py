@@ -26,6 +26,18 @@ OPT_RADIX_BITS = 5
 OPT_Q9_SMEM_SLOTS = 6
 OPT_Q9_GLOBAL_SLOTS = 7
 OPT_GRAPHS = 8
+TBL_LINEITEM, TBL_ORDERS, TBL_CUSTOMER, TBL_PART, TBL_SUPPLIER, TBL_PARTSUPP = 1, 2, 3, 4, 5, 6
+TBL_MAX_COLS = 10
+# columns a .tbl parse keeps, in the order of gpudb_tbl_parse's cols[]
+TBL_COLUMNS = {
+    "lineitem": (TBL_LINEITEM, ("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax",
+                                "flag", "status", "ship_date")),
+    "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date")),
+    "customer": (TBL_CUSTOMER, ("cust_key", "segment")),
+    "part": (TBL_PART, ("part_key", "flag")),
+    "supplier": (TBL_SUPPLIER, ("supp_key", "nation")),
+    "partsupp": (TBL_PARTSUPP, ("part_key", "supp_key", "supply_cost")),
+}
 OPT_NAMES = {1: "chunk_rows", 2: "q1_variant", 3: "q6_variant", 4: "ht_load_pct", 5: "radix_bits",
              6: "q9_smem_slots", 7: "q9_global_slots", 8: "graphs"}
 JOIN_GLOBAL, JOIN_RADIX = 0, 1
@@ -219,6 +231,9 @@ PROTOTYPES = {
     "gpudb_request_footprint": (C.c_uint64, [P(Request)]),
     "gpudb_serve_close": (C.c_int, [vp]),
     "gpudb_get_option": (C.c_int, [ctx_p, C.c_int32, P(C.c_int64)]),
+    "gpudb_tbl_count_rows": (C.c_int, [ctx_p, vp, C.c_uint64, C.c_int32, P(C.c_uint64)]),
+    "gpudb_tbl_parse": (C.c_int, [ctx_p, C.c_int32, vp, C.c_uint64, C.c_int32, P(vp), C.c_uint64, P(C.c_uint64),
+                                  P(C.c_int32), P(Timing)]),
     "gpudb_autotune": (C.c_int, [ctx_p, P(Request), C.c_uint32, P(TuneResult)]),
     "gpudb_tune_save": (C.c_int, [ctx_p, C.c_char_p]),
     "gpudb_tune_load": (C.c_int, [ctx_p, C.c_char_p, P(C.c_uint32)]),

@@ -226,6 +226,38 @@ class Engine:
         self.tables.append(t)
         return t
 
+    def load_tbl(self, kind, source, columns=None, timing=None):
+        """Parse dbgen-style '|'-separated text (a path, or bytes) on the GPU into a new
+        device table of `kind` (gpudb_tbl_parse); `columns` limits the columns kept."""
+        data = source if isinstance(source, (bytes, bytearray)) else open(source, "rb").read()
+        buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
+        code, names = capi.TBL_COLUMNS[kind]
+        n = C.c_uint64()
+        self._check(self.lib.gpudb_tbl_count_rows(self.ctx, buf.ctypes.data, len(data), MEM_HOST, C.byref(n)))
+        t = Table(self, kind, n.value, MEM_DEVICE)
+        cols = (C.c_void_p * capi.TBL_MAX_COLS)()
+        for i, name in enumerate(names):
+            if columns is not None and name not in columns:
+                continue
+            cid = TABLE_COLS[kind][name]
+            ptr = self._alloc(n.value * self.lib.gpudb_column_width(cid), MEM_DEVICE)
+            t.cols[name] = (ptr, cid)
+            cols[i] = ptr
+        self.tables.append(t)
+        got = C.c_uint64()
+        col_max = (C.c_int32 * capi.TBL_MAX_COLS)()
+        self._check(self.lib.gpudb_tbl_parse(self.ctx, code, buf.ctypes.data, len(data), MEM_HOST, cols, n.value,
+                                             C.byref(got), col_max, C.byref(timing) if timing is not None else None))
+        assert got.value == n.value
+        if kind == "lineitem":
+            t.key_max["order_key"] = col_max[0] if n.value else -1
+        elif kind == "orders":
+            t.key_max["order_key"] = col_max[0] if n.value else -1
+            t.key_max["cust_key"] = col_max[1] if n.value else -1
+        elif kind in ("customer", "part", "supplier"):
+            t.key_max["key"] = col_max[0] if n.value else -1
+        return t
+
     def free(self, table):
         table.close()
         if table in self.tables:

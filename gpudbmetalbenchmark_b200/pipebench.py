@@ -70,6 +70,57 @@ def q9_tables(eng, n_pa, n_su, n_or):
     return pa, su, ps, od
 
 
+def lineitem_text(eng, n, seed=42):
+    """n lineitem rows of the seeded generator as dbgen-style text (numpy string ops)."""
+    import numpy as np
+    cols = ("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag", "status",
+            "ship_date")
+    t = eng.generate("lineitem", n, seed=seed, columns=cols, n_orders=max(1, n // 4), n_parts=200_000, n_supp=10_000,
+                     order_mode=capi.ORDERS_CLUSTERED)
+    c = {k: t.to_numpy(k) for k in cols}
+    eng.free(t)
+    days = np.datetime64("1992-01-01") + c["ship_date"].astype("timedelta64[D]")
+    date = np.datetime_as_string(days, unit="D").astype(object)
+    money = (c["ext_price"] // 100).astype(str).astype(object) + "." + \
+        np.char.zfill((c["ext_price"] % 100).astype(str), 2).astype(object)
+    frac = lambda a: "0." + np.char.zfill(a.astype(str), 2).astype(object)  # noqa: E731
+    f = lambda a: a.astype(str).astype(object)  # noqa: E731
+    rows = (f(c["order_key"]) + "|" + f(c["part_key"]) + "|" + f(c["supp_key"]) + "|1|" + f(c["quantity"]) + "|" +
+            money + "|" + frac(c["discount"]) + "|" + frac(c["tax"]) + "|" +
+            np.array(list("ANR"), dtype=object)[c["flag"]] + "|" + np.array(list("FO"), dtype=object)[c["status"]] +
+            "|" + date + "|" + date + "|" + date + "|DELIVER IN PERSON|TRUCK|a lineitem row|\n")
+    return "".join(rows.tolist()).encode()
+
+
+def tbl_cases(eng, reps):
+    import ctypes as C
+    import numpy as np
+    from .engine import TABLE_COLS
+    n = 6_000_000
+    text = lineitem_text(eng, n)
+    buf = np.frombuffer(text, dtype=np.uint8)
+    code, names = capi.TBL_COLUMNS["lineitem"]
+    cols = (C.c_void_p * capi.TBL_MAX_COLS)()
+    ptrs = []
+    for i, name in enumerate(names):
+        ptrs.append(eng.device_array(n * eng.lib.gpudb_column_width(TABLE_COLS["lineitem"][name])))
+        cols[i] = ptrs[-1]
+    dev = eng.device_array(len(text) + 16)
+    eng._check(eng.lib.gpudb_copy(eng.ctx, dev, buf.ctypes.data, len(text)))
+    got = C.c_uint64()
+    for where, src, loc in (("pageable host text, H2D copy inside the call", buf.ctypes.data, capi.MEM_HOST),
+                            ("device-resident text", dev, capi.MEM_DEVICE)):
+        def run(tm):
+            eng._check(eng.lib.gpudb_tbl_parse(eng.ctx, code, src, len(text), loc, cols, n, C.byref(got), None,
+                                               C.byref(tm) if tm is not None else None))
+        ms, t = timed(run, max(3, reps // 4))
+        emit("tbl_parse", "lineitem, %d rows, %.0f MB of text, %s" % (n, len(text) / 1e6, where), n, ms, len(text),
+             {"kernels": t.kernels, "text_gb_per_s": round(len(text) / (ms * 1e-3) / 1e9, 1)})
+    eng.device_free(dev)
+    for p in ptrs:
+        eng.device_free(p)
+
+
 def batch_cases(eng, reps):
     """Batched forms beside the same requests run one by one (gpudb_batch_run with one
     request each): the device time of the whole batch and the per-request share."""
@@ -197,6 +248,8 @@ def main(argv=None):
             eng.free(x)
     if on("batch"):
         batch_cases(eng, a.reps)
+    if on("tbl"):
+        tbl_cases(eng, a.reps)
     if on("micro"):
         rows = 60_000_000
         t = eng.generate("lineitem", rows, seed=42, columns=("ship_date", "quantity"))

@@ -228,3 +228,84 @@ def join_pairs(b, p, cap=None):
     ob, op = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
     n = int(oracle().or_join_pairs(len(b), _p(b), len(p), _p(p), cap, ob.ctypes.data, op.ctypes.data))
     return ob[:min(n, cap)], op[:min(n, cap)], n
+
+
+# ---- dbgen-style text (test infrastructure for the .tbl loader) ------------------------
+# Field layouts of dbgen's '|'-separated rows; the loader keeps the fields listed in
+# include/gpudb_capi.h. Filler fields hold made-up text of plausible length.
+import datetime as _dt
+
+_EPOCH = _dt.date(1992, 1, 1)
+_SEGMENTS = ("AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY")
+_FLAGS, _STATUS = "ANR", "FO"
+
+
+def _date(d):
+    return (_EPOCH + _dt.timedelta(days=int(d))).isoformat()
+
+
+def _money(h):
+    h = int(h)
+    return "%s%d.%02d" % ("-" if h < 0 else "", abs(h) // 100, abs(h) % 100)
+
+
+def format_tbl(kind, c):
+    """Rows of table `kind` as dbgen text (bytes) from numpy columns in the engine's encoding."""
+    out = []
+    if kind == "lineitem":
+        n = len(c["order_key"])
+        for i in range(n):
+            sd = int(c["ship_date"][i])
+            out.append("%d|%d|%d|%d|%d|%s|0.%02d|0.%02d|%s|%s|%s|%s|%s|DELIVER IN PERSON|TRUCK|row %d of the sample|"
+                       % (c["order_key"][i], c["part_key"][i], c["supp_key"][i], i % 7 + 1, c["quantity"][i],
+                          _money(c["ext_price"][i]), c["discount"][i], c["tax"][i], _FLAGS[c["flag"][i]],
+                          _STATUS[c["status"][i]], _date(sd), _date(sd + 30), _date(sd + 45), i))
+    elif kind == "orders":
+        for i in range(len(c["order_key"])):
+            out.append("%d|%d|O|%s|%s|3-MEDIUM|Clerk#%09d|0|an order|" % (c["order_key"][i], c["cust_key"][i],
+                                                                             _money(12345 + i), _date(c["order_date"][i]), i))
+    elif kind == "customer":
+        for i in range(len(c["cust_key"])):
+            out.append("%d|Customer#%09d|addr %d|%d|10-123-456-7890|%s|%s|a customer|"
+                       % (c["cust_key"][i], c["cust_key"][i], i, i % 25, _money(100 * i - 5000), _SEGMENTS[c["segment"][i]]))
+    elif kind == "part":
+        for i in range(len(c["part_key"])):
+            name = "forest green lace" if c["flag"][i] else "steel ivory lace"
+            out.append("%d|%s %d|Manufacturer#1|Brand#13|SMALL PLATED TIN|7|JUMBO PKG|%s|a part|"
+                       % (c["part_key"][i], name, i, _money(90000 + i)))
+    elif kind == "supplier":
+        for i in range(len(c["supp_key"])):
+            out.append("%d|Supplier#%09d|addr %d|%d|11-222-333-4444|%s|a supplier|"
+                       % (c["supp_key"][i], c["supp_key"][i], i, c["nation"][i], _money(500 * i)))
+    elif kind == "partsupp":
+        for i in range(len(c["part_key"])):
+            out.append("%d|%d|%d|%s|a partsupp row|" % (c["part_key"][i], c["supp_key"][i], 1000 + i % 9000,
+                                                         _money(c["supply_cost"][i])))
+    else:
+        raise ValueError(kind)
+    return ("\n".join(out) + ("\n" if out else "")).encode()
+
+
+def parse_tbl_cpu(kind, text):
+    """The loader's contract restated on the CPU: the kept fields of every row as numpy
+    columns in the engine's encoding."""
+    keep = {"lineitem": [(0, "order_key", "i"), (1, "part_key", "i"), (2, "supp_key", "i"), (4, "quantity", "q"),
+                         (5, "ext_price", "m"), (6, "discount", "m"), (7, "tax", "m"), (8, "flag", "r"),
+                         (9, "status", "s"), (10, "ship_date", "d")],
+            "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d")],
+            "customer": [(0, "cust_key", "i"), (6, "segment", "g")],
+            "part": [(0, "part_key", "i"), (1, "flag", "n")],
+            "supplier": [(0, "supp_key", "i"), (3, "nation", "i")],
+            "partsupp": [(0, "part_key", "i"), (1, "supp_key", "i"), (3, "supply_cost", "m")]}[kind]
+
+    def money(s):
+        neg = s.startswith("-")
+        ip, _, fp = s.lstrip("-").partition(".")
+        v = int(ip) * 100 + (int((fp + "00")[:2]) if fp else 0)
+        return -v if neg else v
+
+    conv = {"i": int, "q": lambda s: money(s) // 100, "m": money, "r": _FLAGS.index, "s": _STATUS.index,
+            "d": lambda s: (_dt.date.fromisoformat(s) - _EPOCH).days, "g": _SEGMENTS.index,
+            "n": lambda s: int("green" in s)}
+    rows = [l.rstrip("\r").split("|") for l in text.decode().split("\n") if l != ""]
+    return {name: [conv[t](r[f]) for r in rows] for f, name, t in keep}

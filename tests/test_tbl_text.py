@@ -1,0 +1,23 @@
+"""The .tbl text layout used by the loader's tests, on the CPU: formatting the engine's
+columns as dbgen rows and parsing them back (the CPU restatement of the loader's contract)
+is the identity, and hand-written rows parse to known values."""
+import numpy as np
+
+import oracle_py as orc
+
+
+def test_format_parse_round_trip_cpu():
+    li = orc.lineitem(2000, seed=5, n_orders=500, order_mode=1, n_parts=300, n_supp=40,
+                      cols=("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag",
+                            "status", "ship_date"))
+    got = orc.parse_tbl_cpu("lineitem", orc.format_tbl("lineitem", li))
+    for k, v in li.items():
+        assert np.array_equal(np.asarray(got[k]), v), k
+
+
+def test_hand_written_rows_cpu():
+    text = (b"7|11|3|1|17|1234.50|0.05|0.08|R|F|1992-01-01|x|y|z|w|c|\r\n"
+            b"9|12|4|2|3|-0.5|0.1|0.00|N|O|1996-02-29|x|y|z|w|c|")
+    got = orc.parse_tbl_cpu("lineitem", text)
+    assert got["ext_price"] == [123450, -50] and got["discount"] == [5, 10] and got["tax"] == [8, 0]
+    assert got["ship_date"] == [0, 1520] and got["flag"] == [2, 1] and got["status"] == [0, 1]
