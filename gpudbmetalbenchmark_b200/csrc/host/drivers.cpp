@@ -30,10 +30,57 @@ struct Lineitem {
   gpudb_lineitem li{};
 };
 
-// The fact columns a pipeline needs; device-resident, or pinned host memory when streamed.
+// Column id -> (position in gpudb_tbl_parse's lineitem columns, width).
+std::pair<int, int> li_tbl_column(int32_t id) {
+  switch (id) {
+    case GPUDB_COL_LI_ORDER_KEY: return {0, 4};
+    case GPUDB_COL_LI_PART_KEY: return {1, 4};
+    case GPUDB_COL_LI_SUPP_KEY: return {2, 4};
+    case GPUDB_COL_LI_QUANTITY: return {3, 4};
+    case GPUDB_COL_LI_EXT_PRICE: return {4, 8};
+    case GPUDB_COL_LI_DISCOUNT: return {5, 4};
+    case GPUDB_COL_LI_TAX: return {6, 4};
+    case GPUDB_COL_LI_FLAG: return {7, 1};
+    case GPUDB_COL_LI_STATUS: return {8, 1};
+    default: return {9, 4};   // ship date
+  }
+}
+
+void set_li_column(gpudb_lineitem& li, int32_t id, void* p) {
+  switch (id) {
+    case GPUDB_COL_LI_SHIP_DATE: li.ship_date = (const int32_t*)p; break;
+    case GPUDB_COL_LI_QUANTITY: li.quantity = (const int32_t*)p; break;
+    case GPUDB_COL_LI_EXT_PRICE: li.ext_price = (const int64_t*)p; break;
+    case GPUDB_COL_LI_DISCOUNT: li.discount = (const int32_t*)p; break;
+    case GPUDB_COL_LI_TAX: li.tax = (const int32_t*)p; break;
+    case GPUDB_COL_LI_FLAG: li.flag = (const uint8_t*)p; break;
+    case GPUDB_COL_LI_STATUS: li.status = (const uint8_t*)p; break;
+    case GPUDB_COL_LI_ORDER_KEY: li.order_key = (const int32_t*)p; break;
+    case GPUDB_COL_LI_PART_KEY: li.part_key = (const int32_t*)p; break;
+    case GPUDB_COL_LI_SUPP_KEY: li.supp_key = (const int32_t*)p; break;
+  }
+}
+
+// The fact columns a pipeline needs: generated (device-resident, or pinned host memory when
+// streamed), or parsed from <data_dir>/lineitem.tbl into device memory.
 Lineitem make_lineitem(gpudb_ctx* ctx, const RunOptions& o, std::initializer_list<int32_t> ids, int32_t order_mode,
                        int64_t n_orders, int64_t n_parts, int64_t n_supp) {
   Lineitem L;
+  if (!o.data_dir.empty()) {
+    std::vector<int> keep, widths;
+    for (int32_t id : ids) {
+      keep.push_back(li_tbl_column(id).first);
+      widths.push_back(li_tbl_column(id).second);
+    }
+    TblTable t = load_tbl(ctx, o.data_dir, "lineitem", GPUDB_TBL_LINEITEM, keep, widths, o.tbl_piece);
+    L.li.n_rows = t.rows;
+    L.li.location = GPUDB_MEM_DEVICE;
+    L.li.order_key_max = t.col_max[0];
+    for (int32_t id : ids) set_li_column(L.li, id, t.cols[li_tbl_column(id).first].as<void>());
+    for (auto& b : t.cols)
+      if (b.bytes()) L.cols.push_back(std::move(b));
+    return L;
+  }
   gpudb_gen_spec spec{};
   spec.seed = o.seed;
   spec.n_rows = o.scale.lineitem;
@@ -47,22 +94,13 @@ Lineitem make_lineitem(gpudb_ctx* ctx, const RunOptions& o, std::initializer_lis
   L.li.order_key_max = n_orders > 0 ? (int32_t)(4 * (n_orders - 1) + 1) : -1;
   for (int32_t id : ids) {
     L.cols.push_back(generate(ctx, spec, id, loc));
-    void* p = L.cols.back().as<void>();
-    switch (id) {
-      case GPUDB_COL_LI_SHIP_DATE: L.li.ship_date = (const int32_t*)p; break;
-      case GPUDB_COL_LI_QUANTITY: L.li.quantity = (const int32_t*)p; break;
-      case GPUDB_COL_LI_EXT_PRICE: L.li.ext_price = (const int64_t*)p; break;
-      case GPUDB_COL_LI_DISCOUNT: L.li.discount = (const int32_t*)p; break;
-      case GPUDB_COL_LI_TAX: L.li.tax = (const int32_t*)p; break;
-      case GPUDB_COL_LI_FLAG: L.li.flag = (const uint8_t*)p; break;
-      case GPUDB_COL_LI_STATUS: L.li.status = (const uint8_t*)p; break;
-      case GPUDB_COL_LI_ORDER_KEY: L.li.order_key = (const int32_t*)p; break;
-      case GPUDB_COL_LI_PART_KEY: L.li.part_key = (const int32_t*)p; break;
-      case GPUDB_COL_LI_SUPP_KEY: L.li.supp_key = (const int32_t*)p; break;
-    }
+    set_li_column(L.li, id, L.cols.back().as<void>());
   }
   return L;
 }
+
+void q9_report(gpudb_ctx* ctx, const RunOptions& o, const gpudb_part& pa, const gpudb_supplier& su,
+               const gpudb_partsupp& pt, const gpudb_orders& orr, const Lineitem& L, double gen_ms);
 
 void header(const RunOptions& o, const char* q, uint64_t rows, const gpudb_timing& t, const char* suffix = "") {
   if (o.scale.streamed)
@@ -129,25 +167,36 @@ void runQ3Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("\n--- Running TPC-H Query 3 Benchmark ---\n");
   const Scale& s = o.scale;
   double t0 = now_ms();
-  gpudb_gen_spec cs{};
-  cs.seed = o.seed;
-  cs.n_rows = s.customer;
-  Buffer ck = generate(ctx, cs, GPUDB_COL_CU_CUST_KEY, GPUDB_MEM_DEVICE);
-  Buffer cg = generate(ctx, cs, GPUDB_COL_CU_SEGMENT, GPUDB_MEM_DEVICE);
-  gpudb_gen_spec os = cs;
-  os.n_rows = s.orders;
-  os.n_cust = (int64_t)s.customer;
-  Buffer ok = generate(ctx, os, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
-  Buffer oc = generate(ctx, os, GPUDB_COL_OR_CUST_KEY, GPUDB_MEM_DEVICE);
-  Buffer od = generate(ctx, os, GPUDB_COL_OR_ORDER_DATE, GPUDB_MEM_DEVICE);
+  gpudb_customer cu{};
+  gpudb_orders orr{};
+  TblTable ct, ot;
+  Buffer ck, cg, ok, oc, od;
+  if (!o.data_dir.empty()) {
+    ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0, 1}, {4, 1}, o.tbl_piece);
+    ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 1, 2}, {4, 4, 4}, o.tbl_piece);
+    cu = {ct.rows, ct.col_max[0], 0, ct.col<int32_t>(0), ct.col<uint8_t>(1)};
+    orr = {ot.rows, ot.col_max[0], ot.col_max[1], ot.col<int32_t>(0), ot.col<int32_t>(1), ot.col<int32_t>(2)};
+  } else {
+    gpudb_gen_spec cs{};
+    cs.seed = o.seed;
+    cs.n_rows = s.customer;
+    ck = generate(ctx, cs, GPUDB_COL_CU_CUST_KEY, GPUDB_MEM_DEVICE);
+    cg = generate(ctx, cs, GPUDB_COL_CU_SEGMENT, GPUDB_MEM_DEVICE);
+    gpudb_gen_spec os = cs;
+    os.n_rows = s.orders;
+    os.n_cust = (int64_t)s.customer;
+    ok = generate(ctx, os, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
+    oc = generate(ctx, os, GPUDB_COL_OR_CUST_KEY, GPUDB_MEM_DEVICE);
+    od = generate(ctx, os, GPUDB_COL_OR_ORDER_DATE, GPUDB_MEM_DEVICE);
+    cu = {s.customer, (int32_t)s.customer - 1, 0, ck.as<int32_t>(), cg.as<uint8_t>()};
+    orr = {s.orders, (int32_t)(4 * (s.orders - 1) + 1), (int32_t)s.customer - 1, ok.as<int32_t>(), oc.as<int32_t>(),
+           od.as<int32_t>()};
+  }
   Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_SHIP_DATE, GPUDB_COL_LI_EXT_PRICE,
                                       GPUDB_COL_LI_DISCOUNT}, GPUDB_ORDERS_CLUSTERED, (int64_t)s.orders, 0, 0);
   const double gen_ms = now_ms() - t0;
-  std::printf("Loaded %" PRIu64 " customers, %" PRIu64 " orders, %" PRIu64 " lineitem rows.\n", s.customer, s.orders,
-              s.lineitem);
-  gpudb_customer cu{s.customer, (int32_t)s.customer - 1, 0, ck.as<int32_t>(), cg.as<uint8_t>()};
-  gpudb_orders orr{s.orders, (int32_t)(4 * (s.orders - 1) + 1), (int32_t)s.customer - 1, ok.as<int32_t>(),
-                   oc.as<int32_t>(), od.as<int32_t>()};
+  std::printf("Loaded %" PRIu64 " customers, %" PRIu64 " orders, %" PRIu64 " lineitem rows.\n", cu.n_rows, orr.n_rows,
+              L.li.n_rows);
   for (int mode : {GPUDB_JOIN_GLOBAL, GPUDB_JOIN_RADIX}) {
     gpudb_q3_params p{1, 1170, 1170, 10, mode, 0};
     gpudb_q3_result r{};
@@ -171,6 +220,22 @@ void runQ3Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
 void runQ9Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("\n--- Running TPC-H Query 9 Benchmark ---\n");
   const Scale& s = o.scale;
+  if (!o.data_dir.empty()) {
+    double t0 = now_ms();
+    TblTable pt = load_tbl(ctx, o.data_dir, "part", GPUDB_TBL_PART, {0, 1}, {4, 1}, o.tbl_piece);
+    TblTable st = load_tbl(ctx, o.data_dir, "supplier", GPUDB_TBL_SUPPLIER, {0, 1}, {4, 1}, o.tbl_piece);
+    TblTable pst = load_tbl(ctx, o.data_dir, "partsupp", GPUDB_TBL_PARTSUPP, {0, 1, 2}, {4, 4, 8}, o.tbl_piece);
+    TblTable ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 2}, {4, 4}, o.tbl_piece);
+    Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_PART_KEY, GPUDB_COL_LI_SUPP_KEY, GPUDB_COL_LI_ORDER_KEY,
+                                        GPUDB_COL_LI_EXT_PRICE, GPUDB_COL_LI_DISCOUNT, GPUDB_COL_LI_QUANTITY},
+                               GPUDB_ORDERS_UNIFORM, 0, 0, 0);
+    gpudb_part pa{pt.rows, pt.col_max[0], 0, pt.col<int32_t>(0), pt.col<uint8_t>(1)};
+    gpudb_supplier su{st.rows, st.col_max[0], 0, st.col<int32_t>(0), st.col<uint8_t>(1)};
+    gpudb_partsupp pp{pst.rows, pst.col<int32_t>(0), pst.col<int32_t>(1), pst.col<int64_t>(2)};
+    gpudb_orders orr{ot.rows, ot.col_max[0], 0, ot.col<int32_t>(0), nullptr, ot.col<int32_t>(2)};
+    q9_report(ctx, o, pa, su, pp, orr, L, now_ms() - t0);
+    return;
+  }
   double t0 = now_ms();
   gpudb_gen_spec ps{};
   ps.seed = o.seed;
@@ -199,6 +264,13 @@ void runQ9Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   gpudb_supplier su{s.supplier, (int32_t)s.supplier - 1, 0, sk.as<int32_t>(), sn.as<uint8_t>()};
   gpudb_partsupp pt{4 * s.part, psp.as<int32_t>(), pssk.as<int32_t>(), psc.as<int64_t>()};
   gpudb_orders orr{s.orders, (int32_t)(4 * (s.orders - 1) + 1), 0, ok.as<int32_t>(), nullptr, od.as<int32_t>()};
+  q9_report(ctx, o, pa, su, pt, orr, L, gen_ms);
+}
+
+namespace {
+
+void q9_report(gpudb_ctx* ctx, const RunOptions& o, const gpudb_part& pa, const gpudb_supplier& su,
+               const gpudb_partsupp& pt, const gpudb_orders& orr, const Lineitem& L, double gen_ms) {
   std::vector<gpudb_q9_group> groups(4096);
   uint32_t n = 0;
   gpudb_timing t{};
@@ -217,12 +289,16 @@ void runQ9Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
+}  // namespace
+
 void runSelectionBenchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("--- Running Selection Benchmark ---\n");
+  RunOptions od = o;
+  od.scale.streamed = false;   // a device column
+  Lineitem L = make_lineitem(ctx, od, {GPUDB_COL_LI_SHIP_DATE}, GPUDB_ORDERS_NONE, 0, 0, 0);
   gpudb_gen_spec spec{};
-  spec.seed = o.seed;
-  spec.n_rows = o.scale.lineitem;
-  Buffer col = generate(ctx, spec, GPUDB_COL_LI_SHIP_DATE, GPUDB_MEM_DEVICE);
+  spec.n_rows = L.li.n_rows;
+  const Buffer& col = L.cols[0];
   Buffer bits(ctx, ((spec.n_rows + 31) / 32) * 4, GPUDB_MEM_DEVICE);
   std::printf("Loaded %" PRIu64 " rows for selection.\n", spec.n_rows);
   for (int32_t v : {100, 1000, 2000}) {
@@ -240,10 +316,12 @@ void runSelectionBenchmark(gpudb_ctx* ctx, const RunOptions& o) {
 
 void runAggregationBenchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("--- Running Aggregation Benchmark ---\n");
+  RunOptions od = o;
+  od.scale.streamed = false;   // a device column
+  Lineitem L = make_lineitem(ctx, od, {GPUDB_COL_LI_QUANTITY}, GPUDB_ORDERS_NONE, 0, 0, 0);
   gpudb_gen_spec spec{};
-  spec.seed = o.seed;
-  spec.n_rows = o.scale.lineitem;
-  Buffer col = generate(ctx, spec, GPUDB_COL_LI_QUANTITY, GPUDB_MEM_DEVICE);
+  spec.n_rows = L.li.n_rows;
+  const Buffer& col = L.cols[0];
   std::printf("Loaded %" PRIu64 " rows for aggregation.\n", spec.n_rows);
   int64_t sum = 0;
   gpudb_timing t{};
@@ -258,12 +336,22 @@ void runJoinBenchmark(gpudb_ctx* ctx, const RunOptions& o) {
   gpudb_gen_spec bs{};
   bs.seed = o.seed;
   bs.n_rows = o.scale.orders;
-  Buffer build = generate(ctx, bs, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
   gpudb_gen_spec ps = bs;
-  ps.n_rows = o.scale.lineitem;
-  ps.n_orders = (int64_t)o.scale.orders;
-  ps.order_mode = GPUDB_ORDERS_CLUSTERED;
-  Buffer probe = generate(ctx, ps, GPUDB_COL_LI_ORDER_KEY, GPUDB_MEM_DEVICE);
+  Buffer build, probe;
+  if (!o.data_dir.empty()) {
+    TblTable ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0}, {4}, o.tbl_piece);
+    TblTable lt = load_tbl(ctx, o.data_dir, "lineitem", GPUDB_TBL_LINEITEM, {0}, {4}, o.tbl_piece);
+    bs.n_rows = ot.rows;
+    ps.n_rows = lt.rows;
+    build = std::move(ot.cols[0]);
+    probe = std::move(lt.cols[0]);
+  } else {
+    build = generate(ctx, bs, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
+    ps.n_rows = o.scale.lineitem;
+    ps.n_orders = (int64_t)o.scale.orders;
+    ps.order_mode = GPUDB_ORDERS_CLUSTERED;
+    probe = generate(ctx, ps, GPUDB_COL_LI_ORDER_KEY, GPUDB_MEM_DEVICE);
+  }
   std::printf("Loaded %" PRIu64 " rows for build phase, %" PRIu64 " rows for probe phase.\n", bs.n_rows, ps.n_rows);
   for (int mode : {GPUDB_JOIN_GLOBAL, GPUDB_JOIN_RADIX}) {
     uint64_t m = 0;

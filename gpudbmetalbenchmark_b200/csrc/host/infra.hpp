@@ -2,15 +2,19 @@
 //
 // Mirrors the reference's src/infra.h: buffers (newBuffer / createFilledBuffer /
 // createBitmapBuffer / releaseAll, src/infra.h:173-229,499-531) become RAII DeviceBuffer /
-// HostBuffer; the .tbl loaders (src/infra.h:262-361) become the seeded generator; the
+// HostBuffer; the .tbl loaders (src/infra.h:262-361) become the seeded generator, or with
+// --data the GPU text loader (load_tbl, gpudb_tbl_parse); the
 // chunk configuration (src/infra.h:42-57) becomes gpudb_set_option(GPUDB_OPT_CHUNK_ROWS);
 // printTimingSummary (src/infra.h:511-516) keeps its exact text so the reference's
 // harness (scripts/benchmark_gpu.sh:50-60) parses our output unchanged.
 #pragma once
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -118,7 +122,81 @@ struct RunOptions {
   Scale scale;
   uint64_t seed = 42;
   int reps = 3;             // the reference times the third of three runs
+  std::string data_dir;     // non-empty: tables come from <data_dir>/<table>.tbl (dbgen text)
+  size_t tbl_piece = (size_t)1 << 30;   // bytes of text read and parsed at a time
 };
+
+// One table read from dbgen text: device columns in gpudb_tbl_parse's order for its kind
+// (only the requested ones are kept), the row count and the int32 columns' largest values.
+struct TblTable {
+  std::vector<Buffer> cols;
+  uint64_t rows = 0;
+  int32_t col_max[GPUDB_TBL_MAX_COLS];
+  template <class T> T* col(int i) const { return cols[i].bytes() ? cols[i].template as<T>() : nullptr; }
+};
+
+// Reads `dir`/`name`.tbl in pieces of about `piece` bytes that end at a line end, through
+// one pinned host buffer, and parses every piece on the GPU straight into the columns at its
+// row offset (a first pass counts the rows). `keep` marks the columns to store; `widths` are
+// their element sizes. The reference's equivalent is loadColumnsMulti (src/infra.h:262-361).
+inline TblTable load_tbl(gpudb_ctx* ctx, const std::string& dir, const char* name, int32_t table,
+                         const std::vector<int>& keep, const std::vector<int>& widths,
+                         size_t piece = (size_t)1 << 30) {
+  const std::string path = dir + "/" + name + ".tbl";
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    std::fprintf(stderr, "Cannot open: %s\n", path.c_str());
+    std::exit(1);
+  }
+  Buffer host(ctx, piece + 1, GPUDB_MEM_HOST);
+  char* buf = host.as<char>();
+  // visits the file as pieces that end at a newline (or at the end of the file)
+  auto pieces = [&](const std::function<void(const char*, size_t)>& fn) {
+    std::fseek(f, 0, SEEK_SET);
+    size_t carry = 0;
+    for (;;) {
+      const size_t got = std::fread(buf + carry, 1, piece - carry, f);
+      const size_t have = carry + got;
+      if (have == 0) break;
+      size_t cut = have;
+      if (got != 0 && have == piece) {
+        while (cut > 0 && buf[cut - 1] != '\n') cut--;
+        if (cut == 0) {
+          std::fprintf(stderr, "%s: a line longer than %zu bytes\n", path.c_str(), piece);
+          std::exit(1);
+        }
+      }
+      fn(buf, cut);
+      carry = have - cut;
+      std::memmove(buf, buf + cut, carry);
+      if (got == 0) break;   // the last piece (carry is 0: at the end of the file nothing is cut)
+    }
+  };
+  TblTable t;
+  pieces([&](const char* p, size_t n) {
+    uint64_t r = 0;
+    check(ctx, gpudb_tbl_count_rows(ctx, p, n, GPUDB_MEM_HOST, &r), "gpudb_tbl_count_rows");
+    t.rows += r;
+  });
+  const std::vector<int>& k = keep;
+  const std::vector<int>& w = widths;
+  t.cols.resize(GPUDB_TBL_MAX_COLS);
+  for (size_t i = 0; i < k.size(); i++) t.cols[k[i]] = Buffer(ctx, t.rows * (size_t)w[i], GPUDB_MEM_DEVICE);
+  for (int i = 0; i < GPUDB_TBL_MAX_COLS; i++) t.col_max[i] = INT32_MIN;
+  uint64_t done = 0;
+  pieces([&](const char* p, size_t n) {
+    void* cols[GPUDB_TBL_MAX_COLS] = {};
+    for (size_t i = 0; i < k.size(); i++) cols[k[i]] = t.cols[k[i]].as<uint8_t>() + done * (size_t)w[i];
+    uint64_t r = 0;
+    int32_t mx[GPUDB_TBL_MAX_COLS];
+    check(ctx, gpudb_tbl_parse(ctx, table, p, n, GPUDB_MEM_HOST, cols, t.rows - done, &r, mx, nullptr),
+          "gpudb_tbl_parse");
+    for (int i = 0; i < GPUDB_TBL_MAX_COLS; i++) t.col_max[i] = std::max(t.col_max[i], mx[i]);
+    done += r;
+  });
+  std::fclose(f);
+  return t;
+}
 
 using Driver = void (*)(gpudb_ctx*, const RunOptions&);
 

@@ -3,7 +3,8 @@
 // where query is one of the registered pipelines or `all` (src/main.cpp:158-203). sf100
 // keeps the fact table in pinned host memory and streams it in chunks, like the
 // reference's SF-100 mode. Extra options: --scale F (multiply every table size), --seed N,
-// --reps N, --device N.
+// --reps N, --device N, and --data DIR: read DIR/<table>.tbl (dbgen text, parsed on the GPU)
+// instead of generating the tables (the reference reads data/SF-N/*.tbl).
 #include <cstring>
 #include <string>
 #include <utility>
@@ -14,9 +15,10 @@
 using namespace gpudb_host;
 
 static void show_help() {
-  std::printf("Usage: gpudb [sf1|sf10|sf100] [query] [--scale F] [--seed N] [--reps N] [--device N]\n");
+  std::printf("Usage: gpudb [sf1|sf10|sf100] [query] [--scale F] [--seed N] [--reps N] [--device N] [--data DIR]\n");
   std::printf("Queries: q1 q3 q6 q9 selection aggregation join all (default: all)\n");
-  std::printf("Examples:\n  gpudb            # all pipelines on SF-1\n  gpudb sf10 q1\n  gpudb sf100 q6   # streamed\n");
+  std::printf("Examples:\n  gpudb            # all pipelines on SF-1\n  gpudb sf10 q1\n  gpudb sf100 q6   # streamed\n"
+              "  gpudb q3 --data data/SF-1   # tables from dbgen .tbl files\n");
 }
 
 int main(int argc, const char* argv[]) {
@@ -32,9 +34,12 @@ int main(int argc, const char* argv[]) {
     if (a == "--seed" && i + 1 < argc) { o.seed = std::strtoull(argv[++i], nullptr, 10); continue; }
     if (a == "--reps" && i + 1 < argc) { o.reps = std::max(1, std::atoi(argv[++i])); continue; }
     if (a == "--device" && i + 1 < argc) { device = std::atoi(argv[++i]); continue; }
+    if (a == "--data" && i + 1 < argc) { o.data_dir = argv[++i]; continue; }
+    if (a == "--tbl-piece" && i + 1 < argc) { o.tbl_piece = std::max<size_t>(4096, std::strtoull(argv[++i], nullptr, 10)); continue; }
     query = a;
   }
   o.scale = scale_of(size, factor);
+  if (!o.data_dir.empty()) o.scale.streamed = false;   // parsed tables live in HBM
   const std::vector<std::pair<std::string, Driver>> pipelines = {
       {"selection", runSelectionBenchmark}, {"aggregation", runAggregationBenchmark}, {"join", runJoinBenchmark},
       {"q1", runQ1Benchmark},          {"q3", runQ3Benchmark},                {"q6", runQ6Benchmark},

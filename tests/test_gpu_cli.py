@@ -99,3 +99,53 @@ def test_cli_sf100_streams_the_fact_table(orc):
 def test_cli_unknown_query_exits_1():
     r = subprocess.run([CLI, "sf1", "q42"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unknown query" in r.stderr
+
+
+def test_cli_reads_tbl_files(orc, tmp_path):
+    """`gpudb <query> --data DIR` parses DIR/<table>.tbl on the GPU (in pieces that end at a
+    line end) and prints the same exact results as the oracle on those rows."""
+    n_or, n_cu, n_pa, n_su, n_li = 15_000, 1_500, 2_000, 100, 60_000
+    li = orc.lineitem(n_li, seed=7, n_orders=n_or, order_mode=1, n_parts=n_pa, n_supp=n_su,
+                      cols=("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag",
+                            "status", "ship_date"))
+    od = dict(order_key=orc.gen(30, n_or, 7), cust_key=orc.gen(31, n_or, 7, n_cust=n_cu), order_date=orc.gen(32, n_or, 7))
+    cu = dict(cust_key=orc.gen(20, n_cu, 7), segment=orc.gen(21, n_cu, 7))
+    pa = dict(part_key=orc.gen(40, n_pa, 7), flag=orc.gen(41, n_pa, 7))
+    su = dict(supp_key=orc.gen(50, n_su, 7), nation=orc.gen(51, n_su, 7))
+    ps = dict(part_key=orc.gen(60, 4 * n_pa, 7), supp_key=orc.gen(61, 4 * n_pa, 7, n_supp=n_su),
+              supply_cost=orc.gen(62, 4 * n_pa, 7))
+    for name, cols in (("lineitem", li), ("orders", od), ("customer", cu), ("part", pa), ("supplier", su),
+                       ("partsupp", ps)):
+        (tmp_path / (name + ".tbl")).write_bytes(orc.format_tbl(name, cols))
+    d = str(tmp_path)
+    out = run("q6", "--data", d)
+    rev = scaled(re.search(r"Total Revenue: \$(\S+)", out).group(1), 4)
+    assert (rev, int(re.search(r"Rows matched: (\d+)", out).group(1))) == orc.q6(li)
+    timing_ok(out, "Q6", n_li)
+    out = run("q1", "--data", d)
+    want = orc.q1(li)
+    cnts = [int(x) for x in re.findall(r"\|\s+(\d+)\s+\|$", out, re.M)]
+    assert sorted(cnts) == sorted(g["count"] for g in want.values())
+    out = run("q3", "--data", d)
+    top, groups = orc.q3(cu, od, li)
+    b = out.split("TPC-H Q3 Results")[1]
+    rows = re.findall(r"^\|\s+(\d+) \| \$\s*(\S+) \|\s+(\d+) \|", b, re.M)
+    assert [(int(k), int(dd), scaled(r, 4)) for k, r, dd in rows] == top
+    assert int(re.search(r"Total results found: (\d+)", b).group(1)) == groups
+    out = run("q9", "--data", d)
+    want9, n9 = orc.q9(pa, su, ps, dict(order_key=od["order_key"], order_date=od["order_date"]),
+                       {k: li[k] for k in ("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity")})
+    rows = re.findall(r"^\|\s+(\d+) \|\s+(\d+) \| \$\s*(\S+) \|$", out, re.M)
+    assert [(int(a), int(bb), scaled(c, 4)) for a, bb, c in rows] == want9[:15]
+    out = run("join", "--data", d)
+    assert [int(x) for x in re.findall(r"Found (\d+) total matches", out)] == [orc.join_count(od["order_key"],
+                                                                                                li["order_key"])] * 2
+    out = run("aggregation", "--data", d)
+    assert int(re.search(r"SUM\(l_quantity\): (-?\d+)", out).group(1)) == orc.sum_i32(li["quantity"])
+    # the same files read 64 KB at a time: rows that straddle pieces are carried over whole
+    out = run("q6", "--data", d, "--tbl-piece", "65536")
+    rev = scaled(re.search(r"Total Revenue: \$(\S+)", out).group(1), 4)
+    assert (rev, int(re.search(r"Rows matched: (\d+)", out).group(1))) == orc.q6(li)
+    out = run("q3", "--data", d, "--tbl-piece", "65536")
+    b = out.split("TPC-H Q3 Results")[1]
+    assert int(re.search(r"Total results found: (\d+)", b).group(1)) == groups
