@@ -330,7 +330,7 @@ def run_ours(args, rank, world, local):
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded generator, inputs larger than L2)",
             "config": {"workload": "config 1: Q6-like filtered sum (1a) + Q1-like 6-group aggregate (1b) over a "
                                    "%d-row lineitem table per GPU" % rows,
-                       "rows_per_gpu": rows, "l2": "inputs 1.56 GB per pass > 126 MB L2, no flush needed",
+                       "rows_per_gpu": rows, "l2": "inputs %.2f GB per step > 126 MB L2, no flush needed" % (46 * rows / 1e9),
                        "parallelism": "row shards, one per GPU" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": "q1_vec_smem_kernel", "achieved": q1_gbs, "peak": peak,
                          "unit": "GB/s", "frac": q1_gbs / peak, "peak_kind": peak_kind,
