@@ -231,6 +231,7 @@ PROTOTYPES = {
     "gpudb_request_footprint": (C.c_uint64, [P(Request)]),
     "gpudb_serve_close": (C.c_int, [vp]),
     "gpudb_get_option": (C.c_int, [ctx_p, C.c_int32, P(C.c_int64)]),
+    "gpudb_selftest_bounded_wait": (C.c_int, [ctx_p, C.c_uint32, C.c_int32]),
     "gpudb_tbl_count_rows": (C.c_int, [ctx_p, vp, C.c_uint64, C.c_int32, P(C.c_uint64)]),
     "gpudb_tbl_parse": (C.c_int, [ctx_p, C.c_int32, vp, C.c_uint64, C.c_int32, P(vp), C.c_uint64, P(C.c_uint64),
                                   P(C.c_int32), P(Timing)]),

@@ -25,6 +25,7 @@ int fail(gpudb_ctx* ctx, int code, const char* fmt, ...) {
 }
 
 int cuda_fail(gpudb_ctx* ctx, cudaError_t e, const char* what) {
+  (void)cudaGetLastError();   // reported here: a later launch check must not see it again
   int code = (e == cudaErrorMemoryAllocation) ? GPUDB_E_OOM : GPUDB_E_CUDA;
   return fail(ctx, code, "%s: %s", what, cudaGetErrorString(e));
 }
@@ -139,6 +140,9 @@ Call::~Call() {
 }
 
 int Call::begin(size_t result_bytes) {
+  // a non-sticky error left by earlier, unrelated runtime calls is not this call's (a
+  // sticky one still shows at this call's first launch)
+  (void)cudaGetLastError();
   big_ = kSlotHeader + result_bytes > kSlotBytes;
   if (kSlotHeader + result_bytes > (big_ ? kBigSlotBytes : kSlotBytes))
     return fail(ctx_, GPUDB_E_INVALID, "result too large");

@@ -389,6 +389,13 @@ int gpudb_tbl_parse(gpudb_ctx* ctx, int32_t table, const char* text, uint64_t by
                     void* const* cols, uint64_t capacity, uint64_t* n_rows, int32_t* col_max,
                     gpudb_timing* t);
 
+/* ---- self-test of the bounded device waits (no reference counterpart) ---------------------
+ * One warp waits on a shared-memory mbarrier through the same bounded wait the TMA scan
+ * kernels use. arrive != 0: a thread arrives first, the call returns GPUDB_OK. arrive == 0:
+ * nothing arrives, the wait gives up after `polls` polls (1..2^26; it also stops after 2 s)
+ * and the call returns GPUDB_E_TIMEOUT with the context still usable. */
+int gpudb_selftest_bounded_wait(gpudb_ctx* ctx, uint32_t polls, int32_t arrive);
+
 /* ---- autotuner (no reference counterpart) --------------------------------------------
  * gpudb_autotune times the candidate settings of one request's pipeline on the request's
  * own tables (reps runs each, median device time) and sets the fastest on the context:
