@@ -79,3 +79,36 @@ def test_two_rank_shards_add_up_to_the_whole_table(orc):
             for f, x in v.items():
                 m[f] += x
     assert merged == orc.q1(whole)
+
+
+def _leaving_worker(rank, world, port, out):
+    import datetime
+    import torch
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    t = torch.ones(1)
+    dist.all_reduce(t)                      # step 1: both ranks
+    if rank == 1:
+        os._exit(0)                         # leaves between steps, with nothing in flight
+    try:
+        dist.all_reduce(t)                  # step 2: the peer is gone
+        out.put("completed")
+    except Exception as e:                  # noqa: BLE001 -- any error is the expected outcome
+        out.put("error: " + type(e).__name__)
+
+
+def test_a_rank_that_leaves_between_steps_fails_the_next_collective():
+    """The survivor's next collective ends with an error inside the process-group timeout
+    (5 s) instead of waiting for good."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaving_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    outcome = q.get(timeout=60)
+    for p in procs:
+        p.join(timeout=60)
+    assert outcome.startswith("error"), outcome
