@@ -20,8 +20,9 @@
 //     revenue is summed with a warp prefix scan, so each run costs one 64-bit atomicAdd.
 //     ext_price and discount are loaded only for rows that passed the date filter and found
 //     their order (late materialisation).
-//  6. q3_topk_slots_kernel: block top-k over each 4096-slot tile of the live table, then the
-//     last block to finish merges the tiles' winners (one launch).
+//  6. q3_hist_kernel: groups and a log-scale revenue histogram of the live table.
+//  7. q3_select_kernel: the slots in the histogram bins that can hold the top-k are
+//     appended, and the last block to finish ranks them.
 // Radix mode partitions both sides by key hash and joins each partition in shared memory
 // (radix.cu).
 #include <algorithm>
@@ -189,51 +190,22 @@ __global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict
   }
 }
 
-// Top-k of the table: block b takes slots [b*4096, +4096) (and counts groups), writes its
-// k best to cand[b*k..]; the last block to finish then merges the candidates of the live
-// tiles (the table holds *cap_p slots) in chunks, carrying the running top-k, into out.
-__global__ void __launch_bounds__(kTopkThreads) q3_topk_slots_kernel(const Q3Slot* __restrict__ ht,
-                                                                     const uint32_t* __restrict__ hits,
-                                                                     const uint32_t* cap_p, int k, u128* cand,
-                                                                     unsigned long long* groups, unsigned* ticket,
-                                                                     u128* out) {
+// Top-k of the table: the revenue histogram pass, then the select-and-rank pass
+// (q3_table_hist / q3_table_select).
+__global__ void __launch_bounds__(kTopkThreads) q3_hist_kernel(const Q3Slot* __restrict__ ht,
+                                                               const uint32_t* __restrict__ hits, const uint32_t* cap_p,
+                                                               uint32_t* state, unsigned long long* groups) {
+  __shared__ uint32_t sh[kRevBins];
+  q3_table_hist(ht, hits, *cap_p, state, groups, sh);
+}
+
+__global__ void __launch_bounds__(kTopkThreads) q3_select_kernel(const Q3Slot* __restrict__ ht,
+                                                                 const uint32_t* __restrict__ hits,
+                                                                 const uint32_t* cap_p, int k, uint32_t* state,
+                                                                 u128* cand, u128* out) {
   __shared__ u128 sm[kTopkScratch];
   __shared__ u128 carry[GPUDB_Q3_MAX_K];
-  const uint32_t cap = *cap_p;
-  u128 v[kTopkPerThread];
-  if ((uint64_t)blockIdx.x * kTopkTile < cap) {   // blocks past the live table have no work
-    uint32_t cnt = 0;
-    const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
-#pragma unroll
-    for (int j = 0; j < kTopkPerThread; j++) {
-      v[j] = 0;
-      const uint64_t s = base + j;
-      if (s < cap && hits[s]) {
-        v[j] = topk_compose((int64_t)ht[s].rev, ht[s].date, ht[s].key);
-        cnt++;
-      }
-    }
-    cnt = __reduce_add_sync(FULL_MASK, cnt);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(groups, (unsigned long long)cnt);
-    block_topk(v, k, cand + (size_t)blockIdx.x * k, sm);
-  }
-  if (!grid_last_block(ticket)) return;
-  // merge: live tiles' candidates, kTopkTile - k per chunk plus the carried top-k
-  const uint64_t n = ((uint64_t)cap + kTopkTile - 1) / kTopkTile * k;
-  const uint64_t per = (uint64_t)kTopkTile - k;
-  for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
-  __syncthreads();
-  for (uint64_t c0 = 0; c0 < n; c0 += per) {
-#pragma unroll
-    for (int j = 0; j < kTopkPerThread; j++) {
-      const uint64_t idx = (uint64_t)threadIdx.x * kTopkPerThread + j;   // position in this chunk
-      if (idx < (uint64_t)k) v[j] = carry[idx];
-      else v[j] = (c0 + idx - k < n) ? ld_cg_u128(cand + c0 + idx - k) : (u128)0;
-    }
-    __syncthreads();
-    block_topk(v, k, carry, sm);
-  }
-  for (int i = threadIdx.x; i < k; i += kTopkThreads) out[i] = carry[i];
+  q3_table_select(ht, hits, *cap_p, k, state, cand, out, sm, carry);
 }
 
 // ---- radix mode ----------------------------------------------------------------------
@@ -424,15 +396,16 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   if (!rc) rc = scratch(ctx, "q3.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q3.ht", (size_t)max_cap * sizeof(Q3Slot), &ht);
   if (!rc) rc = scratch(ctx, "q3.hits", (size_t)max_cap * 4, &hits);
-  const uint64_t tiles = (max_cap + kTopkTile - 1) / kTopkTile;
-  const size_t cand_elems = tiles * (size_t)p.k;
-  if (!rc) rc = scratch(ctx, "q3.cand", (cand_elems * 2 + 64) * sizeof(u128), &cand);
+  void* tstate;
+  if (!rc) rc = scratch(ctx, "q3.topk", (size_t)kTopkStateWords * 4, &tstate);
+  if (!rc) rc = scratch(ctx, "q3.cand", (size_t)kTopkCandCap * sizeof(u128), &cand);
   if (rc) return rc;
   uint32_t* cnt = static_cast<uint32_t*>(count);
   uint32_t* cap = cnt + 1;
   GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
   GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));   // [0] count, [1] capacity, [2] okbm off, [3] ticket
   if (use_okbm) GPUDB_CUDA(ctx, cudaMemsetAsync(okbm, 0, okbm_bytes, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(tstate, 0, (size_t)kTopkStateWords * 4, s));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
   if (cu.n_rows)
@@ -462,8 +435,11 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   u128* cbuf = static_cast<u128*>(cand);
   unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
   u128* rows = reinterpret_cast<u128*>(result + 16);
-  GPUDB_LAUNCH(call, q3_topk_slots_kernel, (unsigned)tiles, kTopkThreads, 0, (const Q3Slot*)ht, (const uint32_t*)hits,
-               (const uint32_t*)cap, p.k, cbuf, groups, (unsigned*)(cnt + 3), rows);
+  uint32_t* ts = static_cast<uint32_t*>(tstate);
+  GPUDB_LAUNCH(call, q3_hist_kernel, q3_topk_grid(max_cap, sms, 1, 4), kTopkThreads, 0, (const Q3Slot*)ht, (const uint32_t*)hits,
+               (const uint32_t*)cap, ts, groups);
+  GPUDB_LAUNCH(call, q3_select_kernel, q3_topk_grid(max_cap, sms, 1, 2), kTopkThreads, 0, (const Q3Slot*)ht, (const uint32_t*)hits,
+               (const uint32_t*)cap, p.k, ts, cbuf, rows);
   return GPUDB_OK;
 }
 

@@ -14,8 +14,8 @@
 //     probes its table, and the run's revenue over the rows passing that request's ship
 //     bound goes to the slot with one atomicAdd. ext_price/discount are loaded only for
 //     rows that joined some request.
-//  6. q3m_topk_kernel: block top-k over each request's table tiles (blockIdx.y), then the
-//     last block of the request merges its tiles' winners.
+//  6. q3m_hist_kernel / q3m_select_kernel: per request (blockIdx.y), the two top-k passes of
+//     the single Q3 (revenue histogram, then select and rank).
 // Results are the same as running each request alone (integer sums, the same top-k order).
 #include <algorithm>
 #include <cstring>
@@ -52,8 +52,8 @@ struct Q3Multi {
   int32_t* sdate;
   uint32_t* smask;
   uint32_t* n_stage;
-  u128* cand;                                 // per request: tiles * k candidates
-  uint32_t tiles;
+  u128* cand;                                 // per request: kTopkCandCap top-k candidates
+  uint32_t* tstate;                           // per request: kTopkStateWords (histogram, count, ticket)
   uint32_t* status;                           // per request status words
   uint32_t* dstatus;                          // per distinct segment status words
   uint8_t* res;                               // per request kReqBytes
@@ -233,50 +233,21 @@ __global__ void __launch_bounds__(256) q3m_probe_kernel(const int32_t* __restric
   }
 }
 
-__global__ void __launch_bounds__(kTopkThreads) q3m_topk_kernel(Q3Multi m) {
+__global__ void __launch_bounds__(kTopkThreads) q3m_hist_kernel(Q3Multi m) {
+  __shared__ uint32_t sh[kRevBins];
+  const int r = blockIdx.y;
+  q3_table_hist(m.ht + (size_t)r * m.max_cap, m.hits + (size_t)r * m.max_cap, m.cnt[4 * r + 1],
+                m.tstate + (size_t)r * kTopkStateWords, reinterpret_cast<unsigned long long*>(m.res + (size_t)r * kReqBytes),
+                sh);
+}
+
+__global__ void __launch_bounds__(kTopkThreads) q3m_select_kernel(Q3Multi m) {
   __shared__ u128 sm[kTopkScratch];
   __shared__ u128 carry[GPUDB_Q3_MAX_K];
-  const int r = blockIdx.y, k = m.k[r];
-  const uint32_t cap = m.cnt[4 * r + 1];
-  const Q3Slot* ht = m.ht + (size_t)r * m.max_cap;
-  const uint32_t* hits = m.hits + (size_t)r * m.max_cap;
-  u128* cand = m.cand + (size_t)r * m.tiles * GPUDB_Q3_MAX_K;
-  uint8_t* res = m.res + (size_t)r * kReqBytes;
-  unsigned long long* groups = reinterpret_cast<unsigned long long*>(res);
-  u128 v[kTopkPerThread];
-  if ((uint64_t)blockIdx.x * kTopkTile < cap) {
-    uint32_t cnt = 0;
-    const uint64_t base = (uint64_t)blockIdx.x * kTopkTile + (uint64_t)threadIdx.x * kTopkPerThread;
-#pragma unroll
-    for (int j = 0; j < kTopkPerThread; j++) {
-      v[j] = 0;
-      const uint64_t s = base + j;
-      if (s < cap && hits[s]) {
-        v[j] = topk_compose((int64_t)ht[s].rev, ht[s].date, ht[s].key);
-        cnt++;
-      }
-    }
-    cnt = __reduce_add_sync(FULL_MASK, cnt);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(groups, (unsigned long long)cnt);
-    block_topk(v, k, cand + (size_t)blockIdx.x * k, sm);
-  }
-  if (!grid_last_block(m.cnt + 4 * r + 3)) return;
-  const uint64_t n = ((uint64_t)cap + kTopkTile - 1) / kTopkTile * k;
-  const uint64_t per = (uint64_t)kTopkTile - k;
-  for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
-  __syncthreads();
-  for (uint64_t c0 = 0; c0 < n; c0 += per) {
-#pragma unroll
-    for (int j = 0; j < kTopkPerThread; j++) {
-      const uint64_t idx = (uint64_t)threadIdx.x * kTopkPerThread + j;
-      if (idx < (uint64_t)k) v[j] = carry[idx];
-      else v[j] = (c0 + idx - k < n) ? ld_cg_u128(cand + c0 + idx - k) : (u128)0;
-    }
-    __syncthreads();
-    block_topk(v, k, carry, sm);
-  }
-  u128* rows = reinterpret_cast<u128*>(res + 16);
-  for (int i = threadIdx.x; i < k; i += kTopkThreads) rows[i] = carry[i];
+  const int r = blockIdx.y;
+  q3_table_select(m.ht + (size_t)r * m.max_cap, m.hits + (size_t)r * m.max_cap, m.cnt[4 * r + 1], m.k[r],
+                  m.tstate + (size_t)r * kTopkStateWords, m.cand + (size_t)r * kTopkCandCap,
+                  reinterpret_cast<u128*>(m.res + (size_t)r * kReqBytes + 16), sm, carry);
 }
 
 }  // namespace
@@ -319,7 +290,6 @@ int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t
   while (max_cap < (n_or << ctx->ht_shift) && max_cap < (1u << 31)) max_cap <<= 1;
   m.max_cap = max_cap;
   m.shift = ctx->ht_shift;
-  m.tiles = (max_cap + kTopkTile - 1) / kTopkTile;
   m.words = (uint32_t)((uint32_t)cu.key_max >> 5) + 1;
   const bool use_okbm = od.key_max >= 0;
   m.okwords = use_okbm ? (uint32_t)((uint32_t)od.key_max >> 5) + 1 : 0;
@@ -342,7 +312,9 @@ int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t
   if (!rc) rc = scratch(ctx, "q3m.count", 256, &cnt);
   if (!rc) rc = scratch(ctx, "q3m.ht", (size_t)K * max_cap * sizeof(Q3Slot), &ht);
   if (!rc) rc = scratch(ctx, "q3m.hits", (size_t)K * max_cap * 4, &hits);
-  if (!rc) rc = scratch(ctx, "q3m.cand", (size_t)K * m.tiles * GPUDB_Q3_MAX_K * sizeof(u128), &cand);
+  void* tstate = nullptr;
+  if (!rc) rc = scratch(ctx, "q3m.topk", (size_t)K * kTopkStateWords * 4, &tstate);
+  if (!rc) rc = scratch(ctx, "q3m.cand", (size_t)K * kTopkCandCap * sizeof(u128), &cand);
   if (rc) return rc;
   m.bm = static_cast<uint32_t*>(bm);
   m.okbm = static_cast<uint32_t*>(okbm);
@@ -354,9 +326,11 @@ int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t
   m.ht = static_cast<Q3Slot*>(ht);
   m.hits = static_cast<uint32_t*>(hits);
   m.cand = static_cast<u128*>(cand);
+  m.tstate = static_cast<uint32_t*>(tstate);
   GPUDB_CUDA(ctx, cudaMemsetAsync(bm, 0, (size_t)m.D * m.words * 4, s));
   if (use_okbm) GPUDB_CUDA(ctx, cudaMemsetAsync(okbm, 0, (size_t)K * m.okwords * 4, s));
   GPUDB_CUDA(ctx, cudaMemsetAsync(cnt, 0, (4 * kB + 1) * 4, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(tstate, 0, (size_t)K * kTopkStateWords * 4, s));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
   GPUDB_LAUNCH(call, q3m_bitmap_kernel, dim3(grid(cu.n_rows), m.D), 256, 0, cu.cust_key, cu.segment, cu.n_rows, cu.key_max, m);
@@ -367,7 +341,8 @@ int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t
   const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((li.n_rows + 255) / 256, (uint64_t)sms * 8));
   if (li.n_rows)
     GPUDB_LAUNCH(call, q3m_probe_kernel, g, 256, 0, li.order_key, li.ship_date, li.ext_price, li.discount, li.n_rows, m);
-  GPUDB_LAUNCH(call, q3m_topk_kernel, dim3(m.tiles, K), kTopkThreads, 0, m);
+  GPUDB_LAUNCH(call, q3m_hist_kernel, dim3(q3_topk_grid(max_cap, sms, K, 4), K), kTopkThreads, 0, m);
+  GPUDB_LAUNCH(call, q3m_select_kernel, dim3(q3_topk_grid(max_cap, sms, K, 2), K), kTopkThreads, 0, m);
   std::vector<uint32_t> idv = ids;
   std::vector<int32_t> req_seg(m.req_seg, m.req_seg + K);
   return call.finish(bytes, [ctx, reqs, idv, req_seg, st_bytes](const uint8_t* h) {

@@ -65,18 +65,29 @@ __global__ void year_map_kernel(const int32_t* __restrict__ keys, const int32_t*
   }
 }
 
-__global__ void ps_filter_kernel(const int32_t* __restrict__ part, uint64_t n, const uint32_t* __restrict__ bits,
-                                 int32_t part_max, uint32_t* stage, uint32_t* count) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t end = (n + 31) & ~31ull;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
-    bool take = false;
-    if (i < n) {
-      const int32_t p = part[i];
-      take = p >= 0 && p <= part_max && bitmap_test(bits, p);
+constexpr int kPsRows = 4;   // rows per thread per block step of ps_filter_kernel
+
+// Partsupp rows whose part passes the bitmap, compacted (block prefix sum, one atomicAdd
+// per 1024 rows).
+__global__ void __launch_bounds__(256) ps_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
+                                                        const uint32_t* __restrict__ bits, int32_t part_max,
+                                                        uint32_t* stage, uint32_t* count) {
+  __shared__ uint32_t sh[33];
+  const uint64_t step = (uint64_t)gridDim.x * 256 * kPsRows;
+  for (uint64_t b = (uint64_t)blockIdx.x * 256 * kPsRows; b < n; b += step) {   // whole blocks
+    uint32_t take = 0;
+#pragma unroll
+    for (int j = 0; j < kPsRows; j++) {
+      const uint64_t i = b + (uint64_t)j * 256 + threadIdx.x;
+      if (i < n) {
+        const int32_t p = part[i];
+        take |= (uint32_t)(p >= 0 && p <= part_max && bitmap_test(bits, p)) << j;
+      }
     }
-    const uint32_t pos = warp_append(take, count);
-    if (take) stage[pos] = (uint32_t)i;
+    uint32_t pos = block_reserve<256>(__popc(take), count, sh);
+#pragma unroll
+    for (int j = 0; j < kPsRows; j++)
+      if (take & (1u << j)) stage[pos++] = (uint32_t)(b + (uint64_t)j * 256 + threadIdx.x);
   }
 }
 
@@ -371,7 +382,8 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
       GPUDB_LAUNCH(call, year_map_kernel, grid(od->n_rows), 256, 0, od->order_key, od->order_date, od->n_rows,
                    order_max, (uint8_t*)year, call.status());
     if (ps->n_rows)
-      GPUDB_LAUNCH(call, ps_filter_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->n_rows, (const uint32_t*)bits,
+      GPUDB_LAUNCH(call, ps_filter_kernel, grid((ps->n_rows + kPsRows - 1) / kPsRows), 256, 0, ps->part_key, ps->n_rows,
+                   (const uint32_t*)bits,
                    part_max, (uint32_t*)stage, cnt);
     GPUDB_LAUNCH(call, ps_clear_kernel, grid(ps_max_cap), 256, 0, (const uint32_t*)cnt, ps_max_cap, ctx->ht_shift, cap,
                  (PsSlot*)pst);

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 from gpudbmetalbenchmark_b200 import capi
+from gpudbmetalbenchmark_b200.engine import q3_to_list
 
 pytestmark = pytest.mark.gpu
 
@@ -47,9 +48,22 @@ def test_q3_random_constants_and_k(engine, orc, mode):
             engine.free(t)
 
 
+def tie_tables(n_or):
+    cu = dict(cust_key=np.arange(10, dtype=np.int32), segment=np.ones(10, np.uint8))
+    od = dict(order_key=(4 * np.arange(n_or) + 1).astype(np.int32),
+              cust_key=(np.arange(n_or) % 10).astype(np.int32),
+              order_date=(np.arange(n_or) % 3).astype(np.int32))
+    li = dict(order_key=od["order_key"].copy(), ship_date=np.full(n_or, 2000, np.int32),
+              ext_price=np.full(n_or, 123456, np.int64), discount=np.full(n_or, 4, np.int32))
+    return cu, od, li
+
+
 @pytest.mark.parametrize("mode", MODES)
-def test_q3_ties_break_by_date_then_key(engine, orc, mode):
-    n_or = 5000
+@pytest.mark.parametrize("n_or", [5000, 40000])
+def test_q3_ties_break_by_date_then_key(engine, orc, mode, n_or):
+    """All revenues equal: the global table's select pass keeps every group as a candidate
+    (5000: ranked from the candidate buffer; 40000: more than the buffer holds, so the last
+    block merges the whole table)."""
     cu = dict(cust_key=np.arange(10, dtype=np.int32), segment=np.ones(10, np.uint8))
     od = dict(order_key=(4 * np.arange(n_or) + 1).astype(np.int32),
               cust_key=(np.arange(n_or) % 10).astype(np.int32),
@@ -60,6 +74,44 @@ def test_q3_ties_break_by_date_then_key(engine, orc, mode):
     got = run(engine, cu, od, li, mode, k=64)
     assert got == orc.q3(cu, od, li, k=64)
     assert [r[0] for r in got[0][:3]] == [1, 13, 25]
+
+
+def test_q3_near_ties_in_one_revenue_bin(engine, orc):
+    """Revenues within a few units of each other share a histogram bin: the select pass
+    ranks them by the full revenue, then date and key."""
+    rng = np.random.default_rng(8)
+    n_or = 30000
+    cu, od, li = tie_tables(n_or)
+    li["ext_price"] = (1_000_000 + rng.integers(0, 40, n_or)).astype(np.int64)
+    for k in (1, 10, 64):
+        assert run(engine, cu, od, li, k=k) == orc.q3(cu, od, li, k=k)
+
+
+def test_q3_batched_ties_match_oracle(engine, orc):
+    """The batched Q3 (several requests over one set of tables) runs the same select pass:
+    equal and near-equal revenues give the oracle's order for every request."""
+    import ctypes as C
+    n_or = 20000
+    cu, od, li = tie_tables(n_or)
+    li["ext_price"][::3] += 1
+    tc, to, tl = engine.upload("customer", cu), engine.upload("orders", od), engine.upload("lineitem", li)
+    try:
+        tables = capi.Q3Tables(tc.struct(), to.struct(), tl.lineitem())
+        cases = [(1, 3, 1500, 64), (1, 2, 1500, 10), (1, 1, 1999, 1), (2, 3, 1500, 5)]
+        reqs, outs = (capi.Request * len(cases))(), []
+        for i, (seg, d, s, k) in enumerate(cases):
+            reqs[i].pipeline = capi.PIPE_Q3
+            reqs[i].q3 = C.pointer(tables)
+            reqs[i].q3p = capi.Q3Params(seg, d, s, k, capi.JOIN_GLOBAL, 0)
+            outs.append(capi.Q3Result())
+            reqs[i].q3_out = C.pointer(outs[-1])
+        engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, len(cases), None, None))
+        for i, (seg, d, s, k) in enumerate(cases):
+            assert reqs[i].status == capi.OK
+            assert q3_to_list(outs[i]) == orc.q3(cu, od, li, seg, d, s, k), cases[i]
+    finally:
+        for t in (tc, to, tl):
+            engine.free(t)
 
 
 @pytest.mark.parametrize("mode", MODES)
