@@ -16,10 +16,10 @@
 //     (the group key equals the join key).
 //  5. q3_probe_kernel: one lane per fact row; runs of equal order keys (adjacent rows of one
 //     order) are found with a warp ballot, only the run head probes the table (after a test
-//     of the order-key bitmap that step 4 sets, which turns away most misses), and the run's
-//     revenue is summed with a warp prefix scan, so each run costs one 64-bit atomicAdd.
+//     of the order-key bitmap that step 4 sets, which turns away most misses), and each row
+//     that joins adds its revenue and a count with one atomic each (a few percent of rows).
 //     ext_price and discount are loaded only for rows that passed the date filter and found
-//     their order (late materialisation).
+//     their order (late materialisation); the next step's keys and dates load meanwhile.
 //  6. q3_hist_kernel: groups and a log-scale revenue histogram of the live table.
 //  7. q3_select_kernel: the slots in the histogram bins that can hold the top-k are
 //     appended, and the last block to finish ranks them.
@@ -48,23 +48,23 @@ __global__ void __launch_bounds__(256) orders_filter_kernel(const int32_t* __res
   const uint64_t step = (uint64_t)gridDim.x * 256 * kFilterRows;
   // whole blocks stay in the loop: block_reserve needs every thread of the block
   for (uint64_t b = (uint64_t)blockIdx.x * 256 * kFilterRows; b < n; b += step) {
-    int32_t key[kFilterRows], date[kFilterRows];
-    uint32_t take = 0;
+    // the three columns load together (one memory latency per step, not three in a chain)
+    int32_t key[kFilterRows], date[kFilterRows], cust[kFilterRows];
 #pragma unroll
     for (int j = 0; j < kFilterRows; j++) {
       const uint64_t i = b + (uint64_t)j * 256 + threadIdx.x;
-      key[j] = 0;
-      date[j] = 0;
-      if (i < n) {
-        date[j] = odate[i];
-        if (date[j] < date_lt) {
-          const int32_t c = ocust[i];
-          if (c >= 0 && c <= cust_max && bitmap_test(bitmap, c)) {
-            key[j] = okey[i];
-            if (key[j] == kEmptyKey) set_status(status, ST_KEY_RANGE);
-            else take |= 1u << j;
-          }
-        }
+      const bool in = i < n;
+      date[j] = in ? ld_stream(odate + i) : date_lt;
+      cust[j] = in ? ld_stream(ocust + i) : -1;
+      key[j] = in ? ld_stream(okey + i) : 0;
+    }
+    uint32_t take = 0;
+#pragma unroll
+    for (int j = 0; j < kFilterRows; j++) {
+      const int32_t c = cust[j];
+      if (date[j] < date_lt && c >= 0 && c <= cust_max && bitmap_test(bitmap, c)) {
+        if (key[j] == kEmptyKey) set_status(status, ST_KEY_RANGE);
+        else take |= 1u << j;
       }
     }
     uint32_t pos = block_reserve<256>(__popc(take), count, sh);
@@ -126,65 +126,54 @@ __global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict
   const int lane = threadIdx.x & 31;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   constexpr int U = kProbeBatches;
-  for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U; base < n;
-       base += warps * 32 * U) {
+  const uint64_t step = warps * 32 * U;
+  uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U;
+  // the next step's keys and ship dates are loaded while this step is processed
+  int32_t nkey[U], nship[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const uint64_t row = base + u * 32 + lane;
+    nkey[u] = row < n ? ld_stream(lkey + row) : kEmptyKey;
+    nship[u] = row < n ? ld_stream(lship + row) : ship_gt;
+  }
+  for (; base < n; base += step) {
     int32_t key[U];
     bool pass[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const uint64_t row = base + u * 32 + lane;
-      const bool valid = row < n;
-      key[u] = valid ? ld_stream(lkey + row) : kEmptyKey;
-      pass[u] = valid && ld_stream(lship + row) > ship_gt;
+      key[u] = nkey[u];
+      pass[u] = nship[u] > ship_gt;
+      const uint64_t row = base + step + u * 32 + lane;
+      nkey[u] = row < n ? ld_stream(lkey + row) : kEmptyKey;
+      nship[u] = row < n ? ld_stream(lship + row) : ship_gt;
     }
     int32_t slot[U];
-    uint32_t run_mask[U];
-    int my_head[U], last[U];
-    bool head[U];
+    int my_head[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int32_t prev = __shfl_up_sync(FULL_MASK, key[u], 1);
-      head[u] = (lane == 0) || (key[u] != prev);
-      const uint32_t heads = __ballot_sync(FULL_MASK, head[u]);
+      const bool head = (lane == 0) || (key[u] != prev);
+      const uint32_t heads = __ballot_sync(FULL_MASK, head);
       const uint32_t passm = __ballot_sync(FULL_MASK, pass[u]);
-      // run = [head lane, next head); `last` = last lane of this lane's run
+      // run = [head lane, next head); probe once per run that has a passing row
       my_head[u] = 31 - __clz(heads & lanemask_le());
       const uint32_t later = heads & lanemask_gt();
-      last[u] = later ? (__ffs(later) - 2) : 31;
-      run_mask[u] = (last[u] == 31 ? 0xFFFFFFFFu : ((1u << (last[u] + 1)) - 1u)) & ~((1u << my_head[u]) - 1u);
+      const uint32_t upto = later ? (1u << (__ffs(later) - 1)) - 1u : 0xFFFFFFFFu;
       slot[u] = -1;
-      if (head[u] && (passm & run_mask[u]) && key[u] != kEmptyKey) {
+      if (head && (passm & upto & ~((1u << lane) - 1u)) && key[u] != kEmptyKey) {
         const bool maybe = !bm || (key[u] >= 0 && key[u] <= key_max && bitmap_test(bm, key[u]));
         if (maybe) slot[u] = ht_find(ht, cap, key[u]);
       }
     }
-    int64_t v[U];
+    // rows that join add their revenue and count (integer sums: the order does not matter)
 #pragma unroll
     for (int u = 0; u < U; u++) {
       slot[u] = __shfl_sync(FULL_MASK, slot[u], my_head[u]);
-      const uint64_t row = base + u * 32 + lane;
-      v[u] = 0;
-      if (pass[u] && slot[u] >= 0) v[u] = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const bool hit = pass[u] && slot[u] >= 0;
-      // inclusive prefix sum of v across the warp
-      int64_t inc = v[u];
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const int64_t o = __shfl_up_sync(FULL_MASK, inc, d);
-        if (lane >= d) inc += o;
-      }
-      const int64_t run_end = __shfl_sync(FULL_MASK, inc, last[u]);
-      const int64_t before = inc - v[u];   // exclusive prefix at this lane
-      const uint32_t hitm = __ballot_sync(FULL_MASK, hit);
-      if (head[u] && slot[u] >= 0) {
-        const uint32_t c = __popc(hitm & run_mask[u]);
-        if (c) {
-          atomicAdd(&ht[slot[u]].rev, (unsigned long long)(run_end - before));
-          atomicAdd(&hits[slot[u]], c);
-        }
+      if (pass[u] && slot[u] >= 0) {
+        const uint64_t row = base + u * 32 + lane;
+        const int64_t v = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
+        atomicAdd(&ht[slot[u]].rev, (unsigned long long)v);
+        atomicAdd(&hits[slot[u]], 1u);
       }
     }
   }

@@ -11,9 +11,9 @@
 //     the request's order-key bitmap is set.
 //  5. q3m_probe_kernel: one pass over the fact table. Runs of equal order keys are found
 //     once per warp; per request, the run head tests the request's order-key bitmap and
-//     probes its table, and the run's revenue over the rows passing that request's ship
-//     bound goes to the slot with one atomicAdd. ext_price/discount are loaded only for
-//     rows that joined some request.
+//     probes its table; each row passing that request's ship bound adds its revenue and a
+//     count to the slot. ext_price/discount are loaded only for rows that joined some
+//     request.
 //  6. q3m_hist_kernel / q3m_select_kernel: per request (blockIdx.y), the two top-k passes of
 //     the single Q3 (revenue histogram, then select and rank).
 // Results are the same as running each request alone (integer sums, the same top-k order).
@@ -88,15 +88,15 @@ __global__ void __launch_bounds__(256) q3m_orders_kernel(const int32_t* __restri
       key[j] = 0;
       date[j] = 0;
       if (i < n) {
-        date[j] = odate[i];
-        const int32_t c = ocust[i];
+        date[j] = ld_stream(odate + i);
+        const int32_t c = ld_stream(ocust + i);
+        key[j] = ld_stream(okey + i);   // with the other columns: no dependent load later
         uint32_t segs = 0;   // distinct segments whose bitmap holds the customer
         if (c >= 0 && c <= cust_max)
           for (int d = 0; d < m.D; d++) segs |= (uint32_t)bitmap_test(m.bm + (size_t)d * m.words, c) << d;
         for (int r = 0; r < m.K; r++)
           mask[j] |= (uint32_t)((date[j] < m.date_lt[r]) & ((segs >> m.req_seg[r]) & 1u)) << r;
         if (mask[j]) {
-          key[j] = okey[i];
           if (key[j] == kEmptyKey) {
             for (int r = 0; r < m.K; r++)
               if (mask[j] & (1u << r)) set_status(m.status + r, ST_KEY_RANGE);
@@ -176,19 +176,24 @@ __global__ void __launch_bounds__(256) q3m_probe_kernel(const int32_t* __restric
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n; base += warps * 32) {
+  const uint64_t step = (uint64_t)gridDim.x * (blockDim.x >> 5) * 32;
+  uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+  // the next step's key and ship date are loaded while this step is processed
+  int32_t nkey = base + lane < n ? ld_stream(lkey + base + lane) : kEmptyKey;
+  int32_t nship = base + lane < n ? ld_stream(lship + base + lane) : INT32_MIN;
+  for (; base < n; base += step) {
     const uint64_t row = base + lane;
     const bool valid = row < n;
-    const int32_t key = valid ? ld_stream(lkey + row) : kEmptyKey;
-    const int32_t ship = valid ? ld_stream(lship + row) : INT32_MIN;
+    const int32_t key = nkey, ship = nship;
+    nkey = row + step < n ? ld_stream(lkey + row + step) : kEmptyKey;
+    nship = row + step < n ? ld_stream(lship + row + step) : INT32_MIN;
     const int32_t prev = __shfl_up_sync(FULL_MASK, key, 1);
     const bool head = (lane == 0) || (key != prev);
     const uint32_t heads = __ballot_sync(FULL_MASK, head);
     const int my_head = 31 - __clz(heads & lanemask_le());
     const uint32_t later = heads & lanemask_gt();
-    const int last = later ? (__ffs(later) - 2) : 31;
-    const uint32_t run_mask = (last == 31 ? 0xFFFFFFFFu : ((1u << (last + 1)) - 1u)) & ~((1u << my_head) - 1u);
+    const uint32_t upto = later ? (1u << (__ffs(later) - 1)) - 1u : 0xFFFFFFFFu;
+    const uint32_t run_mask = upto & ~((1u << lane) - 1u);   // used by head lanes only
     int32_t slot[kB];
     uint32_t hitbits = 0;   // requests this row joins
 #pragma unroll
@@ -206,27 +211,15 @@ __global__ void __launch_bounds__(256) q3m_probe_kernel(const int32_t* __restric
       slot[r] = __shfl_sync(FULL_MASK, s, my_head);
       hitbits |= (uint32_t)(pass && slot[r] >= 0) << r;
     }
-    int64_t v = 0;
-    if (hitbits) v = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
+    // rows that join add their revenue and count per request (integer sums: order-free)
+    if (hitbits) {
+      const int64_t v = ld_stream(lext + row) * (int64_t)(100 - ld_stream(ldisc + row));
 #pragma unroll
-    for (int r = 0; r < kB; r++) {
-      if (r >= m.K) continue;
-      const uint32_t hitm = __ballot_sync(FULL_MASK, (hitbits >> r) & 1u);
-      if (!(hitm & FULL_MASK)) continue;   // warp-uniform
-      const int64_t vr = ((hitbits >> r) & 1u) ? v : 0;
-      int64_t inc = vr;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const int64_t o = __shfl_up_sync(FULL_MASK, inc, d);
-        if (lane >= d) inc += o;
-      }
-      const int64_t run_end = __shfl_sync(FULL_MASK, inc, last);
-      if (head && slot[r] >= 0) {
-        const uint32_t c = __popc(hitm & run_mask);
-        if (c) {
+      for (int r = 0; r < kB; r++) {
+        if ((hitbits >> r) & 1u) {
           const size_t at = (size_t)r * m.max_cap + (uint32_t)slot[r];
-          atomicAdd(&m.ht[at].rev, (unsigned long long)(run_end - (inc - vr)));
-          atomicAdd(&m.hits[at], c);
+          atomicAdd(&m.ht[at].rev, (unsigned long long)v);
+          atomicAdd(&m.hits[at], 1u);
         }
       }
     }

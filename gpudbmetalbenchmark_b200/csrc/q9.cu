@@ -9,8 +9,11 @@
 //  - partsupp rows whose part passes the bitmap are compacted, then inserted into an
 //    open-addressing table keyed by the 64-bit (part, supp) composite with a 64-bit
 //    atomicCAS; the table is sized on the device from the qualifying count;
-//  - the probe reads part_key for every fact row (128-bit loads) and touches the other five
-//    columns only for rows whose part passes (late materialisation, ~5.5%);
+//  - the fact table goes through in pieces of at most 64M rows, two kernels each:
+//    li_filter_kernel streams part_key (128-bit loads) and compacts the (row, part) pairs
+//    whose part passes the bitmap (~5.5%); q9_resolve_kernel takes one pair per thread and
+//    gathers the row's other five columns and its lookups together (late materialisation,
+//    all resident threads' misses in flight at once);
 //  - aggregation goes to a per-block shared-memory hash table keyed by (nation<<16 | year)
 //    (CAS + 64-bit shared atomics); a group that finds no shared slot spills straight to the
 //    global open-addressing table, and each block merges its shared table into the global
@@ -152,102 +155,85 @@ struct Q9Maps {
 };
 
 constexpr int kQ9Threads = 256;
-constexpr int kQ9Warps = kQ9Threads / 32;
 
-// Fact rows that passed the part bitmap wait in a per-warp queue until 32 are there; then
-// every lane resolves one of them (supplier -> nation, (part, supp) -> cost, order -> year,
-// the row's measures), so the dependent lookups of 32 rows are in flight together instead
-// of a few lanes at a time. Groups are aggregated in a shared table that spills to the
-// global table.
-__global__ void __launch_bounds__(kQ9Threads) q9_probe_kernel(const int32_t* __restrict__ part, const int32_t* __restrict__ supp,
-                                                       const int32_t* __restrict__ order, const int64_t* __restrict__ ext,
-                                                       const int32_t* __restrict__ disc, const int32_t* __restrict__ qty,
-                                                       uint64_t n, Q9Maps m, uint32_t* gkeys, unsigned long long* gvals,
-                                                       uint32_t gcap, uint32_t scap, uint32_t* status) {
+constexpr int kLiRows = 4;                 // fact rows per thread per block step of li_filter_kernel
+constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve pair (bounds the pair buffer)
+
+// Fact rows whose part passes the bitmap, as (row, part) pairs (block prefix sum, one
+// atomicAdd per 1024 rows); thread t of a block step covers 4 consecutive rows, one 16-byte
+// load when the column is aligned. A pure stream: nothing waits on a lookup chain here.
+__global__ void __launch_bounds__(256) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
+                                                        const uint32_t* __restrict__ bits, int32_t part_max,
+                                                        uint32_t* rows, int32_t* parts, uint32_t* count) {
+  __shared__ uint32_t sh[33];
+  const bool vec = (reinterpret_cast<uintptr_t>(part) & 15u) == 0;
+  const uint64_t step = (uint64_t)gridDim.x * 256 * kLiRows;
+  for (uint64_t b = (uint64_t)blockIdx.x * 256 * kLiRows; b < n; b += step) {   // whole blocks
+    const uint64_t r0 = b + (uint64_t)threadIdx.x * kLiRows;
+    int32_t p[kLiRows];
+    if (vec && r0 + kLiRows <= n) {
+      const int4 v = ld_stream(reinterpret_cast<const int4*>(part + r0));
+      p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < kLiRows; j++) p[j] = r0 + j < n ? ld_stream(part + r0 + j) : -1;
+    }
+    uint32_t take = 0;
+#pragma unroll
+    for (int j = 0; j < kLiRows; j++)
+      take |= (uint32_t)(p[j] >= 0 && p[j] <= part_max && bitmap_test(bits, p[j])) << j;
+    uint32_t pos = block_reserve<256>(__popc(take), count, sh);
+#pragma unroll
+    for (int j = 0; j < kLiRows; j++)
+      if (take & (1u << j)) { rows[pos] = (uint32_t)(r0 + j); parts[pos] = p[j]; pos++; }
+  }
+}
+
+// One (row, part) pair per thread: the row's five columns are gathered together, then
+// supplier -> nation, order -> year and (part, supp) -> cost, and the profit goes to a
+// shared (nation, year) table that spills to the global one. Every resident thread has its
+// own independent misses in flight.
+__global__ void __launch_bounds__(kQ9Threads) q9_resolve_kernel(const uint32_t* __restrict__ rows,
+                                                                 const int32_t* __restrict__ parts, const uint32_t* count,
+                                                                 const int32_t* __restrict__ supp,
+                                                                 const int32_t* __restrict__ order,
+                                                                 const int64_t* __restrict__ ext,
+                                                                 const int32_t* __restrict__ disc,
+                                                                 const int32_t* __restrict__ qty, Q9Maps m,
+                                                                 uint32_t* gkeys, unsigned long long* gvals, uint32_t gcap,
+                                                                 uint32_t scap, uint32_t* status) {
   extern __shared__ unsigned long long q9_smem[];
-  __shared__ uint64_t qrow[kQ9Warps][64];
-  __shared__ int32_t qpart[kQ9Warps][64];
   unsigned long long* svals = q9_smem;
   uint32_t* skeys = reinterpret_cast<uint32_t*>(svals + scap);
   for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x) { skeys[i] = kGroupEmpty; svals[i] = 0; }
   __syncthreads();
-  const uint32_t ps_cap = *m.ps_cap, smask = scap - 1;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t n = *count, ps_cap = *m.ps_cap, smask = scap - 1;
   uint32_t bad = 0;
-  // resolves queue entries [0, cnt) of this warp, one per lane
-  auto resolve = [&](int cnt) {
-    if (lane < cnt) {
-      const uint64_t r = qrow[warp][lane];
-      const int32_t p = qpart[warp][lane];
-      const int32_t s = supp[r], o = order[r];
-      const int64_t e = ext[r];
-      const int32_t d = disc[r], q = qty[r];
-      const bool s_ok = s >= 0 && s <= m.supp_max, o_ok = o >= 0 && o <= m.order_max;
-      const uint8_t nat = s_ok ? __ldg(m.nation + s) : kNoValue;
-      const uint8_t yoff = o_ok ? __ldg(m.year + o) : kNoValue;
-      long long cost = 0;
-      const bool found = s_ok && ps_find(m.ps, ps_cap, ps_key(p, s), &cost);
-      if (found && nat != kNoValue && yoff != kNoValue) {
-        bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
-        const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
-        const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
-        uint32_t h = slot_hash64(key) & smask;
-        bool done = false;
-        for (uint32_t t = 0; t < scap && !done; t++, h = (h + 1) & smask) {
-          const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
-          if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); done = true; }
-        }
-        if (!done) global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t r = ld_stream(rows + i);
+    const int32_t p = ld_stream(parts + i);
+    const int32_t s = ld_stream(supp + r), o = ld_stream(order + r);
+    const int64_t e = ld_stream(ext + r);
+    const int32_t d = ld_stream(disc + r), q = ld_stream(qty + r);
+    const bool s_ok = s >= 0 && s <= m.supp_max, o_ok = o >= 0 && o <= m.order_max;
+    const uint8_t nat = s_ok ? __ldg(m.nation + s) : kNoValue;
+    const uint8_t yoff = o_ok ? __ldg(m.year + o) : kNoValue;
+    long long cost = 0;
+    const bool found = s_ok && ps_find(m.ps, ps_cap, ps_key(p, s), &cost);
+    if (found && nat != kNoValue && yoff != kNoValue) {
+      bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
+      const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
+      const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
+      uint32_t h = slot_hash64(key) & smask;
+      bool done = false;
+      for (uint32_t t = 0; t < scap && !done; t++, h = (h + 1) & smask) {
+        const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
+        if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); done = true; }
       }
-    }
-    __syncwarp();
-  };
-  int queued = 0;   // warp-uniform
-  auto offer = [&](bool take, uint64_t r, int32_t p) {
-    const uint32_t bal = __ballot_sync(FULL_MASK, take);
-    if (take) {
-      const int at = queued + __popc(bal & lanemask_lt());
-      qrow[warp][at] = r;
-      qpart[warp][at] = p;
-    }
-    queued += __popc(bal);
-    __syncwarp();
-    if (queued >= 32) {
-      resolve(32);
-      if (lane < queued - 32) { qrow[warp][lane] = qrow[warp][lane + 32]; qpart[warp][lane] = qpart[warp][lane + 32]; }
-      queued -= 32;
-      __syncwarp();
-    }
-  };
-  auto passes = [&](int32_t p) { return p >= 0 && p <= m.part_max && bitmap_test(m.part_bits, p); };
-  const uint64_t warps = (uint64_t)gridDim.x * kQ9Warps;
-  const uint64_t gwarp = (uint64_t)blockIdx.x * kQ9Warps + warp;
-  if ((reinterpret_cast<uintptr_t>(part) & 15u) == 0) {
-    const uint64_t nq = n >> 2;
-    const int4* p4 = reinterpret_cast<const int4*>(part);
-    for (uint64_t qb = gwarp * 32; qb < nq; qb += warps * 32) {   // warp-uniform trip count
-      const uint64_t q = qb + lane;
-      int4 v = make_int4(-1, -1, -1, -1);
-      if (q < nq) v = ld_stream(p4 + q);
-      const bool t0 = passes(v.x), t1 = passes(v.y), t2 = passes(v.z), t3 = passes(v.w);
-      offer(t0, 4 * q + 0, v.x);
-      offer(t1, 4 * q + 1, v.y);
-      offer(t2, 4 * q + 2, v.z);
-      offer(t3, 4 * q + 3, v.w);
-    }
-    if (gwarp == 0) {   // the last n % 4 rows
-      const uint64_t r = (nq << 2) + lane;
-      const int32_t p = r < n ? part[r] : -1;
-      offer(r < n && passes(p), r, p);
-    }
-  } else {
-    for (uint64_t rb = gwarp * 32; rb < n; rb += warps * 32) {
-      const uint64_t r = rb + lane;
-      const int32_t p = r < n ? part[r] : -1;
-      offer(r < n && passes(p), r, p);
+      if (!done) global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
     }
   }
-  resolve(queued);
   if (__syncthreads_or(bad) && threadIdx.x == 0) set_status(status, ST_DOMAIN);
   for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x)
     if (skeys[i] != kGroupEmpty) global_group_add(gkeys, gvals, gcap, skeys[i], svals[i], status);
@@ -352,14 +338,24 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (!rc) rc = scratch(ctx, "q9.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q9.ps", (size_t)ps_max_cap * sizeof(PsSlot), &pst);
   if (!rc) rc = scratch(ctx, "q9.groups", (size_t)gcap * 12, &groups);
+  // (row, part) pairs of one piece of the fact table that passed the part bitmap
+  // (chunk_rows, when given, also sets the piece size of a device-resident table)
+  const uint64_t piece =
+      std::max<uint64_t>(1, std::min<uint64_t>(pp.chunk_rows ? (uint64_t)pp.chunk_rows : li->n_rows, kQ9Piece));
+  void* pairs = nullptr;
+  if (!rc) rc = scratch(ctx, "q9.pairs", (size_t)piece * 8, &pairs);
   if (rc) return rc;
+  uint32_t* prow = static_cast<uint32_t*>(pairs);
+  int32_t* ppart = reinterpret_cast<int32_t*>(prow + piece);
   uint32_t* cnt = static_cast<uint32_t*>(count);
   uint32_t* cap = cnt + 1;
   uint32_t* gkeys = reinterpret_cast<uint32_t*>(static_cast<unsigned long long*>(groups) + gcap);
   unsigned long long* gvals = static_cast<unsigned long long*>(groups);
   const size_t probe_smem = (size_t)scap * 12, sort_smem = (size_t)gcap * 12;
   // dynamic + static shared memory may pass the 48 KB default: always opt in (before any capture)
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
+  int resolve_per_sm = 0;
+  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resolve_per_sm, q9_resolve_kernel, kQ9Threads, probe_smem));
   GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
@@ -369,7 +365,7 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
     GPUDB_CUDA(ctx, cudaMemsetAsync(bits, 0, (size_t)words * 4, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, s));
-    GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));   // [0] partsupp count, [1] capacity, [2] pair count
     GPUDB_CUDA(ctx, cudaMemsetAsync(gvals, 0, (size_t)gcap * 8, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(gkeys, 0xFF, (size_t)gcap * 4, s));
     if (pa->n_rows)
@@ -392,10 +388,19 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
     const Q9Maps maps{(const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,
                       (const uint32_t*)cap, (const uint8_t*)year, order_max};
     int r = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
-      if (c.n_rows == 0) return (int)GPUDB_OK;
-      const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((c.n_rows / 4 + 255) / 256, (uint64_t)sms * 8));
-      GPUDB_LAUNCH(call, q9_probe_kernel, g, kQ9Threads, probe_smem, c.part_key, c.supp_key, c.order_key, c.ext_price,
-                   c.discount, c.quantity, c.n_rows, maps, gkeys, gvals, gcap, scap, call.status());
+      for (uint64_t off = 0; off < c.n_rows; off += piece) {
+        const uint64_t n = std::min<uint64_t>(piece, c.n_rows - off);
+        // the piece's pair count (the previous piece's resolve is done with it: stream order)
+        uint32_t* pc = cnt + 2;
+        GPUDB_CUDA(ctx, cudaMemsetAsync(pc, 0, 4, s));
+        GPUDB_LAUNCH(call, li_filter_kernel, grid((n + kLiRows - 1) / kLiRows), 256, 0, c.part_key + off, n,
+                     (const uint32_t*)bits, part_max, prow, ppart, pc);
+        const unsigned g = (unsigned)std::max<uint64_t>(
+            1, std::min<uint64_t>((n + kQ9Threads - 1) / kQ9Threads, (uint64_t)sms * std::max(1, resolve_per_sm)));
+        GPUDB_LAUNCH(call, q9_resolve_kernel, g, kQ9Threads, probe_smem, (const uint32_t*)prow, (const int32_t*)ppart,
+                     (const uint32_t*)pc, c.supp_key + off, c.order_key + off, c.ext_price + off, c.discount + off,
+                     c.quantity + off, maps, gkeys, gvals, gcap, scap, call.status());
+      }
       return (int)GPUDB_OK;
     });
     if (r) return r;

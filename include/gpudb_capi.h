@@ -272,7 +272,8 @@ int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_ord
 typedef struct gpudb_q9_params {
   int32_t smem_slots;          /* per-block aggregation slots, 0 = default (power of two) */
   int32_t global_slots;        /* global aggregation table slots, 0 = default (power of two) */
-  uint64_t chunk_rows;         /* host-resident lineitem: rows per streamed chunk, 0 = default */
+  uint64_t chunk_rows;         /* host-resident lineitem: rows per streamed chunk, 0 = default;
+                                  also the rows per filter + resolve piece (at most 64M) */
 } gpudb_q9_params;
 typedef struct gpudb_q9_group { int32_t nation; int32_t year; int64_t profit; } gpudb_q9_group;
 /* profit = sum(ext_price*(100-discount) - supply_cost*quantity*100), hundredths^2.
