@@ -48,6 +48,78 @@ static __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, con
                     (uint64_t)gridDim.x * blockDim.x);
 }
 
+// ---- key filter held in shared memory ------------------------------------------------------
+// A fact scan that tests every row's key against a dimension bitmap makes one scattered
+// 4-byte load per row; from global memory those are bound by L1/L2 transaction rates (one
+// sector each), from shared memory by bank conflicts (a few cycles per warp). The filter is
+// the exact bitmap when keys 0..key_max fit kSmemFilterBits bits, else a hashed bitmap of
+// kSmemFilterBits bits (key -> one bit; a key passes when its bit is set) whose hits the
+// caller confirms with the exact bitmap in global memory.
+constexpr uint32_t kSmemFilterWords = 51200;   // 200 KB of shared memory
+constexpr uint32_t kSmemFilterBits = kSmemFilterWords * 32;
+
+__host__ __device__ inline bool smem_filter_exact(int32_t key_max) {
+  return key_max >= 0 && (uint32_t)key_max < kSmemFilterBits;
+}
+// Words of the filter: the exact bitmap's words, or all kSmemFilterWords.
+__host__ __device__ inline uint32_t smem_filter_words(int32_t key_max) {
+  return smem_filter_exact(key_max) ? ((uint32_t)key_max >> 5) + 1 : kSmemFilterWords;
+}
+__device__ __forceinline__ uint32_t smem_filter_slot(int32_t key) {
+  return __umulhi((uint32_t)key * 0x9E3779B1u, kSmemFilterBits);   // multiplicative hash onto [0, bits)
+}
+
+// Hashed filter of an exact bitmap of `words` words: every set key sets its hashed bit.
+// `filt` holds kSmemFilterWords zeroed words.
+static __global__ void hashed_filter_kernel(const uint32_t* __restrict__ bits, uint32_t words, uint32_t* filt) {
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+    uint32_t x = bits[w];
+    while (x) {
+      const uint32_t b = __ffs(x) - 1;
+      x &= x - 1;
+      const uint32_t slot = smem_filter_slot((int32_t)(w * 32 + b));
+      atomicOr(filt + (slot >> 5), 1u << (slot & 31u));
+    }
+  }
+}
+
+// Copies `words` filter words into shared memory (whole block; 16-byte copies where the
+// source allows) and waits for the block.
+__device__ __forceinline__ void smem_filter_load(const uint32_t* __restrict__ src, uint32_t words, uint32_t* dst) {
+  if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+    const uint32_t quads = words >> 2;
+    for (uint32_t i = threadIdx.x; i < quads; i += blockDim.x)
+      reinterpret_cast<uint4*>(dst)[i] = __ldg(reinterpret_cast<const uint4*>(src) + i);
+    for (uint32_t i = (quads << 2) + threadIdx.x; i < words; i += blockDim.x) dst[i] = __ldg(src + i);
+  } else {
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = __ldg(src + i);
+  }
+  __syncthreads();
+}
+
+// Filter of N keys (ok[j]: key j is in [0, key_max]) -> bit j set where key j passes: the
+// shared-memory tests first, then (hashed filter) every confirming load of `bits` issued
+// before any is used, so a thread waits for one memory latency, not N.
+template <int N>
+__device__ __forceinline__ uint32_t smem_filter_mask(const uint32_t* sfilt, bool exact, const uint32_t* bits,
+                                                     const int32_t (&key)[N], uint32_t ok) {
+  uint32_t hit = 0;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    // a key outside [0, key_max] reads bit 0 and is masked off (its index would be out of range)
+    const uint32_t b = ((ok >> j) & 1u) ? (exact ? (uint32_t)key[j] : smem_filter_slot(key[j])) : 0u;
+    hit |= ((ok >> j) & (sfilt[b >> 5] >> (b & 31u)) & 1u) << j;
+  }
+  if (exact || !hit) return hit;
+  uint32_t w[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) w[j] = ((hit >> j) & 1u) ? __ldg(bits + ((uint32_t)key[j] >> 5)) : 0u;
+  uint32_t pass = 0;
+#pragma unroll
+  for (int j = 0; j < N; j++) pass |= ((w[j] >> ((uint32_t)key[j] & 31u)) & 1u) << j;
+  return pass & hit;
+}
+
 // Warp-aggregated append: returns this lane's output position (valid where `take`).
 __device__ __forceinline__ uint32_t warp_append(bool take, uint32_t* counter) {
   const uint32_t m = __ballot_sync(FULL_MASK, take);
@@ -63,6 +135,7 @@ __device__ __forceinline__ uint32_t warp_append(bool take, uint32_t* counter) {
 // call it the same number of times. `sh` needs 33 words of shared memory.
 template <int T>
 __device__ __forceinline__ uint32_t block_reserve(uint32_t mine, uint32_t* counter, uint32_t* sh) {
+  static_assert(T % 32 == 0 && T <= 1024, "block_reserve: whole warps, at most 1024 threads");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t inc = mine;
 #pragma unroll
@@ -72,13 +145,22 @@ __device__ __forceinline__ uint32_t block_reserve(uint32_t mine, uint32_t* count
   }
   if (lane == 31) sh[warp] = inc;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t run = 0;
-    for (int w = 0; w < T / 32; w++) { const uint32_t c = sh[w]; sh[w] = run; run += c; }
-    sh[32] = run ? atomicAdd(counter, run) : 0u;
+  if (warp == 0) {   // scan of the warp totals, one atomicAdd for the block
+    const uint32_t c = lane < T / 32 ? sh[lane] : 0u;
+    uint32_t x = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(FULL_MASK, x, d);
+      if (lane >= d) x += o;
+    }
+    const uint32_t total = __shfl_sync(FULL_MASK, x, 31);
+    uint32_t base = 0;
+    if (lane == 0 && total) base = atomicAdd(counter, total);
+    base = __shfl_sync(FULL_MASK, base, 0);
+    if (lane < T / 32) sh[lane] = base + x - c;
   }
   __syncthreads();
-  const uint32_t pos = sh[32] + sh[warp] + inc - mine;
+  const uint32_t pos = sh[warp] + inc - mine;
   __syncthreads();
   return pos;
 }

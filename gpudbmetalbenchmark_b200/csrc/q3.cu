@@ -6,8 +6,9 @@
 //
 // B200 design (global-table mode):
 //  1. bitmap_build_kernel: customers with segment == S -> bitmap (warp-combined atomicOr).
-//  2. orders_filter_kernel: orders with order_date < D and cust in the bitmap are compacted
-//     (block prefix sum + one atomicAdd per 1024 rows) into a staging list; the qualifying
+//  2. orders_filter_kernel: orders with order_date < D and cust in the bitmap (a shared-memory
+//     copy of it when it is at most 48 KB, else tested in place) are compacted (block prefix
+//     sum + one atomicAdd per block step) into a staging list; the qualifying
 //     count stays on the device.
 //  3. table_clear_kernel: sizes the hash table from that count on the device (power of two,
 //     <= 50% load) and clears only those slots, so no host round trip is needed.
@@ -38,40 +39,90 @@ namespace gpudb {
 
 namespace {
 
-constexpr int kFilterRows = 4;   // rows per thread per block step of orders_filter_kernel
+constexpr int kFilterRows = 4;                 // rows per thread per block step of orders_filter_kernel
+constexpr uint32_t kSmemCustWords = 12288;     // customer filters up to 48 KB are copied to shared memory
 
-__global__ void __launch_bounds__(256) orders_filter_kernel(const int32_t* __restrict__ okey, const int32_t* __restrict__ ocust,
-                                     const int32_t* __restrict__ odate, uint64_t n, int32_t date_lt,
-                                     const uint32_t* __restrict__ bitmap, int32_t cust_max, int32_t* out_key,
-                                     int32_t* out_date, uint32_t* count, uint32_t* status) {
+// Orders with order_date < date_lt whose customer passes the customer filter, compacted into
+// (key, date) with a block prefix sum and one atomicAdd per T * 4 rows. SMEM: the filter
+// (the exact bitmap, or a hashed one confirmed in `bitmap`) is copied into shared memory, for
+// small filters (1024 threads, two blocks per SM); otherwise the exact bitmap is tested in
+// place (256 threads, several blocks per SM). The three columns load together and the next
+// step's load while this one is tested.
+template <int T, bool SMEM>
+__global__ void __launch_bounds__(T, SMEM ? 2 : 1) orders_filter_kernel(
+    const int32_t* __restrict__ okey, const int32_t* __restrict__ ocust, const int32_t* __restrict__ odate, uint64_t n,
+    int32_t date_lt, const uint32_t* __restrict__ bitmap, int32_t cust_max, const uint32_t* __restrict__ filt,
+    uint32_t filt_words, bool exact, int32_t* out_key, int32_t* out_date, uint32_t* count, uint32_t* status) {
+  extern __shared__ uint32_t sfilt[];
   __shared__ uint32_t sh[33];
-  const uint64_t step = (uint64_t)gridDim.x * 256 * kFilterRows;
+  const uint32_t* f = bitmap;
+  if (SMEM) {
+    smem_filter_load(filt, filt_words, sfilt);
+    f = sfilt;
+  }
+  const bool ex = SMEM ? exact : true;
+  const uint64_t step = (uint64_t)gridDim.x * T * kFilterRows;
+  int32_t nkey[kFilterRows], ndate[kFilterRows], ncust[kFilterRows];
+  auto fetch = [&](uint64_t b) {
+#pragma unroll
+    for (int j = 0; j < kFilterRows; j++) {
+      const uint64_t i = b + (uint64_t)j * T + threadIdx.x;
+      const bool in = i < n;
+      ndate[j] = in ? ld_stream(odate + i) : date_lt;
+      ncust[j] = in ? ld_stream(ocust + i) : -1;
+      nkey[j] = in ? ld_stream(okey + i) : 0;
+    }
+  };
+  uint64_t b = (uint64_t)blockIdx.x * T * kFilterRows;
+  fetch(b);
   // whole blocks stay in the loop: block_reserve needs every thread of the block
-  for (uint64_t b = (uint64_t)blockIdx.x * 256 * kFilterRows; b < n; b += step) {
-    // the three columns load together (one memory latency per step, not three in a chain)
+  for (; b < n; b += step) {
     int32_t key[kFilterRows], date[kFilterRows], cust[kFilterRows];
 #pragma unroll
-    for (int j = 0; j < kFilterRows; j++) {
-      const uint64_t i = b + (uint64_t)j * 256 + threadIdx.x;
-      const bool in = i < n;
-      date[j] = in ? ld_stream(odate + i) : date_lt;
-      cust[j] = in ? ld_stream(ocust + i) : -1;
-      key[j] = in ? ld_stream(okey + i) : 0;
-    }
-    uint32_t take = 0;
+    for (int j = 0; j < kFilterRows; j++) { key[j] = nkey[j]; date[j] = ndate[j]; cust[j] = ncust[j]; }
+    fetch(b + step);
+    uint32_t ok = 0;
 #pragma unroll
-    for (int j = 0; j < kFilterRows; j++) {
-      const int32_t c = cust[j];
-      if (date[j] < date_lt && c >= 0 && c <= cust_max && bitmap_test(bitmap, c)) {
-        if (key[j] == kEmptyKey) set_status(status, ST_KEY_RANGE);
-        else take |= 1u << j;
-      }
-    }
-    uint32_t pos = block_reserve<256>(__popc(take), count, sh);
+    for (int j = 0; j < kFilterRows; j++) ok |= (uint32_t)(date[j] < date_lt && cust[j] >= 0 && cust[j] <= cust_max) << j;
+    uint32_t take = smem_filter_mask(f, ex, bitmap, cust, ok);
+#pragma unroll
+    for (int j = 0; j < kFilterRows; j++)
+      if (((take >> j) & 1u) && key[j] == kEmptyKey) { set_status(status, ST_KEY_RANGE); take &= ~(1u << j); }
+    uint32_t pos = block_reserve<T>(__popc(take), count, sh);
 #pragma unroll
     for (int j = 0; j < kFilterRows; j++)
       if (take & (1u << j)) { out_key[pos] = key[j]; out_date[pos] = date[j]; pos++; }
   }
+}
+
+template <int T, bool SMEM>
+int launch_orders_filter_as(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_q3_params& p,
+                            const uint32_t* bitmap, const uint32_t* filt, uint32_t fwords, bool exact, int32_t* out_key,
+                            int32_t* out_date, uint32_t* cnt) {
+  gpudb_ctx* ctx = call.ctx();
+  const size_t smem = SMEM ? (size_t)fwords * 4 : 0;
+  if (SMEM)
+    GPUDB_CUDA(ctx, cudaFuncSetAttribute(orders_filter_kernel<T, SMEM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, orders_filter_kernel<T, SMEM>, T, smem));
+  const uint64_t per_block = (uint64_t)T * kFilterRows;
+  const unsigned g = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>((od.n_rows + per_block - 1) / per_block, (uint64_t)ctx->sm_count * std::max(1, per_sm)));
+  GPUDB_LAUNCH(call, (orders_filter_kernel<T, SMEM>), g, T, smem, od.order_key, od.cust_key, od.order_date, od.n_rows,
+               p.order_date_lt, bitmap, cu.key_max, filt, fwords, exact, out_key, out_date, cnt, call.status());
+  return GPUDB_OK;
+}
+
+// The orders filter of both join modes, after the customer bitmap: the shared-memory form
+// when the customer filter is at most 48 KB, else the in-place form on the exact bitmap.
+int launch_orders_filter(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_q3_params& p,
+                         const uint32_t* bitmap, uint32_t words, int32_t* out_key, int32_t* out_date, uint32_t* cnt) {
+  if (od.n_rows == 0) return GPUDB_OK;
+  if (smem_filter_exact(cu.key_max) && smem_filter_words(cu.key_max) <= kSmemCustWords)
+    return launch_orders_filter_as<1024, true>(call, cu, od, p, bitmap, bitmap, smem_filter_words(cu.key_max), true,
+                                               out_key, out_date, cnt);
+  (void)words;
+  return launch_orders_filter_as<256, false>(call, cu, od, p, bitmap, bitmap, 0, true, out_key, out_date, cnt);
 }
 
 __global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint32_t max_cap, int shift, uint32_t* cap_out,
@@ -323,9 +374,7 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   if (cu.n_rows)
     GPUDB_LAUNCH(call, bitmap_build_kernel, grid(cu.n_rows), 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows,
                  cu.key_max, (uint32_t*)bitmap, call.status());
-  if (od.n_rows)
-    GPUDB_LAUNCH(call, orders_filter_kernel, grid((od.n_rows + kFilterRows - 1) / kFilterRows), 256, 0, od.order_key, od.cust_key, od.order_date, od.n_rows,
-                 p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, bkey, bdate, cnt, call.status());
+  if ((rc = launch_orders_filter(call, cu, od, p, (const uint32_t*)bitmap, words, bkey, bdate, cnt))) return rc;
   const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
   rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
     if (c.n_rows == 0) return (int)GPUDB_OK;
@@ -402,9 +451,7 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
                  cu.key_max, (uint32_t*)bitmap, call.status());
   int32_t* skey = static_cast<int32_t*>(stage);
   int32_t* sdate = skey + std::max<uint64_t>(n_or, 1);
-  if (n_or)
-    GPUDB_LAUNCH(call, orders_filter_kernel, grid((n_or + kFilterRows - 1) / kFilterRows), 256, 0, od.order_key, od.cust_key, od.order_date, n_or,
-                 p.order_date_lt, (const uint32_t*)bitmap, cu.key_max, skey, sdate, cnt, call.status());
+  if ((rc = launch_orders_filter(call, cu, od, p, (const uint32_t*)bitmap, words, skey, sdate, cnt))) return rc;
   GPUDB_LAUNCH(call, table_clear_kernel, grid(max_cap), 256, 0, (const uint32_t*)cnt, 2048u, max_cap, ctx->ht_shift, cap,
                (Q3Slot*)ht, (uint32_t*)hits);
   GPUDB_LAUNCH(call, orders_insert_kernel, grid(n_or / 4), 256, 0, (const int32_t*)skey, (const int32_t*)sdate,

@@ -10,8 +10,9 @@
 //    open-addressing table keyed by the 64-bit (part, supp) composite with a 64-bit
 //    atomicCAS; the table is sized on the device from the qualifying count;
 //  - the fact table goes through in pieces of at most 64M rows, two kernels each:
-//    li_filter_kernel streams part_key (128-bit loads) and compacts the (row, part) pairs
-//    whose part passes the bitmap (~5.5%); q9_resolve_kernel takes one pair per thread and
+//    li_filter_kernel streams part_key (128-bit loads), tests each part against a filter held
+//    in shared memory (the exact bitmap, or a hashed one confirmed in the global bitmap) and
+//    compacts the (row, part) pairs that pass (~5.5%); q9_resolve_kernel takes one pair per thread and
 //    gathers the row's other five columns and its lookups together (late materialisation,
 //    all resident threads' misses in flight at once);
 //  - aggregation goes to a per-block shared-memory hash table keyed by (nation<<16 | year)
@@ -156,36 +157,64 @@ struct Q9Maps {
 
 constexpr int kQ9Threads = 256;
 
-constexpr int kLiRows = 4;                 // fact rows per thread per block step of li_filter_kernel
+constexpr int kLiThreads = 1024;
+constexpr int kLiQuads = 4;                  // 16-byte loads per thread per block step
+constexpr int kLiRows = 4 * kLiQuads;        // fact rows per thread per block step of li_filter_kernel
 constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve pair (bounds the pair buffer)
 
 // Fact rows whose part passes the bitmap, as (row, part) pairs (block prefix sum, one
-// atomicAdd per 1024 rows); thread t of a block step covers 4 consecutive rows, one 16-byte
-// load when the column is aligned. A pure stream: nothing waits on a lookup chain here.
-__global__ void __launch_bounds__(256) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
-                                                        const uint32_t* __restrict__ bits, int32_t part_max,
-                                                        uint32_t* rows, int32_t* parts, uint32_t* count) {
+// atomicAdd per 16384 rows). The part filter sits in shared memory (smem_filter_*): the
+// exact bitmap, or a hashed one whose hits are confirmed in `bits`. A block step covers
+// kLiThreads * 16 rows; load q of thread t is the 16-byte quad q * kLiThreads + t of the
+// step (coalesced), and the next step's quads load while this one is tested (one block per
+// SM when the filter is large, so the block overlaps its own latencies).
+__global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
+                                                               const uint32_t* __restrict__ bits, int32_t part_max,
+                                                               const uint32_t* __restrict__ filt, uint32_t filt_words,
+                                                               bool exact, uint32_t* rows, int32_t* parts,
+                                                               uint32_t* count) {
+  extern __shared__ uint32_t sfilt[];
   __shared__ uint32_t sh[33];
+  smem_filter_load(filt, filt_words, sfilt);
   const bool vec = (reinterpret_cast<uintptr_t>(part) & 15u) == 0;
-  const uint64_t step = (uint64_t)gridDim.x * 256 * kLiRows;
-  for (uint64_t b = (uint64_t)blockIdx.x * 256 * kLiRows; b < n; b += step) {   // whole blocks
-    const uint64_t r0 = b + (uint64_t)threadIdx.x * kLiRows;
+  constexpr uint64_t kStepRows = (uint64_t)kLiThreads * kLiRows;
+  const uint64_t step = (uint64_t)gridDim.x * kStepRows;
+  // row of element (q, k) of this thread in the step at b
+  auto row_of = [&](uint64_t b, int q, int k) { return b + 4 * ((uint64_t)q * kLiThreads + threadIdx.x) + k; };
+  int4 nv[kLiQuads];
+  auto prefetch = [&](uint64_t b) {
+    if (vec && b + kStepRows <= n) {
+#pragma unroll
+      for (int q = 0; q < kLiQuads; q++) nv[q] = ld_stream(reinterpret_cast<const int4*>(part + row_of(b, q, 0)));
+    }
+  };
+  uint64_t b = (uint64_t)blockIdx.x * kStepRows;
+  prefetch(b);
+  for (; b < n; b += step) {   // whole blocks
     int32_t p[kLiRows];
-    if (vec && r0 + kLiRows <= n) {
-      const int4 v = ld_stream(reinterpret_cast<const int4*>(part + r0));
-      p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
+    if (vec && b + kStepRows <= n) {
+#pragma unroll
+      for (int q = 0; q < kLiQuads; q++) {
+        p[4 * q] = nv[q].x; p[4 * q + 1] = nv[q].y; p[4 * q + 2] = nv[q].z; p[4 * q + 3] = nv[q].w;
+      }
     } else {
 #pragma unroll
-      for (int j = 0; j < kLiRows; j++) p[j] = r0 + j < n ? ld_stream(part + r0 + j) : -1;
+      for (int q = 0; q < kLiQuads; q++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint64_t r = row_of(b, q, k);
+          p[4 * q + k] = r < n ? ld_stream(part + r) : -1;
+        }
     }
-    uint32_t take = 0;
+    prefetch(b + step);
+    uint32_t ok = 0;
+#pragma unroll
+    for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
+    const uint32_t take = smem_filter_mask(sfilt, exact, bits, p, ok);
+    uint32_t pos = block_reserve<kLiThreads>(__popc(take), count, sh);
 #pragma unroll
     for (int j = 0; j < kLiRows; j++)
-      take |= (uint32_t)(p[j] >= 0 && p[j] <= part_max && bitmap_test(bits, p[j])) << j;
-    uint32_t pos = block_reserve<256>(__popc(take), count, sh);
-#pragma unroll
-    for (int j = 0; j < kLiRows; j++)
-      if (take & (1u << j)) { rows[pos] = (uint32_t)(r0 + j); parts[pos] = p[j]; pos++; }
+      if (take & (1u << j)) { rows[pos] = (uint32_t)row_of(b, j >> 2, j & 3); parts[pos] = p[j]; pos++; }
   }
 }
 
@@ -338,6 +367,11 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (!rc) rc = scratch(ctx, "q9.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q9.ps", (size_t)ps_max_cap * sizeof(PsSlot), &pst);
   if (!rc) rc = scratch(ctx, "q9.groups", (size_t)gcap * 12, &groups);
+  // the part filter of li_filter_kernel: the exact bitmap itself, or a hashed one built from it
+  const bool filt_exact = smem_filter_exact(part_max);
+  const uint32_t filt_words = smem_filter_words(part_max);
+  void* hfilt = nullptr;
+  if (!rc && !filt_exact) rc = scratch(ctx, "q9.partfilter", (size_t)kSmemFilterWords * 4, &hfilt);
   // (row, part) pairs of one piece of the fact table that passed the part bitmap
   // (chunk_rows, when given, also sets the piece size of a device-resident table)
   const uint64_t piece =
@@ -354,6 +388,10 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   const size_t probe_smem = (size_t)scap * 12, sort_smem = (size_t)gcap * 12;
   // dynamic + static shared memory may pass the 48 KB default: always opt in (before any capture)
   GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
+  const size_t filt_smem = (size_t)filt_words * 4;
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(li_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)filt_smem));
+  int filter_per_sm = 0;
+  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&filter_per_sm, li_filter_kernel, kLiThreads, filt_smem));
   int resolve_per_sm = 0;
   GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resolve_per_sm, q9_resolve_kernel, kQ9Threads, probe_smem));
   GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
@@ -371,6 +409,10 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
     if (pa->n_rows)
       GPUDB_LAUNCH(call, bitmap_build_kernel, grid(pa->n_rows), 256, 0, pa->part_key, pa->flag, -1, pa->n_rows,
                    part_max, (uint32_t*)bits, call.status());
+    if (!filt_exact) {
+      GPUDB_CUDA(ctx, cudaMemsetAsync(hfilt, 0, (size_t)kSmemFilterWords * 4, s));
+      GPUDB_LAUNCH(call, hashed_filter_kernel, grid(words), 256, 0, (const uint32_t*)bits, words, (uint32_t*)hfilt);
+    }
     if (su->n_rows)
       GPUDB_LAUNCH(call, map_u8_kernel, grid(su->n_rows), 256, 0, su->supp_key, su->nation, su->n_rows, supp_max,
                    (uint8_t*)nation, call.status());
@@ -393,8 +435,11 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
         // the piece's pair count (the previous piece's resolve is done with it: stream order)
         uint32_t* pc = cnt + 2;
         GPUDB_CUDA(ctx, cudaMemsetAsync(pc, 0, 4, s));
-        GPUDB_LAUNCH(call, li_filter_kernel, grid((n + kLiRows - 1) / kLiRows), 256, 0, c.part_key + off, n,
-                     (const uint32_t*)bits, part_max, prow, ppart, pc);
+        const unsigned fg = (unsigned)std::max<uint64_t>(
+            1, std::min<uint64_t>((n + kLiThreads * kLiRows - 1) / (kLiThreads * kLiRows),
+                                  (uint64_t)sms * std::max(1, filter_per_sm)));
+        GPUDB_LAUNCH(call, li_filter_kernel, fg, kLiThreads, filt_smem, c.part_key + off, n, (const uint32_t*)bits,
+                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_exact, prow, ppart, pc);
         const unsigned g = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((n + kQ9Threads - 1) / kQ9Threads, (uint64_t)sms * std::max(1, resolve_per_sm)));
         GPUDB_LAUNCH(call, q9_resolve_kernel, g, kQ9Threads, probe_smem, (const uint32_t*)prow, (const int32_t*)ppart,

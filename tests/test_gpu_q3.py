@@ -31,6 +31,14 @@ def test_q3_matches_oracle(engine, orc, mode, sizes, seed):
 
 
 @pytest.mark.parametrize("mode", MODES)
+def test_q3_large_customer_key_range(engine, orc, mode):
+    """1.7M customer keys: a customer bitmap too large for the shared-memory copy is tested in
+    place by the orders filter (small ones are copied; the other tests cover those)."""
+    cu, od, li = orc.q3_tables(1_700_000, 400_000, 1_600_000, 21)
+    assert run(engine, cu, od, li, mode) == orc.q3(cu, od, li)
+
+
+@pytest.mark.parametrize("mode", MODES)
 def test_q3_random_constants_and_k(engine, orc, mode):
     rng = np.random.default_rng(5)
     cu, od, li = orc.q3_tables(20_000, 200_000, 800_000, 11)

@@ -51,6 +51,17 @@ def test_q9_shared_table_spill_and_small_global_table(engine, orc):
         free_all(engine, ts)
 
 
+def test_q9_hashed_part_filter(engine, orc):
+    """Part keys past the shared-memory filter's 1,638,400 bits: the fact filter tests a hashed
+    bitmap in shared memory and confirms its hits in the exact one."""
+    tabs = orc.q9_tables(1_700_000, 2_000, 200_000, 800_000, 17)
+    ts = upload_all(engine, tabs)
+    try:
+        assert engine.q9(*ts) == orc.q9(*tabs)
+    finally:
+        free_all(engine, ts)
+
+
 @pytest.mark.parametrize("piece", [40_000, 30_001])
 def test_q9_fact_table_in_pieces(engine, orc, piece):
     """A device-resident fact table goes through the filter + resolve kernels in pieces of
