@@ -43,13 +43,17 @@ OPT_NAMES = {1: "chunk_rows", 2: "q1_variant", 3: "q6_variant", 4: "ht_load_pct"
 JOIN_GLOBAL, JOIN_RADIX = 0, 1
 ORDERS_NONE, ORDERS_CLUSTERED, ORDERS_UNIFORM = 0, 1, 2
 Q3_MAX_K = 64
+# l_shipmode codes (alphabetical: ORDER BY l_shipmode)
+MODE_AIR, MODE_FOB, MODE_MAIL, MODE_RAIL, MODE_REG_AIR, MODE_SHIP, MODE_TRUCK = range(7)
+SHIP_MODES = ("AIR", "FOB", "MAIL", "RAIL", "REG AIR", "SHIP", "TRUCK")
+PRIORITIES = ("1-URGENT", "2-HIGH", "3-MEDIUM", "4-NOT SPECIFIED", "5-LOW")
 
 # column ids
 COL = dict(
     LI_SHIP_DATE=1, LI_QUANTITY=2, LI_EXT_PRICE=3, LI_DISCOUNT=4, LI_TAX=5, LI_FLAG=6, LI_STATUS=7,
-    LI_ORDER_KEY=8, LI_PART_KEY=9, LI_SUPP_KEY=10,
+    LI_ORDER_KEY=8, LI_PART_KEY=9, LI_SUPP_KEY=10, LI_COMMIT_DATE=11, LI_RECEIPT_DATE=12, LI_SHIP_MODE=13,
     CU_CUST_KEY=20, CU_SEGMENT=21,
-    OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32,
+    OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32, OR_PRIORITY=33,
     PA_PART_KEY=40, PA_FLAG=41,
     SU_SUPP_KEY=50, SU_NATION=51,
     PS_PART_KEY=60, PS_SUPP_KEY=61, PS_SUPPLY_COST=62,
@@ -77,7 +81,8 @@ class Timing(C.Structure):
 class Lineitem(C.Structure):
     _fields_ = [("n_rows", C.c_uint64), ("location", C.c_int32), ("order_key_max", C.c_int32),
                 ("ship_date", vp), ("quantity", vp), ("ext_price", vp), ("discount", vp), ("tax", vp),
-                ("flag", vp), ("status", vp), ("order_key", vp), ("part_key", vp), ("supp_key", vp)]
+                ("flag", vp), ("status", vp), ("order_key", vp), ("part_key", vp), ("supp_key", vp),
+                ("commit_date", vp), ("receipt_date", vp), ("ship_mode", vp)]
 
 
 class Customer(C.Structure):
@@ -87,7 +92,7 @@ class Customer(C.Structure):
 
 class Orders(C.Structure):
     _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("cust_key_max", C.c_int32),
-                ("order_key", vp), ("cust_key", vp), ("order_date", vp)]
+                ("order_key", vp), ("cust_key", vp), ("order_date", vp), ("priority", vp)]
 
 
 class Part(C.Structure):
@@ -108,6 +113,23 @@ class GenSpec(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("row_offset", C.c_uint64), ("n_rows", C.c_uint64),
                 ("n_orders", C.c_int64), ("n_cust", C.c_int64), ("n_parts", C.c_int64),
                 ("n_supp", C.c_int64), ("order_mode", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Q4Params(C.Structure):
+    _fields_ = [("date_lo", C.c_int32), ("date_hi", C.c_int32)]
+
+
+class Q4Result(C.Structure):
+    _fields_ = [("count", C.c_uint64 * 5)]
+
+
+class Q12Params(C.Structure):
+    _fields_ = [("receipt_lo", C.c_int32), ("receipt_hi", C.c_int32), ("mode", C.c_int32 * 2),
+                ("high_max", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Q12Result(C.Structure):
+    _fields_ = [("high", C.c_uint64 * 2), ("low", C.c_uint64 * 2)]
 
 
 class Q6Params(C.Structure):
@@ -212,6 +234,9 @@ PROTOTYPES = {
     "gpudb_q6_sum": (C.c_int, [ctx_p, P(Lineitem), P(Q6Params), P(Q6Result), P(Timing), P(Exec)]),
     "gpudb_q6_sum_noalloc": (C.c_int, [P(Lineitem), P(Q6Params), vp, vp]),
     "gpudb_q1_group6": (C.c_int, [ctx_p, P(Lineitem), P(Q1Params), P(Q1Result), P(Timing), P(Exec)]),
+    "gpudb_q4_priority": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q4Params), P(Q4Result), P(Timing), P(Exec)]),
+    "gpudb_q12_shipmode": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q12Params), P(Q12Result), P(Timing),
+                                     P(Exec)]),
     "gpudb_q3_join_topk": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q3Params), P(Q3Result),
                                      P(Timing), P(Exec)]),
     "gpudb_q9_star": (C.c_int, [ctx_p, P(Part), P(Supplier), P(Partsupp), P(Orders), P(Lineitem), P(Q9Params),

@@ -256,6 +256,9 @@ uint64_t lineitem_row_bytes(uint32_t m) {
   if (m & LI_ORDER) b += 4;
   if (m & LI_PART) b += 4;
   if (m & LI_SUPP) b += 4;
+  if (m & LI_COMMIT) b += 4;
+  if (m & LI_RECEIPT) b += 4;
+  if (m & LI_MODE) b += 1;
   return b;
 }
 
@@ -269,7 +272,9 @@ int lineitem_check(gpudb_ctx* ctx, const gpudb_lineitem* li, uint32_t m) {
       {LI_EXT, li->ext_price, "ext_price"},  {LI_DISC, li->discount, "discount"},
       {LI_TAX, li->tax, "tax"},              {LI_FLAG, li->flag, "flag"},
       {LI_STATUS, li->status, "status"},     {LI_ORDER, li->order_key, "order_key"},
-      {LI_PART, li->part_key, "part_key"},   {LI_SUPP, li->supp_key, "supp_key"}};
+      {LI_PART, li->part_key, "part_key"},   {LI_SUPP, li->supp_key, "supp_key"},
+      {LI_COMMIT, li->commit_date, "commit_date"}, {LI_RECEIPT, li->receipt_date, "receipt_date"},
+      {LI_MODE, li->ship_mode, "ship_mode"}};
   for (auto& c : cols)
     if ((m & c.bit) && !c.p) return fail(ctx, GPUDB_E_INVALID, "lineitem.%s is NULL", c.name);
   return GPUDB_OK;
@@ -290,7 +295,9 @@ int stream_lineitem(Call& call, const gpudb_lineitem* li, uint32_t mask, uint64_
                 {LI_EXT, li->ext_price, 8, 0},  {LI_DISC, li->discount, 4, 0},
                 {LI_TAX, li->tax, 4, 0},        {LI_FLAG, li->flag, 1, 0},
                 {LI_STATUS, li->status, 1, 0},  {LI_ORDER, li->order_key, 4, 0},
-                {LI_PART, li->part_key, 4, 0},  {LI_SUPP, li->supp_key, 4, 0}};
+                {LI_PART, li->part_key, 4, 0},  {LI_SUPP, li->supp_key, 4, 0},
+                {LI_COMMIT, li->commit_date, 4, 0}, {LI_RECEIPT, li->receipt_date, 4, 0},
+                {LI_MODE, li->ship_mode, 1, 0}};
   size_t slot_bytes = 0;
   for (auto& c : cols)
     if (mask & c.bit) { c.off = slot_bytes; slot_bytes += ((chunk_rows * c.w + 255) / 256) * 256; }
@@ -335,6 +342,9 @@ int stream_lineitem(Call& call, const gpudb_lineitem* li, uint32_t mask, uint64_
         case LI_ORDER: dev.order_key = (const int32_t*)dst; break;
         case LI_PART: dev.part_key = (const int32_t*)dst; break;
         case LI_SUPP: dev.supp_key = (const int32_t*)dst; break;
+        case LI_COMMIT: dev.commit_date = (const int32_t*)dst; break;
+        case LI_RECEIPT: dev.receipt_date = (const int32_t*)dst; break;
+        case LI_MODE: dev.ship_mode = (const uint8_t*)dst; break;
       }
     }
     if (e == cudaSuccess) e = cudaEventRecord(copied[s], ctx->copy_stream);

@@ -178,7 +178,8 @@ int status_to_error(gpudb_ctx* ctx, uint32_t st);
 // Columns of a lineitem chunk that a pipeline reads.
 enum : uint32_t {
   LI_SHIP = 1u << 0, LI_QTY = 1u << 1, LI_EXT = 1u << 2, LI_DISC = 1u << 3, LI_TAX = 1u << 4,
-  LI_FLAG = 1u << 5, LI_STATUS = 1u << 6, LI_ORDER = 1u << 7, LI_PART = 1u << 8, LI_SUPP = 1u << 9
+  LI_FLAG = 1u << 5, LI_STATUS = 1u << 6, LI_ORDER = 1u << 7, LI_PART = 1u << 8, LI_SUPP = 1u << 9,
+  LI_COMMIT = 1u << 10, LI_RECEIPT = 1u << 11, LI_MODE = 1u << 12
 };
 uint64_t lineitem_row_bytes(uint32_t mask);
 int lineitem_check(gpudb_ctx* ctx, const gpudb_lineitem* li, uint32_t mask);

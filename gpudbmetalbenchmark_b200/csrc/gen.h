@@ -37,8 +37,9 @@
 enum gd_column {
   GD_LI_SHIP_DATE = 16, GD_LI_QUANTITY, GD_LI_UNIT_PRICE, GD_LI_DISCOUNT, GD_LI_TAX,
   GD_LI_FLAG, GD_LI_STATUS, GD_LI_ORDER_PICK, GD_LI_PART, GD_LI_SUPP_SLOT, GD_LI_ORDER_RUN,
+  GD_LI_COMMIT, GD_LI_RECEIPT, GD_LI_MODE,
   GD_CU_SEGMENT = 32,
-  GD_OR_CUST = 48, GD_OR_DATE,
+  GD_OR_CUST = 48, GD_OR_DATE, GD_OR_PRIORITY,
   GD_PA_FLAG = 64,
   GD_SU_NATION = 80,
   GD_PS_COST = 96
@@ -106,6 +107,16 @@ GD_HD int32_t gd_li_supp(uint64_t seed, uint64_t r, int64_t n_parts, int64_t n_s
   return gd_partsupp_supp(gd_li_part(seed, r, n_parts), gd_uniform(seed, GD_LI_SUPP_SLOT, r, 0, 3), n_supp);
 }
 
+// Commit and receipt dates follow TPC-H's offsets: commit = order date + [30, 90] and ship =
+// order date + [1, 121] give commit - ship in [-91, 89]; receipt = ship + [1, 30].
+GD_HD int32_t gd_li_commit_date(uint64_t seed, uint64_t r) {
+  return gd_li_ship_date(seed, r) + (int32_t)gd_uniform(seed, GD_LI_COMMIT, r, -91, 89);
+}
+GD_HD int32_t gd_li_receipt_date(uint64_t seed, uint64_t r) {
+  return gd_li_ship_date(seed, r) + (int32_t)gd_uniform(seed, GD_LI_RECEIPT, r, 1, 30);
+}
+GD_HD uint8_t gd_li_ship_mode(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_LI_MODE, r, 0, 6); }
+GD_HD uint8_t gd_or_priority(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_OR_PRIORITY, r, 1, 5); }
 GD_HD uint8_t gd_cu_segment(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_CU_SEGMENT, r, 0, 4); }
 GD_HD int32_t gd_or_cust(uint64_t seed, uint64_t r, int64_t n_cust) { return (int32_t)gd_uniform(seed, GD_OR_CUST, r, 0, n_cust - 1); }
 GD_HD int32_t gd_or_date(uint64_t seed, uint64_t r) { return (int32_t)gd_uniform(seed, GD_OR_DATE, r, 0, GD_ORDER_DATE_MAX); }

@@ -21,12 +21,16 @@ LINEITEM_COLS = {  # field of capi.Lineitem -> column id
     "ship_date": COL["LI_SHIP_DATE"], "quantity": COL["LI_QUANTITY"], "ext_price": COL["LI_EXT_PRICE"],
     "discount": COL["LI_DISCOUNT"], "tax": COL["LI_TAX"], "flag": COL["LI_FLAG"], "status": COL["LI_STATUS"],
     "order_key": COL["LI_ORDER_KEY"], "part_key": COL["LI_PART_KEY"], "supp_key": COL["LI_SUPP_KEY"],
+    "commit_date": COL["LI_COMMIT_DATE"], "receipt_date": COL["LI_RECEIPT_DATE"], "ship_mode": COL["LI_SHIP_MODE"],
 }
+Q4_LI_COLS = ("order_key", "commit_date", "receipt_date")
+Q12_LI_COLS = ("order_key", "ship_date", "commit_date", "receipt_date", "ship_mode")
 Q1_COLS = ("ship_date", "quantity", "ext_price", "discount", "tax", "flag", "status")
 Q6_COLS = ("ship_date", "discount", "quantity", "ext_price")
 TABLE_COLS = {
     "customer": {"cust_key": COL["CU_CUST_KEY"], "segment": COL["CU_SEGMENT"]},
-    "orders": {"order_key": COL["OR_ORDER_KEY"], "cust_key": COL["OR_CUST_KEY"], "order_date": COL["OR_ORDER_DATE"]},
+    "orders": {"order_key": COL["OR_ORDER_KEY"], "cust_key": COL["OR_CUST_KEY"], "order_date": COL["OR_ORDER_DATE"],
+               "priority": COL["OR_PRIORITY"]},
     "part": {"part_key": COL["PA_PART_KEY"], "flag": COL["PA_FLAG"]},
     "supplier": {"supp_key": COL["SU_SUPP_KEY"], "nation": COL["SU_NATION"]},
     "partsupp": {"part_key": COL["PS_PART_KEY"], "supp_key": COL["PS_SUPP_KEY"], "supply_cost": COL["PS_SUPPLY_COST"]},
@@ -301,6 +305,30 @@ class Engine:
                                                 C.byref(r), C.byref(timing) if timing is not None else None,
                                                 self._exec(async_, None)))
         return r if async_ else q3_to_list(r)
+
+    def q4(self, od, li, date_lo=547, date_hi=639, timing=None, async_=False, out=None):
+        """Orders per priority 1..5 in [date_lo, date_hi) with a late lineitem (commit < receipt).
+        The defaults are the query's 1993-07-01 .. 1993-10-01 as day numbers."""
+        p = capi.Q4Params(date_lo, date_hi)
+        r = out if out is not None else capi.Q4Result()
+        ls = li if isinstance(li, capi.Lineitem) else li.lineitem()
+        self._check(self.lib.gpudb_q4_priority(self.ctx, C.byref(od.struct()), C.byref(ls), C.byref(p), C.byref(r),
+                                               C.byref(timing) if timing is not None else None,
+                                               self._exec(async_, None)))
+        return r if async_ else list(r.count)
+
+    def q12(self, od, li, receipt_lo=731, receipt_hi=1096, modes=(capi.MODE_MAIL, capi.MODE_SHIP), high_max=2,
+            timing=None, async_=False, out=None):
+        """[(high, low) for each of the two ship modes]: lineitem rows of that mode received in
+        [receipt_lo, receipt_hi) (default: 1994) with ship < commit < receipt, split by order
+        priority 1..high_max (high) or other (low)."""
+        p = capi.Q12Params(receipt_lo, receipt_hi, (C.c_int32 * 2)(*modes), high_max, 0)
+        r = out if out is not None else capi.Q12Result()
+        ls = li if isinstance(li, capi.Lineitem) else li.lineitem()
+        self._check(self.lib.gpudb_q12_shipmode(self.ctx, C.byref(od.struct()), C.byref(ls), C.byref(p), C.byref(r),
+                                                C.byref(timing) if timing is not None else None,
+                                                self._exec(async_, None)))
+        return r if async_ else [(r.high[0], r.low[0]), (r.high[1], r.low[1])]
 
     def q9(self, pa, su, ps, od, li, smem_slots=0, global_slots=0, chunk_rows=0, capacity=4096, timing=None):
         """[(nation, year, profit)] ordered by nation asc, year desc."""

@@ -15,7 +15,7 @@ import statistics
 import sys
 
 from . import capi
-from .engine import Engine, Q1_COLS
+from .engine import Q12_LI_COLS, Engine, Q1_COLS
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -225,6 +225,17 @@ def main(argv=None):
     if on("q3"):
         q3_case(eng, 150_000, 1_500_000, 6_000_000, a.reps, "config 2 (1x)")
         q3_case(eng, 1_500_000, 15_000_000, 60_000_000, max(3, a.reps // 4), "config 2 (10x)")
+    if on("q4q12"):
+        for n_or, n_li, label in ((1_500_000, 6_000_000, "SF-1 sizes"), (15_000_000, 60_000_000, "SF-10 sizes")):
+            od = eng.generate("orders", n_or, seed=42, columns=("order_key", "order_date", "priority"))
+            li = eng.generate("lineitem", n_li, seed=42, columns=Q12_LI_COLS, n_orders=n_or,
+                              order_mode=capi.ORDERS_CLUSTERED)
+            ms, t = timed(lambda tm: eng.q4(od, li, timing=tm), a.reps)
+            emit("q4_priority", label, n_li, ms, n_li * 12 + n_or * 9, {"kernels": t.kernels})
+            ms, t = timed(lambda tm: eng.q12(od, li, timing=tm), a.reps)
+            emit("q12_shipmode", label, n_li, ms, n_li * 17 + n_or * 5, {"kernels": t.kernels})
+            eng.free(li)
+            eng.free(od)
     if on("q9"):
         pa, su, ps, od = q9_tables(eng, 2_000_000, 100_000, 15_000_000)
         li = eng.generate("lineitem", 60_000_000, seed=42,

@@ -132,7 +132,14 @@ typedef struct gpudb_lineitem {
   const int32_t* order_key;
   const int32_t* part_key;
   const int32_t* supp_key;
+  const int32_t* commit_date;  /* day number (Q4, Q12) */
+  const int32_t* receipt_date; /* day number (Q4, Q12) */
+  const uint8_t* ship_mode;    /* GPUDB_MODE_*: 0..6 (Q12) */
 } gpudb_lineitem;
+
+/* l_shipmode codes, in the order of the strings (ORDER BY l_shipmode) */
+enum { GPUDB_MODE_AIR = 0, GPUDB_MODE_FOB, GPUDB_MODE_MAIL, GPUDB_MODE_RAIL, GPUDB_MODE_REG_AIR,
+       GPUDB_MODE_SHIP, GPUDB_MODE_TRUCK };
 
 typedef struct gpudb_customer {
   uint64_t n_rows; int32_t key_max; int32_t reserved;
@@ -142,6 +149,7 @@ typedef struct gpudb_customer {
 typedef struct gpudb_orders {
   uint64_t n_rows; int32_t key_max; int32_t cust_key_max;
   const int32_t* order_key; const int32_t* cust_key; const int32_t* order_date;
+  const uint8_t* priority;     /* o_orderpriority 1..5 = '1-URGENT' .. '5-LOW' (Q4, Q12) */
 } gpudb_orders;
 
 typedef struct gpudb_part {
@@ -164,8 +172,9 @@ enum gpudb_column_id {
   GPUDB_COL_LI_SHIP_DATE = 1, GPUDB_COL_LI_QUANTITY, GPUDB_COL_LI_EXT_PRICE,
   GPUDB_COL_LI_DISCOUNT, GPUDB_COL_LI_TAX, GPUDB_COL_LI_FLAG, GPUDB_COL_LI_STATUS,
   GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_PART_KEY, GPUDB_COL_LI_SUPP_KEY,
+  GPUDB_COL_LI_COMMIT_DATE, GPUDB_COL_LI_RECEIPT_DATE, GPUDB_COL_LI_SHIP_MODE,
   GPUDB_COL_CU_CUST_KEY = 20, GPUDB_COL_CU_SEGMENT,
-  GPUDB_COL_OR_ORDER_KEY = 30, GPUDB_COL_OR_CUST_KEY, GPUDB_COL_OR_ORDER_DATE,
+  GPUDB_COL_OR_ORDER_KEY = 30, GPUDB_COL_OR_CUST_KEY, GPUDB_COL_OR_ORDER_DATE, GPUDB_COL_OR_PRIORITY,
   GPUDB_COL_PA_PART_KEY = 40, GPUDB_COL_PA_FLAG,
   GPUDB_COL_SU_SUPP_KEY = 50, GPUDB_COL_SU_NATION,
   GPUDB_COL_PS_PART_KEY = 60, GPUDB_COL_PS_SUPP_KEY, GPUDB_COL_PS_SUPPLY_COST
@@ -283,6 +292,35 @@ int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_supplier* su
                   const gpudb_partsupp* ps, const gpudb_orders* od, const gpudb_lineitem* li,
                   const gpudb_q9_params* p, gpudb_q9_group* out, uint32_t capacity,
                   uint32_t* n_groups, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- Q4 order priority checking (replaces runQ4Benchmark src/q4.cpp:8-127 and its kernels
+ *      q4_build_late_bitmap / q4_count_by_priority_stage1 / q4_final_count_stage2
+ *      kernels/q4.metal:21-94; the streamed form replaces runQ4BenchmarkSF100
+ *      src/q4.cpp:130-282) ------------------------------------------------------------------
+ * count[p - 1] = number of orders with priority p (1..5) and date_lo <= order_date < date_hi
+ * that have a lineitem row with commit_date < receipt_date (EXISTS). The "late" bitmap covers
+ * order keys 0..od->key_max; lineitem keys outside it match no order. Lineitem may be
+ * host-resident (streamed in chunks). */
+typedef struct gpudb_q4_params { int32_t date_lo; int32_t date_hi; } gpudb_q4_params;
+typedef struct gpudb_q4_result { uint64_t count[5]; } gpudb_q4_result;
+int gpudb_q4_priority(gpudb_ctx* ctx, const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q4_params* p,
+                      gpudb_q4_result* out, gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- Q12 shipping modes and order priority (replaces runQ12Benchmark src/q12.cpp:8-125 and
+ *      its kernels q12_build_priority_bitmap / q12_filter_and_count_stage1 /
+ *      q12_final_count_stage2 kernels/q12.metal:22-99; the streamed form replaces
+ *      runQ12BenchmarkSF100 src/q12.cpp:128-277) --------------------------------------------
+ * For lineitem rows with ship_mode == mode[m] (m = 0, 1), receipt_lo <= receipt_date <
+ * receipt_hi, commit_date < receipt_date and ship_date < commit_date: high[m] counts the rows
+ * whose order has priority 1..high_max (the query's '1-URGENT', '2-HIGH': high_max = 2), low[m]
+ * the others (as the reference's priority bitmap does: a row whose order key is outside
+ * 0..od->key_max or has no order counts as low). */
+typedef struct gpudb_q12_params {
+  int32_t receipt_lo; int32_t receipt_hi; int32_t mode[2]; int32_t high_max; int32_t reserved;
+} gpudb_q12_params;
+typedef struct gpudb_q12_result { uint64_t high[2]; uint64_t low[2]; } gpudb_q12_result;
+int gpudb_q12_shipmode(gpudb_ctx* ctx, const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q12_params* p,
+                       gpudb_q12_result* out, gpudb_timing* t, const gpudb_exec* ex);
 
 /* ---- microbenchmarks (replace runSelectionBenchmark / runAggregationBenchmark /
  *      runJoinBenchmark src/microbenchmarks.cpp:8-251 and their kernels

@@ -36,7 +36,8 @@ static int64_t unif(uint64_t key, uint64_t row, int64_t lo, int64_t hi) {
 
 /* random stream ids (table*16 + column) */
 enum { S_SHIP = 16, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG, S_STATUS, S_OPICK, S_PART, S_SSLOT, S_RUN,
-       S_SEG = 32, S_OCUST = 48, S_ODATE, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
+       S_COMMIT, S_RECEIPT, S_MODE,
+       S_SEG = 32, S_OCUST = 48, S_ODATE, S_OPRIO, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
 
 static int32_t supp_of(int64_t part, int64_t j, int64_t n_supp) { return (int32_t)((part + j * (n_supp / 4)) % n_supp); }
 
@@ -78,6 +79,13 @@ int or_gen_column(const or_spec* sp, int32_t column, void* dst) {
              uint64_t kp = stream_of(seed, S_PART), ks = stream_of(seed, S_SSLOT);
              for (i = 0; i < n; i++) i32[i] = supp_of(unif(kp, off + i, 0, sp->n_parts - 1), unif(ks, off + i, 0, 3), sp->n_supp);
              return 0; }
+  /* commit = ship + [-91, 89], receipt = ship + [1, 30], mode 0..6, priority 1..5 */
+  case 11: { uint64_t ks = stream_of(seed, S_SHIP), k = stream_of(seed, S_COMMIT);
+             for (i = 0; i < n; i++) i32[i] = (int32_t)(unif(ks, off + i, 0, 2526) + unif(k, off + i, -91, 89)); return 0; }
+  case 12: { uint64_t ks = stream_of(seed, S_SHIP), k = stream_of(seed, S_RECEIPT);
+             for (i = 0; i < n; i++) i32[i] = (int32_t)(unif(ks, off + i, 0, 2526) + unif(k, off + i, 1, 30)); return 0; }
+  case 13: { uint64_t k = stream_of(seed, S_MODE); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 6); return 0; }
+  case 33: { uint64_t k = stream_of(seed, S_OPRIO); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 1, 5); return 0; }
   case 20: case 30: case 40: case 50:
     for (i = 0; i < n; i++) i32[i] = (column == 30) ? (int32_t)(4 * (off + i) + 1) : (int32_t)(off + i);
     return 0;
@@ -345,6 +353,48 @@ uint32_t or_q9(uint64_t n_pa, const int32_t* pa_key, const uint8_t* pa_flag, int
 
 /* ---- microbenchmarks: selection (kernels/microbenchmarks.metal:160-171), sum
  *      (:178-220), join count (:225-294), radix partition (:15-99), pairs (:104-156) ---- */
+/* ---- Q4: kernels/q4.metal:21-37 (late bitmap) and :40-72 (date window, bitmap, bins) ---- */
+void or_q4(uint64_t n_or, const int32_t* o_key, const int32_t* o_date, const uint8_t* o_prio, int32_t or_key_max,
+           uint64_t n_li, const int32_t* l_key, const int32_t* l_commit, const int32_t* l_receipt, int32_t date_lo,
+           int32_t date_hi, uint64_t* count5) {
+  uint64_t i;
+  uint8_t* late = or_key_max >= 0 ? (uint8_t*)calloc((size_t)or_key_max + 1, 1) : NULL;
+  for (int b = 0; b < 5; b++) count5[b] = 0;
+  if (!late) return;
+  for (i = 0; i < n_li; i++)
+    if (l_commit[i] < l_receipt[i] && l_key[i] >= 0 && l_key[i] <= or_key_max) late[l_key[i]] = 1;
+  for (i = 0; i < n_or; i++) {
+    if (o_date[i] < date_lo || o_date[i] >= date_hi) continue;
+    if (o_key[i] < 0 || o_key[i] > or_key_max || !late[o_key[i]]) continue;
+    if (o_prio[i] >= 1 && o_prio[i] <= 5) count5[o_prio[i] - 1]++;
+  }
+  free(late);
+}
+
+/* ---- Q12: kernels/q12.metal:87-99 (priority bitmap) and :22-66 (filters, 4 bins) ---- */
+void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t or_key_max, uint64_t n_li,
+            const int32_t* l_key, const int32_t* l_ship, const int32_t* l_commit, const int32_t* l_receipt,
+            const uint8_t* l_mode, int32_t receipt_lo, int32_t receipt_hi, int32_t mode0, int32_t mode1,
+            int32_t high_max, uint64_t* out4) {
+  uint64_t i;
+  uint8_t* high = or_key_max >= 0 ? (uint8_t*)calloc((size_t)or_key_max + 1, 1) : NULL;
+  for (int b = 0; b < 4; b++) out4[b] = 0;
+  if (high)
+    for (i = 0; i < n_or; i++)
+      if (o_prio[i] >= 1 && o_prio[i] <= high_max && o_key[i] >= 0 && o_key[i] <= or_key_max) high[o_key[i]] = 1;
+  for (i = 0; i < n_li; i++) {
+    const int m = l_mode[i] == mode0 ? 0 : (l_mode[i] == mode1 ? 1 : -1);
+    if (m < 0) continue;
+    const int32_t rd = l_receipt[i];
+    if (rd < receipt_lo || rd >= receipt_hi) continue;
+    if (l_commit[i] >= rd) continue;
+    if (l_ship[i] >= l_commit[i]) continue;
+    const int h = high && l_key[i] >= 0 && l_key[i] <= or_key_max && high[l_key[i]];
+    out4[(h ? 0 : 2) + m]++;
+  }
+  free(high);
+}
+
 uint64_t or_select_lt(uint64_t n, const int32_t* col, int32_t value, uint32_t* bits, uint32_t* rows) {
   uint64_t c = 0;
   if (bits) memset(bits, 0, ((n + 31) / 32) * sizeof(uint32_t));

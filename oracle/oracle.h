@@ -68,6 +68,20 @@ uint32_t or_q9(uint64_t n_pa, const int32_t* pa_key, const uint8_t* pa_flag, int
                uint32_t cap, int32_t* g_nation, int32_t* g_year, int64_t* g_profit);
 
 /* Microbenchmarks. */
+/* Q4: the late-delivery bitmap of kernels/q4.metal:21-37 (order keys of lineitem rows with
+ * commit < receipt; keys outside 0..or_key_max match no order) and the count of
+ * kernels/q4.metal:40-72 (orders in [date_lo, date_hi) whose key is in it, by priority 1..5). */
+void or_q4(uint64_t n_or, const int32_t* o_key, const int32_t* o_date, const uint8_t* o_prio, int32_t or_key_max,
+           uint64_t n_li, const int32_t* l_key, const int32_t* l_commit, const int32_t* l_receipt, int32_t date_lo,
+           int32_t date_hi, uint64_t* count5);
+/* Q12: the priority bitmap of kernels/q12.metal:87-99 (orders with priority 1..high_max) and the
+ * filter + 4-bin count of kernels/q12.metal:22-66. out = {high[mode0], high[mode1], low[mode0],
+ * low[mode1]}; a row whose key is outside 0..or_key_max is low. */
+void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t or_key_max, uint64_t n_li,
+            const int32_t* l_key, const int32_t* l_ship, const int32_t* l_commit, const int32_t* l_receipt,
+            const uint8_t* l_mode, int32_t receipt_lo, int32_t receipt_hi, int32_t mode0, int32_t mode1,
+            int32_t high_max, uint64_t* out4);
+
 uint64_t or_select_lt(uint64_t n, const int32_t* col, int32_t value, uint32_t* bits, uint32_t* rows);
 int64_t or_sum_i32(uint64_t n, const int32_t* col);
 uint64_t or_join_count(uint64_t nb, const int32_t* bkeys, uint64_t np, const int32_t* pkeys);

@@ -1,5 +1,5 @@
 // ref_harness.cpp -- runs the reference's own Metal kernels (kernels/q1.metal, q3.metal,
-// q6.metal, q9.metal, microbenchmarks.metal, compiled in place from the reference tree
+// q4.metal, q6.metal, q9.metal, q12.metal, microbenchmarks.metal, compiled in place from the reference tree
 // through the CPU shim in oracle/refshim) on the synthetic tables. TEST INFRASTRUCTURE
 // ONLY: it pins the oracle's query logic to the reference's code, and it is the timed
 // reference arm of bench.py. It is never linked into the engine.
@@ -17,16 +17,20 @@ using namespace metal;
 #include "common.h"
 #include "microbenchmarks.metal"
 #include "q1.metal"
+#include "q12.metal"
 #include "q3.metal"
+#include "q4.metal"
 #include "q6.metal"
 #include "q9.metal"
 
 namespace {
 
-// Day number (0 = 1992-01-01) -> YYYYMMDD, proleptic Gregorian calendar.
+// Day number (0 = 1992-01-01, negative before it) -> YYYYMMDD, proleptic Gregorian calendar.
 int yyyymmdd(int day) {
   static const int mdays[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+  auto year_len = [](int y) { return ((y % 4 == 0 && y % 100 != 0) || y % 400 == 0) ? 366 : 365; };
   int y = 1992;
+  while (day < 0) day += year_len(--y);
   for (;;) {
     bool leap = (y % 4 == 0 && y % 100 != 0) || y % 400 == 0;
     int len = leap ? 366 : 365;
@@ -43,12 +47,12 @@ int yyyymmdd(int day) {
 }
 
 std::vector<int> dates(uint64_t n, const int32_t* d) {
-  int hi = 0;
-  for (uint64_t i = 0; i < n; i++) hi = std::max(hi, d[i]);
-  std::vector<int> table(hi + 2);
-  for (int i = 0; i <= hi + 1; i++) table[i] = yyyymmdd(i);
+  int lo = 0, hi = 0;
+  for (uint64_t i = 0; i < n; i++) { lo = std::min(lo, d[i]); hi = std::max(hi, d[i]); }
+  std::vector<int> table(hi - lo + 2);
+  for (int i = lo; i <= hi + 1; i++) table[i - lo] = yyyymmdd(i);
   std::vector<int> out(n);
-  for (uint64_t i = 0; i < n; i++) out[i] = table[d[i]];
+  for (uint64_t i = 0; i < n; i++) out[i] = table[d[i] - lo];
   return out;
 }
 
@@ -180,6 +184,62 @@ uint32_t ref_q3(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_seg,
     g_date[i] = row >= 0 ? or_date[row] : -1;
   }
   return count.v;
+}
+
+// Q4 through q4_build_late_bitmap, q4_count_by_priority_stage1 and q4_final_count_stage2
+// (kernels/q4.metal:21-94); priorities 1..5 are the characters '1'..'5'. out5 = counts.
+void ref_q4(uint64_t n_or, const int32_t* or_key, const int32_t* or_date, const uint8_t* or_prio,
+            uint64_t n_li, const int32_t* li_key, const int32_t* li_commit, const int32_t* li_receipt,
+            int32_t date_lo, int32_t date_hi, int groups, int threads, uint32_t* out5) {
+  int max_key = 0;
+  for (uint64_t i = 0; i < n_or; i++) max_key = std::max(max_key, or_key[i]);
+  for (uint64_t i = 0; i < n_li; i++) max_key = std::max(max_key, li_key[i]);
+  std::vector<atomic_uint> late((size_t)(max_key + 31) / 32 + 1);
+  for (auto& w : late) w.v = 0;
+  std::vector<int> lc = dates(n_li, li_commit), lr = dates(n_li, li_receipt), od = dates(n_or, or_date);
+  uint nli = (uint)n_li, nor = (uint)n_or;
+  for (uint i = 0; i < nli; i++) q4_build_late_bitmap(li_key, lc.data(), lr.data(), late.data(), nli, i);
+  std::vector<char> pr(n_or);
+  for (uint64_t i = 0; i < n_or; i++) pr[i] = (char)('0' + or_prio[i]);
+  std::vector<uint> partial((size_t)groups * 5);
+  int ds = yyyymmdd(date_lo), de = yyyymmdd(date_hi);
+  const uint* bm = reinterpret_cast<const uint*>(late.data());
+  run_groups((uint)groups, threads, [&](uint g) {
+    q4_count_by_priority_stage1(or_key, od.data(), pr.data(), bm, partial.data(), nor, ds, de, g, 0, 1, (uint)groups);
+  });
+  uint ng = (uint)groups;
+  q4_final_count_stage2(partial.data(), out5, ng, 0);
+}
+
+// Q12 through q12_build_priority_bitmap, q12_filter_and_count_stage1 and
+// q12_final_count_stage2 (kernels/q12.metal:22-99): ship modes as the first character of
+// their names ('M' MAIL, 'S' SHIP are counted), high priority = '1' or '2'.
+// out4 = MAIL high, MAIL low, SHIP high, SHIP low.
+void ref_q12(uint64_t n_or, const int32_t* or_key, const uint8_t* or_prio, uint64_t n_li,
+             const int32_t* li_key, const int32_t* li_ship, const int32_t* li_commit,
+             const int32_t* li_receipt, const uint8_t* li_mode, int32_t receipt_lo, int32_t receipt_hi,
+             int groups, int threads, uint32_t* out4) {
+  int max_key = 0;
+  for (uint64_t i = 0; i < n_or; i++) max_key = std::max(max_key, or_key[i]);
+  for (uint64_t i = 0; i < n_li; i++) max_key = std::max(max_key, li_key[i]);
+  std::vector<atomic_uint> bitmap((size_t)(max_key + 31) / 32 + 1);
+  for (auto& w : bitmap) w.v = 0;
+  std::vector<char> pr(n_or);
+  for (uint64_t i = 0; i < n_or; i++) pr[i] = (char)('0' + or_prio[i]);
+  uint nor = (uint)n_or, nli = (uint)n_li;
+  for (uint i = 0; i < nor; i++) q12_build_priority_bitmap(or_key, pr.data(), bitmap.data(), nor, i);
+  std::vector<char> sm(n_li);
+  for (uint64_t i = 0; i < n_li; i++) sm[i] = "AFMRRST"[li_mode[i] % 7];   // AIR FOB MAIL RAIL REG AIR SHIP TRUCK
+  std::vector<int> ls = dates(n_li, li_ship), lc = dates(n_li, li_commit), lr = dates(n_li, li_receipt);
+  std::vector<uint> partial((size_t)groups * 4);
+  int rs = yyyymmdd(receipt_lo), re = yyyymmdd(receipt_hi);
+  const uint* bm = reinterpret_cast<const uint*>(bitmap.data());
+  run_groups((uint)groups, threads, [&](uint g) {
+    q12_filter_and_count_stage1(li_key, sm.data(), ls.data(), lc.data(), lr.data(), bm, partial.data(), nli, rs, re,
+                                g, 0, 1, (uint)groups);
+  });
+  uint ng = (uint)groups;
+  q12_final_count_stage2(partial.data(), out4, ng, 0);
 }
 
 // Q9 through q9_build_part_ht_kernel, q9_build_supplier_ht_kernel,

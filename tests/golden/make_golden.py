@@ -55,6 +55,14 @@ def column(name, n, seed, off=0, n_orders=0, n_cust=0, n_parts=0, n_supp=0, mode
         return [uniform(k(24), r, 0, n_parts - 1) for r in rows]
     if name == "supp_key":
         return [(uniform(k(24), r, 0, n_parts - 1) + uniform(k(25), r, 0, 3) * (n_supp // 4)) % n_supp for r in rows]
+    if name == "commit_date":
+        return [uniform(k(16), r, 0, 2526) + uniform(k(27), r, -91, 89) for r in rows]
+    if name == "receipt_date":
+        return [uniform(k(16), r, 0, 2526) + uniform(k(28), r, 1, 30) for r in rows]
+    if name == "ship_mode":
+        return [uniform(k(29), r, 0, 6) for r in rows]
+    if name == "o_priority":
+        return [uniform(k(50), r, 1, 5) for r in rows]
     if name == "segment":
         return [uniform(k(32), r, 0, 4) for r in rows]
     if name == "o_cust":
@@ -130,8 +138,38 @@ def q9(n_pa, n_su, n_or, n_li, seed):
     return [[a, b, str(v)] for (a, b), v in rows]
 
 
+def q4_q12_tables(n_or, n_li, seed):
+    od = {"order_key": [4 * i + 1 for i in range(n_or)], "order_date": column("o_date", n_or, seed),
+          "priority": column("o_priority", n_or, seed)}
+    li = {c: column(c, n_li, seed, n_orders=n_or, mode=1)
+          for c in ("order_key", "ship_date", "commit_date", "receipt_date", "ship_mode")}
+    return od, li
+
+
+def q4(n_or, n_li, seed, date_lo=547, date_hi=639):
+    od, li = q4_q12_tables(n_or, n_li, seed)
+    late = {k for k, c, r in zip(li["order_key"], li["commit_date"], li["receipt_date"]) if c < r}
+    cnt = [0] * 5
+    for k, d, p in zip(od["order_key"], od["order_date"], od["priority"]):
+        if date_lo <= d < date_hi and k in late:
+            cnt[p - 1] += 1
+    return cnt
+
+
+def q12(n_or, n_li, seed, receipt_lo=731, receipt_hi=1096, modes=(2, 5), high_max=2):
+    od, li = q4_q12_tables(n_or, n_li, seed)
+    high = {k for k, p in zip(od["order_key"], od["priority"]) if 1 <= p <= high_max}
+    out = [[0, 0], [0, 0]]
+    for k, s, c, r, m in zip(*(li[x] for x in ("order_key", "ship_date", "commit_date", "receipt_date",
+                                                "ship_mode"))):
+        if m not in modes or not (receipt_lo <= r < receipt_hi) or c >= r or s >= c:
+            continue
+        out[modes.index(m)][0 if k in high else 1] += 1
+    return out
+
+
 def main():
-    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}}
+    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}}
     # generator: first values and column sums for two seeds and a shifted window
     for seed, off in ((42, 0), (7, 1000)):
         cols = {}
@@ -145,6 +183,9 @@ def main():
             cols["order_key_uniform"] = {"head": v2[:8], "sum": sum(v2)}
         v = column("supp_key", 64, seed, off, n_parts=1000, n_supp=100)
         cols["supp_key"] = {"head": v[:8], "sum": sum(v)}
+        for name in ("commit_date", "receipt_date", "ship_mode", "o_priority"):
+            v = column(name, 64, seed, off)
+            cols[name] = {"head": v[:8], "sum": sum(v)}
         out["generator"]["%d_%d" % (seed, off)] = cols
     for n, seed in ((3000, 42), (2500, 9)):
         li = {c: column(c, n, seed) for c in ("ship_date", "quantity", "ext_price", "discount", "tax", "flag",
@@ -156,6 +197,10 @@ def main():
     out["q3"]["300_1200_4800_42"] = q3(300, 1200, 4800, 42)
     out["q3"]["200_900_3000_5_seg3"] = q3(200, 900, 3000, 5, segment=3, date_lt=2000, ship_gt=300, k=20)
     out["q9"]["400_40_1500_6000_42"] = q9(400, 40, 1500, 6000, 42)
+    out["q4"]["3000_12000_42"] = q4(3000, 12000, 42)
+    out["q4"]["2000_9000_5_wide"] = q4(2000, 9000, 5, 0, 2406)
+    out["q12"]["3000_12000_42"] = q12(3000, 12000, 42)
+    out["q12"]["2000_9000_5_air_truck_hi3"] = q12(2000, 9000, 5, 0, 2600, (0, 6), 3)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

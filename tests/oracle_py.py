@@ -9,8 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgpudbref.so")
 
-WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 20: 4, 21: 1, 30: 4, 31: 4, 32: 4,
-         40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
+WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 11: 4, 12: 4, 13: 1, 20: 4, 21: 1, 30: 4,
+         31: 4, 32: 4, 33: 1, 40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
 DT = {1: np.uint8, 4: np.int32, 8: np.int64}
 
 
@@ -33,6 +33,8 @@ ORACLE_ARGS = {
     "or_q1_mt": [C.c_int, U64, V, V, V, V, V, V, V, I32, V],
     "or_q3": [U64, V, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, I32, I32, V, V, V],
     "or_q9": [U64, V, V, I32, U64, V, V, I32, U64, V, V, V, U64, V, V, I32, U64, V, V, V, V, V, V, U32, V, V, V],
+    "or_q4": [U64, V, V, V, I32, U64, V, V, V, I32, I32, V],
+    "or_q12": [U64, V, V, I32, U64, V, V, V, V, V, I32, I32, I32, I32, I32, V],
     "or_select_lt": [U64, V, I32, V, V],
     "or_sum_i32": [U64, V],
     "or_join_count": [U64, V, U64, V],
@@ -46,6 +48,8 @@ REF_ARGS = {
     "ref_q1": [U64, V, V, V, V, V, V, V, I32, C.c_int, C.c_int, V],
     "ref_q3": [U64, V, V, U64, V, V, V, U64, V, V, V, V, I32, I32, I32, C.c_int, C.c_int, V, V, V, U32],
     "ref_q9": [U64, V, V, U64, V, V, U64, V, V, V, U64, V, V, U64, V, V, V, V, V, V, C.c_int, C.c_int, V, V, V, U32],
+    "ref_q4": [U64, V, V, V, U64, V, V, V, I32, I32, C.c_int, C.c_int, V],
+    "ref_q12": [U64, V, V, U64, V, V, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_select_lt": [U64, V, I32, V],
     "ref_sum": [U64, V, C.c_int, C.c_int],
     "ref_join_count": [U64, V, U64, V],
@@ -111,7 +115,7 @@ def gen(column, n_rows, seed=42, row_offset=0, n_orders=0, n_cust=0, n_parts=0, 
 def lineitem(n, seed=42, n_orders=0, order_mode=0, n_parts=0, n_supp=0, row_offset=0,
              cols=("ship_date", "quantity", "ext_price", "discount", "tax", "flag", "status")):
     ids = dict(ship_date=1, quantity=2, ext_price=3, discount=4, tax=5, flag=6, status=7, order_key=8,
-               part_key=9, supp_key=10)
+               part_key=9, supp_key=10, commit_date=11, receipt_date=12, ship_mode=13)
     return {c: gen(ids[c], n, seed, row_offset, n_orders, 0, n_parts, n_supp, order_mode) for c in cols}
 
 
@@ -120,6 +124,15 @@ def q3_tables(n_cu, n_or, n_li, seed=42):
     od = dict(order_key=gen(30, n_or, seed), cust_key=gen(31, n_or, seed, n_cust=n_cu), order_date=gen(32, n_or, seed))
     li = lineitem(n_li, seed, n_orders=n_or, order_mode=1, cols=("order_key", "ship_date", "ext_price", "discount"))
     return cu, od, li
+
+
+def q4_tables(n_or, n_li, seed=42, order_mode=1):
+    """Orders (key, date, priority) and lineitem (order key, ship/commit/receipt dates, ship
+    mode) of the seeded generator: the tables of Q4 and Q12."""
+    od = dict(order_key=gen(30, n_or, seed), order_date=gen(32, n_or, seed), priority=gen(33, n_or, seed))
+    li = lineitem(n_li, seed, n_orders=n_or, order_mode=order_mode,
+                  cols=("order_key", "ship_date", "commit_date", "receipt_date", "ship_mode"))
+    return od, li
 
 
 def q9_tables(n_pa, n_su, n_or, n_li, seed=42):
@@ -197,6 +210,26 @@ def q9(pa, su, ps, od, li, cap=4096):
                        gy.ctypes.data, gp.ctypes.data)
     m = min(n, cap)
     return [(int(gn[i]), int(gy[i]), int(gp[i])) for i in range(m)], int(n)
+
+
+def q4(od, li, date_lo=547, date_hi=639, or_key_max=None):
+    """[count of priority 1..5]."""
+    out = np.zeros(5, np.uint64)
+    kmax = int(od["order_key"].max()) if or_key_max is None and len(od["order_key"]) else (or_key_max or 0)
+    oracle().or_q4(len(od["order_key"]), _p(od["order_key"]), _p(od["order_date"]), _p(od["priority"]), kmax,
+                   len(li["order_key"]), _p(li["order_key"]), _p(li["commit_date"]), _p(li["receipt_date"]),
+                   date_lo, date_hi, out.ctypes.data)
+    return [int(x) for x in out]
+
+
+def q12(od, li, receipt_lo=731, receipt_hi=1096, modes=(2, 5), high_max=2, or_key_max=None):
+    """[(high, low) for mode0, (high, low) for mode1]."""
+    out = np.zeros(4, np.uint64)
+    kmax = int(od["order_key"].max()) if or_key_max is None and len(od["order_key"]) else (or_key_max or 0)
+    oracle().or_q12(len(od["order_key"]), _p(od["order_key"]), _p(od["priority"]), kmax, len(li["order_key"]),
+                    _p(li["order_key"]), _p(li["ship_date"]), _p(li["commit_date"]), _p(li["receipt_date"]),
+                    _p(li["ship_mode"]), receipt_lo, receipt_hi, modes[0], modes[1], high_max, out.ctypes.data)
+    return [(int(out[0]), int(out[2])), (int(out[1]), int(out[3]))]
 
 
 def select_lt(col, value):

@@ -35,6 +35,10 @@ def test_generator_matches_golden(orc):
         assert int(ou.sum()) == cols["order_key_uniform"]["sum"]
         sk = orc.gen(10, 64, seed, off, n_parts=1000, n_supp=100)
         assert sk[:8].tolist() == cols["supp_key"]["head"]
+        for name, cid in (("commit_date", 11), ("receipt_date", 12), ("ship_mode", 13), ("o_priority", 33)):
+            v = orc.gen(cid, 64, seed, off)
+            assert v[:8].tolist() == cols[name]["head"], (key, name)
+            assert int(v.astype(np.int64).sum()) == cols[name]["sum"], (key, name)
 
 
 @pytest.mark.parametrize("n,seed", [(3000, 42), (2500, 9)])
@@ -70,6 +74,15 @@ def test_q9_matches_golden(orc):
     rows, n = orc.q9(*tabs)
     assert [[a, b, str(c)] for a, b, c in rows] == GOLDEN["q9"]["400_40_1500_6000_42"]
     assert n == len(rows)
+
+
+def test_q4_q12_match_golden(orc):
+    od, li = orc.q4_tables(3000, 12000, 42)
+    assert orc.q4(od, li) == GOLDEN["q4"]["3000_12000_42"]
+    assert orc.q12(od, li) == [tuple(x) for x in GOLDEN["q12"]["3000_12000_42"]]
+    od, li = orc.q4_tables(2000, 9000, 5)
+    assert orc.q4(od, li, 0, 2406) == GOLDEN["q4"]["2000_9000_5_wide"]
+    assert orc.q12(od, li, 0, 2600, (0, 6), 3) == [tuple(x) for x in GOLDEN["q12"]["2000_9000_5_air_truck_hi3"]]
 
 
 def test_q1_q6_threaded_equal_serial(orc):
@@ -161,6 +174,34 @@ def test_q9_pinned_to_reference_kernels(orc):
     assert set(theirs) == {(a, b) for a, b, _ in mine}
     for a, b, p in mine:
         assert theirs[(a, b)] == pytest.approx(p / 10000.0, rel=1e-4, abs=1.0)
+
+
+@pytest.mark.parametrize("n_or,n_li,seed,window", [(3000, 12000, 42, (547, 639)), (20000, 90000, 7, (0, 2406)),
+                                                    (5000, 20000, 3, (1500, 1530))])
+def test_q4_pinned_to_reference_kernels(orc, n_or, n_li, seed, window):
+    """Q4 counts are integers in the reference too: bit-exact against its kernels."""
+    ref = need_ref(orc)
+    od, li = orc.q4_tables(n_or, n_li, seed)
+    out = np.zeros(5, np.uint32)
+    ref.ref_q4(n_or, od["order_key"].ctypes.data, od["order_date"].ctypes.data, od["priority"].ctypes.data, n_li,
+               li["order_key"].ctypes.data, li["commit_date"].ctypes.data, li["receipt_date"].ctypes.data, *window,
+               16, 4, out.ctypes.data)
+    assert orc.q4(od, li, *window) == out.tolist()
+
+
+@pytest.mark.parametrize("n_or,n_li,seed,window", [(3000, 12000, 42, (731, 1096)), (20000, 90000, 7, (0, 2600)),
+                                                    (5000, 20000, 3, (900, 960))])
+def test_q12_pinned_to_reference_kernels(orc, n_or, n_li, seed, window):
+    """Q12 with the query's modes (MAIL, SHIP) and priorities ('1-URGENT', '2-HIGH'): bit-exact
+    against the reference's kernels (bins MAIL high, MAIL low, SHIP high, SHIP low)."""
+    ref = need_ref(orc)
+    od, li = orc.q4_tables(n_or, n_li, seed)
+    out = np.zeros(4, np.uint32)
+    ref.ref_q12(n_or, od["order_key"].ctypes.data, od["priority"].ctypes.data, n_li, li["order_key"].ctypes.data,
+                li["ship_date"].ctypes.data, li["commit_date"].ctypes.data, li["receipt_date"].ctypes.data,
+                li["ship_mode"].ctypes.data, *window, 16, 4, out.ctypes.data)
+    (mh, ml), (sh, sl) = orc.q12(od, li, *window)
+    assert [mh, ml, sh, sl] == out.tolist()
 
 
 def test_micro_pinned_to_reference_kernels(orc):
