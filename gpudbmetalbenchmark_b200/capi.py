@@ -27,12 +27,12 @@ OPT_Q9_SMEM_SLOTS = 6
 OPT_Q9_GLOBAL_SLOTS = 7
 OPT_GRAPHS = 8
 TBL_LINEITEM, TBL_ORDERS, TBL_CUSTOMER, TBL_PART, TBL_SUPPLIER, TBL_PARTSUPP = 1, 2, 3, 4, 5, 6
-TBL_MAX_COLS = 10
+TBL_MAX_COLS = 13
 # columns a .tbl parse keeps, in the order of gpudb_tbl_parse's cols[]
 TBL_COLUMNS = {
     "lineitem": (TBL_LINEITEM, ("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax",
-                                "flag", "status", "ship_date")),
-    "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date")),
+                                "flag", "status", "ship_date", "commit_date", "receipt_date", "ship_mode")),
+    "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date", "priority")),
     "customer": (TBL_CUSTOMER, ("cust_key", "segment")),
     "part": (TBL_PART, ("part_key", "flag")),
     "supplier": (TBL_SUPPLIER, ("supp_key", "nation")),

@@ -42,6 +42,9 @@ std::pair<int, int> li_tbl_column(int32_t id) {
     case GPUDB_COL_LI_TAX: return {6, 4};
     case GPUDB_COL_LI_FLAG: return {7, 1};
     case GPUDB_COL_LI_STATUS: return {8, 1};
+    case GPUDB_COL_LI_COMMIT_DATE: return {10, 4};
+    case GPUDB_COL_LI_RECEIPT_DATE: return {11, 4};
+    case GPUDB_COL_LI_SHIP_MODE: return {12, 1};
     default: return {9, 4};   // ship date
   }
 }
@@ -58,7 +61,33 @@ void set_li_column(gpudb_lineitem& li, int32_t id, void* p) {
     case GPUDB_COL_LI_ORDER_KEY: li.order_key = (const int32_t*)p; break;
     case GPUDB_COL_LI_PART_KEY: li.part_key = (const int32_t*)p; break;
     case GPUDB_COL_LI_SUPP_KEY: li.supp_key = (const int32_t*)p; break;
+    case GPUDB_COL_LI_COMMIT_DATE: li.commit_date = (const int32_t*)p; break;
+    case GPUDB_COL_LI_RECEIPT_DATE: li.receipt_date = (const int32_t*)p; break;
+    case GPUDB_COL_LI_SHIP_MODE: li.ship_mode = (const uint8_t*)p; break;
   }
+}
+
+// Orders with key, date and priority (Q4, Q12): generated, or parsed from orders.tbl.
+struct OrdersKDP {
+  gpudb_orders od{};
+  TblTable t;
+  Buffer key, date, prio;
+};
+
+void make_orders_kdp(gpudb_ctx* ctx, const RunOptions& o, OrdersKDP& O) {
+  if (!o.data_dir.empty()) {
+    O.t = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 2, 3}, {4, 4, 1}, o.tbl_piece);
+    O.od = {O.t.rows, O.t.col_max[0], 0, O.t.col<int32_t>(0), nullptr, O.t.col<int32_t>(2), O.t.col<uint8_t>(3)};
+    return;
+  }
+  gpudb_gen_spec os{};
+  os.seed = o.seed;
+  os.n_rows = o.scale.orders;
+  O.key = generate(ctx, os, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
+  O.date = generate(ctx, os, GPUDB_COL_OR_ORDER_DATE, GPUDB_MEM_DEVICE);
+  O.prio = generate(ctx, os, GPUDB_COL_OR_PRIORITY, GPUDB_MEM_DEVICE);
+  O.od = {o.scale.orders, (int32_t)(4 * (o.scale.orders - 1) + 1), 0, O.key.as<int32_t>(), nullptr,
+          O.date.as<int32_t>(), O.prio.as<uint8_t>()};
 }
 
 // The fact columns a pipeline needs: generated (device-resident, or pinned host memory when
@@ -215,6 +244,59 @@ void runQ3Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
     header(o, "Q3", L.li.n_rows, t, mode == GPUDB_JOIN_GLOBAL ? " (lineitem)" : " (lineitem, radix)");
     printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
   }
+}
+
+void runQ4Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 4 Benchmark ---\n");
+  const double t0 = now_ms();
+  OrdersKDP O;
+  make_orders_kdp(ctx, o, O);
+  Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_COMMIT_DATE, GPUDB_COL_LI_RECEIPT_DATE},
+                             GPUDB_ORDERS_CLUSTERED, (int64_t)O.od.n_rows, 0, 0);
+  const double gen_ms = now_ms() - t0;
+  std::printf("Loaded %" PRIu64 " lineitem, %" PRIu64 " orders rows for Q4.\n", L.li.n_rows, O.od.n_rows);
+  const gpudb_q4_params p{547, 639};   // 1993-07-01 <= o_orderdate < 1993-10-01
+  gpudb_q4_result r{};
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q4_priority(ctx, &O.od, &L.li, &p, &r, &t, nullptr), "gpudb_q4");
+  const double p0 = now_ms();
+  static const char* names[5] = {"1-URGENT", "2-HIGH", "3-MEDIUM", "4-NOT SPECIFIED", "5-LOW"};
+  std::printf("\nTPC-H Q4 Results:\n");
+  std::printf("+------------------+-------------+\n");
+  std::printf("| o_orderpriority  | order_count |\n");
+  std::printf("+------------------+-------------+\n");
+  for (int i = 0; i < 5; i++) std::printf("| %-16s | %11" PRIu64 " |\n", names[i], r.count[i]);
+  std::printf("+------------------+-------------+\n");
+  if (o.scale.streamed) header(o, "Q4", L.li.n_rows, t);
+  else std::printf("\nQ4 | %" PRIu64 " lineitem, %" PRIu64 " orders\n", L.li.n_rows, O.od.n_rows);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
+}
+
+void runQ12Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 12 Benchmark ---\n");
+  const double t0 = now_ms();
+  OrdersKDP O;
+  make_orders_kdp(ctx, o, O);
+  Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_SHIP_DATE, GPUDB_COL_LI_COMMIT_DATE,
+                                      GPUDB_COL_LI_RECEIPT_DATE, GPUDB_COL_LI_SHIP_MODE},
+                             GPUDB_ORDERS_CLUSTERED, (int64_t)O.od.n_rows, 0, 0);
+  const double gen_ms = now_ms() - t0;
+  std::printf("Loaded %" PRIu64 " orders, %" PRIu64 " lineitem rows for Q12.\n", O.od.n_rows, L.li.n_rows);
+  // 1994-01-01 <= l_receiptdate < 1995-01-01, MAIL and SHIP, priorities 1-URGENT and 2-HIGH
+  const gpudb_q12_params p{731, 1096, {GPUDB_MODE_MAIL, GPUDB_MODE_SHIP}, 2, 0};
+  gpudb_q12_result r{};
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q12_shipmode(ctx, &O.od, &L.li, &p, &r, &t, nullptr), "gpudb_q12");
+  const double p0 = now_ms();
+  std::printf("\nTPC-H Q12 Results:\n");
+  std::printf("+----------+------------------+-----------------+\n");
+  std::printf("| shipmode | high_line_count  | low_line_count  |\n");
+  std::printf("+----------+------------------+-----------------+\n");
+  std::printf("| MAIL     | %16" PRIu64 " | %15" PRIu64 " |\n", r.high[0], r.low[0]);
+  std::printf("| SHIP     | %16" PRIu64 " | %15" PRIu64 " |\n", r.high[1], r.low[1]);
+  std::printf("+----------+------------------+-----------------+\n");
+  header(o, "Q12", L.li.n_rows, t);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
 void runQ9Benchmark(gpudb_ctx* ctx, const RunOptions& o) {

@@ -29,7 +29,9 @@ namespace {
 constexpr int kTT = 256;                              // threads per tile
 constexpr uint64_t kTileBytes = (uint64_t)kTT * 64;   // 64 bytes per thread
 
-enum FieldType : int32_t { F_I32, F_DEC64, F_DEC32, F_QTY, F_DATE, F_RETFLAG, F_LINESTATUS, F_SEGMENT, F_GREEN, F_U8 };
+enum FieldType : int32_t {
+  F_I32, F_DEC64, F_DEC32, F_QTY, F_DATE, F_RETFLAG, F_LINESTATUS, F_SEGMENT, F_GREEN, F_U8, F_SHIPMODE, F_PRIORITY
+};
 
 struct TblSpec {
   int32_t n;                                  // columns kept
@@ -40,9 +42,10 @@ struct TblSpec {
 
 bool spec_for(int32_t table, TblSpec* s) {
   static const struct { int32_t table, n, field[GPUDB_TBL_MAX_COLS], type[GPUDB_TBL_MAX_COLS]; } specs[] = {
-      {GPUDB_TBL_LINEITEM, 10, {0, 1, 2, 4, 5, 6, 7, 8, 9, 10},
-       {F_I32, F_I32, F_I32, F_QTY, F_DEC64, F_DEC32, F_DEC32, F_RETFLAG, F_LINESTATUS, F_DATE}},
-      {GPUDB_TBL_ORDERS, 3, {0, 1, 4}, {F_I32, F_I32, F_DATE}},
+      {GPUDB_TBL_LINEITEM, 13, {0, 1, 2, 4, 5, 6, 7, 8, 9, 10, 11, 12, 14},
+       {F_I32, F_I32, F_I32, F_QTY, F_DEC64, F_DEC32, F_DEC32, F_RETFLAG, F_LINESTATUS, F_DATE, F_DATE, F_DATE,
+        F_SHIPMODE}},
+      {GPUDB_TBL_ORDERS, 4, {0, 1, 4, 5}, {F_I32, F_I32, F_DATE, F_PRIORITY}},
       {GPUDB_TBL_CUSTOMER, 2, {0, 6}, {F_I32, F_SEGMENT}},
       {GPUDB_TBL_PART, 2, {0, 1}, {F_I32, F_GREEN}},
       {GPUDB_TBL_SUPPLIER, 2, {0, 3}, {F_I32, F_U8}},
@@ -221,6 +224,16 @@ __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ 
                 : field_equals(s, fe, "MACHINERY") ? 4 : -1;
             ok = v >= 0;
             break;
+          case F_SHIPMODE:   // alphabetical codes: ORDER BY l_shipmode
+            v = field_equals(s, fe, "AIR") ? 0 : field_equals(s, fe, "FOB") ? 1 : field_equals(s, fe, "MAIL") ? 2
+                : field_equals(s, fe, "RAIL") ? 3 : field_equals(s, fe, "REG AIR") ? 4
+                : field_equals(s, fe, "SHIP") ? 5 : field_equals(s, fe, "TRUCK") ? 6 : -1;
+            ok = v >= 0;
+            break;
+          case F_PRIORITY:   // "1-URGENT" .. "5-LOW": the leading digit
+            ok = fe - s >= 2 && *s >= '1' && *s <= '5' && s[1] == '-';
+            v = ok ? *s - '0' : 0;
+            break;
           case F_GREEN: {
             v = 0;
             for (const uint8_t* p = s; p + 5 <= fe && !v; p++)
@@ -233,7 +246,8 @@ __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ 
         if (col) {
           switch (spec.type[k]) {
             case F_DEC64: static_cast<int64_t*>(col)[r] = v; break;
-            case F_RETFLAG: case F_LINESTATUS: case F_SEGMENT: case F_GREEN: case F_U8:
+            case F_RETFLAG: case F_LINESTATUS: case F_SEGMENT: case F_GREEN: case F_U8: case F_SHIPMODE:
+            case F_PRIORITY:
               static_cast<uint8_t*>(col)[r] = (uint8_t)v; break;
             default: static_cast<int32_t*>(col)[r] = (int32_t)v; break;
           }

@@ -404,12 +404,14 @@ int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timin
  * allowed) on the GPU into the engine's columns. Encodings: integers as int32; decimals (at
  * most two fraction digits) as hundredths; dates "YYYY-MM-DD" as days since 1992-01-01;
  * return flag A/N/R -> 0/1/2; line status F/O -> 0/1; market segment AUTOMOBILE, BUILDING,
- * FURNITURE, HOUSEHOLD, MACHINERY -> 0..4; part name -> 1 if it contains "green". (The
+ * FURNITURE, HOUSEHOLD, MACHINERY -> 0..4; part name -> 1 if it contains "green"; ship mode
+ * AIR, FOB, MAIL, RAIL, REG AIR, SHIP, TRUCK -> 0..6; order priority "1-URGENT".."5-LOW" -> 1..5. (The
  * reference keeps dates as YYYYMMDD ints and money as float.) Columns kept, in cols[] order,
  * with the dbgen fields they come from:
  *   LINEITEM: order_key, part_key, supp_key, quantity, ext_price (int64), discount, tax,
- *             flag (u8), status (u8), ship_date                  fields 0,1,2,4,5,6,7,8,9,10
- *   ORDERS:   order_key, cust_key, order_date                      fields 0,1,4
+ *             flag (u8), status (u8), ship_date, commit_date, receipt_date, ship_mode (u8)
+ *                                                     fields 0,1,2,4,5,6,7,8,9,10,11,12,14
+ *   ORDERS:   order_key, cust_key, order_date, priority (u8)       fields 0,1,4,5
  *   CUSTOMER: cust_key, segment (u8)                               fields 0,6
  *   PART:     part_key, flag (u8)                                  fields 0,1
  *   SUPPLIER: supp_key, nation (u8)                                fields 0,3
@@ -422,7 +424,7 @@ int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timin
  * GPUDB_E_CAPACITY. gpudb_tbl_count_rows counts the rows without parsing them. */
 enum { GPUDB_TBL_LINEITEM = 1, GPUDB_TBL_ORDERS = 2, GPUDB_TBL_CUSTOMER = 3, GPUDB_TBL_PART = 4,
        GPUDB_TBL_SUPPLIER = 5, GPUDB_TBL_PARTSUPP = 6 };
-#define GPUDB_TBL_MAX_COLS 10
+#define GPUDB_TBL_MAX_COLS 13
 int gpudb_tbl_count_rows(gpudb_ctx* ctx, const char* text, uint64_t bytes, int32_t location, uint64_t* n_rows);
 int gpudb_tbl_parse(gpudb_ctx* ctx, int32_t table, const char* text, uint64_t bytes, int32_t location,
                     void* const* cols, uint64_t capacity, uint64_t* n_rows, int32_t* col_max,

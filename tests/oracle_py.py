@@ -271,6 +271,8 @@ import datetime as _dt
 _EPOCH = _dt.date(1992, 1, 1)
 _SEGMENTS = ("AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY")
 _FLAGS, _STATUS = "ANR", "FO"
+_MODES = ("AIR", "FOB", "MAIL", "RAIL", "REG AIR", "SHIP", "TRUCK")
+_PRIORITIES = ("1-URGENT", "2-HIGH", "3-MEDIUM", "4-NOT SPECIFIED", "5-LOW")
 
 
 def _date(d):
@@ -289,14 +291,19 @@ def format_tbl(kind, c):
         n = len(c["order_key"])
         for i in range(n):
             sd = int(c["ship_date"][i])
-            out.append("%d|%d|%d|%d|%d|%s|0.%02d|0.%02d|%s|%s|%s|%s|%s|DELIVER IN PERSON|TRUCK|row %d of the sample|"
+            cd = int(c["commit_date"][i]) if "commit_date" in c else sd + 30
+            rd = int(c["receipt_date"][i]) if "receipt_date" in c else sd + 45
+            mode = _MODES[c["ship_mode"][i]] if "ship_mode" in c else "TRUCK"
+            out.append("%d|%d|%d|%d|%d|%s|0.%02d|0.%02d|%s|%s|%s|%s|%s|DELIVER IN PERSON|%s|row %d of the sample|"
                        % (c["order_key"][i], c["part_key"][i], c["supp_key"][i], i % 7 + 1, c["quantity"][i],
                           _money(c["ext_price"][i]), c["discount"][i], c["tax"][i], _FLAGS[c["flag"][i]],
-                          _STATUS[c["status"][i]], _date(sd), _date(sd + 30), _date(sd + 45), i))
+                          _STATUS[c["status"][i]], _date(sd), _date(cd), _date(rd), mode, i))
     elif kind == "orders":
         for i in range(len(c["order_key"])):
-            out.append("%d|%d|O|%s|%s|3-MEDIUM|Clerk#%09d|0|an order|" % (c["order_key"][i], c["cust_key"][i],
-                                                                             _money(12345 + i), _date(c["order_date"][i]), i))
+            prio = _PRIORITIES[c["priority"][i] - 1] if "priority" in c else "3-MEDIUM"
+            out.append("%d|%d|O|%s|%s|%s|Clerk#%09d|0|an order|" % (c["order_key"][i], c["cust_key"][i],
+                                                                        _money(12345 + i), _date(c["order_date"][i]),
+                                                                        prio, i))
     elif kind == "customer":
         for i in range(len(c["cust_key"])):
             out.append("%d|Customer#%09d|addr %d|%d|10-123-456-7890|%s|%s|a customer|"
@@ -324,8 +331,9 @@ def parse_tbl_cpu(kind, text):
     columns in the engine's encoding."""
     keep = {"lineitem": [(0, "order_key", "i"), (1, "part_key", "i"), (2, "supp_key", "i"), (4, "quantity", "q"),
                          (5, "ext_price", "m"), (6, "discount", "m"), (7, "tax", "m"), (8, "flag", "r"),
-                         (9, "status", "s"), (10, "ship_date", "d")],
-            "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d")],
+                         (9, "status", "s"), (10, "ship_date", "d"), (11, "commit_date", "d"),
+                         (12, "receipt_date", "d"), (14, "ship_mode", "e")],
+            "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d"), (5, "priority", "p")],
             "customer": [(0, "cust_key", "i"), (6, "segment", "g")],
             "part": [(0, "part_key", "i"), (1, "flag", "n")],
             "supplier": [(0, "supp_key", "i"), (3, "nation", "i")],
@@ -339,6 +347,6 @@ def parse_tbl_cpu(kind, text):
 
     conv = {"i": int, "q": lambda s: money(s) // 100, "m": money, "r": _FLAGS.index, "s": _STATUS.index,
             "d": lambda s: (_dt.date.fromisoformat(s) - _EPOCH).days, "g": _SEGMENTS.index,
-            "n": lambda s: int("green" in s)}
+            "n": lambda s: int("green" in s), "e": _MODES.index, "p": lambda s: _PRIORITIES.index(s) + 1}
     rows = [l.rstrip("\r").split("|") for l in text.decode().split("\n") if l != ""]
     return {name: [conv[t](r[f]) for r in rows] for f, name, t in keep}

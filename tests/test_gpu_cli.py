@@ -74,6 +74,29 @@ def test_cli_q9(orc):
     timing_ok(out, "Q9", 60000)
 
 
+def q4_rows(out):
+    return [int(x) for x in re.findall(r"^\| [1-5]-[A-Z ]+?\s+\|\s+(\d+) \|$", out, re.M)]
+
+
+def q12_rows(out):
+    return [(int(h), int(l)) for h, l in re.findall(r"^\| (?:MAIL|SHIP)\s+\|\s+(\d+) \|\s+(\d+) \|$", out, re.M)]
+
+
+def test_cli_q4_and_q12(orc):
+    od, li = orc.q4_tables(15_000, 60_000, 42)
+    out = run("sf1", "q4", "--scale", "0.01")
+    assert q4_rows(out) == orc.q4(od, li)
+    assert re.search(r"^Q4 \| 60000 lineitem, 15000 orders", out, re.M)
+    for t in TIMING:
+        assert t in out
+    out = run("sf1", "q12", "--scale", "0.01")
+    assert q12_rows(out) == orc.q12(od, li)
+    timing_ok(out, "Q12", 60000)
+    out = run("sf100", "q12", "--scale", "0.001")   # streamed lineitem
+    od, li = orc.q4_tables(150_000, 600_000, 42)
+    assert q12_rows(out) == orc.q12(od, li)
+
+
 def test_cli_microbenchmarks(orc):
     out = run("sf1", "selection", "--scale", "0.01")
     col = orc.gen(1, 60000, 42)
@@ -107,8 +130,9 @@ def test_cli_reads_tbl_files(orc, tmp_path):
     n_or, n_cu, n_pa, n_su, n_li = 15_000, 1_500, 2_000, 100, 60_000
     li = orc.lineitem(n_li, seed=7, n_orders=n_or, order_mode=1, n_parts=n_pa, n_supp=n_su,
                       cols=("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag",
-                            "status", "ship_date"))
-    od = dict(order_key=orc.gen(30, n_or, 7), cust_key=orc.gen(31, n_or, 7, n_cust=n_cu), order_date=orc.gen(32, n_or, 7))
+                            "status", "ship_date", "commit_date", "receipt_date", "ship_mode"))
+    od = dict(order_key=orc.gen(30, n_or, 7), cust_key=orc.gen(31, n_or, 7, n_cust=n_cu), order_date=orc.gen(32, n_or, 7),
+              priority=orc.gen(33, n_or, 7))
     cu = dict(cust_key=orc.gen(20, n_cu, 7), segment=orc.gen(21, n_cu, 7))
     pa = dict(part_key=orc.gen(40, n_pa, 7), flag=orc.gen(41, n_pa, 7))
     su = dict(supp_key=orc.gen(50, n_su, 7), nation=orc.gen(51, n_su, 7))
@@ -140,6 +164,10 @@ def test_cli_reads_tbl_files(orc, tmp_path):
     out = run("join", "--data", d)
     assert [int(x) for x in re.findall(r"Found (\d+) total matches", out)] == [orc.join_count(od["order_key"],
                                                                                                 li["order_key"])] * 2
+    out = run("q4", "--data", d)
+    assert q4_rows(out) == orc.q4(od, li)
+    out = run("q12", "--data", d)
+    assert q12_rows(out) == orc.q12(od, li)
     out = run("aggregation", "--data", d)
     assert int(re.search(r"SUM\(l_quantity\): (-?\d+)", out).group(1)) == orc.sum_i32(li["quantity"])
     # the same files read 64 KB at a time: rows that straddle pieces are carried over whole

@@ -12,7 +12,7 @@ from gpudbmetalbenchmark_b200 import capi
 pytestmark = pytest.mark.gpu
 
 LI_COLS = ("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag", "status",
-           "ship_date")
+           "ship_date", "commit_date", "receipt_date", "ship_mode")
 
 
 def tables(orc):
@@ -20,7 +20,7 @@ def tables(orc):
     return {
         "lineitem": orc.lineitem(20_011, seed=3, n_orders=n_or, order_mode=1, n_parts=n_pa, n_supp=n_su, cols=LI_COLS),
         "orders": dict(order_key=orc.gen(30, n_or, 3), cust_key=orc.gen(31, n_or, 3, n_cust=n_cu),
-                       order_date=orc.gen(32, n_or, 3)),
+                       order_date=orc.gen(32, n_or, 3), priority=orc.gen(33, n_or, 3)),
         "customer": dict(cust_key=orc.gen(20, n_cu, 3), segment=orc.gen(21, n_cu, 3)),
         "part": dict(part_key=orc.gen(40, n_pa, 3), flag=orc.gen(41, n_pa, 3)),
         "supplier": dict(supp_key=orc.gen(50, n_su, 3), nation=orc.gen(51, n_su, 3)),
@@ -46,9 +46,9 @@ def test_round_trip(engine, orc, kind):
 
 
 def test_hand_written_rows(engine, orc):
-    text = (b"7|11|3|1|17|1234.50|0.05|0.08|R|F|1992-01-01|x|y|z|w|c|\r\n"
-            b"9|12|4|2|3|-0.5|0.1|0.00|N|O|1996-02-29|x|y|z|w|c|\n"
-            b"2147483647|0|0|3|0|0|0|0|A|F|1998-12-01|x|y|z|w|c|")
+    text = (b"7|11|3|1|17|1234.50|0.05|0.08|R|F|1992-01-01|1991-12-01|1992-01-20|NONE|MAIL|c|\r\n"
+            b"9|12|4|2|3|-0.5|0.1|0.00|N|O|1996-02-29|1996-03-01|1996-03-31|COLLECT COD|REG AIR|c|\n"
+            b"2147483647|0|0|3|0|0|0|0|A|F|1998-12-01|1998-12-31|1999-01-01|TAKE BACK RETURN|TRUCK|c|")
     t = engine.load_tbl("lineitem", text)
     try:
         want = orc.parse_tbl_cpu("lineitem", text)
@@ -56,6 +56,8 @@ def test_hand_written_rows(engine, orc):
         for name in LI_COLS:
             assert t.to_numpy(name).tolist() == want[name], name
         assert t.to_numpy("ship_date").tolist() == [0, 1520, 2526]
+        assert t.to_numpy("commit_date").tolist() == [-31, 1521, 2556]
+        assert t.to_numpy("ship_mode").tolist() == [2, 4, 6]
         assert t.key_max["order_key"] == 2147483647
     finally:
         engine.free(t)
@@ -68,6 +70,8 @@ def test_hand_written_rows(engine, orc):
     b"7|1|3|1|17|1.00|0.05|0.08|R|F|1992-1-01|",        # date not YYYY-MM-DD
     b"7|1|3|1|17|1.00|0.05",                            # too few fields
     b"7|1|3|1|17|1.00|0.05|0.08|R|F|1992-01-01|\n\n",   # an empty line
+    b"7|1|3|1|17|1.00|0.05|0.08|R|F|1992-01-01|1992-01-02|1992-01-03|NONE|BOAT|c|",   # unknown ship mode
+    b"7|1|3|1|17|1.00|0.05|0.08|R|F|1992-01-01|1992-13-02|1992-01-03|NONE|AIR|c|",    # month 13
 ])
 def test_malformed_text_is_rejected(engine, bad):
     with pytest.raises(capi.GpudbError) as e:

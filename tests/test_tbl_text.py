@@ -9,15 +9,24 @@ import oracle_py as orc
 def test_format_parse_round_trip_cpu():
     li = orc.lineitem(2000, seed=5, n_orders=500, order_mode=1, n_parts=300, n_supp=40,
                       cols=("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag",
-                            "status", "ship_date"))
+                            "status", "ship_date", "commit_date", "receipt_date", "ship_mode"))
     got = orc.parse_tbl_cpu("lineitem", orc.format_tbl("lineitem", li))
     for k, v in li.items():
         assert np.array_equal(np.asarray(got[k]), v), k
 
 
 def test_hand_written_rows_cpu():
-    text = (b"7|11|3|1|17|1234.50|0.05|0.08|R|F|1992-01-01|x|y|z|w|c|\r\n"
-            b"9|12|4|2|3|-0.5|0.1|0.00|N|O|1996-02-29|x|y|z|w|c|")
+    text = (b"7|11|3|1|17|1234.50|0.05|0.08|R|F|1992-01-01|1991-12-01|1992-01-20|NONE|MAIL|c|\r\n"
+            b"9|12|4|2|3|-0.5|0.1|0.00|N|O|1996-02-29|1996-03-01|1996-03-31|COLLECT COD|REG AIR|c|")
     got = orc.parse_tbl_cpu("lineitem", text)
     assert got["ext_price"] == [123450, -50] and got["discount"] == [5, 10] and got["tax"] == [8, 0]
     assert got["ship_date"] == [0, 1520] and got["flag"] == [2, 1] and got["status"] == [0, 1]
+    assert got["commit_date"] == [-31, 1521] and got["receipt_date"] == [19, 1551] and got["ship_mode"] == [2, 4]
+
+
+def test_orders_priority_round_trip_cpu():
+    od = dict(order_key=orc.gen(30, 500, 4), cust_key=orc.gen(31, 500, 4, n_cust=50), order_date=orc.gen(32, 500, 4),
+              priority=orc.gen(33, 500, 4))
+    got = orc.parse_tbl_cpu("orders", orc.format_tbl("orders", od))
+    for k, v in od.items():
+        assert np.array_equal(np.asarray(got[k]), v), k
