@@ -32,7 +32,7 @@ TBL_MAX_COLS = 13
 TBL_COLUMNS = {
     "lineitem": (TBL_LINEITEM, ("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax",
                                 "flag", "status", "ship_date", "commit_date", "receipt_date", "ship_mode")),
-    "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date", "priority")),
+    "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date", "priority", "comment")),
     "customer": (TBL_CUSTOMER, ("cust_key", "segment")),
     "part": (TBL_PART, ("part_key", "flag")),
     "supplier": (TBL_SUPPLIER, ("supp_key", "nation")),
@@ -47,13 +47,15 @@ Q3_MAX_K = 64
 MODE_AIR, MODE_FOB, MODE_MAIL, MODE_RAIL, MODE_REG_AIR, MODE_SHIP, MODE_TRUCK = range(7)
 SHIP_MODES = ("AIR", "FOB", "MAIL", "RAIL", "REG AIR", "SHIP", "TRUCK")
 PRIORITIES = ("1-URGENT", "2-HIGH", "3-MEDIUM", "4-NOT SPECIFIED", "5-LOW")
+COMMENT_WIDTH = 80      # o_comment bytes per row, NUL-padded
+Q13_MAX_COUNT = 1023
 
 # column ids
 COL = dict(
     LI_SHIP_DATE=1, LI_QUANTITY=2, LI_EXT_PRICE=3, LI_DISCOUNT=4, LI_TAX=5, LI_FLAG=6, LI_STATUS=7,
     LI_ORDER_KEY=8, LI_PART_KEY=9, LI_SUPP_KEY=10, LI_COMMIT_DATE=11, LI_RECEIPT_DATE=12, LI_SHIP_MODE=13,
     CU_CUST_KEY=20, CU_SEGMENT=21,
-    OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32, OR_PRIORITY=33,
+    OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32, OR_PRIORITY=33, OR_COMMENT=34,
     PA_PART_KEY=40, PA_FLAG=41,
     SU_SUPP_KEY=50, SU_NATION=51,
     PS_PART_KEY=60, PS_SUPP_KEY=61, PS_SUPPLY_COST=62,
@@ -92,7 +94,7 @@ class Customer(C.Structure):
 
 class Orders(C.Structure):
     _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("cust_key_max", C.c_int32),
-                ("order_key", vp), ("cust_key", vp), ("order_date", vp), ("priority", vp)]
+                ("order_key", vp), ("cust_key", vp), ("order_date", vp), ("priority", vp), ("comment", vp)]
 
 
 class Part(C.Structure):
@@ -130,6 +132,14 @@ class Q12Params(C.Structure):
 
 class Q12Result(C.Structure):
     _fields_ = [("high", C.c_uint64 * 2), ("low", C.c_uint64 * 2)]
+
+
+class Q13Params(C.Structure):
+    _fields_ = [("word1", C.c_char * 16), ("word2", C.c_char * 16)]
+
+
+class Q13Row(C.Structure):
+    _fields_ = [("c_count", C.c_uint32), ("custdist", C.c_uint32)]
 
 
 class Q6Params(C.Structure):
@@ -237,6 +247,8 @@ PROTOTYPES = {
     "gpudb_q4_priority": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q4Params), P(Q4Result), P(Timing), P(Exec)]),
     "gpudb_q12_shipmode": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q12Params), P(Q12Result), P(Timing),
                                      P(Exec)]),
+    "gpudb_q13_distribution": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Q13Params), P(Q13Row), C.c_uint32,
+                                         P(C.c_uint32), P(Timing), P(Exec)]),
     "gpudb_q3_join_topk": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q3Params), P(Q3Result),
                                      P(Timing), P(Exec)]),
     "gpudb_q9_star": (C.c_int, [ctx_p, P(Part), P(Supplier), P(Partsupp), P(Orders), P(Lineitem), P(Q9Params),

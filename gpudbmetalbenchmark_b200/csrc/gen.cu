@@ -44,6 +44,7 @@ __host__ __device__ __forceinline__ void gen_value(const GenArgs& a, uint64_t r,
     case GPUDB_COL_OR_CUST_KEY: i32[i] = gd_or_cust(a.seed, r, a.n_cust); break;
     case GPUDB_COL_OR_ORDER_DATE: i32[i] = gd_or_date(a.seed, r); break;
     case GPUDB_COL_OR_PRIORITY: u8[i] = gd_or_priority(a.seed, r); break;
+    case GPUDB_COL_OR_COMMENT: gd_or_comment(a.seed, r, reinterpret_cast<char*>(u8) + i * GD_COMMENT_WIDTH); break;
     case GPUDB_COL_PA_PART_KEY: i32[i] = (int32_t)r; break;
     case GPUDB_COL_PA_FLAG: u8[i] = gd_pa_flag(a.seed, r); break;
     case GPUDB_COL_SU_SUPP_KEY: i32[i] = (int32_t)r; break;
@@ -88,6 +89,7 @@ int column_width(int32_t c) {
     case GPUDB_COL_PA_FLAG: case GPUDB_COL_SU_NATION: case GPUDB_COL_LI_SHIP_MODE: case GPUDB_COL_OR_PRIORITY:
       return 1;
     case GPUDB_COL_LI_COMMIT_DATE: case GPUDB_COL_LI_RECEIPT_DATE: return 4;
+    case GPUDB_COL_OR_COMMENT: return GD_COMMENT_WIDTH;
     case GPUDB_COL_LI_SHIP_DATE: case GPUDB_COL_LI_QUANTITY: case GPUDB_COL_LI_DISCOUNT:
     case GPUDB_COL_LI_TAX: case GPUDB_COL_LI_ORDER_KEY: case GPUDB_COL_LI_PART_KEY:
     case GPUDB_COL_LI_SUPP_KEY: case GPUDB_COL_CU_CUST_KEY: case GPUDB_COL_OR_ORDER_KEY:

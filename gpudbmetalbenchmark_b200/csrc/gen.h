@@ -39,7 +39,7 @@ enum gd_column {
   GD_LI_FLAG, GD_LI_STATUS, GD_LI_ORDER_PICK, GD_LI_PART, GD_LI_SUPP_SLOT, GD_LI_ORDER_RUN,
   GD_LI_COMMIT, GD_LI_RECEIPT, GD_LI_MODE,
   GD_CU_SEGMENT = 32,
-  GD_OR_CUST = 48, GD_OR_DATE, GD_OR_PRIORITY,
+  GD_OR_CUST = 48, GD_OR_DATE, GD_OR_PRIORITY, GD_OR_COMMENT,
   GD_PA_FLAG = 64,
   GD_SU_NATION = 80,
   GD_PS_COST = 96
@@ -117,6 +117,28 @@ GD_HD int32_t gd_li_receipt_date(uint64_t seed, uint64_t r) {
 }
 GD_HD uint8_t gd_li_ship_mode(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_LI_MODE, r, 0, 6); }
 GD_HD uint8_t gd_or_priority(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_OR_PRIORITY, r, 1, 5); }
+// Order comments: 2..9 words drawn from a 24-word vocabulary (draw 0 of row r's sub-stream
+// r*16 is the word count, draws 1.. the words), separated by one space; a word that would
+// pass 79 characters ends the comment; the rest of the 80 bytes is 0.
+#define GD_COMMENT_WIDTH 80
+#define GD_VOCAB "specialrequestspackagesdepositsaccountsinstructionsfoxesideastheodolitespintobeans" \
+                 "plateletsfuriouslycarefullyquicklyslylyblithelyregularfinalpendingironicexpressboldeven"
+GD_HD void gd_or_comment(uint64_t seed, uint64_t r, char* out) {
+  const uint8_t len[24] = {7, 8, 8, 8, 8, 12, 5, 5, 11, 5, 5, 9, 9, 9, 7, 5, 8, 7, 5, 7, 6, 7, 4, 4};
+  const uint8_t off[24] = {0, 7, 15, 23, 31, 39, 51, 56, 61, 72, 77, 82, 91, 100, 109, 116, 121, 129, 136, 141, 148,
+                           154, 161, 165};
+  const char* vocab = GD_VOCAB;
+  const uint64_t key = gd_stream_key(seed, GD_OR_COMMENT);
+  const int words = (int)gd_uniform_k(key, r * 16, 2, 9);
+  int n = 0;
+  for (int i = 0; i < words; i++) {
+    const int w = (int)gd_uniform_k(key, r * 16 + 1 + i, 0, 23);
+    if (n + (n ? 1 : 0) + len[w] > GD_COMMENT_WIDTH - 1) break;
+    if (n) out[n++] = ' ';
+    for (int c = 0; c < len[w]; c++) out[n++] = vocab[off[w] + c];
+  }
+  for (; n < GD_COMMENT_WIDTH; n++) out[n] = 0;
+}
 GD_HD uint8_t gd_cu_segment(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_CU_SEGMENT, r, 0, 4); }
 GD_HD int32_t gd_or_cust(uint64_t seed, uint64_t r, int64_t n_cust) { return (int32_t)gd_uniform(seed, GD_OR_CUST, r, 0, n_cust - 1); }
 GD_HD int32_t gd_or_date(uint64_t seed, uint64_t r) { return (int32_t)gd_uniform(seed, GD_OR_DATE, r, 0, GD_ORDER_DATE_MAX); }

@@ -299,6 +299,56 @@ void runQ12Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
+void runQ13Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 13 Benchmark ---\n");
+  const double t0 = now_ms();
+  gpudb_customer cu{};
+  gpudb_orders orr{};
+  TblTable ct, ot;
+  Buffer ck, oc, om;
+  if (!o.data_dir.empty()) {
+    ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0}, {4}, o.tbl_piece);
+    ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {1, 4}, {4, GPUDB_COMMENT_WIDTH}, o.tbl_piece);
+    cu = {ct.rows, ct.col_max[0], 0, ct.col<int32_t>(0), nullptr};
+    orr.n_rows = ot.rows;
+    orr.cust_key = ot.col<int32_t>(1);
+    orr.comment = ot.col<char>(4);
+  } else {
+    gpudb_gen_spec cs{};
+    cs.seed = o.seed;
+    cs.n_rows = o.scale.customer;
+    ck = generate(ctx, cs, GPUDB_COL_CU_CUST_KEY, GPUDB_MEM_DEVICE);
+    gpudb_gen_spec os = cs;
+    os.n_rows = o.scale.orders;
+    os.n_cust = (int64_t)o.scale.customer;
+    oc = generate(ctx, os, GPUDB_COL_OR_CUST_KEY, GPUDB_MEM_DEVICE);
+    om = generate(ctx, os, GPUDB_COL_OR_COMMENT, GPUDB_MEM_DEVICE);
+    cu = {o.scale.customer, (int32_t)o.scale.customer - 1, 0, ck.as<int32_t>(), nullptr};
+    orr.n_rows = o.scale.orders;
+    orr.cust_key = oc.as<int32_t>();
+    orr.comment = om.as<char>();
+  }
+  const double gen_ms = now_ms() - t0;
+  gpudb_q13_params p{};
+  std::strcpy(p.word1, "special");
+  std::strcpy(p.word2, "requests");
+  std::vector<gpudb_q13_row> rows(GPUDB_Q13_MAX_COUNT + 1);
+  uint32_t n = 0;
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++)
+    check(ctx, gpudb_q13_distribution(ctx, &cu, &orr, &p, rows.data(), (uint32_t)rows.size(), &n, &t, nullptr),
+          "gpudb_q13");
+  const double p0 = now_ms();
+  std::printf("\nTPC-H Query 13 Results (Comparable histogram):\n");
+  std::printf("+---------+----------+\n");
+  std::printf("| c_count | custdist |\n");
+  std::printf("+---------+----------+\n");
+  for (uint32_t i = 0; i < n && i < rows.size(); i++) std::printf("| %7u | %8u |\n", rows[i].c_count, rows[i].custdist);
+  std::printf("+---------+----------+\n");
+  std::printf("\nQ13 | %" PRIu64 " orders | %" PRIu64 " customers\n", orr.n_rows, cu.n_rows);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
+}
+
 void runQ9Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("\n--- Running TPC-H Query 9 Benchmark ---\n");
   const Scale& s = o.scale;

@@ -204,6 +204,7 @@ void runQ1Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ3Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ4Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ12Benchmark(gpudb_ctx*, const RunOptions&);
+void runQ13Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ6Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ9Benchmark(gpudb_ctx*, const RunOptions&);
 void runSelectionBenchmark(gpudb_ctx*, const RunOptions&);

@@ -30,7 +30,8 @@ constexpr int kTT = 256;                              // threads per tile
 constexpr uint64_t kTileBytes = (uint64_t)kTT * 64;   // 64 bytes per thread
 
 enum FieldType : int32_t {
-  F_I32, F_DEC64, F_DEC32, F_QTY, F_DATE, F_RETFLAG, F_LINESTATUS, F_SEGMENT, F_GREEN, F_U8, F_SHIPMODE, F_PRIORITY
+  F_I32, F_DEC64, F_DEC32, F_QTY, F_DATE, F_RETFLAG, F_LINESTATUS, F_SEGMENT, F_GREEN, F_U8, F_SHIPMODE, F_PRIORITY,
+  F_COMMENT
 };
 
 struct TblSpec {
@@ -45,7 +46,7 @@ bool spec_for(int32_t table, TblSpec* s) {
       {GPUDB_TBL_LINEITEM, 13, {0, 1, 2, 4, 5, 6, 7, 8, 9, 10, 11, 12, 14},
        {F_I32, F_I32, F_I32, F_QTY, F_DEC64, F_DEC32, F_DEC32, F_RETFLAG, F_LINESTATUS, F_DATE, F_DATE, F_DATE,
         F_SHIPMODE}},
-      {GPUDB_TBL_ORDERS, 4, {0, 1, 4, 5}, {F_I32, F_I32, F_DATE, F_PRIORITY}},
+      {GPUDB_TBL_ORDERS, 5, {0, 1, 4, 5, 8}, {F_I32, F_I32, F_DATE, F_PRIORITY, F_COMMENT}},
       {GPUDB_TBL_CUSTOMER, 2, {0, 6}, {F_I32, F_SEGMENT}},
       {GPUDB_TBL_PART, 2, {0, 1}, {F_I32, F_GREEN}},
       {GPUDB_TBL_SUPPLIER, 2, {0, 3}, {F_I32, F_U8}},
@@ -234,6 +235,16 @@ __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ 
             ok = fe - s >= 2 && *s >= '1' && *s <= '5' && s[1] == '-';
             v = ok ? *s - '0' : 0;
             break;
+          case F_COMMENT: {   // at most 79 bytes, copied into a NUL-padded slot
+            ok = fe - s < GPUDB_COMMENT_WIDTH;
+            if (ok && spec.col[k]) {
+              char* d = static_cast<char*>(spec.col[k]) + r * GPUDB_COMMENT_WIDTH;
+              int i = 0;
+              for (const uint8_t* p = s; p < fe; p++) d[i++] = (char)*p;
+              for (; i < GPUDB_COMMENT_WIDTH; i++) d[i] = 0;
+            }
+            break;
+          }
           case F_GREEN: {
             v = 0;
             for (const uint8_t* p = s; p + 5 <= fe && !v; p++)
@@ -242,7 +253,7 @@ __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ 
           }
         }
         if (!ok) bad |= ST_DOMAIN;
-        void* col = spec.col[k];
+        void* col = spec.type[k] == F_COMMENT ? nullptr : spec.col[k];   // comments are written above
         if (col) {
           switch (spec.type[k]) {
             case F_DEC64: static_cast<int64_t*>(col)[r] = v; break;

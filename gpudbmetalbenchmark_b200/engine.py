@@ -15,7 +15,7 @@ import numpy as np
 from . import capi
 from .capi import COL, MEM_DEVICE, MEM_HOST
 
-DTYPES = {1: np.uint8, 4: np.int32, 8: np.int64}
+DTYPES = {1: np.uint8, 4: np.int32, 8: np.int64, capi.COMMENT_WIDTH: np.dtype("S%d" % capi.COMMENT_WIDTH)}
 
 LINEITEM_COLS = {  # field of capi.Lineitem -> column id
     "ship_date": COL["LI_SHIP_DATE"], "quantity": COL["LI_QUANTITY"], "ext_price": COL["LI_EXT_PRICE"],
@@ -30,7 +30,7 @@ Q6_COLS = ("ship_date", "discount", "quantity", "ext_price")
 TABLE_COLS = {
     "customer": {"cust_key": COL["CU_CUST_KEY"], "segment": COL["CU_SEGMENT"]},
     "orders": {"order_key": COL["OR_ORDER_KEY"], "cust_key": COL["OR_CUST_KEY"], "order_date": COL["OR_ORDER_DATE"],
-               "priority": COL["OR_PRIORITY"]},
+               "priority": COL["OR_PRIORITY"], "comment": COL["OR_COMMENT"]},
     "part": {"part_key": COL["PA_PART_KEY"], "flag": COL["PA_FLAG"]},
     "supplier": {"supp_key": COL["SU_SUPP_KEY"], "nation": COL["SU_NATION"]},
     "partsupp": {"part_key": COL["PS_PART_KEY"], "supp_key": COL["PS_SUPP_KEY"], "supply_cost": COL["PS_SUPPLY_COST"]},
@@ -221,7 +221,8 @@ class Engine:
             if kind == "lineitem" and "order_key" in arrays:
                 t.key_max["order_key"] = int(arrays["order_key"].max()) if n else -1
             elif kind == "orders":
-                t.key_max["order_key"] = int(arrays["order_key"].max()) if n else -1
+                if "order_key" in arrays:
+                    t.key_max["order_key"] = int(arrays["order_key"].max()) if n else -1
                 if "cust_key" in arrays:
                     t.key_max["cust_key"] = int(arrays["cust_key"].max()) if n else -1
             elif kind in ("customer", "part", "supplier"):
@@ -329,6 +330,17 @@ class Engine:
                                                 C.byref(timing) if timing is not None else None,
                                                 self._exec(async_, None)))
         return r if async_ else [(r.high[0], r.low[0]), (r.high[1], r.low[1])]
+
+    def q13(self, cu, od, word1=b"special", word2=b"requests", capacity=capi.Q13_MAX_COUNT + 1, timing=None):
+        """[(c_count, custdist)] ordered by custdist desc, c_count desc: customers per number of
+        their orders whose comment is NOT LIKE '%word1%word2%'."""
+        p = capi.Q13Params(word1, word2)
+        rows = (capi.Q13Row * capacity)()
+        n = C.c_uint32()
+        self._check(self.lib.gpudb_q13_distribution(self.ctx, C.byref(cu.struct()), C.byref(od.struct()), C.byref(p),
+                                                    rows, capacity, C.byref(n),
+                                                    C.byref(timing) if timing is not None else None, None))
+        return [(r.c_count, r.custdist) for r in rows[:min(n.value, capacity)]]
 
     def q9(self, pa, su, ps, od, li, smem_slots=0, global_slots=0, chunk_rows=0, capacity=4096, timing=None):
         """[(nation, year, profit)] ordered by nation asc, year desc."""

@@ -236,6 +236,14 @@ def main(argv=None):
             emit("q12_shipmode", label, n_li, ms, n_li * 17 + n_or * 5, {"kernels": t.kernels})
             eng.free(li)
             eng.free(od)
+    if on("q13"):
+        for n_cu, n_or, label in ((150_000, 1_500_000, "SF-1 sizes"), (1_500_000, 15_000_000, "SF-10 sizes")):
+            cu = eng.generate("customer", n_cu, seed=42, columns=("cust_key",))
+            od = eng.generate("orders", n_or, seed=42, columns=("cust_key", "comment"), n_cust=n_cu)
+            ms, t = timed(lambda tm: eng.q13(cu, od, timing=tm), a.reps)
+            emit("q13_distribution", label, n_or, ms, n_or * (4 + capi.COMMENT_WIDTH) + n_cu * 8, {"kernels": t.kernels})
+            eng.free(od)
+            eng.free(cu)
     if on("q9"):
         pa, su, ps, od = q9_tables(eng, 2_000_000, 100_000, 15_000_000)
         li = eng.generate("lineitem", 60_000_000, seed=42,

@@ -150,7 +150,9 @@ typedef struct gpudb_orders {
   uint64_t n_rows; int32_t key_max; int32_t cust_key_max;
   const int32_t* order_key; const int32_t* cust_key; const int32_t* order_date;
   const uint8_t* priority;     /* o_orderpriority 1..5 = '1-URGENT' .. '5-LOW' (Q4, Q12) */
+  const char* comment;         /* o_comment: GPUDB_COMMENT_WIDTH bytes per row, NUL-padded (Q13) */
 } gpudb_orders;
+#define GPUDB_COMMENT_WIDTH 80   /* at most 79 characters; the bytes after the text are 0 */
 
 typedef struct gpudb_part {
   uint64_t n_rows; int32_t key_max; int32_t reserved;
@@ -175,6 +177,7 @@ enum gpudb_column_id {
   GPUDB_COL_LI_COMMIT_DATE, GPUDB_COL_LI_RECEIPT_DATE, GPUDB_COL_LI_SHIP_MODE,
   GPUDB_COL_CU_CUST_KEY = 20, GPUDB_COL_CU_SEGMENT,
   GPUDB_COL_OR_ORDER_KEY = 30, GPUDB_COL_OR_CUST_KEY, GPUDB_COL_OR_ORDER_DATE, GPUDB_COL_OR_PRIORITY,
+  GPUDB_COL_OR_COMMENT,        /* GPUDB_COMMENT_WIDTH bytes per row */
   GPUDB_COL_PA_PART_KEY = 40, GPUDB_COL_PA_FLAG,
   GPUDB_COL_SU_SUPP_KEY = 50, GPUDB_COL_SU_NATION,
   GPUDB_COL_PS_PART_KEY = 60, GPUDB_COL_PS_SUPP_KEY, GPUDB_COL_PS_SUPPLY_COST
@@ -322,6 +325,23 @@ typedef struct gpudb_q12_result { uint64_t high[2]; uint64_t low[2]; } gpudb_q12
 int gpudb_q12_shipmode(gpudb_ctx* ctx, const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q12_params* p,
                        gpudb_q12_result* out, gpudb_timing* t, const gpudb_exec* ex);
 
+/* ---- Q13 customer distribution (replaces runQ13Benchmark src/q13.cpp:8-117 with its kernels
+ *      q13_pattern_match_kernel / q13_count_prefiltered_kernel / q13_build_histogram_kernel
+ *      kernels/q13.metal:33-168 and postProcessQ13 src/infra.h:778-800) -------------------------
+ * c_count(customer) = number of its orders whose comment is NOT LIKE '%word1%word2%' (word1
+ * followed, later in the comment, by word2; 1..15 characters each, NUL-terminated); custdist =
+ * number of customers per c_count, over every row of `cu` (customers without such orders have
+ * c_count 0: the LEFT OUTER JOIN). Rows are ordered by custdist desc, c_count desc; *n_rows is
+ * the number of distinct c_count values and at most `capacity` rows are written. Orders whose
+ * customer key is outside 0..cu->key_max count for no customer; a c_count above
+ * GPUDB_Q13_MAX_COUNT fails the call with GPUDB_E_CAPACITY. */
+#define GPUDB_Q13_MAX_COUNT 1023
+typedef struct gpudb_q13_params { char word1[16]; char word2[16]; } gpudb_q13_params;
+typedef struct gpudb_q13_row { uint32_t c_count; uint32_t custdist; } gpudb_q13_row;
+int gpudb_q13_distribution(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_orders* od,
+                           const gpudb_q13_params* p, gpudb_q13_row* out, uint32_t capacity, uint32_t* n_rows,
+                           gpudb_timing* t, const gpudb_exec* ex);
+
 /* ---- microbenchmarks (replace runSelectionBenchmark / runAggregationBenchmark /
  *      runJoinBenchmark src/microbenchmarks.cpp:8-251 and their kernels
  *      kernels/microbenchmarks.metal:160-294) ------------------------------------------ */
@@ -411,7 +431,8 @@ int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timin
  *   LINEITEM: order_key, part_key, supp_key, quantity, ext_price (int64), discount, tax,
  *             flag (u8), status (u8), ship_date, commit_date, receipt_date, ship_mode (u8)
  *                                                     fields 0,1,2,4,5,6,7,8,9,10,11,12,14
- *   ORDERS:   order_key, cust_key, order_date, priority (u8)       fields 0,1,4,5
+ *   ORDERS:   order_key, cust_key, order_date, priority (u8), comment (GPUDB_COMMENT_WIDTH
+ *             bytes per row: at most 79 characters, NUL-padded)    fields 0,1,4,5,8
  *   CUSTOMER: cust_key, segment (u8)                               fields 0,6
  *   PART:     part_key, flag (u8)                                  fields 0,1
  *   SUPPLIER: supp_key, nation (u8)                                fields 0,3

@@ -37,7 +37,28 @@ static int64_t unif(uint64_t key, uint64_t row, int64_t lo, int64_t hi) {
 /* random stream ids (table*16 + column) */
 enum { S_SHIP = 16, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG, S_STATUS, S_OPICK, S_PART, S_SSLOT, S_RUN,
        S_COMMIT, S_RECEIPT, S_MODE,
-       S_SEG = 32, S_OCUST = 48, S_ODATE, S_OPRIO, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
+       S_SEG = 32, S_OCUST = 48, S_ODATE, S_OPRIO, S_OCOMMENT, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
+
+/* order comment: n = U[2,9] words (sub-draw r*16), word i = U[0,23] (sub-draw r*16+1+i) of the
+ * vocabulary below, joined by single spaces, stopping at the first word that would pass 79
+ * characters; NUL-padded to 80 bytes */
+static const char* const VOCAB[24] = {
+  "special", "requests", "packages", "deposits", "accounts", "instructions", "foxes", "ideas", "theodolites",
+  "pinto", "beans", "platelets", "furiously", "carefully", "quickly", "slyly", "blithely", "regular", "final",
+  "pending", "ironic", "express", "bold", "even"};
+static void comment_of(uint64_t key, uint64_t r, char* out) {
+  int n = 0;
+  const int words = (int)unif(key, r * 16, 2, 9);
+  for (int i = 0; i < words; i++) {
+    const char* w = VOCAB[unif(key, r * 16 + 1 + i, 0, 23)];
+    const int wl = (int)strlen(w);
+    if (n + (n ? 1 : 0) + wl > 79) break;
+    if (n) out[n++] = ' ';
+    memcpy(out + n, w, (size_t)wl);
+    n += wl;
+  }
+  memset(out + n, 0, (size_t)(80 - n));
+}
 
 static int32_t supp_of(int64_t part, int64_t j, int64_t n_supp) { return (int32_t)((part + j * (n_supp / 4)) % n_supp); }
 
@@ -86,6 +107,7 @@ int or_gen_column(const or_spec* sp, int32_t column, void* dst) {
              for (i = 0; i < n; i++) i32[i] = (int32_t)(unif(ks, off + i, 0, 2526) + unif(k, off + i, 1, 30)); return 0; }
   case 13: { uint64_t k = stream_of(seed, S_MODE); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 6); return 0; }
   case 33: { uint64_t k = stream_of(seed, S_OPRIO); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 1, 5); return 0; }
+  case 34: { uint64_t k = stream_of(seed, S_OCOMMENT); for (i = 0; i < n; i++) comment_of(k, off + i, (char*)u8 + i * 80); return 0; }
   case 20: case 30: case 40: case 50:
     for (i = 0; i < n; i++) i32[i] = (column == 30) ? (int32_t)(4 * (off + i) + 1) : (int32_t)(off + i);
     return 0;
@@ -393,6 +415,42 @@ void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t 
     out4[(h ? 0 : 2) + m]++;
   }
   free(high);
+}
+
+/* ---- Q13: kernels/q13.metal:33-68 (first w1, then w2 after it), :110-127 (counts),
+ * :133-168 (histogram), src/infra.h:783-800 (custdist desc, c_count desc) ---- */
+static int like2(const char* s, const char* w1, const char* w2) {
+  char buf[81];
+  memcpy(buf, s, 80);
+  buf[80] = 0;
+  const char* a = strstr(buf, w1);
+  return a && strstr(a + strlen(w1), w2) != NULL;
+}
+typedef struct { uint32_t c, d; } q13row;
+static int q13_cmp(const void* a, const void* b) {
+  const q13row *x = (const q13row*)a, *y = (const q13row*)b;
+  if (x->d != y->d) return x->d > y->d ? -1 : 1;
+  return x->c > y->c ? -1 : (x->c < y->c);
+}
+uint32_t or_q13(uint64_t n_cu, const int32_t* cu_key, int32_t cu_key_max, uint64_t n_or, const int32_t* o_cust,
+                const char* o_comment, const char* w1, const char* w2, uint32_t* c_count, uint32_t* custdist,
+                uint32_t cap) {
+  uint64_t i;
+  if (cu_key_max < 0 || n_cu == 0) return 0;
+  uint32_t* cnt = (uint32_t*)calloc((size_t)cu_key_max + 1, 4);
+  uint32_t top = 0;
+  for (i = 0; i < n_or; i++)
+    if (o_cust[i] >= 0 && o_cust[i] <= cu_key_max && !like2(o_comment + 80 * i, w1, w2)) cnt[o_cust[i]]++;
+  for (i = 0; i < n_cu; i++) if (cnt[cu_key[i]] > top) top = cnt[cu_key[i]];
+  uint32_t* hist = (uint32_t*)calloc((size_t)top + 1, 4);
+  for (i = 0; i < n_cu; i++) hist[cnt[cu_key[i]]]++;
+  q13row* rows = (q13row*)malloc(((size_t)top + 1) * sizeof(q13row));
+  uint32_t n = 0;
+  for (uint32_t c = 0; c <= top; c++) if (hist[c]) { rows[n].c = c; rows[n].d = hist[c]; n++; }
+  qsort(rows, n, sizeof(q13row), q13_cmp);
+  for (uint32_t r = 0; r < n && r < cap; r++) { c_count[r] = rows[r].c; custdist[r] = rows[r].d; }
+  free(cnt); free(hist); free(rows);
+  return n;
 }
 
 uint64_t or_select_lt(uint64_t n, const int32_t* col, int32_t value, uint32_t* bits, uint32_t* rows) {

@@ -82,6 +82,14 @@ void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t 
             const uint8_t* l_mode, int32_t receipt_lo, int32_t receipt_hi, int32_t mode0, int32_t mode1,
             int32_t high_max, uint64_t* out4);
 
+/* Q13: per-customer counts of orders whose 80-byte NUL-padded comment is NOT LIKE
+ * '%w1%w2%' (kernels/q13.metal:33-127), the histogram of those counts over the customer rows
+ * (kernels/q13.metal:133-168) ordered by custdist desc, c_count desc (postProcessQ13
+ * src/infra.h:783-800). Writes up to cap rows, returns the number of distinct counts. */
+uint32_t or_q13(uint64_t n_cu, const int32_t* cu_key, int32_t cu_key_max, uint64_t n_or, const int32_t* o_cust,
+                const char* o_comment, const char* w1, const char* w2, uint32_t* c_count, uint32_t* custdist,
+                uint32_t cap);
+
 uint64_t or_select_lt(uint64_t n, const int32_t* col, int32_t value, uint32_t* bits, uint32_t* rows);
 int64_t or_sum_i32(uint64_t n, const int32_t* col);
 uint64_t or_join_count(uint64_t nb, const int32_t* bkeys, uint64_t np, const int32_t* pkeys);

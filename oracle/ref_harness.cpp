@@ -1,5 +1,5 @@
 // ref_harness.cpp -- runs the reference's own Metal kernels (kernels/q1.metal, q3.metal,
-// q4.metal, q6.metal, q9.metal, q12.metal, microbenchmarks.metal, compiled in place from the reference tree
+// q4.metal, q6.metal, q9.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
 // through the CPU shim in oracle/refshim) on the synthetic tables. TEST INFRASTRUCTURE
 // ONLY: it pins the oracle's query logic to the reference's code, and it is the timed
 // reference arm of bench.py. It is never linked into the engine.
@@ -18,6 +18,7 @@ using namespace metal;
 #include "microbenchmarks.metal"
 #include "q1.metal"
 #include "q12.metal"
+#include "q13.metal"
 #include "q3.metal"
 #include "q4.metal"
 #include "q6.metal"
@@ -240,6 +241,31 @@ void ref_q12(uint64_t n_or, const int32_t* or_key, const uint8_t* or_prio, uint6
   });
   uint ng = (uint)groups;
   q12_final_count_stage2(partial.data(), out4, ng, 0);
+}
+
+// Q13 through q13_pattern_match_kernel, q13_count_prefiltered_kernel and
+// q13_build_histogram_kernel (kernels/q13.metal:33-168), with the reference's 80-byte comment
+// stride and 256 bins. Its customer keys are 1-based (counts[ck - 1]): the synthetic keys
+// 0..n_cu-1 go in as 1..n_cu. hist256[c] = customers with c qualifying orders.
+void ref_q13(uint64_t n_cu, uint64_t n_or, const int32_t* or_cust, const char* or_comment, int groups, int threads,
+             uint32_t* hist256) {
+  uint nor = (uint)n_or, ncu = (uint)n_cu, stride = 80, bins = 256;
+  std::vector<uchar> q(n_or);
+  for (uint i = 0; i < nor; i++) q13_pattern_match_kernel(or_comment, q.data(), nor, stride, i);
+  std::vector<int> ck(n_or);
+  for (uint64_t i = 0; i < n_or; i++) ck[i] = or_cust[i] + 1;
+  std::vector<atomic_uint> counts(n_cu);
+  for (auto& c : counts) c.v = 0;
+  run_groups((uint)groups, threads, [&](uint g) {
+    q13_count_prefiltered_kernel(ck.data(), q.data(), counts.data(), nor, ncu, g, 0, 1, (uint)groups);
+  });
+  std::vector<atomic_uint> hist(bins);
+  for (auto& h : hist) h.v = 0;
+  const uint* cc = reinterpret_cast<const uint*>(counts.data());
+  run_groups((uint)groups, threads, [&](uint g) {
+    q13_build_histogram_kernel(cc, hist.data(), ncu, bins, g, 0, 1, (uint)groups);
+  });
+  for (uint b = 0; b < bins; b++) hist256[b] = hist[b].v;
 }
 
 // Q9 through q9_build_part_ht_kernel, q9_build_supplier_ht_kernel,

@@ -63,6 +63,21 @@ def column(name, n, seed, off=0, n_orders=0, n_cust=0, n_parts=0, n_supp=0, mode
         return [uniform(k(29), r, 0, 6) for r in rows]
     if name == "o_priority":
         return [uniform(k(50), r, 1, 5) for r in rows]
+    if name == "o_comment":
+        vocab = ("special requests packages deposits accounts instructions foxes ideas theodolites pinto beans "
+                 "platelets furiously carefully quickly slyly blithely regular final pending ironic express bold "
+                 "even").split()
+        out = []
+        for r in rows:
+            words, text = uniform(k(51), r * 16, 2, 9), ""
+            for i in range(words):
+                w = vocab[uniform(k(51), r * 16 + 1 + i, 0, 23)]
+                nxt = (text + " " + w) if text else w
+                if len(nxt) > 79:
+                    break
+                text = nxt
+            out.append(text)
+        return out
     if name == "segment":
         return [uniform(k(32), r, 0, 4) for r in rows]
     if name == "o_cust":
@@ -168,8 +183,22 @@ def q12(n_or, n_li, seed, receipt_lo=731, receipt_hi=1096, modes=(2, 5), high_ma
     return out
 
 
+def q13(n_cu, n_or, seed, w1="special", w2="requests"):
+    cust = column("o_cust", n_or, seed, n_cust=n_cu)
+    comment = column("o_comment", n_or, seed)
+    cnt = [0] * n_cu
+    for c, t in zip(cust, comment):
+        a = t.find(w1)
+        if a < 0 or t.find(w2, a + len(w1)) < 0:
+            cnt[c] += 1
+    hist = {}
+    for v in cnt:
+        hist[v] = hist.get(v, 0) + 1
+    return sorted(([c, d] for c, d in hist.items()), key=lambda x: (-x[1], -x[0]))
+
+
 def main():
-    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}}
+    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}}
     # generator: first values and column sums for two seeds and a shifted window
     for seed, off in ((42, 0), (7, 1000)):
         cols = {}
@@ -186,6 +215,7 @@ def main():
         for name in ("commit_date", "receipt_date", "ship_mode", "o_priority"):
             v = column(name, 64, seed, off)
             cols[name] = {"head": v[:8], "sum": sum(v)}
+        cols["o_comment"] = {"head": column("o_comment", 4, seed, off)}
         out["generator"]["%d_%d" % (seed, off)] = cols
     for n, seed in ((3000, 42), (2500, 9)):
         li = {c: column(c, n, seed) for c in ("ship_date", "quantity", "ext_price", "discount", "tax", "flag",
@@ -201,6 +231,8 @@ def main():
     out["q4"]["2000_9000_5_wide"] = q4(2000, 9000, 5, 0, 2406)
     out["q12"]["3000_12000_42"] = q12(3000, 12000, 42)
     out["q12"]["2000_9000_5_air_truck_hi3"] = q12(2000, 9000, 5, 0, 2600, (0, 6), 3)
+    out["q13"]["300_3000_42"] = q13(300, 3000, 42)
+    out["q13"]["200_4000_9_pinto_beans"] = q13(200, 4000, 9, "pinto", "beans")
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

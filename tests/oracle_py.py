@@ -10,8 +10,8 @@ ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgpudbref.so")
 
 WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 11: 4, 12: 4, 13: 1, 20: 4, 21: 1, 30: 4,
-         31: 4, 32: 4, 33: 1, 40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
-DT = {1: np.uint8, 4: np.int32, 8: np.int64}
+         31: 4, 32: 4, 33: 1, 34: 80, 40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
+DT = {1: np.uint8, 4: np.int32, 8: np.int64, 80: np.dtype("S80")}
 
 
 class Spec(C.Structure):
@@ -35,6 +35,7 @@ ORACLE_ARGS = {
     "or_q9": [U64, V, V, I32, U64, V, V, I32, U64, V, V, V, U64, V, V, I32, U64, V, V, V, V, V, V, U32, V, V, V],
     "or_q4": [U64, V, V, V, I32, U64, V, V, V, I32, I32, V],
     "or_q12": [U64, V, V, I32, U64, V, V, V, V, V, I32, I32, I32, I32, I32, V],
+    "or_q13": [U64, V, I32, U64, V, V, C.c_char_p, C.c_char_p, V, V, U32],
     "or_select_lt": [U64, V, I32, V, V],
     "or_sum_i32": [U64, V],
     "or_join_count": [U64, V, U64, V],
@@ -50,6 +51,7 @@ REF_ARGS = {
     "ref_q9": [U64, V, V, U64, V, V, U64, V, V, V, U64, V, V, U64, V, V, V, V, V, V, C.c_int, C.c_int, V, V, V, U32],
     "ref_q4": [U64, V, V, V, U64, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_q12": [U64, V, V, U64, V, V, V, V, V, I32, I32, C.c_int, C.c_int, V],
+    "ref_q13": [U64, U64, V, V, C.c_int, C.c_int, V],
     "ref_select_lt": [U64, V, I32, V],
     "ref_sum": [U64, V, C.c_int, C.c_int],
     "ref_join_count": [U64, V, U64, V],
@@ -81,6 +83,7 @@ def oracle():
         _or.or_q3.restype = C.c_uint64
         _or.or_q9.restype = C.c_uint32
         _or.or_select_lt.restype = C.c_uint64
+        _or.or_q13.restype = C.c_uint32
         _or.or_sum_i32.restype = C.c_int64
         _or.or_join_count.restype = C.c_uint64
         _or.or_join_pairs.restype = C.c_uint64
@@ -133,6 +136,12 @@ def q4_tables(n_or, n_li, seed=42, order_mode=1):
     li = lineitem(n_li, seed, n_orders=n_or, order_mode=order_mode,
                   cols=("order_key", "ship_date", "commit_date", "receipt_date", "ship_mode"))
     return od, li
+
+
+def q13_tables(n_cu, n_or, seed=42):
+    cu = dict(cust_key=gen(20, n_cu, seed))
+    od = dict(cust_key=gen(31, n_or, seed, n_cust=n_cu), comment=gen(34, n_or, seed))
+    return cu, od
 
 
 def q9_tables(n_pa, n_su, n_or, n_li, seed=42):
@@ -232,6 +241,18 @@ def q12(od, li, receipt_lo=731, receipt_hi=1096, modes=(2, 5), high_max=2, or_ke
     return [(int(out[0]), int(out[2])), (int(out[1]), int(out[3]))]
 
 
+def q13(cu, od, word1=b"special", word2=b"requests", cu_key_max=None):
+    """[(c_count, custdist)] ordered by custdist desc, c_count desc."""
+    n_cu = len(cu["cust_key"])
+    kmax = (int(cu["cust_key"].max()) if n_cu else -1) if cu_key_max is None else cu_key_max
+    cap = 1 << 16
+    cc, cd = np.zeros(cap, np.uint32), np.zeros(cap, np.uint32)
+    comment = np.ascontiguousarray(od["comment"], dtype="S80")
+    n = oracle().or_q13(n_cu, _p(cu["cust_key"]), kmax, len(od["cust_key"]), _p(od["cust_key"]), _p(comment),
+                        word1, word2, cc.ctypes.data, cd.ctypes.data, cap)
+    return [(int(cc[i]), int(cd[i])) for i in range(min(n, cap))]
+
+
 def select_lt(col, value):
     n = len(col)
     bits = np.zeros((n + 31) // 32, np.uint32)
@@ -301,9 +322,10 @@ def format_tbl(kind, c):
     elif kind == "orders":
         for i in range(len(c["order_key"])):
             prio = _PRIORITIES[c["priority"][i] - 1] if "priority" in c else "3-MEDIUM"
-            out.append("%d|%d|O|%s|%s|%s|Clerk#%09d|0|an order|" % (c["order_key"][i], c["cust_key"][i],
-                                                                        _money(12345 + i), _date(c["order_date"][i]),
-                                                                        prio, i))
+            note = c["comment"][i].decode() if "comment" in c else "an order"
+            out.append("%d|%d|O|%s|%s|%s|Clerk#%09d|0|%s|" % (c["order_key"][i], c["cust_key"][i],
+                                                                  _money(12345 + i), _date(c["order_date"][i]),
+                                                                  prio, i, note))
     elif kind == "customer":
         for i in range(len(c["cust_key"])):
             out.append("%d|Customer#%09d|addr %d|%d|10-123-456-7890|%s|%s|a customer|"
@@ -333,7 +355,8 @@ def parse_tbl_cpu(kind, text):
                          (5, "ext_price", "m"), (6, "discount", "m"), (7, "tax", "m"), (8, "flag", "r"),
                          (9, "status", "s"), (10, "ship_date", "d"), (11, "commit_date", "d"),
                          (12, "receipt_date", "d"), (14, "ship_mode", "e")],
-            "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d"), (5, "priority", "p")],
+            "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d"), (5, "priority", "p"),
+                       (8, "comment", "c")],
             "customer": [(0, "cust_key", "i"), (6, "segment", "g")],
             "part": [(0, "part_key", "i"), (1, "flag", "n")],
             "supplier": [(0, "supp_key", "i"), (3, "nation", "i")],
@@ -347,6 +370,7 @@ def parse_tbl_cpu(kind, text):
 
     conv = {"i": int, "q": lambda s: money(s) // 100, "m": money, "r": _FLAGS.index, "s": _STATUS.index,
             "d": lambda s: (_dt.date.fromisoformat(s) - _EPOCH).days, "g": _SEGMENTS.index,
-            "n": lambda s: int("green" in s), "e": _MODES.index, "p": lambda s: _PRIORITIES.index(s) + 1}
+            "n": lambda s: int("green" in s), "e": _MODES.index, "p": lambda s: _PRIORITIES.index(s) + 1,
+            "c": lambda s: s.encode()}
     rows = [l.rstrip("\r").split("|") for l in text.decode().split("\n") if l != ""]
     return {name: [conv[t](r[f]) for r in rows] for f, name, t in keep}

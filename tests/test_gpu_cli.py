@@ -97,6 +97,17 @@ def test_cli_q4_and_q12(orc):
     assert q12_rows(out) == orc.q12(od, li)
 
 
+def q13_rows(out):
+    return [(int(a), int(b)) for a, b in re.findall(r"^\|\s+(\d+) \|\s+(\d+) \|$", out, re.M)]
+
+
+def test_cli_q13(orc):
+    cu, od = orc.q13_tables(1_500, 15_000, 42)
+    out = run("sf1", "q13", "--scale", "0.01")
+    assert q13_rows(out) == orc.q13(cu, od)
+    assert re.search(r"^Q13 \| 15000 orders \| 1500 customers", out, re.M)
+
+
 def test_cli_microbenchmarks(orc):
     out = run("sf1", "selection", "--scale", "0.01")
     col = orc.gen(1, 60000, 42)
@@ -132,7 +143,7 @@ def test_cli_reads_tbl_files(orc, tmp_path):
                       cols=("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax", "flag",
                             "status", "ship_date", "commit_date", "receipt_date", "ship_mode"))
     od = dict(order_key=orc.gen(30, n_or, 7), cust_key=orc.gen(31, n_or, 7, n_cust=n_cu), order_date=orc.gen(32, n_or, 7),
-              priority=orc.gen(33, n_or, 7))
+              priority=orc.gen(33, n_or, 7), comment=orc.gen(34, n_or, 7))
     cu = dict(cust_key=orc.gen(20, n_cu, 7), segment=orc.gen(21, n_cu, 7))
     pa = dict(part_key=orc.gen(40, n_pa, 7), flag=orc.gen(41, n_pa, 7))
     su = dict(supp_key=orc.gen(50, n_su, 7), nation=orc.gen(51, n_su, 7))
@@ -168,6 +179,8 @@ def test_cli_reads_tbl_files(orc, tmp_path):
     assert q4_rows(out) == orc.q4(od, li)
     out = run("q12", "--data", d)
     assert q12_rows(out) == orc.q12(od, li)
+    out = run("q13", "--data", d)
+    assert q13_rows(out) == orc.q13(cu, od)
     out = run("aggregation", "--data", d)
     assert int(re.search(r"SUM\(l_quantity\): (-?\d+)", out).group(1)) == orc.sum_i32(li["quantity"])
     # the same files read 64 KB at a time: rows that straddle pieces are carried over whole

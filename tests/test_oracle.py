@@ -35,6 +35,7 @@ def test_generator_matches_golden(orc):
         assert int(ou.sum()) == cols["order_key_uniform"]["sum"]
         sk = orc.gen(10, 64, seed, off, n_parts=1000, n_supp=100)
         assert sk[:8].tolist() == cols["supp_key"]["head"]
+        assert [x.decode() for x in orc.gen(34, 4, seed, off)] == cols["o_comment"]["head"], key
         for name, cid in (("commit_date", 11), ("receipt_date", 12), ("ship_mode", 13), ("o_priority", 33)):
             v = orc.gen(cid, 64, seed, off)
             assert v[:8].tolist() == cols[name]["head"], (key, name)
@@ -83,6 +84,13 @@ def test_q4_q12_match_golden(orc):
     od, li = orc.q4_tables(2000, 9000, 5)
     assert orc.q4(od, li, 0, 2406) == GOLDEN["q4"]["2000_9000_5_wide"]
     assert orc.q12(od, li, 0, 2600, (0, 6), 3) == [tuple(x) for x in GOLDEN["q12"]["2000_9000_5_air_truck_hi3"]]
+
+
+def test_q13_matches_golden(orc):
+    cu, od = orc.q13_tables(300, 3000, 42)
+    assert orc.q13(cu, od) == [tuple(x) for x in GOLDEN["q13"]["300_3000_42"]]
+    cu, od = orc.q13_tables(200, 4000, 9)
+    assert orc.q13(cu, od, b"pinto", b"beans") == [tuple(x) for x in GOLDEN["q13"]["200_4000_9_pinto_beans"]]
 
 
 def test_q1_q6_threaded_equal_serial(orc):
@@ -202,6 +210,18 @@ def test_q12_pinned_to_reference_kernels(orc, n_or, n_li, seed, window):
                 li["ship_mode"].ctypes.data, *window, 16, 4, out.ctypes.data)
     (mh, ml), (sh, sl) = orc.q12(od, li, *window)
     assert [mh, ml, sh, sl] == out.tolist()
+
+
+@pytest.mark.parametrize("n_cu,n_or,seed", [(300, 3000, 42), (5000, 60000, 7)])
+def test_q13_pinned_to_reference_kernels(orc, n_cu, n_or, seed):
+    """Q13's pattern match, counts and histogram are integer work in the reference too:
+    bit-exact against its kernels (the reference keeps 256 bins)."""
+    ref = need_ref(orc)
+    cu, od = orc.q13_tables(n_cu, n_or, seed)
+    hist = np.zeros(256, np.uint32)
+    ref.ref_q13(n_cu, n_or, od["cust_key"].ctypes.data, od["comment"].ctypes.data, 8, 4, hist.ctypes.data)
+    theirs = sorted(((c, int(d)) for c, d in enumerate(hist) if d), key=lambda x: (-x[1], -x[0]))
+    assert orc.q13(cu, od) == theirs
 
 
 def test_micro_pinned_to_reference_kernels(orc):

@@ -26,7 +26,7 @@ def test_hand_written_rows_cpu():
 
 def test_orders_priority_round_trip_cpu():
     od = dict(order_key=orc.gen(30, 500, 4), cust_key=orc.gen(31, 500, 4, n_cust=50), order_date=orc.gen(32, 500, 4),
-              priority=orc.gen(33, 500, 4))
+              priority=orc.gen(33, 500, 4), comment=orc.gen(34, 500, 4))
     got = orc.parse_tbl_cpu("orders", orc.format_tbl("orders", od))
     for k, v in od.items():
         assert np.array_equal(np.asarray(got[k]), v), k
