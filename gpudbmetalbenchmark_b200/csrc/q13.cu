@@ -6,12 +6,10 @@
 // postProcessQ13 src/infra.h:778-800 (sort of the histogram).
 //
 // B200 design:
-//  - q13_count_kernel: a block stages the comments of 256 orders in shared memory (16-byte
-//    global loads of the contiguous 80-byte slots, rows laid out 21 words apart so that each
-//    thread's scan of its own row hits a different bank than its warp's other threads), then
-//    each thread scans its row once: a SWAR test marks the bytes equal to the first letter of
-//    the word being looked for (word1 until it is found, then word2 after it), and only those
-//    positions are compared in full. Qualifying orders add 1 to their customer's count
+//  - q13_count_kernel: one order per thread; its 80-byte comment slot goes into 20 registers
+//    (five 16-byte loads), and one branch-free pass marks with SWAR tests the positions whose
+//    first two bytes match word1 or word2; only those (rare) candidates are compared in full,
+//    so the lanes of a warp stay converged. Qualifying orders add 1 to their customer's count
 //    (L2-resident counter array, one atomic per order).
 //  - q13_hist_kernel: every customer row looks up its count and adds to a shared-memory
 //    histogram of GPUDB_Q13_MAX_COUNT + 1 bins, flushed with one atomic per nonzero bin.
@@ -26,7 +24,6 @@ namespace {
 
 constexpr int kQ13Threads = 256;
 constexpr int kSlotWords = GPUDB_COMMENT_WIDTH / 4;   // 20
-constexpr int kRowStride = kSlotWords + 1;            // 21: odd, so per-thread rows spread over the banks
 constexpr int kBins = GPUDB_Q13_MAX_COUNT + 1;
 
 struct Q13Pattern {
@@ -47,64 +44,83 @@ __device__ __forceinline__ bool word_at(const uint8_t* row, int pos, const uint8
   return true;
 }
 
-// LIKE '%w0%w1%' on one NUL-padded row held as kSlotWords words (shared memory).
-__device__ bool like2(const uint32_t* row_words, const uint8_t (&w)[2][16], const int32_t (&len)[2]) {
-  const uint8_t* row = reinterpret_cast<const uint8_t*>(row_words);
-  const uint32_t c0 = w[0][0] * 0x01010101u, c1 = w[1][0] * 0x01010101u;
-  int start = -1;   // first position after word 0, once found
-#pragma unroll 4
+// Byte flags (bits 7, 15, 23, 31) -> 4 consecutive bits: (m >> 7) * (1 + 2^7 + 2^14 + 2^21)
+// puts the flags of bytes 0..3 on bits 21..24 without carries.
+__device__ __forceinline__ uint32_t flags_to_nibble(uint32_t m) { return (((m >> 7) * 0x00204081u) >> 21) & 0xFu; }
+
+// LIKE '%w0%w1%' on one NUL-padded row: its kSlotWords words in registers, its bytes at
+// `row` (global memory, read again only to verify candidates). One branch-free pass marks,
+// for both words, the positions whose first two bytes match (SWAR on the row word and the row
+// word shifted by one byte); only those candidates, rare for two-letter prefixes, are
+// compared in full: the first verified w0, then any verified w1 at or after its end.
+__device__ bool like2(const uint32_t (&rw)[kSlotWords], const uint8_t* row, const uint8_t (&w)[2][16],
+                      const int32_t (&len)[2]) {
+  const uint32_t a0 = w[0][0] * 0x01010101u, b0 = w[0][1] * 0x01010101u;
+  const uint32_t a1 = w[1][0] * 0x01010101u, b1 = w[1][1] * 0x01010101u;
+  const bool two0 = len[0] > 1, two1 = len[1] > 1;
+  uint32_t c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};   // candidate bit per position 0..79
+#pragma unroll
   for (int k = 0; k < kSlotWords; k++) {
-    const uint32_t x = row_words[k];
-    if (start < 0) {
-      uint32_t m = zero_bytes(x ^ c0);
-      while (m) {
-        const int pos = 4 * k + ((__ffs(m) - 1) >> 3);
-        m &= m - 1;
-        if (word_at(row, pos, w[0], len[0])) { start = pos + len[0]; break; }
-      }
+    const uint32_t x = rw[k], nx = k + 1 < kSlotWords ? rw[k + 1] : 0u;
+    const uint32_t y = __funnelshift_r(x, nx, 8);   // the byte after each byte of x
+    const uint32_t m0 = zero_bytes(x ^ a0) & (two0 ? zero_bytes(y ^ b0) : 0x80808080u);
+    const uint32_t m1 = zero_bytes(x ^ a1) & (two1 ? zero_bytes(y ^ b1) : 0x80808080u);
+    c0[(4 * k) >> 5] |= flags_to_nibble(m0) << ((4 * k) & 31);
+    c1[(4 * k) >> 5] |= flags_to_nibble(m1) << ((4 * k) & 31);
+  }
+  int start = -1;
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    uint32_t m = start < 0 ? c0[q] : 0u;
+    while (m) {
+      const int pos = 32 * q + __ffs(m) - 1;
+      m &= m - 1;
+      if (word_at(row, pos, w[0], len[0])) { start = pos + len[0]; break; }
     }
-    if (start >= 0 && start < 4 * k + 4) {
-      uint32_t m = zero_bytes(x ^ c1);
-      while (m) {
-        const int pos = 4 * k + ((__ffs(m) - 1) >> 3);
-        m &= m - 1;
-        if (pos >= start && word_at(row, pos, w[1], len[1])) return true;
-      }
+  }
+  if (start < 0) return false;
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const int lo = start - 32 * q;   // positions >= start within this word
+    uint32_t m = lo <= 0 ? c1[q] : (lo >= 32 ? 0u : c1[q] & (0xFFFFFFFFu << lo));
+    while (m) {
+      const int pos = 32 * q + __ffs(m) - 1;
+      m &= m - 1;
+      if (word_at(row, pos, w[1], len[1])) return true;
     }
   }
   return false;
 }
 
+// One order per thread (grid-stride): its comment goes straight into registers (five 16-byte
+// loads when the column is aligned), no shared staging and no block barrier.
 __global__ void __launch_bounds__(kQ13Threads) q13_count_kernel(const char* __restrict__ comment,
                                                                  const int32_t* __restrict__ ocust, uint64_t n,
                                                                  int32_t cust_max, Q13Pattern pat, uint32_t* counts) {
-  __shared__ uint32_t rows[kQ13Threads * kRowStride];
   __shared__ uint8_t sw[2][16];
   __shared__ int32_t slen[2];
   if (threadIdx.x < 32) sw[threadIdx.x >> 4][threadIdx.x & 15] = pat.w[threadIdx.x >> 4][threadIdx.x & 15];
   if (threadIdx.x < 2) slen[threadIdx.x] = pat.len[threadIdx.x];
+  __syncthreads();
   const bool vec = (reinterpret_cast<uintptr_t>(comment) & 15u) == 0;
-  for (uint64_t base = (uint64_t)blockIdx.x * kQ13Threads; base < n; base += (uint64_t)gridDim.x * kQ13Threads) {
-    const uint32_t here = n - base < (uint64_t)kQ13Threads ? (uint32_t)(n - base) : (uint32_t)kQ13Threads;
-    const int32_t c = threadIdx.x < here ? ld_stream(ocust + base + threadIdx.x) : -1;
-    __syncthreads();   // the previous step's rows are no longer read
-    if (vec) {   // 16-byte pieces never cross a row (rows are 5 pieces)
-      const uint4* g = reinterpret_cast<const uint4*>(comment + base * GPUDB_COMMENT_WIDTH);
-      for (uint32_t i = threadIdx.x; i < here * (kSlotWords / 4); i += kQ13Threads) {
-        const uint4 v = ld_stream(g + i);
-        const uint32_t r = i / (kSlotWords / 4), k = (i - r * (kSlotWords / 4)) * 4;
-        uint32_t* d = rows + r * kRowStride + k;
-        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+  const uint64_t stride = (uint64_t)gridDim.x * kQ13Threads;
+  for (uint64_t r = (uint64_t)blockIdx.x * kQ13Threads + threadIdx.x; r < n; r += stride) {
+    const int32_t c = ld_stream(ocust + r);
+    if (c < 0 || c > cust_max) continue;   // an order of no known customer: its comment is not read
+    const uint8_t* row = reinterpret_cast<const uint8_t*>(comment) + r * GPUDB_COMMENT_WIDTH;
+    uint32_t rw[kSlotWords];
+    if (vec) {
+#pragma unroll
+      for (int q = 0; q < kSlotWords / 4; q++) {
+        const uint4 v = ld_stream(reinterpret_cast<const uint4*>(row) + q);
+        rw[4 * q] = v.x; rw[4 * q + 1] = v.y; rw[4 * q + 2] = v.z; rw[4 * q + 3] = v.w;
       }
     } else {
-      const uint8_t* g = reinterpret_cast<const uint8_t*>(comment + base * GPUDB_COMMENT_WIDTH);
-      for (uint32_t i = threadIdx.x; i < here * GPUDB_COMMENT_WIDTH; i += kQ13Threads) {
-        const uint32_t r = i / GPUDB_COMMENT_WIDTH, b = i - r * GPUDB_COMMENT_WIDTH;
-        reinterpret_cast<uint8_t*>(rows + r * kRowStride)[b] = g[i];
-      }
+#pragma unroll
+      for (int k = 0; k < kSlotWords; k++)
+        rw[k] = row[4 * k] | (uint32_t)row[4 * k + 1] << 8 | (uint32_t)row[4 * k + 2] << 16 | (uint32_t)row[4 * k + 3] << 24;
     }
-    __syncthreads();
-    if (c >= 0 && c <= cust_max && !like2(rows + threadIdx.x * kRowStride, sw, slen)) atomicAdd(counts + c, 1u);
+    if (!like2(rw, row, sw, slen)) atomicAdd(counts + c, 1u);
   }
 }
 
