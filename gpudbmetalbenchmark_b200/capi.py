@@ -134,6 +134,19 @@ class Q12Result(C.Structure):
     _fields_ = [("high", C.c_uint64 * 2), ("low", C.c_uint64 * 2)]
 
 
+class Q10Params(C.Structure):
+    _fields_ = [("date_lo", C.c_int32), ("date_hi", C.c_int32), ("k", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Q10Row(C.Structure):
+    _fields_ = [("cust_key", C.c_int32), ("reserved", C.c_int32), ("revenue", C.c_int64)]
+
+
+class Q10Result(C.Structure):
+    _fields_ = [("n_customers", C.c_uint64), ("n_rows", C.c_uint32), ("reserved", C.c_uint32),
+                ("rows", Q10Row * Q3_MAX_K)]
+
+
 class Q13Params(C.Structure):
     _fields_ = [("word1", C.c_char * 16), ("word2", C.c_char * 16)]
 
@@ -247,6 +260,8 @@ PROTOTYPES = {
     "gpudb_q4_priority": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q4Params), P(Q4Result), P(Timing), P(Exec)]),
     "gpudb_q12_shipmode": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q12Params), P(Q12Result), P(Timing),
                                      P(Exec)]),
+    "gpudb_q10_returned": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q10Params), P(Q10Result),
+                                     P(Timing), P(Exec)]),
     "gpudb_q13_distribution": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Q13Params), P(Q13Row), C.c_uint32,
                                          P(C.c_uint32), P(Timing), P(Exec)]),
     "gpudb_q3_join_topk": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q3Params), P(Q3Result),

@@ -299,6 +299,59 @@ void runQ12Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
+void runQ10Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 10 Benchmark ---\n");
+  const Scale& s = o.scale;
+  const double t0 = now_ms();
+  gpudb_customer cu{};
+  gpudb_orders orr{};
+  TblTable ct, ot;
+  Buffer ck, ok, oc, od;
+  if (!o.data_dir.empty()) {
+    ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0}, {4}, o.tbl_piece);
+    ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 1, 2}, {4, 4, 4}, o.tbl_piece);
+    cu = {ct.rows, ct.col_max[0], 0, ct.col<int32_t>(0), nullptr};
+    orr = {ot.rows, ot.col_max[0], ot.col_max[1], ot.col<int32_t>(0), ot.col<int32_t>(1), ot.col<int32_t>(2)};
+  } else {
+    gpudb_gen_spec cs{};
+    cs.seed = o.seed;
+    cs.n_rows = s.customer;
+    ck = generate(ctx, cs, GPUDB_COL_CU_CUST_KEY, GPUDB_MEM_DEVICE);
+    gpudb_gen_spec os = cs;
+    os.n_rows = s.orders;
+    os.n_cust = (int64_t)s.customer;
+    ok = generate(ctx, os, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
+    oc = generate(ctx, os, GPUDB_COL_OR_CUST_KEY, GPUDB_MEM_DEVICE);
+    od = generate(ctx, os, GPUDB_COL_OR_ORDER_DATE, GPUDB_MEM_DEVICE);
+    cu = {s.customer, (int32_t)s.customer - 1, 0, ck.as<int32_t>(), nullptr};
+    orr = {s.orders, (int32_t)(4 * (s.orders - 1) + 1), (int32_t)s.customer - 1, ok.as<int32_t>(), oc.as<int32_t>(),
+           od.as<int32_t>()};
+  }
+  Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_FLAG, GPUDB_COL_LI_EXT_PRICE,
+                                      GPUDB_COL_LI_DISCOUNT}, GPUDB_ORDERS_CLUSTERED, (int64_t)orr.n_rows, 0, 0);
+  const double gen_ms = now_ms() - t0;
+  std::printf("Loaded %" PRIu64 " customers, %" PRIu64 " orders, %" PRIu64 " lineitem rows for Q10.\n", cu.n_rows,
+              orr.n_rows, L.li.n_rows);
+  const gpudb_q10_params p{639, 731, 20, 0};   // 1993-10-01 <= o_orderdate < 1994-01-01, top 20
+  gpudb_q10_result r{};
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q10_returned(ctx, &cu, &orr, &L.li, &p, &r, &t, nullptr), "gpudb_q10");
+  const double p0 = now_ms();
+  std::printf("\nTPC-H Q10 Results (Top 20):\n");
+  std::printf("+---------+--------------------+--------------------+\n");
+  std::printf("| custkey |             c_name |            revenue |\n");
+  std::printf("+---------+--------------------+--------------------+\n");
+  for (uint32_t i = 0; i < r.n_rows; i++) {
+    char name[32];
+    std::snprintf(name, sizeof name, "Customer#%09d", r.rows[i].cust_key);
+    std::printf("| %7d | %18s | $%17s |\n", r.rows[i].cust_key, name, fixed(r.rows[i].revenue, 4).c_str());
+  }
+  std::printf("+---------+--------------------+--------------------+\n");
+  std::printf("Customers with returned revenue: %" PRIu64 "\n", r.n_customers);
+  header(o, "Q10", L.li.n_rows, t);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
+}
+
 void runQ13Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("\n--- Running TPC-H Query 13 Benchmark ---\n");
   const double t0 = now_ms();

@@ -120,6 +120,18 @@ __device__ __forceinline__ uint32_t smem_filter_mask(const uint32_t* sfilt, bool
   return pass & hit;
 }
 
+// Sets bit `key` of `bitmap` for the lanes with `on` (keys already range-checked): one
+// atomicOr per distinct word of the warp (lanes of a word found with __match_any_sync, their
+// bits merged with a masked OR-reduce). Every lane of the warp calls it.
+__device__ __forceinline__ void warp_bitmap_or(bool on, int32_t key, uint32_t* bitmap) {
+  const uint32_t onmask = __ballot_sync(FULL_MASK, on);
+  if (!on) return;
+  const uint32_t word = (uint32_t)key >> 5;
+  const uint32_t peers = __match_any_sync(onmask, word);
+  const uint32_t bits = __reduce_or_sync(peers, 1u << ((uint32_t)key & 31u));
+  if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicOr(bitmap + word, bits);
+}
+
 // Warp-aggregated append: returns this lane's output position (valid where `take`).
 __device__ __forceinline__ uint32_t warp_append(bool take, uint32_t* counter) {
   const uint32_t m = __ballot_sync(FULL_MASK, take);

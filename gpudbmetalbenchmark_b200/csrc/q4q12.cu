@@ -26,16 +26,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kRows = 4;   // rows per thread per block step
 
-// Sets bit `key` of `bitmap` for the lanes with `on`: one atomicOr per distinct word.
-__device__ __forceinline__ void warp_bitmap_or(bool on, int32_t key, uint32_t* bitmap) {
-  const uint32_t onmask = __ballot_sync(FULL_MASK, on);
-  if (!on) return;
-  const uint32_t word = (uint32_t)key >> 5;
-  const uint32_t peers = __match_any_sync(onmask, word);
-  const uint32_t bits = __reduce_or_sync(peers, 1u << ((uint32_t)key & 31u));
-  if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicOr(bitmap + word, bits);
-}
-
 // Adds the block's per-thread bins into out[0..B) (one atomic per nonzero bin per block).
 template <int B>
 __device__ __forceinline__ void block_add_bins(const uint32_t (&c)[B], unsigned long long* out) {

@@ -331,6 +331,18 @@ class Engine:
                                                 self._exec(async_, None)))
         return r if async_ else [(r.high[0], r.low[0]), (r.high[1], r.low[1])]
 
+    def q10(self, cu, od, li, date_lo=639, date_hi=731, k=20, timing=None):
+        """([(cust_key, revenue)] top k by revenue desc, key asc; customers with revenue > 0):
+        revenue of returned lineitems (flag 2, 'R') of orders in [date_lo, date_hi) per
+        customer (default 1993-10-01 .. 1994-01-01), hundredths^2."""
+        p = capi.Q10Params(date_lo, date_hi, k, 0)
+        r = capi.Q10Result()
+        ls = li if isinstance(li, capi.Lineitem) else li.lineitem()
+        self._check(self.lib.gpudb_q10_returned(self.ctx, C.byref(cu.struct()), C.byref(od.struct()), C.byref(ls),
+                                                C.byref(p), C.byref(r),
+                                                C.byref(timing) if timing is not None else None, None))
+        return [(x.cust_key, x.revenue) for x in r.rows[:r.n_rows]], r.n_customers
+
     def q13(self, cu, od, word1=b"special", word2=b"requests", capacity=capi.Q13_MAX_COUNT + 1, timing=None):
         """[(c_count, custdist)] ordered by custdist desc, c_count desc: customers per number of
         their orders whose comment is NOT LIKE '%word1%word2%'."""

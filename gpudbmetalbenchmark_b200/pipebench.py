@@ -236,6 +236,17 @@ def main(argv=None):
             emit("q12_shipmode", label, n_li, ms, n_li * 17 + n_or * 5, {"kernels": t.kernels})
             eng.free(li)
             eng.free(od)
+    if on("q10"):
+        for n_cu, n_or, n_li, label in ((150_000, 1_500_000, 6_000_000, "SF-1 sizes"),
+                                        (1_500_000, 15_000_000, 60_000_000, "SF-10 sizes")):
+            cu = eng.generate("customer", n_cu, seed=42, columns=("cust_key",))
+            od = eng.generate("orders", n_or, seed=42, columns=("order_key", "cust_key", "order_date"), n_cust=n_cu)
+            li = eng.generate("lineitem", n_li, seed=42, columns=("order_key", "flag", "ext_price", "discount"),
+                              n_orders=n_or, order_mode=capi.ORDERS_CLUSTERED)
+            ms, t = timed(lambda tm: eng.q10(cu, od, li, timing=tm), a.reps)
+            emit("q10_returned", label, n_li, ms, n_li * 5 + n_or * 12 + n_cu * 4, {"kernels": t.kernels})
+            for x in (li, od, cu):
+                eng.free(x)
     if on("q13"):
         for n_cu, n_or, label in ((150_000, 1_500_000, "SF-1 sizes"), (1_500_000, 15_000_000, "SF-10 sizes")):
             cu = eng.generate("customer", n_cu, seed=42, columns=("cust_key",))

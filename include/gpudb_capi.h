@@ -325,6 +325,27 @@ typedef struct gpudb_q12_result { uint64_t high[2]; uint64_t low[2]; } gpudb_q12
 int gpudb_q12_shipmode(gpudb_ctx* ctx, const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q12_params* p,
                        gpudb_q12_result* out, gpudb_timing* t, const gpudb_exec* ex);
 
+/* ---- Q10 returned item reporting (replaces runQ10Benchmark src/q10.cpp:8-140 with its kernels
+ *      q10_build_orders_map_kernel / q10_probe_and_aggregate_kernel kernels/q10.metal:8-54 and
+ *      its host top-20 heap src/q10.cpp:102-121) ------------------------------------------------
+ * revenue(customer) = sum of ext_price * (100 - discount) (hundredths^2) over lineitem rows with
+ * flag 2 ('R', returned) whose order has date_lo <= order_date < date_hi and belongs to a
+ * customer of `cu`. rows[] = the k (1..GPUDB_Q3_MAX_K) customers of largest revenue, ordered
+ * by revenue desc then cust_key asc; n_customers = customers with revenue > 0. An order key
+ * outside 0..od->key_max or a customer key outside 0..cu->key_max in the tables fails with
+ * GPUDB_E_KEY_RANGE; an order of a customer that is not in `cu` and a lineitem row of an
+ * order outside the window count for nobody. Lineitem may be host-resident (streamed). */
+typedef struct gpudb_q10_params { int32_t date_lo; int32_t date_hi; int32_t k; int32_t reserved; } gpudb_q10_params;
+typedef struct gpudb_q10_row { int32_t cust_key; int32_t reserved; int64_t revenue; } gpudb_q10_row;
+typedef struct gpudb_q10_result {
+  uint64_t n_customers;
+  uint32_t n_rows;
+  uint32_t reserved;
+  gpudb_q10_row rows[GPUDB_Q3_MAX_K];
+} gpudb_q10_result;
+int gpudb_q10_returned(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_orders* od, const gpudb_lineitem* li,
+                       const gpudb_q10_params* p, gpudb_q10_result* out, gpudb_timing* t, const gpudb_exec* ex);
+
 /* ---- Q13 customer distribution (replaces runQ13Benchmark src/q13.cpp:8-117 with its kernels
  *      q13_pattern_match_kernel / q13_count_prefiltered_kernel / q13_build_histogram_kernel
  *      kernels/q13.metal:33-168 and postProcessQ13 src/infra.h:778-800) -------------------------

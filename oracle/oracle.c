@@ -417,6 +417,48 @@ void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t 
   free(high);
 }
 
+/* ---- Q10: kernels/q10.metal:8-54 (window map, returned rows), src/q10.cpp:102-121 (top-k) ---- */
+typedef struct { int64_t rev; int32_t key; } q10row;
+static int q10_cmp(const void* a, const void* b) {
+  const q10row *x = (const q10row*)a, *y = (const q10row*)b;
+  if (x->rev != y->rev) return x->rev > y->rev ? -1 : 1;
+  return x->key < y->key ? -1 : (x->key > y->key);
+}
+uint64_t or_q10(uint64_t n_cu, const int32_t* cu_key, int32_t cu_key_max, uint64_t n_or, const int32_t* o_key,
+                const int32_t* o_cust, const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key,
+                const uint8_t* l_flag, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
+                int32_t k, int32_t* top_key, int64_t* top_rev, int64_t* rev_out) {
+  uint64_t i;
+  if (cu_key_max < 0) return 0;
+  uint8_t* is_cust = (uint8_t*)calloc((size_t)cu_key_max + 1, 1);
+  int64_t* rev = (int64_t*)calloc((size_t)cu_key_max + 1, 8);
+  int32_t* cust_of = or_key_max >= 0 ? (int32_t*)malloc(((size_t)or_key_max + 1) * 4) : NULL;
+  for (i = 0; i < n_cu; i++) is_cust[cu_key[i]] = 1;
+  if (cust_of) {
+    for (i = 0; i <= (uint64_t)or_key_max; i++) cust_of[i] = -1;
+    for (i = 0; i < n_or; i++)
+      if (o_date[i] >= date_lo && o_date[i] < date_hi) cust_of[o_key[i]] = o_cust[i];
+    for (i = 0; i < n_li; i++) {
+      if (l_flag[i] != 2 || l_key[i] < 0 || l_key[i] > or_key_max) continue;
+      const int32_t c = cust_of[l_key[i]];
+      if (c < 0 || c > cu_key_max || !is_cust[c]) continue;
+      rev[c] += l_ext[i] * (int64_t)(100 - l_disc[i]);
+    }
+  }
+  q10row* rows = (q10row*)malloc(((size_t)cu_key_max + 1) * sizeof(q10row));
+  uint64_t n = 0;
+  for (int64_t c = 0; c <= cu_key_max; c++)
+    if (rev[c] > 0) { rows[n].rev = rev[c]; rows[n].key = (int32_t)c; n++; }
+  qsort(rows, n, sizeof(q10row), q10_cmp);
+  for (int32_t r = 0; r < k; r++) {
+    top_key[r] = r < (int64_t)n ? rows[r].key : -1;
+    top_rev[r] = r < (int64_t)n ? rows[r].rev : 0;
+  }
+  if (rev_out) memcpy(rev_out, rev, ((size_t)cu_key_max + 1) * 8);
+  free(is_cust); free(rev); free(cust_of); free(rows);
+  return n;
+}
+
 /* ---- Q13: kernels/q13.metal:33-68 (first w1, then w2 after it), :110-127 (counts),
  * :133-168 (histogram), src/infra.h:783-800 (custdist desc, c_count desc) ---- */
 static int like2(const char* s, const char* w1, const char* w2) {

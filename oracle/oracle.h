@@ -82,6 +82,16 @@ void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t 
             const uint8_t* l_mode, int32_t receipt_lo, int32_t receipt_hi, int32_t mode0, int32_t mode1,
             int32_t high_max, uint64_t* out4);
 
+/* Q10: exact revenue sum ext*(100-disc) of returned lineitems (flag 2) per customer of cu, over
+ * orders with date_lo <= date < date_hi (kernels/q10.metal:8-54); the top k by revenue desc,
+ * cust_key asc among customers with revenue > 0 (src/q10.cpp:102-121). rev_out (cu_key_max+1
+ * entries, may be NULL) gets every customer's revenue. Returns the number of customers with
+ * revenue > 0. */
+uint64_t or_q10(uint64_t n_cu, const int32_t* cu_key, int32_t cu_key_max, uint64_t n_or, const int32_t* o_key,
+                const int32_t* o_cust, const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key,
+                const uint8_t* l_flag, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
+                int32_t k, int32_t* top_key, int64_t* top_rev, int64_t* rev_out);
+
 /* Q13: per-customer counts of orders whose 80-byte NUL-padded comment is NOT LIKE
  * '%w1%w2%' (kernels/q13.metal:33-127), the histogram of those counts over the customer rows
  * (kernels/q13.metal:133-168) ordered by custdist desc, c_count desc (postProcessQ13

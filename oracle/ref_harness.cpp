@@ -1,5 +1,5 @@
 // ref_harness.cpp -- runs the reference's own Metal kernels (kernels/q1.metal, q3.metal,
-// q4.metal, q6.metal, q9.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
+// q4.metal, q6.metal, q9.metal, q10.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
 // through the CPU shim in oracle/refshim) on the synthetic tables. TEST INFRASTRUCTURE
 // ONLY: it pins the oracle's query logic to the reference's code, and it is the timed
 // reference arm of bench.py. It is never linked into the engine.
@@ -17,6 +17,7 @@ using namespace metal;
 #include "common.h"
 #include "microbenchmarks.metal"
 #include "q1.metal"
+#include "q10.metal"
 #include "q12.metal"
 #include "q13.metal"
 #include "q3.metal"
@@ -241,6 +242,31 @@ void ref_q12(uint64_t n_or, const int32_t* or_key, const uint8_t* or_prio, uint6
   });
   uint ng = (uint)groups;
   q12_final_count_stage2(partial.data(), out4, ng, 0);
+}
+
+// Q10 through q10_build_orders_map_kernel and q10_probe_and_aggregate_kernel
+// (kernels/q10.metal:8-54): float revenue per customer key (its customers are indexed by
+// key: cust_rev has max key + 1 entries). Return flags are the characters A/N/R.
+void ref_q10(uint64_t n_or, const int32_t* or_key, const int32_t* or_cust, const int32_t* or_date, uint64_t n_li,
+             const int32_t* li_key, const uint8_t* li_flag, const int64_t* li_ext, const int32_t* li_disc,
+             int32_t date_lo, int32_t date_hi, int groups, int threads, float* cust_rev, uint32_t n_cust) {
+  int max_key = 0;
+  for (uint64_t i = 0; i < n_or; i++) max_key = std::max(max_key, or_key[i]);
+  for (uint64_t i = 0; i < n_li; i++) max_key = std::max(max_key, li_key[i]);
+  uint map_size = (uint)max_key + 1, nor = (uint)n_or, nli = (uint)n_li;
+  std::vector<int> omap(map_size, -1), od = dates(n_or, or_date);
+  int ds = yyyymmdd(date_lo), de = yyyymmdd(date_hi);
+  for (uint i = 0; i < nor; i++) q10_build_orders_map_kernel(or_key, or_cust, od.data(), omap.data(), nor, ds, de, i);
+  std::vector<char> rf(n_li);
+  for (uint64_t i = 0; i < n_li; i++) rf[i] = "ANR"[li_flag[i] % 3];
+  std::vector<float> ext = hundredths(n_li, li_ext), dsc = hundredths(n_li, li_disc);
+  std::vector<atomic_float> rev(n_cust);
+  for (auto& r : rev) r.v = 0.0f;
+  run_groups((uint)groups, threads, [&](uint g) {
+    q10_probe_and_aggregate_kernel(li_key, rf.data(), ext.data(), dsc.data(), omap.data(), rev.data(), nli, map_size,
+                                   g, 0, 1, (uint)groups);
+  });
+  for (uint32_t c = 0; c < n_cust; c++) cust_rev[c] = rev[c].v;
 }
 
 // Q13 through q13_pattern_match_kernel, q13_count_prefiltered_kernel and

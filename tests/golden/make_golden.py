@@ -197,8 +197,21 @@ def q13(n_cu, n_or, seed, w1="special", w2="requests"):
     return sorted(([c, d] for c, d in hist.items()), key=lambda x: (-x[1], -x[0]))
 
 
+def q10(n_cu, n_or, n_li, seed, date_lo=639, date_hi=731, k=20):
+    ocust = column("o_cust", n_or, seed, n_cust=n_cu)
+    odate = column("o_date", n_or, seed)
+    cust_of = {4 * i + 1: ocust[i] for i in range(n_or) if date_lo <= odate[i] < date_hi}
+    li = {c: column(c, n_li, seed, n_orders=n_or, mode=1) for c in ("order_key", "flag", "ext_price", "discount")}
+    rev = {}
+    for key, f, e, d in zip(li["order_key"], li["flag"], li["ext_price"], li["discount"]):
+        if f == 2 and key in cust_of:
+            rev[cust_of[key]] = rev.get(cust_of[key], 0) + e * (100 - d)
+    rows = sorted(((c, r) for c, r in rev.items() if r > 0), key=lambda x: (-x[1], x[0]))
+    return {"customers": len(rows), "top": [[c, str(r)] for c, r in rows[:k]]}
+
+
 def main():
-    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}}
+    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}, "q10": {}}
     # generator: first values and column sums for two seeds and a shifted window
     for seed, off in ((42, 0), (7, 1000)):
         cols = {}
@@ -232,6 +245,8 @@ def main():
     out["q12"]["3000_12000_42"] = q12(3000, 12000, 42)
     out["q12"]["2000_9000_5_air_truck_hi3"] = q12(2000, 9000, 5, 0, 2600, (0, 6), 3)
     out["q13"]["300_3000_42"] = q13(300, 3000, 42)
+    out["q10"]["300_3000_12000_42"] = q10(300, 3000, 12000, 42)
+    out["q10"]["200_2000_9000_5_wide"] = q10(200, 2000, 9000, 5, 0, 2406, 7)
     out["q13"]["200_4000_9_pinto_beans"] = q13(200, 4000, 9, "pinto", "beans")
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
     with open(path, "w") as f:

@@ -36,6 +36,7 @@ ORACLE_ARGS = {
     "or_q4": [U64, V, V, V, I32, U64, V, V, V, I32, I32, V],
     "or_q12": [U64, V, V, I32, U64, V, V, V, V, V, I32, I32, I32, I32, I32, V],
     "or_q13": [U64, V, I32, U64, V, V, C.c_char_p, C.c_char_p, V, V, U32],
+    "or_q10": [U64, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, I32, V, V, V],
     "or_select_lt": [U64, V, I32, V, V],
     "or_sum_i32": [U64, V],
     "or_join_count": [U64, V, U64, V],
@@ -52,6 +53,7 @@ REF_ARGS = {
     "ref_q4": [U64, V, V, V, U64, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_q12": [U64, V, V, U64, V, V, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_q13": [U64, U64, V, V, C.c_int, C.c_int, V],
+    "ref_q10": [U64, V, V, V, U64, V, V, V, V, I32, I32, C.c_int, C.c_int, V, U32],
     "ref_select_lt": [U64, V, I32, V],
     "ref_sum": [U64, V, C.c_int, C.c_int],
     "ref_join_count": [U64, V, U64, V],
@@ -84,6 +86,7 @@ def oracle():
         _or.or_q9.restype = C.c_uint32
         _or.or_select_lt.restype = C.c_uint64
         _or.or_q13.restype = C.c_uint32
+        _or.or_q10.restype = C.c_uint64
         _or.or_sum_i32.restype = C.c_int64
         _or.or_join_count.restype = C.c_uint64
         _or.or_join_pairs.restype = C.c_uint64
@@ -136,6 +139,26 @@ def q4_tables(n_or, n_li, seed=42, order_mode=1):
     li = lineitem(n_li, seed, n_orders=n_or, order_mode=order_mode,
                   cols=("order_key", "ship_date", "commit_date", "receipt_date", "ship_mode"))
     return od, li
+
+
+def q10_tables(n_cu, n_or, n_li, seed=42):
+    cu = dict(cust_key=gen(20, n_cu, seed))
+    od = dict(order_key=gen(30, n_or, seed), cust_key=gen(31, n_or, seed, n_cust=n_cu), order_date=gen(32, n_or, seed))
+    li = lineitem(n_li, seed, n_orders=n_or, order_mode=1, cols=("order_key", "flag", "ext_price", "discount"))
+    return cu, od, li
+
+
+def q10(cu, od, li, date_lo=639, date_hi=731, k=20, cu_key_max=None, or_key_max=None, rev_out=None):
+    """([(cust_key, revenue)] top k, number of customers with revenue > 0)."""
+    n_cu = len(cu["cust_key"])
+    ck = (int(cu["cust_key"].max()) if n_cu else -1) if cu_key_max is None else cu_key_max
+    ok = (int(od["order_key"].max()) if len(od["order_key"]) else -1) if or_key_max is None else or_key_max
+    tk, tr = np.zeros(k, np.int32), np.zeros(k, np.int64)
+    n = oracle().or_q10(n_cu, _p(cu["cust_key"]), ck, len(od["order_key"]), _p(od["order_key"]), _p(od["cust_key"]),
+                        _p(od["order_date"]), ok, len(li["order_key"]), _p(li["order_key"]), _p(li["flag"]),
+                        _p(li["ext_price"]), _p(li["discount"]), date_lo, date_hi, k, tk.ctypes.data, tr.ctypes.data,
+                        None if rev_out is None else rev_out.ctypes.data)
+    return [(int(a), int(b)) for a, b in zip(tk, tr) if a >= 0], int(n)
 
 
 def q13_tables(n_cu, n_or, seed=42):

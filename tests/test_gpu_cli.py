@@ -108,6 +108,16 @@ def test_cli_q13(orc):
     assert re.search(r"^Q13 \| 15000 orders \| 1500 customers", out, re.M)
 
 
+def test_cli_q10(orc):
+    cu, od, li = orc.q10_tables(1_500, 15_000, 60_000, 42)
+    top, n = orc.q10(cu, od, li)
+    out = run("sf1", "q10", "--scale", "0.01")
+    rows = re.findall(r"^\|\s+(\d+) \| Customer#\d+ \| \$\s*(\S+) \|$", out, re.M)
+    assert [(int(c), scaled(r, 4)) for c, r in rows] == top
+    assert int(re.search(r"Customers with returned revenue: (\d+)", out).group(1)) == n
+    timing_ok(out, "Q10", 60000)
+
+
 def test_cli_microbenchmarks(orc):
     out = run("sf1", "selection", "--scale", "0.01")
     col = orc.gen(1, 60000, 42)

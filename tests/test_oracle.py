@@ -93,6 +93,15 @@ def test_q13_matches_golden(orc):
     assert orc.q13(cu, od, b"pinto", b"beans") == [tuple(x) for x in GOLDEN["q13"]["200_4000_9_pinto_beans"]]
 
 
+def test_q10_matches_golden(orc):
+    cu, od, li = orc.q10_tables(300, 3000, 12000, 42)
+    g = GOLDEN["q10"]["300_3000_12000_42"]
+    assert orc.q10(cu, od, li) == ([(c, int(r)) for c, r in g["top"]], g["customers"])
+    cu, od, li = orc.q10_tables(200, 2000, 9000, 5)
+    g = GOLDEN["q10"]["200_2000_9000_5_wide"]
+    assert orc.q10(cu, od, li, 0, 2406, 7) == ([(c, int(r)) for c, r in g["top"]], g["customers"])
+
+
 def test_q1_q6_threaded_equal_serial(orc):
     li = orc.lineitem(50_000, 3)
     assert orc.q6(li) == orc.q6(li, threads=4)
@@ -222,6 +231,23 @@ def test_q13_pinned_to_reference_kernels(orc, n_cu, n_or, seed):
     ref.ref_q13(n_cu, n_or, od["cust_key"].ctypes.data, od["comment"].ctypes.data, 8, 4, hist.ctypes.data)
     theirs = sorted(((c, int(d)) for c, d in enumerate(hist) if d), key=lambda x: (-x[1], -x[0]))
     assert orc.q13(cu, od) == theirs
+
+
+@pytest.mark.parametrize("sizes,seed,window", [((300, 3000, 12000), 42, (639, 731)), ((2000, 20000, 80000), 7, (0, 2406))])
+def test_q10_pinned_to_reference_kernels(orc, sizes, seed, window):
+    """Q10 per-customer revenue against the reference's kernels (float32 there: within its
+    tolerance; which customers have revenue, exactly)."""
+    ref = need_ref(orc)
+    cu, od, li = orc.q10_tables(*sizes, seed)
+    n_cu = sizes[0]
+    mine = np.zeros(n_cu, np.int64)
+    orc.q10(cu, od, li, *window, rev_out=mine)
+    theirs = np.zeros(n_cu, np.float32)
+    ref.ref_q10(len(od["order_key"]), od["order_key"].ctypes.data, od["cust_key"].ctypes.data,
+                od["order_date"].ctypes.data, len(li["order_key"]), li["order_key"].ctypes.data, li["flag"].ctypes.data,
+                li["ext_price"].ctypes.data, li["discount"].ctypes.data, *window, 8, 4, theirs.ctypes.data, n_cu)
+    assert np.array_equal(mine > 0, theirs > 0)
+    np.testing.assert_allclose(theirs, mine / 10000.0, rtol=1e-4)
 
 
 def test_micro_pinned_to_reference_kernels(orc):
