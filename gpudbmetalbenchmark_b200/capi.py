@@ -33,7 +33,7 @@ TBL_COLUMNS = {
     "lineitem": (TBL_LINEITEM, ("order_key", "part_key", "supp_key", "quantity", "ext_price", "discount", "tax",
                                 "flag", "status", "ship_date", "commit_date", "receipt_date", "ship_mode")),
     "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date", "priority", "comment")),
-    "customer": (TBL_CUSTOMER, ("cust_key", "segment")),
+    "customer": (TBL_CUSTOMER, ("cust_key", "nation", "segment")),
     "part": (TBL_PART, ("part_key", "flag")),
     "supplier": (TBL_SUPPLIER, ("supp_key", "nation")),
     "partsupp": (TBL_PARTSUPP, ("part_key", "supp_key", "supply_cost")),
@@ -54,7 +54,7 @@ Q13_MAX_COUNT = 1023
 COL = dict(
     LI_SHIP_DATE=1, LI_QUANTITY=2, LI_EXT_PRICE=3, LI_DISCOUNT=4, LI_TAX=5, LI_FLAG=6, LI_STATUS=7,
     LI_ORDER_KEY=8, LI_PART_KEY=9, LI_SUPP_KEY=10, LI_COMMIT_DATE=11, LI_RECEIPT_DATE=12, LI_SHIP_MODE=13,
-    CU_CUST_KEY=20, CU_SEGMENT=21,
+    CU_CUST_KEY=20, CU_SEGMENT=21, CU_NATION=22,
     OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32, OR_PRIORITY=33, OR_COMMENT=34,
     PA_PART_KEY=40, PA_FLAG=41,
     SU_SUPP_KEY=50, SU_NATION=51,
@@ -89,7 +89,7 @@ class Lineitem(C.Structure):
 
 class Customer(C.Structure):
     _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("reserved", C.c_int32),
-                ("cust_key", vp), ("segment", vp)]
+                ("cust_key", vp), ("segment", vp), ("nation", vp)]
 
 
 class Orders(C.Structure):
@@ -132,6 +132,29 @@ class Q12Params(C.Structure):
 
 class Q12Result(C.Structure):
     _fields_ = [("high", C.c_uint64 * 2), ("low", C.c_uint64 * 2)]
+
+
+NATIONS = 25
+# TPC-H nation -> region (the fixed nation table); regions AFRICA, AMERICA, ASIA, EUROPE, MIDDLE EAST
+NATION_REGION = (0, 1, 1, 1, 4, 0, 3, 3, 2, 2, 4, 4, 2, 4, 0, 0, 0, 1, 2, 3, 4, 2, 3, 3, 1)
+NATION_NAMES = ("ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
+                "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
+                "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES")
+REGION_NAMES = ("AFRICA", "AMERICA", "ASIA", "EUROPE", "MIDDLE EAST")
+
+
+def region_mask(region):
+    """Bit n set for the nations of `region` (index or name)."""
+    r = REGION_NAMES.index(region) if isinstance(region, str) else region
+    return sum(1 << n for n, g in enumerate(NATION_REGION) if g == r)
+
+
+class Q5Params(C.Structure):
+    _fields_ = [("date_lo", C.c_int32), ("date_hi", C.c_int32), ("nation_mask", C.c_uint32), ("reserved", C.c_int32)]
+
+
+class Q5Result(C.Structure):
+    _fields_ = [("revenue", C.c_int64 * NATIONS)]
 
 
 class Q10Params(C.Structure):
@@ -260,6 +283,8 @@ PROTOTYPES = {
     "gpudb_q4_priority": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q4Params), P(Q4Result), P(Timing), P(Exec)]),
     "gpudb_q12_shipmode": (C.c_int, [ctx_p, P(Orders), P(Lineitem), P(Q12Params), P(Q12Result), P(Timing),
                                      P(Exec)]),
+    "gpudb_q5_local_supplier": (C.c_int, [ctx_p, P(Customer), P(Supplier), P(Orders), P(Lineitem), P(Q5Params),
+                                          P(Q5Result), P(Timing), P(Exec)]),
     "gpudb_q10_returned": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q10Params), P(Q10Result),
                                      P(Timing), P(Exec)]),
     "gpudb_q13_distribution": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Q13Params), P(Q13Row), C.c_uint32,

@@ -40,6 +40,7 @@ __host__ __device__ __forceinline__ void gen_value(const GenArgs& a, uint64_t r,
     case GPUDB_COL_LI_SHIP_MODE: u8[i] = gd_li_ship_mode(a.seed, r); break;
     case GPUDB_COL_CU_CUST_KEY: i32[i] = (int32_t)r; break;
     case GPUDB_COL_CU_SEGMENT: u8[i] = gd_cu_segment(a.seed, r); break;
+    case GPUDB_COL_CU_NATION: u8[i] = gd_cu_nation(a.seed, r); break;
     case GPUDB_COL_OR_ORDER_KEY: i32[i] = gd_order_key_of((int64_t)r); break;
     case GPUDB_COL_OR_CUST_KEY: i32[i] = gd_or_cust(a.seed, r, a.n_cust); break;
     case GPUDB_COL_OR_ORDER_DATE: i32[i] = gd_or_date(a.seed, r); break;
@@ -87,6 +88,7 @@ int column_width(int32_t c) {
     case GPUDB_COL_LI_EXT_PRICE: case GPUDB_COL_PS_SUPPLY_COST: return 8;
     case GPUDB_COL_LI_FLAG: case GPUDB_COL_LI_STATUS: case GPUDB_COL_CU_SEGMENT:
     case GPUDB_COL_PA_FLAG: case GPUDB_COL_SU_NATION: case GPUDB_COL_LI_SHIP_MODE: case GPUDB_COL_OR_PRIORITY:
+    case GPUDB_COL_CU_NATION:
       return 1;
     case GPUDB_COL_LI_COMMIT_DATE: case GPUDB_COL_LI_RECEIPT_DATE: return 4;
     case GPUDB_COL_OR_COMMENT: return GD_COMMENT_WIDTH;

@@ -38,7 +38,7 @@ enum gd_column {
   GD_LI_SHIP_DATE = 16, GD_LI_QUANTITY, GD_LI_UNIT_PRICE, GD_LI_DISCOUNT, GD_LI_TAX,
   GD_LI_FLAG, GD_LI_STATUS, GD_LI_ORDER_PICK, GD_LI_PART, GD_LI_SUPP_SLOT, GD_LI_ORDER_RUN,
   GD_LI_COMMIT, GD_LI_RECEIPT, GD_LI_MODE,
-  GD_CU_SEGMENT = 32,
+  GD_CU_SEGMENT = 32, GD_CU_NATION,
   GD_OR_CUST = 48, GD_OR_DATE, GD_OR_PRIORITY, GD_OR_COMMENT,
   GD_PA_FLAG = 64,
   GD_SU_NATION = 80,
@@ -139,6 +139,7 @@ GD_HD void gd_or_comment(uint64_t seed, uint64_t r, char* out) {
   }
   for (; n < GD_COMMENT_WIDTH; n++) out[n] = 0;
 }
+GD_HD uint8_t gd_cu_nation(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_CU_NATION, r, 0, 24); }
 GD_HD uint8_t gd_cu_segment(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_CU_SEGMENT, r, 0, 4); }
 GD_HD int32_t gd_or_cust(uint64_t seed, uint64_t r, int64_t n_cust) { return (int32_t)gd_uniform(seed, GD_OR_CUST, r, 0, n_cust - 1); }
 GD_HD int32_t gd_or_date(uint64_t seed, uint64_t r) { return (int32_t)gd_uniform(seed, GD_OR_DATE, r, 0, GD_ORDER_DATE_MAX); }

@@ -201,9 +201,9 @@ void runQ3Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   TblTable ct, ot;
   Buffer ck, cg, ok, oc, od;
   if (!o.data_dir.empty()) {
-    ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0, 1}, {4, 1}, o.tbl_piece);
+    ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0, 2}, {4, 1}, o.tbl_piece);
     ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 1, 2}, {4, 4, 4}, o.tbl_piece);
-    cu = {ct.rows, ct.col_max[0], 0, ct.col<int32_t>(0), ct.col<uint8_t>(1)};
+    cu = {ct.rows, ct.col_max[0], 0, ct.col<int32_t>(0), ct.col<uint8_t>(2)};
     orr = {ot.rows, ot.col_max[0], ot.col_max[1], ot.col<int32_t>(0), ot.col<int32_t>(1), ot.col<int32_t>(2)};
   } else {
     gpudb_gen_spec cs{};
@@ -296,6 +296,75 @@ void runQ12Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("| SHIP     | %16" PRIu64 " | %15" PRIu64 " |\n", r.high[1], r.low[1]);
   std::printf("+----------+------------------+-----------------+\n");
   header(o, "Q12", L.li.n_rows, t);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
+}
+
+void runQ5Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 5 Benchmark ---\n");
+  const Scale& s = o.scale;
+  const double t0 = now_ms();
+  gpudb_customer cu{};
+  gpudb_supplier su{};
+  gpudb_orders orr{};
+  TblTable ct, st, ot;
+  Buffer ck, cn, sk, sn, ok, oc, od;
+  if (!o.data_dir.empty()) {
+    ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0, 1}, {4, 1}, o.tbl_piece);
+    st = load_tbl(ctx, o.data_dir, "supplier", GPUDB_TBL_SUPPLIER, {0, 1}, {4, 1}, o.tbl_piece);
+    ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 1, 2}, {4, 4, 4}, o.tbl_piece);
+    cu = {ct.rows, ct.col_max[0], 0, ct.col<int32_t>(0), nullptr, ct.col<uint8_t>(1)};
+    su = {st.rows, st.col_max[0], 0, st.col<int32_t>(0), st.col<uint8_t>(1)};
+    orr = {ot.rows, ot.col_max[0], ot.col_max[1], ot.col<int32_t>(0), ot.col<int32_t>(1), ot.col<int32_t>(2)};
+  } else {
+    gpudb_gen_spec cs{};
+    cs.seed = o.seed;
+    cs.n_rows = s.customer;
+    ck = generate(ctx, cs, GPUDB_COL_CU_CUST_KEY, GPUDB_MEM_DEVICE);
+    cn = generate(ctx, cs, GPUDB_COL_CU_NATION, GPUDB_MEM_DEVICE);
+    gpudb_gen_spec ss = cs;
+    ss.n_rows = s.supplier;
+    sk = generate(ctx, ss, GPUDB_COL_SU_SUPP_KEY, GPUDB_MEM_DEVICE);
+    sn = generate(ctx, ss, GPUDB_COL_SU_NATION, GPUDB_MEM_DEVICE);
+    gpudb_gen_spec os = cs;
+    os.n_rows = s.orders;
+    os.n_cust = (int64_t)s.customer;
+    ok = generate(ctx, os, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
+    oc = generate(ctx, os, GPUDB_COL_OR_CUST_KEY, GPUDB_MEM_DEVICE);
+    od = generate(ctx, os, GPUDB_COL_OR_ORDER_DATE, GPUDB_MEM_DEVICE);
+    cu = {s.customer, (int32_t)s.customer - 1, 0, ck.as<int32_t>(), nullptr, cn.as<uint8_t>()};
+    su = {s.supplier, (int32_t)s.supplier - 1, 0, sk.as<int32_t>(), sn.as<uint8_t>()};
+    orr = {s.orders, (int32_t)(4 * (s.orders - 1) + 1), (int32_t)s.customer - 1, ok.as<int32_t>(), oc.as<int32_t>(),
+           od.as<int32_t>()};
+  }
+  Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_SUPP_KEY, GPUDB_COL_LI_EXT_PRICE,
+                                      GPUDB_COL_LI_DISCOUNT}, GPUDB_ORDERS_CLUSTERED, (int64_t)orr.n_rows,
+                             (int64_t)s.part, (int64_t)su.n_rows);
+  const double gen_ms = now_ms() - t0;
+  std::printf("Loaded %" PRIu64 " customers, %" PRIu64 " suppliers, %" PRIu64 " orders, %" PRIu64 " lineitem rows.\n",
+              cu.n_rows, su.n_rows, orr.n_rows, L.li.n_rows);
+  static const char* nations[GPUDB_NATIONS] = {
+      "ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
+      "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
+      "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES"};
+  // ASIA (TPC-H nation table: INDIA, INDONESIA, JAPAN, CHINA, VIETNAM), orders of 1994
+  const gpudb_q5_params p{731, 1096, (1u << 8) | (1u << 9) | (1u << 12) | (1u << 18) | (1u << 21), 0};
+  gpudb_q5_result r{};
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q5_local_supplier(ctx, &cu, &su, &orr, &L.li, &p, &r, &t, nullptr), "gpudb_q5");
+  const double p0 = now_ms();
+  std::vector<int> order;
+  for (int n = 0; n < GPUDB_NATIONS; n++)
+    if (r.revenue[n]) order.push_back(n);
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    return r.revenue[a] != r.revenue[b] ? r.revenue[a] > r.revenue[b] : a < b;
+  });
+  std::printf("\nTPC-H Q5 Results:\n");
+  std::printf("+----------------+---------------------+\n");
+  std::printf("| n_name         |             revenue |\n");
+  std::printf("+----------------+---------------------+\n");
+  for (int n : order) std::printf("| %-14s | $%18s |\n", nations[n], fixed(r.revenue[n], 4).c_str());
+  std::printf("+----------------+---------------------+\n");
+  std::printf("\nQ5 | %" PRIu64 " rows (lineitem)\n", L.li.n_rows);
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 

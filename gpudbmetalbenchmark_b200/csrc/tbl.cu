@@ -47,7 +47,7 @@ bool spec_for(int32_t table, TblSpec* s) {
        {F_I32, F_I32, F_I32, F_QTY, F_DEC64, F_DEC32, F_DEC32, F_RETFLAG, F_LINESTATUS, F_DATE, F_DATE, F_DATE,
         F_SHIPMODE}},
       {GPUDB_TBL_ORDERS, 5, {0, 1, 4, 5, 8}, {F_I32, F_I32, F_DATE, F_PRIORITY, F_COMMENT}},
-      {GPUDB_TBL_CUSTOMER, 2, {0, 6}, {F_I32, F_SEGMENT}},
+      {GPUDB_TBL_CUSTOMER, 3, {0, 3, 6}, {F_I32, F_U8, F_SEGMENT}},
       {GPUDB_TBL_PART, 2, {0, 1}, {F_I32, F_GREEN}},
       {GPUDB_TBL_SUPPLIER, 2, {0, 3}, {F_I32, F_U8}},
       {GPUDB_TBL_PARTSUPP, 3, {0, 1, 3}, {F_I32, F_I32, F_DEC64}},

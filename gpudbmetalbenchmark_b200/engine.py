@@ -28,7 +28,7 @@ Q12_LI_COLS = ("order_key", "ship_date", "commit_date", "receipt_date", "ship_mo
 Q1_COLS = ("ship_date", "quantity", "ext_price", "discount", "tax", "flag", "status")
 Q6_COLS = ("ship_date", "discount", "quantity", "ext_price")
 TABLE_COLS = {
-    "customer": {"cust_key": COL["CU_CUST_KEY"], "segment": COL["CU_SEGMENT"]},
+    "customer": {"cust_key": COL["CU_CUST_KEY"], "segment": COL["CU_SEGMENT"], "nation": COL["CU_NATION"]},
     "orders": {"order_key": COL["OR_ORDER_KEY"], "cust_key": COL["OR_CUST_KEY"], "order_date": COL["OR_ORDER_DATE"],
                "priority": COL["OR_PRIORITY"], "comment": COL["OR_COMMENT"]},
     "part": {"part_key": COL["PA_PART_KEY"], "flag": COL["PA_FLAG"]},
@@ -330,6 +330,18 @@ class Engine:
                                                 C.byref(timing) if timing is not None else None,
                                                 self._exec(async_, None)))
         return r if async_ else [(r.high[0], r.low[0]), (r.high[1], r.low[1])]
+
+    def q5(self, cu, su, od, li, date_lo=731, date_hi=1096, region="ASIA", timing=None):
+        """[(nation, revenue)] for the nations of `region` with revenue, ordered by revenue desc
+        (then nation asc): lineitems of orders in [date_lo, date_hi) (default 1994) whose
+        customer and supplier share the nation; revenue in hundredths^2."""
+        p = capi.Q5Params(date_lo, date_hi, capi.region_mask(region), 0)
+        r = capi.Q5Result()
+        ls = li if isinstance(li, capi.Lineitem) else li.lineitem()
+        self._check(self.lib.gpudb_q5_local_supplier(self.ctx, C.byref(cu.struct()), C.byref(su.struct()),
+                                                     C.byref(od.struct()), C.byref(ls), C.byref(p), C.byref(r),
+                                                     C.byref(timing) if timing is not None else None, None))
+        return sorted(((n, r.revenue[n]) for n in range(capi.NATIONS) if r.revenue[n]), key=lambda x: (-x[1], x[0]))
 
     def q10(self, cu, od, li, date_lo=639, date_hi=731, k=20, timing=None):
         """([(cust_key, revenue)] top k by revenue desc, key asc; customers with revenue > 0):

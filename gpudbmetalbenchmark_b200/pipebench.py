@@ -236,6 +236,19 @@ def main(argv=None):
             emit("q12_shipmode", label, n_li, ms, n_li * 17 + n_or * 5, {"kernels": t.kernels})
             eng.free(li)
             eng.free(od)
+    if on("q5"):
+        for n_cu, n_su, n_or, n_li, label in ((150_000, 10_000, 1_500_000, 6_000_000, "SF-1 sizes"),
+                                              (1_500_000, 100_000, 15_000_000, 60_000_000, "SF-10 sizes")):
+            cu = eng.generate("customer", n_cu, seed=42, columns=("cust_key", "nation"))
+            su = eng.generate("supplier", n_su, seed=42)
+            od = eng.generate("orders", n_or, seed=42, columns=("order_key", "cust_key", "order_date"), n_cust=n_cu)
+            li = eng.generate("lineitem", n_li, seed=42, columns=("order_key", "supp_key", "ext_price", "discount"),
+                              n_orders=n_or, n_parts=20 * n_su, n_supp=n_su, order_mode=capi.ORDERS_CLUSTERED)
+            ms, t = timed(lambda tm: eng.q5(cu, su, od, li, timing=tm), a.reps)
+            emit("q5_local_supplier", label, n_li, ms, n_li * 8 + n_or * 12 + n_cu * 5 + n_su * 5,
+                 {"kernels": t.kernels})
+            for x in (li, od, su, cu):
+                eng.free(x)
     if on("q10"):
         for n_cu, n_or, n_li, label in ((150_000, 1_500_000, 6_000_000, "SF-1 sizes"),
                                         (1_500_000, 15_000_000, 60_000_000, "SF-10 sizes")):

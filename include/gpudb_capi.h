@@ -144,6 +144,7 @@ enum { GPUDB_MODE_AIR = 0, GPUDB_MODE_FOB, GPUDB_MODE_MAIL, GPUDB_MODE_RAIL, GPU
 typedef struct gpudb_customer {
   uint64_t n_rows; int32_t key_max; int32_t reserved;
   const int32_t* cust_key; const uint8_t* segment;
+  const uint8_t* nation;       /* c_nationkey 0..24 (Q5) */
 } gpudb_customer;
 
 typedef struct gpudb_orders {
@@ -175,7 +176,7 @@ enum gpudb_column_id {
   GPUDB_COL_LI_DISCOUNT, GPUDB_COL_LI_TAX, GPUDB_COL_LI_FLAG, GPUDB_COL_LI_STATUS,
   GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_PART_KEY, GPUDB_COL_LI_SUPP_KEY,
   GPUDB_COL_LI_COMMIT_DATE, GPUDB_COL_LI_RECEIPT_DATE, GPUDB_COL_LI_SHIP_MODE,
-  GPUDB_COL_CU_CUST_KEY = 20, GPUDB_COL_CU_SEGMENT,
+  GPUDB_COL_CU_CUST_KEY = 20, GPUDB_COL_CU_SEGMENT, GPUDB_COL_CU_NATION,
   GPUDB_COL_OR_ORDER_KEY = 30, GPUDB_COL_OR_CUST_KEY, GPUDB_COL_OR_ORDER_DATE, GPUDB_COL_OR_PRIORITY,
   GPUDB_COL_OR_COMMENT,        /* GPUDB_COMMENT_WIDTH bytes per row */
   GPUDB_COL_PA_PART_KEY = 40, GPUDB_COL_PA_FLAG,
@@ -325,6 +326,21 @@ typedef struct gpudb_q12_result { uint64_t high[2]; uint64_t low[2]; } gpudb_q12
 int gpudb_q12_shipmode(gpudb_ctx* ctx, const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q12_params* p,
                        gpudb_q12_result* out, gpudb_timing* t, const gpudb_exec* ex);
 
+/* ---- Q5 local supplier volume (replaces runQ5Benchmark src/q5.cpp:8-200 with its kernels
+ *      q5_build_customer_nation_map_kernel / q5_build_supplier_nation_map_kernel /
+ *      q5_build_orders_map_kernel / q5_probe_and_aggregate_kernel kernels/q5.metal:19-125) -------
+ * revenue[n] = sum of ext_price * (100 - discount) (hundredths^2) over lineitem rows whose order
+ * has date_lo <= order_date < date_hi, whose customer and supplier are both of nation n, and n
+ * is in nation_mask (bit n: the nations of the region, e.g. ASIA = 8, 9, 12, 18, 21). Customer,
+ * supplier and order keys outside their tables' 0..key_max fail with GPUDB_E_KEY_RANGE;
+ * lineitem keys outside them match nothing. Lineitem may be host-resident (streamed). */
+#define GPUDB_NATIONS 25
+typedef struct gpudb_q5_params { int32_t date_lo; int32_t date_hi; uint32_t nation_mask; int32_t reserved; } gpudb_q5_params;
+typedef struct gpudb_q5_result { int64_t revenue[GPUDB_NATIONS]; } gpudb_q5_result;
+int gpudb_q5_local_supplier(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_supplier* su, const gpudb_orders* od,
+                            const gpudb_lineitem* li, const gpudb_q5_params* p, gpudb_q5_result* out,
+                            gpudb_timing* t, const gpudb_exec* ex);
+
 /* ---- Q10 returned item reporting (replaces runQ10Benchmark src/q10.cpp:8-140 with its kernels
  *      q10_build_orders_map_kernel / q10_probe_and_aggregate_kernel kernels/q10.metal:8-54 and
  *      its host top-20 heap src/q10.cpp:102-121) ------------------------------------------------
@@ -454,7 +470,7 @@ int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timin
  *                                                     fields 0,1,2,4,5,6,7,8,9,10,11,12,14
  *   ORDERS:   order_key, cust_key, order_date, priority (u8), comment (GPUDB_COMMENT_WIDTH
  *             bytes per row: at most 79 characters, NUL-padded)    fields 0,1,4,5,8
- *   CUSTOMER: cust_key, segment (u8)                               fields 0,6
+ *   CUSTOMER: cust_key, nation (u8), segment (u8)                  fields 0,3,6
  *   PART:     part_key, flag (u8)                                  fields 0,1
  *   SUPPLIER: supp_key, nation (u8)                                fields 0,3
  *   PARTSUPP: part_key, supp_key, supply_cost (int64)              fields 0,1,3

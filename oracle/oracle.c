@@ -37,7 +37,7 @@ static int64_t unif(uint64_t key, uint64_t row, int64_t lo, int64_t hi) {
 /* random stream ids (table*16 + column) */
 enum { S_SHIP = 16, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG, S_STATUS, S_OPICK, S_PART, S_SSLOT, S_RUN,
        S_COMMIT, S_RECEIPT, S_MODE,
-       S_SEG = 32, S_OCUST = 48, S_ODATE, S_OPRIO, S_OCOMMENT, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
+       S_SEG = 32, S_CNATION, S_OCUST = 48, S_ODATE, S_OPRIO, S_OCOMMENT, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
 
 /* order comment: n = U[2,9] words (sub-draw r*16), word i = U[0,23] (sub-draw r*16+1+i) of the
  * vocabulary below, joined by single spaces, stopping at the first word that would pass 79
@@ -112,6 +112,7 @@ int or_gen_column(const or_spec* sp, int32_t column, void* dst) {
     for (i = 0; i < n; i++) i32[i] = (column == 30) ? (int32_t)(4 * (off + i) + 1) : (int32_t)(off + i);
     return 0;
   case 21: { uint64_t k = stream_of(seed, S_SEG); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 4); return 0; }
+  case 22: { uint64_t k = stream_of(seed, S_CNATION); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 24); return 0; }
   case 31: { if (sp->n_cust <= 0) return -1; uint64_t k = stream_of(seed, S_OCUST);
              for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, sp->n_cust - 1); return 0; }
   case 32: { uint64_t k = stream_of(seed, S_ODATE); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, 2405); return 0; }
@@ -415,6 +416,38 @@ void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t 
     out4[(h ? 0 : 2) + m]++;
   }
   free(high);
+}
+
+/* ---- Q5: kernels/q5.metal:19-125 (customer and supplier nation maps of the region, the
+ * window's orders -> customer nation, lineitem rows whose supplier nation equals it) ---- */
+void or_q5(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32_t cu_key_max, uint64_t n_su,
+           const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max, uint64_t n_or, const int32_t* o_key,
+           const int32_t* o_cust, const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key,
+           const int32_t* l_supp, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
+           uint32_t nation_mask, int64_t* revenue25) {
+  uint64_t i;
+  for (int n = 0; n < 25; n++) revenue25[n] = 0;
+  if (cu_key_max < 0 || su_key_max < 0 || or_key_max < 0) return;
+  uint8_t* cn = (uint8_t*)malloc((size_t)cu_key_max + 1);
+  uint8_t* sn = (uint8_t*)malloc((size_t)su_key_max + 1);
+  uint8_t* on = (uint8_t*)malloc((size_t)or_key_max + 1);
+  memset(cn, 0xFF, (size_t)cu_key_max + 1);
+  memset(sn, 0xFF, (size_t)su_key_max + 1);
+  memset(on, 0xFF, (size_t)or_key_max + 1);
+  for (i = 0; i < n_cu; i++) if (cu_nation[i] < 25 && (nation_mask >> cu_nation[i] & 1)) cn[cu_key[i]] = cu_nation[i];
+  for (i = 0; i < n_su; i++) if (su_nation[i] < 25 && (nation_mask >> su_nation[i] & 1)) sn[su_key[i]] = su_nation[i];
+  for (i = 0; i < n_or; i++) {
+    if (o_date[i] < date_lo || o_date[i] >= date_hi) continue;
+    if (o_cust[i] < 0 || o_cust[i] > cu_key_max) continue;
+    on[o_key[i]] = cn[o_cust[i]];
+  }
+  for (i = 0; i < n_li; i++) {
+    if (l_key[i] < 0 || l_key[i] > or_key_max || l_supp[i] < 0 || l_supp[i] > su_key_max) continue;
+    const uint8_t n = on[l_key[i]];
+    if (n == 0xFF || sn[l_supp[i]] != n) continue;
+    revenue25[n] += l_ext[i] * (int64_t)(100 - l_disc[i]);
+  }
+  free(cn); free(sn); free(on);
 }
 
 /* ---- Q10: kernels/q10.metal:8-54 (window map, returned rows), src/q10.cpp:102-121 (top-k) ---- */

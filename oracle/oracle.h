@@ -82,6 +82,14 @@ void or_q12(uint64_t n_or, const int32_t* o_key, const uint8_t* o_prio, int32_t 
             const uint8_t* l_mode, int32_t receipt_lo, int32_t receipt_hi, int32_t mode0, int32_t mode1,
             int32_t high_max, uint64_t* out4);
 
+/* Q5: revenue25[n] = exact sum of ext*(100-disc) over lineitem rows whose order is in
+ * [date_lo, date_hi) and whose customer and supplier are both of nation n, n in nation_mask
+ * (kernels/q5.metal:19-125). */
+void or_q5(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32_t cu_key_max, uint64_t n_su,
+           const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max, uint64_t n_or, const int32_t* o_key,
+           const int32_t* o_cust, const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key,
+           const int32_t* l_supp, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
+           uint32_t nation_mask, int64_t* revenue25);
 /* Q10: exact revenue sum ext*(100-disc) of returned lineitems (flag 2) per customer of cu, over
  * orders with date_lo <= date < date_hi (kernels/q10.metal:8-54); the top k by revenue desc,
  * cust_key asc among customers with revenue > 0 (src/q10.cpp:102-121). rev_out (cu_key_max+1

@@ -1,5 +1,5 @@
 // ref_harness.cpp -- runs the reference's own Metal kernels (kernels/q1.metal, q3.metal,
-// q4.metal, q6.metal, q9.metal, q10.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
+// q4.metal, q5.metal, q6.metal, q9.metal, q10.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
 // through the CPU shim in oracle/refshim) on the synthetic tables. TEST INFRASTRUCTURE
 // ONLY: it pins the oracle's query logic to the reference's code, and it is the timed
 // reference arm of bench.py. It is never linked into the engine.
@@ -22,6 +22,7 @@ using namespace metal;
 #include "q13.metal"
 #include "q3.metal"
 #include "q4.metal"
+#include "q5.metal"
 #include "q6.metal"
 #include "q9.metal"
 
@@ -242,6 +243,38 @@ void ref_q12(uint64_t n_or, const int32_t* or_key, const uint8_t* or_prio, uint6
   });
   uint ng = (uint)groups;
   q12_final_count_stage2(partial.data(), out4, ng, 0);
+}
+
+// Q5 through q5_build_customer_nation_map_kernel, q5_build_supplier_nation_map_kernel,
+// q5_build_orders_map_kernel and q5_probe_and_aggregate_kernel (kernels/q5.metal:19-125),
+// with the host's -1-filled direct maps (src/q5.cpp) and the region's nation bitmap.
+void ref_q5(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, uint64_t n_su, const int32_t* su_key,
+            const uint8_t* su_nation, uint64_t n_or, const int32_t* or_key, const int32_t* or_cust,
+            const int32_t* or_date, uint64_t n_li, const int32_t* li_key, const int32_t* li_supp,
+            const int64_t* li_ext, const int32_t* li_disc, int32_t date_lo, int32_t date_hi, uint32_t nation_mask,
+            int groups, int threads, float* revenue25) {
+  int max_c = 0, max_s = 0, max_o = 0;
+  for (uint64_t i = 0; i < n_cu; i++) max_c = std::max(max_c, cu_key[i]);
+  for (uint64_t i = 0; i < n_su; i++) max_s = std::max(max_s, su_key[i]);
+  for (uint64_t i = 0; i < n_or; i++) max_o = std::max(max_o, or_key[i]);
+  for (uint64_t i = 0; i < n_li; i++) max_o = std::max(max_o, li_key[i]);
+  std::vector<int> cmap((size_t)max_c + 1, -1), smap((size_t)max_s + 1, -1), omap((size_t)max_o + 1, -1);
+  std::vector<int> cn(cu_nation, cu_nation + n_cu), sn(su_nation, su_nation + n_su);
+  uint ncu = (uint)n_cu, nsu = (uint)n_su, nor = (uint)n_or, nli = (uint)n_li, map_size = (uint)max_o + 1;
+  for (uint i = 0; i < ncu; i++) q5_build_customer_nation_map_kernel(cu_key, cn.data(), cmap.data(), &nation_mask, ncu, i);
+  for (uint i = 0; i < nsu; i++) q5_build_supplier_nation_map_kernel(su_key, sn.data(), smap.data(), &nation_mask, nsu, i);
+  std::vector<int> od = dates(n_or, or_date);
+  int ds = yyyymmdd(date_lo), de = yyyymmdd(date_hi);
+  for (uint i = 0; i < nor; i++)
+    q5_build_orders_map_kernel(or_key, or_cust, od.data(), omap.data(), nor, ds, de, map_size, cmap.data(), i);
+  std::vector<float> ext = hundredths(n_li, li_ext), dsc = hundredths(n_li, li_disc);
+  std::vector<atomic_float> rev(25);
+  for (auto& r : rev) r.v = 0.0f;
+  run_groups((uint)groups, threads, [&](uint g) {
+    q5_probe_and_aggregate_kernel(li_key, li_supp, ext.data(), dsc.data(), omap.data(), smap.data(), rev.data(), nli,
+                                  map_size, g, 0, 1, (uint)groups);
+  });
+  for (int n = 0; n < 25; n++) revenue25[n] = rev[n].v;
 }
 
 // Q10 through q10_build_orders_map_kernel and q10_probe_and_aggregate_kernel

@@ -78,6 +78,8 @@ def column(name, n, seed, off=0, n_orders=0, n_cust=0, n_parts=0, n_supp=0, mode
                 text = nxt
             out.append(text)
         return out
+    if name == "c_nation":
+        return [uniform(k(33), r, 0, 24) for r in rows]
     if name == "segment":
         return [uniform(k(32), r, 0, 4) for r in rows]
     if name == "o_cust":
@@ -197,6 +199,21 @@ def q13(n_cu, n_or, seed, w1="special", w2="requests"):
     return sorted(([c, d] for c, d in hist.items()), key=lambda x: (-x[1], -x[0]))
 
 
+def q5(n_cu, n_su, n_or, n_li, seed, date_lo=731, date_hi=1096, nations=(8, 9, 12, 18, 21)):
+    cnat = column("c_nation", n_cu, seed)
+    snat = column("nation", n_su, seed)
+    ocust = column("o_cust", n_or, seed, n_cust=n_cu)
+    odate = column("o_date", n_or, seed)
+    onat = {4 * i + 1: cnat[ocust[i]] for i in range(n_or) if date_lo <= odate[i] < date_hi and cnat[ocust[i]] in nations}
+    li = {c: column(c, n_li, seed, n_orders=n_or, n_parts=n_su * 20, n_supp=n_su, mode=1)
+          for c in ("order_key", "supp_key", "ext_price", "discount")}
+    rev = {}
+    for key, sk, e, d in zip(li["order_key"], li["supp_key"], li["ext_price"], li["discount"]):
+        if key in onat and snat[sk] == onat[key]:
+            rev[onat[key]] = rev.get(onat[key], 0) + e * (100 - d)
+    return [[n, str(r)] for n, r in sorted(rev.items(), key=lambda x: (-x[1], x[0])) if r]
+
+
 def q10(n_cu, n_or, n_li, seed, date_lo=639, date_hi=731, k=20):
     ocust = column("o_cust", n_or, seed, n_cust=n_cu)
     odate = column("o_date", n_or, seed)
@@ -211,7 +228,7 @@ def q10(n_cu, n_or, n_li, seed, date_lo=639, date_hi=731, k=20):
 
 
 def main():
-    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}, "q10": {}}
+    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}, "q10": {}, "q5": {}}
     # generator: first values and column sums for two seeds and a shifted window
     for seed, off in ((42, 0), (7, 1000)):
         cols = {}
@@ -225,7 +242,7 @@ def main():
             cols["order_key_uniform"] = {"head": v2[:8], "sum": sum(v2)}
         v = column("supp_key", 64, seed, off, n_parts=1000, n_supp=100)
         cols["supp_key"] = {"head": v[:8], "sum": sum(v)}
-        for name in ("commit_date", "receipt_date", "ship_mode", "o_priority"):
+        for name in ("commit_date", "receipt_date", "ship_mode", "o_priority", "c_nation"):
             v = column(name, 64, seed, off)
             cols[name] = {"head": v[:8], "sum": sum(v)}
         cols["o_comment"] = {"head": column("o_comment", 4, seed, off)}
@@ -246,6 +263,8 @@ def main():
     out["q12"]["2000_9000_5_air_truck_hi3"] = q12(2000, 9000, 5, 0, 2600, (0, 6), 3)
     out["q13"]["300_3000_42"] = q13(300, 3000, 42)
     out["q10"]["300_3000_12000_42"] = q10(300, 3000, 12000, 42)
+    out["q5"]["300_40_3000_12000_42"] = q5(300, 40, 3000, 12000, 42)
+    out["q5"]["500_60_4000_16000_3_europe_all_years"] = q5(500, 60, 4000, 16000, 3, 0, 2406, (6, 7, 19, 22, 23))
     out["q10"]["200_2000_9000_5_wide"] = q10(200, 2000, 9000, 5, 0, 2406, 7)
     out["q13"]["200_4000_9_pinto_beans"] = q13(200, 4000, 9, "pinto", "beans")
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")

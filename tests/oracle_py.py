@@ -9,7 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgpudbref.so")
 
-WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 11: 4, 12: 4, 13: 1, 20: 4, 21: 1, 30: 4,
+WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 11: 4, 12: 4, 13: 1, 20: 4, 21: 1, 22: 1, 30: 4,
          31: 4, 32: 4, 33: 1, 34: 80, 40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
 DT = {1: np.uint8, 4: np.int32, 8: np.int64, 80: np.dtype("S80")}
 
@@ -36,6 +36,7 @@ ORACLE_ARGS = {
     "or_q4": [U64, V, V, V, I32, U64, V, V, V, I32, I32, V],
     "or_q12": [U64, V, V, I32, U64, V, V, V, V, V, I32, I32, I32, I32, I32, V],
     "or_q13": [U64, V, I32, U64, V, V, C.c_char_p, C.c_char_p, V, V, U32],
+    "or_q5": [U64, V, V, I32, U64, V, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, U32, V],
     "or_q10": [U64, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, I32, V, V, V],
     "or_select_lt": [U64, V, I32, V, V],
     "or_sum_i32": [U64, V],
@@ -53,6 +54,7 @@ REF_ARGS = {
     "ref_q4": [U64, V, V, V, U64, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_q12": [U64, V, V, U64, V, V, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_q13": [U64, U64, V, V, C.c_int, C.c_int, V],
+    "ref_q5": [U64, V, V, U64, V, V, U64, V, V, V, U64, V, V, V, V, I32, I32, U32, C.c_int, C.c_int, V],
     "ref_q10": [U64, V, V, V, U64, V, V, V, V, I32, I32, C.c_int, C.c_int, V, U32],
     "ref_select_lt": [U64, V, I32, V],
     "ref_sum": [U64, V, C.c_int, C.c_int],
@@ -139,6 +141,30 @@ def q4_tables(n_or, n_li, seed=42, order_mode=1):
     li = lineitem(n_li, seed, n_orders=n_or, order_mode=order_mode,
                   cols=("order_key", "ship_date", "commit_date", "receipt_date", "ship_mode"))
     return od, li
+
+
+def q5_tables(n_cu, n_su, n_or, n_li, seed=42):
+    cu = dict(cust_key=gen(20, n_cu, seed), nation=gen(22, n_cu, seed))
+    su = dict(supp_key=gen(50, n_su, seed), nation=gen(51, n_su, seed))
+    od = dict(order_key=gen(30, n_or, seed), cust_key=gen(31, n_or, seed, n_cust=n_cu), order_date=gen(32, n_or, seed))
+    li = lineitem(n_li, seed, n_orders=n_or, order_mode=1, n_parts=max(1, n_su * 20), n_supp=n_su,
+                  cols=("order_key", "supp_key", "ext_price", "discount"))
+    return cu, su, od, li
+
+
+ASIA = (1 << 8) | (1 << 9) | (1 << 12) | (1 << 18) | (1 << 21)
+
+
+def q5(cu, su, od, li, date_lo=731, date_hi=1096, mask=ASIA, revenue_out=None):
+    """[(nation, revenue)] nonzero, ordered by revenue desc then nation asc."""
+    rev = np.zeros(25, np.int64) if revenue_out is None else revenue_out
+    kmax = lambda a: int(a.max()) if len(a) else -1  # noqa: E731
+    oracle().or_q5(len(cu["cust_key"]), _p(cu["cust_key"]), _p(cu["nation"]), kmax(cu["cust_key"]),
+                   len(su["supp_key"]), _p(su["supp_key"]), _p(su["nation"]), kmax(su["supp_key"]),
+                   len(od["order_key"]), _p(od["order_key"]), _p(od["cust_key"]), _p(od["order_date"]),
+                   kmax(od["order_key"]), len(li["order_key"]), _p(li["order_key"]), _p(li["supp_key"]),
+                   _p(li["ext_price"]), _p(li["discount"]), date_lo, date_hi, mask, rev.ctypes.data)
+    return sorted(((n, int(rev[n])) for n in range(25) if rev[n]), key=lambda x: (-x[1], x[0]))
 
 
 def q10_tables(n_cu, n_or, n_li, seed=42):
@@ -351,8 +377,9 @@ def format_tbl(kind, c):
                                                                   prio, i, note))
     elif kind == "customer":
         for i in range(len(c["cust_key"])):
+            nation = int(c["nation"][i]) if "nation" in c else i % 25
             out.append("%d|Customer#%09d|addr %d|%d|10-123-456-7890|%s|%s|a customer|"
-                       % (c["cust_key"][i], c["cust_key"][i], i, i % 25, _money(100 * i - 5000), _SEGMENTS[c["segment"][i]]))
+                       % (c["cust_key"][i], c["cust_key"][i], i, nation, _money(100 * i - 5000), _SEGMENTS[c["segment"][i]]))
     elif kind == "part":
         for i in range(len(c["part_key"])):
             name = "forest green lace" if c["flag"][i] else "steel ivory lace"
@@ -380,7 +407,7 @@ def parse_tbl_cpu(kind, text):
                          (12, "receipt_date", "d"), (14, "ship_mode", "e")],
             "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d"), (5, "priority", "p"),
                        (8, "comment", "c")],
-            "customer": [(0, "cust_key", "i"), (6, "segment", "g")],
+            "customer": [(0, "cust_key", "i"), (3, "nation", "i"), (6, "segment", "g")],
             "part": [(0, "part_key", "i"), (1, "flag", "n")],
             "supplier": [(0, "supp_key", "i"), (3, "nation", "i")],
             "partsupp": [(0, "part_key", "i"), (1, "supp_key", "i"), (3, "supply_cost", "m")]}[kind]

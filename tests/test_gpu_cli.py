@@ -8,6 +8,8 @@ from decimal import Decimal
 
 import pytest
 
+from gpudbmetalbenchmark_b200 import capi
+
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -108,6 +110,15 @@ def test_cli_q13(orc):
     assert re.search(r"^Q13 \| 15000 orders \| 1500 customers", out, re.M)
 
 
+def test_cli_q5(orc):
+    cu, su, od, li = orc.q5_tables(1_500, 100, 15_000, 60_000, 42)
+    out = run("sf1", "q5", "--scale", "0.01")
+    names = capi.NATION_NAMES
+    rows = re.findall(r"^\| ([A-Z ]+?)\s+\| \$\s*(\S+) \|$", out, re.M)
+    assert [(names.index(n), scaled(r, 4)) for n, r in rows] == orc.q5(cu, su, od, li)
+    assert re.search(r"^Q5 \| 60000 rows \(lineitem\)", out, re.M)
+
+
 def test_cli_q10(orc):
     cu, od, li = orc.q10_tables(1_500, 15_000, 60_000, 42)
     top, n = orc.q10(cu, od, li)
@@ -154,7 +165,7 @@ def test_cli_reads_tbl_files(orc, tmp_path):
                             "status", "ship_date", "commit_date", "receipt_date", "ship_mode"))
     od = dict(order_key=orc.gen(30, n_or, 7), cust_key=orc.gen(31, n_or, 7, n_cust=n_cu), order_date=orc.gen(32, n_or, 7),
               priority=orc.gen(33, n_or, 7), comment=orc.gen(34, n_or, 7))
-    cu = dict(cust_key=orc.gen(20, n_cu, 7), segment=orc.gen(21, n_cu, 7))
+    cu = dict(cust_key=orc.gen(20, n_cu, 7), segment=orc.gen(21, n_cu, 7), nation=orc.gen(22, n_cu, 7))
     pa = dict(part_key=orc.gen(40, n_pa, 7), flag=orc.gen(41, n_pa, 7))
     su = dict(supp_key=orc.gen(50, n_su, 7), nation=orc.gen(51, n_su, 7))
     ps = dict(part_key=orc.gen(60, 4 * n_pa, 7), supp_key=orc.gen(61, 4 * n_pa, 7, n_supp=n_su),
@@ -189,6 +200,13 @@ def test_cli_reads_tbl_files(orc, tmp_path):
     assert q4_rows(out) == orc.q4(od, li)
     out = run("q12", "--data", d)
     assert q12_rows(out) == orc.q12(od, li)
+    out = run("q5", "--data", d)
+    names = capi.NATION_NAMES
+    rows5 = re.findall(r"^\| ([A-Z ]+?)\s+\| \$\s*(\S+) \|$", out, re.M)
+    assert [(names.index(n), scaled(r, 4)) for n, r in rows5] == orc.q5(cu, su, od, li)
+    out = run("q10", "--data", d)
+    top10, n10 = orc.q10(cu, od, li)
+    assert int(re.search(r"Customers with returned revenue: (\d+)", out).group(1)) == n10
     out = run("q13", "--data", d)
     assert q13_rows(out) == orc.q13(cu, od)
     out = run("aggregation", "--data", d)

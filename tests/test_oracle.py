@@ -36,7 +36,8 @@ def test_generator_matches_golden(orc):
         sk = orc.gen(10, 64, seed, off, n_parts=1000, n_supp=100)
         assert sk[:8].tolist() == cols["supp_key"]["head"]
         assert [x.decode() for x in orc.gen(34, 4, seed, off)] == cols["o_comment"]["head"], key
-        for name, cid in (("commit_date", 11), ("receipt_date", 12), ("ship_mode", 13), ("o_priority", 33)):
+        for name, cid in (("commit_date", 11), ("receipt_date", 12), ("ship_mode", 13), ("o_priority", 33),
+                          ("c_nation", 22)):
             v = orc.gen(cid, 64, seed, off)
             assert v[:8].tolist() == cols[name]["head"], (key, name)
             assert int(v.astype(np.int64).sum()) == cols[name]["sum"], (key, name)
@@ -91,6 +92,37 @@ def test_q13_matches_golden(orc):
     assert orc.q13(cu, od) == [tuple(x) for x in GOLDEN["q13"]["300_3000_42"]]
     cu, od = orc.q13_tables(200, 4000, 9)
     assert orc.q13(cu, od, b"pinto", b"beans") == [tuple(x) for x in GOLDEN["q13"]["200_4000_9_pinto_beans"]]
+
+
+EUROPE = (1 << 6) | (1 << 7) | (1 << 19) | (1 << 22) | (1 << 23)
+
+
+def test_q5_matches_golden(orc):
+    cu, su, od, li = orc.q5_tables(300, 40, 3000, 12000, 42)
+    assert orc.q5(cu, su, od, li) == [(n, int(r)) for n, r in GOLDEN["q5"]["300_40_3000_12000_42"]]
+    cu, su, od, li = orc.q5_tables(500, 60, 4000, 16000, 3)
+    assert orc.q5(cu, su, od, li, 0, 2406, EUROPE) == \
+        [(n, int(r)) for n, r in GOLDEN["q5"]["500_60_4000_16000_3_europe_all_years"]]
+
+
+@pytest.mark.parametrize("sizes,seed,window,mask", [((300, 40, 3000, 12000), 42, (731, 1096), None),
+                                                    ((3000, 200, 30000, 120000), 7, (0, 2406), EUROPE)])
+def test_q5_pinned_to_reference_kernels(orc, sizes, seed, window, mask):
+    """Q5 revenue per nation against the reference's kernels (float32 there: within its
+    tolerance; which nations have revenue, exactly)."""
+    ref = need_ref(orc)
+    cu, su, od, li = orc.q5_tables(*sizes, seed)
+    mask = orc.ASIA if mask is None else mask
+    mine = np.zeros(25, np.int64)
+    orc.q5(cu, su, od, li, *window, mask, revenue_out=mine)
+    theirs = np.zeros(25, np.float32)
+    ref.ref_q5(len(cu["cust_key"]), cu["cust_key"].ctypes.data, cu["nation"].ctypes.data, len(su["supp_key"]),
+               su["supp_key"].ctypes.data, su["nation"].ctypes.data, len(od["order_key"]), od["order_key"].ctypes.data,
+               od["cust_key"].ctypes.data, od["order_date"].ctypes.data, len(li["order_key"]),
+               li["order_key"].ctypes.data, li["supp_key"].ctypes.data, li["ext_price"].ctypes.data,
+               li["discount"].ctypes.data, *window, mask, 8, 4, theirs.ctypes.data)
+    assert np.array_equal(mine > 0, theirs > 0)
+    np.testing.assert_allclose(theirs, mine / 10000.0, rtol=1e-4)
 
 
 def test_q10_matches_golden(orc):
