@@ -34,7 +34,7 @@ TBL_COLUMNS = {
                                 "flag", "status", "ship_date", "commit_date", "receipt_date", "ship_mode")),
     "orders": (TBL_ORDERS, ("order_key", "cust_key", "order_date", "priority", "comment")),
     "customer": (TBL_CUSTOMER, ("cust_key", "nation", "segment")),
-    "part": (TBL_PART, ("part_key", "flag")),
+    "part": (TBL_PART, ("part_key", "flag", "type")),
     "supplier": (TBL_SUPPLIER, ("supp_key", "nation")),
     "partsupp": (TBL_PARTSUPP, ("part_key", "supp_key", "supply_cost")),
 }
@@ -56,7 +56,7 @@ COL = dict(
     LI_ORDER_KEY=8, LI_PART_KEY=9, LI_SUPP_KEY=10, LI_COMMIT_DATE=11, LI_RECEIPT_DATE=12, LI_SHIP_MODE=13,
     CU_CUST_KEY=20, CU_SEGMENT=21, CU_NATION=22,
     OR_ORDER_KEY=30, OR_CUST_KEY=31, OR_ORDER_DATE=32, OR_PRIORITY=33, OR_COMMENT=34,
-    PA_PART_KEY=40, PA_FLAG=41,
+    PA_PART_KEY=40, PA_FLAG=41, PA_TYPE=42,
     SU_SUPP_KEY=50, SU_NATION=51,
     PS_PART_KEY=60, PS_SUPP_KEY=61, PS_SUPPLY_COST=62,
 )
@@ -99,7 +99,7 @@ class Orders(C.Structure):
 
 class Part(C.Structure):
     _fields_ = [("n_rows", C.c_uint64), ("key_max", C.c_int32), ("reserved", C.c_int32),
-                ("part_key", vp), ("flag", vp)]
+                ("part_key", vp), ("flag", vp), ("type", vp)]
 
 
 class Supplier(C.Structure):
@@ -155,6 +155,36 @@ class Q5Params(C.Structure):
 
 class Q5Result(C.Structure):
     _fields_ = [("revenue", C.c_int64 * NATIONS)]
+
+
+MAX_YEARS = 8
+PART_TYPE_WORDS = (("STANDARD", "SMALL", "MEDIUM", "LARGE", "ECONOMY", "PROMO"),
+                   ("ANODIZED", "BURNISHED", "PLATED", "POLISHED", "BRUSHED"),
+                   ("TIN", "NICKEL", "BRASS", "STEEL", "COPPER"))
+
+
+def part_type(name):
+    """p_type code of a type such as "ECONOMY ANODIZED STEEL" (103)."""
+    a, b, c = name.split()
+    return PART_TYPE_WORDS[0].index(a) * 25 + PART_TYPE_WORDS[1].index(b) * 5 + PART_TYPE_WORDS[2].index(c)
+
+
+class Q7Params(C.Structure):
+    _fields_ = [("nation_a", C.c_int32), ("nation_b", C.c_int32), ("ship_lo", C.c_int32), ("ship_hi", C.c_int32)]
+
+
+class Q7Result(C.Structure):
+    _fields_ = [("first_year", C.c_int32), ("n_years", C.c_int32), ("revenue", (C.c_int64 * MAX_YEARS) * 2)]
+
+
+class Q8Params(C.Structure):
+    _fields_ = [("date_lo", C.c_int32), ("date_hi", C.c_int32), ("region_mask", C.c_uint32), ("nation", C.c_int32),
+                ("part_type", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Q8Result(C.Structure):
+    _fields_ = [("first_year", C.c_int32), ("n_years", C.c_int32), ("volume", C.c_int64 * MAX_YEARS),
+                ("nation_volume", C.c_int64 * MAX_YEARS)]
 
 
 class Q10Params(C.Structure):
@@ -285,6 +315,10 @@ PROTOTYPES = {
                                      P(Exec)]),
     "gpudb_q5_local_supplier": (C.c_int, [ctx_p, P(Customer), P(Supplier), P(Orders), P(Lineitem), P(Q5Params),
                                           P(Q5Result), P(Timing), P(Exec)]),
+    "gpudb_q7_volume_shipping": (C.c_int, [ctx_p, P(Customer), P(Supplier), P(Orders), P(Lineitem), P(Q7Params),
+                                           P(Q7Result), P(Timing), P(Exec)]),
+    "gpudb_q8_market_share": (C.c_int, [ctx_p, P(Customer), P(Supplier), P(Part), P(Orders), P(Lineitem),
+                                        P(Q8Params), P(Q8Result), P(Timing), P(Exec)]),
     "gpudb_q10_returned": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Lineitem), P(Q10Params), P(Q10Result),
                                      P(Timing), P(Exec)]),
     "gpudb_q13_distribution": (C.c_int, [ctx_p, P(Customer), P(Orders), P(Q13Params), P(Q13Row), C.c_uint32,

@@ -48,6 +48,7 @@ __host__ __device__ __forceinline__ void gen_value(const GenArgs& a, uint64_t r,
     case GPUDB_COL_OR_COMMENT: gd_or_comment(a.seed, r, reinterpret_cast<char*>(u8) + i * GD_COMMENT_WIDTH); break;
     case GPUDB_COL_PA_PART_KEY: i32[i] = (int32_t)r; break;
     case GPUDB_COL_PA_FLAG: u8[i] = gd_pa_flag(a.seed, r); break;
+    case GPUDB_COL_PA_TYPE: u8[i] = gd_pa_type(a.seed, r); break;
     case GPUDB_COL_SU_SUPP_KEY: i32[i] = (int32_t)r; break;
     case GPUDB_COL_SU_NATION: u8[i] = gd_su_nation(a.seed, r); break;
     case GPUDB_COL_PS_PART_KEY: i32[i] = (int32_t)(r / 4); break;
@@ -88,7 +89,7 @@ int column_width(int32_t c) {
     case GPUDB_COL_LI_EXT_PRICE: case GPUDB_COL_PS_SUPPLY_COST: return 8;
     case GPUDB_COL_LI_FLAG: case GPUDB_COL_LI_STATUS: case GPUDB_COL_CU_SEGMENT:
     case GPUDB_COL_PA_FLAG: case GPUDB_COL_SU_NATION: case GPUDB_COL_LI_SHIP_MODE: case GPUDB_COL_OR_PRIORITY:
-    case GPUDB_COL_CU_NATION:
+    case GPUDB_COL_CU_NATION: case GPUDB_COL_PA_TYPE:
       return 1;
     case GPUDB_COL_LI_COMMIT_DATE: case GPUDB_COL_LI_RECEIPT_DATE: return 4;
     case GPUDB_COL_OR_COMMENT: return GD_COMMENT_WIDTH;

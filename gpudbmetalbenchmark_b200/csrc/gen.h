@@ -40,7 +40,7 @@ enum gd_column {
   GD_LI_COMMIT, GD_LI_RECEIPT, GD_LI_MODE,
   GD_CU_SEGMENT = 32, GD_CU_NATION,
   GD_OR_CUST = 48, GD_OR_DATE, GD_OR_PRIORITY, GD_OR_COMMENT,
-  GD_PA_FLAG = 64,
+  GD_PA_FLAG = 64, GD_PA_TYPE,
   GD_SU_NATION = 80,
   GD_PS_COST = 96
 };
@@ -143,6 +143,7 @@ GD_HD uint8_t gd_cu_nation(uint64_t seed, uint64_t r) { return (uint8_t)gd_unifo
 GD_HD uint8_t gd_cu_segment(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_CU_SEGMENT, r, 0, 4); }
 GD_HD int32_t gd_or_cust(uint64_t seed, uint64_t r, int64_t n_cust) { return (int32_t)gd_uniform(seed, GD_OR_CUST, r, 0, n_cust - 1); }
 GD_HD int32_t gd_or_date(uint64_t seed, uint64_t r) { return (int32_t)gd_uniform(seed, GD_OR_DATE, r, 0, GD_ORDER_DATE_MAX); }
+GD_HD uint8_t gd_pa_type(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_PA_TYPE, r, 0, 149); }
 GD_HD uint8_t gd_pa_flag(uint64_t seed, uint64_t r) { return (uint8_t)(gd_uniform(seed, GD_PA_FLAG, r, 0, 999) < 55); }
 GD_HD uint8_t gd_su_nation(uint64_t seed, uint64_t r) { return (uint8_t)gd_uniform(seed, GD_SU_NATION, r, 0, 24); }
 GD_HD int64_t gd_ps_cost(uint64_t seed, uint64_t r) { return gd_uniform(seed, GD_PS_COST, r, 100, 100000); }

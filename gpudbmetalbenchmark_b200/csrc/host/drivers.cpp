@@ -368,6 +368,133 @@ void runQ5Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
+namespace {
+const char* const kNationNames[GPUDB_NATIONS] = {
+    "ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
+    "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
+    "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES"};
+
+// Customer (key, nation), supplier (key, nation) and orders (key, customer, date): generated,
+// or parsed from the .tbl files (Q7, Q8).
+struct Dims {
+  gpudb_customer cu{};
+  gpudb_supplier su{};
+  gpudb_orders od{};
+  TblTable ct, st, ot;
+  Buffer ck, cn, sk, sn, ok, oc, odt;
+};
+
+void make_dims(gpudb_ctx* ctx, const RunOptions& o, Dims& D) {
+  const Scale& s = o.scale;
+  if (!o.data_dir.empty()) {
+    D.ct = load_tbl(ctx, o.data_dir, "customer", GPUDB_TBL_CUSTOMER, {0, 1}, {4, 1}, o.tbl_piece);
+    D.st = load_tbl(ctx, o.data_dir, "supplier", GPUDB_TBL_SUPPLIER, {0, 1}, {4, 1}, o.tbl_piece);
+    D.ot = load_tbl(ctx, o.data_dir, "orders", GPUDB_TBL_ORDERS, {0, 1, 2}, {4, 4, 4}, o.tbl_piece);
+    D.cu = {D.ct.rows, D.ct.col_max[0], 0, D.ct.col<int32_t>(0), nullptr, D.ct.col<uint8_t>(1)};
+    D.su = {D.st.rows, D.st.col_max[0], 0, D.st.col<int32_t>(0), D.st.col<uint8_t>(1)};
+    D.od = {D.ot.rows, D.ot.col_max[0], D.ot.col_max[1], D.ot.col<int32_t>(0), D.ot.col<int32_t>(1),
+            D.ot.col<int32_t>(2)};
+    return;
+  }
+  gpudb_gen_spec cs{};
+  cs.seed = o.seed;
+  cs.n_rows = s.customer;
+  D.ck = generate(ctx, cs, GPUDB_COL_CU_CUST_KEY, GPUDB_MEM_DEVICE);
+  D.cn = generate(ctx, cs, GPUDB_COL_CU_NATION, GPUDB_MEM_DEVICE);
+  gpudb_gen_spec ss = cs;
+  ss.n_rows = s.supplier;
+  D.sk = generate(ctx, ss, GPUDB_COL_SU_SUPP_KEY, GPUDB_MEM_DEVICE);
+  D.sn = generate(ctx, ss, GPUDB_COL_SU_NATION, GPUDB_MEM_DEVICE);
+  gpudb_gen_spec os = cs;
+  os.n_rows = s.orders;
+  os.n_cust = (int64_t)s.customer;
+  D.ok = generate(ctx, os, GPUDB_COL_OR_ORDER_KEY, GPUDB_MEM_DEVICE);
+  D.oc = generate(ctx, os, GPUDB_COL_OR_CUST_KEY, GPUDB_MEM_DEVICE);
+  D.odt = generate(ctx, os, GPUDB_COL_OR_ORDER_DATE, GPUDB_MEM_DEVICE);
+  D.cu = {s.customer, (int32_t)s.customer - 1, 0, D.ck.as<int32_t>(), nullptr, D.cn.as<uint8_t>()};
+  D.su = {s.supplier, (int32_t)s.supplier - 1, 0, D.sk.as<int32_t>(), D.sn.as<uint8_t>()};
+  D.od = {s.orders, (int32_t)(4 * (s.orders - 1) + 1), (int32_t)s.customer - 1, D.ok.as<int32_t>(),
+          D.oc.as<int32_t>(), D.odt.as<int32_t>()};
+}
+}  // namespace
+
+void runQ7Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 7 Benchmark ---\n");
+  const double t0 = now_ms();
+  Dims D;
+  make_dims(ctx, o, D);
+  Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_SUPP_KEY, GPUDB_COL_LI_SHIP_DATE,
+                                      GPUDB_COL_LI_EXT_PRICE, GPUDB_COL_LI_DISCOUNT}, GPUDB_ORDERS_CLUSTERED,
+                             (int64_t)D.od.n_rows, (int64_t)o.scale.part, (int64_t)D.su.n_rows);
+  const double gen_ms = now_ms() - t0;
+  const gpudb_q7_params p{6, 7, 1096, 1826};   // FRANCE and GERMANY, shipped 1995-01-01 .. 1996-12-31
+  gpudb_q7_result r{};
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q7_volume_shipping(ctx, &D.cu, &D.su, &D.od, &L.li, &p, &r, &t, nullptr), "gpudb_q7");
+  const double p0 = now_ms();
+  std::printf("\nTPC-H Q7 Results:\n");
+  std::printf("+-------------+-------------+--------+---------------------+\n");
+  std::printf("| supp_nation | cust_nation | l_year |             revenue |\n");
+  std::printf("+-------------+-------------+--------+---------------------+\n");
+  const int pairs[2][2] = {{p.nation_a, p.nation_b}, {p.nation_b, p.nation_a}};
+  const int first = std::strcmp(kNationNames[p.nation_a], kNationNames[p.nation_b]) <= 0 ? 0 : 1;
+  for (int q = 0; q < 2; q++) {
+    const int pair = q == 0 ? first : 1 - first;
+    for (int y = 0; y < r.n_years; y++)
+      if (r.revenue[pair][y])
+        std::printf("| %-11s | %-11s | %6d | $%18s |\n", kNationNames[pairs[pair][0]], kNationNames[pairs[pair][1]],
+                    r.first_year + y, fixed(r.revenue[pair][y], 4).c_str());
+  }
+  std::printf("+-------------+-------------+--------+---------------------+\n");
+  header(o, "Q7", L.li.n_rows, t);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
+}
+
+void runQ8Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
+  std::printf("\n--- Running TPC-H Query 8 Benchmark ---\n");
+  const double t0 = now_ms();
+  Dims D;
+  make_dims(ctx, o, D);
+  gpudb_part pa{};
+  TblTable pt;
+  Buffer pk, ptype;
+  if (!o.data_dir.empty()) {
+    pt = load_tbl(ctx, o.data_dir, "part", GPUDB_TBL_PART, {0, 2}, {4, 1}, o.tbl_piece);
+    pa = {pt.rows, pt.col_max[0], 0, pt.col<int32_t>(0), nullptr, pt.col<uint8_t>(2)};
+  } else {
+    gpudb_gen_spec ps{};
+    ps.seed = o.seed;
+    ps.n_rows = o.scale.part;
+    pk = generate(ctx, ps, GPUDB_COL_PA_PART_KEY, GPUDB_MEM_DEVICE);
+    ptype = generate(ctx, ps, GPUDB_COL_PA_TYPE, GPUDB_MEM_DEVICE);
+    pa = {o.scale.part, (int32_t)o.scale.part - 1, 0, pk.as<int32_t>(), nullptr, ptype.as<uint8_t>()};
+  }
+  Lineitem L = make_lineitem(ctx, o, {GPUDB_COL_LI_ORDER_KEY, GPUDB_COL_LI_PART_KEY, GPUDB_COL_LI_SUPP_KEY,
+                                      GPUDB_COL_LI_EXT_PRICE, GPUDB_COL_LI_DISCOUNT}, GPUDB_ORDERS_CLUSTERED,
+                             (int64_t)D.od.n_rows, (int64_t)pa.n_rows, (int64_t)D.su.n_rows);
+  const double gen_ms = now_ms() - t0;
+  // BRAZIL in AMERICA, ECONOMY ANODIZED STEEL, orders of 1995-01-01 .. 1996-12-31
+  const uint32_t america = (1u << 1) | (1u << 2) | (1u << 3) | (1u << 17) | (1u << 24);
+  const gpudb_q8_params p{1096, 1826, america, 2, GPUDB_PART_TYPE(4, 0, 3), 0};
+  gpudb_q8_result r{};
+  gpudb_timing t{};
+  for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q8_market_share(ctx, &D.cu, &D.su, &pa, &D.od, &L.li, &p, &r, &t, nullptr), "gpudb_q8");
+  const double p0 = now_ms();
+  std::printf("\nTPC-H Q8 Results:\n");
+  std::printf("+--------+------------+\n");
+  std::printf("| o_year |  mkt_share |\n");
+  std::printf("+--------+------------+\n");
+  for (int y = 0; y < r.n_years; y++) {
+    const long double share = r.volume[y] ? (long double)r.nation_volume[y] / (long double)r.volume[y] : 0.0L;
+    std::printf("| %6d | %10.6Lf |\n", r.first_year + y, share);
+  }
+  std::printf("+--------+------------+\n");
+  for (int y = 0; y < r.n_years; y++)
+    std::printf("volume %d: %" PRId64 " of %" PRId64 "\n", r.first_year + y, r.nation_volume[y], r.volume[y]);
+  std::printf("\nQ8 | %" PRIu64 " lineitem\n", L.li.n_rows);
+  printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
+}
+
 void runQ10Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("\n--- Running TPC-H Query 10 Benchmark ---\n");
   const Scale& s = o.scale;

@@ -204,6 +204,8 @@ void runQ1Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ3Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ4Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ5Benchmark(gpudb_ctx*, const RunOptions&);
+void runQ7Benchmark(gpudb_ctx*, const RunOptions&);
+void runQ8Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ10Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ12Benchmark(gpudb_ctx*, const RunOptions&);
 void runQ13Benchmark(gpudb_ctx*, const RunOptions&);

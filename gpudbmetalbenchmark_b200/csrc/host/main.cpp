@@ -16,7 +16,7 @@ using namespace gpudb_host;
 
 static void show_help() {
   std::printf("Usage: gpudb [sf1|sf10|sf100] [query] [--scale F] [--seed N] [--reps N] [--device N] [--data DIR]\n");
-  std::printf("Queries: q1 q3 q4 q5 q6 q9 q10 q12 q13 selection aggregation join all (default: all)\n");
+  std::printf("Queries: q1 q3 q4 q5 q6 q7 q8 q9 q10 q12 q13 selection aggregation join all (default: all)\n");
   std::printf("Examples:\n  gpudb            # all pipelines on SF-1\n  gpudb sf10 q1\n  gpudb sf100 q6   # streamed\n"
               "  gpudb q3 --data data/SF-1   # tables from dbgen .tbl files\n");
 }
@@ -44,7 +44,8 @@ int main(int argc, const char* argv[]) {
       {"selection", runSelectionBenchmark}, {"aggregation", runAggregationBenchmark}, {"join", runJoinBenchmark},
       {"q1", runQ1Benchmark},          {"q3", runQ3Benchmark},                {"q4", runQ4Benchmark},
       {"q6", runQ6Benchmark},          {"q9", runQ9Benchmark},                {"q12", runQ12Benchmark},
-      {"q5", runQ5Benchmark},          {"q10", runQ10Benchmark},              {"q13", runQ13Benchmark}};
+      {"q5", runQ5Benchmark},          {"q7", runQ7Benchmark},                {"q8", runQ8Benchmark},
+      {"q10", runQ10Benchmark},        {"q13", runQ13Benchmark}};
   Driver fn = nullptr;
   if (query != "all") {
     for (auto& e : pipelines)

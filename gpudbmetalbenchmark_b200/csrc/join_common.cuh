@@ -132,6 +132,18 @@ __device__ __forceinline__ void warp_bitmap_or(bool on, int32_t key, uint32_t* b
   if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicOr(bitmap + word, bits);
 }
 
+// key -> nation byte for the rows whose nation (0..24) is in `mask`; the map starts at 0xFF
+// (the caller clears it). A key outside 0..key_max sets ST_KEY_RANGE. (Q5, Q7, Q8.)
+static __global__ void nation_map_kernel(const int32_t* __restrict__ key, const uint8_t* __restrict__ nation,
+                                         uint64_t n, int32_t key_max, uint32_t mask, uint8_t* map, uint32_t* status) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int32_t k = ld_stream(key + i);
+    const uint32_t nt = ld_stream(nation + i);
+    if (k < 0 || k > key_max) { set_status(status, ST_KEY_RANGE); continue; }
+    if (nt < 25u && ((mask >> nt) & 1u)) map[k] = (uint8_t)nt;
+  }
+}
+
 // Warp-aggregated append: returns this lane's output position (valid where `take`).
 __device__ __forceinline__ uint32_t warp_append(bool take, uint32_t* counter) {
   const uint32_t m = __ballot_sync(FULL_MASK, take);

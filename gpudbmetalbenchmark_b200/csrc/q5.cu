@@ -6,7 +6,7 @@
 // bitmap of the region on the host, sort by revenue).
 //
 // B200 design:
-//  1. q5_nation_map_kernel (customers, suppliers): key -> nation byte for the nations of the
+//  1. nation_map_kernel (customers, suppliers): key -> nation byte for the nations of the
 //     mask; the maps start at 0xFF (not in the region) and are small (a byte per key).
 //  2. q5_orders_kernel: orders of the window whose customer is in the region set their bit
 //     in an order-key bitmap (one atomicOr per distinct word of a warp) and write the
@@ -28,18 +28,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kRows = 4;
 constexpr uint8_t kNone = 0xFF;
-
-__global__ void __launch_bounds__(kThreads) q5_nation_map_kernel(const int32_t* __restrict__ key,
-                                                                 const uint8_t* __restrict__ nation, uint64_t n,
-                                                                 int32_t key_max, uint32_t mask, uint8_t* map,
-                                                                 uint32_t* status) {
-  for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads) {
-    const int32_t k = ld_stream(key + i);
-    const uint32_t nt = ld_stream(nation + i);
-    if (k < 0 || k > key_max) { set_status(status, ST_KEY_RANGE); continue; }
-    if (nt < GPUDB_NATIONS && ((mask >> nt) & 1u)) map[k] = (uint8_t)nt;
-  }
-}
 
 __global__ void __launch_bounds__(kThreads) q5_orders_kernel(const int32_t* __restrict__ okey,
                                                              const int32_t* __restrict__ ocust,
@@ -154,10 +142,10 @@ extern "C" int gpudb_q5_local_supplier(gpudb_ctx* ctx, const gpudb_customer* cu,
   GPUDB_CUDA(ctx, cudaMemsetAsync(smap, kNone, (size_t)supp_max + 1, s));
   GPUDB_CUDA(ctx, cudaMemsetAsync(okbm, 0, (size_t)owords * 4, s));
   if (cu->n_rows)
-    GPUDB_LAUNCH(call, q5_nation_map_kernel, grid_for(ctx, cu->n_rows, 1, 8), kThreads, 0, cu->cust_key, cu->nation,
+    GPUDB_LAUNCH(call, nation_map_kernel, grid_for(ctx, cu->n_rows, 1, 8), kThreads, 0, cu->cust_key, cu->nation,
                  cu->n_rows, cust_max, p->nation_mask, (uint8_t*)cmap, call.status());
   if (su->n_rows)
-    GPUDB_LAUNCH(call, q5_nation_map_kernel, grid_for(ctx, su->n_rows, 1, 8), kThreads, 0, su->supp_key, su->nation,
+    GPUDB_LAUNCH(call, nation_map_kernel, grid_for(ctx, su->n_rows, 1, 8), kThreads, 0, su->supp_key, su->nation,
                  su->n_rows, supp_max, p->nation_mask, (uint8_t*)smap, call.status());
   if (od->n_rows && cu->n_rows)
     GPUDB_LAUNCH(call, q5_orders_kernel, grid_for(ctx, od->n_rows, kRows, 8), kThreads, 0, od->order_key, od->cust_key,

@@ -31,7 +31,7 @@ constexpr uint64_t kTileBytes = (uint64_t)kTT * 64;   // 64 bytes per thread
 
 enum FieldType : int32_t {
   F_I32, F_DEC64, F_DEC32, F_QTY, F_DATE, F_RETFLAG, F_LINESTATUS, F_SEGMENT, F_GREEN, F_U8, F_SHIPMODE, F_PRIORITY,
-  F_COMMENT
+  F_COMMENT, F_PTYPE
 };
 
 struct TblSpec {
@@ -48,7 +48,7 @@ bool spec_for(int32_t table, TblSpec* s) {
         F_SHIPMODE}},
       {GPUDB_TBL_ORDERS, 5, {0, 1, 4, 5, 8}, {F_I32, F_I32, F_DATE, F_PRIORITY, F_COMMENT}},
       {GPUDB_TBL_CUSTOMER, 3, {0, 3, 6}, {F_I32, F_U8, F_SEGMENT}},
-      {GPUDB_TBL_PART, 2, {0, 1}, {F_I32, F_GREEN}},
+      {GPUDB_TBL_PART, 3, {0, 1, 4}, {F_I32, F_GREEN, F_PTYPE}},
       {GPUDB_TBL_SUPPLIER, 2, {0, 3}, {F_I32, F_U8}},
       {GPUDB_TBL_PARTSUPP, 3, {0, 1, 3}, {F_I32, F_I32, F_DEC64}},
   };
@@ -170,6 +170,37 @@ __device__ __forceinline__ bool field_equals(const uint8_t* s, const uint8_t* e,
   return s == e;
 }
 
+// Position of [s, e) in the n words of `words` (separated by '|'), or -1.
+__device__ __forceinline__ int word_index(const uint8_t* s, const uint8_t* e, const char* words) {
+  int i = 0;
+  const char* w = words;
+  while (*w) {
+    const uint8_t* p = s;
+    const char* q = w;
+    while (*q && *q != '|' && p < e && *p == (uint8_t)*q) { p++; q++; }
+    if (p == e && (*q == '|' || *q == 0)) return i;
+    while (*q && *q != '|') q++;
+    if (*q == '|') q++;
+    w = q;
+    i++;
+  }
+  return -1;
+}
+
+// p_type "S1 S2 S3" -> s1 * 25 + s2 * 5 + s3 (the syllable lists of the TPC-H part types), or -1.
+__device__ int part_type_code(const uint8_t* s, const uint8_t* e) {
+  const uint8_t* a = s;
+  while (a < e && *a != ' ') a++;
+  if (a >= e) return -1;
+  const uint8_t* b = a + 1;
+  while (b < e && *b != ' ') b++;
+  if (b >= e) return -1;
+  const int i1 = word_index(s, a, "STANDARD|SMALL|MEDIUM|LARGE|ECONOMY|PROMO");
+  const int i2 = word_index(a + 1, b, "ANODIZED|BURNISHED|PLATED|POLISHED|BRUSHED");
+  const int i3 = word_index(b + 1, e, "TIN|NICKEL|BRASS|STEEL|COPPER");
+  return (i1 < 0 || i2 < 0 || i3 < 0) ? -1 : i1 * 25 + i2 * 5 + i3;
+}
+
 template <int MAXF>
 __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ text, uint64_t bytes,
                                                     const uint64_t* __restrict__ starts, const uint32_t* __restrict__ n_lines_p,
@@ -245,6 +276,10 @@ __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ 
             }
             break;
           }
+          case F_PTYPE:
+            v = part_type_code(s, fe);
+            ok = v >= 0;
+            break;
           case F_GREEN: {
             v = 0;
             for (const uint8_t* p = s; p + 5 <= fe && !v; p++)
@@ -258,7 +293,7 @@ __global__ void __launch_bounds__(256) parse_kernel(const uint8_t* __restrict__ 
           switch (spec.type[k]) {
             case F_DEC64: static_cast<int64_t*>(col)[r] = v; break;
             case F_RETFLAG: case F_LINESTATUS: case F_SEGMENT: case F_GREEN: case F_U8: case F_SHIPMODE:
-            case F_PRIORITY:
+            case F_PRIORITY: case F_PTYPE:
               static_cast<uint8_t*>(col)[r] = (uint8_t)v; break;
             default: static_cast<int32_t*>(col)[r] = (int32_t)v; break;
           }

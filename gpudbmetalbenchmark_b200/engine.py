@@ -31,7 +31,7 @@ TABLE_COLS = {
     "customer": {"cust_key": COL["CU_CUST_KEY"], "segment": COL["CU_SEGMENT"], "nation": COL["CU_NATION"]},
     "orders": {"order_key": COL["OR_ORDER_KEY"], "cust_key": COL["OR_CUST_KEY"], "order_date": COL["OR_ORDER_DATE"],
                "priority": COL["OR_PRIORITY"], "comment": COL["OR_COMMENT"]},
-    "part": {"part_key": COL["PA_PART_KEY"], "flag": COL["PA_FLAG"]},
+    "part": {"part_key": COL["PA_PART_KEY"], "flag": COL["PA_FLAG"], "type": COL["PA_TYPE"]},
     "supplier": {"supp_key": COL["SU_SUPP_KEY"], "nation": COL["SU_NATION"]},
     "partsupp": {"part_key": COL["PS_PART_KEY"], "supp_key": COL["PS_SUPP_KEY"], "supply_cost": COL["PS_SUPPLY_COST"]},
     "lineitem": LINEITEM_COLS,
@@ -342,6 +342,37 @@ class Engine:
                                                      C.byref(od.struct()), C.byref(ls), C.byref(p), C.byref(r),
                                                      C.byref(timing) if timing is not None else None, None))
         return sorted(((n, r.revenue[n]) for n in range(capi.NATIONS) if r.revenue[n]), key=lambda x: (-x[1], x[0]))
+
+    def q7(self, cu, su, od, li, nation_a="FRANCE", nation_b="GERMANY", ship_lo=1096, ship_hi=1826, timing=None):
+        """[(supp_nation, cust_nation, year, revenue)] ordered by the nations' names, then year:
+        lineitems shipped in [ship_lo, ship_hi] (default 1995-01-01 .. 1996-12-31) from a supplier
+        of one nation to a customer of the other; revenue in hundredths^2."""
+        na = capi.NATION_NAMES.index(nation_a) if isinstance(nation_a, str) else nation_a
+        nb = capi.NATION_NAMES.index(nation_b) if isinstance(nation_b, str) else nation_b
+        p = capi.Q7Params(na, nb, ship_lo, ship_hi)
+        r = capi.Q7Result()
+        ls = li if isinstance(li, capi.Lineitem) else li.lineitem()
+        self._check(self.lib.gpudb_q7_volume_shipping(self.ctx, C.byref(cu.struct()), C.byref(su.struct()),
+                                                      C.byref(od.struct()), C.byref(ls), C.byref(p), C.byref(r),
+                                                      C.byref(timing) if timing is not None else None, None))
+        rows = [(s, c, r.first_year + y, r.revenue[pair][y]) for pair, (s, c) in enumerate(((na, nb), (nb, na)))
+                for y in range(r.n_years) if r.revenue[pair][y]]
+        return sorted(rows, key=lambda x: (capi.NATION_NAMES[x[0]], capi.NATION_NAMES[x[1]], x[2]))
+
+    def q8(self, cu, su, pa, od, li, nation="BRAZIL", region="AMERICA", part_type="ECONOMY ANODIZED STEEL",
+           date_lo=1096, date_hi=1826, timing=None):
+        """[(year, nation_volume, volume)] per calendar year of [date_lo, date_hi] (default 1995 and
+        1996): revenue of the part type's lineitems whose order's customer is in the region, and
+        the part supplied by the nation; the market share is nation_volume / volume."""
+        n = capi.NATION_NAMES.index(nation) if isinstance(nation, str) else nation
+        t = capi.part_type(part_type) if isinstance(part_type, str) else part_type
+        p = capi.Q8Params(date_lo, date_hi, capi.region_mask(region), n, t, 0)
+        r = capi.Q8Result()
+        ls = li if isinstance(li, capi.Lineitem) else li.lineitem()
+        self._check(self.lib.gpudb_q8_market_share(self.ctx, C.byref(cu.struct()), C.byref(su.struct()),
+                                                   C.byref(pa.struct()), C.byref(od.struct()), C.byref(ls), C.byref(p),
+                                                   C.byref(r), C.byref(timing) if timing is not None else None, None))
+        return [(r.first_year + y, r.nation_volume[y], r.volume[y]) for y in range(r.n_years)]
 
     def q10(self, cu, od, li, date_lo=639, date_hi=731, k=20, timing=None):
         """([(cust_key, revenue)] top k by revenue desc, key asc; customers with revenue > 0):

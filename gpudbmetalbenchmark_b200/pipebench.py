@@ -249,6 +249,25 @@ def main(argv=None):
                  {"kernels": t.kernels})
             for x in (li, od, su, cu):
                 eng.free(x)
+    if on("q7q8"):
+        for n_cu, n_su, n_pa, n_or, n_li, label in ((150_000, 10_000, 200_000, 1_500_000, 6_000_000, "SF-1 sizes"),
+                                                    (1_500_000, 100_000, 2_000_000, 15_000_000, 60_000_000,
+                                                     "SF-10 sizes")):
+            cu = eng.generate("customer", n_cu, seed=42, columns=("cust_key", "nation"))
+            su = eng.generate("supplier", n_su, seed=42)
+            pa = eng.generate("part", n_pa, seed=42, columns=("part_key", "type"))
+            od = eng.generate("orders", n_or, seed=42, columns=("order_key", "cust_key", "order_date"), n_cust=n_cu)
+            li = eng.generate("lineitem", n_li, seed=42,
+                              columns=("order_key", "part_key", "supp_key", "ship_date", "ext_price", "discount"),
+                              n_orders=n_or, n_parts=n_pa, n_supp=n_su, order_mode=capi.ORDERS_CLUSTERED)
+            ms, t = timed(lambda tm: eng.q7(cu, su, od, li, timing=tm), a.reps)
+            emit("q7_volume_shipping", label, n_li, ms, n_li * 12 + n_or * 8 + n_cu * 5 + n_su * 5,
+                 {"kernels": t.kernels})
+            ms, t = timed(lambda tm: eng.q8(cu, su, pa, od, li, timing=tm), a.reps)
+            emit("q8_market_share", label, n_li, ms, n_li * 4 + n_or * 12 + n_cu * 5 + n_su * 5 + n_pa * 5,
+                 {"kernels": t.kernels})
+            for x in (li, od, pa, su, cu):
+                eng.free(x)
     if on("q10"):
         for n_cu, n_or, n_li, label in ((150_000, 1_500_000, 6_000_000, "SF-1 sizes"),
                                         (1_500_000, 15_000_000, 60_000_000, "SF-10 sizes")):

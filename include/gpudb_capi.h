@@ -158,7 +158,12 @@ typedef struct gpudb_orders {
 typedef struct gpudb_part {
   uint64_t n_rows; int32_t key_max; int32_t reserved;
   const int32_t* part_key; const uint8_t* flag;      /* flag != 0: the part passes the filter */
+  const uint8_t* type;         /* p_type code 0..149 (Q8): see GPUDB_PART_TYPE */
 } gpudb_part;
+/* p_type code of "S1 S2 S3": s1 in STANDARD, SMALL, MEDIUM, LARGE, ECONOMY, PROMO; s2 in
+ * ANODIZED, BURNISHED, PLATED, POLISHED, BRUSHED; s3 in TIN, NICKEL, BRASS, STEEL, COPPER
+ * (0-based positions in those lists); "ECONOMY ANODIZED STEEL" = 103. */
+#define GPUDB_PART_TYPE(s1, s2, s3) ((s1) * 25 + (s2) * 5 + (s3))
 
 typedef struct gpudb_supplier {
   uint64_t n_rows; int32_t key_max; int32_t reserved;
@@ -179,7 +184,7 @@ enum gpudb_column_id {
   GPUDB_COL_CU_CUST_KEY = 20, GPUDB_COL_CU_SEGMENT, GPUDB_COL_CU_NATION,
   GPUDB_COL_OR_ORDER_KEY = 30, GPUDB_COL_OR_CUST_KEY, GPUDB_COL_OR_ORDER_DATE, GPUDB_COL_OR_PRIORITY,
   GPUDB_COL_OR_COMMENT,        /* GPUDB_COMMENT_WIDTH bytes per row */
-  GPUDB_COL_PA_PART_KEY = 40, GPUDB_COL_PA_FLAG,
+  GPUDB_COL_PA_PART_KEY = 40, GPUDB_COL_PA_FLAG, GPUDB_COL_PA_TYPE,
   GPUDB_COL_SU_SUPP_KEY = 50, GPUDB_COL_SU_NATION,
   GPUDB_COL_PS_PART_KEY = 60, GPUDB_COL_PS_SUPP_KEY, GPUDB_COL_PS_SUPPLY_COST
 };
@@ -341,6 +346,41 @@ int gpudb_q5_local_supplier(gpudb_ctx* ctx, const gpudb_customer* cu, const gpud
                             const gpudb_lineitem* li, const gpudb_q5_params* p, gpudb_q5_result* out,
                             gpudb_timing* t, const gpudb_exec* ex);
 
+/* ---- Q7 volume shipping (replaces runQ7Benchmark src/q7.cpp with its kernels
+ *      q7_build_supplier_map_kernel / q7_build_customer_map_kernel / q7_build_orders_map_kernel /
+ *      q7_probe_and_aggregate_kernel kernels/q7.metal:12-109) ----------------------------------
+ * For lineitem rows with ship_lo <= ship_date <= ship_hi (both ends included, at most
+ * GPUDB_MAX_YEARS calendar years) whose supplier and whose order's customer are of nations
+ * (a, b) or (b, a): revenue[pair][y] += ext_price * (100 - discount), pair 0 = supplier of a
+ * and customer of b, pair 1 = supplier of b and customer of a, y = calendar year of the ship
+ * date - first_year. Keys outside their tables' 0..key_max fail with GPUDB_E_KEY_RANGE (lineitem
+ * keys outside them match nothing). Lineitem may be host-resident (streamed). */
+#define GPUDB_MAX_YEARS 8
+typedef struct gpudb_q7_params { int32_t nation_a; int32_t nation_b; int32_t ship_lo; int32_t ship_hi; } gpudb_q7_params;
+typedef struct gpudb_q7_result {
+  int32_t first_year; int32_t n_years; int64_t revenue[2][GPUDB_MAX_YEARS];
+} gpudb_q7_result;
+int gpudb_q7_volume_shipping(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_supplier* su, const gpudb_orders* od,
+                             const gpudb_lineitem* li, const gpudb_q7_params* p, gpudb_q7_result* out,
+                             gpudb_timing* t, const gpudb_exec* ex);
+
+/* ---- Q8 national market share (replaces runQ8Benchmark src/q8.cpp with its kernels
+ *      q8_build_orders_map_kernel / q8_probe_and_aggregate_kernel kernels/q8.metal:9-76) -------
+ * For lineitem rows whose part has type part_type and whose order has date_lo <= order_date <=
+ * date_hi (both included, at most GPUDB_MAX_YEARS calendar years) and a customer of a nation in
+ * region_mask: volume[y] += ext_price * (100 - discount), and nation_volume[y] too when the
+ * supplier is of `nation`; y = calendar year of the order date - first_year. The market share
+ * of year y is nation_volume[y] / volume[y]. Key errors as for Q7. */
+typedef struct gpudb_q8_params {
+  int32_t date_lo; int32_t date_hi; uint32_t region_mask; int32_t nation; int32_t part_type; int32_t reserved;
+} gpudb_q8_params;
+typedef struct gpudb_q8_result {
+  int32_t first_year; int32_t n_years; int64_t volume[GPUDB_MAX_YEARS]; int64_t nation_volume[GPUDB_MAX_YEARS];
+} gpudb_q8_result;
+int gpudb_q8_market_share(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_supplier* su, const gpudb_part* pa,
+                          const gpudb_orders* od, const gpudb_lineitem* li, const gpudb_q8_params* p,
+                          gpudb_q8_result* out, gpudb_timing* t, const gpudb_exec* ex);
+
 /* ---- Q10 returned item reporting (replaces runQ10Benchmark src/q10.cpp:8-140 with its kernels
  *      q10_build_orders_map_kernel / q10_probe_and_aggregate_kernel kernels/q10.metal:8-54 and
  *      its host top-20 heap src/q10.cpp:102-121) ------------------------------------------------
@@ -471,7 +511,7 @@ int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, gpudb_timin
  *   ORDERS:   order_key, cust_key, order_date, priority (u8), comment (GPUDB_COMMENT_WIDTH
  *             bytes per row: at most 79 characters, NUL-padded)    fields 0,1,4,5,8
  *   CUSTOMER: cust_key, nation (u8), segment (u8)                  fields 0,3,6
- *   PART:     part_key, flag (u8)                                  fields 0,1
+ *   PART:     part_key, flag (u8), type (u8, GPUDB_PART_TYPE)      fields 0,1,4
  *   SUPPLIER: supp_key, nation (u8)                                fields 0,3
  *   PARTSUPP: part_key, supp_key, supply_cost (int64)              fields 0,1,3
  * `cols` are device columns holding `capacity` rows (a NULL column is parsed and checked but

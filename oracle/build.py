@@ -41,7 +41,7 @@ def build_reference():
         return lib if os.path.exists(lib) else None
     os.makedirs(out, exist_ok=True)
     deps = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "refshim", "metal_stdlib")]
-    deps += [os.path.join(kdir, f) for f in ("common.h", "q1.metal", "q3.metal", "q4.metal", "q5.metal", "q6.metal",
+    deps += [os.path.join(kdir, f) for f in ("common.h", "q1.metal", "q3.metal", "q4.metal", "q5.metal", "q6.metal", "q7.metal", "q8.metal",
                                               "q9.metal", "q10.metal", "q12.metal", "q13.metal", "microbenchmarks.metal")]
     if _fresh(lib, deps):
         return lib

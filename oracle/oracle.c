@@ -37,7 +37,7 @@ static int64_t unif(uint64_t key, uint64_t row, int64_t lo, int64_t hi) {
 /* random stream ids (table*16 + column) */
 enum { S_SHIP = 16, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG, S_STATUS, S_OPICK, S_PART, S_SSLOT, S_RUN,
        S_COMMIT, S_RECEIPT, S_MODE,
-       S_SEG = 32, S_CNATION, S_OCUST = 48, S_ODATE, S_OPRIO, S_OCOMMENT, S_PFLAG = 64, S_NATION = 80, S_COST = 96 };
+       S_SEG = 32, S_CNATION, S_OCUST = 48, S_ODATE, S_OPRIO, S_OCOMMENT, S_PFLAG = 64, S_PTYPE, S_NATION = 80, S_COST = 96 };
 
 /* order comment: n = U[2,9] words (sub-draw r*16), word i = U[0,23] (sub-draw r*16+1+i) of the
  * vocabulary below, joined by single spaces, stopping at the first word that would pass 79
@@ -116,6 +116,7 @@ int or_gen_column(const or_spec* sp, int32_t column, void* dst) {
   case 31: { if (sp->n_cust <= 0) return -1; uint64_t k = stream_of(seed, S_OCUST);
              for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, sp->n_cust - 1); return 0; }
   case 32: { uint64_t k = stream_of(seed, S_ODATE); for (i = 0; i < n; i++) i32[i] = (int32_t)unif(k, off + i, 0, 2405); return 0; }
+  case 42: { uint64_t k = stream_of(seed, S_PTYPE); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 149); return 0; }
   case 41: { uint64_t k = stream_of(seed, S_PFLAG); for (i = 0; i < n; i++) u8[i] = unif(k, off + i, 0, 999) < 55; return 0; }
   case 51: { uint64_t k = stream_of(seed, S_NATION); for (i = 0; i < n; i++) u8[i] = (uint8_t)unif(k, off + i, 0, 24); return 0; }
   case 60: for (i = 0; i < n; i++) i32[i] = (int32_t)((off + i) / 4); return 0;
@@ -448,6 +449,92 @@ void or_q5(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32
     revenue25[n] += l_ext[i] * (int64_t)(100 - l_disc[i]);
   }
   free(cn); free(sn); free(on);
+}
+
+/* calendar year of a day number (0 = 1992-01-01) */
+static int year_len(int y) { return ((y % 4 == 0 && y % 100 != 0) || y % 400 == 0) ? 366 : 365; }
+static int year_of_day(int32_t d) {
+  int y = 1992;
+  while (d < 0) { y--; d += year_len(y); }
+  while (d >= year_len(y)) { d -= year_len(y); y++; }
+  return y;
+}
+static uint8_t* nation_bytes(uint64_t n, const int32_t* key, const uint8_t* nation, int32_t key_max, uint32_t mask) {
+  uint8_t* m = (uint8_t*)malloc((size_t)key_max + 1);
+  memset(m, 0xFF, (size_t)key_max + 1);
+  for (uint64_t i = 0; i < n; i++) if (nation[i] < 25 && (mask >> nation[i] & 1)) m[key[i]] = nation[i];
+  return m;
+}
+
+/* ---- Q7: kernels/q7.metal:12-109 (supplier and customer maps of the two nations, orders ->
+ * customer, lineitem in the ship window, pair and calendar year bins) ---- */
+int or_q7(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32_t cu_key_max, uint64_t n_su,
+          const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max, uint64_t n_or, const int32_t* o_key,
+          const int32_t* o_cust, int32_t or_key_max, uint64_t n_li, const int32_t* l_key, const int32_t* l_supp,
+          const int32_t* l_ship, const int64_t* l_ext, const int32_t* l_disc, int32_t a, int32_t b, int32_t ship_lo,
+          int32_t ship_hi, int64_t* rev16, int32_t* first_year, int32_t* n_years) {
+  uint64_t i;
+  for (int j = 0; j < 16; j++) rev16[j] = 0;
+  const int fy = year_of_day(ship_lo), ny = year_of_day(ship_hi) - fy + 1;
+  *first_year = fy;
+  *n_years = ny;
+  if (ny < 1 || ny > 8) return -1;
+  if (cu_key_max < 0 || su_key_max < 0 || or_key_max < 0) return 0;
+  const uint32_t mask = (1u << a) | (1u << b);
+  uint8_t* cn = nation_bytes(n_cu, cu_key, cu_nation, cu_key_max, mask);
+  uint8_t* sn = nation_bytes(n_su, su_key, su_nation, su_key_max, mask);
+  uint8_t* on = (uint8_t*)malloc((size_t)or_key_max + 1);
+  memset(on, 0xFF, (size_t)or_key_max + 1);
+  for (i = 0; i < n_or; i++) if (o_cust[i] >= 0 && o_cust[i] <= cu_key_max) on[o_key[i]] = cn[o_cust[i]];
+  for (i = 0; i < n_li; i++) {
+    if (l_ship[i] < ship_lo || l_ship[i] > ship_hi) continue;
+    if (l_key[i] < 0 || l_key[i] > or_key_max || l_supp[i] < 0 || l_supp[i] > su_key_max) continue;
+    const int c = on[l_key[i]], s = sn[l_supp[i]];
+    const int pair = (s == a && c == b) ? 0 : (s == b && c == a) ? 1 : -1;
+    if (pair < 0) continue;
+    rev16[pair * 8 + year_of_day(l_ship[i]) - fy] += l_ext[i] * (int64_t)(100 - l_disc[i]);
+  }
+  free(cn); free(sn); free(on);
+  return 0;
+}
+
+/* ---- Q8: kernels/q8.metal:9-76 (orders of the window with a customer of the region ->
+ * order year, lineitem of the part type: total and the nation's share per year) ---- */
+int or_q8(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32_t cu_key_max, uint64_t n_su,
+          const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max, uint64_t n_pa, const int32_t* pa_key,
+          const uint8_t* pa_type, int32_t pa_key_max, uint64_t n_or, const int32_t* o_key, const int32_t* o_cust,
+          const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key, const int32_t* l_part,
+          const int32_t* l_supp, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
+          uint32_t region_mask, int32_t nation, int32_t part_type, int64_t* vol8, int64_t* nvol8, int32_t* first_year,
+          int32_t* n_years) {
+  uint64_t i;
+  for (int j = 0; j < 8; j++) vol8[j] = nvol8[j] = 0;
+  const int fy = year_of_day(date_lo), ny = year_of_day(date_hi) - fy + 1;
+  *first_year = fy;
+  *n_years = ny;
+  if (ny < 1 || ny > 8) return -1;
+  if (cu_key_max < 0 || su_key_max < 0 || pa_key_max < 0 || or_key_max < 0) return 0;
+  uint8_t* cn = nation_bytes(n_cu, cu_key, cu_nation, cu_key_max, region_mask);
+  uint8_t* sn = nation_bytes(n_su, su_key, su_nation, su_key_max, 1u << nation);
+  uint8_t* pt = (uint8_t*)calloc((size_t)pa_key_max + 1, 1);
+  uint8_t* oy = (uint8_t*)malloc((size_t)or_key_max + 1);
+  memset(oy, 0xFF, (size_t)or_key_max + 1);
+  for (i = 0; i < n_pa; i++) if (pa_type[i] == part_type) pt[pa_key[i]] = 1;
+  for (i = 0; i < n_or; i++) {
+    if (o_date[i] < date_lo || o_date[i] > date_hi) continue;
+    if (o_cust[i] < 0 || o_cust[i] > cu_key_max || cn[o_cust[i]] == 0xFF) continue;
+    oy[o_key[i]] = (uint8_t)(year_of_day(o_date[i]) - fy);
+  }
+  for (i = 0; i < n_li; i++) {
+    if (l_part[i] < 0 || l_part[i] > pa_key_max || !pt[l_part[i]]) continue;
+    if (l_key[i] < 0 || l_key[i] > or_key_max || oy[l_key[i]] == 0xFF) continue;
+    if (l_supp[i] < 0 || l_supp[i] > su_key_max) continue;
+    const int64_t r = l_ext[i] * (int64_t)(100 - l_disc[i]);
+    vol8[oy[l_key[i]]] += r;
+    if (sn[l_supp[i]] != 0xFF) nvol8[oy[l_key[i]]] += r;
+  }
+  free(cn); free(sn); free(pt); free(oy);
+  return 0;
 }
 
 /* ---- Q10: kernels/q10.metal:8-54 (window map, returned rows), src/q10.cpp:102-121 (top-k) ---- */

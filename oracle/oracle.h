@@ -90,6 +90,24 @@ void or_q5(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32
            const int32_t* o_cust, const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key,
            const int32_t* l_supp, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
            uint32_t nation_mask, int64_t* revenue25);
+/* Q7: rev16[pair * 8 + y], pair 0 = supplier of a / customer of b, 1 = the reverse, y = calendar
+ * year of the ship date (in [ship_lo, ship_hi], both included) - first_year
+ * (kernels/q7.metal:12-109). Returns -1 when the window spans more than 8 years. */
+int or_q7(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32_t cu_key_max, uint64_t n_su,
+          const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max, uint64_t n_or, const int32_t* o_key,
+          const int32_t* o_cust, int32_t or_key_max, uint64_t n_li, const int32_t* l_key, const int32_t* l_supp,
+          const int32_t* l_ship, const int64_t* l_ext, const int32_t* l_disc, int32_t a, int32_t b, int32_t ship_lo,
+          int32_t ship_hi, int64_t* rev16, int32_t* first_year, int32_t* n_years);
+/* Q8: vol8[y] / nvol8[y] = revenue of the part type's lineitems whose order is in [date_lo,
+ * date_hi] (both included) with a customer of region_mask, all suppliers / suppliers of
+ * `nation`; y = calendar year of the order date - first_year (kernels/q8.metal:9-76). */
+int or_q8(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, int32_t cu_key_max, uint64_t n_su,
+          const int32_t* su_key, const uint8_t* su_nation, int32_t su_key_max, uint64_t n_pa, const int32_t* pa_key,
+          const uint8_t* pa_type, int32_t pa_key_max, uint64_t n_or, const int32_t* o_key, const int32_t* o_cust,
+          const int32_t* o_date, int32_t or_key_max, uint64_t n_li, const int32_t* l_key, const int32_t* l_part,
+          const int32_t* l_supp, const int64_t* l_ext, const int32_t* l_disc, int32_t date_lo, int32_t date_hi,
+          uint32_t region_mask, int32_t nation, int32_t part_type, int64_t* vol8, int64_t* nvol8, int32_t* first_year,
+          int32_t* n_years);
 /* Q10: exact revenue sum ext*(100-disc) of returned lineitems (flag 2) per customer of cu, over
  * orders with date_lo <= date < date_hi (kernels/q10.metal:8-54); the top k by revenue desc,
  * cust_key asc among customers with revenue > 0 (src/q10.cpp:102-121). rev_out (cu_key_max+1

@@ -1,5 +1,5 @@
 // ref_harness.cpp -- runs the reference's own Metal kernels (kernels/q1.metal, q3.metal,
-// q4.metal, q5.metal, q6.metal, q9.metal, q10.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
+// q4.metal, q5.metal, q6.metal, q7.metal, q8.metal, q9.metal, q10.metal, q12.metal, q13.metal, microbenchmarks.metal, compiled in place from the reference tree
 // through the CPU shim in oracle/refshim) on the synthetic tables. TEST INFRASTRUCTURE
 // ONLY: it pins the oracle's query logic to the reference's code, and it is the timed
 // reference arm of bench.py. It is never linked into the engine.
@@ -24,6 +24,8 @@ using namespace metal;
 #include "q4.metal"
 #include "q5.metal"
 #include "q6.metal"
+#include "q7.metal"
+#include "q8.metal"
 #include "q9.metal"
 
 namespace {
@@ -81,6 +83,12 @@ template <class F> void run_groups(uint G, int threads, F fn) {
 }
 
 uint next_pow2_u(uint v) { uint p = 1; while (p < v) p <<= 1; return p; }
+
+template <class K> int max_of(uint64_t n, const K* v) {
+  int m = 0;
+  for (uint64_t i = 0; i < n; i++) m = std::max(m, (int)v[i]);
+  return m;
+}
 
 }  // namespace
 
@@ -275,6 +283,66 @@ void ref_q5(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, uint
                                   map_size, g, 0, 1, (uint)groups);
   });
   for (int n = 0; n < 25; n++) revenue25[n] = rev[n].v;
+}
+
+// Q7 through q7_build_supplier_map_kernel, q7_build_customer_map_kernel,
+// q7_build_orders_map_kernel and q7_probe_and_aggregate_kernel (kernels/q7.metal:12-109), with
+// -1-filled maps; the kernel bins the years 1995 and 1996. bins4 = pair * 2 + year.
+void ref_q7(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, uint64_t n_su, const int32_t* su_key,
+            const uint8_t* su_nation, uint64_t n_or, const int32_t* or_key, const int32_t* or_cust, uint64_t n_li,
+            const int32_t* li_key, const int32_t* li_supp, const int32_t* li_ship, const int64_t* li_ext,
+            const int32_t* li_disc, int32_t a, int32_t b, int32_t ship_lo, int32_t ship_hi, int groups, int threads,
+            float* bins4) {
+  const int max_o = std::max(max_of(n_or, or_key), max_of(n_li, li_key));
+  std::vector<int> smap((size_t)max_of(n_su, su_key) + 1, -1), cmap((size_t)max_of(n_cu, cu_key) + 1, -1);
+  std::vector<int> omap((size_t)max_o + 1, -1);
+  std::vector<int> sn(su_nation, su_nation + n_su), cn(cu_nation, cu_nation + n_cu);
+  uint nsu = (uint)n_su, ncu = (uint)n_cu, nor = (uint)n_or, nli = (uint)n_li, map_size = (uint)max_o + 1;
+  for (uint i = 0; i < nsu; i++) q7_build_supplier_map_kernel(su_key, sn.data(), smap.data(), a, b, nsu, i);
+  for (uint i = 0; i < ncu; i++) q7_build_customer_map_kernel(cu_key, cn.data(), cmap.data(), a, b, ncu, i);
+  for (uint i = 0; i < nor; i++) q7_build_orders_map_kernel(or_key, or_cust, omap.data(), nor, i);
+  std::vector<int> ls = dates(n_li, li_ship);
+  std::vector<float> ext = hundredths(n_li, li_ext), dsc = hundredths(n_li, li_disc);
+  std::vector<atomic_float> bins(4);
+  for (auto& x : bins) x.v = 0.0f;
+  int ds = yyyymmdd(ship_lo), de = yyyymmdd(ship_hi);
+  run_groups((uint)groups, threads, [&](uint g) {
+    q7_probe_and_aggregate_kernel(li_key, li_supp, ls.data(), ext.data(), dsc.data(), omap.data(), cmap.data(),
+                                  smap.data(), bins.data(), nli, map_size, a, b, ds, de, g, 0, 1, (uint)groups);
+  });
+  for (int i = 0; i < 4; i++) bins4[i] = bins[i].v;
+}
+
+// Q8 through q8_build_orders_map_kernel and q8_probe_and_aggregate_kernel
+// (kernels/q8.metal:9-76), with the host-side part bitmap (p_type == part_type), customer map
+// of the region's nations and supplier map that the reference's driver builds; the kernel bins
+// the years 1995 and 1996. bins4 = nation 1995, nation 1996, total 1995, total 1996.
+void ref_q8(uint64_t n_cu, const int32_t* cu_key, const uint8_t* cu_nation, uint64_t n_su, const int32_t* su_key,
+            const uint8_t* su_nation, uint64_t n_pa, const int32_t* pa_key, const uint8_t* pa_type, uint64_t n_or,
+            const int32_t* or_key, const int32_t* or_cust, const int32_t* or_date, uint64_t n_li,
+            const int32_t* li_key, const int32_t* li_part, const int32_t* li_supp, const int64_t* li_ext,
+            const int32_t* li_disc, int32_t date_lo, int32_t date_hi, uint32_t region_mask, int32_t nation,
+            int32_t part_type, int groups, int threads, float* bins4) {
+  std::vector<uint> pbits((size_t)max_of(n_pa, pa_key) / 32 + 2, 0u);
+  for (uint64_t i = 0; i < n_pa; i++)
+    if (pa_type[i] == part_type) pbits[(uint)pa_key[i] >> 5] |= 1u << ((uint)pa_key[i] & 31u);
+  std::vector<int> cmap((size_t)max_of(n_cu, cu_key) + 1, -1), smap((size_t)max_of(n_su, su_key) + 1, -1);
+  for (uint64_t i = 0; i < n_cu; i++) if ((region_mask >> cu_nation[i]) & 1u) cmap[cu_key[i]] = cu_nation[i];
+  for (uint64_t i = 0; i < n_su; i++) smap[su_key[i]] = su_nation[i];
+  const int max_o = std::max(max_of(n_or, or_key), max_of(n_li, li_key));
+  std::vector<int> ocust((size_t)max_o + 1, -1), oyear((size_t)max_o + 1, -1), od = dates(n_or, or_date);
+  uint nor = (uint)n_or, nli = (uint)n_li, map_size = (uint)max_o + 1;
+  int ds = yyyymmdd(date_lo), de = yyyymmdd(date_hi);
+  for (uint i = 0; i < nor; i++)
+    q8_build_orders_map_kernel(or_key, or_cust, od.data(), ocust.data(), oyear.data(), cmap.data(), nor, ds, de, i);
+  std::vector<float> ext = hundredths(n_li, li_ext), dsc = hundredths(n_li, li_disc);
+  std::vector<atomic_float> bins(4);
+  for (auto& x : bins) x.v = 0.0f;
+  run_groups((uint)groups, threads, [&](uint g) {
+    q8_probe_and_aggregate_kernel(li_key, li_part, li_supp, ext.data(), dsc.data(), pbits.data(), ocust.data(),
+                                  oyear.data(), smap.data(), bins.data(), nli, map_size, nation, g, 0, 1, (uint)groups);
+  });
+  for (int i = 0; i < 4; i++) bins4[i] = bins[i].v;
 }
 
 // Q10 through q10_build_orders_map_kernel and q10_probe_and_aggregate_kernel

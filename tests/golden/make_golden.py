@@ -78,6 +78,8 @@ def column(name, n, seed, off=0, n_orders=0, n_cust=0, n_parts=0, n_supp=0, mode
                 text = nxt
             out.append(text)
         return out
+    if name == "p_type":
+        return [uniform(k(65), r, 0, 149) for r in rows]
     if name == "c_nation":
         return [uniform(k(33), r, 0, 24) for r in rows]
     if name == "segment":
@@ -214,6 +216,64 @@ def q5(n_cu, n_su, n_or, n_li, seed, date_lo=731, date_hi=1096, nations=(8, 9, 1
     return [[n, str(r)] for n, r in sorted(rev.items(), key=lambda x: (-x[1], x[0])) if r]
 
 
+NATIONS = ("ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA", "INDONESIA",
+           "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA", "ROMANIA",
+           "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES")
+
+
+def year_of_day(d):
+    y = 1992
+    ylen = lambda y: 366 if (y % 4 == 0 and y % 100 != 0) or y % 400 == 0 else 365  # noqa: E731
+    while d < 0:
+        y -= 1
+        d += ylen(y)
+    while d >= ylen(y):
+        d -= ylen(y)
+        y += 1
+    return y
+
+
+def q7q8_tables(n_cu, n_su, n_pa, n_or, n_li, seed):
+    t = {"c_nation": column("c_nation", n_cu, seed), "s_nation": column("nation", n_su, seed),
+         "p_type": column("p_type", n_pa, seed), "o_cust": column("o_cust", n_or, seed, n_cust=n_cu),
+         "o_date": column("o_date", n_or, seed)}
+    t["li"] = {c: column(c, n_li, seed, n_orders=n_or, n_parts=n_pa, n_supp=n_su, mode=1)
+               for c in ("order_key", "part_key", "supp_key", "ship_date", "ext_price", "discount")}
+    return t
+
+
+def q7(n_cu, n_su, n_pa, n_or, n_li, seed, a=6, b=7, lo=1096, hi=1826):
+    t = q7q8_tables(n_cu, n_su, n_pa, n_or, n_li, seed)
+    cust_nation = {4 * i + 1: t["c_nation"][t["o_cust"][i]] for i in range(n_or)}
+    rev = {}
+    li = t["li"]
+    for key, sk, sd, e, d in zip(li["order_key"], li["supp_key"], li["ship_date"], li["ext_price"], li["discount"]):
+        if not lo <= sd <= hi:
+            continue
+        s, c = t["s_nation"][sk], cust_nation[key]
+        if (s, c) in ((a, b), (b, a)):
+            g = (s, c, year_of_day(sd))
+            rev[g] = rev.get(g, 0) + e * (100 - d)
+    order = sorted(rev.items(), key=lambda kv: (NATIONS[kv[0][0]], NATIONS[kv[0][1]], kv[0][2]))
+    return [[s, c, y, str(r)] for (s, c, y), r in order if r]
+
+
+def q8(n_cu, n_su, n_pa, n_or, n_li, seed, nation=2, region=(1, 2, 3, 17, 24), ptype=103, lo=1096, hi=1826):
+    t = q7q8_tables(n_cu, n_su, n_pa, n_or, n_li, seed)
+    year = {4 * i + 1: year_of_day(t["o_date"][i]) for i in range(n_or)
+            if lo <= t["o_date"][i] <= hi and t["c_nation"][t["o_cust"][i]] in region}
+    vol, nvol = {}, {}
+    li = t["li"]
+    for key, pk, sk, e, d in zip(li["order_key"], li["part_key"], li["supp_key"], li["ext_price"], li["discount"]):
+        if t["p_type"][pk] != ptype or key not in year:
+            continue
+        y = year[key]
+        vol[y] = vol.get(y, 0) + e * (100 - d)
+        if t["s_nation"][sk] == nation:
+            nvol[y] = nvol.get(y, 0) + e * (100 - d)
+    return [[y, str(nvol.get(y, 0)), str(vol.get(y, 0))] for y in range(year_of_day(lo), year_of_day(hi) + 1)]
+
+
 def q10(n_cu, n_or, n_li, seed, date_lo=639, date_hi=731, k=20):
     ocust = column("o_cust", n_or, seed, n_cust=n_cu)
     odate = column("o_date", n_or, seed)
@@ -228,7 +288,7 @@ def q10(n_cu, n_or, n_li, seed, date_lo=639, date_hi=731, k=20):
 
 
 def main():
-    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}, "q10": {}, "q5": {}}
+    out = {"generator": {}, "q6": {}, "q1": {}, "q3": {}, "q9": {}, "q4": {}, "q12": {}, "q13": {}, "q10": {}, "q5": {}, "q7": {}, "q8": {}}
     # generator: first values and column sums for two seeds and a shifted window
     for seed, off in ((42, 0), (7, 1000)):
         cols = {}
@@ -242,7 +302,7 @@ def main():
             cols["order_key_uniform"] = {"head": v2[:8], "sum": sum(v2)}
         v = column("supp_key", 64, seed, off, n_parts=1000, n_supp=100)
         cols["supp_key"] = {"head": v[:8], "sum": sum(v)}
-        for name in ("commit_date", "receipt_date", "ship_mode", "o_priority", "c_nation"):
+        for name in ("commit_date", "receipt_date", "ship_mode", "o_priority", "c_nation", "p_type"):
             v = column(name, 64, seed, off)
             cols[name] = {"head": v[:8], "sum": sum(v)}
         cols["o_comment"] = {"head": column("o_comment", 4, seed, off)}
@@ -264,6 +324,11 @@ def main():
     out["q13"]["300_3000_42"] = q13(300, 3000, 42)
     out["q10"]["300_3000_12000_42"] = q10(300, 3000, 12000, 42)
     out["q5"]["300_40_3000_12000_42"] = q5(300, 40, 3000, 12000, 42)
+    out["q7"]["400_40_600_3000_12000_42"] = q7(400, 40, 600, 3000, 12000, 42)
+    out["q7"]["400_40_600_3000_12000_5_peru_china_all"] = q7(400, 40, 600, 3000, 12000, 5, 17, 18, 0, 2556)
+    out["q8"]["400_40_300_3000_12000_42_type7"] = q8(400, 40, 300, 3000, 12000, 42, 2, (1, 2, 3, 17, 24), 7)
+    out["q8"]["500_40_300_4000_16000_9_japan_asia_1993_1997"] = q8(500, 40, 300, 4000, 16000, 9, 12,
+                                                                   (8, 9, 12, 18, 21), 103, 366, 2191)
     out["q5"]["500_60_4000_16000_3_europe_all_years"] = q5(500, 60, 4000, 16000, 3, 0, 2406, (6, 7, 19, 22, 23))
     out["q10"]["200_2000_9000_5_wide"] = q10(200, 2000, 9000, 5, 0, 2406, 7)
     out["q13"]["200_4000_9_pinto_beans"] = q13(200, 4000, 9, "pinto", "beans")

@@ -10,7 +10,7 @@ ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgpudbref.so")
 
 WIDTH = {1: 4, 2: 4, 3: 8, 4: 4, 5: 4, 6: 1, 7: 1, 8: 4, 9: 4, 10: 4, 11: 4, 12: 4, 13: 1, 20: 4, 21: 1, 22: 1, 30: 4,
-         31: 4, 32: 4, 33: 1, 34: 80, 40: 4, 41: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
+         31: 4, 32: 4, 33: 1, 34: 80, 40: 4, 41: 1, 42: 1, 50: 4, 51: 1, 60: 4, 61: 4, 62: 8}
 DT = {1: np.uint8, 4: np.int32, 8: np.int64, 80: np.dtype("S80")}
 
 
@@ -37,6 +37,9 @@ ORACLE_ARGS = {
     "or_q12": [U64, V, V, I32, U64, V, V, V, V, V, I32, I32, I32, I32, I32, V],
     "or_q13": [U64, V, I32, U64, V, V, C.c_char_p, C.c_char_p, V, V, U32],
     "or_q5": [U64, V, V, I32, U64, V, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, U32, V],
+    "or_q7": [U64, V, V, I32, U64, V, V, I32, U64, V, V, I32, U64, V, V, V, V, V, I32, I32, I32, I32, V, V, V],
+    "or_q8": [U64, V, V, I32, U64, V, V, I32, U64, V, V, I32, U64, V, V, V, I32, U64, V, V, V, V, V, I32, I32, U32, I32,
+              I32, V, V, V, V],
     "or_q10": [U64, V, I32, U64, V, V, V, I32, U64, V, V, V, V, I32, I32, I32, V, V, V],
     "or_select_lt": [U64, V, I32, V, V],
     "or_sum_i32": [U64, V],
@@ -55,6 +58,9 @@ REF_ARGS = {
     "ref_q12": [U64, V, V, U64, V, V, V, V, V, I32, I32, C.c_int, C.c_int, V],
     "ref_q13": [U64, U64, V, V, C.c_int, C.c_int, V],
     "ref_q5": [U64, V, V, U64, V, V, U64, V, V, V, U64, V, V, V, V, I32, I32, U32, C.c_int, C.c_int, V],
+    "ref_q7": [U64, V, V, U64, V, V, U64, V, V, U64, V, V, V, V, V, I32, I32, I32, I32, C.c_int, C.c_int, V],
+    "ref_q8": [U64, V, V, U64, V, V, U64, V, V, U64, V, V, V, U64, V, V, V, V, V, I32, I32, U32, I32, I32, C.c_int,
+               C.c_int, V],
     "ref_q10": [U64, V, V, V, U64, V, V, V, V, I32, I32, C.c_int, C.c_int, V, U32],
     "ref_select_lt": [U64, V, I32, V],
     "ref_sum": [U64, V, C.c_int, C.c_int],
@@ -165,6 +171,60 @@ def q5(cu, su, od, li, date_lo=731, date_hi=1096, mask=ASIA, revenue_out=None):
                    kmax(od["order_key"]), len(li["order_key"]), _p(li["order_key"]), _p(li["supp_key"]),
                    _p(li["ext_price"]), _p(li["discount"]), date_lo, date_hi, mask, rev.ctypes.data)
     return sorted(((n, int(rev[n])) for n in range(25) if rev[n]), key=lambda x: (-x[1], x[0]))
+
+
+FRANCE, GERMANY, BRAZIL = 6, 7, 2
+AMERICA = (1 << 1) | (1 << 2) | (1 << 3) | (1 << 17) | (1 << 24)
+NATION_NAMES = ("ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
+                "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
+                "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES")
+
+
+def q8_tables(n_cu, n_su, n_pa, n_or, n_li, seed=42):
+    """Customer (key, nation), supplier (key, nation), part (key, type), orders (key, customer,
+    date) and lineitem (order, part, supplier keys, ext_price, discount): the tables of Q7 and Q8."""
+    cu = dict(cust_key=gen(20, n_cu, seed), nation=gen(22, n_cu, seed))
+    su = dict(supp_key=gen(50, n_su, seed), nation=gen(51, n_su, seed))
+    pa = dict(part_key=gen(40, n_pa, seed), type=gen(42, n_pa, seed))
+    od = dict(order_key=gen(30, n_or, seed), cust_key=gen(31, n_or, seed, n_cust=n_cu), order_date=gen(32, n_or, seed))
+    li = lineitem(n_li, seed, n_orders=n_or, order_mode=1, n_parts=n_pa, n_supp=n_su,
+                  cols=("order_key", "part_key", "supp_key", "ship_date", "ext_price", "discount"))
+    return cu, su, pa, od, li
+
+
+def _kmax(a):
+    return int(a.max()) if len(a) else -1
+
+
+def q7(cu, su, od, li, a=FRANCE, b=GERMANY, ship_lo=1096, ship_hi=1826):
+    """[(supp_nation, cust_nation, year, revenue)] nonzero, ordered by nation names, then year."""
+    rev = np.zeros(16, np.int64)
+    fy, ny = C.c_int32(), C.c_int32()
+    rc = oracle().or_q7(len(cu["cust_key"]), _p(cu["cust_key"]), _p(cu["nation"]), _kmax(cu["cust_key"]),
+                        len(su["supp_key"]), _p(su["supp_key"]), _p(su["nation"]), _kmax(su["supp_key"]),
+                        len(od["order_key"]), _p(od["order_key"]), _p(od["cust_key"]), _kmax(od["order_key"]),
+                        len(li["order_key"]), _p(li["order_key"]), _p(li["supp_key"]), _p(li["ship_date"]),
+                        _p(li["ext_price"]), _p(li["discount"]), a, b, ship_lo, ship_hi, rev.ctypes.data,
+                        C.byref(fy), C.byref(ny))
+    assert rc == 0
+    rows = [(s, c, fy.value + y, int(rev[pair * 8 + y])) for pair, (s, c) in enumerate(((a, b), (b, a)))
+            for y in range(ny.value) if rev[pair * 8 + y]]
+    return sorted(rows, key=lambda x: (NATION_NAMES[x[0]], NATION_NAMES[x[1]], x[2]))
+
+
+def q8(cu, su, pa, od, li, nation=BRAZIL, region_mask=AMERICA, part_type=103, date_lo=1096, date_hi=1826):
+    """[(year, nation_volume, volume)] per calendar year of the window."""
+    vol, nvol = np.zeros(8, np.int64), np.zeros(8, np.int64)
+    fy, ny = C.c_int32(), C.c_int32()
+    rc = oracle().or_q8(len(cu["cust_key"]), _p(cu["cust_key"]), _p(cu["nation"]), _kmax(cu["cust_key"]),
+                        len(su["supp_key"]), _p(su["supp_key"]), _p(su["nation"]), _kmax(su["supp_key"]),
+                        len(pa["part_key"]), _p(pa["part_key"]), _p(pa["type"]), _kmax(pa["part_key"]),
+                        len(od["order_key"]), _p(od["order_key"]), _p(od["cust_key"]), _p(od["order_date"]),
+                        _kmax(od["order_key"]), len(li["order_key"]), _p(li["order_key"]), _p(li["part_key"]),
+                        _p(li["supp_key"]), _p(li["ext_price"]), _p(li["discount"]), date_lo, date_hi, region_mask,
+                        nation, part_type, vol.ctypes.data, nvol.ctypes.data, C.byref(fy), C.byref(ny))
+    assert rc == 0
+    return [(fy.value + y, int(nvol[y]), int(vol[y])) for y in range(ny.value)]
 
 
 def q10_tables(n_cu, n_or, n_li, seed=42):
@@ -342,6 +402,8 @@ _EPOCH = _dt.date(1992, 1, 1)
 _SEGMENTS = ("AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY")
 _FLAGS, _STATUS = "ANR", "FO"
 _MODES = ("AIR", "FOB", "MAIL", "RAIL", "REG AIR", "SHIP", "TRUCK")
+_PTYPE = (("STANDARD", "SMALL", "MEDIUM", "LARGE", "ECONOMY", "PROMO"),
+          ("ANODIZED", "BURNISHED", "PLATED", "POLISHED", "BRUSHED"), ("TIN", "NICKEL", "BRASS", "STEEL", "COPPER"))
 _PRIORITIES = ("1-URGENT", "2-HIGH", "3-MEDIUM", "4-NOT SPECIFIED", "5-LOW")
 
 
@@ -383,8 +445,10 @@ def format_tbl(kind, c):
     elif kind == "part":
         for i in range(len(c["part_key"])):
             name = "forest green lace" if c["flag"][i] else "steel ivory lace"
-            out.append("%d|%s %d|Manufacturer#1|Brand#13|SMALL PLATED TIN|7|JUMBO PKG|%s|a part|"
-                       % (c["part_key"][i], name, i, _money(90000 + i)))
+            t = int(c["type"][i]) if "type" in c else 2 * 25 + 2 * 5 + 0   # MEDIUM PLATED TIN by default
+            ptype = "%s %s %s" % (_PTYPE[0][t // 25], _PTYPE[1][t // 5 % 5], _PTYPE[2][t % 5])
+            out.append("%d|%s %d|Manufacturer#1|Brand#13|%s|7|JUMBO PKG|%s|a part|"
+                       % (c["part_key"][i], name, i, ptype, _money(90000 + i)))
     elif kind == "supplier":
         for i in range(len(c["supp_key"])):
             out.append("%d|Supplier#%09d|addr %d|%d|11-222-333-4444|%s|a supplier|"
@@ -408,7 +472,7 @@ def parse_tbl_cpu(kind, text):
             "orders": [(0, "order_key", "i"), (1, "cust_key", "i"), (4, "order_date", "d"), (5, "priority", "p"),
                        (8, "comment", "c")],
             "customer": [(0, "cust_key", "i"), (3, "nation", "i"), (6, "segment", "g")],
-            "part": [(0, "part_key", "i"), (1, "flag", "n")],
+            "part": [(0, "part_key", "i"), (1, "flag", "n"), (4, "type", "t")],
             "supplier": [(0, "supp_key", "i"), (3, "nation", "i")],
             "partsupp": [(0, "part_key", "i"), (1, "supp_key", "i"), (3, "supply_cost", "m")]}[kind]
 
@@ -421,6 +485,8 @@ def parse_tbl_cpu(kind, text):
     conv = {"i": int, "q": lambda s: money(s) // 100, "m": money, "r": _FLAGS.index, "s": _STATUS.index,
             "d": lambda s: (_dt.date.fromisoformat(s) - _EPOCH).days, "g": _SEGMENTS.index,
             "n": lambda s: int("green" in s), "e": _MODES.index, "p": lambda s: _PRIORITIES.index(s) + 1,
-            "c": lambda s: s.encode()}
+            "c": lambda s: s.encode(),
+            "t": lambda s: _PTYPE[0].index(s.split()[0]) * 25 + _PTYPE[1].index(s.split()[1]) * 5 +
+            _PTYPE[2].index(s.split()[2])}
     rows = [l.rstrip("\r").split("|") for l in text.decode().split("\n") if l != ""]
     return {name: [conv[t](r[f]) for r in rows] for f, name, t in keep}

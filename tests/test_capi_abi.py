@@ -44,7 +44,7 @@ def test_abi_version_and_widths():
 @pytest.mark.parametrize("col,kw", [(1, {}), (3, {}), (6, {}), (8, dict(n_orders=999, order_mode=1)),
                                     (8, dict(n_orders=999, order_mode=2)), (10, dict(n_parts=3000, n_supp=200)),
                                     (31, dict(n_cust=55)), (41, {}), (51, {}), (61, dict(n_supp=200)), (62, {}),
-                                    (11, {}), (12, {}), (13, {}), (33, {}), (34, {}), (22, {})])
+                                    (11, {}), (12, {}), (13, {}), (33, {}), (34, {}), (22, {}), (42, {})])
 def test_host_generator_matches_oracle(orc, col, kw):
     lib = capi.load()
     n, off = 50_000, 777

@@ -119,6 +119,18 @@ def test_cli_q5(orc):
     assert re.search(r"^Q5 \| 60000 rows \(lineitem\)", out, re.M)
 
 
+def test_cli_q7_q8(orc):
+    cu, su, pa, od, li = orc.q8_tables(1_500, 100, 2_000, 15_000, 60_000, 42)
+    out = run("sf1", "q7", "--scale", "0.01")
+    names = capi.NATION_NAMES
+    rows = re.findall(r"^\| ([A-Z ]+?)\s+\| ([A-Z ]+?)\s+\|\s+(\d+) \| \$\s*(\S+) \|$", out, re.M)
+    assert [(names.index(a), names.index(b), int(y), scaled(r, 4)) for a, b, y, r in rows] == orc.q7(cu, su, od, li)
+    out = run("sf1", "q8", "--scale", "0.01")
+    vols = [(int(y), int(a), int(b)) for y, a, b in re.findall(r"^volume (\d+): (-?\d+) of (-?\d+)$", out, re.M)]
+    assert vols == orc.q8(cu, su, pa, od, li)
+    assert re.search(r"^Q8 \| 60000 lineitem", out, re.M)
+
+
 def test_cli_q10(orc):
     cu, od, li = orc.q10_tables(1_500, 15_000, 60_000, 42)
     top, n = orc.q10(cu, od, li)
@@ -204,6 +216,10 @@ def test_cli_reads_tbl_files(orc, tmp_path):
     names = capi.NATION_NAMES
     rows5 = re.findall(r"^\| ([A-Z ]+?)\s+\| \$\s*(\S+) \|$", out, re.M)
     assert [(names.index(n), scaled(r, 4)) for n, r in rows5] == orc.q5(cu, su, od, li)
+    out = run("q7", "--data", d)
+    rows7 = re.findall(r"^\| ([A-Z ]+?)\s+\| ([A-Z ]+?)\s+\|\s+(\d+) \| \$\s*(\S+) \|$", out, re.M)
+    assert [(names.index(a), names.index(b), int(y), scaled(r, 4)) for a, b, y, r in rows7] == \
+        orc.q7(cu, su, od, {k: li[k] for k in ("order_key", "supp_key", "ship_date", "ext_price", "discount")})
     out = run("q10", "--data", d)
     top10, n10 = orc.q10(cu, od, li)
     assert int(re.search(r"Customers with returned revenue: (\d+)", out).group(1)) == n10

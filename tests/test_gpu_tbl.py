@@ -22,7 +22,7 @@ def tables(orc):
         "orders": dict(order_key=orc.gen(30, n_or, 3), cust_key=orc.gen(31, n_or, 3, n_cust=n_cu),
                        order_date=orc.gen(32, n_or, 3), priority=orc.gen(33, n_or, 3), comment=orc.gen(34, n_or, 3)),
         "customer": dict(cust_key=orc.gen(20, n_cu, 3), segment=orc.gen(21, n_cu, 3), nation=orc.gen(22, n_cu, 3)),
-        "part": dict(part_key=orc.gen(40, n_pa, 3), flag=orc.gen(41, n_pa, 3)),
+        "part": dict(part_key=orc.gen(40, n_pa, 3), flag=orc.gen(41, n_pa, 3), type=orc.gen(42, n_pa, 3)),
         "supplier": dict(supp_key=orc.gen(50, n_su, 3), nation=orc.gen(51, n_su, 3)),
         "partsupp": dict(part_key=orc.gen(60, 4 * n_pa, 3), supp_key=orc.gen(61, 4 * n_pa, 3, n_supp=n_su),
                          supply_cost=orc.gen(62, 4 * n_pa, 3)),

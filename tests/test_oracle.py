@@ -37,7 +37,7 @@ def test_generator_matches_golden(orc):
         assert sk[:8].tolist() == cols["supp_key"]["head"]
         assert [x.decode() for x in orc.gen(34, 4, seed, off)] == cols["o_comment"]["head"], key
         for name, cid in (("commit_date", 11), ("receipt_date", 12), ("ship_mode", 13), ("o_priority", 33),
-                          ("c_nation", 22)):
+                          ("c_nation", 22), ("p_type", 42)):
             v = orc.gen(cid, 64, seed, off)
             assert v[:8].tolist() == cols[name]["head"], (key, name)
             assert int(v.astype(np.int64).sum()) == cols[name]["sum"], (key, name)
@@ -123,6 +123,61 @@ def test_q5_pinned_to_reference_kernels(orc, sizes, seed, window, mask):
                li["discount"].ctypes.data, *window, mask, 8, 4, theirs.ctypes.data)
     assert np.array_equal(mine > 0, theirs > 0)
     np.testing.assert_allclose(theirs, mine / 10000.0, rtol=1e-4)
+
+
+ASIA = (1 << 8) | (1 << 9) | (1 << 12) | (1 << 18) | (1 << 21)
+
+
+def test_q7_q8_match_golden(orc):
+    t = orc.q8_tables(400, 40, 600, 3000, 12000, 42)
+    assert orc.q7(t[0], t[1], t[3], t[4]) == [tuple(r[:3]) + (int(r[3]),) for r in GOLDEN["q7"]["400_40_600_3000_12000_42"]]
+    t = orc.q8_tables(400, 40, 600, 3000, 12000, 5)
+    assert orc.q7(t[0], t[1], t[3], t[4], 17, 18, 0, 2556) == \
+        [tuple(r[:3]) + (int(r[3]),) for r in GOLDEN["q7"]["400_40_600_3000_12000_5_peru_china_all"]]
+    t = orc.q8_tables(400, 40, 300, 3000, 12000, 42)
+    assert orc.q8(*t, part_type=7) == [(y, int(a), int(b)) for y, a, b in GOLDEN["q8"]["400_40_300_3000_12000_42_type7"]]
+    t = orc.q8_tables(500, 40, 300, 4000, 16000, 9)
+    assert orc.q8(*t, 12, ASIA, 103, 366, 2191) == \
+        [(y, int(a), int(b)) for y, a, b in GOLDEN["q8"]["500_40_300_4000_16000_9_japan_asia_1993_1997"]]
+
+
+@pytest.mark.parametrize("sizes,seed", [((400, 40, 600, 3000, 12000), 42), ((5000, 400, 8000, 50000, 200000), 7)])
+def test_q7_pinned_to_reference_kernels(orc, sizes, seed):
+    """Q7 bins (FRANCE/GERMANY, 1995-1996: the years the reference's kernel bins) against its
+    kernels, within float32 tolerance; which bins are nonzero, exactly."""
+    ref = need_ref(orc)
+    cu, su, pa, od, li = orc.q8_tables(*sizes, seed)
+    mine = {(s, y): r for s, c, y, r in orc.q7(cu, su, od, li)}
+    bins = np.zeros(4, np.float32)
+    ref.ref_q7(len(cu["cust_key"]), cu["cust_key"].ctypes.data, cu["nation"].ctypes.data, len(su["supp_key"]),
+               su["supp_key"].ctypes.data, su["nation"].ctypes.data, len(od["order_key"]), od["order_key"].ctypes.data,
+               od["cust_key"].ctypes.data, len(li["order_key"]), li["order_key"].ctypes.data, li["supp_key"].ctypes.data,
+               li["ship_date"].ctypes.data, li["ext_price"].ctypes.data, li["discount"].ctypes.data, orc.FRANCE,
+               orc.GERMANY, 1096, 1826, 8, 4, bins.ctypes.data)
+    want = np.array([mine.get((orc.FRANCE, 1995), 0), mine.get((orc.FRANCE, 1996), 0),
+                     mine.get((orc.GERMANY, 1995), 0), mine.get((orc.GERMANY, 1996), 0)], np.float64) / 10000.0
+    assert np.array_equal(bins > 0, want > 0)
+    np.testing.assert_allclose(bins, want, rtol=1e-4)
+
+
+@pytest.mark.parametrize("sizes,seed,ptype", [((3000, 200, 2000, 30000, 120000), 42, 103),
+                                              ((5000, 400, 1000, 50000, 200000), 7, 7)])
+def test_q8_pinned_to_reference_kernels(orc, sizes, seed, ptype):
+    """Q8 per-year nation and total volume (BRAZIL in AMERICA, 1995-1996) against the reference's
+    kernels, within float32 tolerance."""
+    ref = need_ref(orc)
+    cu, su, pa, od, li = orc.q8_tables(*sizes, seed)
+    mine = orc.q8(cu, su, pa, od, li, part_type=ptype)
+    bins = np.zeros(4, np.float32)
+    ref.ref_q8(len(cu["cust_key"]), cu["cust_key"].ctypes.data, cu["nation"].ctypes.data, len(su["supp_key"]),
+               su["supp_key"].ctypes.data, su["nation"].ctypes.data, len(pa["part_key"]), pa["part_key"].ctypes.data,
+               pa["type"].ctypes.data, len(od["order_key"]), od["order_key"].ctypes.data, od["cust_key"].ctypes.data,
+               od["order_date"].ctypes.data, len(li["order_key"]), li["order_key"].ctypes.data,
+               li["part_key"].ctypes.data, li["supp_key"].ctypes.data, li["ext_price"].ctypes.data,
+               li["discount"].ctypes.data, 1096, 1826, orc.AMERICA, orc.BRAZIL, ptype, 8, 4, bins.ctypes.data)
+    want = np.array([mine[0][1], mine[1][1], mine[0][2], mine[1][2]], np.float64) / 10000.0
+    assert want[2] > 0 and np.array_equal(bins > 0, want > 0)
+    np.testing.assert_allclose(bins, want, rtol=1e-4)
 
 
 def test_q10_matches_golden(orc):

@@ -30,3 +30,11 @@ def test_orders_priority_round_trip_cpu():
     got = orc.parse_tbl_cpu("orders", orc.format_tbl("orders", od))
     for k, v in od.items():
         assert np.array_equal(np.asarray(got[k]), v), k
+
+
+def test_part_type_round_trip_cpu():
+    pa = dict(part_key=orc.gen(40, 600, 4), flag=orc.gen(41, 600, 4), type=orc.gen(42, 600, 4))
+    got = orc.parse_tbl_cpu("part", orc.format_tbl("part", pa))
+    for k, v in pa.items():
+        assert np.array_equal(np.asarray(got[k]), v), k
+    assert orc.parse_tbl_cpu("part", b"1|x|M|B|ECONOMY ANODIZED STEEL|1|C|1.00|c|")["type"] == [103]
