@@ -84,3 +84,15 @@ def test_create_without_a_gpu_reports_no_device():
     ctx = C.c_void_p()
     assert lib.gpudb_create(0, C.byref(ctx)) == capi.E_NODEVICE
     assert not ctx.value
+
+
+def test_nation_region_and_part_type_helpers():
+    """The host helpers behind the Q5/Q7/Q8 parameters: the TPC-H nation -> region table
+    (five nations per region), region masks and p_type codes (GPUDB_PART_TYPE)."""
+    assert sorted(capi.NATION_REGION.count(r) for r in range(5)) == [5] * 5
+    assert capi.region_mask("ASIA") == (1 << 8) | (1 << 9) | (1 << 12) | (1 << 18) | (1 << 21)
+    assert capi.region_mask(1) == (1 << 1) | (1 << 2) | (1 << 3) | (1 << 17) | (1 << 24)
+    assert sum(capi.region_mask(r) for r in capi.REGION_NAMES) == (1 << 25) - 1
+    assert capi.part_type("ECONOMY ANODIZED STEEL") == 103 == 4 * 25 + 0 * 5 + 3
+    assert capi.part_type("STANDARD ANODIZED TIN") == 0 and capi.part_type("PROMO BRUSHED COPPER") == 149
+    assert capi.NATION_NAMES.index("BRAZIL") == 2 and capi.NATION_NAMES.index("FRANCE") == 6
