@@ -299,6 +299,14 @@ void runQ12Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
+namespace {
+// TPC-H nation table names by nation key (Q5, Q7 output).
+const char* const kNationNames[GPUDB_NATIONS] = {
+    "ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
+    "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
+    "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES"};
+}  // namespace
+
 void runQ5Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("\n--- Running TPC-H Query 5 Benchmark ---\n");
   const Scale& s = o.scale;
@@ -342,10 +350,6 @@ void runQ5Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   const double gen_ms = now_ms() - t0;
   std::printf("Loaded %" PRIu64 " customers, %" PRIu64 " suppliers, %" PRIu64 " orders, %" PRIu64 " lineitem rows.\n",
               cu.n_rows, su.n_rows, orr.n_rows, L.li.n_rows);
-  static const char* nations[GPUDB_NATIONS] = {
-      "ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
-      "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
-      "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES"};
   // ASIA (TPC-H nation table: INDIA, INDONESIA, JAPAN, CHINA, VIETNAM), orders of 1994
   const gpudb_q5_params p{731, 1096, (1u << 8) | (1u << 9) | (1u << 12) | (1u << 18) | (1u << 21), 0};
   gpudb_q5_result r{};
@@ -362,18 +366,13 @@ void runQ5Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   std::printf("+----------------+---------------------+\n");
   std::printf("| n_name         |             revenue |\n");
   std::printf("+----------------+---------------------+\n");
-  for (int n : order) std::printf("| %-14s | $%18s |\n", nations[n], fixed(r.revenue[n], 4).c_str());
+  for (int n : order) std::printf("| %-14s | $%18s |\n", kNationNames[n], fixed(r.revenue[n], 4).c_str());
   std::printf("+----------------+---------------------+\n");
   std::printf("\nQ5 | %" PRIu64 " rows (lineitem)\n", L.li.n_rows);
   printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
 }
 
 namespace {
-const char* const kNationNames[GPUDB_NATIONS] = {
-    "ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "ETHIOPIA", "FRANCE", "GERMANY", "INDIA",
-    "INDONESIA", "IRAN", "IRAQ", "JAPAN", "JORDAN", "KENYA", "MOROCCO", "MOZAMBIQUE", "PERU", "CHINA",
-    "ROMANIA", "SAUDI ARABIA", "VIETNAM", "RUSSIA", "UNITED KINGDOM", "UNITED STATES"};
-
 // Customer (key, nation), supplier (key, nation) and orders (key, customer, date): generated,
 // or parsed from the .tbl files (Q7, Q8).
 struct Dims {
