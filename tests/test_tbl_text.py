@@ -38,3 +38,15 @@ def test_part_type_round_trip_cpu():
     for k, v in pa.items():
         assert np.array_equal(np.asarray(got[k]), v), k
     assert orc.parse_tbl_cpu("part", b"1|x|M|B|ECONOMY ANODIZED STEEL|1|C|1.00|c|")["type"] == [103]
+
+
+def test_customer_supplier_nation_round_trip_cpu():
+    cu = dict(cust_key=orc.gen(20, 400, 6), segment=orc.gen(21, 400, 6), nation=orc.gen(22, 400, 6))
+    got = orc.parse_tbl_cpu("customer", orc.format_tbl("customer", cu))
+    for k, v in cu.items():
+        assert np.array_equal(np.asarray(got[k]), v), k
+    assert set(np.unique(cu["nation"])) <= set(range(25))
+    su = dict(supp_key=orc.gen(50, 300, 6), nation=orc.gen(51, 300, 6))
+    got = orc.parse_tbl_cpu("supplier", orc.format_tbl("supplier", su))
+    for k, v in su.items():
+        assert np.array_equal(np.asarray(got[k]), v), k
