@@ -1,14 +1,14 @@
 // gpudb_q6_sum_noalloc: the Q6-like filtered sum for callers that cannot allocate.
 //
-// Some callers cannot call cudaMalloc at all: code that runs while a CUDA stream is being
-// captured into a graph (an allocation would break the capture), host programs embedded in
-// a process whose device memory is owned and budgeted by someone else (a database server
-// whose memory manager hands out all of the GPU), and plugins loaded where no context
-// object of this library exists. This entry point needs neither a context nor any
-// allocation: the caller passes the device columns and a device output buffer, and the
-// only scratch memory (the per-block partial sums and the last-block ticket) is a
-// file-scope __device__ array of fixed size that every GPU which loads this library holds
-// until the process exits.
+// Some callers cannot call cudaMalloc at all: host programs embedded in a process whose
+// device memory is owned and budgeted by someone else (a database server whose memory
+// manager hands out all of the GPU, where a stray allocation would fail or push the server
+// over its budget), and plugins loaded where no context object of this library exists
+// (the context is what owns this library's scratch buffers). This entry point needs
+// neither a context nor any allocation: the caller passes the device columns and a device
+// output buffer, and the only scratch memory (the per-block partial sums and the last-block
+// ticket) is a file-scope __device__ array of fixed size that every GPU which loads this
+// library holds until the process exits.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -98,7 +98,9 @@ __global__ void __launch_bounds__(kThreads) q6_noalloc_kernel(const int32_t* __r
   }
 }
 
-// Device address of g_q6_scratch, looked up once per device (with that device current).
+// Device address of g_q6_scratch, looked up once per device (with that device current) and
+// kept for the life of the process: a device reset (cudaDeviceReset) after the first call
+// on that device is not supported, since the array may then load at another address.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_scratch_addr[kMaxDevices] = {};
@@ -134,6 +136,9 @@ extern "C" int gpudb_q6_sum_noalloc(const gpudb_lineitem* li, const gpudb_q6_par
     // nothing to scan: the totals are zero
     return cudaMemsetAsync(out, 0, 2 * sizeof(int64_t), s) == cudaSuccess ? GPUDB_OK : GPUDB_E_CUDA;
   }
+  // An error that the caller's own earlier CUDA work left in the runtime's last-error slot
+  // is the caller's: it is neither reported as this call's failure nor cleared here.
+  const bool clean_before = cudaPeekAtLastError() == cudaSuccess;
   // the ticket must start at zero; the partials are fully rewritten by each launch
   if (cudaMemsetAsync(scratch, 0, sizeof(unsigned), s) != cudaSuccess) return GPUDB_E_CUDA;
   const unsigned grid = (unsigned)((li->n_rows + kRowsPerBlock - 1) / kRowsPerBlock);
@@ -141,5 +146,6 @@ extern "C" int gpudb_q6_sum_noalloc(const gpudb_lineitem* li, const gpudb_q6_par
   const Params pp{p->ship_lo, p->ship_hi, p->disc_lo, p->disc_hi, p->qty_lt};
   q6_noalloc_kernel<<<grid, kThreads, 0, s>>>(li->ship_date, li->discount, li->quantity, li->ext_price, li->n_rows, pp,
                                               vec, static_cast<unsigned char*>(scratch), out);
+  if (!clean_before) return GPUDB_OK;
   return cudaGetLastError() == cudaSuccess ? GPUDB_OK : GPUDB_E_CUDA;
 }

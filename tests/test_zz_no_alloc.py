@@ -1,6 +1,6 @@
 """gpudb_q6_sum_noalloc: the filtered sum for callers that cannot allocate device memory
-(stream capture in progress, device memory owned by another allocator, no gpudb context).
-Its result must equal the allocating entry point gpudb_q6_sum exactly, on consecutive calls
+(device memory owned and budgeted by another memory manager, or no gpudb context). Its
+result must equal the allocating entry point gpudb_q6_sum exactly, on consecutive calls
 that share the static scratch array. This file sorts last so that a failure here comes
 after every other test has run."""
 import ctypes as C
@@ -33,6 +33,23 @@ def test_noalloc_matches_allocating_entry_point(orc):
                 want = eng.q6(view, lo, hi, dlo, dhi, qlt)
                 assert got == want
                 assert got == orc.q6(sub, lo, hi, dlo, dhi, qlt)
+        eng.device_free(out)
+
+
+def test_noalloc_at_its_row_limit():
+    """Exactly 67,108,864 rows: every block of the largest grid writes its partial and the
+    last one folds them all; two calls in a row agree with the allocating entry point."""
+    from gpudbmetalbenchmark_b200.engine import Q6_COLS
+    n = 67_108_864
+    with Engine(0) as eng:
+        t = eng.generate("lineitem", n, seed=5, columns=Q6_COLS)
+        out = eng.device_array(16)
+        stream = eng.lib.gpudb_stream(eng.ctx)
+        for lo, hi, dlo, dhi, qlt in ((365, 730, 5, 7, 24), (0, 2527, 0, 10, 51)):
+            p = capi.Q6Params(lo, hi, dlo, dhi, qlt)
+            assert _noalloc(eng, t.lineitem(), p, out, stream) == capi.OK
+            got = tuple(int(x) for x in eng.to_host(out, 2, np.int64))
+            assert got == eng.q6(t, lo, hi, dlo, dhi, qlt)
         eng.device_free(out)
 
 
