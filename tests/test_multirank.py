@@ -1,7 +1,10 @@
 """The multi-GPU form of the scans on CPU: world size 2 over gloo. Each rank generates its
-row shard [rank*rows, (rank+1)*rows) of one seeded table (bench.py's weak-scaling layout),
-computes its exact partial results, and the gathered partials must equal the result over
-the whole table. Also covers the max-over-ranks timing reduction used by bench.py."""
+row shard [rank*rows, (rank+1)*rows) of one seeded table with the engine's host generator
+(bench.py's weak-scaling layout), computes its partial results (the oracle stands in for
+the GPU here), and the partials travel as the engine's result structs; rank 0 merges them
+with the engine's own merge functions (gpudb_q6_result_merge / gpudb_q1_result_merge), and
+the merge must equal the result over the whole table. Also covers the max-over-ranks
+timing reduction used by bench.py."""
 import os
 import socket
 
@@ -16,6 +19,18 @@ def _free_port():
     port = s.getsockname()[1]
     s.close()
     return port
+
+
+def q1_struct(capi, d):
+    """gpudb_q1_result of a {(flag, status): sums} dict (groups in (flag, status) order)."""
+    r = capi.Q1Result()
+    for (f, st), v in sorted(d.items()):
+        g = r.groups[r.n_groups]
+        r.n_groups += 1
+        g.flag, g.status, g.count = f, st, v["count"]
+        for name in ("sum_qty", "sum_base_price", "sum_disc_price", "sum_charge", "sum_discount"):
+            getattr(g, name).set(v[name])
+    return r
 
 
 def _worker(rank, world, port, rows, out):
@@ -42,10 +57,10 @@ def _worker(rank, world, port, rows, out):
         a = np.empty(rows, dtype=orc.DT[lib.gpudb_column_width(cid)])
         assert lib.gpudb_generate(None, C.byref(spec), cid, a.ctypes.data, capi.MEM_HOST) == capi.OK
         cols[name] = a
-    part6 = orc.q6(cols)
-    part1 = orc.q1(cols)
+    r6 = capi.Q6Result(*orc.q6(cols))
+    r1 = q1_struct(capi, orc.q1(cols))
     gathered = [None] * world
-    dist.all_gather_object(gathered, (part6, part1))
+    dist.all_gather_object(gathered, (bytes(r6), bytes(r1)))
     # the bench's timing reduction: max over ranks
     t = torch.tensor([float(rank + 1)], dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -68,17 +83,15 @@ def test_two_rank_shards_add_up_to_the_whole_table(orc):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert tmax == 2.0
+    from gpudbmetalbenchmark_b200 import capi
+    from gpudbmetalbenchmark_b200.engine import q1_to_dict
     whole = orc.lineitem(world * rows, seed=42)
-    rev = sum(g[0][0] for g in gathered)
-    matched = sum(g[0][1] for g in gathered)
-    assert (rev, matched) == orc.q6(whole)
-    merged = {}
-    for _, q1 in gathered:
-        for k, v in q1.items():
-            m = merged.setdefault(k, dict.fromkeys(v, 0))
-            for f, x in v.items():
-                m[f] += x
-    assert merged == orc.q1(whole)
+    p6 = [capi.Q6Result.from_buffer_copy(g[0]) for g in gathered]
+    p1 = [capi.Q1Result.from_buffer_copy(g[1]) for g in gathered]
+    m6 = capi.merge_q6(p6)
+    assert (m6.revenue, m6.rows_matched) == orc.q6(whole)
+    assert q1_to_dict(capi.merge_q1(p1)) == orc.q1(whole)
+    assert q1_to_dict(capi.merge_q1(p1[::-1])) == orc.q1(whole)
 
 
 def _leaving_worker(rank, world, port, out):
