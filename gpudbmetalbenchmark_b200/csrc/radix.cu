@@ -22,7 +22,7 @@ namespace {
 constexpr int kPJThreads = 256;
 constexpr uint32_t kPJCap = 4096;          // shared hash-table slots (32 KB)
 constexpr uint32_t kChunk = kPJCap / 2;    // build rows per chunk: <= 50% load
-constexpr uint64_t kRowsPerPartition = 1024;
+constexpr uint64_t kRowsPerPartition = 2048;   // average build rows per partition: one chunk
 
 __device__ __forceinline__ uint32_t pj_slot(int32_t key) { return key_slot(key, kPJCap - 1); }
 
@@ -116,30 +116,39 @@ __global__ void __launch_bounds__(kPJThreads) partition_count_kernel(
 }
 
 struct Sides {
-  int32_t *bk, *brow, *pk, *prow;
+  int32_t *bk, *brow, *pk, *prow;   // rows: null when only keys are partitioned
   uint32_t *boff, *poff;
 };
 
-// Partitions both sides (row ids as payload) with `bits` bits into scratch buffers.
-int partition_both(Call& call, const int32_t* build, uint64_t nb, const int32_t* probe, uint64_t np, int bits, Sides* s) {
+// Partitions both sides with `bits` bits into scratch buffers: keys only, or keys with
+// their row ids as payload.
+int partition_both(Call& call, const int32_t* build, uint64_t nb, const int32_t* probe, uint64_t np, int bits,
+                   bool rows, Sides* s) {
   gpudb_ctx* ctx = call.ctx();
   const uint64_t parts = 1ull << bits;
   const size_t nmax = std::max<uint64_t>(std::max(nb, np), 1);
+  const int k = rows ? 2 : 1;
   void *keys, *offs;
-  int rc = scratch(ctx, "rjoin.keys", (2 * nb + 2 * np + 2 * nmax + 64) * sizeof(int32_t), &keys);
+  int rc = scratch(ctx, "rjoin.keys", (size_t)k * (nb + np + nmax + 48) * sizeof(int32_t), &keys);
   if (!rc) rc = scratch(ctx, "rjoin.offs", (2 * (parts + 1) + 64) * sizeof(uint32_t), &offs);
   if (rc) return rc;
-  int32_t* k = static_cast<int32_t*>(keys);
-  s->bk = k;
-  s->brow = s->bk + nb + 16;
-  s->pk = s->brow + nb + 16;
-  s->prow = s->pk + np + 16;
-  int32_t* ktmp = s->prow + np + 16;
-  int32_t* ptmp = ktmp + nmax;
+  int32_t* p = static_cast<int32_t*>(keys);
+  auto take = [&p](uint64_t n) { int32_t* q = p; p += n + 16; return q; };
+  s->bk = take(nb);
+  s->pk = take(np);
+  int32_t* ktmp = take(nmax);
+  s->brow = rows ? take(nb) : nullptr;
+  s->prow = rows ? take(np) : nullptr;
+  int32_t* ptmp = rows ? take(nmax) : nullptr;
   s->boff = static_cast<uint32_t*>(offs);
   s->poff = s->boff + parts + 16;
-  rc = radix_partition_run<int32_t>(call, build, nullptr, nb, nullptr, bits, s->bk, s->brow, s->boff, ktmp, ptmp);
-  if (!rc) rc = radix_partition_run<int32_t>(call, probe, nullptr, np, nullptr, bits, s->pk, s->prow, s->poff, ktmp, ptmp);
+  if (rows) {
+    rc = radix_partition_run<int32_t>(call, build, nullptr, nb, nullptr, bits, s->bk, s->brow, s->boff, ktmp, ptmp);
+    if (!rc) rc = radix_partition_run<int32_t>(call, probe, nullptr, np, nullptr, bits, s->pk, s->prow, s->poff, ktmp, ptmp);
+  } else {
+    rc = radix_partition_keys(call, build, nb, bits, s->bk, s->boff, ktmp);
+    if (!rc) rc = radix_partition_keys(call, probe, np, bits, s->pk, s->poff, ktmp);
+  }
   return rc;
 }
 
@@ -150,7 +159,7 @@ int radix_join_count(Call& call, const int32_t* build_keys, uint64_t n_build, co
   if (n_build == 0 || n_probe == 0) return GPUDB_OK;
   const int bits = radix_bits_for(n_build, kRowsPerPartition);
   Sides s;
-  int rc = partition_both(call, build_keys, n_build, probe_keys, n_probe, bits, &s);
+  int rc = partition_both(call, build_keys, n_build, probe_keys, n_probe, bits, false, &s);
   if (rc) return rc;
   void* flags = nullptr;
   rc = scratch(call.ctx(), "rjoin.flags", n_probe + 16, &flags);
@@ -199,7 +208,7 @@ extern "C" int gpudb_radix_join_pairs(gpudb_ctx* ctx, const int32_t* build_keys,
   if (n_build && n_probe) {
     const int bits = radix_bits_for(n_build, kRowsPerPartition);
     Sides s;
-    rc = partition_both(call, build_keys, n_build, probe_keys, n_probe, bits, &s);
+    rc = partition_both(call, build_keys, n_build, probe_keys, n_probe, bits, true, &s);
     if (rc) return rc;
     GPUDB_LAUNCH(call, partition_pairs_kernel, 1u << bits, kPJThreads, 0, (const int32_t*)s.bk, (const int32_t*)s.brow,
                  (const uint32_t*)s.boff, (const int32_t*)s.pk, (const int32_t*)s.prow, (const uint32_t*)s.poff,

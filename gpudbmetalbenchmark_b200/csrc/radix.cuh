@@ -4,19 +4,26 @@
 // a single-threadgroup Blelloch scan, and an atomic-cursor scatter (unstable, one 4-byte
 // write per row anywhere in memory).
 //
-// B200 design: partition p = key_hash32(key) & (2^bits - 1) (the reference's hash), in
-// LSD passes of at most 8 bits, so the fan-out of a pass (256) fits the per-block counters
-// and staging buffer in shared memory. Per pass:
-//   radix_hist_kernel   per-tile bucket counts (shared atomics), bucket-major [b][tile];
-//   exclusive_scan      over that array: global start of every (bucket, tile) piece;
-//   radix_scatter_kernel ranks the tile's rows inside their bucket in input order
-//                        (__match_any_sync per warp + per-bucket warp prefix in shared
-//                        memory), stages the tile bucket-sorted in shared memory, then
-//                        writes each bucket's run contiguously (coalesced stores).
-// Passes are stable, so after the last pass rows are ordered by p with input order kept
-// inside each partition. Row counts may live on the device (n_dev): grids are sized from
-// a host upper bound and tiles past the device count do no work.
+// B200 design. Partition p = key_hash32(key) & (2^bits - 1) (the reference's hash), in LSD
+// passes of at most kRxPassBits bits (one pass up to 1024 partitions). The input is cut into
+// G super-tiles, about one per SM; per pass:
+//   rx_hist_kernel    counts each super-tile's rows per digit (shared-memory atomics; four
+//                     blocks per super-tile, so every SM streams) into hist[digit][G], and
+//                     in the first pass also the rows per final partition;
+//   exclusive_scan    over hist (digit-major): where each (digit, super-tile) run starts;
+//   rx_scatter_kernel one block per super-tile walks its 8192-row sub-tiles in order. Each
+//                     warp ranks its own 512 contiguous rows by digit (__match_any_sync and
+//                     per-warp counters, no atomics), one block-wide scan turns the
+//                     (digit, warp) counts into staged positions, the sub-tile is staged
+//                     digit-sorted in shared memory and written out run by run from
+//                     per-digit cursors that carry across the super-tile's sub-tiles.
+// The order inside a partition is the input order (stable), so later passes and the final
+// result are deterministic. The row source is a template: plain columns (payload = row id
+// when none is given) or a pipeline's filtered fact rows (Q3), so a filter and the first
+// pass share one read of the columns.
 #pragma once
+#include <algorithm>
+
 #include "common.cuh"
 #include "engine.h"
 #include "join_common.cuh"
@@ -24,179 +31,318 @@
 
 namespace gpudb {
 
-constexpr int kRadixThreads = 256;
-constexpr int kRadixItems = 16;
-constexpr int kRadixTile = kRadixThreads * kRadixItems;   // 4096 rows per block
-constexpr int kRadixPassBits = 8;                          // fan-out 256 per pass
+constexpr int kRxThreads = 512;
+constexpr int kRxWarps = kRxThreads / 32;
+constexpr int kRxItems = 16;                            // rows per lane per sub-tile
+constexpr int kRxTile = kRxThreads * kRxItems;          // 8192 rows per sub-tile
+constexpr int kRxWarpRows = kRxTile / kRxWarps;         // 512 contiguous rows per warp
+constexpr int kRxPassBits = 10;                         // fan-out of one pass <= 1024
+constexpr uint32_t kRxMaxF = 1u << kRxPassBits;
+constexpr int kRxFullSmemBits = 13;                     // final-partition counts in shared memory up to 8192
+constexpr int kRxHistSplit = 4;                         // histogram blocks per super-tile
 
-__device__ __forceinline__ uint32_t radix_digit(int32_t key, int shift, uint32_t dmask) {
-  return (key_hash32(key) >> shift) & dmask;
-}
-
-__device__ __forceinline__ uint64_t radix_rows(uint64_t n_max, const uint32_t* n_dev) {
-  return n_dev ? (uint64_t)*n_dev : n_max;
-}
-
-static __global__ void __launch_bounds__(kRadixThreads) radix_hist_kernel(const int32_t* __restrict__ keys, uint64_t n_max,
-                                                                          const uint32_t* n_dev, int shift, int dbits,
-                                                                          uint32_t tiles, uint32_t* hist) {
-  __shared__ uint32_t cnt[1 << kRadixPassBits];
-  const uint32_t buckets = 1u << dbits, dmask = buckets - 1;
-  for (uint32_t b = threadIdx.x; b < buckets; b += kRadixThreads) cnt[b] = 0;
-  __syncthreads();
-  const uint64_t n = radix_rows(n_max, n_dev);
-  const uint64_t base = (uint64_t)blockIdx.x * kRadixTile;
-#pragma unroll 4
-  for (int j = 0; j < kRadixItems; j++) {
-    const uint64_t r = base + (uint64_t)j * kRadixThreads + threadIdx.x;
-    if (r < n) atomicAdd(&cnt[radix_digit(keys[r], shift, dmask)], 1u);
-  }
-  __syncthreads();
-  for (uint32_t b = threadIdx.x; b < buckets; b += kRadixThreads) hist[(size_t)b * tiles + blockIdx.x] = cnt[b];
-}
-
-// offsets: exclusive scan of hist (bucket-major) with the grand total at [buckets*tiles].
+// Plain columns: keys, and a payload column or (null) the row number. Rows [0, n) with
+// n = *n_dev when given (a count left on the device by an earlier kernel), capped at n_max.
 template <class P>
-__global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const int32_t* __restrict__ keys_in,
-                                                                      const P* __restrict__ pay_in, uint64_t n_max,
-                                                                      const uint32_t* n_dev, int shift, int dbits,
-                                                                      uint32_t tiles, const uint32_t* __restrict__ offsets,
-                                                                      int32_t* __restrict__ keys_out, P* __restrict__ pay_out) {
-  extern __shared__ unsigned long long radix_smem[];
-  P* spay = reinterpret_cast<P*>(radix_smem);                          // kRadixTile
-  int32_t* skey = reinterpret_cast<int32_t*>(spay + kRadixTile);       // kRadixTile
-  __shared__ uint32_t tstart[1 << kRadixPassBits];
-  __shared__ uint32_t run[1 << kRadixPassBits];
-  __shared__ uint32_t wcnt[kRadixThreads / 32][1 << kRadixPassBits];
-  __shared__ uint32_t wt[kRadixThreads / 32];
-  const uint32_t buckets = 1u << dbits, dmask = buckets - 1;
-  const uint64_t n = radix_rows(n_max, n_dev);
-  const uint64_t base = (uint64_t)blockIdx.x * kRadixTile;
-  if (base >= n) return;   // uniform across the block
-  const uint32_t tile_n = (uint32_t)((n - base) < (uint64_t)kRadixTile ? (n - base) : (uint64_t)kRadixTile);
+struct ColumnSource {
+  const int32_t* keys;
+  const P* pay;
+  uint64_t n_max;
+  const uint32_t* n_dev;
+  __device__ __forceinline__ uint64_t rows() const {
+    return n_dev ? min((uint64_t)*n_dev, n_max) : n_max;
+  }
+  __device__ __forceinline__ bool key(uint64_t r, int32_t& k) const {
+    k = __ldg(keys + r);   // cached: the scatter pass reads the keys again
+    return true;
+  }
+  __device__ __forceinline__ P payload(uint64_t r) const { return pay ? __ldcs(pay + r) : (P)r; }
+};
+
+__device__ __forceinline__ uint32_t rx_digit(int32_t key, int shift, uint32_t mask) {
+  return (key_hash32(key) >> shift) & mask;
+}
+
+// Inclusive scan of one value per thread across a block of NT threads.
+template <int NT>
+__device__ __forceinline__ uint32_t rx_block_scan(uint32_t v, uint32_t* warp_tot) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // this tile's bucket counts -> exclusive prefix (one bucket per thread; buckets <= 256)
-  {
-    uint32_t c = 0;
-    const uint32_t b = threadIdx.x;
-    if (b < buckets) {
-      const size_t i = (size_t)b * tiles + blockIdx.x;
-      c = offsets[i + 1] - offsets[i];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(FULL_MASK, v, d);
+    if (lane >= d) v += o;
+  }
+  if (lane == 31) warp_tot[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < NT / 32 ? warp_tot[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(FULL_MASK, w, d);
+      if (lane >= d) w += o;
     }
-    const uint32_t inc = block_inclusive_scan<uint32_t>(c, wt);
-    if (b < buckets) { tstart[b] = inc - c; run[b] = 0; }
+    if (lane < NT / 32) warp_tot[lane] = w;
   }
   __syncthreads();
-  for (int j = 0; j < kRadixItems; j++) {
-    for (int i = threadIdx.x; i < (kRadixThreads / 32) * (1 << kRadixPassBits); i += kRadixThreads)
-      (&wcnt[0][0])[i] = 0;
-    __syncthreads();
-    const uint32_t rr = (uint32_t)j * kRadixThreads + threadIdx.x;
-    const bool valid = rr < tile_n;
-    const uint64_t r = base + rr;
-    const int32_t key = valid ? keys_in[r] : 0;
-    const uint32_t d = valid ? radix_digit(key, shift, dmask) : (0x10000u + lane);
-    const uint32_t peers = __match_any_sync(FULL_MASK, d);
-    const uint32_t rank = __popc(peers & lanemask_lt());
-    if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    if (threadIdx.x < buckets) {
-      uint32_t s = run[threadIdx.x];
+  if (warp > 0) v += warp_tot[warp - 1];
+  __syncthreads();
+  return v;
+}
+
+// Digit counts of super-tile blockIdx.x / kRxHistSplit (one quarter of it per block) into
+// hist[digit * G + super-tile] (zeroed), and with `full` the rows per final partition
+// (fbits bits; zeroed).
+template <class Src>
+__global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint64_t super_rows, uint32_t G, int shift,
+                                                             int dbits, int fbits, uint32_t* __restrict__ hist,
+                                                             uint32_t* __restrict__ full) {
+  __shared__ uint32_t cnt[kRxMaxF];
+  __shared__ uint32_t fcnt[1u << kRxFullSmemBits];
+  const uint32_t F = 1u << dbits, dmask = F - 1, fmask = (1u << fbits) - 1;
+  const bool fs = full && fbits <= kRxFullSmemBits;
+  for (uint32_t i = threadIdx.x; i < F; i += kRxThreads) cnt[i] = 0;
+  if (fs)
+    for (uint32_t i = threadIdx.x; i <= fmask; i += kRxThreads) fcnt[i] = 0;
+  __syncthreads();
+  const uint32_t g = blockIdx.x / kRxHistSplit, part = blockIdx.x % kRxHistSplit;
+  const uint64_t n = src.rows();
+  const uint64_t quarter = super_rows / kRxHistSplit;
+  const uint64_t r0 = (uint64_t)g * super_rows + part * quarter;
+  const uint64_t r1 = min(r0 + quarter, n);
+  constexpr int U = 8;
+  for (uint64_t r = r0 + threadIdx.x; r < r1; r += (uint64_t)U * kRxThreads) {
+    int32_t k[U];
+    bool v[U];
 #pragma unroll
-      for (int w = 0; w < kRadixThreads / 32; w++) {
-        const uint32_t c = wcnt[w][threadIdx.x];
-        wcnt[w][threadIdx.x] = s;
-        s += c;
+    for (int u = 0; u < U; u++) {
+      const uint64_t rr = r + (uint64_t)u * kRxThreads;
+      v[u] = rr < r1 && src.key(rr, k[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (v[u]) {
+        const uint32_t h = key_hash32(k[u]);
+        atomicAdd(&cnt[(h >> shift) & dmask], 1u);
+        if (fs) atomicAdd(&fcnt[h & fmask], 1u);
+        else if (full) atomicAdd(&full[h & fmask], 1u);
       }
-      run[threadIdx.x] = s;
-    }
-    __syncthreads();
-    if (valid) {
-      const uint32_t lp = tstart[d] + wcnt[warp][d] + rank;
-      skey[lp] = key;
-      spay[lp] = pay_in ? pay_in[r] : (P)r;
-    }
-    __syncthreads();
   }
-  for (uint32_t i = threadIdx.x; i < tile_n; i += kRadixThreads) {
-    const int32_t k = skey[i];
-    const uint32_t b = radix_digit(k, shift, dmask);
-    const uint32_t o = offsets[(size_t)b * tiles + blockIdx.x] + (i - tstart[b]);
-    keys_out[o] = k;
-    pay_out[o] = spay[i];
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < F; b += kRxThreads)
+    if (cnt[b]) atomicAdd(&hist[(size_t)b * G + g], cnt[b]);
+  if (fs)
+    for (uint32_t i = threadIdx.x; i <= fmask; i += kRxThreads)
+      if (fcnt[i]) atomicAdd(&full[i], fcnt[i]);
+}
+
+template <class P, bool PAY>
+__host__ __device__ constexpr size_t rx_scatter_smem(uint32_t F) {
+  return (PAY ? sizeof(P) * kRxTile : 0) + sizeof(int32_t) * kRxTile + sizeof(uint16_t) * kRxWarps * F +
+         sizeof(uint32_t) * F;
+}
+
+// One block per super-tile (see the file comment). offs: exclusive scan of hist.
+template <class Src, class P, bool PAY>
+__global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint64_t super_rows, uint32_t G, int shift,
+                                                                   int dbits, const uint32_t* __restrict__ offs,
+                                                                   int32_t* __restrict__ kout, P* __restrict__ pout) {
+  extern __shared__ __align__(16) unsigned char rx_smem[];
+  const uint32_t F = 1u << dbits, dmask = F - 1;
+  P* spay = reinterpret_cast<P*>(rx_smem);
+  int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + (PAY ? sizeof(P) * kRxTile : 0));
+  uint16_t* wcnt = reinterpret_cast<uint16_t*>(skey + kRxTile);        // [warp][digit]
+  uint32_t* cur = reinterpret_cast<uint32_t*>(wcnt + kRxWarps * F);    // next output row per digit
+  __shared__ uint32_t wt[kRxWarps];
+  __shared__ uint32_t s_total;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t n = src.rows();
+  const uint64_t g0 = (uint64_t)blockIdx.x * super_rows;
+  if (g0 >= n) return;   // uniform across the block
+  const uint64_t g1 = min(g0 + super_rows, n);
+  for (uint32_t d = threadIdx.x; d < F; d += kRxThreads) cur[d] = offs[(size_t)d * G + blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < kRxWarps * F; i += kRxThreads) wcnt[i] = 0;
+  __syncthreads();
+  uint16_t* mine = wcnt + warp * F;
+  const uint32_t dpt = (F + kRxThreads - 1) / kRxThreads;   // digits per thread in the scan
+  for (uint64_t t0 = g0; t0 < g1; t0 += kRxTile) {
+    int32_t key[kRxItems];
+    P pay[kRxItems];
+    uint32_t dr[kRxItems];   // digit << 16 | rank among the warp's rows of that digit; ~0u: no row
+    const uint64_t wb = t0 + (uint64_t)warp * kRxWarpRows + lane;
+#pragma unroll
+    for (int j = 0; j < kRxItems; j++) {
+      const uint64_t r = wb + (uint64_t)j * 32;
+      const bool v = r < g1 && src.key(r, key[j]);
+      dr[j] = v ? 0u : ~0u;
+      if (PAY && v) pay[j] = src.payload(r);
+    }
+    // rank inside the warp, 32 rows at a time in row order: the first lane of each digit
+    // reads and advances the warp's counter for it
+#pragma unroll
+    for (int j = 0; j < kRxItems; j++) {
+      const bool v = dr[j] == 0u;
+      const uint32_t d = v ? rx_digit(key[j], shift, dmask) : 0x10000u + lane;
+      const uint32_t peers = __match_any_sync(FULL_MASK, d);
+      const int leader = __ffs(peers) - 1;
+      uint32_t base = (v && lane == leader) ? (uint32_t)mine[d] : 0u;
+      base = __shfl_sync(FULL_MASK, base, leader);
+      if (v) {
+        if (lane == leader) mine[d] = (uint16_t)(base + __popc(peers));
+        dr[j] = (d << 16) | (base + __popc(peers & lanemask_lt()));
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    // (digit, warp) counts -> staged positions, digit-major: digit d's rows of warp 0, then
+    // of warp 1, ... (row order); wcnt[0][d] becomes the start of digit d
+    {
+      const uint32_t b0 = min(threadIdx.x * dpt, F), b1 = min(b0 + dpt, F);
+      uint32_t s = 0;
+      for (uint32_t b = b0; b < b1; b++)
+#pragma unroll
+        for (int w = 0; w < kRxWarps; w++) s += wcnt[w * F + b];
+      const uint32_t inc = rx_block_scan<kRxThreads>(s, wt);
+      uint32_t run = inc - s;
+      for (uint32_t b = b0; b < b1; b++)
+#pragma unroll
+        for (int w = 0; w < kRxWarps; w++) {
+          const uint32_t c = wcnt[w * F + b];
+          wcnt[w * F + b] = (uint16_t)run;
+          run += c;
+        }
+      if (threadIdx.x == kRxThreads - 1) s_total = inc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kRxItems; j++)
+      if (dr[j] != ~0u) {
+        const uint32_t pos = (uint32_t)mine[dr[j] >> 16] + (dr[j] & 0xFFFFu);
+        skey[pos] = key[j];
+        if (PAY) spay[pos] = pay[j];
+      }
+    __syncthreads();
+    // write out: consecutive threads take consecutive staged rows, i.e. consecutive output
+    // rows inside each digit's run
+    const uint32_t m = s_total;
+    for (uint32_t i = threadIdx.x; i < m; i += kRxThreads) {
+      const int32_t k = skey[i];
+      const uint32_t d = rx_digit(k, shift, dmask);
+      const uint32_t o = cur[d] + (i - (uint32_t)wcnt[d]);
+      kout[o] = k;
+      if (PAY) pout[o] = spay[i];
+    }
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < F; d += kRxThreads) {
+      const uint32_t end = d + 1 < F ? (uint32_t)wcnt[d + 1] : m;
+      cur[d] += end - (uint32_t)wcnt[d];
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kRxWarps * F; i += kRxThreads) wcnt[i] = 0;
+    __syncthreads();
   }
 }
 
-// Full-width partition histogram (2^bits counters): shared counters up to 4096 partitions,
-// global atomics beyond.
-static __global__ void __launch_bounds__(kRadixThreads) part_hist_kernel(const int32_t* __restrict__ keys, uint64_t n_max,
-                                                                         const uint32_t* n_dev, int bits, uint32_t* hist) {
-  __shared__ uint32_t cnt[4096];
-  const uint32_t parts = 1u << bits, pmask = parts - 1;
-  const bool local = parts <= 4096;
-  if (local) {
-    for (uint32_t i = threadIdx.x; i < parts; i += kRadixThreads) cnt[i] = 0;
-    __syncthreads();
-  }
-  const uint64_t n = radix_rows(n_max, n_dev);
-  const uint64_t stride = (uint64_t)gridDim.x * kRadixThreads;
-  for (uint64_t r = (uint64_t)blockIdx.x * kRadixThreads + threadIdx.x; r < n; r += stride) {
-    const uint32_t p = key_hash32(keys[r]) & pmask;
-    if (local) atomicAdd(&cnt[p], 1u);
-    else atomicAdd(&hist[p], 1u);
-  }
-  if (local) {
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < parts; i += kRadixThreads)
-      if (cnt[i]) atomicAdd(&hist[i], cnt[i]);
-  }
+// offsets[b] = where digit b starts (the first super-tile's run), offsets[F] = total.
+static __global__ void rx_starts_kernel(const uint32_t* __restrict__ offs, uint32_t F, uint32_t G,
+                                        const uint32_t* __restrict__ total, uint32_t* __restrict__ offsets) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= F; b += gridDim.x * blockDim.x)
+    offsets[b] = b < F ? offs[(size_t)b * G] : *total;
 }
 
-// Partitions rows [0, n) (n = *n_dev when given, else n_max) into 2^bits partitions.
-// pay == nullptr partitions the row ids. keys_tmp/pay_tmp: n_max elements for the first
-// of two passes. offsets: 2^bits + 1 entries (partition starts, total last).
+// Super-tile size: about one super-tile per SM, whole sub-tiles.
+inline uint64_t rx_super_rows(uint64_t n_max, int sms) {
+  const uint64_t per = (n_max + sms - 1) / std::max(sms, 1);
+  return std::max<uint64_t>(kRxTile, (per + kRxTile - 1) / kRxTile * kRxTile);
+}
+
+// Scratch words for one partitioning of at most n_max rows with `bits` bits.
+inline size_t rx_scratch_words(uint64_t n_max, int bits, int sms) {
+  const uint64_t G = (std::max<uint64_t>(n_max, 1) + rx_super_rows(n_max, sms) - 1) / rx_super_rows(n_max, sms);
+  const size_t hn = (size_t)kRxMaxF * G + 1;
+  const size_t parts = (size_t)1 << bits;
+  return 2 * hn + std::max(scan_tiles_count(hn), scan_tiles_count(parts)) + 8 + parts + 8;
+}
+
+// Partitions the rows of `src` (at most n_max) into 2^bits partitions: keys (and payloads
+// when PAY) to kout/pout, partition starts to offsets[0 .. 2^bits] (the total last). Two
+// passes when bits > kRxPassBits, through ktmp/ptmp (n_max rows each).
+template <class Src, class P, bool PAY>
+int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout, uint32_t* offsets,
+                 int32_t* ktmp, P* ptmp) {
+  gpudb_ctx* ctx = call.ctx();
+  cudaStream_t s = call.stream();
+  const int passes = bits <= kRxPassBits ? 1 : 2;
+  const int d0 = passes == 1 ? bits : (bits + 1) / 2;
+  const uint64_t S = rx_super_rows(n_max, ctx->sm_count);
+  const uint32_t G = (uint32_t)((std::max<uint64_t>(n_max, 1) + S - 1) / S);
+  const size_t hn = (size_t)kRxMaxF * G + 1;
+  const size_t parts = (size_t)1 << bits;
+  void* sc = nullptr;
+  int rc = scratch(ctx, "radix.meta", rx_scratch_words(n_max, bits, ctx->sm_count) * sizeof(uint32_t), &sc);
+  if (rc) return rc;
+  uint32_t* hist = static_cast<uint32_t*>(sc);
+  uint32_t* offs = hist + hn;
+  uint32_t* stmp = offs + hn;
+  uint32_t* full = stmp + std::max(scan_tiles_count(hn), scan_tiles_count(parts)) + 8;
+  for (int pass = 0; pass < passes; pass++) {
+    const int shift = pass == 0 ? 0 : d0;
+    const int dbits = pass == 0 ? d0 : bits - d0;
+    const uint32_t F = 1u << dbits;
+    const size_t hf = (size_t)F * G;
+    int32_t* ko = pass == passes - 1 ? kout : ktmp;
+    P* po = pass == passes - 1 ? pout : ptmp;
+    const size_t smem = rx_scatter_smem<P, PAY>(F);
+    GPUDB_CUDA(ctx, cudaMemsetAsync(hist, 0, hf * sizeof(uint32_t), s));
+    if (pass == 0 && passes > 1) GPUDB_CUDA(ctx, cudaMemsetAsync(full, 0, parts * sizeof(uint32_t), s));
+    uint32_t* fullp = (pass == 0 && passes > 1) ? full : nullptr;
+    if (pass == 0) {
+      GPUDB_LAUNCH(call, (rx_hist_kernel<Src>), G * kRxHistSplit, kRxThreads, 0, src, S, G, shift, dbits, bits, hist,
+                   fullp);
+      rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
+      if (rc) return rc;
+      GPUDB_CUDA(ctx, cudaFuncSetAttribute(rx_scatter_kernel<Src, P, PAY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+      GPUDB_LAUNCH(call, (rx_scatter_kernel<Src, P, PAY>), G, kRxThreads, smem, src, S, G, shift, dbits,
+                   (const uint32_t*)offs, ko, po);
+    } else {
+      // rows of the first pass, in their pass-one order; their count is the first scan's total
+      const uint32_t* total0 = full + parts;   // copied below
+      const ColumnSource<P> s2{ktmp, PAY ? ptmp : nullptr, n_max, total0};
+      GPUDB_LAUNCH(call, (rx_hist_kernel<ColumnSource<P>>), G * kRxHistSplit, kRxThreads, 0, s2, S, G, shift, dbits,
+                   bits, hist, (uint32_t*)nullptr);
+      rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
+      if (rc) return rc;
+      GPUDB_CUDA(ctx, cudaFuncSetAttribute(rx_scatter_kernel<ColumnSource<P>, P, PAY>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      GPUDB_LAUNCH(call, (rx_scatter_kernel<ColumnSource<P>, P, PAY>), G, kRxThreads, smem, s2, S, G, shift, dbits,
+                   (const uint32_t*)offs, ko, po);
+    }
+    if (pass == 0 && passes > 1)
+      GPUDB_CUDA(ctx, cudaMemcpyAsync(full + parts, offs + hf, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  }
+  if (passes == 1) {
+    const uint32_t F = 1u << bits;
+    GPUDB_LAUNCH(call, rx_starts_kernel, (F + 256) / 256, 256, 0, (const uint32_t*)offs, F, G,
+                 (const uint32_t*)(offs + (size_t)F * G), offsets);
+    return GPUDB_OK;
+  }
+  return exclusive_scan<uint32_t, uint32_t>(call, full, parts, offsets, stmp, offsets + parts);
+}
+
+// Plain columns (payload = row id when pay is null); the row count may be on the device.
 template <class P>
 int radix_partition_run(Call& call, const int32_t* keys, const P* pay, uint64_t n_max, const uint32_t* n_dev, int bits,
                         int32_t* keys_out, P* pay_out, uint32_t* offsets, int32_t* keys_tmp, P* pay_tmp) {
-  gpudb_ctx* ctx = call.ctx();
-  cudaStream_t s = call.stream();
-  const uint64_t tiles = std::max<uint64_t>(1, (n_max + kRadixTile - 1) / kRadixTile);
-  const int passes = bits <= kRadixPassBits ? 1 : 2;
-  const int lo_bits = passes == 1 ? bits : bits - kRadixPassBits;
-  const uint32_t parts = 1u << bits;
-  // hist [256 x tiles] + total, its scan, scan scratch, full histogram
-  const size_t hist_n = (size_t)(1u << kRadixPassBits) * tiles + 1;
-  // the scan scratch serves both the per-pass histogram scan and the partition scan
-  const size_t stmp_n = std::max<size_t>(scan_tiles_count(hist_n), scan_tiles_count(parts)) + 8;
-  void* sc = nullptr;
-  int rc = scratch(ctx, "radix.hist", (hist_n * 2 + stmp_n + parts + 1) * sizeof(uint32_t), &sc);
-  if (rc) return rc;
-  uint32_t* hist = static_cast<uint32_t*>(sc);
-  uint32_t* offs = hist + hist_n;
-  uint32_t* stmp = offs + hist_n;
-  uint32_t* phist = stmp + stmp_n;
-  const size_t smem = (size_t)kRadixTile * (sizeof(P) + sizeof(int32_t));
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(radix_scatter_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  for (int pass = 0; pass < passes; pass++) {
-    const int shift = pass == 0 ? 0 : lo_bits;
-    const int dbits = pass == 0 ? lo_bits : kRadixPassBits;
-    const int32_t* kin = pass == 0 ? keys : keys_tmp;
-    const P* pin = pass == 0 ? pay : pay_tmp;
-    int32_t* kout = (pass == passes - 1) ? keys_out : keys_tmp;
-    P* pout = (pass == passes - 1) ? pay_out : pay_tmp;
-    const size_t hn = (size_t)(1u << dbits) * tiles;
-    GPUDB_LAUNCH(call, radix_hist_kernel, (unsigned)tiles, kRadixThreads, 0, kin, n_max, n_dev, shift, dbits,
-                 (uint32_t)tiles, hist);
-    rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hn, offs, stmp, offs + hn);
-    if (rc) return rc;
-    GPUDB_LAUNCH(call, radix_scatter_kernel<P>, (unsigned)tiles, kRadixThreads, smem, kin, pin, n_max, n_dev, shift, dbits,
-                 (uint32_t)tiles, (const uint32_t*)offs, kout, pout);
-  }
-  GPUDB_CUDA(ctx, cudaMemsetAsync(phist, 0, (size_t)parts * 4, s));
-  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n_max + kRadixThreads - 1) / kRadixThreads,
-                                                                       (uint64_t)ctx->sm_count * 8));
-  GPUDB_LAUNCH(call, part_hist_kernel, g, kRadixThreads, 0, keys, n_max, n_dev, bits, phist);
-  return exclusive_scan<uint32_t, uint32_t>(call, phist, parts, offsets, stmp, offsets + parts);
+  const ColumnSource<P> src{keys, pay, n_max, n_dev};
+  return rx_partition<ColumnSource<P>, P, true>(call, src, n_max, bits, keys_out, pay_out, offsets, keys_tmp, pay_tmp);
+}
+
+// Keys only (no payload column is read or written).
+inline int radix_partition_keys(Call& call, const int32_t* keys, uint64_t n, int bits, int32_t* keys_out,
+                                uint32_t* offsets, int32_t* keys_tmp) {
+  const ColumnSource<int32_t> src{keys, nullptr, n, nullptr};
+  return rx_partition<ColumnSource<int32_t>, int32_t, false>(call, src, n, bits, keys_out, nullptr, offsets, keys_tmp,
+                                                             nullptr);
 }
 
 // Partition bits so that the average partition holds about `per_part` rows.

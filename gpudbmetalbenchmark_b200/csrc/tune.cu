@@ -140,12 +140,14 @@ extern "C" int gpudb_autotune(gpudb_ctx* ctx, const gpudb_request* req, uint32_t
       break;
     case GPUDB_PIPE_Q3:
       if (q.q3p.join_mode == GPUDB_JOIN_RADIX) {
-        // fan-outs that keep a partition's build side within a few shared-table chunks
-        // (4096 rows); fewer partitions would re-probe the fact rows once per chunk
+        // fan-outs around the default (about 16K orders rows per partition): fewer partitions
+        // re-probe the fact rows once per shared-table chunk, more than 1024 take a second
+        // partitioning pass
         def = {GPUDB_OPT_RADIX_BITS, 0, 0, 0};
         int lo = 4;
-        while (lo < kRadixMaxBits && (q.q3->od.n_rows >> lo) > 4096) lo++;
-        for (int b = lo; b <= std::min(lo + 6, (int)kRadixMaxBits); b += 2) cands.push_back({GPUDB_OPT_RADIX_BITS, b, 0, 0});
+        while (lo < kRadixMaxBits && (q.q3->od.n_rows >> lo) > 65536) lo++;
+        for (int b = std::max(lo, 8); b <= std::min(lo + 5, (int)kRadixMaxBits); b++)
+          cands.push_back({GPUDB_OPT_RADIX_BITS, b, 0, 0});
       } else {
         def = {GPUDB_OPT_HT_LOAD, 50, 0, 0};
         cands.push_back({GPUDB_OPT_HT_LOAD, 25, 0, 0});

@@ -89,6 +89,25 @@ def test_radix_partition_is_the_oracle_partition(engine, orc, bits, n):
             engine.device_free(x)
 
 
+@pytest.mark.parametrize("bits,n", [(10, 3_000_017), (13, 2_500_001), (7, 1_300_000)])
+def test_radix_partition_large_inputs(engine, orc, bits, n):
+    """Inputs of many 8192-row sub-tiles per super-tile: the per-digit cursors carry the
+    rows of one super-tile across its sub-tiles in input order."""
+    keys = orc.gen(8, n, seed=bits, n_orders=n // 2, order_mode=1)
+    pay = np.arange(n, dtype=np.int32) ^ 0x5A5A
+    dk, dp = engine.to_device(keys), engine.to_device(pay)
+    ko, po, off = (engine.device_array(n * 4), engine.device_array(n * 4), engine.device_array(((1 << bits) + 1) * 4))
+    try:
+        engine.radix_partition(dk, dp, n, bits, ko, po, off)
+        wk, wp, woff = orc.radix_partition(keys, pay, bits)
+        assert np.array_equal(engine.to_host(off, (1 << bits) + 1, np.uint32), woff)
+        assert np.array_equal(engine.to_host(ko, n, np.int32), wk)
+        assert np.array_equal(engine.to_host(po, n, np.int32), wp)
+    finally:
+        for x in (dk, dp, ko, po, off):
+            engine.device_free(x)
+
+
 def test_radix_partition_bad_bits(engine):
     with pytest.raises(capi.GpudbError) as e:
         engine.radix_partition(None, None, 0, 17, 1, 1, 1)
