@@ -226,13 +226,20 @@ void runQ3Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
   const double gen_ms = now_ms() - t0;
   std::printf("Loaded %" PRIu64 " customers, %" PRIu64 " orders, %" PRIu64 " lineitem rows.\n", cu.n_rows, orr.n_rows,
               L.li.n_rows);
-  for (int mode : {GPUDB_JOIN_GLOBAL, GPUDB_JOIN_RADIX}) {
+  // AUTO first: the direct map when the orders' key range fits 30% of device memory (the
+  // reference's choice, src/q3.cpp:246), else the hash table; then the other two modes
+  for (int mode : {GPUDB_JOIN_AUTO, GPUDB_JOIN_GLOBAL, GPUDB_JOIN_RADIX}) {
     gpudb_q3_params p{1, 1170, 1170, 10, mode, 0};
     gpudb_q3_result r{};
     gpudb_timing t{};
     for (int i = 0; i < o.reps; i++) check(ctx, gpudb_q3_join_topk(ctx, &cu, &orr, &L.li, &p, &r, &t, nullptr), "gpudb_q3");
     const double p0 = now_ms();
-    std::printf("\nTPC-H Q3 Results (Top 10, %s join):\n", mode == GPUDB_JOIN_GLOBAL ? "global hash table" : "radix partitioned");
+    const char* name = r.join_mode == GPUDB_JOIN_DIRECT ? "direct map" : r.join_mode == GPUDB_JOIN_RADIX
+                                                                            ? "radix partitioned" : "global hash table";
+    if (mode == GPUDB_JOIN_AUTO)
+      std::printf("Orders map: %d entries (%.1f MB): using the %s join\n", orr.key_max + 1,
+                  (orr.key_max + 1) * 4.0 / (1024.0 * 1024.0), name);
+    std::printf("\nTPC-H Q3 Results (Top 10, %s join):\n", name);
     std::printf("+----------+------------------+------------+--------------+\n");
     std::printf("| orderkey |          revenue | orderdate  | shippriority |\n");
     std::printf("+----------+------------------+------------+--------------+\n");
@@ -241,7 +248,8 @@ void runQ3Benchmark(gpudb_ctx* ctx, const RunOptions& o) {
                   r.rows[i].order_date, 0);
     std::printf("+----------+------------------+------------+--------------+\n");
     std::printf("Total results found: %" PRIu64 "\n", r.n_groups);
-    header(o, "Q3", L.li.n_rows, t, mode == GPUDB_JOIN_GLOBAL ? " (lineitem)" : " (lineitem, radix)");
+    header(o, "Q3", L.li.n_rows, t, r.join_mode == GPUDB_JOIN_GLOBAL ? " (lineitem)"
+                                    : r.join_mode == GPUDB_JOIN_DIRECT ? " (lineitem, direct)" : " (lineitem, radix)");
     printTimingSummary(gen_ms, t.gpu_ms, now_ms() - p0);
   }
 }

@@ -24,8 +24,8 @@
 //  6. q3_hist_kernel: groups and a log-scale revenue histogram of the live table.
 //  7. q3_select_kernel: the slots in the histogram bins that can hold the top-k are
 //     appended, and the last block to finish ranks them.
-// Radix mode partitions both sides by key hash and joins each partition in shared memory
-// (radix.cu).
+// Radix mode partitions both sides by key hash (radix.cuh; the fact filter runs inside the
+// first partitioning pass) and joins each partition in shared memory.
 #include <algorithm>
 #include <cstring>
 
@@ -48,11 +48,24 @@ constexpr uint32_t kSmemCustWords = 12288;     // customer filters up to 48 KB a
 // small filters (1024 threads, two blocks per SM); otherwise the exact bitmap is tested in
 // place (256 threads, several blocks per SM). The three columns load together and the next
 // step's load while this one is tested.
-template <int T, bool SMEM>
+// Where the orders that pass go: (key, date) staging lists (global and radix modes), or in
+// direct mode a dense slot per order ({key, date, revenue 0}, hit count 0) whose number the
+// direct map omap[key] receives, and the order's bit in the order-key bitmap okbm.
+struct FilterOut {
+  int32_t* key;
+  int32_t* date;
+  Q3Slot* slots;
+  uint32_t* hits;
+  int32_t* omap;
+  uint32_t* okbm;
+  int32_t key_max;
+};
+
+template <int T, bool SMEM, bool DIRECT>
 __global__ void __launch_bounds__(T, SMEM ? 2 : 1) orders_filter_kernel(
     const int32_t* __restrict__ okey, const int32_t* __restrict__ ocust, const int32_t* __restrict__ odate, uint64_t n,
     int32_t date_lt, const uint32_t* __restrict__ bitmap, int32_t cust_max, const uint32_t* __restrict__ filt,
-    uint32_t filt_words, bool exact, int32_t* out_key, int32_t* out_date, uint32_t* count, uint32_t* status) {
+    uint32_t filt_words, bool exact, FilterOut out, uint32_t* count, uint32_t* status) {
   extern __shared__ uint32_t sfilt[];
   __shared__ uint32_t sh[33];
   const uint32_t* f = bitmap;
@@ -87,43 +100,61 @@ __global__ void __launch_bounds__(T, SMEM ? 2 : 1) orders_filter_kernel(
     uint32_t take = smem_filter_mask(f, ex, bitmap, cust, ok);
 #pragma unroll
     for (int j = 0; j < kFilterRows; j++)
-      if (((take >> j) & 1u) && key[j] == kEmptyKey) { set_status(status, ST_KEY_RANGE); take &= ~(1u << j); }
+      if (((take >> j) & 1u) && (key[j] == kEmptyKey || (DIRECT && (key[j] < 0 || key[j] > out.key_max)))) {
+        set_status(status, ST_KEY_RANGE);
+        take &= ~(1u << j);
+      }
     uint32_t pos = block_reserve<T>(__popc(take), count, sh);
 #pragma unroll
     for (int j = 0; j < kFilterRows; j++)
-      if (take & (1u << j)) { out_key[pos] = key[j]; out_date[pos] = date[j]; pos++; }
+      if (take & (1u << j)) {
+        if (DIRECT) {
+          *reinterpret_cast<ulonglong2*>(out.slots + pos) =
+              make_ulonglong2((unsigned long long)(uint32_t)key[j] | ((unsigned long long)(uint32_t)date[j] << 32), 0ull);
+          out.hits[pos] = 0;
+          out.omap[key[j]] = (int32_t)pos;
+          const uint32_t bit = 1u << ((uint32_t)key[j] & 31u);
+          if (atomicOr(out.okbm + ((uint32_t)key[j] >> 5), bit) & bit) set_status(status, ST_DUPLICATE);
+        } else {
+          out.key[pos] = key[j];
+          out.date[pos] = date[j];
+        }
+        pos++;
+      }
   }
 }
 
-template <int T, bool SMEM>
+template <int T, bool SMEM, bool DIRECT>
 int launch_orders_filter_as(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_q3_params& p,
-                            const uint32_t* bitmap, const uint32_t* filt, uint32_t fwords, bool exact, int32_t* out_key,
-                            int32_t* out_date, uint32_t* cnt) {
+                            const uint32_t* bitmap, const uint32_t* filt, uint32_t fwords, bool exact,
+                            const FilterOut& out, uint32_t* cnt) {
   gpudb_ctx* ctx = call.ctx();
+  auto kern = orders_filter_kernel<T, SMEM, DIRECT>;
   const size_t smem = SMEM ? (size_t)fwords * 4 : 0;
-  if (SMEM)
-    GPUDB_CUDA(ctx, cudaFuncSetAttribute(orders_filter_kernel<T, SMEM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (SMEM) GPUDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, orders_filter_kernel<T, SMEM>, T, smem));
+  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem));
   const uint64_t per_block = (uint64_t)T * kFilterRows;
   const unsigned g = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>((od.n_rows + per_block - 1) / per_block, (uint64_t)ctx->sm_count * std::max(1, per_sm)));
-  GPUDB_LAUNCH(call, (orders_filter_kernel<T, SMEM>), g, T, smem, od.order_key, od.cust_key, od.order_date, od.n_rows,
-               p.order_date_lt, bitmap, cu.key_max, filt, fwords, exact, out_key, out_date, cnt, call.status());
+  GPUDB_LAUNCH(call, kern, g, T, smem, od.order_key, od.cust_key, od.order_date, od.n_rows, p.order_date_lt, bitmap,
+               cu.key_max, filt, fwords, exact, out, cnt, call.status());
   return GPUDB_OK;
 }
 
-// The orders filter of both join modes, after the customer bitmap: the shared-memory form
+// The orders filter of every join mode, after the customer bitmap: the shared-memory form
 // when the customer filter is at most 48 KB, else the in-place form on the exact bitmap.
+template <bool DIRECT>
 int launch_orders_filter(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_q3_params& p,
-                         const uint32_t* bitmap, uint32_t words, int32_t* out_key, int32_t* out_date, uint32_t* cnt) {
+                         const uint32_t* bitmap, const FilterOut& out, uint32_t* cnt) {
   if (od.n_rows == 0) return GPUDB_OK;
   if (smem_filter_exact(cu.key_max) && smem_filter_words(cu.key_max) <= kSmemCustWords)
-    return launch_orders_filter_as<1024, true>(call, cu, od, p, bitmap, bitmap, smem_filter_words(cu.key_max), true,
-                                               out_key, out_date, cnt);
-  (void)words;
-  return launch_orders_filter_as<256, false>(call, cu, od, p, bitmap, bitmap, 0, true, out_key, out_date, cnt);
+    return launch_orders_filter_as<1024, true, DIRECT>(call, cu, od, p, bitmap, bitmap, smem_filter_words(cu.key_max),
+                                                       true, out, cnt);
+  return launch_orders_filter_as<256, false, DIRECT>(call, cu, od, p, bitmap, bitmap, 0, true, out, cnt);
 }
+
+FilterOut staging_out(int32_t* key, int32_t* date) { return FilterOut{key, date, nullptr, nullptr, nullptr, nullptr, 0}; }
 
 __global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint32_t max_cap, int shift, uint32_t* cap_out,
                                    Q3Slot* ht, uint32_t* hits) {
@@ -230,6 +261,90 @@ __global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict
   }
 }
 
+// ---- direct mode ---------------------------------------------------------------------
+// The orders filter gave every qualifying order a dense slot and set its bit in the order-key
+// bitmap; the direct map omap (order key -> slot) is read only where that bit is set, so it is
+// never cleared. Per warp step, kDirectBatches independent 32-row batches go through three
+// phases whose loads are all in flight together: run heads (adjacent rows of one order) with
+// a passing row read their bitmap word, heads whose bit is set read their slot, and rows that
+// join load ext_price/discount and add revenue and a count with one atomic each. The next
+// step's keys and ship dates load meanwhile. Block 0 also zeroes the hit counts of the slots
+// between the order count and the next multiple of 128 (the top-k passes read whole 128-slot
+// chunks) and publishes that capacity.
+constexpr int kDirectBatches = 8;
+
+__global__ void __launch_bounds__(256) q3_direct_probe_kernel(
+    const int32_t* __restrict__ lkey, const int32_t* __restrict__ lship, const int64_t* __restrict__ lext,
+    const int32_t* __restrict__ ldisc, uint64_t n, int32_t ship_gt, const uint32_t* __restrict__ okbm,
+    const int32_t* __restrict__ omap, int32_t key_max, Q3Slot* ht, uint32_t* hits, const uint32_t* count,
+    uint32_t* cap_out) {
+  if (blockIdx.x == 0) {
+    const uint32_t c = *count, cap = max(128u, (c + 127u) & ~127u);
+    for (uint32_t i = c + threadIdx.x; i < cap; i += blockDim.x) hits[i] = 0;
+    if (threadIdx.x == 0) *cap_out = cap;
+  }
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  constexpr int U = kDirectBatches;
+  const uint64_t step = warps * 32 * U;
+  uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U;
+  int32_t nkey[U], nship[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const uint64_t row = base + u * 32 + lane;
+    nkey[u] = row < n ? ld_stream(lkey + row) : kEmptyKey;
+    nship[u] = row < n ? ld_stream(lship + row) : ship_gt;
+  }
+  for (; base < n; base += step) {
+    int32_t key[U];
+    uint32_t pass = 0, want = 0;
+    int head_lane[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      key[u] = nkey[u];
+      pass |= (uint32_t)(nship[u] > ship_gt) << u;
+      const uint64_t row = base + step + u * 32 + lane;
+      nkey[u] = row < n ? ld_stream(lkey + row) : kEmptyKey;
+      nship[u] = row < n ? ld_stream(lship + row) : ship_gt;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int32_t prev = __shfl_up_sync(FULL_MASK, key[u], 1);
+      const bool head = (lane == 0) || (key[u] != prev);
+      const uint32_t heads = __ballot_sync(FULL_MASK, head);
+      const uint32_t passm = __ballot_sync(FULL_MASK, (pass >> u) & 1u);
+      head_lane[u] = 31 - __clz(heads & lanemask_le());
+      const uint32_t later = heads & lanemask_gt();
+      const uint32_t upto = later ? (1u << (__ffs(later) - 1)) - 1u : 0xFFFFFFFFu;
+      // the run [head, next head) has a passing row and a key the map covers
+      if (head && (passm & upto & ~((1u << lane) - 1u)) && key[u] >= 0 && key[u] <= key_max) want |= 1u << u;
+    }
+    uint32_t word[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) word[u] = (want >> u & 1u) ? __ldg(okbm + ((uint32_t)key[u] >> 5)) : 0u;
+    int32_t slot[U];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      slot[u] = ((want >> u & 1u) && (word[u] >> ((uint32_t)key[u] & 31u) & 1u)) ? __ldg(omap + key[u]) : -1;
+    int64_t ext[U];
+    int32_t disc[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      slot[u] = __shfl_sync(FULL_MASK, slot[u], head_lane[u]);
+      const uint64_t row = base + u * 32 + lane;
+      const bool join = (pass >> u & 1u) && slot[u] >= 0;
+      ext[u] = join ? ld_stream(lext + row) : 0;
+      disc[u] = join ? ld_stream(ldisc + row) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if ((pass >> u & 1u) && slot[u] >= 0) {
+        atomicAdd(&ht[slot[u]].rev, (unsigned long long)(ext[u] * (int64_t)(100 - disc[u])));
+        atomicAdd(&hits[slot[u]], 1u);
+      }
+  }
+}
+
 // Top-k of the table: the revenue histogram pass, then the select-and-rank pass
 // (q3_table_hist / q3_table_select).
 __global__ void __launch_bounds__(kTopkThreads) q3_hist_kernel(const Q3Slot* __restrict__ ht,
@@ -265,24 +380,49 @@ __global__ void q3_fact_filter_kernel(const int32_t* __restrict__ lkey, const in
   }
 }
 
-constexpr uint32_t kQ3PartCap = 2048;               // shared slots per partition table
+constexpr uint32_t kQ3PartCap = 4096;               // shared slots per partition table
 constexpr uint32_t kQ3PartChunk = kQ3PartCap / 2;   // build rows per chunk
+constexpr int kQ3SlotsPerRound = kTopkThreads * (kTopkPerThread - 1);   // table slots per top-k round
+
+// Fact rows of a device-resident lineitem table for the radix mode: a row takes part when
+// ship_date > ship_gt; its payload is ext_price * (100 - discount). The first partitioning
+// pass reads the columns directly, so no filtered copy of the fact table is written.
+struct Q3FactSource {
+  const int32_t* okey;
+  const int32_t* ship;
+  const int64_t* ext;
+  const int32_t* disc;
+  uint64_t n;
+  int32_t ship_gt;
+  __device__ __forceinline__ uint64_t rows() const { return n; }
+  __device__ __forceinline__ bool key(uint64_t r, int32_t& k) const {
+    const int32_t s = __ldg(ship + r);
+    k = __ldg(okey + r);
+    return s > ship_gt;
+  }
+  __device__ __forceinline__ int64_t payload(uint64_t r) const {
+    return __ldcs(ext + r) * (int64_t)(100 - __ldcs(disc + r));
+  }
+};
+
+constexpr size_t q3_partition_smem() {
+  return (size_t)kQ3PartCap * (8 + 4 + 4 + 4) + (size_t)kTopkScratch * sizeof(u128);
+}
 
 // One block per partition: shared table of the partition's orders (in chunks), probe of its
-// fact rows with shared 64-bit atomics, then a block top-k carried across chunks.
+// fact rows with shared 64-bit atomics, then a block top-k carried across chunks (the table
+// in rounds of kQ3SlotsPerRound slots, the carry riding along).
 __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
     const int32_t* __restrict__ bk, const int32_t* __restrict__ bdate, const uint32_t* __restrict__ boff,
     const int32_t* __restrict__ pk, const int64_t* __restrict__ pval, const uint32_t* __restrict__ poff, int k,
     u128* cand, unsigned long long* groups, uint32_t* status) {
-  // one pool: the partition's table {rev, key, date, hits}, reused as the top-k scratch
-  constexpr size_t kPool = (size_t)kQ3PartCap * (8 + 4 + 4 + 4);
-  static_assert(kPool >= kTopkScratch * sizeof(u128), "top-k scratch");
-  __shared__ __align__(16) unsigned char pool[kPool];
+  extern __shared__ __align__(16) unsigned char q3p_pool[];
   __shared__ u128 carry[GPUDB_Q3_MAX_K];
-  unsigned long long* hrev = reinterpret_cast<unsigned long long*>(pool);
+  unsigned long long* hrev = reinterpret_cast<unsigned long long*>(q3p_pool);
   int32_t* hkey = reinterpret_cast<int32_t*>(hrev + kQ3PartCap);
   int32_t* hdate = hkey + kQ3PartCap;
   uint32_t* hhit = reinterpret_cast<uint32_t*>(hdate + kQ3PartCap);
+  u128* topk_scratch = reinterpret_cast<u128*>(hhit + kQ3PartCap);
   const uint32_t part = blockIdx.x, mask = kQ3PartCap - 1;
   const uint32_t b0 = boff[part], b1 = boff[part + 1], p0 = poff[part], p1 = poff[part + 1];
   for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
@@ -312,18 +452,19 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
       }
     }
     __syncthreads();
-    u128 v[kTopkPerThread];
+    for (uint32_t r0 = 0; r0 < kQ3PartCap; r0 += kQ3SlotsPerRound) {
+      u128 v[kTopkPerThread];
 #pragma unroll
-    for (int j = 0; j < kTopkPerThread; j++) v[j] = 0;
-#pragma unroll
-    for (int j = 0; j < (int)(kQ3PartCap / kTopkThreads); j++) {
-      const uint32_t s = threadIdx.x * (kQ3PartCap / kTopkThreads) + j;
-      if (hhit[s]) { v[j] = topk_compose((int64_t)hrev[s], hdate[s], hkey[s]); ngroups++; }
+      for (int j = 0; j < kTopkPerThread - 1; j++) {
+        const uint32_t s = r0 + threadIdx.x * (kTopkPerThread - 1) + j;
+        v[j] = 0;
+        if (s < kQ3PartCap && hhit[s]) { v[j] = topk_compose((int64_t)hrev[s], hdate[s], hkey[s]); ngroups++; }
+      }
+      v[kTopkPerThread - 1] = (int)threadIdx.x < k ? carry[threadIdx.x] : (u128)0;
+      __syncthreads();
+      block_topk(v, k, carry, topk_scratch);
+      __syncthreads();
     }
-    if ((int)threadIdx.x < k) v[kTopkPerThread - 1] = carry[threadIdx.x];
-    __syncthreads();
-    block_topk(v, k, carry, reinterpret_cast<u128*>(pool));
-    __syncthreads();
   }
   for (int i = threadIdx.x; i < k; i += kTopkThreads) cand[(size_t)part * k + i] = carry[i];
   ngroups = __reduce_add_sync(FULL_MASK, ngroups);
@@ -338,8 +479,11 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   cudaStream_t s = call.stream();
   const uint32_t words = (uint32_t)(cu.key_max >> 5) + 1;
   const uint64_t n_or = std::max<uint64_t>(od.n_rows, 1), n_li = std::max<uint64_t>(li->n_rows, 1);
+  // default fan-out: about 16K orders rows per partition (~1.6K after the filters of the
+  // default query), and at least 512 partitions so that every SM has some
   const int bits = p.radix_bits > 0 ? std::min(p.radix_bits, (int)kRadixMaxBits)
-                 : ctx->radix_bits > 0 ? ctx->radix_bits : radix_bits_for(od.n_rows, 4096);
+                 : ctx->radix_bits > 0 ? ctx->radix_bits
+                                       : std::min(kRxPassBits, std::max(9, radix_bits_for(od.n_rows, 16384)));
   const uint64_t parts = 1ull << bits;
   void *bitmap, *bstage, *fstage, *count, *bpart, *fpart, *offs, *cand;
   int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
@@ -374,22 +518,30 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   if (cu.n_rows)
     GPUDB_LAUNCH(call, bitmap_build_kernel, grid(cu.n_rows), 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows,
                  cu.key_max, (uint32_t*)bitmap, call.status());
-  if ((rc = launch_orders_filter(call, cu, od, p, (const uint32_t*)bitmap, words, bkey, bdate, cnt))) return rc;
-  const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
-  rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
-    if (c.n_rows == 0) return (int)GPUDB_OK;
-    GPUDB_LAUNCH(call, q3_fact_filter_kernel, grid(c.n_rows), 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount,
-                 c.n_rows, p.ship_date_gt, fkey, fval, cnt + 1);
-    return (int)GPUDB_OK;
-  });
-  if (rc) return rc;
+  if ((rc = launch_orders_filter<false>(call, cu, od, p, (const uint32_t*)bitmap, staging_out(bkey, bdate), cnt))) return rc;
   rc = radix_partition_run<int32_t>(call, bkey, bdate, n_or, cnt, bits, bk, bd, boff, bkey_t, bdate_t);
-  if (!rc) rc = radix_partition_run<int64_t>(call, fkey, fval, n_li, cnt + 1, bits, pk, pv, poff, fkey_t, fval_t);
+  if (rc) return rc;
+  if (li->location == GPUDB_MEM_DEVICE) {
+    // the filter runs inside the first partitioning pass: no filtered copy of the fact rows
+    const Q3FactSource src{li->order_key, li->ship_date, li->ext_price, li->discount, li->n_rows, p.ship_date_gt};
+    rc = rx_partition<Q3FactSource, int64_t, true>(call, src, n_li, bits, pk, pv, poff, fkey_t, fval_t);
+  } else {
+    const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
+    rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
+      if (c.n_rows == 0) return (int)GPUDB_OK;
+      GPUDB_LAUNCH(call, q3_fact_filter_kernel, grid(c.n_rows), 256, 0, c.order_key, c.ship_date, c.ext_price,
+                   c.discount, c.n_rows, p.ship_date_gt, fkey, fval, cnt + 1);
+      return (int)GPUDB_OK;
+    });
+    if (!rc) rc = radix_partition_run<int64_t>(call, fkey, fval, n_li, cnt + 1, bits, pk, pv, poff, fkey_t, fval_t);
+  }
   if (rc) return rc;
   u128* cbuf = static_cast<u128*>(cand);
   unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
   u128* rows = reinterpret_cast<u128*>(result + 16);
-  GPUDB_LAUNCH(call, q3_partition_kernel, (unsigned)parts, kTopkThreads, 0, (const int32_t*)bk, (const int32_t*)bd,
+  const size_t psmem = q3_partition_smem();
+  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q3_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
+  GPUDB_LAUNCH(call, q3_partition_kernel, (unsigned)parts, kTopkThreads, psmem, (const int32_t*)bk, (const int32_t*)bd,
                (const uint32_t*)boff, (const int32_t*)pk, (const int64_t*)pv, (const uint32_t*)poff, p.k, cbuf, groups,
                call.status());
   if (parts == 1) {
@@ -413,6 +565,78 @@ int q3_topk_levels(Call& call, u128* cand, uint64_t n_cand, int k, u128* scratch
     n_cand = blocks * (uint64_t)k;
     flip ^= 1;
   }
+}
+
+// Direct-map Q3: customer bitmap, the orders filter into dense slots + order-key bitmap +
+// direct map, the probe, and the top-k passes over the dense slots. Result payload as in
+// q3_global. The orders' key_max bounds the map (od.key_max + 1 int32).
+int q3_direct(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_lineitem* li,
+              const gpudb_q3_params& p, uint8_t* result) {
+  gpudb_ctx* ctx = call.ctx();
+  cudaStream_t s = call.stream();
+  const uint32_t words = (uint32_t)(cu.key_max >> 5) + 1;
+  const uint64_t n_or = od.n_rows;
+  const uint64_t slots = std::max<uint64_t>(128, (n_or + 127) / 128 * 128);
+  const int32_t key_max = std::max<int32_t>(od.key_max, 0);
+  const size_t okbm_bytes = ((size_t)((uint32_t)key_max >> 5) + 1) * 4;
+  void *bitmap, *okbm, *omap, *ht, *hits, *count, *tstate, *cand;
+  int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
+  if (!rc) rc = scratch(ctx, "q3.okbm", okbm_bytes, &okbm);
+  if (!rc) rc = scratch(ctx, "q3d.map", ((size_t)key_max + 1) * 4, &omap);   // never cleared
+  if (!rc) rc = scratch(ctx, "q3d.slots", (size_t)slots * sizeof(Q3Slot), &ht);
+  if (!rc) rc = scratch(ctx, "q3d.hits", (size_t)slots * 4, &hits);
+  if (!rc) rc = scratch(ctx, "q3.count", 256, &count);
+  if (!rc) rc = scratch(ctx, "q3.topk", (size_t)kTopkStateWords * 4, &tstate);
+  if (!rc) rc = scratch(ctx, "q3.cand", (size_t)kTopkCandCap * sizeof(u128), &cand);
+  if (rc) return rc;
+  uint32_t* cnt = static_cast<uint32_t*>(count);   // [0] orders, [1] top-k capacity
+  GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(okbm, 0, okbm_bytes, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(tstate, 0, (size_t)kTopkStateWords * 4, s));
+  const int sms = ctx->sm_count;
+  if (cu.n_rows) {
+    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((cu.n_rows + 255) / 256, (uint64_t)sms * 16));
+    GPUDB_LAUNCH(call, bitmap_build_kernel, g, 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows, cu.key_max,
+                 (uint32_t*)bitmap, call.status());
+  }
+  const FilterOut out{nullptr, nullptr, (Q3Slot*)ht, (uint32_t*)hits, (int32_t*)omap, (uint32_t*)okbm, key_max};
+  if ((rc = launch_orders_filter<true>(call, cu, od, p, (const uint32_t*)bitmap, out, cnt))) return rc;
+  const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
+  rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
+    if (c.n_rows == 0) return (int)GPUDB_OK;
+    const uint64_t per_block = 256 * kDirectBatches;
+    const unsigned g = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((c.n_rows + per_block - 1) / per_block, (uint64_t)sms * 8));
+    GPUDB_LAUNCH(call, q3_direct_probe_kernel, g, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount, c.n_rows,
+                 p.ship_date_gt, (const uint32_t*)okbm, (const int32_t*)omap, key_max, (Q3Slot*)ht, (uint32_t*)hits,
+                 (const uint32_t*)cnt, cnt + 1);
+    return (int)GPUDB_OK;
+  });
+  if (rc) return rc;
+  u128* cbuf = static_cast<u128*>(cand);
+  unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
+  u128* rows = reinterpret_cast<u128*>(result + 16);
+  uint32_t* ts = static_cast<uint32_t*>(tstate);
+  const uint32_t max_cap = (uint32_t)slots;
+  GPUDB_LAUNCH(call, q3_hist_kernel, q3_topk_grid(max_cap, sms, 1, 4), kTopkThreads, 0, (const Q3Slot*)ht,
+               (const uint32_t*)hits, (const uint32_t*)(cnt + 1), ts, groups);
+  GPUDB_LAUNCH(call, q3_select_kernel, q3_topk_grid(max_cap, sms, 1, 2), kTopkThreads, 0, (const Q3Slot*)ht,
+               (const uint32_t*)hits, (const uint32_t*)(cnt + 1), p.k, ts, cbuf, rows);
+  return GPUDB_OK;
+}
+
+// Whether the direct map of the orders' key range fits 30% of the device's memory (the
+// reference's choice between its direct map and its hash table, src/q3.cpp:246).
+bool q3_direct_fits(gpudb_ctx* ctx, const gpudb_orders& od) {
+  if (od.key_max < 0) return false;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  (void)ctx;
+  return ((double)od.key_max + 1.0) * 4.0 <= 0.3 * (double)total_b;
 }
 
 // Global-table Q3 (steps 1-6 above). Result payload: {u64 groups, u128 rows[k]}.
@@ -451,7 +675,8 @@ int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
                  cu.key_max, (uint32_t*)bitmap, call.status());
   int32_t* skey = static_cast<int32_t*>(stage);
   int32_t* sdate = skey + std::max<uint64_t>(n_or, 1);
-  if ((rc = launch_orders_filter(call, cu, od, p, (const uint32_t*)bitmap, words, skey, sdate, cnt))) return rc;
+  if ((rc = launch_orders_filter<false>(call, cu, od, p, (const uint32_t*)bitmap, staging_out(skey, sdate), cnt)))
+    return rc;
   GPUDB_LAUNCH(call, table_clear_kernel, grid(max_cap), 256, 0, (const uint32_t*)cnt, 2048u, max_cap, ctx->ht_shift, cap,
                (Q3Slot*)ht, (uint32_t*)hits);
   GPUDB_LAUNCH(call, orders_insert_kernel, grid(n_or / 4), 256, 0, (const int32_t*)skey, (const int32_t*)sdate,
@@ -489,7 +714,7 @@ extern "C" int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, cons
   if (!ctx) return GPUDB_E_INVALID;
   if (!cu || !od || !p || !out) return fail(ctx, GPUDB_E_INVALID, "q3: tables, params and result are required");
   if (p->k < 1 || p->k > GPUDB_Q3_MAX_K) return fail(ctx, GPUDB_E_INVALID, "q3: k must be in 1..%d", GPUDB_Q3_MAX_K);
-  if (p->join_mode != GPUDB_JOIN_GLOBAL && p->join_mode != GPUDB_JOIN_RADIX)
+  if (p->join_mode < GPUDB_JOIN_GLOBAL || p->join_mode > GPUDB_JOIN_AUTO)
     return fail(ctx, GPUDB_E_INVALID, "q3: unknown join mode %d", p->join_mode);
   if (cu->n_rows && (!cu->cust_key || !cu->segment)) return fail(ctx, GPUDB_E_INVALID, "q3: customer columns are NULL");
   if (cu->key_max < 0 && cu->n_rows) return fail(ctx, GPUDB_E_INVALID, "q3: customer.key_max is required");
@@ -502,25 +727,32 @@ extern "C" int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, cons
   if (c.key_max < 0) c.key_max = 0;
   const gpudb_orders o = *od;
   const gpudb_q3_params pp = *p;
+  int mode = pp.join_mode;
+  if (mode == GPUDB_JOIN_AUTO) mode = q3_direct_fits(ctx, o) ? GPUDB_JOIN_DIRECT : GPUDB_JOIN_GLOBAL;
+  if (mode == GPUDB_JOIN_DIRECT && o.n_rows && o.key_max < 0)
+    return fail(ctx, GPUDB_E_INVALID, "q3: the direct mode needs orders.key_max");
   Call call(ctx, ex, t);
   const size_t bytes = 16 + (size_t)GPUDB_Q3_MAX_K * sizeof(u128);
   if ((rc = call.begin(bytes))) return rc;
   uint8_t* res = call.result<uint8_t>();
-  rc = (pp.join_mode == GPUDB_JOIN_GLOBAL) ? q3_global(call, c, o, li, pp, res) : q3_radix(call, c, o, li, pp, res);
+  rc = mode == GPUDB_JOIN_GLOBAL ? q3_global(call, c, o, li, pp, res)
+     : mode == GPUDB_JOIN_DIRECT ? q3_direct(call, c, o, li, pp, res)
+                                 : q3_radix(call, c, o, li, pp, res);
   if (rc) return rc;
   const int k = pp.k;
-  return call.finish(bytes, [out, k](const uint8_t* h) {
-    q3_result_from(h, k, out);
+  return call.finish(bytes, [out, k, mode](const uint8_t* h) {
+    q3_result_from(h, k, out, mode);
     return GPUDB_OK;
   });
 }
 
 namespace gpudb {
 
-void q3_result_from(const uint8_t* h, int k, gpudb_q3_result* out) {
+void q3_result_from(const uint8_t* h, int k, gpudb_q3_result* out, int mode) {
   uint64_t groups;
   std::memcpy(&groups, h, 8);
   out->n_groups = groups;
+  out->join_mode = mode;
   out->n_rows = (uint32_t)std::min<uint64_t>(groups, (uint64_t)k);
   for (uint32_t i = 0; i < out->n_rows; i++) {
     u128 c;

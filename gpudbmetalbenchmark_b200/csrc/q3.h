@@ -224,7 +224,7 @@ __device__ __forceinline__ void q3_table_select(const Q3Slot* __restrict__ ht, c
 
 // Result conversion shared by the single and the batched Q3: payload {u64 groups, u64 pad,
 // u128 rows[k]} -> gpudb_q3_result.
-void q3_result_from(const uint8_t* h, int k, gpudb_q3_result* out);
+void q3_result_from(const uint8_t* h, int k, gpudb_q3_result* out, int join_mode);
 
 // Q3 requests (global-table mode, device-resident lineitem, identical tables) evaluated
 // together: every stage is one launch for all of them and the fact table is probed once.

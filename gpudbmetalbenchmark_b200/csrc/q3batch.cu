@@ -345,7 +345,7 @@ int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t
       std::memcpy(&st, h + 4 * r, 4);
       std::memcpy(&dst, h + 4 * (kB + req_seg[r]), 4);
       q.status = status_to_error(ctx, st | dst);
-      if (q.status == GPUDB_OK) q3_result_from(h + st_bytes + r * kReqBytes, q.q3p.k, q.q3_out);
+      if (q.status == GPUDB_OK) q3_result_from(h + st_bytes + r * kReqBytes, q.q3p.k, q.q3_out, GPUDB_JOIN_GLOBAL);
       if (ctx->on_done) ctx->on_done(ctx->on_done_arg, &q.status);
     }
     return GPUDB_OK;

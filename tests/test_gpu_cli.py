@@ -53,12 +53,15 @@ def test_cli_q6_and_q1(orc):
     timing_ok(out, "Q1", n)
 
 
-def test_cli_q3_both_join_modes(orc):
+def test_cli_q3_every_join_mode(orc):
     cu, od, li = orc.q3_tables(1500, 15000, 60000, 42)
     top, groups = orc.q3(cu, od, li)
     out = run("sf1", "q3", "--scale", "0.01")
+    assert "using the direct map join" in out
     blocks = out.split("TPC-H Q3 Results")[1:]
-    assert len(blocks) == 2
+    assert len(blocks) == 3
+    assert [re.match(r" \(Top 10, ([a-z ]+) join\)", b).group(1) for b in blocks] == \
+        ["direct map", "global hash table", "radix partitioned"]
     for b in blocks:
         rows = re.findall(r"^\|\s+(\d+) \| \$\s*(\S+) \|\s+(\d+) \|", b, re.M)
         assert [(int(k), int(d), scaled(r, 4)) for k, r, d in rows] == top

@@ -9,7 +9,7 @@ from gpudbmetalbenchmark_b200.engine import q3_to_list
 
 pytestmark = pytest.mark.gpu
 
-MODES = [capi.JOIN_GLOBAL, capi.JOIN_RADIX]
+MODES = [capi.JOIN_GLOBAL, capi.JOIN_RADIX, capi.JOIN_DIRECT]
 
 
 def run(engine, cu, od, li, mode=capi.JOIN_GLOBAL, location=capi.MEM_DEVICE, **kw):
@@ -134,15 +134,49 @@ def test_q3_empty_sides(engine, orc, mode):
     assert run(engine, cu, od, li, mode, order_date_lt=0) == ([], 0)
 
 
-def test_q3_duplicate_build_key_reported(engine, orc):
+@pytest.mark.parametrize("mode", MODES)
+def test_q3_duplicate_build_key_reported(engine, orc, mode):
     cu, od, li = orc.q3_tables(100, 1000, 4000, 4)
     od["order_key"][7] = od["order_key"][8]
     od["order_date"][7] = od["order_date"][8] = 0
     od["cust_key"][7] = od["cust_key"][8]
     cu["segment"][od["cust_key"][8]] = 1
     with pytest.raises(capi.GpudbError) as e:
-        run(engine, cu, od, li)
+        run(engine, cu, od, li, mode)
     assert e.value.code == capi.E_INVALID
+
+
+def test_q3_auto_mode_picks_the_direct_map(engine, orc):
+    """AUTO takes the direct map when the orders' key range fits 30% of device memory (any
+    realistic range on a 180 GB B200) and reports the mode that ran; the direct mode refuses
+    orders without a key bound, and a key above the declared bound is an error."""
+    import ctypes as C
+    cu, od, li = orc.q3_tables(2000, 20_000, 80_000, 6)
+    tc, to, tl = engine.upload("customer", cu), engine.upload("orders", od), engine.upload("lineitem", li)
+    try:
+        r = capi.Q3Result()
+        engine.q3(tc, to, tl, join_mode=capi.JOIN_AUTO, out=r, async_=True)
+        engine.sync()
+        assert r.join_mode == capi.JOIN_DIRECT
+        assert q3_to_list(r) == orc.q3(cu, od, li)
+        for mode in (capi.JOIN_GLOBAL, capi.JOIN_RADIX):
+            engine.q3(tc, to, tl, join_mode=mode, out=r)
+            assert r.join_mode == mode
+        os_ = to.struct()
+        os_.key_max = -1
+        p = capi.Q3Params(1, 1170, 1170, 10, capi.JOIN_DIRECT, 0)
+        rc = engine.lib.gpudb_q3_join_topk(engine.ctx, C.byref(tc.struct()), C.byref(os_), C.byref(tl.lineitem()),
+                                           C.byref(p), C.byref(r), None, None)
+        assert rc == capi.E_INVALID
+        os_.key_max = int(od["order_key"].max()) - 4   # the largest key is above the bound
+        p.order_date_lt = 2406
+        p.segment = int(cu["segment"][od["cust_key"][np.argmax(od["order_key"])]])
+        rc = engine.lib.gpudb_q3_join_topk(engine.ctx, C.byref(tc.struct()), C.byref(os_), C.byref(tl.lineitem()),
+                                           C.byref(p), C.byref(r), None, None)
+        assert rc == capi.E_KEY_RANGE
+    finally:
+        for t in (tc, to, tl):
+            engine.free(t)
 
 
 @pytest.mark.parametrize("mode", MODES)
