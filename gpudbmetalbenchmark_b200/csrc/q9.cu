@@ -12,9 +12,9 @@
 //  - the fact table goes through in pieces of at most 64M rows, two kernels each:
 //    li_filter_kernel streams part_key (128-bit loads), tests each part against a filter held
 //    in shared memory (the exact bitmap, or a hashed one confirmed in the global bitmap) and
-//    compacts the (row, part) pairs that pass (~5.5%); q9_resolve_kernel takes one pair per thread and
-//    gathers the row's other five columns and its lookups together (late materialisation,
-//    all resident threads' misses in flight at once);
+//    writes a bitmask of the rows that pass (~5.5%); q9_resolve_kernel expands the bitmask a
+//    warp at a time (one set bit per lane) and gathers each row's six columns and its
+//    lookups together (late materialisation, all resident threads' misses in flight);
 //  - aggregation goes to a per-block shared-memory hash table keyed by (nation<<16 | year)
 //    (CAS + 64-bit shared atomics); a group that finds no shared slot spills straight to the
 //    global open-addressing table, and each block merges its shared table into the global
@@ -162,21 +162,22 @@ constexpr int kLiQuads = 4;                  // 16-byte loads per thread per blo
 constexpr int kLiRows = 4 * kLiQuads;        // fact rows per thread per block step of li_filter_kernel
 constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve pair (bounds the pair buffer)
 
-// Fact rows whose part passes the bitmap, as (row, part) pairs (block prefix sum, one
-// atomicAdd per 16384 rows). The part filter sits in shared memory (smem_filter_*): the
-// exact bitmap, or a hashed one whose hits are confirmed in `bits`. A block step covers
-// kLiThreads * 16 rows; load q of thread t is the 16-byte quad q * kLiThreads + t of the
-// step (coalesced), and the next step's quads load while this one is tested (one block per
-// SM when the filter is large, so the block overlaps its own latencies).
+// Fact rows whose part passes the bitmap -> bit (r & 31) of passbits[r >> 5] (rows of the
+// piece). The part filter sits in shared memory (smem_filter_*): the exact bitmap, or a
+// hashed one whose hits are confirmed in `bits`. A block step covers kLiThreads * 16 rows;
+// load q of thread t is the 16-byte quad q * kLiThreads + t of the step (coalesced), and the
+// next step's quads load while this one is tested. The four rows of a quad are four bits of
+// one word that eight lanes share: an OR across the eight lanes and one store per word, so
+// warps never wait for each other (no block barrier, no atomic) and the bitmask is dense
+// (one bit per row, 1/32 of the column read).
 __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
                                                                const uint32_t* __restrict__ bits, int32_t part_max,
                                                                const uint32_t* __restrict__ filt, uint32_t filt_words,
-                                                               bool exact, uint32_t* rows, int32_t* parts,
-                                                               uint32_t* count) {
+                                                               bool exact, uint32_t* __restrict__ passbits) {
   extern __shared__ uint32_t sfilt[];
-  __shared__ uint32_t sh[33];
   smem_filter_load(filt, filt_words, sfilt);
   const bool vec = (reinterpret_cast<uintptr_t>(part) & 15u) == 0;
+  const int lane = threadIdx.x & 31;
   constexpr uint64_t kStepRows = (uint64_t)kLiThreads * kLiRows;
   const uint64_t step = (uint64_t)gridDim.x * kStepRows;
   // row of element (q, k) of this thread in the step at b
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
   };
   uint64_t b = (uint64_t)blockIdx.x * kStepRows;
   prefetch(b);
-  for (; b < n; b += step) {   // whole blocks
+  for (; b < n; b += step) {
     int32_t p[kLiRows];
     if (vec && b + kStepRows <= n) {
 #pragma unroll
@@ -211,19 +212,38 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
 #pragma unroll
     for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
     const uint32_t take = smem_filter_mask(sfilt, exact, bits, p, ok);
-    uint32_t pos = block_reserve<kLiThreads>(__popc(take), count, sh);
 #pragma unroll
-    for (int j = 0; j < kLiRows; j++)
-      if (take & (1u << j)) { rows[pos] = (uint32_t)row_of(b, j >> 2, j & 3); parts[pos] = p[j]; pos++; }
+    for (int q = 0; q < kLiQuads; q++) {
+      // rows 4*lane .. 4*lane+3 of this quad's 128 rows: bits 4*(lane & 7) .. of word lane / 8
+      uint32_t v = ((take >> (4 * q)) & 0xFu) << (4 * (lane & 7));
+      v |= __shfl_xor_sync(FULL_MASK, v, 1);
+      v |= __shfl_xor_sync(FULL_MASK, v, 2);
+      v |= __shfl_xor_sync(FULL_MASK, v, 4);
+      const uint64_t r0 = row_of(b, q, 0);
+      if ((lane & 7) == 0 && r0 < n) passbits[r0 >> 5] = v;
+    }
   }
 }
 
-// One (row, part) pair per thread: the row's five columns are gathered together, then
-// supplier -> nation, order -> year and (part, supp) -> cost, and the profit goes to a
-// shared (nation, year) table that spills to the global one. Every resident thread has its
-// own independent misses in flight.
-__global__ void __launch_bounds__(kQ9Threads) q9_resolve_kernel(const uint32_t* __restrict__ rows,
-                                                                 const int32_t* __restrict__ parts, const uint32_t* count,
+// Position of the k-th (from 0) set bit of w: halving, by the bit counts of the low halves.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t width = 16; width >= 1; width >>= 1) {
+    const uint32_t lo = __popc(w & ((1u << width) - 1u));
+    if (k >= lo) { k -= lo; w >>= width; pos += width; }
+  }
+  return pos;
+}
+
+// The rows of the pass bitmask, 1024 rows (32 words) per warp step: the warp counts every
+// word's bits, and in rounds of 32 each lane takes one set bit (its word found by a binary
+// search over the word counts), so all lanes work whatever the density.
+// For each row the five other columns are gathered together, then supplier -> nation,
+// order -> year and (part, supp) -> cost; the profit goes to a shared (nation, year) table
+// that spills to the global one.
+__global__ void __launch_bounds__(kQ9Threads) q9_resolve_kernel(const uint32_t* __restrict__ passbits, uint64_t n,
+                                                                 const int32_t* __restrict__ part,
                                                                  const int32_t* __restrict__ supp,
                                                                  const int32_t* __restrict__ order,
                                                                  const int64_t* __restrict__ ext,
@@ -236,31 +256,53 @@ __global__ void __launch_bounds__(kQ9Threads) q9_resolve_kernel(const uint32_t* 
   uint32_t* skeys = reinterpret_cast<uint32_t*>(svals + scap);
   for (uint32_t i = threadIdx.x; i < scap; i += blockDim.x) { skeys[i] = kGroupEmpty; svals[i] = 0; }
   __syncthreads();
-  const uint32_t n = *count, ps_cap = *m.ps_cap, smask = scap - 1;
+  const uint32_t ps_cap = *m.ps_cap, smask = scap - 1;
+  const int lane = threadIdx.x & 31;
+  const uint64_t words = (n + 31) >> 5, groups = (words + 31) >> 5;
+  const uint64_t W = (uint64_t)gridDim.x * (blockDim.x >> 5);
   uint32_t bad = 0;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const uint32_t r = ld_stream(rows + i);
-    const int32_t p = ld_stream(parts + i);
-    const int32_t s = ld_stream(supp + r), o = ld_stream(order + r);
-    const int64_t e = ld_stream(ext + r);
-    const int32_t d = ld_stream(disc + r), q = ld_stream(qty + r);
-    const bool s_ok = s >= 0 && s <= m.supp_max, o_ok = o >= 0 && o <= m.order_max;
-    const uint8_t nat = s_ok ? __ldg(m.nation + s) : kNoValue;
-    const uint8_t yoff = o_ok ? __ldg(m.year + o) : kNoValue;
-    long long cost = 0;
-    const bool found = s_ok && ps_find(m.ps, ps_cap, ps_key(p, s), &cost);
-    if (found && nat != kNoValue && yoff != kNoValue) {
-      bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
-      const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
-      const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
-      uint32_t h = slot_hash64(key) & smask;
-      bool done = false;
-      for (uint32_t t = 0; t < scap && !done; t++, h = (h + 1) & smask) {
-        const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
-        if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); done = true; }
+  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < groups; g += W) {
+    const uint64_t w = g * 32 + lane;
+    const uint32_t word = w < words ? ld_stream(passbits + w) : 0u;
+    const uint32_t c = __popc(word);
+    uint32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(FULL_MASK, incl, d);
+      if (lane >= d) incl += o;
+    }
+    const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+    for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+      const uint32_t j = j0 + (uint32_t)lane;
+      // source lane: the number of lanes whose inclusive count is <= j
+      uint32_t src = 0;
+#pragma unroll
+      for (uint32_t stp = 16; stp >= 1; stp >>= 1)
+        if (__shfl_sync(FULL_MASK, incl, src + stp - 1) <= j) src += stp;
+      const uint32_t sw = __shfl_sync(FULL_MASK, word, src);
+      const uint32_t sx = __shfl_sync(FULL_MASK, incl - c, src);
+      if (j >= total) continue;
+      const uint64_t r = ((g * 32 + src) << 5) + nth_set_bit(sw, j - sx);
+      const int32_t pk = ld_stream(part + r), sk = ld_stream(supp + r), o = ld_stream(order + r);
+      const int64_t e = ld_stream(ext + r);
+      const int32_t d = ld_stream(disc + r), q = ld_stream(qty + r);
+      const bool s_ok = sk >= 0 && sk <= m.supp_max, o_ok = o >= 0 && o <= m.order_max;
+      const uint8_t nat = s_ok ? __ldg(m.nation + sk) : kNoValue;
+      const uint8_t yoff = o_ok ? __ldg(m.year + o) : kNoValue;
+      long long cost = 0;
+      const bool found = s_ok && ps_find(m.ps, ps_cap, ps_key(pk, sk), &cost);
+      if (found && nat != kNoValue && yoff != kNoValue) {
+        bad |= ((uint64_t)e >= (1ull << 36)) | ((uint32_t)d > 100u) | ((uint32_t)q >= 65536u);
+        const long long profit = e * (int64_t)(100 - d) - cost * (int64_t)q * 100;
+        const uint32_t key = ((uint32_t)nat << 16) | (uint32_t)(1992 + yoff);
+        uint32_t h = slot_hash64(key) & smask;
+        bool done = false;
+        for (uint32_t t = 0; t < scap && !done; t++, h = (h + 1) & smask) {
+          const uint32_t prev = atomicCAS(&skeys[h], kGroupEmpty, key);
+          if (prev == kGroupEmpty || prev == key) { atomicAdd(&svals[h], (unsigned long long)profit); done = true; }
+        }
+        if (!done) global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
       }
-      if (!done) global_group_add(gkeys, gvals, gcap, key, (unsigned long long)profit, status);   // shared table full
     }
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) set_status(status, ST_DOMAIN);
@@ -372,15 +414,13 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   const uint32_t filt_words = smem_filter_words(part_max);
   void* hfilt = nullptr;
   if (!rc && !filt_exact) rc = scratch(ctx, "q9.partfilter", (size_t)kSmemFilterWords * 4, &hfilt);
-  // (row, part) pairs of one piece of the fact table that passed the part bitmap
-  // (chunk_rows, when given, also sets the piece size of a device-resident table)
+  // pass bitmask of one piece of the fact table (rows whose part passed the part filter;
+  // chunk_rows, when given, also sets the piece size of a device-resident table)
   const uint64_t piece =
       std::max<uint64_t>(1, std::min<uint64_t>(pp.chunk_rows ? (uint64_t)pp.chunk_rows : li->n_rows, kQ9Piece));
-  void* pairs = nullptr;
-  if (!rc) rc = scratch(ctx, "q9.pairs", (size_t)piece * 8, &pairs);
+  void* passbits = nullptr;
+  if (!rc) rc = scratch(ctx, "q9.passbits", ((piece + 31) / 32 + 32) * 4, &passbits);
   if (rc) return rc;
-  uint32_t* prow = static_cast<uint32_t*>(pairs);
-  int32_t* ppart = reinterpret_cast<int32_t*>(prow + piece);
   uint32_t* cnt = static_cast<uint32_t*>(count);
   uint32_t* cap = cnt + 1;
   uint32_t* gkeys = reinterpret_cast<uint32_t*>(static_cast<unsigned long long*>(groups) + gcap);
@@ -403,7 +443,7 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
     GPUDB_CUDA(ctx, cudaMemsetAsync(bits, 0, (size_t)words * 4, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, s));
-    GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));   // [0] partsupp count, [1] capacity, [2] pair count
+    GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));   // [0] partsupp count, [1] capacity
     GPUDB_CUDA(ctx, cudaMemsetAsync(gvals, 0, (size_t)gcap * 8, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(gkeys, 0xFF, (size_t)gcap * 4, s));
     if (pa->n_rows)
@@ -431,19 +471,20 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
                       (const uint32_t*)cap, (const uint8_t*)year, order_max};
     int r = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
       for (uint64_t off = 0; off < c.n_rows; off += piece) {
+        // (the previous piece's resolve is done with the bitmask: stream order)
         const uint64_t n = std::min<uint64_t>(piece, c.n_rows - off);
-        // the piece's pair count (the previous piece's resolve is done with it: stream order)
-        uint32_t* pc = cnt + 2;
-        GPUDB_CUDA(ctx, cudaMemsetAsync(pc, 0, 4, s));
         const unsigned fg = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((n + kLiThreads * kLiRows - 1) / (kLiThreads * kLiRows),
                                   (uint64_t)sms * std::max(1, filter_per_sm)));
         GPUDB_LAUNCH(call, li_filter_kernel, fg, kLiThreads, filt_smem, c.part_key + off, n, (const uint32_t*)bits,
-                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_exact, prow, ppart, pc);
+                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_exact,
+                     (uint32_t*)passbits);
+        const uint64_t warps_needed = (n + 1023) / 1024;
         const unsigned g = (unsigned)std::max<uint64_t>(
-            1, std::min<uint64_t>((n + kQ9Threads - 1) / kQ9Threads, (uint64_t)sms * std::max(1, resolve_per_sm)));
-        GPUDB_LAUNCH(call, q9_resolve_kernel, g, kQ9Threads, probe_smem, (const uint32_t*)prow, (const int32_t*)ppart,
-                     (const uint32_t*)pc, c.supp_key + off, c.order_key + off, c.ext_price + off, c.discount + off,
+            1, std::min<uint64_t>((warps_needed + kQ9Threads / 32 - 1) / (kQ9Threads / 32),
+                                  (uint64_t)sms * std::max(1, resolve_per_sm)));
+        GPUDB_LAUNCH(call, q9_resolve_kernel, g, kQ9Threads, probe_smem, (const uint32_t*)passbits, n,
+                     c.part_key + off, c.supp_key + off, c.order_key + off, c.ext_price + off, c.discount + off,
                      c.quantity + off, maps, gkeys, gvals, gcap, scap, call.status());
       }
       return (int)GPUDB_OK;
