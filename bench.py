@@ -6,9 +6,18 @@ one step = one pass of each pipeline over the table.
 
 Prints one JSON line (rank 0). value = lineitem rows scanned per second by the whole job
 (2 x rows x N per step); e2e = the same metric through the C ABI with the table in pinned
-host memory (chunked host->HBM streaming inside the timed region). For N > 1 (torchrun)
-every rank scans its own 60M-row shard of one table (weak scaling, no collective on the
-data path); times are the max over ranks.
+host memory (chunked host->HBM streaming inside the timed region), one call per pipeline;
+e2e_batched = the same two requests as one gpudb_batch_run call, which copies each chunk
+once for both scans. For N > 1 (torchrun) every rank scans its own 60M-row shard of one
+table (weak scaling, no collective on the data path); times are the max over ranks.
+
+On one GPU the line also carries, under `pipelines`, the device time, rows/s and HBM
+roofline fraction of every other configuration of the workload: the Q1 aggregate at 6M
+rows, the Q3 join + top-10 at 1x and 10x in each join mode, the Q9 star join at 60M fact
+rows and streamed at 600M, the join microbenchmark; under `serve`, the served mixed
+stream against the plain one-query-per-launch form (queries/s, p50/p99, bit-exact flag);
+and two CPU baselines: the reference's own kernels on all host cores (`cpu_baseline`) and
+the single-threaded C oracle (`cpu_baseline_oracle`).
 
 --impl reference times the reference's own kernels (kernels/q6.metal, kernels/q1.metal of
 nd-tung/GPUDBMetalBenchmark) compiled for the host CPU (oracle/_ref), on all host cores.
@@ -40,7 +49,11 @@ def parse():
     ap.add_argument("--rows", type=int, default=60_000_000)
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--skip-cpu", action="store_true", help="no CPU baseline (profiling runs)")
+    ap.add_argument("--skip-cpu", action="store_true", help="no CPU baselines (profiling runs)")
+    ap.add_argument("--skip-extra", action="store_true",
+                    help="only the config-1 step: no per-pipeline block, serving comparison or CPU baselines")
+    ap.add_argument("--no-stream600m", action="store_true", help="leave out the 600M-row streamed Q9 case")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     return ap.parse_args()
 
 
@@ -173,6 +186,30 @@ def cpu_baseline(rows_total, seed):
             "step_s": t}
 
 
+def cpu_baseline_oracle(li_host, rows):
+    """The project's single-threaded C oracle (exact int128 sums) over the same 60M-row table
+    in host memory, Q6 + Q1 per step, median of 5 steps."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as orc
+    times = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        orc.q6(li_host)
+        orc.q1(li_host)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    return {"value": 2 * rows / t, "unit": "rows/s", "cores": 1, "kind": "port",
+            "sample": "all %d rows of the workload (Q6 + Q1 per step), single-threaded C oracle, median of 5" % rows,
+            "step_s": t}
+
+
+def workload_config(rows, world):
+    return {"workload": "config 1: Q6-like filtered sum (1a) + Q1-like 6-group aggregate (1b) over a "
+                        "%d-row lineitem table per GPU" % rows,
+            "rows_per_gpu": rows, "l2": "inputs %.2f GB per step > 126 MB L2, no flush needed" % (46 * rows / 1e9),
+            "parallelism": "row shards, one per GPU" if world > 1 else "single GPU"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -219,16 +256,88 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "Q6-like + Q1-like scans, sample of %d lineitem rows per step" % sample,
-                       "rows": sample, "threads": threads},
+            "config": workload_config(args.rows, world),
             "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "reference",
-                             "sample": "%d rows per step (the 60M-row workload scaled to the step budget)" % sample},
+                             "sample": "%d of the %d rows per step (the reference's Q6 and Q1 kernels compiled for "
+                                       "the host, float32 columns prepared once outside the timing)" % (sample, args.rows)},
             "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
 # ---------------------------------------------------------------------------------------
+def h2d_probe(local, gb=1.0, reps=5):
+    """Pinned host -> HBM copy bandwidth (GB/s), the bound of every streamed table."""
+    import torch
+    n = int(gb * 1e9)
+    src = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    dst = torch.empty(n, dtype=torch.uint8, device="cuda:%d" % local)
+    dst.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        dst.copy_(src, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    gbs = n * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    del src, dst
+    torch.cuda.empty_cache()
+    return gbs
+
+
+def shared_pass(eng, li, steps, stream, ref6, ref1):
+    """The same two requests as one gpudb_batch_run over the device-resident table: one
+    shared scan pass reads the union of the columns (26 B/row) once for both."""
+    import torch
+    from gpudbmetalbenchmark_b200 import capi
+    reqs = (capi.Request * 2)()
+    o6, o1 = capi.Q6Result(), capi.Q1Result()
+    reqs[0].pipeline, reqs[0].li, reqs[0].q6 = capi.PIPE_Q6, C.pointer(li), capi.Q6Params(365, 730, 5, 7, 24)
+    reqs[0].q6_out = C.pointer(o6)
+    reqs[1].pipeline, reqs[1].li, reqs[1].q1 = capi.PIPE_Q1, C.pointer(li), capi.Q1Params(2436, 0)
+    reqs[1].q1_out = C.pointer(o1)
+    eng._check(eng.lib.gpudb_batch_run(eng.ctx, reqs, 2, None, None))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        eng._check(eng.lib.gpudb_batch_run(eng.ctx, reqs, 2, None, None))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert (o6.revenue, o6.rows_matched) == ref6 and bytes(o1) == ref1
+    ms = e0.elapsed_time(e1) / steps
+    rows = li.n_rows
+    return {"ms": ms, "rows_per_s": 2 * rows / (ms * 1e-3), "gbs_algorithmic": 26 * rows / (ms * 1e-3) / 1e9,
+            "call": "gpudb_batch_run with the Q6 and the Q1 request over the device-resident table (one shared "
+                    "scan pass, 26 B/row), synchronous per step"}
+
+
+def pipelines_block(eng, reps, stream600m, h2d_gbs):
+    """Every other configuration of the workload on this GPU (device time of the call's
+    kernels, CUDA events on its stream, median of `reps` after a warm-up call)."""
+    from gpudbmetalbenchmark_b200 import pipebench as pb
+    quiet = pb.record
+    out = {}
+    r6, r1 = pb.scan_case(eng, 6_000_000, reps, out=quiet)
+    out["q1_cfg0_6m"] = r1
+    out["q6_6m"] = r6
+    for label, key, sizes in (("config 2 (1x)", "q3_1x", (150_000, 1_500_000, 6_000_000)),
+                              ("config 2 (10x)", "q3_10x", (1_500_000, 15_000_000, 60_000_000))):
+        for mode, rec in pb.q3_case(eng, *sizes, reps, label, out=quiet).items():
+            out["%s_%s" % (key, mode)] = rec
+    q9 = pb.q9_case(eng, reps, stream600m, out=quiet)
+    out["q9_60m"] = q9["resident"]
+    if "streamed" in q9:
+        rec = q9["streamed"]
+        rec["h2d_probe_gbs"] = h2d_gbs
+        rec["frac_of_h2d"] = rec["h2d_gbs"] / h2d_gbs if h2d_gbs else None
+        out["q9_600m_streamed"] = rec
+    for mode, rec in pb.join_count_case(eng, max(3, reps // 2), out=quiet).items():
+        out["join_count_15m_60m_%s" % mode] = rec
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
     from gpudbmetalbenchmark_b200 import Engine, capi
@@ -253,6 +362,13 @@ def run_ours(args, rank, world, local):
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_ms(ms):
+        if dist is None:
+            return ms
+        m = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        return float(m.item())
+
     r6, r1 = capi.Q6Result(), capi.Q1Result()
     for _ in range(args.warmup):
         eng.q6(li, async_=True, out=r6)
@@ -276,77 +392,132 @@ def run_ours(args, rank, world, local):
         eng.sync()
         launches = eng.launches() - launches0
         barrier()
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        m = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        ms = float(m.item())
+    ms = max_ms(ev0.elapsed_time(ev1))
     # every step's result equals the first (same input): a cheap live consistency check
     assert all(o.revenue == o6[0].revenue for o in o6) and all(bytes(o) == bytes(o1[0]) for o in o1)
+    ref6, ref1 = (o6[0].revenue, o6[0].rows_matched), bytes(o1[0])
 
+    # the shards' results, merged with the engine's exact merge (one small all-gather after
+    # the timed region): the whole job's answer
+    merged = None
+    if dist is not None:
+        parts = [None] * world
+        dist.all_gather_object(parts, (bytes(o6[0]), bytes(o1[0])))
+        p6 = [capi.Q6Result.from_buffer_copy(x[0]) for x in parts]
+        p1 = [capi.Q1Result.from_buffer_copy(x[1]) for x in parts]
+        m6, m1 = capi.merge_q6(p6), capi.merge_q1(p1)
+        assert bytes(capi.merge_q1(p1[::-1])) == bytes(m1)   # order-independent
+        assert m6.rows_matched == sum(x.rows_matched for x in p6)
+        merged = {"q6_revenue": m6.revenue, "q6_rows": m6.rows_matched,
+                  "q1_rows": sum(g.count for g in m1.groups[:m1.n_groups]), "q1_groups": m1.n_groups,
+                  "how": "all_gather of each rank's result structs, gpudb_q6/q1_result_merge on every rank"}
     q6_ms = statistics.mean(x.gpu_ms for x in t6)
     q1_ms = statistics.mean(x.gpu_ms for x in t1)
     peak, peak_kind = peaks()
     q1_gbs = Q1_BYTES_PER_ROW * rows / (q1_ms * 1e-3) / 1e9
     q6_gbs = Q6_BYTES_PER_ROW * rows / (q6_ms * 1e-3) / 1e9
     tr = ncu_traffic("q1_vec_smem_kernel")
+    shared = None
+    if world == 1 and not args.skip_extra:
+        shared = shared_pass(eng, li, K, stream, ref6, ref1)
+    eng.free(t)
 
     # ---- end to end: the same step through the C ABI from pinned host memory -------------
-    e2e = None
+    e2e = e2e_b = None
+    cpu_oracle = None
     if args.e2e_steps > 0:
         th = eng.generate("lineitem", rows, seed=args.seed, columns=Q1_COLS, row_offset=rank * rows,
                           location=capi.MEM_HOST)
         lh = th.lineitem()
-        eng.q6(lh)
-        eng.q1(lh)
-        h2d = d2h = 0
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier()
-        e0.record(stream)
-        for _ in range(args.e2e_steps):
+
+        def timed_e2e(step):
+            step()   # warm-up: sizes the streaming ring
+            h2d = d2h = 0
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            barrier()
+            e0.record(stream)
+            for _ in range(args.e2e_steps):
+                a, b = step()
+                h2d += a
+                d2h += b
+            e1.record(stream)
+            barrier()
+            ems = max_ms(e0.elapsed_time(e1))
+            return {"value": 2 * rows * world * args.e2e_steps / (ems * 1e-3), "unit": "rows/s",
+                    "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
+                    "ms_per_step": ems / args.e2e_steps, "h2d_gbs": h2d / (ems * 1e-3) / 1e9}
+
+        def plain_step():
             a, b = capi.Timing(), capi.Timing()
-            eng.q6(lh, timing=a)
-            eng.q1(lh, timing=b)
-            h2d += a.h2d_bytes + b.h2d_bytes
-            d2h += a.d2h_bytes + b.d2h_bytes
-        e1.record(stream)
-        barrier()
-        ems = e0.elapsed_time(e1)
-        if dist is not None:
-            m = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(m, op=dist.ReduceOp.MAX)
-            ems = float(m.item())
-        e2e = {"value": 2 * rows * world * args.e2e_steps / (ems * 1e-3), "unit": "rows/s",
-               "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
-               "ms_per_step": ems / args.e2e_steps,
-               "h2d_gbs": h2d / (ems * 1e-3) / 1e9}
+            out1 = capi.Q1Result()
+            got6 = eng.q6(lh, timing=a)
+            eng.q1(lh, timing=b, out=out1)
+            assert got6 == ref6 and bytes(out1) == ref1
+            return a.h2d_bytes + b.h2d_bytes, a.d2h_bytes + b.d2h_bytes
+
+        reqs = (capi.Request * 2)()
+        q6o, q1o = capi.Q6Result(), capi.Q1Result()
+        reqs[0].pipeline, reqs[0].li, reqs[0].q6 = capi.PIPE_Q6, C.pointer(lh), capi.Q6Params(365, 730, 5, 7, 24)
+        reqs[0].q6_out = C.pointer(q6o)
+        reqs[1].pipeline, reqs[1].li, reqs[1].q1 = capi.PIPE_Q1, C.pointer(lh), capi.Q1Params(2436, 0)
+        reqs[1].q1_out = C.pointer(q1o)
+
+        def batched_step():
+            tm = capi.Timing()
+            eng._check(eng.lib.gpudb_batch_run(eng.ctx, reqs, 2, C.byref(tm), None))
+            assert reqs[0].status == capi.OK and reqs[1].status == capi.OK
+            assert (q6o.revenue, q6o.rows_matched) == ref6 and bytes(q1o) == ref1
+            return tm.h2d_bytes, tm.d2h_bytes
+
+        e2e = timed_e2e(plain_step)
+        e2e_b = timed_e2e(batched_step)
+        e2e_b["call"] = "gpudb_batch_run with the Q6 and the Q1 request: each chunk copied once for both"
+        if rank == 0 and world == 1 and not (args.skip_cpu or args.skip_extra):
+            cpu_oracle = cpu_baseline_oracle({c: th.host_view(c) for c in Q1_COLS}, rows)
         eng.free(th)
 
-    cpu = cpu_baseline(rows, args.seed) if (rank == 0 and world == 1 and not args.skip_cpu) else None
+    extra = {}
+    if world == 1 and not args.skip_extra:
+        h2d = h2d_probe(local)
+        extra["h2d_probe_gbs"] = h2d
+        extra["pipelines"] = pipelines_block(eng, 10, not args.no_stream600m, h2d)
+        from gpudbmetalbenchmark_b200 import serve
+        extra["serve"] = serve.compare(eng, seconds=args.serve_seconds)
+
+    cpu = cpu_baseline(rows, args.seed) if (rank == 0 and world == 1 and not (args.skip_cpu or args.skip_extra)) \
+        else None
     if rank == 0:
+        pipes = {
+            "q1_cfg1b_60m": {"ms": q1_ms, "rows_per_s": rows / (q1_ms * 1e-3), "gbs_algorithmic": q1_gbs,
+                             "frac": q1_gbs / peak, "peak_kind": peak_kind},
+            "q6_cfg1a_60m": {"ms": q6_ms, "rows_per_s": rows / (q6_ms * 1e-3), "gbs_algorithmic": q6_gbs,
+                             "frac": q6_gbs / peak, "peak_kind": peak_kind,
+                             "traffic": (ncu_traffic("q6_vec_kernel") * rows if ncu_traffic("q6_vec_kernel") else None)},
+        }
+        if shared is not None:
+            shared["frac"] = shared["gbs_algorithmic"] / peak
+            pipes["q6_q1_shared_pass_60m"] = shared
+        pipes.update(extra.pop("pipelines", {}))
         line = {
             "metric": METRIC, "value": 2 * rows * world * K / (ms * 1e-3), "unit": "rows/s", "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded generator, inputs larger than L2)",
-            "config": {"workload": "config 1: Q6-like filtered sum (1a) + Q1-like 6-group aggregate (1b) over a "
-                                   "%d-row lineitem table per GPU" % rows,
-                       "rows_per_gpu": rows, "l2": "inputs %.2f GB per step > 126 MB L2, no flush needed" % (46 * rows / 1e9),
-                       "parallelism": "row shards, one per GPU" if world > 1 else "single GPU"},
+            "config": workload_config(rows, world),
             "roofline": {"bound": "hbm", "kernel": "q1_vec_smem_kernel", "achieved": q1_gbs, "peak": peak,
                          "unit": "GB/s", "frac": q1_gbs / peak, "peak_kind": peak_kind,
                          "traffic": (tr * rows if tr else None),
                          "algorithmic_bytes": Q1_BYTES_PER_ROW * rows, "ms_per_launch": q1_ms},
-            "pipelines": {
-                "q1": {"ms": q1_ms, "rows_per_s": rows / (q1_ms * 1e-3), "gbs": q1_gbs, "frac": q1_gbs / peak},
-                "q6": {"ms": q6_ms, "rows_per_s": rows / (q6_ms * 1e-3), "gbs_algorithmic": q6_gbs,
-                       "frac_algorithmic": q6_gbs / peak,
-                       "traffic": (ncu_traffic("q6_vec_kernel") * rows if ncu_traffic("q6_vec_kernel") else None)},
-            },
+            "pipelines": pipes,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "e2e": e2e,
+            "e2e_batched": e2e_b,
             "cpu_baseline": cpu,
+            "cpu_baseline_oracle": cpu_oracle,
         }
+        if merged is not None:
+            line["merged_result"] = merged
+        line.update(extra)
         print(json.dumps(line))
     eng.close()
     if dist is not None:

@@ -40,7 +40,9 @@ TBL_COLUMNS = {
 }
 OPT_NAMES = {1: "chunk_rows", 2: "q1_variant", 3: "q6_variant", 4: "ht_load_pct", 5: "radix_bits",
              6: "q9_smem_slots", 7: "q9_global_slots", 8: "graphs"}
-JOIN_GLOBAL, JOIN_RADIX = 0, 1
+JOIN_GLOBAL, JOIN_RADIX, JOIN_DIRECT, JOIN_AUTO = 0, 1, 2, 3
+JOIN_MODES = (JOIN_GLOBAL, JOIN_RADIX, JOIN_DIRECT)
+JOIN_NAMES = {JOIN_GLOBAL: "global", JOIN_RADIX: "radix", JOIN_DIRECT: "direct", JOIN_AUTO: "auto"}
 ORDERS_NONE, ORDERS_CLUSTERED, ORDERS_UNIFORM = 0, 1, 2
 Q3_MAX_K = 64
 # l_shipmode codes (alphabetical: ORDER BY l_shipmode)
@@ -69,6 +71,9 @@ class I128(C.Structure):
 
     def value(self):
         return (self.hi << 64) + self.lo
+
+    def set(self, v):
+        self.lo, self.hi = v & ((1 << 64) - 1), v >> 64
 
 
 class Exec(C.Structure):
@@ -241,7 +246,7 @@ class Q3Row(C.Structure):
 
 
 class Q3Result(C.Structure):
-    _fields_ = [("n_groups", C.c_uint64), ("n_rows", C.c_uint32), ("reserved", C.c_uint32),
+    _fields_ = [("n_groups", C.c_uint64), ("n_rows", C.c_uint32), ("join_mode", C.c_int32),
                 ("rows", Q3Row * Q3_MAX_K)]
 
 
@@ -350,6 +355,11 @@ PROTOTYPES = {
     "gpudb_tune_save": (C.c_int, [ctx_p, C.c_char_p]),
     "gpudb_tune_load": (C.c_int, [ctx_p, C.c_char_p, P(C.c_uint32)]),
     "gpudb_serve_warmup": (C.c_int, [vp, P(Request), C.c_uint32]),
+    "gpudb_q6_result_merge": (C.c_int, [P(Q6Result), C.c_uint32, P(Q6Result)]),
+    "gpudb_q1_result_merge": (C.c_int, [P(Q1Result), C.c_uint32, P(Q1Result)]),
+    "gpudb_q9_result_merge": (C.c_int, [P(Q9Group), P(C.c_uint32), C.c_uint32, P(Q9Group), C.c_uint32,
+                                        P(C.c_uint32)]),
+    "gpudb_q3_result_merge": (C.c_int, [P(Q3Result), C.c_uint32, C.c_int32, P(Q3Result)]),
 }
 
 _lib = None
@@ -375,3 +385,45 @@ class GpudbError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__("%s (%d): %s" % (ERROR_NAMES.get(code, "?"), code, msg))
         self.code = code
+
+
+# ---- shard merges (gpudb_*_result_merge: host-only, exact) ---------------------------------
+def merge_q6(parts):
+    """Q6 results of disjoint row shards -> their total."""
+    arr = (Q6Result * len(parts))(*parts)
+    out = Q6Result()
+    _check_merge(load().gpudb_q6_result_merge(arr, len(parts), C.byref(out)))
+    return out
+
+
+def merge_q1(parts):
+    """Q1 results of disjoint row shards -> the result of the union."""
+    arr = (Q1Result * len(parts))(*parts)
+    out = Q1Result()
+    _check_merge(load().gpudb_q1_result_merge(arr, len(parts), C.byref(out)))
+    return out
+
+
+def merge_q9(parts, capacity=4096):
+    """Q9 group lists [(nation, year, profit)] of disjoint fact shards -> merged list
+    (nation asc, year desc) and the group count."""
+    flat = [g for p in parts for g in p]
+    groups = (Q9Group * max(1, len(flat)))(*[Q9Group(*g) for g in flat])
+    counts = (C.c_uint32 * max(1, len(parts)))(*[len(p) for p in parts])
+    out = (Q9Group * capacity)()
+    n = C.c_uint32()
+    _check_merge(load().gpudb_q9_result_merge(groups, counts, len(parts), out, capacity, C.byref(n)))
+    return [(g.nation, g.year, g.profit) for g in out[:min(n.value, capacity)]], n.value
+
+
+def merge_q3(parts, k):
+    """Q3 results of shards with disjoint orders -> the top k of their union."""
+    arr = (Q3Result * len(parts))(*parts)
+    out = Q3Result()
+    _check_merge(load().gpudb_q3_result_merge(arr, len(parts), k, C.byref(out)))
+    return out
+
+
+def _check_merge(rc):
+    if rc != OK:
+        raise GpudbError(rc, "shard merge rejected its input")

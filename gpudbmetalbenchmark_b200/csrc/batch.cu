@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "q3.h"
+#include "scans.h"
 
 namespace gpudb {
 namespace {
@@ -494,6 +495,132 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
 }
 
 
+// ---- scans of host-resident tables ----------------------------------------------------
+// Q6/Q1 requests over one host-resident table (same host columns and row range) share its
+// chunked copy into HBM: the table streams once with the union of the columns the group
+// reads (26 B/row when a Q1 request is in it, 20 B/row for Q6 alone), and every request's
+// kernel runs on each chunk while it is resident (chunkedStreamLoop, src/infra.h:817-869,
+// copies a table once per query). A request's result is the single-request pipeline's:
+// the same kernels add into its own zeroed words chunk by chunk.
+constexpr uint32_t kMaxHostGroup = 64;   // requests per shared copy (result words in one big slot)
+
+bool host_scan_ok(const gpudb_request& r) {
+  const gpudb_lineitem* li = r.li;
+  if (!li || li->location != GPUDB_MEM_HOST) return false;
+  if (r.pipeline == GPUDB_PIPE_Q6) return li->ship_date && li->discount && li->quantity && li->ext_price;
+  return li->ship_date && li->quantity && li->ext_price && li->discount && li->tax && li->flag && li->status;
+}
+
+struct HostGroup {
+  gpudb_lineitem view;          // the row range as its own table; Q1 columns from the first Q1 member
+  bool has_q1 = false;
+  std::vector<uint32_t> members;
+};
+
+// Rows [begin, end) of `li` as a table of their own.
+gpudb_lineitem row_view(const gpudb_lineitem& li, uint64_t begin, uint64_t end) {
+  gpudb_lineitem v = li;
+  v.n_rows = end - begin;
+  auto adv = [begin](const void* p, size_t w) { return p ? (const void*)((const uint8_t*)p + begin * w) : nullptr; };
+  v.ship_date = (const int32_t*)adv(li.ship_date, 4);
+  v.quantity = (const int32_t*)adv(li.quantity, 4);
+  v.ext_price = (const int64_t*)adv(li.ext_price, 8);
+  v.discount = (const int32_t*)adv(li.discount, 4);
+  v.tax = (const int32_t*)adv(li.tax, 4);
+  v.flag = (const uint8_t*)adv(li.flag, 1);
+  v.status = (const uint8_t*)adv(li.status, 1);
+  return v;
+}
+
+int run_host_group(gpudb_ctx* ctx, gpudb_request* reqs, const HostGroup& g, gpudb_timing* t, const gpudb_exec* ex) {
+  const uint32_t m = (uint32_t)g.members.size();
+  const size_t status_bytes = ((m * 4 + 15) / 16) * 16;
+  std::vector<size_t> offs(m);
+  size_t bytes = status_bytes;
+  for (uint32_t k = 0; k < m; k++) {
+    offs[k] = bytes;
+    bytes += reqs[g.members[k]].pipeline == GPUDB_PIPE_Q6 ? kQ6ResultBytes : kQ1ResultBytes;
+  }
+  const uint32_t mask = LI_SHIP | LI_DISC | LI_QTY | LI_EXT | (g.has_q1 ? (LI_TAX | LI_FLAG | LI_STATUS) : 0u);
+  int rc = lineitem_check(ctx, &g.view, mask);
+  if (rc) return rc;
+  Call call(ctx, ex, t);
+  if ((rc = call.begin(bytes))) return rc;
+  uint8_t* dres = call.result<uint8_t>();
+  rc = stream_lineitem(call, &g.view, mask, 0, [&](const gpudb_lineitem& c) {
+    for (uint32_t k = 0; k < m; k++) {
+      const gpudb_request& q = reqs[g.members[k]];
+      const int r = q.pipeline == GPUDB_PIPE_Q6
+                        ? launch_q6(call, c, q.q6, dres + offs[k])
+                        : launch_q1(call, c, q.q1, dres + offs[k], reinterpret_cast<uint32_t*>(dres) + k);
+      if (r) return r;
+    }
+    return (int)GPUDB_OK;
+  });
+  if (rc) return rc;
+  const std::vector<uint32_t> members = g.members;
+  return call.finish(bytes, [reqs, members, offs, ctx](const uint8_t* h) {
+    for (size_t k = 0; k < members.size(); k++) {
+      gpudb_request& q = reqs[members[k]];
+      uint32_t st;
+      std::memcpy(&st, h + 4 * k, 4);
+      q.status = status_to_error(ctx, st);
+      const uint8_t* w = h + offs[k];
+      if (q.pipeline == GPUDB_PIPE_Q6) {
+        std::memcpy(&q.q6_out->revenue, w, 8);
+        std::memcpy(&q.q6_out->rows_matched, w + 8, 8);
+      } else {
+        q1_result_from(w, q.q1_out);
+      }
+      if (ctx->on_done) ctx->on_done(ctx->on_done_arg, &q.status);
+    }
+    return GPUDB_OK;
+  });
+}
+
+// Groups the host-table scan requests `ids` by table and row range and runs each group as
+// one streamed pass.
+void run_host_scans(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t>& ids, gpudb_timing* t,
+                    const gpudb_exec* ex) {
+  std::vector<HostGroup> groups;
+  for (uint32_t i : ids) {
+    const gpudb_request& q = reqs[i];
+    const gpudb_lineitem& li = *q.li;
+    const uint64_t end = q.row_end ? std::min<uint64_t>(q.row_end, li.n_rows) : li.n_rows;
+    const uint64_t begin = std::min<uint64_t>(q.row_begin, end);
+    const gpudb_lineitem v = row_view(li, begin, end);
+    const bool q1 = q.pipeline == GPUDB_PIPE_Q1;
+    HostGroup* hit = nullptr;
+    for (HostGroup& g : groups) {
+      const gpudb_lineitem& w = g.view;
+      if (g.members.size() >= kMaxHostGroup || w.n_rows != v.n_rows || w.ship_date != v.ship_date ||
+          w.quantity != v.quantity || w.discount != v.discount || w.ext_price != v.ext_price)
+        continue;
+      if (q1 && g.has_q1 && (w.tax != v.tax || w.flag != v.flag || w.status != v.status)) continue;
+      hit = &g;
+      break;
+    }
+    if (!hit) {
+      groups.emplace_back();
+      hit = &groups.back();
+      hit->view = v;
+    }
+    if (q1 && !hit->has_q1) {
+      hit->has_q1 = true;
+      hit->view.tax = v.tax;
+      hit->view.flag = v.flag;
+      hit->view.status = v.status;
+    }
+    hit->members.push_back(i);
+  }
+  for (const HostGroup& g : groups) {
+    const int rc = run_host_group(ctx, reqs, g, t, ex);
+    if (rc)
+      for (uint32_t i : g.members) reqs[i].status = rc;
+  }
+}
+
+
 }  // namespace
 }  // namespace gpudb
 
@@ -581,8 +708,9 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     te1 = event_get(ctx);
     if (te0) cudaEventRecord(te0, bs);
   }
-  std::vector<uint32_t> scans;
+  std::vector<uint32_t> scans, host_scans;
   size_t scan_bytes = 0;
+  const uint64_t h2d0 = ctx->h2d_total, d2h0 = ctx->d2h_total;
   auto flush_scans = [&]() -> int {
     if (scans.empty()) return GPUDB_OK;
     int rc = run_scan_batch(ctx, reqs, scans, async ? t : nullptr, &aex);
@@ -621,6 +749,10 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
           scan_bytes += b;
           break;
         }
+        if (n > 1 && host_scan_ok(q)) {   // shares the table's copy into HBM with the others
+          host_scans.push_back(i);
+          break;
+        }
         gpudb_lineitem view = q.li ? *q.li : gpudb_lineitem{};
         if (q.li && (q.row_begin || q.row_end)) {
           const uint64_t end = q.row_end ? std::min<uint64_t>(q.row_end, view.n_rows) : view.n_rows;
@@ -644,6 +776,7 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     if (rc != GPUDB_OK) q.status = rc;
   }
   flush_scans();
+  if (!host_scans.empty()) run_host_scans(ctx, reqs, host_scans, async ? t : nullptr, &aex);
   auto set_failed = [&](uint32_t i, int rc) {
     reqs[i].status = rc;
     if (!async)
@@ -694,7 +827,8 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     t->gpu_ms = ms;
     t->host_ms = now_ms() - host0;
     t->kernels = (uint32_t)(ctx->launches - launches0);
-    t->h2d_bytes = t->d2h_bytes = 0;
+    t->h2d_bytes = ctx->h2d_total - h2d0;
+    t->d2h_bytes = ctx->d2h_total - d2h0;
     t->chunks = 0;
   }
   event_put(ctx, te0);

@@ -191,6 +191,8 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
   size_t bytes = kSlotHeader + result_bytes;
   GPUDB_CUDA(ctx_, cudaMemcpyAsync(hslot_, dslot_, bytes, cudaMemcpyDeviceToHost, s_));
   d2h_ += bytes;
+  ctx_->h2d_total += h2d_;
+  ctx_->d2h_total += d2h_;
   gpudb_ctx* ctx = ctx_;
   int slot = slot_;
   bool big = big_;

@@ -45,6 +45,7 @@ struct gpudb_ctx {
   cudaStream_t copy_stream = nullptr;  // host->device copies of streamed chunks
   std::string err;
   uint64_t launches = 0;
+  uint64_t h2d_total = 0, d2h_total = 0;   // bytes moved by finished calls (batch timing)
   uint64_t chunk_rows = gpudb::kDefaultChunkRows;
   int scan_variant = 0;                // Q1 scan kernel choice (GPUDB_OPT_SCAN_VARIANT)
   int q6_variant = 0;                  // Q6 scan kernel choice (GPUDB_OPT_Q6_VARIANT)

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "scans.h"
 #include "tma.cuh"
 
 namespace gpudb {
@@ -191,13 +192,29 @@ __device__ __forceinline__ void q1_fold(Q1Acc& a, u128* partials, unsigned* tick
     partials[(size_t)blockIdx.x * 6 * kQ1Raw + threadIdx.x] = s;
   }
   if (!grid_last_block(ticket)) return;
-  if (threadIdx.x < 6 * kQ1Raw) {
-    u128 s = 0;
+  // the last block folds every block's partials: thread t sums metric t % 36 over the blocks
+  // b = t / 36, t / 36 + kLanes, ... (all threads, independent loads in flight), then the
+  // kLanes sums per metric are added up in shared memory (reusing `red`)
+  constexpr int kMetrics = 6 * kQ1Raw;
+  constexpr int kLanes = T / kMetrics;
+  static_assert(kLanes >= 1 && kLanes <= T / 32, "fold lanes fit the reduction buffer");
+  u128* fold = &red[0][0];
+  __syncthreads();
+  if (threadIdx.x < kLanes * kMetrics) {
+    const int m = threadIdx.x % kMetrics, l = threadIdx.x / kMetrics;
     const uint64_t* pp = reinterpret_cast<const uint64_t*>(partials);
-    for (unsigned b = 0; b < gridDim.x; b++) {
-      size_t i = ((size_t)b * 6 * kQ1Raw + threadIdx.x) * 2;
+    u128 s = 0;
+#pragma unroll 4
+    for (unsigned b = l; b < gridDim.x; b += kLanes) {
+      const size_t i = ((size_t)b * kMetrics + m) * 2;
       s += ((u128)__ldcg(pp + i + 1) << 64) | __ldcg(pp + i);
     }
+    fold[l * kMetrics + m] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < kMetrics) {
+    u128 s = 0;
+    for (int l = 0; l < kLanes; l++) s += fold[l * kMetrics + threadIdx.x];
     tot[threadIdx.x] = s;
   }
   __syncthreads();
@@ -675,8 +692,9 @@ int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, voi
 }
 
 // Enqueue one Q1 scan of device-resident columns, adding into `out` (device, 36 x u128).
-int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out) {
+int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status) {
   gpudb_ctx* ctx = call.ctx();
+  if (!status) status = call.status();
   if (c.n_rows == 0) return GPUDB_OK;
   const bool vec = aligned(c.ship_date, 16) && aligned(c.quantity, 16) && aligned(c.ext_price, 16) &&
                    aligned(c.discount, 16) && aligned(c.tax, 16) && aligned(c.flag, 4) && aligned(c.status, 4);
@@ -704,7 +722,7 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
     if (rc) return rc;
     GPUDB_LAUNCH(call, q1_vec_smem_kernel, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
                  (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
-                 (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, call.status());
+                 (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status);
     return GPUDB_OK;
   }
   if ((variant == 1 || variant >= 4) && !tma_ok) variant = vec ? 2 : 3;
@@ -731,7 +749,7 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
       const uint64_t rows = std::min<uint64_t>(per_launch, c.n_rows - r0);
       GPUDB_LAUNCH(call, kernel, grid, threads, smem, c.ship_date + r0, c.quantity + r0, c.ext_price + r0,
                    c.discount + r0, c.tax + r0, c.flag + r0, c.status + r0, rows, p.ship_le, (u128*)part, ticket,
-                   (u128*)out, call.status());
+                   (u128*)out, status);
     }
     return GPUDB_OK;
   }
@@ -745,10 +763,10 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
   if (variant == 2) {
     GPUDB_LAUNCH(call, q1_vec_kernel, grid, kThreads, 0, (const int4*)c.ship_date, (const int4*)c.quantity,
                  (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
-                 (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, call.status());
+                 (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status);
   } else {
     GPUDB_LAUNCH(call, q1_row_kernel, grid, kThreads, 0, c.ship_date, c.quantity, c.ext_price, c.discount, c.tax,
-                 c.flag, c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, call.status());
+                 c.flag, c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status);
   }
   return GPUDB_OK;
 }
@@ -785,25 +803,34 @@ extern "C" int gpudb_q1_group6(gpudb_ctx* ctx, const gpudb_lineitem* li, const g
   int rc = lineitem_check(ctx, li, mask);
   if (rc) return rc;
   Call call(ctx, ex, t);
-  const size_t bytes = 6 * kQ1Metrics * sizeof(u128);
+  const size_t bytes = kQ1ResultBytes;
+  static_assert(kQ1ResultBytes == 6 * kQ1Metrics * sizeof(u128), "Q1 result layout");
   if ((rc = call.begin(bytes))) return rc;
   const gpudb_q1_params pp = *p;
   void* dout = call.result<void>();
   rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) { return launch_q1(call, c, pp, dout); });
   if (rc) return rc;
   return call.finish(bytes, [out](const uint8_t* h) {
-    std::memset(out, 0, sizeof *out);
-    for (int g = 0; g < 6; g++) {
-      uint64_t w[12];
-      std::memcpy(w, h + g * kQ1Metrics * 16, sizeof w);
-      if (w[0] == 0 && w[1] == 0) continue;
-      gpudb_q1_group& o = out->groups[out->n_groups++];
-      o.flag = (uint8_t)(g / 2);
-      o.status = (uint8_t)(g % 2);
-      o.count = w[0];
-      gpudb_i128* f[5] = {&o.sum_qty, &o.sum_base_price, &o.sum_disc_price, &o.sum_charge, &o.sum_discount};
-      for (int m = 0; m < 5; m++) { f[m]->lo = w[2 + 2 * m]; f[m]->hi = (int64_t)w[3 + 2 * m]; }
-    }
+    q1_result_from(h, out);
     return GPUDB_OK;
   });
 }
+
+namespace gpudb {
+
+void q1_result_from(const uint8_t* h, gpudb_q1_result* out) {
+  std::memset(out, 0, sizeof *out);
+  for (int g = 0; g < 6; g++) {
+    uint64_t w[12];
+    std::memcpy(w, h + g * kQ1Metrics * 16, sizeof w);
+    if (w[0] == 0 && w[1] == 0) continue;
+    gpudb_q1_group& o = out->groups[out->n_groups++];
+    o.flag = (uint8_t)(g / 2);
+    o.status = (uint8_t)(g % 2);
+    o.count = w[0];
+    gpudb_i128* f[5] = {&o.sum_qty, &o.sum_base_price, &o.sum_disc_price, &o.sum_charge, &o.sum_discount};
+    for (int m = 0; m < 5; m++) { f[m]->lo = w[2 + 2 * m]; f[m]->hi = (int64_t)w[3 + 2 * m]; }
+  }
+}
+
+}  // namespace gpudb

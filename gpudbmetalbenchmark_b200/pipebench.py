@@ -38,28 +38,98 @@ def timed(fn, reps):
     return statistics.median(t.gpu_ms for t in ts), ts[-1]
 
 
-def emit(name, config, rows, ms, alg_bytes, extra=None):
+def record(name, config, rows, ms, alg_bytes, extra=None):
+    """One measurement: device ms, rows/s, algorithmic GB/s and its fraction of the HBM
+    peak (`peak_kind` says whether that peak is the measured one or the fallback)."""
     pk, kind = peak()
     gbs = alg_bytes / (ms * 1e-3) / 1e9
     line = {"pipeline": name, "config": config, "rows": rows, "ms": round(ms, 4),
             "rows_per_s": rows / (ms * 1e-3), "algorithmic_bytes": alg_bytes, "gbs_algorithmic": round(gbs, 1),
-            "frac_of_%s_peak" % kind: round(gbs / pk, 3)}
+            "frac": round(gbs / pk, 3), "peak_gbs": pk, "peak_kind": kind}
     if extra:
         line.update(extra)
+    return line
+
+
+def emit(name, config, rows, ms, alg_bytes, extra=None):
+    line = record(name, config, rows, ms, alg_bytes, extra)
     print(json.dumps(line), flush=True)
+    return line
 
 
-def q3_case(eng, n_cu, n_or, n_li, reps, label):
+Q3_MODES = ((capi.JOIN_DIRECT, "direct"), (capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix"))
+
+
+def q3_case(eng, n_cu, n_or, n_li, reps, label, out=emit):
+    """Q3 join + top-10 on the config-2 tables (1x: 150K/1.5M/6M rows) in every join mode;
+    returns {mode: record}."""
     cu = eng.generate("customer", n_cu, seed=42)
     od = eng.generate("orders", n_or, seed=42, n_cust=n_cu)
     li = eng.generate("lineitem", n_li, seed=42, columns=("order_key", "ship_date", "ext_price", "discount"),
                       n_orders=n_or, order_mode=capi.ORDERS_CLUSTERED)
     alg = n_cu * 5 + n_or * 12 + n_li * 20
-    for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix")):
+    res = {}
+    for mode, mname in Q3_MODES:
         ms, t = timed(lambda tm: eng.q3(cu, od, li, join_mode=mode, timing=tm), reps)
-        emit("q3_join_topk", "%s, %s table" % (label, mname), n_li, ms, alg, {"kernels": t.kernels})
+        res[mname] = out("q3_join_topk", "%s, %s table" % (label, mname), n_li, ms, alg, {"kernels": t.kernels})
     for x in (cu, od, li):
         eng.free(x)
+    return res
+
+
+def scan_case(eng, rows, reps, out=emit):
+    """Q6 and Q1 over a device-resident lineitem table of `rows` rows: (q6, q1) records."""
+    t = eng.generate("lineitem", rows, seed=42, columns=Q1_COLS)
+    ms6, _ = timed(lambda tm: eng.q6(t, timing=tm), reps)
+    r6 = out("q6_sum", "config %s" % ("1a" if rows > 6e6 else "1a at 6M"), rows, ms6, 20 * rows,
+             {"note": "6M rows = 120 MB, inside L2" if rows == 6_000_000 else ""})
+    ms1, t1 = timed(lambda tm: eng.q1(t, timing=tm), reps)
+    r1 = out("q1_group6", "config %s" % ("1b" if rows > 6e6 else "0"), rows, ms1, 26 * rows,
+             {"note": "6M rows = 156 MB" if rows == 6_000_000 else "", "kernels": t1.kernels})
+    eng.free(t)
+    return r6, r1
+
+
+def q9_case(eng, reps, stream600m=False, out=emit):
+    """Q9 star join on the config-3 tables at 60M fact rows (HBM-resident) and, with
+    stream600m, at 600M fact rows streamed from pinned host memory in 64M-row chunks."""
+    res = {}
+    pa, su, ps, od = q9_tables(eng, 2_000_000, 100_000, 15_000_000)
+    cols = ("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity")
+    li = eng.generate("lineitem", 60_000_000, seed=42, columns=cols, n_orders=15_000_000, n_parts=2_000_000,
+                      n_supp=100_000, order_mode=capi.ORDERS_UNIFORM)
+    ms, t = timed(lambda tm: eng.q9(pa, su, ps, od, li, timing=tm), reps)
+    res["resident"] = out("q9_star", "config 3 (HBM-resident)", 60_000_000, ms,
+                          60_000_000 * 28 + 8_000_000 * 16 + 15_000_000 * 8 + 2_000_000 + 100_000, {"kernels": t.kernels})
+    eng.free(li)
+    if stream600m:
+        rows = 600_000_000
+        lh = eng.generate("lineitem", rows, seed=42, columns=cols, n_orders=15_000_000, n_parts=2_000_000,
+                          n_supp=100_000, order_mode=capi.ORDERS_UNIFORM, location=capi.MEM_HOST)
+        ms, t = timed(lambda tm: eng.q9(pa, su, ps, od, lh, chunk_rows=64 << 20, timing=tm), max(2, reps // 10))
+        res["streamed"] = out("q9_star", "config 3 streamed (600M rows, 64M-row chunks, pinned host)", rows, ms,
+                              rows * 28, {"chunks": t.chunks, "h2d_gbs": t.h2d_bytes / (ms * 1e-3) / 1e9,
+                                          "bound": "host link", "kernels": t.kernels})
+        eng.free(lh)
+    for x in (pa, su, ps, od):
+        eng.free(x)
+    return res
+
+
+def join_count_case(eng, reps, out=emit):
+    """Join microbenchmark: 15M-key build x 60M-key probe, global table and radix partitions."""
+    b = eng.generate("orders", 15_000_000, seed=42, columns=("order_key",))
+    p = eng.generate("lineitem", 60_000_000, seed=42, columns=("order_key",), n_orders=15_000_000,
+                     order_mode=capi.ORDERS_CLUSTERED)
+    res = {}
+    for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix")):
+        ms, t = timed(lambda tm: eng.hash_join_count(b.ptr("order_key"), 15_000_000, p.ptr("order_key"),
+                                                     60_000_000, mode, timing=tm), reps)
+        res[mname] = out("hash_join_count", "15M build x 60M probe, %s" % mname, 60_000_000, ms, 75_000_000 * 4,
+                         {"kernels": t.kernels})
+    eng.free(b)
+    eng.free(p)
+    return res
 
 
 def q9_tables(eng, n_pa, n_su, n_or):
@@ -214,14 +284,7 @@ def main(argv=None):
 
     if on("scans"):
         for rows in (6_000_000, 60_000_000):
-            t = eng.generate("lineitem", rows, seed=42, columns=Q1_COLS)
-            ms, _ = timed(lambda tm: eng.q6(t, timing=tm), a.reps)
-            emit("q6_sum", "config %s" % ("1a" if rows > 6e6 else "1a at 6M"), rows, ms, 20 * rows,
-                 {"note": "6M rows = 120 MB, inside L2" if rows == 6_000_000 else ""})
-            ms, _ = timed(lambda tm: eng.q1(t, timing=tm), a.reps)
-            emit("q1_group6", "config %s" % ("1b" if rows > 6e6 else "0"), rows, ms, 26 * rows,
-                 {"note": "6M rows = 156 MB" if rows == 6_000_000 else ""})
-            eng.free(t)
+            scan_case(eng, rows, a.reps)
     if on("q3"):
         q3_case(eng, 150_000, 1_500_000, 6_000_000, a.reps, "config 2 (1x)")
         q3_case(eng, 1_500_000, 15_000_000, 60_000_000, max(3, a.reps // 4), "config 2 (10x)")
@@ -288,26 +351,7 @@ def main(argv=None):
             eng.free(od)
             eng.free(cu)
     if on("q9"):
-        pa, su, ps, od = q9_tables(eng, 2_000_000, 100_000, 15_000_000)
-        li = eng.generate("lineitem", 60_000_000, seed=42,
-                          columns=("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity"),
-                          n_orders=15_000_000, n_parts=2_000_000, n_supp=100_000, order_mode=capi.ORDERS_UNIFORM)
-        ms, t = timed(lambda tm: eng.q9(pa, su, ps, od, li, timing=tm), a.reps)
-        emit("q9_star", "config 3 (HBM-resident)", 60_000_000, ms, 60_000_000 * 28 + 8_000_000 * 16 + 15_000_000 * 8
-             + 2_000_000 + 100_000, {"kernels": t.kernels})
-        eng.free(li)
-        if a.stream600m:
-            rows = 600_000_000
-            lh = eng.generate("lineitem", rows, seed=42,
-                              columns=("part_key", "supp_key", "order_key", "ext_price", "discount", "quantity"),
-                              n_orders=15_000_000, n_parts=2_000_000, n_supp=100_000, order_mode=capi.ORDERS_UNIFORM,
-                              location=capi.MEM_HOST)
-            ms, t = timed(lambda tm: eng.q9(pa, su, ps, od, lh, chunk_rows=64 << 20, timing=tm), max(2, a.reps // 10))
-            emit("q9_star", "config 3 streamed (600M rows, 64M-row chunks, pinned host)", rows, ms, rows * 28,
-                 {"chunks": t.chunks, "h2d_gbs": t.h2d_bytes / (ms * 1e-3) / 1e9, "bound": "host link"})
-            eng.free(lh)
-        for x in (pa, su, ps, od):
-            eng.free(x)
+        q9_case(eng, a.reps, a.stream600m)
     if on("batch"):
         batch_cases(eng, a.reps)
     if on("tbl"):
@@ -322,15 +366,7 @@ def main(argv=None):
         emit("sum_i32", "aggregation", rows, ms, rows * 4)
         eng.device_free(bits)
         eng.free(t)
-        b = eng.generate("orders", 15_000_000, seed=42, columns=("order_key",))
-        p = eng.generate("lineitem", 60_000_000, seed=42, columns=("order_key",), n_orders=15_000_000,
-                         order_mode=capi.ORDERS_CLUSTERED)
-        for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix")):
-            ms, _ = timed(lambda tm: eng.hash_join_count(b.ptr("order_key"), 15_000_000, p.ptr("order_key"),
-                                                         60_000_000, mode, timing=tm), max(3, a.reps // 4))
-            emit("hash_join_count", "15M build x 60M probe, %s" % mname, 60_000_000, ms, 75_000_000 * 4)
-        eng.free(b)
-        eng.free(p)
+        join_count_case(eng, max(3, a.reps // 4))
     eng.close()
     return 0
 

@@ -223,6 +223,59 @@ def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None):
             st["completed"] / max(1, st["batches"]), "all_ok": ok, "bit_exact_vs_solo": exact}
 
 
+def compare(eng, seconds=1.0, lanes=4, max_batch=64, load=0.85, factor=3.0, seed=11):
+    """Served form against the plain one-query-per-launch form on the same mixed stream.
+
+    1. plain saturation: requests submitted back to back (closed loop), queries/s;
+    2. plain at `load` x its saturation rate (Poisson): queries/s, p50, p99;
+    3. served at the same offered rate: p50, p99;
+    4. served at `factor` x that rate: queries/s, p50, p99 (the ">= 3x the queries/s at
+       equal or lower p99" comparison is 4 against 2);
+    5. served saturation (closed loop).
+    Every result of every run is compared with the same request run alone."""
+    wl = Workload(eng)
+    out = {"lanes": lanes, "max_batch": max_batch, "seconds_per_rate": seconds,
+           "workload": "Q6/Q1 over lineitem at 1M/6M/60M rows, Q3 at config-2 1x, Q9 at 6M fact rows; "
+                       "random pipeline and constants per request, Poisson arrivals"}
+
+    solos = {}
+
+    def run(name, ln, mb, rate, n, sd):
+        if (n, sd) not in solos:
+            solos[(n, sd)] = wl.solo_results(wl.jobs(n, sd))
+        return _run_checked(eng, wl, name, ln, mb, rate, n, sd, wl.jobs(n, sd), solos[(n, sd)])
+
+    sat = run("plain", 1, 1, 1e9, 3000, seed)
+    out["plain_saturation"] = sat
+    rate = load * sat["achieved_qps"]
+    n = max(500, int(rate * seconds))
+    out["plain"] = run("plain", 1, 1, rate, n, seed + 1)
+    out["served_same_rate"] = run("served", lanes, max_batch, rate, n, seed + 1)
+    n3 = max(500, int(factor * rate * seconds))
+    out["served"] = run("served", lanes, max_batch, factor * rate, n3, seed + 2)
+    out["served_saturation"] = run("served", lanes, max_batch, 1e9, max(4000, n3), seed + 3)
+    p, s = out["plain"], out["served"]
+    out["qps_ratio"] = s["achieved_qps"] / p["achieved_qps"]
+    out["p99_ratio"] = s["p99_ms"] / p["p99_ms"]
+    out["bit_exact"] = all(out[k]["bit_exact_vs_solo"] and out[k]["all_ok"]
+                           for k in ("plain_saturation", "plain", "served_same_rate", "served", "served_saturation"))
+    return out
+
+
+def _run_checked(eng, wl, name, lanes, max_batch, rate, n, seed, jobs, solo):
+    srv = Server(lanes=lanes, max_batch=max_batch)
+    try:
+        srv.warmup(wl.jobs(max(max_batch, 16), seed + 7))
+        lat, status, wall = open_loop(srv, jobs, rate, seed + 1)
+        st = srv.stats()
+    finally:
+        srv.close()
+    return {"mode": name, "offered_qps": None if rate >= 1e9 else rate, "requests": n, "achieved_qps": n / wall,
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mean_batch": st["completed"] / max(1, st["batches"]),
+            "all_ok": all(x == capi.OK for x in status),
+            "bit_exact_vs_solo": all(j.result() == w for j, w in zip(jobs, solo))}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--rates", type=float, nargs="*", default=[1000, 2000, 4000, 8000, 16000, 32000])

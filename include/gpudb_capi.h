@@ -49,7 +49,12 @@ enum {
 };
 
 enum { GPUDB_MEM_DEVICE = 0, GPUDB_MEM_HOST = 1 };
-enum { GPUDB_JOIN_GLOBAL = 0, GPUDB_JOIN_RADIX = 1 };
+/* Join modes. GLOBAL: one open-addressing hash table; RADIX: both sides hash-partitioned,
+ * each partition joined in shared memory; DIRECT (Q3): an order-key bitmap and a direct map
+ * key -> slot, the reference's orders_map (kernels/q3.metal:59-78); AUTO (Q3): DIRECT when the
+ * map of the orders' key range fits 30% of device memory (the reference's rule,
+ * src/q3.cpp:246), else GLOBAL. */
+enum { GPUDB_JOIN_GLOBAL = 0, GPUDB_JOIN_RADIX = 1, GPUDB_JOIN_DIRECT = 2, GPUDB_JOIN_AUTO = 3 };
 
 typedef struct gpudb_ctx gpudb_ctx;
 
@@ -224,17 +229,21 @@ int gpudb_q6_sum(gpudb_ctx* ctx, const gpudb_lineitem* li, const gpudb_q6_params
                  gpudb_q6_result* out, gpudb_timing* t, const gpudb_exec* ex);
 
 /* Q6-like filtered sum that allocates nothing. No counterpart in the reference: it exists
- * for callers that cannot call cudaMalloc -- code running while a stream is captured into a
- * CUDA graph, programs whose device memory is owned by another memory manager, and plugins
- * that have no gpudb_ctx. It needs no context. li must be device-resident; `out` is a
+ * for callers that cannot call cudaMalloc -- programs whose device memory is owned and
+ * budgeted by another memory manager (a server that hands out all of the GPU), and plugins
+ * that have no gpudb_ctx (the context owns every other call's scratch memory). It needs no
+ * context. li must be device-resident; `out` is a
  * caller-owned device buffer of two int64 (revenue, rows matched) that the call overwrites;
  * the work is enqueued on `stream` (a cudaStream_t, NULL = default stream) of the current
  * device and the call does not wait for it. Scratch is a fixed 262,400-byte static device
  * array that every GPU loading this library holds until exit, so li->n_rows is limited to
  * 67,108,864 rows (GPUDB_E_CAPACITY beyond). The first call on a device looks up that
  * array's device address (cudaGetSymbolAddress); make that first call before any stream
- * capture. All calls on a device share the one array: calls that overlap on the GPU (for
- * example on two streams at once) race and give wrong results. */
+ * capture. The address is kept for the life of the process, so a device reset after that
+ * first call is not supported. All calls on a device share the one array: calls that
+ * overlap on the GPU (for example on two streams at once) race and give wrong results. A
+ * launch failure returns GPUDB_E_CUDA; an error already pending from the caller's own
+ * earlier CUDA work is left in place for the caller. */
 int gpudb_q6_sum_noalloc(const gpudb_lineitem* li, const gpudb_q6_params* p, int64_t* out, void* stream);
 
 /* ---- Q1-like filter + 6-group aggregate (replaces runQ1Benchmark src/q1.cpp:8-173 and
@@ -268,14 +277,15 @@ typedef struct gpudb_q3_params {
   int32_t order_date_lt;       /* orders.order_date < order_date_lt */
   int32_t ship_date_gt;        /* lineitem.ship_date > ship_date_gt */
   int32_t k;                   /* rows of the top-k, 1..GPUDB_Q3_MAX_K */
-  int32_t join_mode;           /* GPUDB_JOIN_GLOBAL or GPUDB_JOIN_RADIX */
+  int32_t join_mode;           /* GPUDB_JOIN_GLOBAL, _RADIX, _DIRECT (needs orders.key_max) or _AUTO */
   int32_t radix_bits;          /* radix mode: partition bits, 0 = chosen from the build size */
 } gpudb_q3_params;
 typedef struct gpudb_q3_row { int32_t order_key; int32_t order_date; int64_t revenue; } gpudb_q3_row;
 /* Rows ordered by revenue desc, order_date asc, order_key asc. revenue is in hundredths^2. */
 typedef struct gpudb_q3_result {
   uint64_t n_groups;           /* orders with at least one joined lineitem row */
-  uint32_t n_rows; uint32_t reserved;
+  uint32_t n_rows;
+  int32_t join_mode;           /* the mode that ran (AUTO resolved) */
   gpudb_q3_row rows[GPUDB_Q3_MAX_K];
 } gpudb_q3_result;
 int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, const gpudb_orders* od,
@@ -599,6 +609,21 @@ int gpudb_serve_warmup(gpudb_server* s, gpudb_request* reqs, uint32_t n);
 uint64_t gpudb_request_footprint(const gpudb_request* req);
 /* Stops accepting requests, finishes the queued ones, and frees the lanes. */
 int gpudb_serve_close(gpudb_server* s);
+
+/* ---- merging shard results (the reference runs on one device and merges nothing; these
+ *      combine the results of row shards, one per GPU or per call) ------------------------
+ * Host-only and exact: they need no context and no GPU. Q6 and Q1 partials of disjoint row
+ * ranges add (int64 / int128 sums); Q9 groups of disjoint fact rows add per (nation, year)
+ * and come out ordered by nation asc, year desc; Q3 top-k lists merge into the top k of
+ * their union when the shards hold disjoint sets of orders (lineitem split by order key, so
+ * each order's revenue is complete in one shard). */
+int gpudb_q6_result_merge(const gpudb_q6_result* parts, uint32_t n, gpudb_q6_result* out);
+int gpudb_q1_result_merge(const gpudb_q1_result* parts, uint32_t n, gpudb_q1_result* out);
+/* groups: the parts' groups back to back, counts[i] of part i; at most `capacity` groups
+ * written, *n_out the total. */
+int gpudb_q9_result_merge(const gpudb_q9_group* groups, const uint32_t* counts, uint32_t n,
+                          gpudb_q9_group* out, uint32_t capacity, uint32_t* n_out);
+int gpudb_q3_result_merge(const gpudb_q3_result* parts, uint32_t n, int32_t k, gpudb_q3_result* out);
 
 #ifdef __cplusplus
 }

@@ -4,8 +4,9 @@
   oracle/_ref/libgpudbref.so   the reference's own kernels (kernels/*.metal of
                                nd-tung/GPUDBMetalBenchmark) compiled in place for the CPU
                                through oracle/refshim; built only where the reference
-                               source tree is present (GPUDB_REFERENCE_DIR, default
-                               /root/reference). Elsewhere the prebuilt file is used.
+                               source tree is present (GPUDB_REFERENCE_DIR, else a
+                               checkout named `reference` beside this repository).
+                               Elsewhere the prebuilt file is used.
 
 Usage: python oracle/build.py
 """
@@ -14,7 +15,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DIR = os.environ.get("GPUDB_REFERENCE_DIR", "/root/reference")
+REF_DIR = os.environ.get("GPUDB_REFERENCE_DIR",
+                         os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 def _run(cmd):

@@ -179,6 +179,68 @@ def test_streamed_host_table(engine, orc, chunk):
         engine.free(t)
 
 
+def _scan_requests(li_struct, params):
+    """gpudb_request array of ("q6", (lo, hi, dlo, dhi, qlt), rows) and ("q1", (ship_le,),
+    rows) requests over one table (rows = (begin, end) or None), with their result structs."""
+    reqs = (capi.Request * len(params))()
+    outs = []
+    for r, (kind, args, rows) in zip(reqs, params):
+        r.li = C.pointer(li_struct)
+        if kind == "q6":
+            r.pipeline, r.q6 = capi.PIPE_Q6, capi.Q6Params(*args)
+            o = capi.Q6Result()
+            r.q6_out = C.pointer(o)
+        else:
+            r.pipeline, r.q1 = capi.PIPE_Q1, capi.Q1Params(args[0], 0)
+            o = capi.Q1Result()
+            r.q1_out = C.pointer(o)
+        if rows:
+            r.row_begin, r.row_end = rows
+        outs.append(o)
+    return reqs, outs
+
+
+@pytest.mark.parametrize("chunk", [16, 1000, 33_333, 64 << 20])
+def test_batched_scans_of_host_table_share_the_copy(engine, orc, chunk):
+    """Q6 and Q1 requests over one host-resident table in one batch: the table crosses the
+    host link once (26 B/row for the union of the columns), and every result equals the
+    oracle's, bit-exactly, with ragged chunks and row ranges."""
+    from gpudbmetalbenchmark_b200.engine import q1_to_dict
+    n = 100_003
+    li = orc.lineitem(n, seed=23)
+    t = engine.upload("lineitem", li, location=capi.MEM_HOST)
+    ls = t.lineitem()
+    sub = lambda a, b: {k: v[a:b] for k, v in li.items()}  # noqa: E731
+
+    def check(params, h2d=None):
+        reqs, outs = _scan_requests(ls, params)
+        tm = capi.Timing()
+        engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, len(params), C.byref(tm), None))
+        if h2d is not None:
+            assert tm.h2d_bytes == h2d
+        for r, o, (kind, args, rows) in zip(reqs, outs, params):
+            assert r.status == capi.OK
+            part = sub(*rows) if rows else li
+            if kind == "q6":
+                assert (o.revenue, o.rows_matched) == orc.q6(part, *args)
+            else:
+                assert q1_to_dict(o) == orc.q1(part, args[0])
+
+    try:
+        engine.set_chunk_rows(chunk)
+        check([("q6", (365, 730, 5, 7, 24), None), ("q1", (2436,), None), ("q6", (0, 2527, 0, 10, 51), None),
+               ("q1", (1200,), None), ("q6", (100, 900, 2, 8, 30), None)], h2d=26 * n)
+        # Q6 alone: only its four columns cross
+        check([("q6", (365, 730, 5, 7, 24), None), ("q6", (0, 1000, 3, 9, 40), None)], h2d=20 * n)
+        # row ranges: each range streams once for the requests over it
+        check([("q6", (365, 730, 5, 7, 24), (1000, 60_001)), ("q1", (2436,), (7, 99_000)),
+               ("q1", (2000,), (7, 99_000)), ("q6", (0, 2527, 0, 10, 51), (7, 99_000))],
+              h2d=20 * 59_001 + 26 * 98_993)
+    finally:
+        engine.set_chunk_rows(64 << 20)
+        engine.free(t)
+
+
 def test_async_calls_complete_at_sync(engine, orc):
     n = 200_000
     li = orc.lineitem(n, seed=4)
