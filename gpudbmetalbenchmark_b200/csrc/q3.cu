@@ -261,6 +261,18 @@ __global__ void __launch_bounds__(256) q3_probe_kernel(const int32_t* __restrict
   }
 }
 
+// Hit counts of the dense slots between `count` and the next multiple of 128 (at least 128)
+// are zeroed and that capacity is published: the top-k passes read whole 128-slot chunks.
+__device__ __forceinline__ void seal_dense_slots(const uint32_t* count, uint32_t* hits, uint32_t* cap_out) {
+  const uint32_t c = *count, cap = max(128u, (c + 127u) & ~127u);
+  for (uint32_t i = c + threadIdx.x; i < cap; i += blockDim.x) hits[i] = 0;
+  if (threadIdx.x == 0) *cap_out = cap;
+}
+
+__global__ void q3_seal_kernel(const uint32_t* count, uint32_t* hits, uint32_t* cap_out) {
+  seal_dense_slots(count, hits, cap_out);
+}
+
 // ---- direct mode ---------------------------------------------------------------------
 // The orders filter gave every qualifying order a dense slot and set its bit in the order-key
 // bitmap; the direct map omap (order key -> slot) is read only where that bit is set, so it is
@@ -278,11 +290,7 @@ __global__ void __launch_bounds__(256) q3_direct_probe_kernel(
     const int32_t* __restrict__ ldisc, uint64_t n, int32_t ship_gt, const uint32_t* __restrict__ okbm,
     const int32_t* __restrict__ omap, int32_t key_max, Q3Slot* ht, uint32_t* hits, const uint32_t* count,
     uint32_t* cap_out) {
-  if (blockIdx.x == 0) {
-    const uint32_t c = *count, cap = max(128u, (c + 127u) & ~127u);
-    for (uint32_t i = c + threadIdx.x; i < cap; i += blockDim.x) hits[i] = 0;
-    if (threadIdx.x == 0) *cap_out = cap;
-  }
+  if (blockIdx.x == 0) seal_dense_slots(count, hits, cap_out);
   const int lane = threadIdx.x & 31;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   constexpr int U = kDirectBatches;
@@ -382,7 +390,6 @@ __global__ void q3_fact_filter_kernel(const int32_t* __restrict__ lkey, const in
 
 constexpr uint32_t kQ3PartCap = 4096;               // shared slots per partition table
 constexpr uint32_t kQ3PartChunk = kQ3PartCap / 2;   // build rows per chunk
-constexpr int kQ3SlotsPerRound = kTopkThreads * (kTopkPerThread - 1);   // table slots per top-k round
 
 // Fact rows of a device-resident lineitem table for the radix mode: a row takes part when
 // ship_date > ship_gt; its payload is ext_price * (100 - discount). The first partitioning
@@ -405,28 +412,25 @@ struct Q3FactSource {
   }
 };
 
-constexpr size_t q3_partition_smem() {
-  return (size_t)kQ3PartCap * (8 + 4 + 4 + 4) + (size_t)kTopkScratch * sizeof(u128);
-}
+constexpr size_t q3_partition_smem() { return (size_t)kQ3PartCap * (8 + 4 + 4 + 4); }
 
 // One block per partition: shared table of the partition's orders (in chunks), probe of its
-// fact rows with shared 64-bit atomics, then a block top-k carried across chunks (the table
-// in rounds of kQ3SlotsPerRound slots, the carry riding along).
+// fact rows with shared 64-bit atomics, then the chunk's groups (orders with a joined row)
+// are appended to the dense slot array (one reservation per block per chunk); the top-k runs
+// over the dense slots afterwards, as in the other modes.
 __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
     const int32_t* __restrict__ bk, const int32_t* __restrict__ bdate, const uint32_t* __restrict__ boff,
-    const int32_t* __restrict__ pk, const int64_t* __restrict__ pval, const uint32_t* __restrict__ poff, int k,
-    u128* cand, unsigned long long* groups, uint32_t* status) {
+    const int32_t* __restrict__ pk, const int64_t* __restrict__ pval, const uint32_t* __restrict__ poff,
+    Q3Slot* __restrict__ dense, uint32_t* __restrict__ dense_hits, uint32_t* dense_count, uint32_t* status) {
   extern __shared__ __align__(16) unsigned char q3p_pool[];
-  __shared__ u128 carry[GPUDB_Q3_MAX_K];
+  __shared__ uint32_t sh[33];
   unsigned long long* hrev = reinterpret_cast<unsigned long long*>(q3p_pool);
   int32_t* hkey = reinterpret_cast<int32_t*>(hrev + kQ3PartCap);
   int32_t* hdate = hkey + kQ3PartCap;
   uint32_t* hhit = reinterpret_cast<uint32_t*>(hdate + kQ3PartCap);
-  u128* topk_scratch = reinterpret_cast<u128*>(hhit + kQ3PartCap);
   const uint32_t part = blockIdx.x, mask = kQ3PartCap - 1;
   const uint32_t b0 = boff[part], b1 = boff[part + 1], p0 = poff[part], p1 = poff[part + 1];
-  for (int i = threadIdx.x; i < k; i += kTopkThreads) carry[i] = 0;
-  uint32_t ngroups = 0;
+  constexpr uint32_t kPerThread = kQ3PartCap / kTopkThreads;
   for (uint32_t c0 = b0; c0 < b1; c0 += kQ3PartChunk) {
     const uint32_t c1 = min(c0 + kQ3PartChunk, b1);
     for (uint32_t i = threadIdx.x; i < kQ3PartCap; i += kTopkThreads) { hkey[i] = kEmptyKey; hrev[i] = 0; hhit[i] = 0; }
@@ -452,23 +456,23 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
       }
     }
     __syncthreads();
-    for (uint32_t r0 = 0; r0 < kQ3PartCap; r0 += kQ3SlotsPerRound) {
-      u128 v[kTopkPerThread];
+    // append the chunk's groups: thread t owns slots [t * kPerThread, (t + 1) * kPerThread)
+    uint32_t mine = 0;
 #pragma unroll
-      for (int j = 0; j < kTopkPerThread - 1; j++) {
-        const uint32_t s = r0 + threadIdx.x * (kTopkPerThread - 1) + j;
-        v[j] = 0;
-        if (s < kQ3PartCap && hhit[s]) { v[j] = topk_compose((int64_t)hrev[s], hdate[s], hkey[s]); ngroups++; }
+    for (uint32_t j = 0; j < kPerThread; j++) mine += hhit[threadIdx.x * kPerThread + j] != 0;
+    uint32_t pos = block_reserve<kTopkThreads>(mine, dense_count, sh);
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; j++) {
+      const uint32_t s = threadIdx.x * kPerThread + j;
+      if (hhit[s]) {
+        *reinterpret_cast<ulonglong2*>(dense + pos) =
+            make_ulonglong2((unsigned long long)(uint32_t)hkey[s] | ((unsigned long long)(uint32_t)hdate[s] << 32), hrev[s]);
+        dense_hits[pos] = hhit[s];
+        pos++;
       }
-      v[kTopkPerThread - 1] = (int)threadIdx.x < k ? carry[threadIdx.x] : (u128)0;
-      __syncthreads();
-      block_topk(v, k, carry, topk_scratch);
-      __syncthreads();
     }
+    __syncthreads();
   }
-  for (int i = threadIdx.x; i < k; i += kTopkThreads) cand[(size_t)part * k + i] = carry[i];
-  ngroups = __reduce_add_sync(FULL_MASK, ngroups);
-  if ((threadIdx.x & 31) == 0 && ngroups) atomicAdd(groups, (unsigned long long)ngroups);
 }
 
 }  // namespace
@@ -493,12 +497,17 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   if (!rc) rc = scratch(ctx, "q3r.bpart", n_or * 8 + 256, &bpart);
   if (!rc) rc = scratch(ctx, "q3r.fpart", n_li * 12 + 1024, &fpart);
   if (!rc) rc = scratch(ctx, "q3r.offs", (2 * (parts + 1) + 64) * 4, &offs);
-  const size_t cand_elems = (size_t)parts * p.k;
-  if (!rc) rc = scratch(ctx, "q3.cand", (cand_elems * 2 + 64) * sizeof(u128), &cand);
+  const uint64_t dslots = std::max<uint64_t>(128, (n_or + 127) / 128 * 128);
+  void *dense, *dhits, *tstate;
+  if (!rc) rc = scratch(ctx, "q3.cand", (size_t)kTopkCandCap * sizeof(u128), &cand);
+  if (!rc) rc = scratch(ctx, "q3r.dense", (size_t)dslots * sizeof(Q3Slot), &dense);
+  if (!rc) rc = scratch(ctx, "q3r.dhits", (size_t)dslots * 4, &dhits);
+  if (!rc) rc = scratch(ctx, "q3.topk", (size_t)kTopkStateWords * 4, &tstate);
   if (rc) return rc;
-  uint32_t* cnt = static_cast<uint32_t*>(count);   // [0] orders, [1] fact rows
+  uint32_t* cnt = static_cast<uint32_t*>(count);   // [0] orders, [1] fact rows, [2] groups, [3] top-k capacity
   GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
   GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(tstate, 0, (size_t)kTopkStateWords * 4, s));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
   int32_t* bkey = static_cast<int32_t*>(bstage);
@@ -542,29 +551,15 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   const size_t psmem = q3_partition_smem();
   GPUDB_CUDA(ctx, cudaFuncSetAttribute(q3_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
   GPUDB_LAUNCH(call, q3_partition_kernel, (unsigned)parts, kTopkThreads, psmem, (const int32_t*)bk, (const int32_t*)bd,
-               (const uint32_t*)boff, (const int32_t*)pk, (const int64_t*)pv, (const uint32_t*)poff, p.k, cbuf, groups,
-               call.status());
-  if (parts == 1) {
-    GPUDB_CUDA(ctx, cudaMemcpyAsync(rows, cbuf, (size_t)p.k * sizeof(u128), cudaMemcpyDeviceToDevice, s));
-    return GPUDB_OK;
-  }
-  return q3_topk_levels(call, cbuf, cand_elems, p.k, cbuf + cand_elems, cbuf + cand_elems + cand_elems / 2 + 32, rows);
-}
-
-int q3_topk_levels(Call& call, u128* cand, uint64_t n_cand, int k, u128* scratch_a, u128* scratch_b, u128* final_out) {
-  // reduce n_cand candidates (k per 4096-candidate tile) until one block remains
-  const u128* in = cand;
-  u128* bufs[2] = {scratch_a, scratch_b};
-  int flip = 0;
-  while (true) {
-    const uint64_t blocks = (n_cand + kTopkTile - 1) / kTopkTile;
-    u128* out = (blocks == 1) ? final_out : bufs[flip];
-    GPUDB_LAUNCH(call, topk_merge_kernel, (unsigned)std::max<uint64_t>(blocks, 1), kTopkThreads, 0, in, n_cand, k, out);
-    if (blocks <= 1) return GPUDB_OK;
-    in = out;
-    n_cand = blocks * (uint64_t)k;
-    flip ^= 1;
-  }
+               (const uint32_t*)boff, (const int32_t*)pk, (const int64_t*)pv, (const uint32_t*)poff, (Q3Slot*)dense,
+               (uint32_t*)dhits, cnt + 2, call.status());
+  GPUDB_LAUNCH(call, q3_seal_kernel, 1, 256, 0, (const uint32_t*)(cnt + 2), (uint32_t*)dhits, cnt + 3);
+  uint32_t* ts = static_cast<uint32_t*>(tstate);
+  GPUDB_LAUNCH(call, q3_hist_kernel, q3_topk_grid((uint32_t)dslots, ctx->sm_count, 1, 4), kTopkThreads, 0,
+               (const Q3Slot*)dense, (const uint32_t*)dhits, (const uint32_t*)(cnt + 3), ts, groups);
+  GPUDB_LAUNCH(call, q3_select_kernel, q3_topk_grid((uint32_t)dslots, ctx->sm_count, 1, 2), kTopkThreads, 0,
+               (const Q3Slot*)dense, (const uint32_t*)dhits, (const uint32_t*)(cnt + 3), p.k, ts, cbuf, rows);
+  return GPUDB_OK;
 }
 
 // Direct-map Q3: customer bitmap, the orders filter into dense slots + order-key bitmap +
@@ -728,7 +723,9 @@ extern "C" int gpudb_q3_join_topk(gpudb_ctx* ctx, const gpudb_customer* cu, cons
   const gpudb_orders o = *od;
   const gpudb_q3_params pp = *p;
   int mode = pp.join_mode;
-  if (mode == GPUDB_JOIN_AUTO) mode = q3_direct_fits(ctx, o) ? GPUDB_JOIN_DIRECT : GPUDB_JOIN_GLOBAL;
+  if (mode == GPUDB_JOIN_AUTO)
+    mode = ctx->q3_auto_mode >= 0 ? ctx->q3_auto_mode : q3_direct_fits(ctx, o) ? GPUDB_JOIN_DIRECT : GPUDB_JOIN_GLOBAL;
+  if (mode == GPUDB_JOIN_DIRECT && o.key_max < 0 && pp.join_mode == GPUDB_JOIN_AUTO) mode = GPUDB_JOIN_GLOBAL;
   if (mode == GPUDB_JOIN_DIRECT && o.n_rows && o.key_max < 0)
     return fail(ctx, GPUDB_E_INVALID, "q3: the direct mode needs orders.key_max");
   Call call(ctx, ex, t);

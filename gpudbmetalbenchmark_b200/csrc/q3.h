@@ -233,13 +233,11 @@ constexpr int kQ3Batch = 8;
 bool q3_batchable(const gpudb_request& q);
 int q3_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t>& ids, const gpudb_exec* ex);
 
-// Result payload of both modes: {u64 groups, u64 pad, u128 rows[k]} (rows as top-k
+// Result payload of every mode: {u64 groups, u64 pad, u128 rows[k]} (rows as top-k
 // composites, see topk_compose).
 int q3_global(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_lineitem* li,
               const gpudb_q3_params& p, uint8_t* result);
 int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_lineitem* li,
              const gpudb_q3_params& p, uint8_t* result);
-// Reduces n_cand composites to the top k (k per 4096-candidate tile per level).
-int q3_topk_levels(Call& call, u128* cand, uint64_t n_cand, int k, u128* scratch_a, u128* scratch_b, u128* final_out);
 
 }  // namespace gpudb

@@ -3,7 +3,8 @@
 // options: the Q1 kernel variant (block size, rows per thread, 128-bit loads, TMA staging,
 // shared-memory accumulators), the Q6 kernel variant (row kernel or 128-bit loads with 1, 2
 // or 4 quads per thread per step), the hash-table load factor of the Q3 build (50% or 25%),
-// the radix fan-out of the Q3 radix mode, and the Q9 aggregation slot counts (shared and
+// the radix fan-out of the Q3 radix mode, the join mode that a Q3 AUTO request runs (direct
+// map, global table or radix partitions), and the Q9 aggregation slot counts (shared and
 // global). Every candidate must give the same result as the default configuration; a
 // candidate that does not is dropped (and reported) rather than chosen.
 //
@@ -59,6 +60,7 @@ int run_once(gpudb_ctx* ctx, const gpudb_request& q, double* ms, std::string* di
     case GPUDB_PIPE_Q3: {
       gpudb_q3_result o{};
       rc = gpudb_q3_join_topk(ctx, &q.q3->cu, &q.q3->od, &q.q3->li, &q.q3p, &o, &t, nullptr);
+      o.join_mode = 0;   // the mode that ran differs between candidates; the answer must not
       digest->assign(reinterpret_cast<const char*>(&o), sizeof o);
       break;
     }
@@ -139,7 +141,14 @@ extern "C" int gpudb_autotune(gpudb_ctx* ctx, const gpudb_request* req, uint32_t
       for (int v = 1; v <= 4; v++) cands.push_back({GPUDB_OPT_Q6_VARIANT, v, 0, 0});
       break;
     case GPUDB_PIPE_Q3:
-      if (q.q3p.join_mode == GPUDB_JOIN_RADIX) {
+      if (q.q3p.join_mode == GPUDB_JOIN_AUTO) {
+        // the join mode itself: direct map (when the orders carry a key bound), global
+        // table, radix partitions
+        def = {GPUDB_OPT_Q3_AUTO_MODE, -1, 0, 0};
+        if (q.q3->od.key_max >= 0) cands.push_back({GPUDB_OPT_Q3_AUTO_MODE, GPUDB_JOIN_DIRECT, 0, 0});
+        cands.push_back({GPUDB_OPT_Q3_AUTO_MODE, GPUDB_JOIN_GLOBAL, 0, 0});
+        cands.push_back({GPUDB_OPT_Q3_AUTO_MODE, GPUDB_JOIN_RADIX, 0, 0});
+      } else if (q.q3p.join_mode == GPUDB_JOIN_RADIX) {
         // fan-outs around the default (about 16K orders rows per partition): fewer partitions
         // re-probe the fact rows once per shared-table chunk, more than 1024 take a second
         // partitioning pass

@@ -108,7 +108,10 @@ enum {
   GPUDB_OPT_Q9_GLOBAL_SLOTS = 7, /* Q9 global aggregation slots when a call's global_slots is 0 (4096) */
   GPUDB_OPT_GRAPHS = 8           /* 1 (default): a Q9 call over device-resident tables on the context's
                                     stream is captured into a CUDA graph once per (tables, parameters)
-                                    and replayed after; 0: its kernels are launched one by one */
+                                    and replayed after; 0: its kernels are launched one by one */,
+  GPUDB_OPT_Q3_AUTO_MODE = 9     /* what a Q3 call with join_mode GPUDB_JOIN_AUTO runs: -1 (default) the
+                                    30% rule (direct map when it fits, else the global table), or
+                                    GPUDB_JOIN_GLOBAL / _RADIX / _DIRECT (the autotuner's choice) */
 };
 int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value);
 int gpudb_get_option(const gpudb_ctx* ctx, int32_t option, int64_t* value);
@@ -551,7 +554,8 @@ int gpudb_selftest_bounded_wait(gpudb_ctx* ctx, uint32_t polls, int32_t arrive);
  *   Q1: GPUDB_OPT_SCAN_VARIANT 1..7 (block size, rows per thread, 128-bit loads, TMA
  *       staging, shared-memory accumulators); Q6: GPUDB_OPT_Q6_VARIANT 1..4 (row kernel or
  *       128-bit loads with 1/2/4 quads per thread per step); Q3 global mode:
- *       GPUDB_OPT_HT_LOAD 50/25; Q3 radix mode: GPUDB_OPT_RADIX_BITS; Q9:
+ *       GPUDB_OPT_HT_LOAD 50/25; Q3 radix mode: GPUDB_OPT_RADIX_BITS; Q3 AUTO mode:
+ *       GPUDB_OPT_Q3_AUTO_MODE (direct map, global table or radix partitions); Q9:
  *       GPUDB_OPT_Q9_SMEM_SLOTS x GPUDB_OPT_Q9_GLOBAL_SLOTS.
  * A candidate whose result differs from the default setting's is dropped. The choices of a
  * context are written by gpudb_tune_save as lines "device|pipeline|rows_log2|option|value"

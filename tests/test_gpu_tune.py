@@ -51,7 +51,8 @@ def test_tune_joins_then_results_match_oracle(orc):
         tc, to, tl = e.upload("customer", cu), e.upload("orders", od), e.upload("lineitem", l3)
         tables = capi.Q3Tables(tc.struct(), to.struct(), tl.lineitem())
         want = orc.q3(cu, od, l3, 1, 1170, 1170, 10)
-        for mode, opt in ((capi.JOIN_GLOBAL, "ht_load_pct"), (capi.JOIN_RADIX, "radix_bits")):
+        for mode, opt in ((capi.JOIN_GLOBAL, "ht_load_pct"), (capi.JOIN_RADIX, "radix_bits"),
+                          (capi.JOIN_AUTO, "q3_auto_mode")):
             r = capi.Request(pipeline=capi.PIPE_Q3)
             r.q3 = C.pointer(tables)
             r.q3p = capi.Q3Params(1, 1170, 1170, 10, mode, 0)
@@ -61,6 +62,12 @@ def test_tune_joins_then_results_match_oracle(orc):
             e._check(e.lib.gpudb_q3_join_topk(e.ctx, C.byref(tables.cu), C.byref(tables.od), C.byref(tables.li),
                                               C.byref(r.q3p), C.byref(out), None, None))
             assert q3_to_list(out) == want
+            if mode == capi.JOIN_AUTO:   # the tuned mode is what AUTO now runs
+                assert res["q3_auto_mode"] in (-1, capi.JOIN_GLOBAL, capi.JOIN_RADIX, capi.JOIN_DIRECT)
+                assert res["candidates"] == 4
+                ran = capi.JOIN_DIRECT if res["q3_auto_mode"] == -1 else res["q3_auto_mode"]
+                assert out.join_mode == ran
+        e.set_option(capi.OPT_Q3_AUTO_MODE, -1)
         # every load factor gives the same answer
         for load in (50, 25):
             e.set_option(capi.OPT_HT_LOAD, load)
