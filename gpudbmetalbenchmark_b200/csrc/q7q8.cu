@@ -185,32 +185,59 @@ struct Q8Args {
 };
 
 // Lineitems of parts of the type (part bitmap) and orders of okbm: bins[year] += revenue,
-// bins[kYears + year] too when the supplier is of the nation. Order and supplier keys are
-// loaded only for rows whose part passes (a type is about 1 part in 150).
-__global__ void __launch_bounds__(kThreads) q8_probe_kernel(const int32_t* __restrict__ lkey,
-                                                            const int32_t* __restrict__ lpart,
-                                                            const int32_t* __restrict__ lsupp,
-                                                            const int64_t* __restrict__ lext,
-                                                            const int32_t* __restrict__ ldisc, uint64_t n, Q8Args a,
-                                                            const uint32_t* __restrict__ pbits,
-                                                            const uint32_t* __restrict__ okbm,
-                                                            const uint8_t* __restrict__ omap,
-                                                            const uint8_t* __restrict__ smap, long long* out) {
+// bins[kYears + year] too when the supplier is of the nation. Every row's part is tested
+// against a filter in shared memory (smem_filter_*: the exact part bitmap when it fits,
+// else a hashed one whose hits are confirmed in `pbits`): a type is about 1 part in 150, so
+// nearly every row is turned away without a global-memory access. Part keys stream with
+// 128-bit loads, 16 rows per thread per step; order and supplier keys, the maps and ext/disc
+// are loaded only for the rows that pass.
+constexpr int kQ8Threads = 1024;
+constexpr int kQ8Quads = 4;
+constexpr int kQ8Rows = 4 * kQ8Quads;
+
+__global__ void __launch_bounds__(kQ8Threads) q8_probe_kernel(const int32_t* __restrict__ lkey,
+                                                              const int32_t* __restrict__ lpart,
+                                                              const int32_t* __restrict__ lsupp,
+                                                              const int64_t* __restrict__ lext,
+                                                              const int32_t* __restrict__ ldisc, uint64_t n, Q8Args a,
+                                                              const uint32_t* __restrict__ pbits,
+                                                              const uint32_t* __restrict__ filt, uint32_t filt_words,
+                                                              bool exact, const uint32_t* __restrict__ okbm,
+                                                              const uint8_t* __restrict__ omap,
+                                                              const uint8_t* __restrict__ smap, long long* out) {
+  extern __shared__ uint32_t q8_filt[];
   __shared__ long long bins[2 * kYears];
   if (threadIdx.x < 2 * kYears) bins[threadIdx.x] = 0;
-  __syncthreads();
-  const uint64_t step = (uint64_t)gridDim.x * kThreads * kRows;
-  for (uint64_t b = (uint64_t)blockIdx.x * kThreads * kRows; b < n; b += step) {
-    int32_t p[kRows];
+  smem_filter_load(filt, filt_words, q8_filt);   // ends with a block barrier
+  const bool vec = (reinterpret_cast<uintptr_t>(lpart) & 15u) == 0;
+  constexpr uint64_t kStepRows = (uint64_t)kQ8Threads * kQ8Rows;
+  const uint64_t step = (uint64_t)gridDim.x * kStepRows;
+  auto row_of = [&](uint64_t b, int q, int k) { return b + 4 * ((uint64_t)q * kQ8Threads + threadIdx.x) + k; };
+  for (uint64_t b = (uint64_t)blockIdx.x * kStepRows; b < n; b += step) {
+    int32_t p[kQ8Rows];
+    if (vec && b + kStepRows <= n) {
 #pragma unroll
-    for (int j = 0; j < kRows; j++) {
-      const uint64_t i = b + (uint64_t)j * kThreads + threadIdx.x;
-      p[j] = i < n ? ld_stream(lpart + i) : -1;
+      for (int q = 0; q < kQ8Quads; q++) {
+        const int4 v = ld_stream(reinterpret_cast<const int4*>(lpart + row_of(b, q, 0)));
+        p[4 * q] = v.x; p[4 * q + 1] = v.y; p[4 * q + 2] = v.z; p[4 * q + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < kQ8Quads; q++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint64_t r = row_of(b, q, k);
+          p[4 * q + k] = r < n ? ld_stream(lpart + r) : -1;
+        }
     }
+    uint32_t ok = 0;
 #pragma unroll
-    for (int j = 0; j < kRows; j++) {
-      if (p[j] < 0 || p[j] > a.part_max || !bitmap_test(pbits, p[j])) continue;
-      const uint64_t i = b + (uint64_t)j * kThreads + threadIdx.x;
+    for (int j = 0; j < kQ8Rows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= a.part_max) << j;
+    uint32_t take = smem_filter_mask(q8_filt, exact, pbits, p, ok);
+    while (take) {
+      const int j = __ffs(take) - 1;
+      take &= take - 1;
+      const uint64_t i = row_of(b, j >> 2, j & 3);
       const int32_t k = ld_stream(lkey + i), s = ld_stream(lsupp + i);
       if (k < 0 || k > a.order_max || s < 0 || s > a.supp_max || !bitmap_test(okbm, k)) continue;
       const int y = __ldg(omap + k);
@@ -358,11 +385,30 @@ extern "C" int gpudb_q8_market_share(gpudb_ctx* ctx, const gpudb_customer* cu, c
                  (const uint8_t*)cmap, Y, (uint32_t*)okbm, (uint8_t*)omap, call.status());
   if (od->n_rows && cu->n_rows && su->n_rows && pa->n_rows) {
     const Q8Args a{part_max, order_max, supp_max};
+    // the probe's part filter: the exact bitmap itself, or a hashed one built from it
+    const bool exact = smem_filter_exact(part_max);
+    const uint32_t fwords = smem_filter_words(part_max);
+    void* hfilt = nullptr;
+    if (!exact) {
+      if ((rc = scratch(ctx, "q8.partfilter", (size_t)kSmemFilterWords * 4, &hfilt))) return rc;
+      GPUDB_CUDA(ctx, cudaMemsetAsync(hfilt, 0, (size_t)kSmemFilterWords * 4, s));
+      GPUDB_LAUNCH(call, hashed_filter_kernel, grid_for(ctx, pwords, 1, 8), kThreads, 0, (const uint32_t*)pbits, pwords,
+                   (uint32_t*)hfilt);
+    }
+    const size_t fsmem = (size_t)fwords * 4;
+    GPUDB_CUDA(ctx, cudaFuncSetAttribute(q8_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
+    int per_sm = 0;
+    GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, q8_probe_kernel, kQ8Threads, fsmem));
     rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
-      if (c.n_rows)
-        GPUDB_LAUNCH(call, q8_probe_kernel, grid_for(ctx, c.n_rows, kRows, 8), kThreads, 0, c.order_key, c.part_key,
-                     c.supp_key, c.ext_price, c.discount, c.n_rows, a, (const uint32_t*)pbits, (const uint32_t*)okbm,
-                     (const uint8_t*)omap, (const uint8_t*)smap, call.result<long long>());
+      if (c.n_rows) {
+        const uint64_t per_block = (uint64_t)kQ8Threads * kQ8Rows;
+        const unsigned g = (unsigned)std::max<uint64_t>(
+            1, std::min<uint64_t>((c.n_rows + per_block - 1) / per_block, (uint64_t)ctx->sm_count * std::max(1, per_sm)));
+        GPUDB_LAUNCH(call, q8_probe_kernel, g, kQ8Threads, fsmem, c.order_key, c.part_key, c.supp_key, c.ext_price,
+                     c.discount, c.n_rows, a, (const uint32_t*)pbits, (const uint32_t*)(exact ? pbits : hfilt), fwords,
+                     exact, (const uint32_t*)okbm, (const uint8_t*)omap, (const uint8_t*)smap,
+                     call.result<long long>());
+      }
       return (int)GPUDB_OK;
     });
     if (rc) return rc;
