@@ -44,49 +44,53 @@ __device__ __forceinline__ bool word_at(const uint8_t* row, int pos, const uint8
   return true;
 }
 
-// Byte flags (bits 7, 15, 23, 31) -> 4 consecutive bits: (m >> 7) * (1 + 2^7 + 2^14 + 2^21)
-// puts the flags of bytes 0..3 on bits 21..24 without carries.
-__device__ __forceinline__ uint32_t flags_to_nibble(uint32_t m) { return (((m >> 7) * 0x00204081u) >> 21) & 0xFu; }
-
 // LIKE '%w0%w1%' on one NUL-padded row: its kSlotWords words in registers, its bytes at
 // `row` (global memory, read again only to verify candidates). One branch-free pass marks,
 // for both words, the positions whose first two bytes match (SWAR on the row word and the row
 // word shifted by one byte); only those candidates, rare for two-letter prefixes, are
 // compared in full: the first verified w0, then any verified w1 at or after its end.
+// Candidate flags (bits 7, 15, 23, 31 of a word's test) are packed eight words to a register
+// with two operations: word k's flags land on bits (k & 7) + {0, 8, 16, 24} of c[k >> 3], so
+// bit b of c[q] is position 4 * (8q + (b & 7)) + (b >> 3). Bits are visited in bit order,
+// not position order: the first w0 is the smallest verified position.
 __device__ bool like2(const uint32_t (&rw)[kSlotWords], const uint8_t* row, const uint8_t (&w)[2][16],
                       const int32_t (&len)[2]) {
   const uint32_t a0 = w[0][0] * 0x01010101u, b0 = w[0][1] * 0x01010101u;
   const uint32_t a1 = w[1][0] * 0x01010101u, b1 = w[1][1] * 0x01010101u;
   const bool two0 = len[0] > 1, two1 = len[1] > 1;
-  uint32_t c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};   // candidate bit per position 0..79
+  uint32_t c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};
 #pragma unroll
   for (int k = 0; k < kSlotWords; k++) {
     const uint32_t x = rw[k], nx = k + 1 < kSlotWords ? rw[k + 1] : 0u;
     const uint32_t y = __funnelshift_r(x, nx, 8);   // the byte after each byte of x
     const uint32_t m0 = zero_bytes(x ^ a0) & (two0 ? zero_bytes(y ^ b0) : 0x80808080u);
     const uint32_t m1 = zero_bytes(x ^ a1) & (two1 ? zero_bytes(y ^ b1) : 0x80808080u);
-    c0[(4 * k) >> 5] |= flags_to_nibble(m0) << ((4 * k) & 31);
-    c1[(4 * k) >> 5] |= flags_to_nibble(m1) << ((4 * k) & 31);
+    const int j = k & 7;
+    c0[k >> 3] |= (m0 >> (7 - j)) & (0x01010101u << j);
+    c1[k >> 3] |= (m1 >> (7 - j)) & (0x01010101u << j);
   }
-  int start = -1;
+  constexpr int kNone = 1 << 30;
+  int first = kNone;
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    uint32_t m = start < 0 ? c0[q] : 0u;
+    uint32_t m = c0[q];
     while (m) {
-      const int pos = 32 * q + __ffs(m) - 1;
+      const int b = __ffs(m) - 1;
       m &= m - 1;
-      if (word_at(row, pos, w[0], len[0])) { start = pos + len[0]; break; }
+      const int pos = 4 * (8 * q + (b & 7)) + (b >> 3);
+      if (pos < first && word_at(row, pos, w[0], len[0])) first = pos;
     }
   }
-  if (start < 0) return false;
+  if (first == kNone) return false;
+  const int start = first + len[0];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    const int lo = start - 32 * q;   // positions >= start within this word
-    uint32_t m = lo <= 0 ? c1[q] : (lo >= 32 ? 0u : c1[q] & (0xFFFFFFFFu << lo));
+    uint32_t m = c1[q];
     while (m) {
-      const int pos = 32 * q + __ffs(m) - 1;
+      const int b = __ffs(m) - 1;
       m &= m - 1;
-      if (word_at(row, pos, w[1], len[1])) return true;
+      const int pos = 4 * (8 * q + (b & 7)) + (b >> 3);
+      if (pos >= start && word_at(row, pos, w[1], len[1])) return true;
     }
   }
   return false;
