@@ -6,7 +6,7 @@
 //
 // B200 design. Partition p = key_hash32(key) & (2^bits - 1) (the reference's hash), in LSD
 // passes of at most kRxPassBits bits (one pass up to 1024 partitions). The input is cut into
-// G super-tiles, about one per SM; per pass:
+// G super-tiles, about one per SM, sized on the device from the row count; per pass:
 //   rx_hist_kernel    counts each super-tile's rows per digit (shared-memory atomics; four
 //                     blocks per super-tile, so every SM streams) into hist[digit][G], and
 //                     in the first pass also the rows per final partition;
@@ -59,6 +59,15 @@ struct ColumnSource {
   __device__ __forceinline__ P payload(uint64_t r) const { return pay ? __ldcs(pay + r) : (P)r; }
 };
 
+// Rows per super-tile for n rows over G super-tiles: whole sub-tiles, at least one. Both
+// kernels of a pass derive it from the same device row count, so a count that an earlier
+// kernel left on the device (a filtered input) still spreads over all G blocks.
+__host__ __device__ __forceinline__ uint64_t rx_super_rows_for(uint64_t n, uint32_t G) {
+  const uint64_t per = (n + G - 1) / (G ? G : 1);
+  const uint64_t s = (per + kRxTile - 1) / kRxTile * kRxTile;
+  return s < (uint64_t)kRxTile ? (uint64_t)kRxTile : s;
+}
+
 __device__ __forceinline__ uint32_t rx_digit(int32_t key, int shift, uint32_t mask) {
   return (key_hash32(key) >> shift) & mask;
 }
@@ -93,9 +102,8 @@ __device__ __forceinline__ uint32_t rx_block_scan(uint32_t v, uint32_t* warp_tot
 // hist[digit * G + super-tile] (zeroed), and with `full` the rows per final partition
 // (fbits bits; zeroed).
 template <class Src>
-__global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint64_t super_rows, uint32_t G, int shift,
-                                                             int dbits, int fbits, uint32_t* __restrict__ hist,
-                                                             uint32_t* __restrict__ full) {
+__global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G, int shift, int dbits, int fbits,
+                                                             uint32_t* __restrict__ hist, uint32_t* __restrict__ full) {
   __shared__ uint32_t cnt[kRxMaxF];
   __shared__ uint32_t fcnt[1u << kRxFullSmemBits];
   const uint32_t F = 1u << dbits, dmask = F - 1, fmask = (1u << fbits) - 1;
@@ -106,6 +114,7 @@ __global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint64_t s
   __syncthreads();
   const uint32_t g = blockIdx.x / kRxHistSplit, part = blockIdx.x % kRxHistSplit;
   const uint64_t n = src.rows();
+  const uint64_t super_rows = rx_super_rows_for(n, G);
   const uint64_t quarter = super_rows / kRxHistSplit;
   const uint64_t r0 = (uint64_t)g * super_rows + part * quarter;
   const uint64_t r1 = min(r0 + quarter, n);
@@ -143,8 +152,8 @@ __host__ __device__ constexpr size_t rx_scatter_smem(uint32_t F) {
 
 // One block per super-tile (see the file comment). offs: exclusive scan of hist.
 template <class Src, class P, bool PAY>
-__global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint64_t super_rows, uint32_t G, int shift,
-                                                                   int dbits, const uint32_t* __restrict__ offs,
+__global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint32_t G, int shift, int dbits,
+                                                                   const uint32_t* __restrict__ offs,
                                                                    int32_t* __restrict__ kout, P* __restrict__ pout) {
   extern __shared__ __align__(16) unsigned char rx_smem[];
   const uint32_t F = 1u << dbits, dmask = F - 1;
@@ -156,6 +165,7 @@ __global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint
   __shared__ uint32_t s_total;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t n = src.rows();
+  const uint64_t super_rows = rx_super_rows_for(n, G);
   const uint64_t g0 = (uint64_t)blockIdx.x * super_rows;
   if (g0 >= n) return;   // uniform across the block
   const uint64_t g1 = min(g0 + super_rows, n);
@@ -249,15 +259,16 @@ static __global__ void rx_starts_kernel(const uint32_t* __restrict__ offs, uint3
     offsets[b] = b < F ? offs[(size_t)b * G] : *total;
 }
 
-// Super-tile size: about one super-tile per SM, whole sub-tiles.
-inline uint64_t rx_super_rows(uint64_t n_max, int sms) {
-  const uint64_t per = (n_max + sms - 1) / std::max(sms, 1);
-  return std::max<uint64_t>(kRxTile, (per + kRxTile - 1) / kRxTile * kRxTile);
+// Super-tiles: about one per SM, fewer for an input of fewer sub-tiles (the kernels size
+// them from the device row count, at most n_max rows).
+inline uint32_t rx_super_tiles(uint64_t n_max, int sms) {
+  const uint64_t sub = (std::max<uint64_t>(n_max, 1) + kRxTile - 1) / kRxTile;
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sub, (uint64_t)std::max(sms, 1)));
 }
 
 // Scratch words for one partitioning of at most n_max rows with `bits` bits.
 inline size_t rx_scratch_words(uint64_t n_max, int bits, int sms) {
-  const uint64_t G = (std::max<uint64_t>(n_max, 1) + rx_super_rows(n_max, sms) - 1) / rx_super_rows(n_max, sms);
+  const uint64_t G = rx_super_tiles(n_max, sms);
   const size_t hn = (size_t)kRxMaxF * G + 1;
   const size_t parts = (size_t)1 << bits;
   return 2 * hn + std::max(scan_tiles_count(hn), scan_tiles_count(parts)) + 8 + parts + 8;
@@ -273,8 +284,7 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
   cudaStream_t s = call.stream();
   const int passes = bits <= kRxPassBits ? 1 : 2;
   const int d0 = passes == 1 ? bits : (bits + 1) / 2;
-  const uint64_t S = rx_super_rows(n_max, ctx->sm_count);
-  const uint32_t G = (uint32_t)((std::max<uint64_t>(n_max, 1) + S - 1) / S);
+  const uint32_t G = rx_super_tiles(n_max, ctx->sm_count);
   const size_t hn = (size_t)kRxMaxF * G + 1;
   const size_t parts = (size_t)1 << bits;
   void* sc = nullptr;
@@ -296,25 +306,25 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
     if (pass == 0 && passes > 1) GPUDB_CUDA(ctx, cudaMemsetAsync(full, 0, parts * sizeof(uint32_t), s));
     uint32_t* fullp = (pass == 0 && passes > 1) ? full : nullptr;
     if (pass == 0) {
-      GPUDB_LAUNCH(call, (rx_hist_kernel<Src>), G * kRxHistSplit, kRxThreads, 0, src, S, G, shift, dbits, bits, hist,
+      GPUDB_LAUNCH(call, (rx_hist_kernel<Src>), G * kRxHistSplit, kRxThreads, 0, src, G, shift, dbits, bits, hist,
                    fullp);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
       GPUDB_CUDA(ctx, cudaFuncSetAttribute(rx_scatter_kernel<Src, P, PAY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
-      GPUDB_LAUNCH(call, (rx_scatter_kernel<Src, P, PAY>), G, kRxThreads, smem, src, S, G, shift, dbits,
+      GPUDB_LAUNCH(call, (rx_scatter_kernel<Src, P, PAY>), G, kRxThreads, smem, src, G, shift, dbits,
                    (const uint32_t*)offs, ko, po);
     } else {
       // rows of the first pass, in their pass-one order; their count is the first scan's total
       const uint32_t* total0 = full + parts;   // copied below
       const ColumnSource<P> s2{ktmp, PAY ? ptmp : nullptr, n_max, total0};
-      GPUDB_LAUNCH(call, (rx_hist_kernel<ColumnSource<P>>), G * kRxHistSplit, kRxThreads, 0, s2, S, G, shift, dbits,
+      GPUDB_LAUNCH(call, (rx_hist_kernel<ColumnSource<P>>), G * kRxHistSplit, kRxThreads, 0, s2, G, shift, dbits,
                    bits, hist, (uint32_t*)nullptr);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
       GPUDB_CUDA(ctx, cudaFuncSetAttribute(rx_scatter_kernel<ColumnSource<P>, P, PAY>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      GPUDB_LAUNCH(call, (rx_scatter_kernel<ColumnSource<P>, P, PAY>), G, kRxThreads, smem, s2, S, G, shift, dbits,
+      GPUDB_LAUNCH(call, (rx_scatter_kernel<ColumnSource<P>, P, PAY>), G, kRxThreads, smem, s2, G, shift, dbits,
                    (const uint32_t*)offs, ko, po);
     }
     if (pass == 0 && passes > 1)
