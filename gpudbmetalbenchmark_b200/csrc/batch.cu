@@ -330,9 +330,8 @@ int launch_pass(gpudb_ctx* ctx, Call& call, const ScanGroup* dgrp, const std::ve
   if (tiles.empty()) return GPUDB_OK;
   auto kern = scan_pass_kernel<NB, Q6>;
   const size_t smem = pass_smem<NB, Q6>();
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kern, smem));
+  const int per_sm = kernel_occupancy(ctx, (const void*)kern, kBT, smem);
   const unsigned grid = std::max<unsigned>(1, std::min<unsigned>((unsigned)tiles.size(), (unsigned)(ctx->sm_count * per_sm)));
   GPUDB_CUDA(ctx, cudaMemcpyAsync(dtile, tiles.data(), tiles.size() * sizeof(ScanTile), cudaMemcpyHostToDevice, call.stream()));
   GPUDB_LAUNCH(call, kern, grid, kBT, smem, dgrp, (const ScanTile*)dtile, (uint32_t)tiles.size(), queue, res, status);

@@ -1,6 +1,9 @@
 // Context lifecycle, memory, result slots, async completion and chunked streaming.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 #include "engine.h"
@@ -88,6 +91,34 @@ void graph_store(gpudb_ctx* ctx, const std::string& key, cudaGraphExec_t exec, u
 void release_retired(gpudb_ctx* ctx) {
   for (void* p : ctx->retired) cudaFreeAsync(p, ctx->stream);
   ctx->retired.clear();
+}
+
+namespace {
+std::mutex g_attr_mu;
+std::map<std::pair<int, const void*>, size_t> g_smem_set;
+std::map<std::tuple<int, const void*, int, size_t>, int> g_occupancy;
+}  // namespace
+
+cudaError_t kernel_smem(gpudb_ctx* ctx, const void* fn, size_t smem) {
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  size_t& have = g_smem_set[{ctx->device, fn}];
+  if (smem <= have) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) have = smem;
+  return e;
+}
+
+int kernel_occupancy(gpudb_ctx* ctx, const void* fn, int threads, size_t smem) {
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  auto it = g_occupancy.find({ctx->device, fn, threads, smem});
+  if (it != g_occupancy.end()) return it->second;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1) {
+    (void)cudaGetLastError();
+    per_sm = 1;
+  }
+  g_occupancy[{ctx->device, fn, threads, smem}] = per_sm;
+  return per_sm;
 }
 
 cudaEvent_t event_get(gpudb_ctx* ctx) {

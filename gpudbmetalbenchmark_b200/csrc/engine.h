@@ -118,6 +118,13 @@ constexpr size_t kMaxGraphs = 16;
 gpudb_ctx::Graph* graph_find(gpudb_ctx* ctx, const std::string& key);
 void graph_store(gpudb_ctx* ctx, const std::string& key, cudaGraphExec_t exec, uint32_t kernels);
 
+// Kernel attributes cached per device (the runtime calls cost host time on every pipeline
+// call otherwise): kernel_smem raises a kernel's dynamic shared-memory limit when `smem` is
+// above what was set before; kernel_occupancy is the blocks per SM (at least 1) of a launch
+// shape.
+cudaError_t kernel_smem(gpudb_ctx* ctx, const void* fn, size_t smem);
+int kernel_occupancy(gpudb_ctx* ctx, const void* fn, int threads, size_t smem);
+
 cudaEvent_t event_get(gpudb_ctx* ctx);
 void event_put(gpudb_ctx* ctx, cudaEvent_t e);
 

@@ -131,9 +131,8 @@ int launch_orders_filter_as(Call& call, const gpudb_customer& cu, const gpudb_or
   gpudb_ctx* ctx = call.ctx();
   auto kern = orders_filter_kernel<T, SMEM, DIRECT>;
   const size_t smem = SMEM ? (size_t)fwords * 4 : 0;
-  if (SMEM) GPUDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem));
+  if (SMEM) GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kern, smem));
+  const int per_sm = kernel_occupancy(ctx, (const void*)kern, T, smem);
   const uint64_t per_block = (uint64_t)T * kFilterRows;
   const unsigned g = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>((od.n_rows + per_block - 1) / per_block, (uint64_t)ctx->sm_count * std::max(1, per_sm)));
@@ -549,7 +548,7 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);
   u128* rows = reinterpret_cast<u128*>(result + 16);
   const size_t psmem = q3_partition_smem();
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q3_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q3_partition_kernel, psmem));
   GPUDB_LAUNCH(call, q3_partition_kernel, (unsigned)parts, kTopkThreads, psmem, (const int32_t*)bk, (const int32_t*)bd,
                (const uint32_t*)boff, (const int32_t*)pk, (const int64_t*)pv, (const uint32_t*)poff, (Q3Slot*)dense,
                (uint32_t*)dhits, cnt + 2, call.status());

@@ -396,9 +396,8 @@ extern "C" int gpudb_q8_market_share(gpudb_ctx* ctx, const gpudb_customer* cu, c
                    (uint32_t*)hfilt);
     }
     const size_t fsmem = (size_t)fwords * 4;
-    GPUDB_CUDA(ctx, cudaFuncSetAttribute(q8_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
-    int per_sm = 0;
-    GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, q8_probe_kernel, kQ8Threads, fsmem));
+    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q8_probe_kernel, fsmem));
+    const int per_sm = kernel_occupancy(ctx, (const void*)q8_probe_kernel, kQ8Threads, fsmem);
     rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
       if (c.n_rows) {
         const uint64_t per_block = (uint64_t)kQ8Threads * kQ8Rows;

@@ -439,14 +439,12 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   unsigned long long* gvals = static_cast<unsigned long long*>(groups);
   const size_t probe_smem = (size_t)scap * 12, sort_smem = (size_t)gcap * 12;
   // dynamic + static shared memory may pass the 48 KB default: always opt in (before any capture)
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)probe_smem));
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q9_resolve_kernel, probe_smem));
   const size_t filt_smem = (size_t)filt_words * 4;
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(li_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)filt_smem));
-  int filter_per_sm = 0;
-  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&filter_per_sm, li_filter_kernel, kLiThreads, filt_smem));
-  int resolve_per_sm = 0;
-  GPUDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resolve_per_sm, q9_resolve_kernel, kQ9Threads, probe_smem));
-  GPUDB_CUDA(ctx, cudaFuncSetAttribute(q9_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)li_filter_kernel, filt_smem));
+  const int filter_per_sm = kernel_occupancy(ctx, (const void*)li_filter_kernel, kLiThreads, filt_smem);
+  const int resolve_per_sm = kernel_occupancy(ctx, (const void*)q9_resolve_kernel, kQ9Threads, probe_smem);
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q9_sort_kernel, sort_smem));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
   // Every device operation of the pipeline, in stream order (status and result through

@@ -310,8 +310,7 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
                    fullp);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
-      GPUDB_CUDA(ctx, cudaFuncSetAttribute(rx_scatter_kernel<Src, P, PAY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
+      GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)rx_scatter_kernel<Src, P, PAY>, smem));
       GPUDB_LAUNCH(call, (rx_scatter_kernel<Src, P, PAY>), G, kRxThreads, smem, src, G, shift, dbits,
                    (const uint32_t*)offs, ko, po);
     } else {
@@ -322,8 +321,7 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
                    bits, hist, (uint32_t*)nullptr);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
-      GPUDB_CUDA(ctx, cudaFuncSetAttribute(rx_scatter_kernel<ColumnSource<P>, P, PAY>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)rx_scatter_kernel<ColumnSource<P>, P, PAY>, smem));
       GPUDB_LAUNCH(call, (rx_scatter_kernel<ColumnSource<P>, P, PAY>), G, kRxThreads, smem, s2, G, shift, dbits,
                    (const uint32_t*)offs, ko, po);
     }

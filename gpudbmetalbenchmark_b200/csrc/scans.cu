@@ -635,8 +635,7 @@ __global__ void __launch_bounds__(kQ1SmemThreads) q1_vec_smem_kernel(const int4*
 bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
 
 int grid_for(gpudb_ctx* ctx, const void* kernel, uint64_t work_items, int min_blocks) {
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  const int per_sm = kernel_occupancy(ctx, kernel, kThreads, 0);
   uint64_t want = (work_items + kThreads - 1) / kThreads;
   uint64_t cap = (uint64_t)ctx->sm_count * per_sm;
   uint64_t g = std::min<uint64_t>(want, cap);
@@ -706,11 +705,8 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
   if (variant == 7 && !vec) variant = 3;
   if (variant == 7) {
     const size_t smem = kQ1AccBytes;
-    GPUDB_CUDA(ctx, cudaFuncSetAttribute(q1_vec_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, q1_vec_smem_kernel, kQ1SmemThreads, smem) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
+    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q1_vec_smem_kernel, smem));
+    const int per_sm = kernel_occupancy(ctx, (const void*)q1_vec_smem_kernel, kQ1SmemThreads, smem);
     const uint64_t min_blocks = (c.n_rows + (uint64_t)kQ1SmemThreads * kQ1RowsPerThread - 1) /
                                 ((uint64_t)kQ1SmemThreads * kQ1RowsPerThread);
     const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
@@ -738,7 +734,7 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ctx->sm_count, tiles));
     // 212,992 bytes of tiles; the shared-accumulator ring: 6 x 26,624 tiles + 49,152 accumulators
     const size_t smem = variant == 6 ? (size_t)6 * 26 * 1024 + 4 * 6 * 256 * 8 : (size_t)26 * 2048 * 4;
-    GPUDB_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kernel, smem));
     void* part = nullptr;
     unsigned* ticket = nullptr;
     int rc = scan_scratch(ctx, "q1.partials", (size_t)grid * 6 * kQ1Raw * sizeof(u128), &part, &ticket);
