@@ -393,7 +393,7 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
     words += q.pipeline == GPUDB_PIPE_Q6 ? kQ6Words : kQ1Words;
   }
   std::vector<ScanGroup> groups;
-  std::vector<ScanTile> tiles6, tiles1;   // Q6 passes, Q1 passes
+  std::vector<ScanTile> tiles6, tiles1, tiles11;   // Q6 passes, Q1 passes of two / of one Q1 request
   for (auto& kv : by_table) {
     Members& mb = kv.second;
     for (auto& c : mb.q1)
@@ -439,7 +439,8 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
               aligned(g.tax, 16) && aligned(g.flag, 4) && aligned(g.stat, 4);
       const uint32_t gi = (uint32_t)groups.size();
       groups.push_back(g);
-      std::vector<ScanTile>& tl = q1pass ? tiles1 : tiles6;
+      // a pass with one Q1 request keeps half the per-thread sums (twice the blocks per SM)
+      std::vector<ScanTile>& tl = q1pass ? (g.n_q1 == 1 ? tiles11 : tiles1) : tiles6;
       for (uint64_t b = g.begin; b < g.end;) {
         const uint64_t e = std::min<uint64_t>(g.end, (b / kTileRows + 1) * kTileRows);
         tl.push_back(ScanTile{gi, 0, b, e});
@@ -456,22 +457,25 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
   if (!groups.empty()) {
     void* desc = nullptr;
     const size_t qbytes = 256, gbytes = ((groups.size() * sizeof(ScanGroup) + 15) / 16) * 16;
-    const size_t t6 = ((tiles6.size() * sizeof(ScanTile) + 15) / 16) * 16, t1 = tiles1.size() * sizeof(ScanTile);
-    rc = scratch(ctx, "batch.desc", qbytes + gbytes + t6 + t1 + 256, &desc);
+    const size_t t6 = ((tiles6.size() * sizeof(ScanTile) + 15) / 16) * 16;
+    const size_t t1 = ((tiles1.size() * sizeof(ScanTile) + 15) / 16) * 16, t11 = tiles11.size() * sizeof(ScanTile);
+    rc = scratch(ctx, "batch.desc", qbytes + gbytes + t6 + t1 + t11 + 256, &desc);
     if (rc) return rc;
     uint8_t* base = static_cast<uint8_t*>(desc);
-    unsigned* queue = reinterpret_cast<unsigned*>(base);   // [0] Q6 passes, [1] Q1 passes
+    unsigned* queue = reinterpret_cast<unsigned*>(base);   // [0] Q6 passes, [1] two-Q1 passes, [2] one-Q1 passes
     ScanGroup* dgrp = reinterpret_cast<ScanGroup*>(base + qbytes);
     ScanTile* dt6 = reinterpret_cast<ScanTile*>(base + qbytes + gbytes);
     ScanTile* dt1 = reinterpret_cast<ScanTile*>(base + qbytes + gbytes + t6);
+    ScanTile* dt11 = reinterpret_cast<ScanTile*>(base + qbytes + gbytes + t6 + t1);
     // pageable sources: the copies stage the descriptors before returning
-    GPUDB_CUDA(ctx, cudaMemsetAsync(queue, 0, 8, call.stream()));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(queue, 0, 12, call.stream()));
     GPUDB_CUDA(ctx, cudaMemcpyAsync(dgrp, groups.data(), groups.size() * sizeof(ScanGroup), cudaMemcpyHostToDevice,
                                     call.stream()));
     unsigned long long* res = reinterpret_cast<unsigned long long*>(dres + status_bytes);
     uint32_t* st = reinterpret_cast<uint32_t*>(dres);
     rc = launch_pass<0, kMaxQ6>(ctx, call, dgrp, tiles6, dt6, queue, res, st);
     if (!rc) rc = launch_pass<kMaxQ1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles1, dt1, queue + 1, res, st);
+    if (!rc) rc = launch_pass<1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles11, dt11, queue + 2, res, st);
     if (rc) return rc;
   }
   std::vector<uint32_t> ids_copy = ids;
