@@ -27,6 +27,7 @@ OPT_Q9_SMEM_SLOTS = 6
 OPT_Q9_GLOBAL_SLOTS = 7
 OPT_GRAPHS = 8
 OPT_Q3_AUTO_MODE = 9
+OPT_RADIX_SHAPE = 10
 TBL_LINEITEM, TBL_ORDERS, TBL_CUSTOMER, TBL_PART, TBL_SUPPLIER, TBL_PARTSUPP = 1, 2, 3, 4, 5, 6
 TBL_MAX_COLS = 13
 # columns a .tbl parse keeps, in the order of gpudb_tbl_parse's cols[]
@@ -40,7 +41,7 @@ TBL_COLUMNS = {
     "partsupp": (TBL_PARTSUPP, ("part_key", "supp_key", "supply_cost")),
 }
 OPT_NAMES = {1: "chunk_rows", 2: "q1_variant", 3: "q6_variant", 4: "ht_load_pct", 5: "radix_bits",
-             6: "q9_smem_slots", 7: "q9_global_slots", 8: "graphs", 9: "q3_auto_mode"}
+             6: "q9_smem_slots", 7: "q9_global_slots", 8: "graphs", 9: "q3_auto_mode", 10: "radix_shape"}
 JOIN_GLOBAL, JOIN_RADIX, JOIN_DIRECT, JOIN_AUTO = 0, 1, 2, 3
 JOIN_MODES = (JOIN_GLOBAL, JOIN_RADIX, JOIN_DIRECT)
 JOIN_NAMES = {JOIN_GLOBAL: "global", JOIN_RADIX: "radix", JOIN_DIRECT: "direct", JOIN_AUTO: "auto"}

@@ -508,6 +508,10 @@ int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value) {
         return fail(ctx, GPUDB_E_INVALID, "radix bits must be 0 or 1..%d", (int)kRadixMaxBits);
       ctx->radix_bits = (int)value;
       return GPUDB_OK;
+    case GPUDB_OPT_RADIX_SHAPE:
+      if (value < 0 || value > 3) return fail(ctx, GPUDB_E_INVALID, "radix shape must be 0..3");
+      ctx->radix_shape = (int)value;
+      return GPUDB_OK;
     case GPUDB_OPT_Q3_AUTO_MODE:
       if (value != -1 && value != GPUDB_JOIN_GLOBAL && value != GPUDB_JOIN_RADIX && value != GPUDB_JOIN_DIRECT)
         return fail(ctx, GPUDB_E_INVALID, "Q3 AUTO mode must be -1 or a join mode (global, radix, direct)");
@@ -540,6 +544,7 @@ int gpudb_get_option(const gpudb_ctx* ctx, int32_t option, int64_t* value) {
     case GPUDB_OPT_Q9_GLOBAL_SLOTS: *value = ctx->q9_global_slots; return GPUDB_OK;
     case GPUDB_OPT_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return GPUDB_OK;
     case GPUDB_OPT_Q3_AUTO_MODE: *value = ctx->q3_auto_mode; return GPUDB_OK;
+    case GPUDB_OPT_RADIX_SHAPE: *value = ctx->radix_shape; return GPUDB_OK;
     default: return GPUDB_E_INVALID;
   }
 }

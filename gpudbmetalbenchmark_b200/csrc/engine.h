@@ -51,6 +51,7 @@ struct gpudb_ctx {
   int q6_variant = 0;                  // Q6 scan kernel choice (GPUDB_OPT_Q6_VARIANT)
   int ht_shift = 1;                    // hash tables hold <= 1/2^ht_shift load (GPUDB_OPT_HT_LOAD)
   int radix_bits = 0;                  // Q3 radix fan-out when a call leaves it 0 (GPUDB_OPT_RADIX_BITS)
+  int radix_shape = 0;                 // radix scatter block shape (GPUDB_OPT_RADIX_SHAPE)
   int q3_auto_mode = -1;               // what a Q3 AUTO call runs; -1: the 30% rule (GPUDB_OPT_Q3_AUTO_MODE)
   int q9_smem_slots = 1024;            // Q9 aggregation slots when a call leaves them 0
   int q9_global_slots = 4096;

@@ -352,6 +352,116 @@ __global__ void __launch_bounds__(256) q3_direct_probe_kernel(
   }
 }
 
+// Quad form of the direct probe, for 16-byte aligned columns: a lane takes kDirectQuads quads
+// (4 consecutive rows each: one 16-byte load of keys and one of ship dates per quad). Inside a
+// quad, rows of one order are adjacent, so the lane looks up each distinct key among its
+// passing rows once (bitmap word, then slot), and rows of equal slot are summed before one
+// atomic pair. ext_price / discount of a quad load only when one of its rows joins. The
+// kDirectQuads quads' loads are issued phase by phase, all in flight together. Tail rows past
+// the last whole quad go one per thread.
+constexpr int kDirectQuads = 2;
+
+__global__ void __launch_bounds__(256) q3_direct_quad_kernel(
+    const int4* __restrict__ lkey4, const int4* __restrict__ lship4, const longlong2* __restrict__ lext2,
+    const int4* __restrict__ ldisc4, uint64_t n, int32_t ship_gt, const uint32_t* __restrict__ okbm,
+    const int32_t* __restrict__ omap, int32_t key_max, Q3Slot* ht, uint32_t* hits, const uint32_t* count,
+    uint32_t* cap_out) {
+  if (blockIdx.x == 0) seal_dense_slots(count, hits, cap_out);
+  constexpr int U = kDirectQuads;
+  const uint64_t nq = n >> 2;
+  const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t q0 = tid; q0 < nq; q0 += U * T) {
+    int32_t key[4 * U], ship[4 * U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint64_t q = q0 + u * T;
+      const int4 k = q < nq ? ld_stream(lkey4 + q) : make_int4(-1, -1, -1, -1);
+      const int4 sh = q < nq ? ld_stream(lship4 + q) : make_int4(ship_gt, ship_gt, ship_gt, ship_gt);
+      key[4 * u] = k.x; key[4 * u + 1] = k.y; key[4 * u + 2] = k.z; key[4 * u + 3] = k.w;
+      ship[4 * u] = sh.x; ship[4 * u + 1] = sh.y; ship[4 * u + 2] = sh.z; ship[4 * u + 3] = sh.w;
+    }
+    // rows that look their key up: passing, in range, and a key other than the previous
+    // looked-up row's in the quad
+    uint32_t want = 0, pass = 0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      int32_t last = INT32_MIN;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = 4 * u + i;
+        const bool p = ship[r] > ship_gt && key[r] >= 0 && key[r] <= key_max;
+        pass |= (uint32_t)p << r;
+        if (p && key[r] != last) { want |= 1u << r; last = key[r]; }
+      }
+    }
+    uint32_t word[4 * U];
+#pragma unroll
+    for (int r = 0; r < 4 * U; r++) word[r] = (want >> r & 1u) ? __ldg(okbm + ((uint32_t)key[r] >> 5)) : 0u;
+    int32_t slot[4 * U];
+#pragma unroll
+    for (int r = 0; r < 4 * U; r++)
+      slot[r] = ((want >> r & 1u) && (word[r] >> ((uint32_t)key[r] & 31u) & 1u)) ? __ldg(omap + key[r]) : -1;
+    // rows that did not look up take the slot of the previous row of the quad (same key)
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int i = 1; i < 4; i++) {
+        const int r = 4 * u + i;
+        if (!(want >> r & 1u)) slot[r] = slot[r - 1];
+      }
+    uint32_t join = 0;
+#pragma unroll
+    for (int r = 0; r < 4 * U; r++) join |= (uint32_t)((pass >> r & 1u) && slot[r] >= 0) << r;
+    if (!join) continue;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint32_t jq = (join >> (4 * u)) & 0xFu;
+      if (!jq) continue;
+      const uint64_t q = q0 + u * T;
+      const longlong2 e01 = ld_stream(lext2 + 2 * q), e23 = ld_stream(lext2 + 2 * q + 1);
+      const int4 d = ld_stream(ldisc4 + q);
+      const int64_t ev[4] = {e01.x, e01.y, e23.x, e23.y};
+      const int32_t dv[4] = {d.x, d.y, d.z, d.w};
+      unsigned long long acc = 0;
+      uint32_t cnt = 0;
+      int32_t cur = -1;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = 4 * u + i;
+        if (!(jq >> i & 1u)) continue;
+        if (slot[r] != cur && cnt) {
+          atomicAdd(&ht[cur].rev, acc);
+          atomicAdd(&hits[cur], cnt);
+          acc = 0;
+          cnt = 0;
+        }
+        cur = slot[r];
+        acc += (unsigned long long)(ev[i] * (int64_t)(100 - dv[i]));
+        cnt++;
+      }
+      if (cnt) {
+        atomicAdd(&ht[cur].rev, acc);
+        atomicAdd(&hits[cur], cnt);
+      }
+    }
+  }
+  // rows past the last whole quad (at most 3)
+  const uint64_t r = (nq << 2) + tid;
+  if (r < n) {
+    const int32_t* k1 = reinterpret_cast<const int32_t*>(lkey4);
+    const int32_t* s1 = reinterpret_cast<const int32_t*>(lship4);
+    const int32_t k = k1[r];
+    if (s1[r] > ship_gt && k >= 0 && k <= key_max && bitmap_test(okbm, k)) {
+      const int32_t sl = omap[k];
+      const int64_t e = reinterpret_cast<const int64_t*>(lext2)[r];
+      const int32_t dd = reinterpret_cast<const int32_t*>(ldisc4)[r];
+      atomicAdd(&ht[sl].rev, (unsigned long long)(e * (int64_t)(100 - dd)));
+      atomicAdd(&hits[sl], 1u);
+    }
+  }
+}
+
 // Top-k of the table: the revenue histogram pass, then the select-and-rank pass
 // (q3_table_hist / q3_table_select).
 __global__ void __launch_bounds__(kTopkThreads) q3_hist_kernel(const Q3Slot* __restrict__ ht,
@@ -444,13 +554,31 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
       }
     }
     __syncthreads();
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kTopkThreads) {
-      const int32_t key = pk[i];
-      if (key == kEmptyKey) continue;
+    // the partition keeps the input order, so an order's rows are adjacent: whole warps take
+    // 32 rows at a time, runs of equal keys are summed across their lanes (segmented shuffle
+    // scan) and the last lane of a run probes and adds once for the run
+    const int lane = threadIdx.x & 31;
+    for (uint32_t base = p0 + (threadIdx.x & ~31u); base < p1; base += kTopkThreads) {
+      const uint32_t i = base + lane;
+      const bool valid = i < p1;
+      const int32_t key = valid ? pk[i] : kEmptyKey;
+      long long v = valid ? (long long)pval[i] : 0ll;
+      uint32_t c = valid ? 1u : 0u;
+      const int32_t prev = __shfl_up_sync(FULL_MASK, key, 1);
+      const uint32_t heads = __ballot_sync(FULL_MASK, lane == 0 || key != prev);
+      const int seg = 31 - __clz(heads & lanemask_le());   // first lane of this lane's run
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const long long ov = __shfl_up_sync(FULL_MASK, v, d);
+        const uint32_t oc = __shfl_up_sync(FULL_MASK, c, d);
+        if (lane - d >= seg) { v += ov; c += oc; }
+      }
+      const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+      if (!tail || !valid || key == kEmptyKey) continue;
       uint32_t s = key_slot(key, mask);
       for (uint32_t t = 0; t < kQ3PartCap; t++, s = (s + 1) & mask) {
         const int32_t hk = hkey[s];
-        if (hk == key) { atomicAdd(&hrev[s], (unsigned long long)pval[i]); atomicAdd(&hhit[s], 1u); break; }
+        if (hk == key) { atomicAdd(&hrev[s], (unsigned long long)v); atomicAdd(&hhit[s], c); break; }
         if (hk == kEmptyKey) break;
       }
     }
@@ -599,12 +727,24 @@ int q3_direct(Call& call, const gpudb_customer& cu, const gpudb_orders& od, cons
   const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
   rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
     if (c.n_rows == 0) return (int)GPUDB_OK;
-    const uint64_t per_block = 256 * kDirectBatches;
-    const unsigned g = (unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>((c.n_rows + per_block - 1) / per_block, (uint64_t)sms * 8));
-    GPUDB_LAUNCH(call, q3_direct_probe_kernel, g, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount, c.n_rows,
-                 p.ship_date_gt, (const uint32_t*)okbm, (const int32_t*)omap, key_max, (Q3Slot*)ht, (uint32_t*)hits,
-                 (const uint32_t*)cnt, cnt + 1);
+    auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    if (a16(c.order_key) && a16(c.ship_date) && a16(c.ext_price) && a16(c.discount)) {
+      const uint64_t per_block = 256 * 4 * kDirectQuads;
+      const unsigned g = (unsigned)std::max<uint64_t>(
+          1, std::min<uint64_t>((c.n_rows + per_block - 1) / per_block,
+                                (uint64_t)sms * kernel_occupancy(ctx, (const void*)q3_direct_quad_kernel, 256, 0)));
+      GPUDB_LAUNCH(call, q3_direct_quad_kernel, g, 256, 0, (const int4*)c.order_key, (const int4*)c.ship_date,
+                   (const longlong2*)c.ext_price, (const int4*)c.discount, c.n_rows, p.ship_date_gt,
+                   (const uint32_t*)okbm, (const int32_t*)omap, key_max, (Q3Slot*)ht, (uint32_t*)hits,
+                   (const uint32_t*)cnt, cnt + 1);
+    } else {
+      const uint64_t per_block = 256 * kDirectBatches;
+      const unsigned g = (unsigned)std::max<uint64_t>(
+          1, std::min<uint64_t>((c.n_rows + per_block - 1) / per_block, (uint64_t)sms * 8));
+      GPUDB_LAUNCH(call, q3_direct_probe_kernel, g, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount,
+                   c.n_rows, p.ship_date_gt, (const uint32_t*)okbm, (const int32_t*)omap, key_max, (Q3Slot*)ht,
+                   (uint32_t*)hits, (const uint32_t*)cnt, cnt + 1);
+    }
     return (int)GPUDB_OK;
   });
   if (rc) return rc;

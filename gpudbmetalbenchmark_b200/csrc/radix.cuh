@@ -6,14 +6,15 @@
 //
 // B200 design. Partition p = key_hash32(key) & (2^bits - 1) (the reference's hash), in LSD
 // passes of at most kRxPassBits bits (one pass up to 1024 partitions). The input is cut into
-// G super-tiles, about one per SM, sized on the device from the row count; per pass:
+// G super-tiles, as many as the scatter kernel's blocks that fit on the GPU at once, sized
+// on the device from the row count; per pass:
 //   rx_hist_kernel    counts each super-tile's rows per digit (shared-memory atomics; four
 //                     blocks per super-tile, so every SM streams) into hist[digit][G], and
 //                     in the first pass also the rows per final partition;
 //   exclusive_scan    over hist (digit-major): where each (digit, super-tile) run starts;
-//   rx_scatter_kernel one block per super-tile walks its 8192-row sub-tiles in order. Each
-//                     warp ranks its own 512 contiguous rows by digit (__match_any_sync and
-//                     per-warp counters, no atomics), one block-wide scan turns the
+//   rx_scatter_kernel one block per super-tile walks its sub-tiles (2048 rows by default) in
+//                     order. Each warp ranks its own contiguous rows by digit (__match_any_sync
+//                     and per-warp counters, no atomics), one block-wide scan turns the
 //                     (digit, warp) counts into staged positions, the sub-tile is staged
 //                     digit-sorted in shared memory and written out run by run from
 //                     per-digit cursors that carry across the super-tile's sub-tiles.
@@ -31,11 +32,7 @@
 
 namespace gpudb {
 
-constexpr int kRxThreads = 512;
-constexpr int kRxWarps = kRxThreads / 32;
-constexpr int kRxItems = 16;                            // rows per lane per sub-tile
-constexpr int kRxTile = kRxThreads * kRxItems;          // 8192 rows per sub-tile
-constexpr int kRxWarpRows = kRxTile / kRxWarps;         // 512 contiguous rows per warp
+constexpr int kRxThreads = 512;                         // histogram blocks
 constexpr int kRxPassBits = 10;                         // fan-out of one pass <= 1024
 constexpr uint32_t kRxMaxF = 1u << kRxPassBits;
 constexpr int kRxFullSmemBits = 13;                     // final-partition counts in shared memory up to 8192
@@ -59,13 +56,13 @@ struct ColumnSource {
   __device__ __forceinline__ P payload(uint64_t r) const { return pay ? __ldcs(pay + r) : (P)r; }
 };
 
-// Rows per super-tile for n rows over G super-tiles: whole sub-tiles, at least one. Both
-// kernels of a pass derive it from the same device row count, so a count that an earlier
-// kernel left on the device (a filtered input) still spreads over all G blocks.
-__host__ __device__ __forceinline__ uint64_t rx_super_rows_for(uint64_t n, uint32_t G) {
+// Rows per super-tile for n rows over G super-tiles: whole sub-tiles of `tile` rows, at least
+// one. Both kernels of a pass derive it from the same device row count, so a count that an
+// earlier kernel left on the device (a filtered input) still spreads over all G blocks.
+__host__ __device__ __forceinline__ uint64_t rx_super_rows_for(uint64_t n, uint32_t G, uint32_t tile) {
   const uint64_t per = (n + G - 1) / (G ? G : 1);
-  const uint64_t s = (per + kRxTile - 1) / kRxTile * kRxTile;
-  return s < (uint64_t)kRxTile ? (uint64_t)kRxTile : s;
+  const uint64_t s = (per + tile - 1) / tile * tile;
+  return s < (uint64_t)tile ? (uint64_t)tile : s;
 }
 
 __device__ __forceinline__ uint32_t rx_digit(int32_t key, int shift, uint32_t mask) {
@@ -102,8 +99,9 @@ __device__ __forceinline__ uint32_t rx_block_scan(uint32_t v, uint32_t* warp_tot
 // hist[digit * G + super-tile] (zeroed), and with `full` the rows per final partition
 // (fbits bits; zeroed).
 template <class Src>
-__global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G, int shift, int dbits, int fbits,
-                                                             uint32_t* __restrict__ hist, uint32_t* __restrict__ full) {
+__global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G, uint32_t tile, int shift, int dbits,
+                                                             int fbits, uint32_t* __restrict__ hist,
+                                                             uint32_t* __restrict__ full) {
   __shared__ uint32_t cnt[kRxMaxF];
   __shared__ uint32_t fcnt[1u << kRxFullSmemBits];
   const uint32_t F = 1u << dbits, dmask = F - 1, fmask = (1u << fbits) - 1;
@@ -114,7 +112,7 @@ __global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G
   __syncthreads();
   const uint32_t g = blockIdx.x / kRxHistSplit, part = blockIdx.x % kRxHistSplit;
   const uint64_t n = src.rows();
-  const uint64_t super_rows = rx_super_rows_for(n, G);
+  const uint64_t super_rows = rx_super_rows_for(n, G, tile);
   const uint64_t quarter = super_rows / kRxHistSplit;
   const uint64_t r0 = (uint64_t)g * super_rows + part * quarter;
   const uint64_t r1 = min(r0 + quarter, n);
@@ -144,43 +142,46 @@ __global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G
       if (fcnt[i]) atomicAdd(&full[i], fcnt[i]);
 }
 
-template <class P, bool PAY>
+template <class P, bool PAY, int T, int I>
 __host__ __device__ constexpr size_t rx_scatter_smem(uint32_t F) {
-  return (PAY ? sizeof(P) * kRxTile : 0) + sizeof(int32_t) * kRxTile + sizeof(uint16_t) * kRxWarps * F +
-         sizeof(uint32_t) * F;
+  return (PAY ? sizeof(P) * T * I : 0) + (sizeof(int32_t) + sizeof(uint16_t)) * T * I +
+         sizeof(uint16_t) * (T / 32) * F + sizeof(uint32_t) * F;
 }
 
-// One block per super-tile (see the file comment). offs: exclusive scan of hist.
-template <class Src, class P, bool PAY>
-__global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint32_t G, int shift, int dbits,
-                                                                   const uint32_t* __restrict__ offs,
-                                                                   int32_t* __restrict__ kout, P* __restrict__ pout) {
+// One block of T threads per super-tile (see the file comment), sub-tiles of T * I rows.
+// offs: exclusive scan of hist.
+template <class Src, class P, bool PAY, int T, int I>
+__global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int shift, int dbits,
+                                                       const uint32_t* __restrict__ offs, int32_t* __restrict__ kout,
+                                                       P* __restrict__ pout) {
+  constexpr int W = T / 32, TILE = T * I, WROWS = TILE / W;
   extern __shared__ __align__(16) unsigned char rx_smem[];
   const uint32_t F = 1u << dbits, dmask = F - 1;
   P* spay = reinterpret_cast<P*>(rx_smem);
-  int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + (PAY ? sizeof(P) * kRxTile : 0));
-  uint16_t* wcnt = reinterpret_cast<uint16_t*>(skey + kRxTile);        // [warp][digit]
-  uint32_t* cur = reinterpret_cast<uint32_t*>(wcnt + kRxWarps * F);    // next output row per digit
-  __shared__ uint32_t wt[kRxWarps];
+  int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + (PAY ? sizeof(P) * TILE : 0));
+  uint16_t* sdig = reinterpret_cast<uint16_t*>(skey + TILE);            // digit of each staged row
+  uint16_t* wcnt = sdig + TILE;                                         // [warp][digit]
+  uint32_t* cur = reinterpret_cast<uint32_t*>(wcnt + W * F);            // next output row per digit
+  __shared__ uint32_t wt[W];
   __shared__ uint32_t s_total;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t n = src.rows();
-  const uint64_t super_rows = rx_super_rows_for(n, G);
+  const uint64_t super_rows = rx_super_rows_for(n, G, TILE);
   const uint64_t g0 = (uint64_t)blockIdx.x * super_rows;
   if (g0 >= n) return;   // uniform across the block
   const uint64_t g1 = min(g0 + super_rows, n);
-  for (uint32_t d = threadIdx.x; d < F; d += kRxThreads) cur[d] = offs[(size_t)d * G + blockIdx.x];
-  for (uint32_t i = threadIdx.x; i < kRxWarps * F; i += kRxThreads) wcnt[i] = 0;
+  for (uint32_t d = threadIdx.x; d < F; d += T) cur[d] = offs[(size_t)d * G + blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
   __syncthreads();
   uint16_t* mine = wcnt + warp * F;
-  const uint32_t dpt = (F + kRxThreads - 1) / kRxThreads;   // digits per thread in the scan
-  for (uint64_t t0 = g0; t0 < g1; t0 += kRxTile) {
-    int32_t key[kRxItems];
-    P pay[kRxItems];
-    uint32_t dr[kRxItems];   // digit << 16 | rank among the warp's rows of that digit; ~0u: no row
-    const uint64_t wb = t0 + (uint64_t)warp * kRxWarpRows + lane;
+  const uint32_t dpt = (F + T - 1) / T;   // digits per thread in the scan
+  for (uint64_t t0 = g0; t0 < g1; t0 += TILE) {
+    int32_t key[I];
+    P pay[I];
+    uint32_t dr[I];   // digit << 16 | rank among the warp's rows of that digit; ~0u: no row
+    const uint64_t wb = t0 + (uint64_t)warp * WROWS + lane;
 #pragma unroll
-    for (int j = 0; j < kRxItems; j++) {
+    for (int j = 0; j < I; j++) {
       const uint64_t r = wb + (uint64_t)j * 32;
       const bool v = r < g1 && src.key(r, key[j]);
       dr[j] = v ? 0u : ~0u;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint
     // rank inside the warp, 32 rows at a time in row order: the first lane of each digit
     // reads and advances the warp's counter for it
 #pragma unroll
-    for (int j = 0; j < kRxItems; j++) {
+    for (int j = 0; j < I; j++) {
       const bool v = dr[j] == 0u;
       const uint32_t d = v ? rx_digit(key[j], shift, dmask) : 0x10000u + lane;
       const uint32_t peers = __match_any_sync(FULL_MASK, d);
@@ -207,47 +208,48 @@ __global__ void __launch_bounds__(kRxThreads, 1) rx_scatter_kernel(Src src, uint
     // of warp 1, ... (row order); wcnt[0][d] becomes the start of digit d
     {
       const uint32_t b0 = min(threadIdx.x * dpt, F), b1 = min(b0 + dpt, F);
-      uint32_t s = 0;
+      uint32_t sum = 0;
       for (uint32_t b = b0; b < b1; b++)
 #pragma unroll
-        for (int w = 0; w < kRxWarps; w++) s += wcnt[w * F + b];
-      const uint32_t inc = rx_block_scan<kRxThreads>(s, wt);
-      uint32_t run = inc - s;
+        for (int w = 0; w < W; w++) sum += wcnt[w * F + b];
+      const uint32_t inc = rx_block_scan<T>(sum, wt);
+      uint32_t run = inc - sum;
       for (uint32_t b = b0; b < b1; b++)
 #pragma unroll
-        for (int w = 0; w < kRxWarps; w++) {
+        for (int w = 0; w < W; w++) {
           const uint32_t c = wcnt[w * F + b];
           wcnt[w * F + b] = (uint16_t)run;
           run += c;
         }
-      if (threadIdx.x == kRxThreads - 1) s_total = inc;
+      if (threadIdx.x == T - 1) s_total = inc;
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < kRxItems; j++)
+    for (int j = 0; j < I; j++)
       if (dr[j] != ~0u) {
-        const uint32_t pos = (uint32_t)mine[dr[j] >> 16] + (dr[j] & 0xFFFFu);
+        const uint32_t d = dr[j] >> 16;
+        const uint32_t pos = (uint32_t)mine[d] + (dr[j] & 0xFFFFu);
         skey[pos] = key[j];
+        sdig[pos] = (uint16_t)d;
         if (PAY) spay[pos] = pay[j];
       }
     __syncthreads();
     // write out: consecutive threads take consecutive staged rows, i.e. consecutive output
     // rows inside each digit's run
     const uint32_t m = s_total;
-    for (uint32_t i = threadIdx.x; i < m; i += kRxThreads) {
-      const int32_t k = skey[i];
-      const uint32_t d = rx_digit(k, shift, dmask);
+    for (uint32_t i = threadIdx.x; i < m; i += T) {
+      const uint32_t d = sdig[i];
       const uint32_t o = cur[d] + (i - (uint32_t)wcnt[d]);
-      kout[o] = k;
+      kout[o] = skey[i];
       if (PAY) pout[o] = spay[i];
     }
     __syncthreads();
-    for (uint32_t d = threadIdx.x; d < F; d += kRxThreads) {
+    for (uint32_t d = threadIdx.x; d < F; d += T) {
       const uint32_t end = d + 1 < F ? (uint32_t)wcnt[d + 1] : m;
       cur[d] += end - (uint32_t)wcnt[d];
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kRxWarps * F; i += kRxThreads) wcnt[i] = 0;
+    for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
     __syncthreads();
   }
 }
@@ -259,16 +261,8 @@ static __global__ void rx_starts_kernel(const uint32_t* __restrict__ offs, uint3
     offsets[b] = b < F ? offs[(size_t)b * G] : *total;
 }
 
-// Super-tiles: about one per SM, fewer for an input of fewer sub-tiles (the kernels size
-// them from the device row count, at most n_max rows).
-inline uint32_t rx_super_tiles(uint64_t n_max, int sms) {
-  const uint64_t sub = (std::max<uint64_t>(n_max, 1) + kRxTile - 1) / kRxTile;
-  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sub, (uint64_t)std::max(sms, 1)));
-}
-
-// Scratch words for one partitioning of at most n_max rows with `bits` bits.
-inline size_t rx_scratch_words(uint64_t n_max, int bits, int sms) {
-  const uint64_t G = rx_super_tiles(n_max, sms);
+// Scratch words for one partitioning with `bits` bits over G super-tiles.
+inline size_t rx_scratch_words(uint32_t G, int bits) {
   const size_t hn = (size_t)kRxMaxF * G + 1;
   const size_t parts = (size_t)1 << bits;
   return 2 * hn + std::max(scan_tiles_count(hn), scan_tiles_count(parts)) + 8 + parts + 8;
@@ -276,19 +270,29 @@ inline size_t rx_scratch_words(uint64_t n_max, int bits, int sms) {
 
 // Partitions the rows of `src` (at most n_max) into 2^bits partitions: keys (and payloads
 // when PAY) to kout/pout, partition starts to offsets[0 .. 2^bits] (the total last). Two
-// passes when bits > kRxPassBits, through ktmp/ptmp (n_max rows each).
-template <class Src, class P, bool PAY>
-int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout, uint32_t* offsets,
-                 int32_t* ktmp, P* ptmp) {
+// passes when bits > kRxPassBits, through ktmp/ptmp (n_max rows each). The scatter kernel
+// runs with T threads and I rows per thread; there are as many super-tiles as its blocks
+// fit on the GPU at once (fewer for a small input).
+template <class Src, class P, bool PAY, int T, int I>
+int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout,
+                        uint32_t* offsets, int32_t* ktmp, P* ptmp) {
+  constexpr uint32_t TILE = T * I;
   gpudb_ctx* ctx = call.ctx();
   cudaStream_t s = call.stream();
   const int passes = bits <= kRxPassBits ? 1 : 2;
   const int d0 = passes == 1 ? bits : (bits + 1) / 2;
-  const uint32_t G = rx_super_tiles(n_max, ctx->sm_count);
+  auto k0 = rx_scatter_kernel<Src, P, PAY, T, I>;
+  auto k1 = rx_scatter_kernel<ColumnSource<P>, P, PAY, T, I>;
+  const size_t smem_max = rx_scatter_smem<P, PAY, T, I>(1u << std::max(d0, bits - d0));
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k0, smem_max));
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k1, smem_max));
+  const int per_sm = kernel_occupancy(ctx, (const void*)k0, T, smem_max);
+  const uint64_t sub = (std::max<uint64_t>(n_max, 1) + TILE - 1) / TILE;
+  const uint32_t G = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sub, (uint64_t)ctx->sm_count * per_sm));
   const size_t hn = (size_t)kRxMaxF * G + 1;
   const size_t parts = (size_t)1 << bits;
   void* sc = nullptr;
-  int rc = scratch(ctx, "radix.meta", rx_scratch_words(n_max, bits, ctx->sm_count) * sizeof(uint32_t), &sc);
+  int rc = scratch(ctx, "radix.meta", rx_scratch_words(G, bits) * sizeof(uint32_t), &sc);
   if (rc) return rc;
   uint32_t* hist = static_cast<uint32_t*>(sc);
   uint32_t* offs = hist + hn;
@@ -301,29 +305,25 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
     const size_t hf = (size_t)F * G;
     int32_t* ko = pass == passes - 1 ? kout : ktmp;
     P* po = pass == passes - 1 ? pout : ptmp;
-    const size_t smem = rx_scatter_smem<P, PAY>(F);
+    const size_t smem = rx_scatter_smem<P, PAY, T, I>(F);
     GPUDB_CUDA(ctx, cudaMemsetAsync(hist, 0, hf * sizeof(uint32_t), s));
     if (pass == 0 && passes > 1) GPUDB_CUDA(ctx, cudaMemsetAsync(full, 0, parts * sizeof(uint32_t), s));
     uint32_t* fullp = (pass == 0 && passes > 1) ? full : nullptr;
     if (pass == 0) {
-      GPUDB_LAUNCH(call, (rx_hist_kernel<Src>), G * kRxHistSplit, kRxThreads, 0, src, G, shift, dbits, bits, hist,
-                   fullp);
+      GPUDB_LAUNCH(call, (rx_hist_kernel<Src>), G * kRxHistSplit, kRxThreads, 0, src, G, TILE, shift, dbits, bits,
+                   hist, fullp);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
-      GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)rx_scatter_kernel<Src, P, PAY>, smem));
-      GPUDB_LAUNCH(call, (rx_scatter_kernel<Src, P, PAY>), G, kRxThreads, smem, src, G, shift, dbits,
-                   (const uint32_t*)offs, ko, po);
+      GPUDB_LAUNCH(call, k0, G, T, smem, src, G, shift, dbits, (const uint32_t*)offs, ko, po);
     } else {
       // rows of the first pass, in their pass-one order; their count is the first scan's total
       const uint32_t* total0 = full + parts;   // copied below
       const ColumnSource<P> s2{ktmp, PAY ? ptmp : nullptr, n_max, total0};
-      GPUDB_LAUNCH(call, (rx_hist_kernel<ColumnSource<P>>), G * kRxHistSplit, kRxThreads, 0, s2, G, shift, dbits,
-                   bits, hist, (uint32_t*)nullptr);
+      GPUDB_LAUNCH(call, (rx_hist_kernel<ColumnSource<P>>), G * kRxHistSplit, kRxThreads, 0, s2, G, TILE, shift,
+                   dbits, bits, hist, (uint32_t*)nullptr);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
-      GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)rx_scatter_kernel<ColumnSource<P>, P, PAY>, smem));
-      GPUDB_LAUNCH(call, (rx_scatter_kernel<ColumnSource<P>, P, PAY>), G, kRxThreads, smem, s2, G, shift, dbits,
-                   (const uint32_t*)offs, ko, po);
+      GPUDB_LAUNCH(call, k1, G, T, smem, s2, G, shift, dbits, (const uint32_t*)offs, ko, po);
     }
     if (pass == 0 && passes > 1)
       GPUDB_CUDA(ctx, cudaMemcpyAsync(full + parts, offs + hf, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -335,6 +335,18 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
     return GPUDB_OK;
   }
   return exclusive_scan<uint32_t, uint32_t>(call, full, parts, offsets, stmp, offsets + parts);
+}
+
+// The scatter block shape of the context (GPUDB_OPT_RADIX_SHAPE): 256 threads x 8 rows by
+// default (several blocks per SM), 512 x 16 or 256 x 16.
+template <class Src, class P, bool PAY>
+int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout, uint32_t* offsets,
+                 int32_t* ktmp, P* ptmp) {
+  switch (call.ctx()->radix_shape) {
+    case 1: return rx_partition_shaped<Src, P, PAY, 512, 16>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    case 3: return rx_partition_shaped<Src, P, PAY, 256, 16>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    default: return rx_partition_shaped<Src, P, PAY, 256, 8>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+  }
 }
 
 // Plain columns (payload = row id when pay is null); the row count may be on the device.

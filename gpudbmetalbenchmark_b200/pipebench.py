@@ -277,9 +277,16 @@ def main(argv=None):
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--stream600m", action="store_true", help="config 3 streamed at 600M fact rows (16.8 GB pinned)")
+    ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
+                    help="context option before measuring, e.g. radix_shape=1 (names: capi.OPT_NAMES)")
     a = ap.parse_args(argv)
     want = set(a.only) if a.only else None
     eng = Engine(0)
+    for o in a.opt:
+        name, value = o.split("=")
+        ids = {v: k for k, v in capi.OPT_NAMES.items()}
+        eng.set_option(ids[name], int(value))
+        print(json.dumps({"option": name, "value": int(value)}), flush=True)
     on = lambda name: want is None or name in want  # noqa: E731
 
     if on("scans"):
