@@ -108,6 +108,31 @@ def test_radix_partition_large_inputs(engine, orc, bits, n):
             engine.device_free(x)
 
 
+@pytest.mark.parametrize("shape", [1, 2, 3])
+def test_radix_partition_every_block_shape(engine, orc, shape):
+    """Every scatter block shape (GPUDB_OPT_RADIX_SHAPE) gives the oracle's stable partition,
+    in one pass (10 bits) and in two (13 bits), and the same join count."""
+    n = 2_000_003
+    keys = orc.gen(8, n, seed=shape, n_orders=n // 3, order_mode=1)
+    pay = np.arange(n, dtype=np.int32) * 3
+    dk, dp = engine.to_device(keys), engine.to_device(pay)
+    ko, po, off = engine.device_array(n * 4), engine.device_array(n * 4), engine.device_array(((1 << 13) + 1) * 4)
+    try:
+        engine.set_option(capi.OPT_RADIX_SHAPE, shape)
+        for bits in (10, 13):
+            engine.radix_partition(dk, dp, n, bits, ko, po, off)
+            wk, wp, woff = orc.radix_partition(keys, pay, bits)
+            assert np.array_equal(engine.to_host(off, (1 << bits) + 1, np.uint32), woff)
+            assert np.array_equal(engine.to_host(ko, n, np.int32), wk)
+            assert np.array_equal(engine.to_host(po, n, np.int32), wp)
+        b = keys[: n // 4]
+        assert engine.hash_join_count(dk, n // 4, dk, n, capi.JOIN_RADIX) == orc.join_count(b, keys)
+    finally:
+        engine.set_option(capi.OPT_RADIX_SHAPE, 0)
+        for x in (dk, dp, ko, po, off):
+            engine.device_free(x)
+
+
 def test_radix_partition_bad_bits(engine):
     with pytest.raises(capi.GpudbError) as e:
         engine.radix_partition(None, None, 0, 17, 1, 1, 1)
