@@ -564,7 +564,10 @@ __global__ void __launch_bounds__(THREADS, 1) q1_ring_smem_kernel(const int32_t*
 constexpr int kQ1SmemThreads = 256;
 constexpr size_t kQ1AccBytes = (size_t)4 * 6 * kQ1SmemThreads * 8;   // 49,152
 
-__global__ void __launch_bounds__(kQ1SmemThreads) q1_vec_smem_kernel(const int4* __restrict__ ship4, const int4* __restrict__ qty4,
+// MINB: resident blocks per SM the registers are sized for (2: the default; 3: variant 8,
+// more loads in flight for tables that end in one short wave).
+template <int MINB>
+__global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const int4* __restrict__ ship4, const int4* __restrict__ qty4,
                                                                      const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
                                                                      const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
                                                                      const uint32_t* __restrict__ stat4, uint64_t n, int32_t ship_le,
@@ -702,11 +705,12 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
   // 4 TMA 4096-row tiles x 2 stages
   int variant = ctx->scan_variant;
   if (variant == 0) variant = vec ? 7 : 3;
-  if (variant == 7 && !vec) variant = 3;
-  if (variant == 7) {
+  if ((variant == 7 || variant == 8) && !vec) variant = 3;
+  if (variant == 7 || variant == 8) {
+    auto kern = variant == 8 ? q1_vec_smem_kernel<3> : q1_vec_smem_kernel<2>;
     const size_t smem = kQ1AccBytes;
-    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q1_vec_smem_kernel, smem));
-    const int per_sm = kernel_occupancy(ctx, (const void*)q1_vec_smem_kernel, kQ1SmemThreads, smem);
+    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kern, smem));
+    const int per_sm = kernel_occupancy(ctx, (const void*)kern, kQ1SmemThreads, smem);
     const uint64_t min_blocks = (c.n_rows + (uint64_t)kQ1SmemThreads * kQ1RowsPerThread - 1) /
                                 ((uint64_t)kQ1SmemThreads * kQ1RowsPerThread);
     const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
@@ -716,7 +720,7 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
     unsigned* ticket = nullptr;
     int rc = scan_scratch(ctx, "q1.partials", (size_t)grid * 6 * kQ1Raw * sizeof(u128), &part, &ticket);
     if (rc) return rc;
-    GPUDB_LAUNCH(call, q1_vec_smem_kernel, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
+    GPUDB_LAUNCH(call, kern, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
                  (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
                  (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status);
     return GPUDB_OK;

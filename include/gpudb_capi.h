@@ -98,7 +98,8 @@ enum {
   GPUDB_OPT_CHUNK_ROWS = 1,  /* rows per streamed chunk of a host-resident fact table (default 64M) */
   GPUDB_OPT_SCAN_VARIANT = 2, /* Q1 scan kernel: 0 auto (7), 1 TMA 2048-row tiles x 4 stages, 2 128-bit loads,
                                  3 one row per thread, 4 TMA 4096-row tiles x 2 stages, 5 TMA ring,
-                                 6 TMA ring + shared accumulators, 7 128-bit loads + shared accumulators */
+                                 6 TMA ring + shared accumulators, 7 128-bit loads + shared accumulators,
+                                 8 as 7 with registers for three blocks per SM */
   GPUDB_OPT_Q6_VARIANT = 3,   /* Q6 scan kernel: 0 auto (1 below 2^24 rows, else 2), 1 one row per thread,
                                  2/3/4 128-bit loads with 1/2/4 quads (4/8/16 rows) per thread per step */
   GPUDB_OPT_HT_LOAD = 4,      /* largest load of the Q3/Q9 build hash tables, percent: 50 (default) or 25 */

@@ -56,7 +56,7 @@ def test_q6_q1_small_sizes(engine, orc, n):
         engine.free(t)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7, 8])
 @pytest.mark.parametrize("n", [2047, 2048, 2049, 3 * 4096 + 5, 1_000_003])
 def test_q1_every_kernel_variant(engine, orc, variant, n):
     """TMA-staged tiles (1), 128-bit loads (2) and one row per thread (3) agree exactly."""
@@ -273,7 +273,7 @@ def test_full_size_60m_bit_exact(engine, orc):
         li = orc.lineitem(n, seed=42)
         assert engine.q6(t) == orc.q6(li, threads=8)
         want = orc.q1(li, threads=8)
-        for variant in (1, 2, 3, 4, 5, 6, 7):
+        for variant in (1, 2, 3, 4, 5, 6, 7, 8):
             engine.set_scan_variant(variant)
             assert engine.q1(t) == want
         engine.set_scan_variant(0)
