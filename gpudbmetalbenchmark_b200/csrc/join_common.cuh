@@ -52,9 +52,12 @@ static __global__ void bitmap_build_kernel(const int32_t* __restrict__ keys, con
 // A fact scan that tests every row's key against a dimension bitmap makes one scattered
 // 4-byte load per row; from global memory those are bound by L1/L2 transaction rates (one
 // sector each), from shared memory by bank conflicts (a few cycles per warp). The filter is
-// the exact bitmap when keys 0..key_max fit kSmemFilterBits bits, else a hashed bitmap of
-// kSmemFilterBits bits (key -> one bit; a key passes when its bit is set) whose hits the
-// caller confirms with the exact bitmap in global memory.
+// the exact bitmap when keys 0..key_max fit kSmemFilterBits bits, else a blocked Bloom filter
+// of kSmemFilterWords words: a key maps to one word and three bit positions in it and passes
+// when all three are set (one shared-memory load per test; with ~110K keys, the Q9 parts
+// that pass at 2M parts, about 1% of the other keys pass too). Its hits are either confirmed
+// by the caller with the exact bitmap in global memory, or, where a later step drops a false
+// positive by itself, left unconfirmed.
 constexpr uint32_t kSmemFilterWords = 51200;   // 200 KB of shared memory
 constexpr uint32_t kSmemFilterBits = kSmemFilterWords * 32;
 
@@ -65,11 +68,24 @@ __host__ __device__ inline bool smem_filter_exact(int32_t key_max) {
 __host__ __device__ inline uint32_t smem_filter_words(int32_t key_max) {
   return smem_filter_exact(key_max) ? ((uint32_t)key_max >> 5) + 1 : kSmemFilterWords;
 }
-__device__ __forceinline__ uint32_t smem_filter_slot(int32_t key) {
-  return __umulhi((uint32_t)key * 0x9E3779B1u, kSmemFilterBits);   // multiplicative hash onto [0, bits)
+// The Bloom form's 32-bit mix of a key: the MurmurHash3 finaliser (fmix32). Its high bits
+// pick the word (multiplied onto [0, kSmemFilterWords)), three 5-bit fields of its low 15 bits
+// the bit positions.
+__device__ __forceinline__ uint32_t smem_filter_mix(int32_t key) {
+  uint32_t h = (uint32_t)key;
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+__device__ __forceinline__ uint32_t smem_filter_word(uint32_t h) { return __umulhi(h, kSmemFilterWords); }
+__device__ __forceinline__ uint32_t smem_filter_bits(uint32_t h) {
+  return (1u << (h & 31u)) | (1u << ((h >> 5) & 31u)) | (1u << ((h >> 10) & 31u));
 }
 
-// Hashed filter of an exact bitmap of `words` words: every set key sets its hashed bit.
+// Bloom filter of an exact bitmap of `words` words: every set key sets its three bits.
 // `filt` holds kSmemFilterWords zeroed words.
 static __global__ void hashed_filter_kernel(const uint32_t* __restrict__ bits, uint32_t words, uint32_t* filt) {
   for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
@@ -77,8 +93,8 @@ static __global__ void hashed_filter_kernel(const uint32_t* __restrict__ bits, u
     while (x) {
       const uint32_t b = __ffs(x) - 1;
       x &= x - 1;
-      const uint32_t slot = smem_filter_slot((int32_t)(w * 32 + b));
-      atomicOr(filt + (slot >> 5), 1u << (slot & 31u));
+      const uint32_t h = smem_filter_mix((int32_t)(w * 32 + b));
+      atomicOr(filt + smem_filter_word(h), smem_filter_bits(h));
     }
   }
 }
@@ -98,19 +114,27 @@ __device__ __forceinline__ void smem_filter_load(const uint32_t* __restrict__ sr
 }
 
 // Filter of N keys (ok[j]: key j is in [0, key_max]) -> bit j set where key j passes: the
-// shared-memory tests first, then (hashed filter) every confirming load of `bits` issued
-// before any is used, so a thread waits for one memory latency, not N.
-template <int N>
+// shared-memory tests first, then (Bloom form, CONFIRM) every confirming load of `bits`
+// issued before any is used, so a thread waits for one memory latency, not N.
+template <int N, bool CONFIRM = true>
 __device__ __forceinline__ uint32_t smem_filter_mask(const uint32_t* sfilt, bool exact, const uint32_t* bits,
                                                      const int32_t (&key)[N], uint32_t ok) {
   uint32_t hit = 0;
+  if (exact) {
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      // a key outside [0, key_max] reads bit 0 and is masked off (its index would be out of range)
+      const uint32_t b = ((ok >> j) & 1u) ? (uint32_t)key[j] : 0u;
+      hit |= ((ok >> j) & (sfilt[b >> 5] >> (b & 31u)) & 1u) << j;
+    }
+    return hit;
+  }
 #pragma unroll
   for (int j = 0; j < N; j++) {
-    // a key outside [0, key_max] reads bit 0 and is masked off (its index would be out of range)
-    const uint32_t b = ((ok >> j) & 1u) ? (exact ? (uint32_t)key[j] : smem_filter_slot(key[j])) : 0u;
-    hit |= ((ok >> j) & (sfilt[b >> 5] >> (b & 31u)) & 1u) << j;
+    const uint32_t h = smem_filter_mix(key[j]), m = smem_filter_bits(h);
+    hit |= (uint32_t)(((ok >> j) & 1u) && (sfilt[smem_filter_word(h)] & m) == m) << j;
   }
-  if (exact || !hit) return hit;
+  if (!CONFIRM || !hit) return hit;
   uint32_t w[N];
 #pragma unroll
   for (int j = 0; j < N; j++) w[j] = ((hit >> j) & 1u) ? __ldg(bits + ((uint32_t)key[j] >> 5)) : 0u;

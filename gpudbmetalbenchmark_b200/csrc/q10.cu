@@ -10,9 +10,8 @@
 //     atomicOr per distinct word of a warp) and write their customer into a direct map
 //     order key -> customer. The map is read only where the bit is set, so it is never
 //     cleared (at SF-10 it is 240 MB; the bitmap 7.5 MB).
-//  3. q10_probe_kernel: lineitem rows with flag 2 ('R'): the head of each run of equal order
-//     keys tests the bitmap (L2-resident) and reads the map once for the run, and every
-//     returned row adds ext_price * (100 - discount) to its customer's int64 revenue
+//  3. q10_probe_kernel: lineitem rows with flag 2 ('R') test the bitmap (L2-resident),
+//     read the map, and add ext_price * (100 - discount) to their customer's int64 revenue
 //     (ext/discount loaded only for those rows).
 //  4. q10_hist_kernel + q10_select_kernel: the top-k of the per-customer revenue array by the
 //     revenue-histogram select of the Q3 top-k (q3.h): a log-scale histogram, the bin that
@@ -55,10 +54,8 @@ __global__ void __launch_bounds__(kThreads) q10_orders_kernel(const int32_t* __r
   }
 }
 
-// Rows of one order are adjacent: per 32-row group only the head of each run of equal keys
-// that holds a returned row looks the order up (bitmap, map, customer bitmap), and the run's
-// rows take its customer by a shuffle. The lookups of the kRows groups of a thread go in
-// phases, so their loads are in flight together.
+// The bitmap words of a thread's kRows rows are loaded in one phase and the map entries of the
+// rows whose bit is set in the next, so the loads of each phase are in flight together.
 __global__ void __launch_bounds__(kThreads) q10_probe_kernel(const int32_t* __restrict__ lkey,
                                                              const uint8_t* __restrict__ lflag,
                                                              const int64_t* __restrict__ lext,
@@ -67,45 +64,27 @@ __global__ void __launch_bounds__(kThreads) q10_probe_kernel(const int32_t* __re
                                                              const int32_t* __restrict__ map, int32_t cust_max,
                                                              const uint32_t* __restrict__ custbm,
                                                              unsigned long long* rev) {
-  const int lane = threadIdx.x & 31;
   const uint64_t step = (uint64_t)gridDim.x * kThreads * kRows;
-  for (uint64_t b = (uint64_t)blockIdx.x * kThreads * kRows; b < n; b += step) {   // whole warps
+  for (uint64_t b = (uint64_t)blockIdx.x * kThreads * kRows; b < n; b += step) {
     int32_t k[kRows];
-    uint32_t ret = 0, want = 0;
+    bool want[kRows];
 #pragma unroll
     for (int j = 0; j < kRows; j++) {
       const uint64_t i = b + (uint64_t)j * kThreads + threadIdx.x;
       const bool in = i < n;
-      ret |= (uint32_t)(in && ld_stream(lflag + i) == 2u) << j;
+      const uint32_t f = in ? ld_stream(lflag + i) : 0u;
       k[j] = in ? ld_stream(lkey + i) : -1;
-    }
-    int head_lane[kRows];
-#pragma unroll
-    for (int j = 0; j < kRows; j++) {
-      const int32_t prev = __shfl_up_sync(FULL_MASK, k[j], 1);
-      const bool head = lane == 0 || k[j] != prev;
-      const uint32_t heads = __ballot_sync(FULL_MASK, head);
-      const uint32_t retm = __ballot_sync(FULL_MASK, (ret >> j) & 1u);
-      head_lane[j] = 31 - __clz(heads & lanemask_le());
-      const uint32_t later = heads & lanemask_gt();
-      const uint32_t upto = later ? (1u << (__ffs(later) - 1)) - 1u : 0xFFFFFFFFu;
-      if (head && (retm & upto & ~((1u << lane) - 1u)) && k[j] >= 0 && k[j] <= order_max) want |= 1u << j;
+      want[j] = f == 2u && k[j] >= 0 && k[j] <= order_max;
     }
     uint32_t w[kRows];
 #pragma unroll
-    for (int j = 0; j < kRows; j++) w[j] = (want >> j & 1u) ? __ldg(okbm + ((uint32_t)k[j] >> 5)) : 0u;
+    for (int j = 0; j < kRows; j++) w[j] = want[j] ? __ldg(okbm + ((uint32_t)k[j] >> 5)) : 0u;
     int32_t c[kRows];
 #pragma unroll
-    for (int j = 0; j < kRows; j++)
-      c[j] = ((want >> j & 1u) && (w[j] >> ((uint32_t)k[j] & 31u) & 1u)) ? __ldg(map + k[j]) : -1;
+    for (int j = 0; j < kRows; j++) c[j] = (w[j] >> ((uint32_t)k[j] & 31u) & 1u) ? __ldg(map + k[j]) : -1;
 #pragma unroll
     for (int j = 0; j < kRows; j++) {
-      if (c[j] >= 0 && (c[j] > cust_max || !bitmap_test(custbm, c[j]))) c[j] = -1;
-      c[j] = __shfl_sync(FULL_MASK, c[j], head_lane[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < kRows; j++) {
-      if (!((ret >> j) & 1u) || c[j] < 0) continue;
+      if (c[j] < 0 || c[j] > cust_max || !bitmap_test(custbm, c[j])) continue;
       const uint64_t i = b + (uint64_t)j * kThreads + threadIdx.x;
       atomicAdd(rev + c[j], (unsigned long long)(ld_stream(lext + i) * (int64_t)(100 - ld_stream(ldisc + i))));
     }

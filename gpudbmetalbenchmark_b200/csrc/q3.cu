@@ -24,8 +24,11 @@
 //  6. q3_hist_kernel: groups and a log-scale revenue histogram of the live table.
 //  7. q3_select_kernel: the slots in the histogram bins that can hold the top-k are
 //     appended, and the last block to finish ranks them.
-// Radix mode partitions both sides by key hash (radix.cuh; the fact filter runs inside the
-// first partitioning pass) and joins each partition in shared memory.
+// Radix mode partitions both sides by key hash (radix.cuh) and joins each partition in
+// shared memory. The kept orders also set a hashed key set (8 bits per orders row, no key
+// range needed), and the fact filter drops the rows whose order key misses it before they
+// are compacted and partitioned: a semi-join reduction, so only rows that may join (plus
+// about 1% false positives, which the partition join drops) are partitioned.
 #include <algorithm>
 #include <cstring>
 
@@ -59,7 +62,23 @@ struct FilterOut {
   int32_t* omap;
   uint32_t* okbm;
   int32_t key_max;
+  uint32_t* kset;       // radix mode: hashed set of the kept order keys (kset_mask + 1 words), or null
+  uint32_t kset_mask;
 };
+
+// The hashed key set of the radix mode: one bit per key hash in a power-of-two array of
+// words, sized from the orders row count (8 bits per row), so it needs no key range. A
+// fact row whose order key misses it cannot join; a hit may be a false positive (about
+// kept orders / (8 x orders rows)), which the partition join then drops.
+__device__ __forceinline__ uint32_t kset_hash(int32_t key) { return slot_hash64((uint64_t)(uint32_t)key); }
+__device__ __forceinline__ void kset_add(uint32_t* set, uint32_t mask, int32_t key) {
+  const uint32_t h = kset_hash(key);
+  atomicOr(set + ((h >> 5) & mask), 1u << (h & 31u));
+}
+__device__ __forceinline__ bool kset_test(const uint32_t* set, uint32_t mask, int32_t key) {
+  const uint32_t h = kset_hash(key);
+  return (__ldg(set + ((h >> 5) & mask)) >> (h & 31u)) & 1u;
+}
 
 template <int T, bool SMEM, bool DIRECT>
 __global__ void __launch_bounds__(T, SMEM ? 2 : 1) orders_filter_kernel(
@@ -118,6 +137,7 @@ __global__ void __launch_bounds__(T, SMEM ? 2 : 1) orders_filter_kernel(
         } else {
           out.key[pos] = key[j];
           out.date[pos] = date[j];
+          if (out.kset) kset_add(out.kset, out.kset_mask, key[j]);
         }
         pos++;
       }
@@ -153,7 +173,9 @@ int launch_orders_filter(Call& call, const gpudb_customer& cu, const gpudb_order
   return launch_orders_filter_as<256, false, DIRECT>(call, cu, od, p, bitmap, bitmap, 0, true, out, cnt);
 }
 
-FilterOut staging_out(int32_t* key, int32_t* date) { return FilterOut{key, date, nullptr, nullptr, nullptr, nullptr, 0}; }
+FilterOut staging_out(int32_t* key, int32_t* date, uint32_t* kset = nullptr, uint32_t kset_mask = 0) {
+  return FilterOut{key, date, nullptr, nullptr, nullptr, nullptr, 0, kset, kset_mask};
+}
 
 __global__ void table_clear_kernel(const uint32_t* count, uint32_t min_cap, uint32_t max_cap, int shift, uint32_t* cap_out,
                                    Q3Slot* ht, uint32_t* hits) {
@@ -481,45 +503,64 @@ __global__ void __launch_bounds__(kTopkThreads) q3_select_kernel(const Q3Slot* _
 }
 
 // ---- radix mode ----------------------------------------------------------------------
-// Fact rows with ship_date > cutoff, compacted to (order_key, ext*(100-disc)).
-__global__ void q3_fact_filter_kernel(const int32_t* __restrict__ lkey, const int32_t* __restrict__ lship,
-                                      const int64_t* __restrict__ lext, const int32_t* __restrict__ ldisc, uint64_t n,
-                                      int32_t ship_gt, int32_t* out_key, int64_t* out_val, uint32_t* count) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t end = (n + 31) & ~31ull;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
-    const bool take = i < n && ld_stream(lship + i) > ship_gt;
-    const uint32_t pos = warp_append(take, count);
-    if (take) {
-      out_key[pos] = lkey[i];
-      out_val[pos] = lext[i] * (int64_t)(100 - ldisc[i]);
+constexpr int kFactRows = 4;   // rows per thread per warp step of q3_fact_filter_kernel
+
+// Fact rows that may join: ship_date > ship_gt and the order key in the hashed key set of
+// the kept orders, compacted to (order_key, ext * (100 - disc)). A warp step covers 128 rows
+// (row j*32 + lane of the step for j < 4): ship dates and keys load together, then the key
+// set words of the rows whose date passes, then one append per warp for the step's rows and
+// ext/discount only for the rows kept.
+__global__ void __launch_bounds__(256) q3_fact_filter_kernel(const int32_t* __restrict__ lkey,
+                                                             const int32_t* __restrict__ lship,
+                                                             const int64_t* __restrict__ lext,
+                                                             const int32_t* __restrict__ ldisc, uint64_t n,
+                                                             int32_t ship_gt, const uint32_t* __restrict__ kset,
+                                                             uint32_t kset_mask, int32_t* __restrict__ out_key,
+                                                             int64_t* __restrict__ out_val, uint32_t* count) {
+  const int lane = threadIdx.x & 31;
+  constexpr uint64_t kWarpRows = 32 * kFactRows;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t b = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kWarpRows; b < n;
+       b += warps * kWarpRows) {   // whole warps: the append below needs every lane
+    int32_t k[kFactRows];
+    bool on[kFactRows];
+#pragma unroll
+    for (int j = 0; j < kFactRows; j++) {
+      const uint64_t i = b + (uint64_t)j * 32 + lane;
+      on[j] = i < n && ld_stream(lship + i) > ship_gt;
+      k[j] = i < n ? ld_stream(lkey + i) : 0;
+    }
+    uint32_t w[kFactRows];
+#pragma unroll
+    for (int j = 0; j < kFactRows; j++) {
+      const uint32_t h = kset_hash(k[j]);
+      w[j] = on[j] ? (__ldg(kset + ((h >> 5) & kset_mask)) >> (h & 31u)) & 1u : 0u;
+    }
+    uint32_t m[kFactRows], tot = 0;
+#pragma unroll
+    for (int j = 0; j < kFactRows; j++) {
+      m[j] = __ballot_sync(FULL_MASK, w[j] != 0u);
+      tot += __popc(m[j]);
+    }
+    if (tot == 0) continue;   // uniform across the warp
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, tot);
+    base = __shfl_sync(FULL_MASK, base, 0);
+#pragma unroll
+    for (int j = 0; j < kFactRows; j++) {
+      if (w[j]) {
+        const uint64_t i = b + (uint64_t)j * 32 + lane;
+        const uint32_t pos = base + __popc(m[j] & lanemask_lt());
+        out_key[pos] = k[j];
+        out_val[pos] = ld_stream(lext + i) * (int64_t)(100 - ld_stream(ldisc + i));
+      }
+      base += __popc(m[j]);
     }
   }
 }
 
 constexpr uint32_t kQ3PartCap = 4096;               // shared slots per partition table
 constexpr uint32_t kQ3PartChunk = kQ3PartCap / 2;   // build rows per chunk
-
-// Fact rows of a device-resident lineitem table for the radix mode: a row takes part when
-// ship_date > ship_gt; its payload is ext_price * (100 - discount). The first partitioning
-// pass reads the columns directly, so no filtered copy of the fact table is written.
-struct Q3FactSource {
-  const int32_t* okey;
-  const int32_t* ship;
-  const int64_t* ext;
-  const int32_t* disc;
-  uint64_t n;
-  int32_t ship_gt;
-  __device__ __forceinline__ uint64_t rows() const { return n; }
-  __device__ __forceinline__ bool key(uint64_t r, int32_t& k) const {
-    const int32_t s = __ldg(ship + r);
-    k = __ldg(okey + r);
-    return s > ship_gt;
-  }
-  __device__ __forceinline__ int64_t payload(uint64_t r) const {
-    return __ldcs(ext + r) * (int64_t)(100 - __ldcs(disc + r));
-  }
-};
 
 constexpr size_t q3_partition_smem() { return (size_t)kQ3PartCap * (8 + 4 + 4 + 4); }
 
@@ -616,12 +657,17 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
                  : ctx->radix_bits > 0 ? ctx->radix_bits
                                        : std::min(kRxPassBits, std::max(9, radix_bits_for(od.n_rows, 16384)));
   const uint64_t parts = 1ull << bits;
-  void *bitmap, *bstage, *fstage, *count, *bpart, *fpart, *offs, *cand;
+  // hashed set of the kept order keys: 8 bits per orders row, a power of two of words
+  uint64_t kwords = 32;
+  while (kwords < n_or / 4 && kwords < (1ull << 28)) kwords <<= 1;
+  const uint64_t n_or_a = (n_or + 31) / 32 * 32;   // 128-byte aligned column starts
+  void *bitmap, *bstage, *fstage, *count, *bpart, *fpart, *offs, *cand, *kset;
   int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);
-  if (!rc) rc = scratch(ctx, "q3r.build", n_or * 4 * 4 + 256, &bstage);          // key, date, tmp key, tmp date
+  if (!rc) rc = scratch(ctx, "q3r.kset", (size_t)kwords * 4, &kset);
+  if (!rc) rc = scratch(ctx, "q3r.build", n_or_a * 4 * 4 + 256, &bstage);        // key, date, tmp key, tmp date
   if (!rc) rc = scratch(ctx, "q3r.fact", n_li * 12 * 2 + 1024, &fstage);           // key, value, tmp
   if (!rc) rc = scratch(ctx, "q3.count", 256, &count);
-  if (!rc) rc = scratch(ctx, "q3r.bpart", n_or * 8 + 256, &bpart);
+  if (!rc) rc = scratch(ctx, "q3r.bpart", n_or_a * 8 + 256, &bpart);
   if (!rc) rc = scratch(ctx, "q3r.fpart", n_li * 12 + 1024, &fpart);
   if (!rc) rc = scratch(ctx, "q3r.offs", (2 * (parts + 1) + 64) * 4, &offs);
   const uint64_t dslots = std::max<uint64_t>(128, (n_or + 127) / 128 * 128);
@@ -633,20 +679,23 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   if (rc) return rc;
   uint32_t* cnt = static_cast<uint32_t*>(count);   // [0] orders, [1] fact rows, [2] groups, [3] top-k capacity
   GPUDB_CUDA(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
+  GPUDB_CUDA(ctx, cudaMemsetAsync(kset, 0, (size_t)kwords * 4, s));
   GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));
   GPUDB_CUDA(ctx, cudaMemsetAsync(tstate, 0, (size_t)kTopkStateWords * 4, s));
   const int sms = ctx->sm_count;
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
+  uint32_t* ks = static_cast<uint32_t*>(kset);
+  const uint32_t kmask = (uint32_t)(kwords - 1);
   int32_t* bkey = static_cast<int32_t*>(bstage);
-  int32_t* bdate = bkey + n_or;
-  int32_t* bkey_t = bdate + n_or;
-  int32_t* bdate_t = bkey_t + n_or;
+  int32_t* bdate = bkey + n_or_a;
+  int32_t* bkey_t = bdate + n_or_a;
+  int32_t* bdate_t = bkey_t + n_or_a;
   int32_t* fkey = static_cast<int32_t*>(fstage);
   int64_t* fval = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(fstage) + ((n_li * 4 + 255) / 256) * 256);
   int32_t* fkey_t = reinterpret_cast<int32_t*>(fval + n_li);
   int64_t* fval_t = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(static_cast<void*>(fkey_t)) + ((n_li * 4 + 255) / 256) * 256);
   int32_t* bk = static_cast<int32_t*>(bpart);
-  int32_t* bd = bk + n_or;
+  int32_t* bd = bk + n_or_a;
   int32_t* pk = static_cast<int32_t*>(fpart);
   int64_t* pv = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(fpart) + ((n_li * 4 + 255) / 256) * 256);
   uint32_t* boff = static_cast<uint32_t*>(offs);
@@ -654,23 +703,19 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   if (cu.n_rows)
     GPUDB_LAUNCH(call, bitmap_build_kernel, grid(cu.n_rows), 256, 0, cu.cust_key, cu.segment, p.segment, cu.n_rows,
                  cu.key_max, (uint32_t*)bitmap, call.status());
-  if ((rc = launch_orders_filter<false>(call, cu, od, p, (const uint32_t*)bitmap, staging_out(bkey, bdate), cnt))) return rc;
-  rc = radix_partition_run<int32_t>(call, bkey, bdate, n_or, cnt, bits, bk, bd, boff, bkey_t, bdate_t);
+  if ((rc = launch_orders_filter<false>(call, cu, od, p, (const uint32_t*)bitmap, staging_out(bkey, bdate, ks, kmask), cnt)))
+    return rc;
+  rc = radix_partition_run<int32_t, false>(call, bkey, bdate, n_or, cnt, bits, bk, bd, boff, bkey_t, bdate_t);
   if (rc) return rc;
-  if (li->location == GPUDB_MEM_DEVICE) {
-    // the filter runs inside the first partitioning pass: no filtered copy of the fact rows
-    const Q3FactSource src{li->order_key, li->ship_date, li->ext_price, li->discount, li->n_rows, p.ship_date_gt};
-    rc = rx_partition<Q3FactSource, int64_t, true>(call, src, n_li, bits, pk, pv, poff, fkey_t, fval_t);
-  } else {
-    const uint32_t mask = LI_ORDER | LI_SHIP | LI_EXT | LI_DISC;
-    rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) {
-      if (c.n_rows == 0) return (int)GPUDB_OK;
-      GPUDB_LAUNCH(call, q3_fact_filter_kernel, grid(c.n_rows), 256, 0, c.order_key, c.ship_date, c.ext_price,
-                   c.discount, c.n_rows, p.ship_date_gt, fkey, fval, cnt + 1);
-      return (int)GPUDB_OK;
-    });
-    if (!rc) rc = radix_partition_run<int64_t>(call, fkey, fval, n_li, cnt + 1, bits, pk, pv, poff, fkey_t, fval_t);
-  }
+  // fact rows that may join, compacted (a few percent of the table), then partitioned
+  const int fgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n_li + 1023) / 1024, (uint64_t)sms * 8));
+  rc = stream_lineitem(call, li, LI_ORDER | LI_SHIP | LI_EXT | LI_DISC, 0, [&](const gpudb_lineitem& c) {
+    if (c.n_rows == 0) return (int)GPUDB_OK;
+    GPUDB_LAUNCH(call, q3_fact_filter_kernel, fgrid, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount,
+                 c.n_rows, p.ship_date_gt, (const uint32_t*)ks, kmask, fkey, fval, cnt + 1);
+    return (int)GPUDB_OK;
+  });
+  if (!rc) rc = radix_partition_run<int64_t, false>(call, fkey, fval, n_li, cnt + 1, bits, pk, pv, poff, fkey_t, fval_t);
   if (rc) return rc;
   u128* cbuf = static_cast<u128*>(cand);
   unsigned long long* groups = reinterpret_cast<unsigned long long*>(result);

@@ -11,7 +11,8 @@
 //    atomicCAS; the table is sized on the device from the qualifying count;
 //  - the fact table goes through in pieces of at most 64M rows, two kernels each:
 //    li_filter_kernel streams part_key (128-bit loads), tests each part against a filter held
-//    in shared memory (the exact bitmap, or a hashed one confirmed in the global bitmap) and
+//    in shared memory (the exact bitmap, or a blocked Bloom filter whose ~1% false positives
+//    the resolve drops, since their (part, supp) is not in the partsupp table) and
 //    writes a bitmask of the rows that pass (~5.5%); q9_resolve_kernel expands the bitmask a
 //    warp at a time (one set bit per lane) and gathers each row's six columns and its
 //    lookups together (late materialisation, all resident threads' misses in flight);
@@ -174,9 +175,9 @@ constexpr int kLiQuads = 4;                  // 16-byte loads per thread per blo
 constexpr int kLiRows = 4 * kLiQuads;        // fact rows per thread per block step of li_filter_kernel
 constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve pair (bounds the pair buffer)
 
-// Fact rows whose part passes the bitmap -> bit (r & 31) of passbits[r >> 5] (rows of the
+// Fact rows whose part passes the filter -> bit (r & 31) of passbits[r >> 5] (rows of the
 // piece). The part filter sits in shared memory (smem_filter_*): the exact bitmap, or a
-// hashed one whose hits are confirmed in `bits`. A block step covers kLiThreads * 16 rows;
+// blocked Bloom filter whose hits are not confirmed here. A block step covers kLiThreads * 16 rows;
 // load q of thread t is the 16-byte quad q * kLiThreads + t of the step (coalesced), and the
 // next step's quads load while this one is tested. The four rows of a quad are four bits of
 // one word that eight lanes share: an OR across the eight lanes and one store per word, so
@@ -223,7 +224,9 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
     uint32_t ok = 0;
 #pragma unroll
     for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
-    const uint32_t take = smem_filter_mask(sfilt, exact, bits, p, ok);
+    // Bloom-form hits go unconfirmed: a false positive's (part, supp) is not in the partsupp
+    // table, which holds only parts that pass, so the resolve drops it
+    const uint32_t take = smem_filter_mask<kLiRows, false>(sfilt, exact, bits, p, ok);
 #pragma unroll
     for (int q = 0; q < kLiQuads; q++) {
       // rows 4*lane .. 4*lane+3 of this quad's 128 rows: bits 4*(lane & 7) .. of word lane / 8

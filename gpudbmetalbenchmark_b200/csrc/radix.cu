@@ -83,34 +83,64 @@ __global__ void __launch_bounds__(kPJThreads) partition_pairs_kernel(
   }
 }
 
-// Semi-join count: probe rows with at least one match. Partitions whose build side needs
-// more than one chunk mark matches in `flags` (one byte per partitioned probe row) and
-// count them after the last chunk.
-__global__ void __launch_bounds__(kPJThreads) partition_count_kernel(
+// Semi-join count: probe rows with at least one match. One 1024-thread block per partition
+// with a kPCCap-slot shared table (128 KB), so a partition of up to kPCChunk build keys is one
+// chunk and one 10-bit pass per side covers 15M build rows. Partitions whose build side needs
+// more than one chunk mark matches in `flags` (one byte per partitioned probe row) and count
+// them after the last chunk. Each thread keeps kPCRows probe keys in flight.
+constexpr int kPCThreads = 1024;
+constexpr uint32_t kPCCap = 32768;
+constexpr uint32_t kPCChunk = kPCCap / 2;
+constexpr uint64_t kCountRowsPerPartition = 15360;   // average build keys per partition (<= kPCChunk with margin)
+constexpr int kPCRows = 4;
+
+__global__ void __launch_bounds__(kPCThreads) partition_count_kernel(
     const int32_t* __restrict__ bk, const uint32_t* __restrict__ boff, const int32_t* __restrict__ pk,
     const uint32_t* __restrict__ poff, uint8_t* flags, unsigned long long* count) {
-  __shared__ int32_t hkey[kPJCap];
-  const uint32_t part = blockIdx.x;
+  extern __shared__ __align__(16) int32_t pc_key[];
+  const uint32_t part = blockIdx.x, mask = kPCCap - 1;
   const uint32_t b0 = boff[part], b1 = boff[part + 1], p0 = poff[part], p1 = poff[part + 1];
-  const bool multi = (b1 - b0) > kChunk;
+  const bool multi = (b1 - b0) > kPCChunk;
   uint32_t c = 0;
   if (multi)
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kPJThreads) flags[i] = 0;
-  for (uint32_t c0 = b0; c0 < b1; c0 += kChunk) {
-    pj_build(bk, nullptr, c0, min(c0 + kChunk, b1), hkey, nullptr);
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kPJThreads) {
-      const int32_t k = pk[i];
-      bool hit = false;
-      if (k != kEmptyKey)
-        for (uint32_t s = pj_slot(k), t = 0; t < kPJCap && hkey[s] != kEmptyKey; t++, s = (s + 1) & (kPJCap - 1))
-          if (hkey[s] == k) { hit = true; break; }
-      if (multi) { if (hit) flags[i] = 1; }
-      else c += hit;
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kPCThreads) flags[i] = 0;
+  for (uint32_t c0 = b0; c0 < b1; c0 += kPCChunk) {
+    const uint32_t c1 = min(c0 + kPCChunk, b1);
+    for (uint32_t i = threadIdx.x; i < kPCCap / 4; i += kPCThreads)
+      reinterpret_cast<int4*>(pc_key)[i] = make_int4(kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey);
+    __syncthreads();
+    // duplicates take their own slots; a chunk fills at most half the table
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += kPCThreads) {
+      const int32_t k = __ldg(bk + i);
+      uint32_t s = key_slot(k, mask);
+      for (uint32_t t = 0; t < kPCCap; t++, s = (s + 1) & mask)
+        if (atomicCAS(&pc_key[s], kEmptyKey, k) == kEmptyKey) break;
+    }
+    __syncthreads();
+    for (uint32_t i0 = p0 + threadIdx.x; i0 < p1; i0 += kPCRows * kPCThreads) {
+      int32_t k[kPCRows];
+#pragma unroll
+      for (int u = 0; u < kPCRows; u++) {
+        const uint32_t i = i0 + u * kPCThreads;
+        k[u] = i < p1 ? __ldcs(pk + i) : kEmptyKey;
+      }
+#pragma unroll
+      for (int u = 0; u < kPCRows; u++) {
+        bool hit = false;
+        if (k[u] != kEmptyKey)
+          for (uint32_t s = key_slot(k[u], mask), t = 0; t < kPCCap; t++, s = (s + 1) & mask) {
+            const int32_t h = pc_key[s];
+            if (h == k[u]) { hit = true; break; }
+            if (h == kEmptyKey) break;
+          }
+        if (multi) { if (hit) flags[i0 + u * kPCThreads] = 1; }
+        else c += hit;
+      }
     }
     __syncthreads();
   }
   if (multi)
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kPJThreads) c += flags[i];
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += kPCThreads) c += flags[i];
   c = __reduce_add_sync(FULL_MASK, c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
@@ -129,11 +159,11 @@ int partition_both(Call& call, const int32_t* build, uint64_t nb, const int32_t*
   const size_t nmax = std::max<uint64_t>(std::max(nb, np), 1);
   const int k = rows ? 2 : 1;
   void *keys, *offs;
-  int rc = scratch(ctx, "rjoin.keys", (size_t)k * (nb + np + nmax + 48) * sizeof(int32_t), &keys);
+  int rc = scratch(ctx, "rjoin.keys", (size_t)k * (nb + np + nmax + 3 * 48) * sizeof(int32_t), &keys);
   if (!rc) rc = scratch(ctx, "rjoin.offs", (2 * (parts + 1) + 64) * sizeof(uint32_t), &offs);
   if (rc) return rc;
   int32_t* p = static_cast<int32_t*>(keys);
-  auto take = [&p](uint64_t n) { int32_t* q = p; p += n + 16; return q; };
+  auto take = [&p](uint64_t n) { int32_t* q = p; p += (n + 16 + 31) / 32 * 32; return q; };   // 128-byte aligned
   s->bk = take(nb);
   s->pk = take(np);
   int32_t* ktmp = take(nmax);
@@ -143,8 +173,8 @@ int partition_both(Call& call, const int32_t* build, uint64_t nb, const int32_t*
   s->boff = static_cast<uint32_t*>(offs);
   s->poff = s->boff + parts + 16;
   if (rows) {
-    rc = radix_partition_run<int32_t>(call, build, nullptr, nb, nullptr, bits, s->bk, s->brow, s->boff, ktmp, ptmp);
-    if (!rc) rc = radix_partition_run<int32_t>(call, probe, nullptr, np, nullptr, bits, s->pk, s->prow, s->poff, ktmp, ptmp);
+    rc = radix_partition_run<int32_t, false>(call, build, nullptr, nb, nullptr, bits, s->bk, s->brow, s->boff, ktmp, ptmp);
+    if (!rc) rc = radix_partition_run<int32_t, false>(call, probe, nullptr, np, nullptr, bits, s->pk, s->prow, s->poff, ktmp, ptmp);
   } else {
     rc = radix_partition_keys(call, build, nb, bits, s->bk, s->boff, ktmp);
     if (!rc) rc = radix_partition_keys(call, probe, np, bits, s->pk, s->poff, ktmp);
@@ -157,14 +187,16 @@ int partition_both(Call& call, const int32_t* build, uint64_t nb, const int32_t*
 int radix_join_count(Call& call, const int32_t* build_keys, uint64_t n_build, const int32_t* probe_keys, uint64_t n_probe,
                      unsigned long long* count) {
   if (n_build == 0 || n_probe == 0) return GPUDB_OK;
-  const int bits = radix_bits_for(n_build, kRowsPerPartition);
+  const int bits = radix_bits_for(n_build, kCountRowsPerPartition);
   Sides s;
   int rc = partition_both(call, build_keys, n_build, probe_keys, n_probe, bits, false, &s);
   if (rc) return rc;
   void* flags = nullptr;
   rc = scratch(call.ctx(), "rjoin.flags", n_probe + 16, &flags);
   if (rc) return rc;
-  GPUDB_LAUNCH(call, partition_count_kernel, 1u << bits, kPJThreads, 0, (const int32_t*)s.bk, (const uint32_t*)s.boff,
+  const size_t smem = kPCCap * sizeof(int32_t);
+  GPUDB_CUDA(call.ctx(), kernel_smem(call.ctx(), (const void*)partition_count_kernel, smem));
+  GPUDB_LAUNCH(call, partition_count_kernel, 1u << bits, kPCThreads, smem, (const int32_t*)s.bk, (const uint32_t*)s.boff,
                (const int32_t*)s.pk, (const uint32_t*)s.poff, (uint8_t*)flags, count);
   return GPUDB_OK;
 }
@@ -184,11 +216,11 @@ extern "C" int gpudb_radix_partition(gpudb_ctx* ctx, const int32_t* keys, const 
   int rc = call.begin(16);
   if (rc) return rc;
   void* tmp = nullptr;
-  rc = scratch(ctx, "radix.tmp", (2 * std::max<uint64_t>(n, 1) + 32) * sizeof(int32_t), &tmp);
+  rc = scratch(ctx, "radix.tmp", (2 * std::max<uint64_t>(n, 1) + 96) * sizeof(int32_t), &tmp);
   if (rc) return rc;
   int32_t* ktmp = static_cast<int32_t*>(tmp);
-  int32_t* ptmp = ktmp + std::max<uint64_t>(n, 1) + 16;
-  rc = radix_partition_run<int32_t>(call, keys, payload, n, nullptr, bits, keys_out, payload_out, offsets, ktmp, ptmp);
+  int32_t* ptmp = ktmp + (std::max<uint64_t>(n, 1) + 16 + 31) / 32 * 32;   // 128-byte aligned
+  rc = radix_partition_run<int32_t, true>(call, keys, payload, n, nullptr, bits, keys_out, payload_out, offsets, ktmp, ptmp);
   if (rc) return rc;
   return call.finish(16, [](const uint8_t*) { return GPUDB_OK; });
 }

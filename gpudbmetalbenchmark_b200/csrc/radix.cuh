@@ -12,8 +12,9 @@
 //                     blocks per super-tile, so every SM streams) into hist[digit][G], and
 //                     in the first pass also the rows per final partition;
 //   exclusive_scan    over hist (digit-major): where each (digit, super-tile) run starts;
-//   rx_scatter_kernel one block per super-tile walks its sub-tiles (2048 rows by default) in
-//                     order. Each warp ranks its own contiguous rows by digit (__match_any_sync
+//   rx_scatter_kernel one block per super-tile walks its sub-tiles (4096 rows by default) in
+//                     order, the next two in flight as bulk copies (TMA) into a shared-memory
+//                     ring. Each warp ranks its own contiguous rows by digit (__match_any_sync
 //                     and per-warp counters, no atomics), one block-wide scan turns the
 //                     (digit, warp) counts into staged positions, the sub-tile is staged
 //                     digit-sorted in shared memory and written out run by run from
@@ -29,6 +30,7 @@
 #include "engine.h"
 #include "join_common.cuh"
 #include "scan.cuh"
+#include "tma.cuh"
 
 namespace gpudb {
 
@@ -40,6 +42,8 @@ constexpr int kRxHistSplit = 4;                         // histogram blocks per 
 
 // Plain columns: keys, and a payload column or (null) the row number. Rows [0, n) with
 // n = *n_dev when given (a count left on the device by an earlier kernel), capped at n_max.
+// Whole sub-tiles can also come through the scatter's bulk-copy ring: stage_bytes() per
+// sub-tile (keys, then payloads), issue() posts the copies, staged() reads one row back.
 template <class P>
 struct ColumnSource {
   const int32_t* keys;
@@ -54,6 +58,26 @@ struct ColumnSource {
     return true;
   }
   __device__ __forceinline__ P payload(uint64_t r) const { return pay ? __ldcs(pay + r) : (P)r; }
+  template <bool PAY>
+  __host__ __device__ static constexpr uint32_t stage_bytes(uint32_t tile) { return tile * (4u + (PAY ? (uint32_t)sizeof(P) : 0u)); }
+  // both columns start on 16 bytes, so every whole sub-tile does (sub-tiles start at
+  // multiples of their row count, a multiple of 4)
+  __device__ __forceinline__ bool bulk_ok() const {
+    return ((uintptr_t)keys & 15u) == 0 && ((uintptr_t)pay & 15u) == 0;
+  }
+  template <bool PAY, uint32_t TILE>
+  __device__ __forceinline__ void issue(uint64_t r0, unsigned char* st, uint64_t* bar) const {
+    const bool pc = PAY && pay != nullptr;
+    mbar_arrive_expect_tx(bar, TILE * 4u + (pc ? TILE * (uint32_t)sizeof(P) : 0u));
+    bulk_copy_g2s(st, keys + r0, TILE * 4u, bar);
+    if (pc) bulk_copy_g2s(st + TILE * 4u, pay + r0, TILE * (uint32_t)sizeof(P), bar);
+  }
+  template <bool PAY, uint32_t TILE>
+  __device__ __forceinline__ bool staged(const unsigned char* st, uint32_t i, uint64_t r, int32_t& k, P& p) const {
+    k = reinterpret_cast<const int32_t*>(st)[i];
+    if (PAY) p = pay ? reinterpret_cast<const P*>(st + TILE * 4u)[i] : (P)r;
+    return true;
+  }
 };
 
 // Rows per super-tile for n rows over G super-tiles: whole sub-tiles of `tile` rows, at least
@@ -142,26 +166,44 @@ __global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G
       if (fcnt[i]) atomicAdd(&full[i], fcnt[i]);
 }
 
-template <class P, bool PAY, int T, int I>
+// Shared memory of one scatter block: STG staged input sub-tiles (the bulk-copy ring), the
+// digit-sorted staging of one sub-tile, the digit counters (stable: per warp, u16; unstable:
+// per block and the digit starts, u32) and the per-digit output cursors.
+template <class Src, class P, bool PAY, int T, int I, int STG, bool STABLE>
 __host__ __device__ constexpr size_t rx_scatter_smem(uint32_t F) {
-  return (PAY ? sizeof(P) * T * I : 0) + (sizeof(int32_t) + sizeof(uint16_t)) * T * I +
-         sizeof(uint16_t) * (T / 32) * F + sizeof(uint32_t) * F;
+  return (size_t)STG * Src::template stage_bytes<PAY>(T * I) + (PAY ? sizeof(P) * T * I : 0) +
+         (sizeof(int32_t) + sizeof(uint16_t)) * T * I +
+         (STABLE ? sizeof(uint16_t) * (T / 32) * F : 2 * sizeof(uint32_t) * F) + sizeof(uint32_t) * F;
 }
 
 // One block of T threads per super-tile (see the file comment), sub-tiles of T * I rows.
-// offs: exclusive scan of hist.
-template <class Src, class P, bool PAY, int T, int I>
+// offs: exclusive scan of hist. With STG > 0 and 16-byte aligned columns, thread 0 keeps the
+// next STG whole sub-tiles in flight as bulk copies (TMA) into a shared-memory ring while the
+// block ranks and writes the current one; the last, partial sub-tile is loaded directly. A
+// ring wait is bounded: when it runs out the block sets ST_TIMEOUT in `status`, lets its
+// copies land and leaves.
+// STABLE ranks each warp's rows in row order (per-warp digit counters and a block scan over
+// warps x digits). Otherwise a row's rank inside its sub-tile is the arrival order of one
+// shared-memory atomic on its digit's counter, and only F counters are scanned: super-tiles
+// and sub-tiles still go out in input order, the rows of one sub-tile and digit in any order.
+template <class Src, class P, bool PAY, int T, int I, int STG, bool STABLE>
 __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int shift, int dbits,
                                                        const uint32_t* __restrict__ offs, int32_t* __restrict__ kout,
-                                                       P* __restrict__ pout) {
+                                                       P* __restrict__ pout, uint32_t* status) {
   constexpr int W = T / 32, TILE = T * I, WROWS = TILE / W;
-  extern __shared__ __align__(16) unsigned char rx_smem[];
+  constexpr int NS = STG > 0 ? STG : 1;   // ring stages (1 when there is no ring)
+  constexpr uint32_t SB = STG ? Src::template stage_bytes<PAY>(TILE) : 0u;
+  extern __shared__ __align__(128) unsigned char rx_smem[];
+  __shared__ __align__(8) uint64_t full[NS];
   const uint32_t F = 1u << dbits, dmask = F - 1;
-  P* spay = reinterpret_cast<P*>(rx_smem);
-  int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + (PAY ? sizeof(P) * TILE : 0));
+  unsigned char* ring = rx_smem;
+  P* spay = reinterpret_cast<P*>(rx_smem + STG * SB);
+  int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + STG * SB + (PAY ? sizeof(P) * TILE : 0));
   uint16_t* sdig = reinterpret_cast<uint16_t*>(skey + TILE);            // digit of each staged row
-  uint16_t* wcnt = sdig + TILE;                                         // [warp][digit]
-  uint32_t* cur = reinterpret_cast<uint32_t*>(wcnt + W * F);            // next output row per digit
+  uint16_t* wcnt = sdig + TILE;                                         // stable: [warp][digit]
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(wcnt);                    // unstable: [digit] counts
+  uint32_t* start = cnt + F;                                            // unstable: [digit] staged starts
+  uint32_t* cur = STABLE ? reinterpret_cast<uint32_t*>(wcnt + W * F) : start + F;   // next output row per digit
   __shared__ uint32_t wt[W];
   __shared__ uint32_t s_total;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -170,43 +212,88 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
   const uint64_t g0 = (uint64_t)blockIdx.x * super_rows;
   if (g0 >= n) return;   // uniform across the block
   const uint64_t g1 = min(g0 + super_rows, n);
+  // whole sub-tiles that come through the ring
+  const uint64_t nring = (STG > 0 && src.bulk_ok()) ? (g1 - g0) / TILE : 0;
+  if (STG > 0 && threadIdx.x == 0 && nring) {
+    for (int q = 0; q < NS; q++) mbar_init(&full[q], 1);
+    mbar_fence_init();
+  }
   for (uint32_t d = threadIdx.x; d < F; d += T) cur[d] = offs[(size_t)d * G + blockIdx.x];
-  for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
+  if (STABLE)
+    for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
+  else
+    for (uint32_t d = threadIdx.x; d < F; d += T) cnt[d] = 0;
   __syncthreads();
+  if (STG > 0 && threadIdx.x == 0)
+    for (uint64_t q = 0; q < nring && q < (uint64_t)NS; q++)
+      src.template issue<PAY, TILE>(g0 + q * TILE, ring + (q % NS) * SB, &full[q % NS]);
   uint16_t* mine = wcnt + warp * F;
   const uint32_t dpt = (F + T - 1) / T;   // digits per thread in the scan
-  for (uint64_t t0 = g0; t0 < g1; t0 += TILE) {
+  uint64_t k = 0;
+  for (uint64_t t0 = g0; t0 < g1; t0 += TILE, k++) {
     int32_t key[I];
     P pay[I];
-    uint32_t dr[I];   // digit << 16 | rank among the warp's rows of that digit; ~0u: no row
-    const uint64_t wb = t0 + (uint64_t)warp * WROWS + lane;
-#pragma unroll
-    for (int j = 0; j < I; j++) {
-      const uint64_t r = wb + (uint64_t)j * 32;
-      const bool v = r < g1 && src.key(r, key[j]);
-      dr[j] = v ? 0u : ~0u;
-      if (PAY && v) pay[j] = src.payload(r);
-    }
-    // rank inside the warp, 32 rows at a time in row order: the first lane of each digit
-    // reads and advances the warp's counter for it
-#pragma unroll
-    for (int j = 0; j < I; j++) {
-      const bool v = dr[j] == 0u;
-      const uint32_t d = v ? rx_digit(key[j], shift, dmask) : 0x10000u + lane;
-      const uint32_t peers = __match_any_sync(FULL_MASK, d);
-      const int leader = __ffs(peers) - 1;
-      uint32_t base = (v && lane == leader) ? (uint32_t)mine[d] : 0u;
-      base = __shfl_sync(FULL_MASK, base, leader);
-      if (v) {
-        if (lane == leader) mine[d] = (uint16_t)(base + __popc(peers));
-        dr[j] = (d << 16) | (base + __popc(peers & lanemask_lt()));
+    uint32_t dr[I];   // digit << 16 | rank (stable: among the warp's rows of that digit); ~0u: no row
+    const uint32_t wo = (uint32_t)warp * WROWS + lane;   // this thread's first row of the sub-tile
+    if (STG > 0 && k < nring) {
+      const int q = (int)(k % NS);
+      const bool ok = mbar_wait(&full[q], (uint32_t)((k / NS) & 1), kMbarPollLimit);
+      if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+          set_status(status, ST_TIMEOUT);
+          for (uint64_t x = k; x < nring && x < k + NS; x++)
+            mbar_wait(&full[x % NS], (uint32_t)((x / NS) & 1), kMbarPollLimit);
+        }
+        return;
       }
-      __syncwarp();
+      const unsigned char* st = ring + q * SB;
+#pragma unroll
+      for (int j = 0; j < I; j++) {
+        const uint32_t i = wo + (uint32_t)j * 32;
+        const bool v = src.template staged<PAY, TILE>(st, i, t0 + i, key[j], pay[j]);
+        dr[j] = v ? 0u : ~0u;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < I; j++) {
+        const uint64_t r = t0 + wo + (uint64_t)j * 32;
+        const bool v = r < g1 && src.key(r, key[j]);
+        dr[j] = v ? 0u : ~0u;
+        if (PAY && v) pay[j] = src.payload(r);
+      }
+    }
+    if (STABLE) {
+      // rank inside the warp, 32 rows at a time in row order: the first lane of each digit
+      // reads and advances the warp's counter for it
+#pragma unroll
+      for (int j = 0; j < I; j++) {
+        const bool v = dr[j] == 0u;
+        const uint32_t d = v ? rx_digit(key[j], shift, dmask) : 0x10000u + lane;
+        const uint32_t peers = __match_any_sync(FULL_MASK, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = (v && lane == leader) ? (uint32_t)mine[d] : 0u;
+        base = __shfl_sync(FULL_MASK, base, leader);
+        if (v) {
+          if (lane == leader) mine[d] = (uint16_t)(base + __popc(peers));
+          dr[j] = (d << 16) | (base + __popc(peers & lanemask_lt()));
+        }
+        __syncwarp();
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < I; j++)
+        if (dr[j] == 0u) {
+          const uint32_t d = rx_digit(key[j], shift, dmask);
+          dr[j] = (d << 16) | atomicAdd(&cnt[d], 1u);
+        }
     }
     __syncthreads();
-    // (digit, warp) counts -> staged positions, digit-major: digit d's rows of warp 0, then
-    // of warp 1, ... (row order); wcnt[0][d] becomes the start of digit d
-    {
+    // every thread has read its rows of the ring stage: refill it STG sub-tiles ahead
+    if (STG > 0 && threadIdx.x == 0 && k + NS < nring)
+      src.template issue<PAY, TILE>(g0 + (k + NS) * TILE, ring + (k % NS) * SB, &full[k % NS]);
+    if (STABLE) {
+      // (digit, warp) counts -> staged positions, digit-major: digit d's rows of warp 0, then
+      // of warp 1, ... (row order); wcnt[0][d] becomes the start of digit d
       const uint32_t b0 = min(threadIdx.x * dpt, F), b1 = min(b0 + dpt, F);
       uint32_t sum = 0;
       for (uint32_t b = b0; b < b1; b++)
@@ -222,13 +309,25 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
           run += c;
         }
       if (threadIdx.x == T - 1) s_total = inc;
+    } else {
+      // digit counts -> where each digit's rows start in the staging
+      const uint32_t b0 = min(threadIdx.x * dpt, F), b1 = min(b0 + dpt, F);
+      uint32_t sum = 0;
+      for (uint32_t b = b0; b < b1; b++) sum += cnt[b];
+      const uint32_t inc = rx_block_scan<T>(sum, wt);
+      uint32_t run = inc - sum;
+      for (uint32_t b = b0; b < b1; b++) {
+        start[b] = run;
+        run += cnt[b];
+      }
+      if (threadIdx.x == T - 1) s_total = inc;
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < I; j++)
       if (dr[j] != ~0u) {
         const uint32_t d = dr[j] >> 16;
-        const uint32_t pos = (uint32_t)mine[d] + (dr[j] & 0xFFFFu);
+        const uint32_t pos = (STABLE ? (uint32_t)mine[d] : start[d]) + (dr[j] & 0xFFFFu);
         skey[pos] = key[j];
         sdig[pos] = (uint16_t)d;
         if (PAY) spay[pos] = pay[j];
@@ -239,17 +338,24 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
     const uint32_t m = s_total;
     for (uint32_t i = threadIdx.x; i < m; i += T) {
       const uint32_t d = sdig[i];
-      const uint32_t o = cur[d] + (i - (uint32_t)wcnt[d]);
+      const uint32_t o = cur[d] + (i - (STABLE ? (uint32_t)wcnt[d] : start[d]));
       kout[o] = skey[i];
       if (PAY) pout[o] = spay[i];
     }
     __syncthreads();
-    for (uint32_t d = threadIdx.x; d < F; d += T) {
-      const uint32_t end = d + 1 < F ? (uint32_t)wcnt[d + 1] : m;
-      cur[d] += end - (uint32_t)wcnt[d];
+    if (STABLE) {
+      for (uint32_t d = threadIdx.x; d < F; d += T) {
+        const uint32_t end = d + 1 < F ? (uint32_t)wcnt[d + 1] : m;
+        cur[d] += end - (uint32_t)wcnt[d];
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
+    } else {
+      for (uint32_t d = threadIdx.x; d < F; d += T) {
+        cur[d] += cnt[d];
+        cnt[d] = 0;
+      }
     }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
     __syncthreads();
   }
 }
@@ -271,9 +377,10 @@ inline size_t rx_scratch_words(uint32_t G, int bits) {
 // Partitions the rows of `src` (at most n_max) into 2^bits partitions: keys (and payloads
 // when PAY) to kout/pout, partition starts to offsets[0 .. 2^bits] (the total last). Two
 // passes when bits > kRxPassBits, through ktmp/ptmp (n_max rows each). The scatter kernel
-// runs with T threads and I rows per thread; there are as many super-tiles as its blocks
-// fit on the GPU at once (fewer for a small input).
-template <class Src, class P, bool PAY, int T, int I>
+// runs with T threads, I rows per thread and an STG-stage bulk-copy ring (0: direct loads);
+// there are as many super-tiles as its blocks fit on the GPU at once (fewer for a small
+// input).
+template <class Src, class P, bool PAY, int T, int I, int STG, bool STABLE>
 int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout,
                         uint32_t* offsets, int32_t* ktmp, P* ptmp) {
   constexpr uint32_t TILE = T * I;
@@ -281,14 +388,15 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
   cudaStream_t s = call.stream();
   const int passes = bits <= kRxPassBits ? 1 : 2;
   const int d0 = passes == 1 ? bits : (bits + 1) / 2;
-  auto k0 = rx_scatter_kernel<Src, P, PAY, T, I>;
-  auto k1 = rx_scatter_kernel<ColumnSource<P>, P, PAY, T, I>;
-  const size_t smem_max = rx_scatter_smem<P, PAY, T, I>(1u << std::max(d0, bits - d0));
-  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k0, smem_max));
-  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k1, smem_max));
-  const int per_sm = kernel_occupancy(ctx, (const void*)k0, T, smem_max);
+  auto k0 = rx_scatter_kernel<Src, P, PAY, T, I, STG, STABLE>;
+  auto k1 = rx_scatter_kernel<ColumnSource<P>, P, PAY, T, I, STG, STABLE>;
+  const size_t smem0 = rx_scatter_smem<Src, P, PAY, T, I, STG, STABLE>(1u << d0);
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k0, smem0));
+  if (passes > 1)
+    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k1, rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, STABLE>(1u << (bits - d0))));
+  const int per_sm = kernel_occupancy(ctx, (const void*)k0, T, smem0);
   const uint64_t sub = (std::max<uint64_t>(n_max, 1) + TILE - 1) / TILE;
-  const uint32_t G = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sub, (uint64_t)ctx->sm_count * per_sm));
+  const uint32_t G = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sub, (uint64_t)ctx->sm_count * std::max(per_sm, 1)));
   const size_t hn = (size_t)kRxMaxF * G + 1;
   const size_t parts = (size_t)1 << bits;
   void* sc = nullptr;
@@ -305,7 +413,8 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
     const size_t hf = (size_t)F * G;
     int32_t* ko = pass == passes - 1 ? kout : ktmp;
     P* po = pass == passes - 1 ? pout : ptmp;
-    const size_t smem = rx_scatter_smem<P, PAY, T, I>(F);
+    const size_t sm0 = rx_scatter_smem<Src, P, PAY, T, I, STG, STABLE>(F);
+    const size_t sm1 = rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, STABLE>(F);
     GPUDB_CUDA(ctx, cudaMemsetAsync(hist, 0, hf * sizeof(uint32_t), s));
     if (pass == 0 && passes > 1) GPUDB_CUDA(ctx, cudaMemsetAsync(full, 0, parts * sizeof(uint32_t), s));
     uint32_t* fullp = (pass == 0 && passes > 1) ? full : nullptr;
@@ -314,7 +423,8 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
                    hist, fullp);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
-      GPUDB_LAUNCH(call, k0, G, T, smem, src, G, shift, dbits, (const uint32_t*)offs, ko, po);
+      GPUDB_LAUNCH(call, k0, G, T, sm0, src, G, shift, dbits,
+                   (const uint32_t*)offs, ko, po, call.status());
     } else {
       // rows of the first pass, in their pass-one order; their count is the first scan's total
       const uint32_t* total0 = full + parts;   // copied below
@@ -323,7 +433,8 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
                    dbits, bits, hist, (uint32_t*)nullptr);
       rc = exclusive_scan<uint32_t, uint32_t>(call, hist, hf, offs, stmp, offs + hf);
       if (rc) return rc;
-      GPUDB_LAUNCH(call, k1, G, T, smem, s2, G, shift, dbits, (const uint32_t*)offs, ko, po);
+      GPUDB_LAUNCH(call, k1, G, T, sm1, s2, G, shift, dbits,
+                   (const uint32_t*)offs, ko, po, call.status());
     }
     if (pass == 0 && passes > 1)
       GPUDB_CUDA(ctx, cudaMemcpyAsync(full + parts, offs + hf, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -337,32 +448,59 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
   return exclusive_scan<uint32_t, uint32_t>(call, full, parts, offsets, stmp, offsets + parts);
 }
 
-// The scatter block shape of the context (GPUDB_OPT_RADIX_SHAPE): 256 threads x 8 rows by
-// default (several blocks per SM), 512 x 16 or 256 x 16.
-template <class Src, class P, bool PAY>
+// Largest shared memory a scatter block may use (the B200 opt-in limit per block).
+constexpr size_t kRxSmemLimit = 226 * 1024;
+
+// Whether a scatter shape's blocks fit in shared memory for a partitioning of `bits` bits.
+template <class Src, class P, bool PAY, int T, int I, int STG, bool STABLE>
+constexpr bool rx_shape_fits(int bits) {
+  const int d0 = bits <= kRxPassBits ? bits : (bits + 1) / 2;
+  return rx_scatter_smem<Src, P, PAY, T, I, STG, STABLE>(1u << d0) <= kRxSmemLimit &&
+         rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, STABLE>(1u << (bits - d0 > 0 ? bits - d0 : 0)) <= kRxSmemLimit;
+}
+
+// The scatter block shape of the context (GPUDB_OPT_RADIX_SHAPE): 1 512 threads x 16 rows,
+// 2 256 x 8 (both with direct loads), 3 512 x 8, 4 256 x 8, 5 512 x 16 (each with a
+// two-stage bulk-copy ring); 0 (default) picks 3. A shape whose shared memory does not fit
+// falls back to 4 and then to 2. STABLE: rows keep their input order inside a partition.
+template <class Src, class P, bool PAY, bool STABLE>
 int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout, uint32_t* offsets,
                  int32_t* ktmp, P* ptmp) {
-  switch (call.ctx()->radix_shape) {
-    case 1: return rx_partition_shaped<Src, P, PAY, 512, 16>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
-    case 3: return rx_partition_shaped<Src, P, PAY, 256, 16>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
-    default: return rx_partition_shaped<Src, P, PAY, 256, 8>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+  int shape = call.ctx()->radix_shape ? call.ctx()->radix_shape : 3;
+  if (shape == 5 && !rx_shape_fits<Src, P, PAY, 512, 16, 2, STABLE>(bits)) shape = 3;
+  if (shape == 3 && !rx_shape_fits<Src, P, PAY, 512, 8, 2, STABLE>(bits)) shape = 4;
+  if (shape == 4 && !rx_shape_fits<Src, P, PAY, 256, 8, 2, STABLE>(bits)) shape = 2;
+  switch (shape) {
+    case 1:
+      return rx_partition_shaped<Src, P, PAY, 512, 16, 0, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    case 3:
+      return rx_partition_shaped<Src, P, PAY, 512, 8, 2, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    case 4:
+      return rx_partition_shaped<Src, P, PAY, 256, 8, 2, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    case 5:
+      return rx_partition_shaped<Src, P, PAY, 512, 16, 2, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    default:
+      return rx_partition_shaped<Src, P, PAY, 256, 8, 0, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
   }
 }
 
 // Plain columns (payload = row id when pay is null); the row count may be on the device.
-template <class P>
+// STABLE (the C ABI's partitioning) keeps the input order inside each partition; the joins,
+// whose results do not depend on it, take the unstable form.
+template <class P, bool STABLE>
 int radix_partition_run(Call& call, const int32_t* keys, const P* pay, uint64_t n_max, const uint32_t* n_dev, int bits,
                         int32_t* keys_out, P* pay_out, uint32_t* offsets, int32_t* keys_tmp, P* pay_tmp) {
   const ColumnSource<P> src{keys, pay, n_max, n_dev};
-  return rx_partition<ColumnSource<P>, P, true>(call, src, n_max, bits, keys_out, pay_out, offsets, keys_tmp, pay_tmp);
+  return rx_partition<ColumnSource<P>, P, true, STABLE>(call, src, n_max, bits, keys_out, pay_out, offsets, keys_tmp,
+                                                       pay_tmp);
 }
 
-// Keys only (no payload column is read or written).
+// Keys only (no payload column is read or written), unstable.
 inline int radix_partition_keys(Call& call, const int32_t* keys, uint64_t n, int bits, int32_t* keys_out,
                                 uint32_t* offsets, int32_t* keys_tmp) {
   const ColumnSource<int32_t> src{keys, nullptr, n, nullptr};
-  return rx_partition<ColumnSource<int32_t>, int32_t, false>(call, src, n, bits, keys_out, nullptr, offsets, keys_tmp,
-                                                             nullptr);
+  return rx_partition<ColumnSource<int32_t>, int32_t, false, false>(call, src, n, bits, keys_out, nullptr, offsets,
+                                                                    keys_tmp, nullptr);
 }
 
 // Partition bits so that the average partition holds about `per_part` rows.

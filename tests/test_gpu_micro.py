@@ -108,10 +108,11 @@ def test_radix_partition_large_inputs(engine, orc, bits, n):
             engine.device_free(x)
 
 
-@pytest.mark.parametrize("shape", [1, 2, 3])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5])
 def test_radix_partition_every_block_shape(engine, orc, shape):
     """Every scatter block shape (GPUDB_OPT_RADIX_SHAPE) gives the oracle's stable partition,
-    in one pass (10 bits) and in two (13 bits), and the same join count."""
+    in one pass (10 bits) and in two (13 bits), and the same join count; columns that start
+    off a 16-byte boundary (which the bulk-copy ring cannot stage) give it too."""
     n = 2_000_003
     keys = orc.gen(8, n, seed=shape, n_orders=n // 3, order_mode=1)
     pay = np.arange(n, dtype=np.int32) * 3
@@ -125,6 +126,13 @@ def test_radix_partition_every_block_shape(engine, orc, shape):
             assert np.array_equal(engine.to_host(off, (1 << bits) + 1, np.uint32), woff)
             assert np.array_equal(engine.to_host(ko, n, np.int32), wk)
             assert np.array_equal(engine.to_host(po, n, np.int32), wp)
+        # one row in: both columns 4 bytes past a 16-byte boundary
+        m = n - 1
+        engine.radix_partition(dk + 4, dp + 4, m, 10, ko, po, off)
+        wk, wp, woff = orc.radix_partition(keys[1:], pay[1:], 10)
+        assert np.array_equal(engine.to_host(off, (1 << 10) + 1, np.uint32), woff)
+        assert np.array_equal(engine.to_host(ko, m, np.int32), wk)
+        assert np.array_equal(engine.to_host(po, m, np.int32), wp)
         b = keys[: n // 4]
         assert engine.hash_join_count(dk, n // 4, dk, n, capi.JOIN_RADIX) == orc.join_count(b, keys)
     finally:
@@ -174,4 +182,17 @@ def test_radix_join_skewed_partition(engine, orc):
         assert engine.hash_join_count(db, len(b), dp, len(p), capi.JOIN_RADIX) == orc.join_count(b, p)
     finally:
         for x in (db, dp, ob, op):
+            engine.device_free(x)
+
+
+def test_radix_join_count_multi_chunk_partition(engine, orc):
+    """A build partition larger than one shared-memory chunk of the count kernel (one key
+    40,000 times next to 20,000 distinct keys): matches are flagged per chunk and counted once."""
+    b = np.concatenate([np.full(40_000, 77, np.int32), np.arange(100_000, 120_000, dtype=np.int32)])
+    p = np.concatenate([np.full(5, 77, np.int32), np.arange(90_000, 130_000, 3, dtype=np.int32), np.array([76, 78], np.int32)])
+    db, dp = engine.to_device(b), engine.to_device(p)
+    try:
+        assert engine.hash_join_count(db, len(b), dp, len(p), capi.JOIN_RADIX) == orc.join_count(b, p)
+    finally:
+        for x in (db, dp):
             engine.device_free(x)
