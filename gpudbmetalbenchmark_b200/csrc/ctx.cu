@@ -163,6 +163,9 @@ Call::Call(gpudb_ctx* ctx, const gpudb_exec* ex, gpudb_timing* t)
 }
 
 Call::~Call() {
+  // a call that failed between side_begin() and side_join(): later work on its stream still
+  // waits for the side stream, so scratch buffers are not reused under it
+  if (side_open_) (void)side_join();
   if (!handed_off_) {
     if (slot_ >= 0) (big_ ? ctx_->big_busy : ctx_->slot_busy)[slot_] = false;
     event_put(ctx_, e0_);
@@ -217,7 +220,33 @@ int Call::check_launch(const char* name) {
   return GPUDB_OK;
 }
 
+int Call::side_begin() {
+  if (main_) return fail(ctx_, GPUDB_E_INVALID, "side stream already in use by this call");
+  GPUDB_CUDA(ctx_, cudaEventRecord(ctx_->fork_ev, s_));
+  GPUDB_CUDA(ctx_, cudaStreamWaitEvent(ctx_->side_stream, ctx_->fork_ev, 0));
+  main_ = s_;
+  s_ = ctx_->side_stream;
+  side_open_ = true;
+  return GPUDB_OK;
+}
+
+void Call::side_end() {
+  if (main_) {
+    s_ = main_;
+    main_ = nullptr;
+  }
+}
+
+int Call::side_join() {
+  side_end();
+  side_open_ = false;
+  GPUDB_CUDA(ctx_, cudaEventRecord(ctx_->join_ev, ctx_->side_stream));
+  GPUDB_CUDA(ctx_, cudaStreamWaitEvent(s_, ctx_->join_ev, 0));
+  return GPUDB_OK;
+}
+
 int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert) {
+  side_end();   // (a stage that failed on the side stream may have left it selected)
   if (t_) GPUDB_CUDA(ctx_, cudaEventRecord(e1_, s_));
   size_t bytes = kSlotHeader + result_bytes;
   GPUDB_CUDA(ctx_, cudaMemcpyAsync(hslot_, dslot_, bytes, cudaMemcpyDeviceToHost, s_));
@@ -419,6 +448,9 @@ int gpudb_create(int device, gpudb_ctx** out) {
   ctx->sm_count = prop.multiProcessorCount;
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_slots, (size_t)kResultSlots * kSlotBytes);
   if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_slots, (size_t)kResultSlots * kSlotBytes, cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_big, (size_t)kBigSlots * kBigSlotBytes);
@@ -435,6 +467,7 @@ int gpudb_destroy(gpudb_ctx* ctx) {
   if (!ctx) return GPUDB_OK;
   cudaSetDevice(ctx->device);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
   if (ctx->stream) {
     cudaStreamSynchronize(ctx->stream);
     release_retired(ctx);
@@ -450,6 +483,9 @@ int gpudb_destroy(gpudb_ctx* ctx) {
   if (ctx->h_big) cudaFreeHost(ctx->h_big);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
   delete ctx;
   return GPUDB_OK;
 }

@@ -43,6 +43,8 @@ struct gpudb_ctx {
   int sm_count = 0;
   cudaStream_t stream = nullptr;       // compute stream
   cudaStream_t copy_stream = nullptr;  // host->device copies of streamed chunks
+  cudaStream_t side_stream = nullptr;  // independent stages of one call (Call::side_begin)
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   std::string err;
   uint64_t launches = 0;
   uint64_t h2d_total = 0, d2h_total = 0;   // bytes moved by finished calls (batch timing)
@@ -154,10 +156,20 @@ class Call {
   int finish(size_t result_bytes, std::function<int(const uint8_t*)> convert);
   gpudb_ctx* ctx() const { return ctx_; }
   int check_launch(const char* name);
+  // Independent stages on the context's side stream: side_begin() makes the side stream wait
+  // for what the call has queued so far and sends the call's work there (stream() is the side
+  // stream), side_end() sends it back without waiting, side_join() makes the call's stream
+  // wait for the side stream's work. Under stream capture the side stream joins the capture
+  // through the fork event and leaves it at the join.
+  int side_begin();
+  void side_end();
+  int side_join();
 
  private:
   gpudb_ctx* ctx_;
   cudaStream_t s_;
+  cudaStream_t main_ = nullptr;   // the call's stream while stream() is the side stream
+  bool side_open_ = false;        // side work queued that the call's stream has not waited for
   bool async_;
   gpudb_timing* t_;
   cudaEvent_t e0_ = nullptr, e1_ = nullptr;

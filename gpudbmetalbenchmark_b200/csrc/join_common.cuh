@@ -68,21 +68,14 @@ __host__ __device__ inline bool smem_filter_exact(int32_t key_max) {
 __host__ __device__ inline uint32_t smem_filter_words(int32_t key_max) {
   return smem_filter_exact(key_max) ? ((uint32_t)key_max >> 5) + 1 : kSmemFilterWords;
 }
-// The Bloom form's 32-bit mix of a key: the MurmurHash3 finaliser (fmix32). Its high bits
-// pick the word (multiplied onto [0, kSmemFilterWords)), three 5-bit fields of its low 15 bits
-// the bit positions.
-__device__ __forceinline__ uint32_t smem_filter_mix(int32_t key) {
-  uint32_t h = (uint32_t)key;
-  h ^= h >> 16;
-  h *= 0x85ebca6bu;
-  h ^= h >> 13;
-  h *= 0xc2b2ae35u;
-  h ^= h >> 16;
-  return h;
-}
+// The Bloom form's hash of a key: Fibonacci hashing (the key times 2^32 / golden ratio, one
+// multiply). Its high bits pick the word (multiplied onto [0, kSmemFilterWords)), the 5-bit
+// fields at bits 1, 6 and 11 the three bit positions (each mask bit a funnel shift, whose
+// shift count wraps at 32). About 1.3% of keys outside a random 5.5% of 2M keys pass.
+__device__ __forceinline__ uint32_t smem_filter_mix(int32_t key) { return (uint32_t)key * 0x9E3779B1u; }
 __device__ __forceinline__ uint32_t smem_filter_word(uint32_t h) { return __umulhi(h, kSmemFilterWords); }
 __device__ __forceinline__ uint32_t smem_filter_bits(uint32_t h) {
-  return (1u << (h & 31u)) | (1u << ((h >> 5) & 31u)) | (1u << ((h >> 10) & 31u));
+  return __funnelshift_l(0u, 1u, h >> 1) | __funnelshift_l(0u, 1u, h >> 6) | __funnelshift_l(0u, 1u, h >> 11);
 }
 
 // Bloom filter of an exact bitmap of `words` words: every set key sets its three bits.

@@ -43,14 +43,14 @@ namespace gpudb {
 namespace {
 
 constexpr int kFilterRows = 4;                 // rows per thread per block step of orders_filter_kernel
-constexpr uint32_t kSmemCustWords = 12288;     // customer filters up to 48 KB are copied to shared memory
 
 // Orders with order_date < date_lt whose customer passes the customer filter, compacted into
 // (key, date) with a block prefix sum and one atomicAdd per T * 4 rows. SMEM: the filter
-// (the exact bitmap, or a hashed one confirmed in `bitmap`) is copied into shared memory, for
-// small filters (1024 threads, two blocks per SM); otherwise the exact bitmap is tested in
-// place (256 threads, several blocks per SM). The three columns load together and the next
-// step's load while this one is tested.
+// (the exact bitmap, or a hashed one confirmed in `bitmap`) is copied into shared memory once
+// per block (1024 threads; as many blocks as fit on the GPU at once, so the copy is made once
+// or twice per SM); otherwise the exact bitmap is tested in place (256 threads, several
+// blocks per SM). The three columns load together and the next step's load while this one
+// is tested.
 // Where the orders that pass go: (key, date) staging lists (global and radix modes), or in
 // direct mode a dense slot per order ({key, date, revenue 0}, hit count 0) whose number the
 // direct map omap[key] receives, and the order's bit in the order-key bitmap okbm.
@@ -162,12 +162,13 @@ int launch_orders_filter_as(Call& call, const gpudb_customer& cu, const gpudb_or
 }
 
 // The orders filter of every join mode, after the customer bitmap: the shared-memory form
-// when the customer filter is at most 48 KB, else the in-place form on the exact bitmap.
+// whenever the exact customer bitmap fits its 200 KB (1.6M customer keys; two blocks per SM
+// up to about 100 KB, one above), else the in-place form on the exact bitmap.
 template <bool DIRECT>
 int launch_orders_filter(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_q3_params& p,
                          const uint32_t* bitmap, const FilterOut& out, uint32_t* cnt) {
   if (od.n_rows == 0) return GPUDB_OK;
-  if (smem_filter_exact(cu.key_max) && smem_filter_words(cu.key_max) <= kSmemCustWords)
+  if (smem_filter_exact(cu.key_max))
     return launch_orders_filter_as<1024, true, DIRECT>(call, cu, od, p, bitmap, bitmap, smem_filter_words(cu.key_max),
                                                        true, out, cnt);
   return launch_orders_filter_as<256, false, DIRECT>(call, cu, od, p, bitmap, bitmap, 0, true, out, cnt);
@@ -503,59 +504,66 @@ __global__ void __launch_bounds__(kTopkThreads) q3_select_kernel(const Q3Slot* _
 }
 
 // ---- radix mode ----------------------------------------------------------------------
-constexpr int kFactRows = 4;   // rows per thread per warp step of q3_fact_filter_kernel
+constexpr int kFactThreads = 256;
+constexpr int kFactQuads = 4;   // 16-byte quads of ship dates and keys per thread per block step
 
 // Fact rows that may join: ship_date > ship_gt and the order key in the hashed key set of
-// the kept orders, compacted to (order_key, ext * (100 - disc)). A warp step covers 128 rows
-// (row j*32 + lane of the step for j < 4): ship dates and keys load together, then the key
-// set words of the rows whose date passes, then one append per warp for the step's rows and
-// ext/discount only for the rows kept.
-__global__ void __launch_bounds__(256) q3_fact_filter_kernel(const int32_t* __restrict__ lkey,
-                                                             const int32_t* __restrict__ lship,
-                                                             const int64_t* __restrict__ lext,
-                                                             const int32_t* __restrict__ ldisc, uint64_t n,
-                                                             int32_t ship_gt, const uint32_t* __restrict__ kset,
-                                                             uint32_t kset_mask, int32_t* __restrict__ out_key,
-                                                             int64_t* __restrict__ out_val, uint32_t* count) {
-  const int lane = threadIdx.x & 31;
-  constexpr uint64_t kWarpRows = 32 * kFactRows;
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t b = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kWarpRows; b < n;
-       b += warps * kWarpRows) {   // whole warps: the append below needs every lane
-    int32_t k[kFactRows];
-    bool on[kFactRows];
+// the kept orders, compacted to (order_key, ext * (100 - disc)). A block step covers
+// kFactThreads * 16 rows (load q of thread t is quad q * kFactThreads + t of the step, 128-bit
+// loads where the columns allow): ship dates and keys load together, then the key-set words
+// of the rows whose date passes (all in flight together), then one block_reserve (a single
+// atomicAdd on the output count per 4096 rows; one per warp step made the counter the
+// bottleneck) and ext/discount only for the rows kept.
+__global__ void __launch_bounds__(kFactThreads) q3_fact_filter_kernel(
+    const int32_t* __restrict__ lkey, const int32_t* __restrict__ lship, const int64_t* __restrict__ lext,
+    const int32_t* __restrict__ ldisc, uint64_t n, int32_t ship_gt, const uint32_t* __restrict__ kset,
+    uint32_t kset_mask, int32_t* __restrict__ out_key, int64_t* __restrict__ out_val, uint32_t* count) {
+  __shared__ uint32_t sh[33];
+  constexpr int R = 4 * kFactQuads;
+  constexpr uint64_t kStep = (uint64_t)kFactThreads * R;
+  const bool vec = ((reinterpret_cast<uintptr_t>(lkey) | reinterpret_cast<uintptr_t>(lship)) & 15u) == 0;
+  auto row_of = [&](uint64_t b, int j) {   // row j (quad j / 4, element j % 4) of this thread
+    return b + 4 * ((uint64_t)(j >> 2) * kFactThreads + threadIdx.x) + (j & 3);
+  };
+  // whole blocks stay in the loop: block_reserve needs every thread of the block
+  for (uint64_t b = (uint64_t)blockIdx.x * kStep; b < n; b += (uint64_t)gridDim.x * kStep) {
+    int32_t k[R];
+    uint32_t on = 0;
+    if (vec && b + kStep <= n) {
 #pragma unroll
-    for (int j = 0; j < kFactRows; j++) {
-      const uint64_t i = b + (uint64_t)j * 32 + lane;
-      on[j] = i < n && ld_stream(lship + i) > ship_gt;
-      k[j] = i < n ? ld_stream(lkey + i) : 0;
-    }
-    uint32_t w[kFactRows];
-#pragma unroll
-    for (int j = 0; j < kFactRows; j++) {
-      const uint32_t h = kset_hash(k[j]);
-      w[j] = on[j] ? (__ldg(kset + ((h >> 5) & kset_mask)) >> (h & 31u)) & 1u : 0u;
-    }
-    uint32_t m[kFactRows], tot = 0;
-#pragma unroll
-    for (int j = 0; j < kFactRows; j++) {
-      m[j] = __ballot_sync(FULL_MASK, w[j] != 0u);
-      tot += __popc(m[j]);
-    }
-    if (tot == 0) continue;   // uniform across the warp
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(count, tot);
-    base = __shfl_sync(FULL_MASK, base, 0);
-#pragma unroll
-    for (int j = 0; j < kFactRows; j++) {
-      if (w[j]) {
-        const uint64_t i = b + (uint64_t)j * 32 + lane;
-        const uint32_t pos = base + __popc(m[j] & lanemask_lt());
-        out_key[pos] = k[j];
-        out_val[pos] = ld_stream(lext + i) * (int64_t)(100 - ld_stream(ldisc + i));
+      for (int q = 0; q < kFactQuads; q++) {
+        const uint64_t r0 = row_of(b, 4 * q);
+        const int4 sv = ld_stream(reinterpret_cast<const int4*>(lship + r0));
+        const int4 kv = ld_stream(reinterpret_cast<const int4*>(lkey + r0));
+        k[4 * q] = kv.x; k[4 * q + 1] = kv.y; k[4 * q + 2] = kv.z; k[4 * q + 3] = kv.w;
+        on |= ((uint32_t)(sv.x > ship_gt) | (uint32_t)(sv.y > ship_gt) << 1 | (uint32_t)(sv.z > ship_gt) << 2 |
+               (uint32_t)(sv.w > ship_gt) << 3) << (4 * q);
       }
-      base += __popc(m[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < R; j++) {
+        const uint64_t r = row_of(b, j);
+        const bool in = r < n;
+        k[j] = in ? ld_stream(lkey + r) : 0;
+        on |= (uint32_t)(in && ld_stream(lship + r) > ship_gt) << j;
+      }
     }
+    uint32_t take = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+      const uint32_t h = kset_hash(k[j]);
+      const uint32_t w = ((on >> j) & 1u) ? __ldg(kset + ((h >> 5) & kset_mask)) : 0u;
+      take |= ((w >> (h & 31u)) & 1u) << j;
+    }
+    uint32_t pos = block_reserve<kFactThreads>(__popc(take), count, sh);
+#pragma unroll
+    for (int j = 0; j < R; j++)
+      if ((take >> j) & 1u) {
+        const uint64_t r = row_of(b, j);
+        out_key[pos] = k[j];
+        out_val[pos] = ld_stream(lext + r) * (int64_t)(100 - ld_stream(ldisc + r));
+        pos++;
+      }
   }
 }
 
@@ -708,10 +716,11 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
   rc = radix_partition_run<int32_t, false>(call, bkey, bdate, n_or, cnt, bits, bk, bd, boff, bkey_t, bdate_t);
   if (rc) return rc;
   // fact rows that may join, compacted (a few percent of the table), then partitioned
-  const int fgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n_li + 1023) / 1024, (uint64_t)sms * 8));
+  const int fgrid = (int)std::max<uint64_t>(
+      1, std::min<uint64_t>((n_li + kFactThreads * 16 - 1) / (kFactThreads * 16), (uint64_t)sms * 8));
   rc = stream_lineitem(call, li, LI_ORDER | LI_SHIP | LI_EXT | LI_DISC, 0, [&](const gpudb_lineitem& c) {
     if (c.n_rows == 0) return (int)GPUDB_OK;
-    GPUDB_LAUNCH(call, q3_fact_filter_kernel, fgrid, 256, 0, c.order_key, c.ship_date, c.ext_price, c.discount,
+    GPUDB_LAUNCH(call, q3_fact_filter_kernel, fgrid, kFactThreads, 0, c.order_key, c.ship_date, c.ext_price, c.discount,
                  c.n_rows, p.ship_date_gt, (const uint32_t*)ks, kmask, fkey, fval, cnt + 1);
     return (int)GPUDB_OK;
   });

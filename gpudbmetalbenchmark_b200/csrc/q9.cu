@@ -11,9 +11,9 @@
 //    atomicCAS; the table is sized on the device from the qualifying count;
 //  - the fact table goes through in pieces of at most 64M rows, two kernels each:
 //    li_filter_kernel streams part_key (128-bit loads), tests each part against a filter held
-//    in shared memory (the exact bitmap, or a blocked Bloom filter whose ~1% false positives
-//    the resolve drops, since their (part, supp) is not in the partsupp table) and
-//    writes a bitmask of the rows that pass (~5.5%); q9_resolve_kernel expands the bitmask a
+//    in shared memory (the exact bitmap, or a blocked Bloom filter whose ~1.3% false
+//    positives the resolve turns away after gathering the part key, with one test of the
+//    exact bitmap) and writes a bitmask of the rows that pass (~5.5%); q9_resolve_kernel expands the bitmask a
 //    warp at a time (one set bit per lane) and gathers each row's six columns and its
 //    lookups together (late materialisation, all resident threads' misses in flight);
 //  - aggregation goes to a per-block shared-memory hash table keyed by (nation<<16 | year)
@@ -162,7 +162,7 @@ __device__ __forceinline__ void global_group_add(uint32_t* gkeys, unsigned long 
 }
 
 struct Q9Maps {
-  const uint32_t* part_bits; int32_t part_max;
+  const uint32_t* part_bits; int32_t part_max;   // part_bits: exact bitmap to confirm a Bloom filter's hits, or null
   const uint8_t* nation; int32_t supp_max;
   const PsSlot* ps; const uint32_t* ps_cap;
   const uint8_t* year; int32_t order_max;
@@ -224,8 +224,8 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
     uint32_t ok = 0;
 #pragma unroll
     for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
-    // Bloom-form hits go unconfirmed: a false positive's (part, supp) is not in the partsupp
-    // table, which holds only parts that pass, so the resolve drops it
+    // Bloom-form hits are not confirmed here: the resolve tests the exact bitmap after it has
+    // gathered the part key, before the other columns
     const uint32_t take = smem_filter_mask<kLiRows, false>(sfilt, exact, bits, p, ok);
 #pragma unroll
     for (int q = 0; q < kLiQuads; q++) {
@@ -298,7 +298,11 @@ __global__ void __launch_bounds__(kQ9Threads) q9_resolve_kernel(const uint32_t* 
       const uint32_t sx = __shfl_sync(FULL_MASK, incl - c, src);
       if (j >= total) continue;
       const uint64_t r = ((g * 32 + src) << 5) + nth_set_bit(sw, j - sx);
-      const int32_t pk = ld_stream(part + r), sk = ld_stream(supp + r), o = ld_stream(order + r);
+      const int32_t pk = ld_stream(part + r);
+      // a Bloom filter's false positive (about 1% of the other parts) stops after one gather
+      // and one test of the exact bitmap (L2-resident); the fact filter checked the range
+      if (m.part_bits && !((__ldg(m.part_bits + ((uint32_t)pk >> 5)) >> ((uint32_t)pk & 31u)) & 1u)) continue;
+      const int32_t sk = ld_stream(supp + r), o = ld_stream(order + r);
       const int64_t e = ld_stream(ext + r);
       const int32_t d = ld_stream(disc + r), q = ld_stream(qty + r);
       const bool s_ok = sk >= 0 && sk <= m.supp_max, o_ok = o >= 0 && o <= m.order_max;
@@ -452,10 +456,11 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   auto grid = [&](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16)); };
   // Every device operation of the pipeline, in stream order (status and result through
   // call.status()/call.result()).
+  // The part bitmap and the fact-row filter of the first piece stay on the call's stream; the
+  // supplier and year maps and the partsupp table, which the filter does not need, go on the
+  // context's side stream meanwhile, and the first resolve waits for both.
   auto enqueue = [&]() -> int {
     GPUDB_CUDA(ctx, cudaMemsetAsync(bits, 0, (size_t)words * 4, s));
-    GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, s));
-    GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(count, 0, 16, s));   // [0] partsupp count, [1] capacity
     GPUDB_CUDA(ctx, cudaMemsetAsync(gvals, 0, (size_t)gcap * 8, s));
     GPUDB_CUDA(ctx, cudaMemsetAsync(gkeys, 0xFF, (size_t)gcap * 4, s));
@@ -466,6 +471,11 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
       GPUDB_CUDA(ctx, cudaMemsetAsync(hfilt, 0, (size_t)kSmemFilterWords * 4, s));
       GPUDB_LAUNCH(call, hashed_filter_kernel, grid(words), 256, 0, (const uint32_t*)bits, words, (uint32_t*)hfilt);
     }
+    int sr = call.side_begin();
+    if (sr) return sr;
+    const cudaStream_t side = call.stream();
+    GPUDB_CUDA(ctx, cudaMemsetAsync(nation, 0xFF, (size_t)supp_max + 1, side));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(year, 0xFF, (size_t)order_max + 1, side));
     if (su->n_rows)
       GPUDB_LAUNCH(call, map_u8_kernel, grid(su->n_rows), 256, 0, su->supp_key, su->nation, su->n_rows, supp_max,
                    (uint8_t*)nation, call.status());
@@ -480,7 +490,9 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
                  (PsSlot*)pst);
     GPUDB_LAUNCH(call, ps_insert_kernel, grid(ps->n_rows), 256, 0, ps->part_key, ps->supp_key, ps->supply_cost,
                  (const uint32_t*)stage, (const uint32_t*)cnt, (const uint32_t*)cap, (PsSlot*)pst, call.status());
-    const Q9Maps maps{(const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,
+    call.side_end();
+    bool joined = false;
+    const Q9Maps maps{filt_exact ? nullptr : (const uint32_t*)bits, part_max, (const uint8_t*)nation, supp_max, (const PsSlot*)pst,
                       (const uint32_t*)cap, (const uint8_t*)year, order_max};
     int r = stream_lineitem(call, li, mask, pp.chunk_rows, [&](const gpudb_lineitem& c) {
       for (uint64_t off = 0; off < c.n_rows; off += piece) {
@@ -492,6 +504,11 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
         GPUDB_LAUNCH(call, li_filter_kernel, fg, kLiThreads, filt_smem, c.part_key + off, n, (const uint32_t*)bits,
                      part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_exact,
                      (uint32_t*)passbits);
+        if (!joined) {
+          const int jr = call.side_join();
+          if (jr) return jr;
+          joined = true;
+        }
         const uint64_t warps_needed = (n + 1023) / 1024;
         const unsigned g = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((warps_needed + kQ9Threads / 32 - 1) / (kQ9Threads / 32),
@@ -503,6 +520,7 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
       return (int)GPUDB_OK;
     });
     if (r) return r;
+    if (!joined && (r = call.side_join())) return r;
     GPUDB_LAUNCH(call, q9_sort_kernel, 1, 1024, sort_smem, (const uint32_t*)gkeys, (const unsigned long long*)gvals,
                  gcap, call.result<uint8_t>());
     return GPUDB_OK;

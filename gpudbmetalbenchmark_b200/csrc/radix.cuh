@@ -12,7 +12,7 @@
 //                     blocks per super-tile, so every SM streams) into hist[digit][G], and
 //                     in the first pass also the rows per final partition;
 //   exclusive_scan    over hist (digit-major): where each (digit, super-tile) run starts;
-//   rx_scatter_kernel one block per super-tile walks its sub-tiles (4096 rows by default) in
+//   rx_scatter_kernel one block per super-tile walks its sub-tiles (8192 rows by default) in
 //                     order, the next two in flight as bulk copies (TMA) into a shared-memory
 //                     ring. Each warp ranks its own contiguous rows by digit (__match_any_sync
 //                     and per-warp counters, no atomics), one block-wide scan turns the
@@ -461,12 +461,12 @@ constexpr bool rx_shape_fits(int bits) {
 
 // The scatter block shape of the context (GPUDB_OPT_RADIX_SHAPE): 1 512 threads x 16 rows,
 // 2 256 x 8 (both with direct loads), 3 512 x 8, 4 256 x 8, 5 512 x 16 (each with a
-// two-stage bulk-copy ring); 0 (default) picks 3. A shape whose shared memory does not fit
-// falls back to 4 and then to 2. STABLE: rows keep their input order inside a partition.
+// two-stage bulk-copy ring); 0 (default) picks 5. A shape whose shared memory does not fit
+// falls back to 3, then 4, then 2. STABLE: rows keep their input order inside a partition.
 template <class Src, class P, bool PAY, bool STABLE>
 int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout, uint32_t* offsets,
                  int32_t* ktmp, P* ptmp) {
-  int shape = call.ctx()->radix_shape ? call.ctx()->radix_shape : 3;
+  int shape = call.ctx()->radix_shape ? call.ctx()->radix_shape : 5;
   if (shape == 5 && !rx_shape_fits<Src, P, PAY, 512, 16, 2, STABLE>(bits)) shape = 3;
   if (shape == 3 && !rx_shape_fits<Src, P, PAY, 512, 8, 2, STABLE>(bits)) shape = 4;
   if (shape == 4 && !rx_shape_fits<Src, P, PAY, 256, 8, 2, STABLE>(bits)) shape = 2;

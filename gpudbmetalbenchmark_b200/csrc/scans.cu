@@ -233,6 +233,84 @@ __device__ __forceinline__ void q1_fold(Q1Acc& a, u128* partials, unsigned* tick
   }
 }
 
+// Exact unsigned 128-bit add into global memory with two 64-bit atomics: the carry out of the
+// low word's add goes into the high word's add, so once every add has landed the 128-bit
+// value is the exact sum, whatever the order of the adds.
+__device__ __forceinline__ void atomic_add_u128(u128* p, u128 v) {
+  unsigned long long* w = reinterpret_cast<unsigned long long*>(p);
+  const unsigned long long lo = (unsigned long long)v, hi = (unsigned long long)(v >> 64);
+  const unsigned long long old = atomicAdd(w, lo);
+  const unsigned long long up = hi + (old + lo < old ? 1ull : 0ull);
+  if (up) atomicAdd(w + 1, up);
+}
+
+// Fold of the shared-memory form's per-thread sums acc[(metric * 6 + group) * T + thread]
+// (metrics P, E, ED, EDT): each warp sums three of the 24 columns (P unpacked into count,
+// quantity and discount sum) and adds the block's totals into the 36 u128 words of `gacc`
+// with exact 128-bit atomics; the last block turns them into the output and zeroes `gacc`
+// for the next launch (it is zero when first allocated). No per-block partials are read back.
+template <int T>
+__device__ __forceinline__ void q1_smem_fold(const uint64_t* acc, uint32_t bad, u128* gacc, unsigned* ticket, u128* out,
+                                             uint32_t* status) {
+  constexpr int W = T / 32;
+  static_assert(24 % W == 0, "whole columns per warp");
+  __shared__ u128 tot[6 * kQ1Raw];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // also orders every thread's shared-memory sums before the column reads
+  if (__syncthreads_or(bad) && threadIdx.x == 0) set_status(status, ST_DOMAIN);
+  for (int c = warp; c < 24; c += W) {
+    const int metric = c / 6, g = c % 6;
+    u128 s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll 4
+    for (int i = lane; i < T; i += 32) {
+      const uint64_t v = acc[c * T + i];
+      if (metric == 0) {
+        s0 += v & 0x1FFFu;
+        s1 += v >> 32;
+        s2 += (v >> 13) & 0x7FFFFu;
+      } else {
+        s0 += v;
+      }
+    }
+    s0 = warp_sum_u128(s0);
+    if (metric == 0) {
+      s1 = warp_sum_u128(s1);
+      s2 = warp_sum_u128(s2);
+    }
+    if (lane == 0) {
+      u128* o = gacc + g * kQ1Raw;   // raw metrics: count, qty, E, ED, EDT, dsum
+      if (metric == 0) {
+        atomic_add_u128(o + 0, s0);
+        atomic_add_u128(o + 1, s1);
+        atomic_add_u128(o + 5, s2);
+      } else {
+        atomic_add_u128(o + 1 + metric, s0);
+      }
+    }
+  }
+  if (!grid_last_block(ticket)) return;
+  if (threadIdx.x < 6 * kQ1Raw) {
+    unsigned long long* w = reinterpret_cast<unsigned long long*>(gacc + threadIdx.x);
+    tot[threadIdx.x] = ((u128)__ldcg(w + 1) << 64) | __ldcg(w);
+    w[0] = 0;
+    w[1] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int g = threadIdx.x;
+    const u128* r = tot + g * kQ1Raw;
+    const u128 disc_price = (u128)100 * r[2] - r[3];
+    const u128 charge = (u128)100 * disc_price + r[4];
+    u128* o = out + g * kQ1Metrics;
+    o[0] += r[0];
+    o[1] += r[1];
+    o[2] += r[2];
+    o[3] += disc_price;
+    o[4] += charge;
+    o[5] += r[5];
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2) q1_vec_kernel(const int4* __restrict__ ship4, const int4* __restrict__ qty4,
                                                              const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
                                                              const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
@@ -571,7 +649,7 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
                                                                      const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
                                                                      const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
                                                                      const uint32_t* __restrict__ stat4, uint64_t n, int32_t ship_le,
-                                                                     u128* partials, unsigned* ticket, u128* out, uint32_t* status) {
+                                                                     u128* gacc, unsigned* ticket, u128* out, uint32_t* status) {
   constexpr int T = kQ1SmemThreads;
   extern __shared__ __align__(16) uint64_t q1_acc[];   // [4 metrics][6 groups][T]
   const int t = threadIdx.x;
@@ -623,16 +701,7 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
         reinterpret_cast<const int32_t*>(tax4)[r], reinterpret_cast<const uint8_t*>(flag4)[r],
         reinterpret_cast<const uint8_t*>(stat4)[r]);
   }
-  Q1Acc a;
-#pragma unroll
-  for (int gi = 0; gi < 6; gi++) {
-    a.P[gi] = q1_acc[(0 * 6 + gi) * T + t];
-    a.E[gi] = q1_acc[(1 * 6 + gi) * T + t];
-    a.ED[gi] = q1_acc[(2 * 6 + gi) * T + t];
-    a.EDT[gi] = q1_acc[(3 * 6 + gi) * T + t];
-  }
-  a.bad = bad;
-  q1_fold<T>(a, partials, ticket, out, status);
+  q1_smem_fold<T>(q1_acc, bad, gacc, ticket, out, status);
 }
 
 bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
@@ -716,9 +785,10 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
     const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
     const int grid = (int)std::max<uint64_t>(
         1, std::max(min_blocks, std::min<uint64_t>(want, (uint64_t)ctx->sm_count * per_sm)));
+    // 36 u128 accumulators and a ticket, both left at zero by every launch's last block
     void* part = nullptr;
     unsigned* ticket = nullptr;
-    int rc = scan_scratch(ctx, "q1.partials", (size_t)grid * 6 * kQ1Raw * sizeof(u128), &part, &ticket);
+    int rc = scan_scratch(ctx, "q1.acc", (size_t)6 * kQ1Raw * sizeof(u128), &part, &ticket);
     if (rc) return rc;
     GPUDB_LAUNCH(call, kern, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
                  (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
