@@ -25,10 +25,10 @@
 //  7. q3_select_kernel: the slots in the histogram bins that can hold the top-k are
 //     appended, and the last block to finish ranks them.
 // Radix mode partitions both sides by key hash (radix.cuh) and joins each partition in
-// shared memory. The kept orders also set a hashed key set (8 bits per orders row, no key
+// shared memory. The kept orders also set a hashed key set (16 bits per orders row, no key
 // range needed), and the fact filter drops the rows whose order key misses it before they
 // are compacted and partitioned: a semi-join reduction, so only rows that may join (plus
-// about 1% false positives, which the partition join drops) are partitioned.
+// about 2% of the others, false positives that the partition join drops) are partitioned.
 #include <algorithm>
 #include <cstring>
 
@@ -43,14 +43,14 @@ namespace gpudb {
 namespace {
 
 constexpr int kFilterRows = 4;                 // rows per thread per block step of orders_filter_kernel
+constexpr uint32_t kSmemCustWords = 12288;     // customer filters up to 48 KB are copied to shared memory
 
 // Orders with order_date < date_lt whose customer passes the customer filter, compacted into
 // (key, date) with a block prefix sum and one atomicAdd per T * 4 rows. SMEM: the filter
-// (the exact bitmap, or a hashed one confirmed in `bitmap`) is copied into shared memory once
-// per block (1024 threads; as many blocks as fit on the GPU at once, so the copy is made once
-// or twice per SM); otherwise the exact bitmap is tested in place (256 threads, several
-// blocks per SM). The three columns load together and the next step's load while this one
-// is tested.
+// (the exact bitmap, or a hashed one confirmed in `bitmap`) is copied into shared memory, for
+// small filters (1024 threads, two blocks per SM); otherwise the exact bitmap is tested in
+// place (256 threads, several blocks per SM). The three columns load together and the next
+// step's load while this one is tested.
 // Where the orders that pass go: (key, date) staging lists (global and radix modes), or in
 // direct mode a dense slot per order ({key, date, revenue 0}, hit count 0) whose number the
 // direct map omap[key] receives, and the order's bit in the order-key bitmap okbm.
@@ -66,18 +66,20 @@ struct FilterOut {
   uint32_t kset_mask;
 };
 
-// The hashed key set of the radix mode: one bit per key hash in a power-of-two array of
-// words, sized from the orders row count (8 bits per row), so it needs no key range. A
-// fact row whose order key misses it cannot join; a hit may be a false positive (about
-// kept orders / (8 x orders rows)), which the partition join then drops.
-__device__ __forceinline__ uint32_t kset_hash(int32_t key) { return slot_hash64((uint64_t)(uint32_t)key); }
+// The hashed key set of the radix mode: a power-of-two array of words sized from the orders
+// row count (16 bits per row), so it needs no key range. Keys come in blocks of 32: the block
+// (key >> 5) is hashed to a word and the key's low 5 bits pick the bit, so the keys of one
+// order-clustered run of fact rows share a word (a warp's 128 rows read a few words, not 128
+// scattered ones). A fact row whose order key misses the set cannot join; a hit may be a
+// false positive (another block hashed to the same word), which the partition join drops.
+__device__ __forceinline__ uint32_t kset_word(int32_t key, uint32_t mask) {
+  return slot_hash64((uint64_t)((uint32_t)key >> 5)) & mask;
+}
 __device__ __forceinline__ void kset_add(uint32_t* set, uint32_t mask, int32_t key) {
-  const uint32_t h = kset_hash(key);
-  atomicOr(set + ((h >> 5) & mask), 1u << (h & 31u));
+  atomicOr(set + kset_word(key, mask), 1u << ((uint32_t)key & 31u));
 }
 __device__ __forceinline__ bool kset_test(const uint32_t* set, uint32_t mask, int32_t key) {
-  const uint32_t h = kset_hash(key);
-  return (__ldg(set + ((h >> 5) & mask)) >> (h & 31u)) & 1u;
+  return (__ldg(set + kset_word(key, mask)) >> ((uint32_t)key & 31u)) & 1u;
 }
 
 template <int T, bool SMEM, bool DIRECT>
@@ -162,13 +164,15 @@ int launch_orders_filter_as(Call& call, const gpudb_customer& cu, const gpudb_or
 }
 
 // The orders filter of every join mode, after the customer bitmap: the shared-memory form
-// whenever the exact customer bitmap fits its 200 KB (1.6M customer keys; two blocks per SM
-// up to about 100 KB, one above), else the in-place form on the exact bitmap.
+// when the customer filter is at most 48 KB (two 1024-thread blocks per SM), else the
+// in-place form on the exact bitmap. (With one block per SM, as a larger filter allows, each
+// step's block barriers leave the SM idle: the 188 KB filter of 1.5M customers took 213 us
+// in shared memory against 115 us in place for 15M orders.)
 template <bool DIRECT>
 int launch_orders_filter(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const gpudb_q3_params& p,
                          const uint32_t* bitmap, const FilterOut& out, uint32_t* cnt) {
   if (od.n_rows == 0) return GPUDB_OK;
-  if (smem_filter_exact(cu.key_max))
+  if (smem_filter_exact(cu.key_max) && smem_filter_words(cu.key_max) <= kSmemCustWords)
     return launch_orders_filter_as<1024, true, DIRECT>(call, cu, od, p, bitmap, bitmap, smem_filter_words(cu.key_max),
                                                        true, out, cnt);
   return launch_orders_filter_as<256, false, DIRECT>(call, cu, od, p, bitmap, bitmap, 0, true, out, cnt);
@@ -551,9 +555,8 @@ __global__ void __launch_bounds__(kFactThreads) q3_fact_filter_kernel(
     uint32_t take = 0;
 #pragma unroll
     for (int j = 0; j < R; j++) {
-      const uint32_t h = kset_hash(k[j]);
-      const uint32_t w = ((on >> j) & 1u) ? __ldg(kset + ((h >> 5) & kset_mask)) : 0u;
-      take |= ((w >> (h & 31u)) & 1u) << j;
+      const uint32_t w = ((on >> j) & 1u) ? __ldg(kset + kset_word(k[j], kset_mask)) : 0u;
+      take |= ((w >> ((uint32_t)k[j] & 31u)) & 1u) << j;
     }
     uint32_t pos = block_reserve<kFactThreads>(__popc(take), count, sh);
 #pragma unroll
@@ -665,9 +668,9 @@ int q3_radix(Call& call, const gpudb_customer& cu, const gpudb_orders& od, const
                  : ctx->radix_bits > 0 ? ctx->radix_bits
                                        : std::min(kRxPassBits, std::max(9, radix_bits_for(od.n_rows, 16384)));
   const uint64_t parts = 1ull << bits;
-  // hashed set of the kept order keys: 8 bits per orders row, a power of two of words
+  // hashed set of the kept order keys: 16 bits per orders row, a power of two of words
   uint64_t kwords = 32;
-  while (kwords < n_or / 4 && kwords < (1ull << 28)) kwords <<= 1;
+  while (kwords < n_or / 2 && kwords < (1ull << 28)) kwords <<= 1;
   const uint64_t n_or_a = (n_or + 31) / 32 * 32;   // 128-byte aligned column starts
   void *bitmap, *bstage, *fstage, *count, *bpart, *fpart, *offs, *cand, *kset;
   int rc = scratch(ctx, "q3.bitmap", (size_t)words * 4, &bitmap);

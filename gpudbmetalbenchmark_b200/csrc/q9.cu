@@ -175,9 +175,37 @@ constexpr int kLiQuads = 4;                  // 16-byte loads per thread per blo
 constexpr int kLiRows = 4 * kLiQuads;        // fact rows per thread per block step of li_filter_kernel
 constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve pair (bounds the pair buffer)
 
+// Part filter forms of li_filter_kernel.
+enum : int {
+  kPartBloom = 0,   // blocked Bloom filter in shared memory (hits confirmed by the resolve)
+  kPartExact = 1,   // the exact bitmap, all of it in shared memory
+  kPartSplit = 2    // the exact bitmap: its first filt_words words in shared memory, the rest
+                    // read in place (L1/L2) for the keys above them
+};
+constexpr uint32_t kSplitWords = 50176;   // 196 KB: the smem carve-out leaves 60 KB of L1 for the rest
+
+// Split exact filter: bit `key` of the first `swords` words from shared memory, of the others
+// from the exact bitmap in global memory; every load issued before any is used.
+template <int N>
+__device__ __forceinline__ uint32_t split_filter_mask(const uint32_t* sfilt, uint32_t swords,
+                                                      const uint32_t* __restrict__ bits, const int32_t (&key)[N],
+                                                      uint32_t ok) {
+  uint32_t w[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    const uint32_t x = (uint32_t)key[j] >> 5;
+    w[j] = !((ok >> j) & 1u) ? 0u : x < swords ? sfilt[x] : __ldg(bits + x);
+  }
+  uint32_t hit = 0;
+#pragma unroll
+  for (int j = 0; j < N; j++) hit |= ((w[j] >> ((uint32_t)key[j] & 31u)) & 1u) << j;
+  return hit & ok;
+}
+
 // Fact rows whose part passes the filter -> bit (r & 31) of passbits[r >> 5] (rows of the
-// piece). The part filter sits in shared memory (smem_filter_*): the exact bitmap, or a
-// blocked Bloom filter whose hits are not confirmed here. A block step covers kLiThreads * 16 rows;
+// piece). The part filter (`mode`): the exact bitmap in shared memory, the exact bitmap split
+// between shared memory and global memory, or a blocked Bloom filter in shared memory whose
+// hits are not confirmed here. A block step covers kLiThreads * 16 rows;
 // load q of thread t is the 16-byte quad q * kLiThreads + t of the step (coalesced), and the
 // next step's quads load while this one is tested. The four rows of a quad are four bits of
 // one word that eight lanes share: an OR across the eight lanes and one store per word, so
@@ -186,7 +214,7 @@ constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve p
 __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
                                                                const uint32_t* __restrict__ bits, int32_t part_max,
                                                                const uint32_t* __restrict__ filt, uint32_t filt_words,
-                                                               bool exact, uint32_t* __restrict__ passbits) {
+                                                               int mode, uint32_t* __restrict__ passbits) {
   extern __shared__ uint32_t sfilt[];
   smem_filter_load(filt, filt_words, sfilt);
   const bool vec = (reinterpret_cast<uintptr_t>(part) & 15u) == 0;
@@ -226,7 +254,8 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
     for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
     // Bloom-form hits are not confirmed here: the resolve tests the exact bitmap after it has
     // gathered the part key, before the other columns
-    const uint32_t take = smem_filter_mask<kLiRows, false>(sfilt, exact, bits, p, ok);
+    const uint32_t take = mode == kPartSplit ? split_filter_mask<kLiRows>(sfilt, filt_words, bits, p, ok)
+                                             : smem_filter_mask<kLiRows, false>(sfilt, mode == kPartExact, bits, p, ok);
 #pragma unroll
     for (int q = 0; q < kLiQuads; q++) {
       // rows 4*lane .. 4*lane+3 of this quad's 128 rows: bits 4*(lane & 7) .. of word lane / 8
@@ -428,11 +457,16 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (!rc) rc = scratch(ctx, "q9.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q9.ps", (size_t)ps_max_cap * sizeof(PsSlot), &pst);
   if (!rc) rc = scratch(ctx, "q9.groups", (size_t)gcap * 12, &groups);
-  // the part filter of li_filter_kernel: the exact bitmap itself, or a hashed one built from it
-  const bool filt_exact = smem_filter_exact(part_max);
-  const uint32_t filt_words = smem_filter_words(part_max);
+  // the part filter of li_filter_kernel: the exact bitmap in shared memory; split between
+  // shared memory and the global bitmap up to twice the shared-memory part (80% of 2M parts
+  // tested in shared memory); beyond that a Bloom filter built from it
+  const int filt_mode = smem_filter_exact(part_max) ? kPartExact
+                      : (uint64_t)part_max < 2ull * 32 * kSplitWords ? kPartSplit : kPartBloom;
+  const bool filt_exact = filt_mode != kPartBloom;   // no false positives for the resolve to drop
+  const uint32_t filt_words = filt_mode == kPartExact ? smem_filter_words(part_max)
+                            : filt_mode == kPartSplit ? kSplitWords : kSmemFilterWords;
   void* hfilt = nullptr;
-  if (!rc && !filt_exact) rc = scratch(ctx, "q9.partfilter", (size_t)kSmemFilterWords * 4, &hfilt);
+  if (!rc && filt_mode == kPartBloom) rc = scratch(ctx, "q9.partfilter", (size_t)kSmemFilterWords * 4, &hfilt);
   // pass bitmask of one piece of the fact table (rows whose part passed the part filter;
   // chunk_rows, when given, also sets the piece size of a device-resident table)
   const uint64_t piece =
@@ -502,7 +536,7 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
             1, std::min<uint64_t>((n + kLiThreads * kLiRows - 1) / (kLiThreads * kLiRows),
                                   (uint64_t)sms * std::max(1, filter_per_sm)));
         GPUDB_LAUNCH(call, li_filter_kernel, fg, kLiThreads, filt_smem, c.part_key + off, n, (const uint32_t*)bits,
-                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_exact,
+                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_mode,
                      (uint32_t*)passbits);
         if (!joined) {
           const int jr = call.side_join();
