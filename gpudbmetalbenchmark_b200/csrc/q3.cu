@@ -75,9 +75,6 @@ struct FilterOut {
 __device__ __forceinline__ uint32_t kset_word(int32_t key, uint32_t mask) {
   return slot_hash64((uint64_t)((uint32_t)key >> 5)) & mask;
 }
-__device__ __forceinline__ void kset_add(uint32_t* set, uint32_t mask, int32_t key) {
-  atomicOr(set + kset_word(key, mask), 1u << ((uint32_t)key & 31u));
-}
 __device__ __forceinline__ bool kset_test(const uint32_t* set, uint32_t mask, int32_t key) {
   return (__ldg(set + kset_word(key, mask)) >> ((uint32_t)key & 31u)) & 1u;
 }
@@ -134,12 +131,18 @@ __global__ void __launch_bounds__(T, SMEM ? 2 : 1) orders_filter_kernel(
               make_ulonglong2((unsigned long long)(uint32_t)key[j] | ((unsigned long long)(uint32_t)date[j] << 32), 0ull);
           out.hits[pos] = 0;
           out.omap[key[j]] = (int32_t)pos;
-          const uint32_t bit = 1u << ((uint32_t)key[j] & 31u);
-          if (atomicOr(out.okbm + ((uint32_t)key[j] >> 5), bit) & bit) set_status(status, ST_DUPLICATE);
         } else {
           out.key[pos] = key[j];
           out.date[pos] = date[j];
-          if (out.kset) kset_add(out.kset, out.kset_mask, key[j]);
+        }
+        // the order-key bit (direct) or key-set bit (radix), one atomicOr per kept order: about
+        // one order in ten is kept, so few lanes of a warp share a word (merging the lanes of
+        // a word with __match_any_sync first was slower)
+        const uint32_t bit = 1u << ((uint32_t)key[j] & 31u);
+        if (DIRECT) {
+          if (atomicOr(out.okbm + ((uint32_t)key[j] >> 5), bit) & bit) set_status(status, ST_DUPLICATE);
+        } else if (out.kset) {
+          atomicOr(out.kset + kset_word(key[j], out.kset_mask), bit);
         }
         pos++;
       }

@@ -178,34 +178,12 @@ constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve p
 // Part filter forms of li_filter_kernel.
 enum : int {
   kPartBloom = 0,   // blocked Bloom filter in shared memory (hits confirmed by the resolve)
-  kPartExact = 1,   // the exact bitmap, all of it in shared memory
-  kPartSplit = 2    // the exact bitmap: its first filt_words words in shared memory, the rest
-                    // read in place (L1/L2) for the keys above them
+  kPartExact = 1    // the exact bitmap, all of it in shared memory
 };
-constexpr uint32_t kSplitWords = 50176;   // 196 KB: the smem carve-out leaves 60 KB of L1 for the rest
-
-// Split exact filter: bit `key` of the first `swords` words from shared memory, of the others
-// from the exact bitmap in global memory; every load issued before any is used.
-template <int N>
-__device__ __forceinline__ uint32_t split_filter_mask(const uint32_t* sfilt, uint32_t swords,
-                                                      const uint32_t* __restrict__ bits, const int32_t (&key)[N],
-                                                      uint32_t ok) {
-  uint32_t w[N];
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    const uint32_t x = (uint32_t)key[j] >> 5;
-    w[j] = !((ok >> j) & 1u) ? 0u : x < swords ? sfilt[x] : __ldg(bits + x);
-  }
-  uint32_t hit = 0;
-#pragma unroll
-  for (int j = 0; j < N; j++) hit |= ((w[j] >> ((uint32_t)key[j] & 31u)) & 1u) << j;
-  return hit & ok;
-}
 
 // Fact rows whose part passes the filter -> bit (r & 31) of passbits[r >> 5] (rows of the
-// piece). The part filter (`mode`): the exact bitmap in shared memory, the exact bitmap split
-// between shared memory and global memory, or a blocked Bloom filter in shared memory whose
-// hits are not confirmed here. A block step covers kLiThreads * 16 rows;
+// piece). The part filter (`mode`): the exact bitmap in shared memory, or a blocked Bloom
+// filter in shared memory whose hits are not confirmed here. A block step covers kLiThreads * 16 rows;
 // load q of thread t is the 16-byte quad q * kLiThreads + t of the step (coalesced), and the
 // next step's quads load while this one is tested. The four rows of a quad are four bits of
 // one word that eight lanes share: an OR across the eight lanes and one store per word, so
@@ -254,8 +232,7 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
     for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
     // Bloom-form hits are not confirmed here: the resolve tests the exact bitmap after it has
     // gathered the part key, before the other columns
-    const uint32_t take = mode == kPartSplit ? split_filter_mask<kLiRows>(sfilt, filt_words, bits, p, ok)
-                                             : smem_filter_mask<kLiRows, false>(sfilt, mode == kPartExact, bits, p, ok);
+    const uint32_t take = smem_filter_mask<kLiRows, false>(sfilt, mode == kPartExact, bits, p, ok);
 #pragma unroll
     for (int q = 0; q < kLiQuads; q++) {
       // rows 4*lane .. 4*lane+3 of this quad's 128 rows: bits 4*(lane & 7) .. of word lane / 8
@@ -457,14 +434,14 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (!rc) rc = scratch(ctx, "q9.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q9.ps", (size_t)ps_max_cap * sizeof(PsSlot), &pst);
   if (!rc) rc = scratch(ctx, "q9.groups", (size_t)gcap * 12, &groups);
-  // the part filter of li_filter_kernel: the exact bitmap in shared memory; split between
-  // shared memory and the global bitmap up to twice the shared-memory part (80% of 2M parts
-  // tested in shared memory); beyond that a Bloom filter built from it
-  const int filt_mode = smem_filter_exact(part_max) ? kPartExact
-                      : (uint64_t)part_max < 2ull * 32 * kSplitWords ? kPartSplit : kPartBloom;
+  // the part filter of li_filter_kernel: the exact bitmap in shared memory, else a Bloom
+  // filter built from it. (Splitting the exact bitmap between shared memory and global memory
+  // spares the resolve the false positives, but the global lookups for the keys above the
+  // shared part leave the filter latency-bound: at 2M parts 121 us against 93 us for the
+  // Bloom form, against 227 us instead of 238 us for the resolve.)
+  const int filt_mode = smem_filter_exact(part_max) ? kPartExact : kPartBloom;
   const bool filt_exact = filt_mode != kPartBloom;   // no false positives for the resolve to drop
-  const uint32_t filt_words = filt_mode == kPartExact ? smem_filter_words(part_max)
-                            : filt_mode == kPartSplit ? kSplitWords : kSmemFilterWords;
+  const uint32_t filt_words = filt_mode == kPartExact ? smem_filter_words(part_max) : kSmemFilterWords;
   void* hfilt = nullptr;
   if (!rc && filt_mode == kPartBloom) rc = scratch(ctx, "q9.partfilter", (size_t)kSmemFilterWords * 4, &hfilt);
   // pass bitmask of one piece of the fact table (rows whose part passed the part filter;

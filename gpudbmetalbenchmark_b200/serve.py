@@ -174,6 +174,26 @@ def pct(xs, p):
     return xs[min(len(xs) - 1, int(round(p / 100.0 * (len(xs) - 1))))]
 
 
+def job_class(job):
+    """Pipeline and, for the scans, the table size: "q6_60m", "q1_6m", "q3", "q9"."""
+    if job.kind in (capi.PIPE_Q6, capi.PIPE_Q1):
+        rows = job.req.li.contents.n_rows
+        return "%s_%dm" % ("q6" if job.kind == capi.PIPE_Q6 else "q1", rows // 1_000_000)
+    return "q3" if job.kind == capi.PIPE_Q3 else "q9"
+
+
+def latency_by_class(jobs, lat):
+    """Per request class: count, p50 and p99 (ms), and its share of the requests above the
+    run's p99 (which classes make the tail)."""
+    cut = pct(lat, 99)
+    groups = {}
+    for j, x in zip(jobs, lat):
+        groups.setdefault(job_class(j), []).append(x)
+    tail = sum(1 for x in lat if x > cut) or 1
+    return {c: {"n": len(v), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99),
+                "tail_share": sum(1 for x in v if x > cut) / tail} for c, v in sorted(groups.items())}
+
+
 def open_loop(server, jobs, rate, seed):
     """Submits jobs at Poisson arrival times (rate per second); returns latencies (ms) and wall time."""
     rng = random.Random(seed)
@@ -220,7 +240,8 @@ def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None):
         exact = all(j.result() == w for j, w in zip(jobs, check))
     return {"mode": name, "lanes": lanes, "max_batch": max_batch, "offered_qps": rate, "requests": n,
             "achieved_qps": n / wall, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mean_batch":
-            st["completed"] / max(1, st["batches"]), "all_ok": ok, "bit_exact_vs_solo": exact}
+            st["completed"] / max(1, st["batches"]), "all_ok": ok, "bit_exact_vs_solo": exact,
+            "by_class": latency_by_class(jobs, lat)}
 
 
 def compare(eng, seconds=1.0, lanes=4, max_batch=64, loads=(0.5, 0.85), factor=3.0, seed=11):
@@ -284,7 +305,8 @@ def _run_checked(eng, wl, name, lanes, max_batch, rate, n, seed, jobs, solo):
     return {"mode": name, "offered_qps": None if rate >= 1e9 else rate, "requests": n, "achieved_qps": n / wall,
             "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mean_batch": st["completed"] / max(1, st["batches"]),
             "all_ok": all(x == capi.OK for x in status),
-            "bit_exact_vs_solo": all(j.result() == w for j, w in zip(jobs, solo))}
+            "bit_exact_vs_solo": all(j.result() == w for j, w in zip(jobs, solo)),
+            "by_class": latency_by_class(jobs, lat)}
 
 
 def main(argv=None):

@@ -53,10 +53,8 @@ def test_q9_shared_table_spill_and_small_global_table(engine, orc):
 
 @pytest.mark.parametrize("n_parts", [1_700_000, 3_300_000])
 def test_q9_part_filter_past_shared_memory(engine, orc, n_parts):
-    """Part keys past the shared-memory filter's 1,638,400 bits. 1.7M parts: the exact bitmap
-    split between shared memory (keys below 1,605,632) and global memory; 3.3M parts: a
-    blocked Bloom filter in shared memory whose false positives the resolve drops after
-    testing the exact bitmap."""
+    """Part keys past the shared-memory filter's 1,638,400 bits: a blocked Bloom filter in
+    shared memory whose false positives the resolve drops after testing the exact bitmap."""
     tabs = orc.q9_tables(n_parts, 2_000, 200_000, 800_000, 17)
     ts = upload_all(engine, tabs)
     try:
