@@ -368,6 +368,8 @@ void q1_from_words(const uint8_t* w, gpudb_q1_result& o) {
 }
 
 // Runs the scan requests `ids` of `reqs` as shared scans (fits one result slot).
+gpudb_lineitem row_view(const gpudb_lineitem& li, uint64_t begin, uint64_t end);
+
 int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32_t>& ids, gpudb_timing* t,
                    const gpudb_exec* ex) {
   // group by (scan columns, row range); within a group, Q1 requests also share their
@@ -394,8 +396,23 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
   }
   std::vector<ScanGroup> groups;
   std::vector<ScanTile> tiles6, tiles1, tiles11;   // Q6 passes, Q1 passes of two / of one Q1 request
+  // A Q1 request alone on its columns runs the single-request Q1 kernel (at the copy peak)
+  // instead of a shared pass (whose per-row work for the Q6 requests riding along and the
+  // cutoff buckets makes it slower than the Q1 kernel and a separate Q6 pass together).
+  std::vector<std::pair<uint32_t, gpudb_lineitem>> solo_q1;   // (position in ids, row range view)
+  std::vector<char> solo(ids.size(), 0);
   for (auto& kv : by_table) {
     Members& mb = kv.second;
+    for (auto it = mb.q1.begin(); it != mb.q1.end();) {
+      if (it->second.size() == 1) {
+        const uint32_t k = it->second[0];
+        solo_q1.emplace_back(k, row_view(*reqs[ids[k]].li, std::get<4>(kv.first), std::get<5>(kv.first)));
+        solo[k] = 1;
+        it = mb.q1.erase(it);
+      } else {
+        ++it;
+      }
+    }
     for (auto& c : mb.q1)
       std::sort(c.second.begin(), c.second.end(),
                 [&](uint32_t a, uint32_t b) { return reqs[ids[a]].q1.ship_le < reqs[ids[b]].q1.ship_le; });
@@ -478,8 +495,14 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
     if (!rc) rc = launch_pass<1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles11, dt11, queue + 2, res, st);
     if (rc) return rc;
   }
+  for (const auto& sq : solo_q1) {
+    const uint32_t k = sq.first;
+    rc = launch_q1(call, sq.second, reqs[ids[k]].q1, dres + status_bytes + (size_t)offs[k] * 8,
+                   reinterpret_cast<uint32_t*>(dres) + k);
+    if (rc) return rc;
+  }
   std::vector<uint32_t> ids_copy = ids;
-  return call.finish(bytes, [reqs, ids_copy, offs, status_bytes, ctx](const uint8_t* h) {
+  return call.finish(bytes, [reqs, ids_copy, offs, status_bytes, ctx, solo](const uint8_t* h) {
     for (size_t k = 0; k < ids_copy.size(); k++) {
       gpudb_request& q = reqs[ids_copy[k]];
       uint32_t st;
@@ -489,7 +512,8 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
       if (q.pipeline == GPUDB_PIPE_Q6) {
         if (q.q6_out) { std::memcpy(&q.q6_out->revenue, w, 8); std::memcpy(&q.q6_out->rows_matched, w + 8, 8); }
       } else if (q.q1_out) {
-        q1_from_words(w, *q.q1_out);
+        if (solo[k]) q1_result_from(w, q.q1_out);   // the Q1 kernel's words
+        else q1_from_words(w, *q.q1_out);           // a shared pass's raw sums
       }
       if (ctx->on_done) ctx->on_done(ctx->on_done_arg, &q.status);
     }

@@ -26,7 +26,7 @@ from .engine import Engine, Q1_COLS
 
 
 class Server:
-    def __init__(self, device=0, lanes=4, max_batch=64, memory_budget=0):
+    def __init__(self, device=0, lanes=2, max_batch=64, memory_budget=0):
         self.lib = capi.load()
         cfg = capi.ServeConfig(device=device, lanes=lanes, max_batch=max_batch, memory_budget=memory_budget)
         h = C.c_void_p()
@@ -244,7 +244,13 @@ def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None):
             "by_class": latency_by_class(jobs, lat)}
 
 
-def compare(eng, seconds=1.0, lanes=4, max_batch=64, loads=(0.5, 0.85), factor=3.0, seed=11):
+# Lanes of the served form: at 22K queries/s of the mixed stream, 1/2/3/4/8 lanes gave p99
+# 5.2/4.4/4.7/5-21/8.0 ms on one B200 (two lanes overlap two batches on the GPU; more lanes
+# contend for it, one leaves it idle between batches).
+DEFAULT_LANES = 2
+
+
+def compare(eng, seconds=1.0, lanes=DEFAULT_LANES, max_batch=64, loads=(0.5, 0.85), factor=3.0, seed=11):
     """Served form against the plain one-query-per-launch form on the same mixed stream.
 
     1. plain saturation: requests submitted back to back (closed loop), queries/s;
@@ -313,7 +319,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--rates", type=float, nargs="*", default=[1000, 2000, 4000, 8000, 16000, 32000])
     ap.add_argument("--seconds", type=float, default=2.0)
-    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--lanes", type=int, default=DEFAULT_LANES)
     ap.add_argument("--max-batch", type=int, default=64)
     ap.add_argument("--modes", nargs="*", default=["plain", "served"], choices=["plain", "served"])
     ap.add_argument("--compare", action="store_true",
