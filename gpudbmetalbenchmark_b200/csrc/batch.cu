@@ -396,22 +396,32 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
   }
   std::vector<ScanGroup> groups;
   std::vector<ScanTile> tiles6, tiles1, tiles11;   // Q6 passes, Q1 passes of two / of one Q1 request
-  // A Q1 request alone on its columns runs the single-request Q1 kernel (at the copy peak)
-  // instead of a shared pass (whose per-row work for the Q6 requests riding along and the
-  // cutoff buckets makes it slower than the Q1 kernel and a separate Q6 pass together).
-  std::vector<std::pair<uint32_t, gpudb_lineitem>> solo_q1;   // (position in ids, row range view)
+  // Few requests on one table run the single-request kernels (both at the copy peak)
+  // instead of shared passes, whose per-row work for several requests makes them
+  // instruction-bound: over 60M rows a Q1 pass takes about 0.45 ms (two Q1 requests, Q6
+  // requests riding along) and a Q6 pass about 0.3 ms, against 0.23 ms for the Q1 kernel and
+  // 0.14 ms for the Q6 kernel. So up to kSoloQ1 Q1 requests on the same columns, and up to
+  // kSoloQ6 Q6 requests of a table without a Q1 pass, run alone.
+  constexpr size_t kSoloQ1 = 2, kSoloQ6 = 3;
+  std::vector<std::pair<uint32_t, gpudb_lineitem>> solo_scans;   // (position in ids, row range view)
   std::vector<char> solo(ids.size(), 0);
   for (auto& kv : by_table) {
     Members& mb = kv.second;
+    auto take_solo = [&](uint32_t k) {
+      solo_scans.emplace_back(k, row_view(*reqs[ids[k]].li, std::get<4>(kv.first), std::get<5>(kv.first)));
+      solo[k] = 1;
+    };
     for (auto it = mb.q1.begin(); it != mb.q1.end();) {
-      if (it->second.size() == 1) {
-        const uint32_t k = it->second[0];
-        solo_q1.emplace_back(k, row_view(*reqs[ids[k]].li, std::get<4>(kv.first), std::get<5>(kv.first)));
-        solo[k] = 1;
+      if (it->second.size() <= kSoloQ1) {
+        for (uint32_t k : it->second) take_solo(k);
         it = mb.q1.erase(it);
       } else {
         ++it;
       }
+    }
+    if (mb.q1.empty() && mb.q6.size() <= kSoloQ6) {
+      for (uint32_t k : mb.q6) take_solo(k);
+      mb.q6.clear();
     }
     for (auto& c : mb.q1)
       std::sort(c.second.begin(), c.second.end(),
@@ -495,10 +505,12 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
     if (!rc) rc = launch_pass<1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles11, dt11, queue + 2, res, st);
     if (rc) return rc;
   }
-  for (const auto& sq : solo_q1) {
+  for (const auto& sq : solo_scans) {
     const uint32_t k = sq.first;
-    rc = launch_q1(call, sq.second, reqs[ids[k]].q1, dres + status_bytes + (size_t)offs[k] * 8,
-                   reinterpret_cast<uint32_t*>(dres) + k);
+    const gpudb_request& q = reqs[ids[k]];
+    uint8_t* w = dres + status_bytes + (size_t)offs[k] * 8;   // the kernel adds into these zeroed words
+    rc = q.pipeline == GPUDB_PIPE_Q6 ? launch_q6(call, sq.second, q.q6, w)
+                                     : launch_q1(call, sq.second, q.q1, w, reinterpret_cast<uint32_t*>(dres) + k);
     if (rc) return rc;
   }
   std::vector<uint32_t> ids_copy = ids;
@@ -512,7 +524,7 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
       if (q.pipeline == GPUDB_PIPE_Q6) {
         if (q.q6_out) { std::memcpy(&q.q6_out->revenue, w, 8); std::memcpy(&q.q6_out->rows_matched, w + 8, 8); }
       } else if (q.q1_out) {
-        if (solo[k]) q1_result_from(w, q.q1_out);   // the Q1 kernel's words
+        if (solo[k]) q1_result_from(w, q.q1_out);   // the Q1 kernel's words (a Q6 kernel's match a pass's)
         else q1_from_words(w, *q.q1_out);           // a shared pass's raw sums
       }
       if (ctx->on_done) ctx->on_done(ctx->on_done_arg, &q.status);
