@@ -402,7 +402,15 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
   // requests riding along) and a Q6 pass about 0.3 ms, against 0.23 ms for the Q1 kernel and
   // 0.14 ms for the Q6 kernel. So up to kSoloQ1 Q1 requests on the same columns, and up to
   // kSoloQ6 Q6 requests of a table without a Q1 pass, run alone.
-  constexpr size_t kSoloQ1 = 2, kSoloQ6 = 3;
+  // One Q1 request with up to kRideQ6 Q6 requests on its table runs the Q1 kernel with the
+  // Q6 requests riding along (one read of the rows for all of them, at the Q1 kernel's speed).
+  constexpr size_t kSoloQ1 = 2, kSoloQ6 = 3, kRideQ6 = 4;
+  struct Riding {
+    uint32_t q1;
+    std::vector<uint32_t> q6;
+    gpudb_lineitem view;
+  };
+  std::vector<Riding> riding;
   std::vector<std::pair<uint32_t, gpudb_lineitem>> solo_scans;   // (position in ids, row range view)
   std::vector<char> solo(ids.size(), 0);
   for (auto& kv : by_table) {
@@ -411,6 +419,14 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
       solo_scans.emplace_back(k, row_view(*reqs[ids[k]].li, std::get<4>(kv.first), std::get<5>(kv.first)));
       solo[k] = 1;
     };
+    if (mb.q1.size() == 1 && mb.q1.begin()->second.size() == 1 && !mb.q6.empty() && mb.q6.size() <= kRideQ6) {
+      const uint32_t k = mb.q1.begin()->second[0];
+      riding.push_back(Riding{k, mb.q6, row_view(*reqs[ids[k]].li, std::get<4>(kv.first), std::get<5>(kv.first))});
+      solo[k] = 1;
+      for (uint32_t j : mb.q6) solo[j] = 1;
+      mb.q1.clear();
+      mb.q6.clear();
+    }
     for (auto it = mb.q1.begin(); it != mb.q1.end();) {
       if (it->second.size() <= kSoloQ1) {
         for (uint32_t k : it->second) take_solo(k);
@@ -503,6 +519,17 @@ int run_scan_batch(gpudb_ctx* ctx, gpudb_request* reqs, const std::vector<uint32
     rc = launch_pass<0, kMaxQ6>(ctx, call, dgrp, tiles6, dt6, queue, res, st);
     if (!rc) rc = launch_pass<kMaxQ1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles1, dt1, queue + 1, res, st);
     if (!rc) rc = launch_pass<1, kMaxQ6WithQ1>(ctx, call, dgrp, tiles11, dt11, queue + 2, res, st);
+    if (rc) return rc;
+  }
+  for (const Riding& rd : riding) {
+    std::vector<gpudb_q6_params> p6;
+    std::vector<void*> o6;
+    for (uint32_t j : rd.q6) {
+      p6.push_back(reqs[ids[j]].q6);
+      o6.push_back(dres + status_bytes + (size_t)offs[j] * 8);
+    }
+    rc = launch_q1_riders(call, rd.view, reqs[ids[rd.q1]].q1, dres + status_bytes + (size_t)offs[rd.q1] * 8,
+                          reinterpret_cast<uint32_t*>(dres) + rd.q1, (int)p6.size(), p6.data(), o6.data());
     if (rc) return rc;
   }
   for (const auto& sq : solo_scans) {

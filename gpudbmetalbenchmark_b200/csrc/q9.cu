@@ -22,7 +22,6 @@
 //    one once at the end (global atomics ~ blocks x groups, not rows);
 //  - one block compacts the global table and sorts it by nation asc, year desc.
 #include <algorithm>
-#include <cooperative_groups.h>
 #include <cstring>
 #include <string>
 
@@ -32,8 +31,6 @@
 
 namespace gpudb {
 namespace {
-
-namespace cg = cooperative_groups;
 
 constexpr uint32_t kGroupEmpty = 0xFFFFFFFFu;
 constexpr unsigned long long kPsEmpty = ~0ull;
@@ -181,27 +178,8 @@ constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve p
 // Part filter forms of li_filter_kernel.
 enum : int {
   kPartBloom = 0,   // blocked Bloom filter in shared memory (hits confirmed by the resolve)
-  kPartExact = 1,   // the exact bitmap, all of it in shared memory
-  kPartPair = 2     // the exact bitmap split over the shared memory of a 2-CTA cluster
+  kPartExact = 1    // the exact bitmap, all of it in shared memory
 };
-
-// Pair form: the bit of key k sits in word k >> 5 of the exact bitmap; words [0, half) are in
-// the shared memory of the cluster's CTA 0, the rest in CTA 1's (distributed shared memory,
-// generic loads through the cluster's shared window). Every load issued before any is used.
-template <int N>
-__device__ __forceinline__ uint32_t pair_filter_mask(const uint32_t* s0, const uint32_t* s1, uint32_t half,
-                                                     const int32_t (&key)[N], uint32_t ok) {
-  uint32_t w[N];
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    const uint32_t x = (uint32_t)key[j] >> 5;
-    w[j] = !((ok >> j) & 1u) ? 0u : x < half ? s0[x] : s1[x - half];
-  }
-  uint32_t hit = 0;
-#pragma unroll
-  for (int j = 0; j < N; j++) hit |= ((w[j] >> ((uint32_t)key[j] & 31u)) & 1u) << j;
-  return hit & ok;
-}
 
 // Fact rows whose part passes the filter -> bit (r & 31) of passbits[r >> 5] (rows of the
 // piece). The part filter (`mode`): the exact bitmap in shared memory, or a blocked Bloom
@@ -211,29 +189,12 @@ __device__ __forceinline__ uint32_t pair_filter_mask(const uint32_t* s0, const u
 // one word that eight lanes share: an OR across the eight lanes and one store per word, so
 // warps never wait for each other (no block barrier, no atomic) and the bitmask is dense
 // (one bit per row, 1/32 of the column read).
-// PAIR: launched in clusters of two CTAs; `filt` is the exact bitmap and filt_words the words
-// each CTA holds (CTA r the words from r * filt_words); both halves are loaded before any CTA
-// of the cluster reads the other's, and neither CTA leaves while the other may still read.
-template <bool PAIR>
 __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
                                                                const uint32_t* __restrict__ bits, int32_t part_max,
                                                                const uint32_t* __restrict__ filt, uint32_t filt_words,
                                                                int mode, uint32_t* __restrict__ passbits) {
   extern __shared__ uint32_t sfilt[];
-  const uint32_t* s0 = sfilt;
-  const uint32_t* s1 = sfilt;
-  if constexpr (PAIR) {
-    cg::cluster_group cluster = cg::this_cluster();
-    const uint32_t rank = cluster.block_rank();
-    const uint32_t words = ((uint32_t)part_max >> 5) + 1;
-    const uint32_t first = rank * filt_words;
-    smem_filter_load(filt + first, first < words ? min(filt_words, words - first) : 0u, sfilt);
-    cluster.sync();
-    s0 = cluster.map_shared_rank(sfilt, 0);
-    s1 = cluster.map_shared_rank(sfilt, 1);
-  } else {
-    smem_filter_load(filt, filt_words, sfilt);
-  }
+  smem_filter_load(filt, filt_words, sfilt);
   const bool vec = (reinterpret_cast<uintptr_t>(part) & 15u) == 0;
   const int lane = threadIdx.x & 31;
   constexpr uint64_t kStepRows = (uint64_t)kLiThreads * kLiRows;
@@ -271,8 +232,7 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
     for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
     // Bloom-form hits are not confirmed here: the resolve tests the exact bitmap after it has
     // gathered the part key, before the other columns
-    const uint32_t take = PAIR ? pair_filter_mask<kLiRows>(s0, s1, filt_words, p, ok)
-                               : smem_filter_mask<kLiRows, false>(sfilt, mode == kPartExact, bits, p, ok);
+    const uint32_t take = smem_filter_mask<kLiRows, false>(sfilt, mode == kPartExact, bits, p, ok);
 #pragma unroll
     for (int q = 0; q < kLiQuads; q++) {
       // rows 4*lane .. 4*lane+3 of this quad's 128 rows: bits 4*(lane & 7) .. of word lane / 8
@@ -284,7 +244,6 @@ __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __
       if ((lane & 7) == 0 && r0 < n) passbits[r0 >> 5] = v;
     }
   }
-  if constexpr (PAIR) cg::this_cluster().sync();   // the peer may still read this CTA's half
 }
 
 // Position of the k-th (from 0) set bit of w: halving, by the bit counts of the low halves.
@@ -475,19 +434,16 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   if (!rc) rc = scratch(ctx, "q9.count", 256, &count);
   if (!rc) rc = scratch(ctx, "q9.ps", (size_t)ps_max_cap * sizeof(PsSlot), &pst);
   if (!rc) rc = scratch(ctx, "q9.groups", (size_t)gcap * 12, &groups);
-  // the part filter of li_filter_kernel: the exact bitmap in shared memory; up to twice
-  // that, the exact bitmap split over a 2-CTA cluster's shared memory; beyond, a Bloom filter
-  // built from it. (Splitting the exact bitmap between shared memory and global memory
-  // instead left the filter latency-bound on its global lookups: at 2M parts 121 us against
-  // 93 us for the Bloom form.)
-  const uint32_t pwords = ((uint32_t)part_max >> 5) + 1;
-  const int filt_mode = smem_filter_exact(part_max)          ? kPartExact
-                      : (pwords + 1) / 2 <= kSmemFilterWords ? kPartPair
-                                                             : kPartBloom;
+  // the part filter of li_filter_kernel: the exact bitmap in shared memory, else a Bloom
+  // filter built from it. Two exact alternatives for 2M parts were measured slower: the exact
+  // bitmap split between shared memory and global memory (121 us against 93 us for the Bloom
+  // form: latency-bound on the global lookups for the keys above the shared part), and the
+  // exact bitmap split over the shared memory of a 2-CTA cluster, read through distributed
+  // shared memory (338 us: random 4-byte reads of the peer's shared memory stall on
+  // long_scoreboard and the memory pipes).
+  const int filt_mode = smem_filter_exact(part_max) ? kPartExact : kPartBloom;
   const bool filt_exact = filt_mode != kPartBloom;   // no false positives for the resolve to drop
-  const uint32_t filt_words = filt_mode == kPartExact  ? smem_filter_words(part_max)
-                            : filt_mode == kPartPair   ? (pwords + 1) / 2
-                                                       : kSmemFilterWords;
+  const uint32_t filt_words = filt_mode == kPartExact ? smem_filter_words(part_max) : kSmemFilterWords;
   void* hfilt = nullptr;
   if (!rc && filt_mode == kPartBloom) rc = scratch(ctx, "q9.partfilter", (size_t)kSmemFilterWords * 4, &hfilt);
   // pass bitmask of one piece of the fact table (rows whose part passed the part filter;
@@ -505,10 +461,8 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   // dynamic + static shared memory may pass the 48 KB default: always opt in (before any capture)
   GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q9_resolve_kernel, probe_smem));
   const size_t filt_smem = (size_t)filt_words * 4;
-  const bool pair = filt_mode == kPartPair;
-  const void* lif = pair ? (const void*)li_filter_kernel<true> : (const void*)li_filter_kernel<false>;
-  GPUDB_CUDA(ctx, kernel_smem(ctx, lif, filt_smem));
-  const int filter_per_sm = kernel_occupancy(ctx, lif, kLiThreads, filt_smem);
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)li_filter_kernel, filt_smem));
+  const int filter_per_sm = kernel_occupancy(ctx, (const void*)li_filter_kernel, kLiThreads, filt_smem);
   const int resolve_per_sm = kernel_occupancy(ctx, (const void*)q9_resolve_kernel, kQ9Threads, probe_smem);
   GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q9_sort_kernel, sort_smem));
   const int sms = ctx->sm_count;
@@ -557,31 +511,12 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
       for (uint64_t off = 0; off < c.n_rows; off += piece) {
         // (the previous piece's resolve is done with the bitmask: stream order)
         const uint64_t n = std::min<uint64_t>(piece, c.n_rows - off);
-        unsigned fg = (unsigned)std::max<uint64_t>(
+        const unsigned fg = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((n + kLiThreads * kLiRows - 1) / (kLiThreads * kLiRows),
                                   (uint64_t)sms * std::max(1, filter_per_sm)));
-        const uint32_t* ffilt = filt_exact ? (const uint32_t*)bits : (const uint32_t*)hfilt;
-        if (pair) {
-          fg = (fg + 1) & ~1u;   // whole clusters of two
-          cudaLaunchConfig_t lc{};
-          cudaLaunchAttribute at{};
-          at.id = cudaLaunchAttributeClusterDimension;
-          at.val.clusterDim.x = 2;
-          at.val.clusterDim.y = 1;
-          at.val.clusterDim.z = 1;
-          lc.gridDim = dim3(fg);
-          lc.blockDim = dim3(kLiThreads);
-          lc.dynamicSmemBytes = filt_smem;
-          lc.stream = call.stream();
-          lc.attrs = &at;
-          lc.numAttrs = 1;
-          GPUDB_CUDA(ctx, cudaLaunchKernelEx(&lc, li_filter_kernel<true>, c.part_key + off, n, (const uint32_t*)bits,
-                                             part_max, ffilt, filt_words, filt_mode, (uint32_t*)passbits));
-          call.count_launch();
-        } else {
-          GPUDB_LAUNCH(call, li_filter_kernel<false>, fg, kLiThreads, filt_smem, c.part_key + off, n,
-                       (const uint32_t*)bits, part_max, ffilt, filt_words, filt_mode, (uint32_t*)passbits);
-        }
+        GPUDB_LAUNCH(call, li_filter_kernel, fg, kLiThreads, filt_smem, c.part_key + off, n, (const uint32_t*)bits,
+                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_mode,
+                     (uint32_t*)passbits);
         if (!joined) {
           const int jr = call.side_join();
           if (jr) return jr;

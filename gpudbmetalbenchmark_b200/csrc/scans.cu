@@ -642,21 +642,41 @@ __global__ void __launch_bounds__(THREADS, 1) q1_ring_smem_kernel(const int32_t*
 constexpr int kQ1SmemThreads = 256;
 constexpr size_t kQ1AccBytes = (size_t)4 * 6 * kQ1SmemThreads * 8;   // 49,152
 
+// Q6 requests evaluated on the rows a Q1 scan reads (one read of the table for both): their
+// constants, and the two words (revenue, rows matched) each one adds into.
+constexpr int kMaxRiders = 4;
+struct Q6Riders {
+  Q6P p[kMaxRiders];
+  unsigned long long* out[kMaxRiders];
+};
+
 // MINB: resident blocks per SM the registers are sized for (2: the default; 3: variant 8,
-// more loads in flight for tables that end in one short wave).
-template <int MINB>
+// more loads in flight for tables that end in one short wave). NQ6: Q6 requests riding along
+// (register sums per request, added into their words at the end).
+template <int MINB, int NQ6>
 __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const int4* __restrict__ ship4, const int4* __restrict__ qty4,
                                                                      const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
                                                                      const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
                                                                      const uint32_t* __restrict__ stat4, uint64_t n, int32_t ship_le,
-                                                                     u128* gacc, unsigned* ticket, u128* out, uint32_t* status) {
+                                                                     u128* gacc, unsigned* ticket, u128* out, uint32_t* status,
+                                                                     Q6Riders riders) {
   constexpr int T = kQ1SmemThreads;
   extern __shared__ __align__(16) uint64_t q1_acc[];   // [4 metrics][6 groups][T]
   const int t = threadIdx.x;
 #pragma unroll
   for (int i = 0; i < 24; i++) q1_acc[i * T + t] = 0;
   uint32_t bad = 0;
+  int64_t rrev[NQ6 > 0 ? NQ6 : 1];
+  uint64_t rcnt[NQ6 > 0 ? NQ6 : 1];
+#pragma unroll
+  for (int r = 0; r < NQ6; r++) { rrev[r] = 0; rcnt[r] = 0; }
   auto row = [&](int32_t s, int32_t qt, int64_t e, int32_t d, int32_t tx, uint32_t f, uint32_t st) {
+#pragma unroll
+    for (int r = 0; r < NQ6; r++) {
+      const bool m = q6_pass(s, d, qt, riders.p[r]);
+      rrev[r] += m ? e * (int64_t)d : 0;
+      rcnt[r] += m;
+    }
     if (!((s <= ship_le) & (f <= 2u) & (st <= 1u))) return;
     bad |= ((uint32_t)qt >= 65536u) | ((uint32_t)d > 100u) | ((uint32_t)tx > 100u) | ((uint64_t)e >= (1ull << 36));
     const uint64_t ed = (uint64_t)e * (uint32_t)d;
@@ -700,6 +720,14 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
         reinterpret_cast<const int64_t*>(ext2)[r], reinterpret_cast<const int32_t*>(disc4)[r],
         reinterpret_cast<const int32_t*>(tax4)[r], reinterpret_cast<const uint8_t*>(flag4)[r],
         reinterpret_cast<const uint8_t*>(stat4)[r]);
+  }
+#pragma unroll
+  for (int r = 0; r < NQ6; r++) {
+    const unsigned long long v = warp_sum_u64((unsigned long long)rrev[r]), c = warp_sum_u64(rcnt[r]);
+    if ((t & 31) == 0) {
+      if (v) atomicAdd(riders.out[r], v);
+      if (c) atomicAdd(riders.out[r] + 1, c);
+    }
   }
   q1_smem_fold<T>(q1_acc, bad, gacc, ticket, out, status);
 }
@@ -763,6 +791,32 @@ int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, voi
 }
 
 // Enqueue one Q1 scan of device-resident columns, adding into `out` (device, 36 x u128).
+// The shared-memory Q1 kernel (16-byte aligned columns): a grid of SMs x occupancy blocks
+// (at most kQ1RowsPerThread rows a thread) over the 36 u128 accumulators of "q1.acc".
+using Q1SmemKernel = void (*)(const int4*, const int4*, const longlong2*, const int4*, const int4*, const uint32_t*,
+                              const uint32_t*, uint64_t, int32_t, u128*, unsigned*, u128*, uint32_t*, Q6Riders);
+static int launch_q1_smem(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status,
+                          Q1SmemKernel kern, const Q6Riders& riders) {
+  gpudb_ctx* ctx = call.ctx();
+  const size_t smem = kQ1AccBytes;
+  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kern, smem));
+  const int per_sm = kernel_occupancy(ctx, (const void*)kern, kQ1SmemThreads, smem);
+  const uint64_t min_blocks = (c.n_rows + (uint64_t)kQ1SmemThreads * kQ1RowsPerThread - 1) /
+                              ((uint64_t)kQ1SmemThreads * kQ1RowsPerThread);
+  const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
+  const int grid = (int)std::max<uint64_t>(
+      1, std::max(min_blocks, std::min<uint64_t>(want, (uint64_t)ctx->sm_count * std::max(per_sm, 1))));
+  // 36 u128 accumulators and a ticket, both left at zero by every launch's last block
+  void* part = nullptr;
+  unsigned* ticket = nullptr;
+  int rc = scan_scratch(ctx, "q1.acc", (size_t)6 * kQ1Raw * sizeof(u128), &part, &ticket);
+  if (rc) return rc;
+  GPUDB_LAUNCH(call, kern, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
+               (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
+               (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status, riders);
+  return GPUDB_OK;
+}
+
 int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status) {
   gpudb_ctx* ctx = call.ctx();
   if (!status) status = call.status();
@@ -775,26 +829,9 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
   int variant = ctx->scan_variant;
   if (variant == 0) variant = vec ? 7 : 3;
   if ((variant == 7 || variant == 8) && !vec) variant = 3;
-  if (variant == 7 || variant == 8) {
-    auto kern = variant == 8 ? q1_vec_smem_kernel<3> : q1_vec_smem_kernel<2>;
-    const size_t smem = kQ1AccBytes;
-    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kern, smem));
-    const int per_sm = kernel_occupancy(ctx, (const void*)kern, kQ1SmemThreads, smem);
-    const uint64_t min_blocks = (c.n_rows + (uint64_t)kQ1SmemThreads * kQ1RowsPerThread - 1) /
-                                ((uint64_t)kQ1SmemThreads * kQ1RowsPerThread);
-    const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
-    const int grid = (int)std::max<uint64_t>(
-        1, std::max(min_blocks, std::min<uint64_t>(want, (uint64_t)ctx->sm_count * per_sm)));
-    // 36 u128 accumulators and a ticket, both left at zero by every launch's last block
-    void* part = nullptr;
-    unsigned* ticket = nullptr;
-    int rc = scan_scratch(ctx, "q1.acc", (size_t)6 * kQ1Raw * sizeof(u128), &part, &ticket);
-    if (rc) return rc;
-    GPUDB_LAUNCH(call, kern, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
-                 (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
-                 (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status);
-    return GPUDB_OK;
-  }
+  if (variant == 7 || variant == 8)
+    return launch_q1_smem(call, c, p, out, status, variant == 8 ? q1_vec_smem_kernel<3, 0> : q1_vec_smem_kernel<2, 0>,
+                          Q6Riders{});
   if ((variant == 1 || variant >= 4) && !tma_ok) variant = vec ? 2 : 3;
   if (variant == 2 && !vec) variant = 3;
   if (variant == 1 || variant >= 4) {
@@ -839,6 +876,25 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
                  c.flag, c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status);
   }
   return GPUDB_OK;
+}
+
+int launch_q1_riders(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status,
+                     int n6, const gpudb_q6_params* q6, void* const* q6out) {
+  const bool vec = aligned(c.ship_date, 16) && aligned(c.quantity, 16) && aligned(c.ext_price, 16) &&
+                   aligned(c.discount, 16) && aligned(c.tax, 16) && aligned(c.flag, 4) && aligned(c.status, 4);
+  if (n6 <= 0 || n6 > kMaxRiders || !vec || c.n_rows == 0 || call.ctx()->scan_variant != 0) {
+    int rc = launch_q1(call, c, p, out, status);   // one kernel per request
+    for (int r = 0; !rc && r < n6; r++) rc = launch_q6(call, c, q6[r], q6out[r]);
+    return rc;
+  }
+  Q6Riders rd{};
+  for (int r = 0; r < n6; r++) {
+    rd.p[r] = Q6P{q6[r].ship_lo, q6[r].ship_hi, q6[r].disc_lo, q6[r].disc_hi, q6[r].qty_lt};
+    rd.out[r] = static_cast<unsigned long long*>(q6out[r]);
+  }
+  static constexpr Q1SmemKernel kRiding[kMaxRiders] = {q1_vec_smem_kernel<2, 1>, q1_vec_smem_kernel<2, 2>,
+                                                       q1_vec_smem_kernel<2, 3>, q1_vec_smem_kernel<2, 4>};
+  return launch_q1_smem(call, c, p, out, status, kRiding[n6 - 1], rd);
 }
 
 }  // namespace gpudb

@@ -12,6 +12,12 @@ constexpr size_t kQ1ResultBytes = 6 * 6 * 16;      // 6 groups x {count, qty, ba
 // value outside its exact-arithmetic domain in `status` (the call's status word if null).
 int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, void* out);
 int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status = nullptr);
+// One Q1 scan that also evaluates up to 4 Q6 requests on the rows it reads (one read of the
+// table for all of them); each Q6 request adds into its own kQ6ResultBytes words. Falls back
+// to one kernel per request for columns off 16 bytes, more Q6 requests, or a Q1 kernel
+// variant chosen on the context.
+int launch_q1_riders(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status,
+                     int n6, const gpudb_q6_params* q6, void* const* q6out);
 
 // Host result from the kQ1ResultBytes device words of one Q1 scan.
 void q1_result_from(const uint8_t* words, gpudb_q1_result* out);

@@ -226,3 +226,26 @@ def test_admission_by_footprint(engine, small):
     assert all(s == capi.OK for s in status)
     assert [j.result() for j in jobs] == solo
     assert st["peak_admitted_bytes"] <= big
+
+
+@pytest.mark.parametrize("n6", [1, 2, 4, 5])
+def test_q6_requests_riding_on_one_q1_scan(engine, orc, n6):
+    """One Q1 request and n6 Q6 requests over the same rows: up to four Q6 requests are
+    evaluated by the Q1 kernel on the rows it reads, five go their own way; every result
+    equals the oracle's."""
+    li = orc.lineitem(300_007, seed=31)
+    s = engine.upload("lineitem", li).lineitem()
+    q6s = [(100 + 300 * i, 900 + 300 * i, i % 5, i % 5 + 4, 20 + 5 * i) for i in range(n6)]
+    q6s[-1] = (2000, 1000, 0, 10, 50)   # an empty ship range: nothing matches
+    reqs = (capi.Request * (1 + n6))()
+    o1 = capi.Q1Result()
+    reqs[0].pipeline, reqs[0].li, reqs[0].q1, reqs[0].q1_out = capi.PIPE_Q1, C.pointer(s), capi.Q1Params(1800, 0), C.pointer(o1)
+    o6 = [capi.Q6Result() for _ in q6s]
+    for i, p in enumerate(q6s):
+        r = reqs[1 + i]
+        r.pipeline, r.li, r.q6, r.q6_out = capi.PIPE_Q6, C.pointer(s), capi.Q6Params(*p), C.pointer(o6[i])
+    engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, len(reqs), None, None))
+    assert all(r.status == capi.OK for r in reqs)
+    assert q1_to_dict(o1) == orc.q1(li, 1800)
+    for p, o in zip(q6s, o6):
+        assert (o.revenue, o.rows_matched) == orc.q6(li, *p), p
