@@ -774,18 +774,25 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     te1 = event_get(ctx);
     if (te0) cudaEventRecord(te0, bs);
   }
-  std::vector<uint32_t> scans, host_scans;
-  size_t scan_bytes = 0;
+  // Scans of small tables (at most kSmallScanRows rows) and of large ones are run apart, so
+  // that each group's requests complete when its own work ends.
+  constexpr uint64_t kSmallScanRows = 1ull << 24;
+  std::vector<uint32_t> scan_lists[2], host_scans;   // [0] small tables, [1] large
+  size_t scan_bytes[2] = {0, 0};
   const uint64_t h2d0 = ctx->h2d_total, d2h0 = ctx->d2h_total;
-  auto flush_scans = [&]() -> int {
+  auto flush_scans = [&](int which) -> int {
+    std::vector<uint32_t>& scans = scan_lists[which];
     if (scans.empty()) return GPUDB_OK;
     int rc = run_scan_batch(ctx, reqs, scans, async ? t : nullptr, &aex);
     if (rc) for (uint32_t i : scans) reqs[i].status = rc;
     scans.clear();
-    scan_bytes = 0;
+    scan_bytes[which] = 0;
     return GPUDB_OK;
   };
-  // order on the stream: shared scan passes, then batched Q3 groups, then the other joins
+  // Order on the stream, by work per request (cheapest first, so that the requests of a
+  // group complete early and the ones waiting for the batch's end are few): scans of small
+  // tables, the joins that run alone (identical Q9 requests run once per batch), the batched
+  // Q3 groups, the scans of large tables, then scans of host-resident tables.
   std::map<std::string, std::vector<uint32_t>> q3_groups;   // batchable Q3 by identical tables
   std::vector<uint32_t> joins;
   for (uint32_t i = 0; i < n; i++) {
@@ -810,9 +817,11 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
         // a lone scan runs through its own pipeline (the plain form); several share passes
         if (n > 1 && scan_columns_ok(q)) {
           const size_t b = (q.pipeline == GPUDB_PIPE_Q6 ? kQ6Words : kQ1Words) * 8 + 4;
-          if (scan_bytes + b + 64 > kBigSlotBytes - kSlotHeader) flush_scans();
-          scans.push_back(i);
-          scan_bytes += b;
+          const uint64_t end = q.row_end ? std::min<uint64_t>(q.row_end, q.li->n_rows) : q.li->n_rows;
+          const int which = end - std::min<uint64_t>(q.row_begin, end) > kSmallScanRows ? 1 : 0;
+          if (scan_bytes[which] + b + 64 > kBigSlotBytes - kSlotHeader) flush_scans(which);
+          scan_lists[which].push_back(i);
+          scan_bytes[which] += b;
           break;
         }
         if (n > 1 && host_scan_ok(q)) {   // shares the table's copy into HBM with the others
@@ -841,22 +850,19 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     }
     if (rc != GPUDB_OK) q.status = rc;
   }
-  flush_scans();
-  if (!host_scans.empty()) run_host_scans(ctx, reqs, host_scans, async ? t : nullptr, &aex);
+  flush_scans(0);
   auto set_failed = [&](uint32_t i, int rc) {
     reqs[i].status = rc;
     if (!async)
       for (uint32_t d : hook.dups[i]) reqs[d].status = rc;
   };
+  std::vector<std::vector<uint32_t>> q3_parts;   // groups of 2..kQ3Batch; a group of one runs alone
   for (auto& kv : q3_groups) {
     std::vector<uint32_t>& l = kv.second;
     for (size_t a = 0; a < l.size(); a += kQ3Batch) {
       const size_t b = std::min(l.size(), a + (size_t)kQ3Batch);
-      if (b - a == 1) { joins.push_back(l[a]); continue; }
-      const std::vector<uint32_t> part(l.begin() + a, l.begin() + b);
-      const int rc = q3_batch_run(ctx, reqs, part, &aex);
-      if (rc != GPUDB_OK)
-        for (uint32_t i : part) set_failed(i, rc);
+      if (b - a == 1) joins.push_back(l[a]);
+      else q3_parts.emplace_back(l.begin() + a, l.begin() + b);
     }
   }
   std::sort(joins.begin(), joins.end());
@@ -882,6 +888,13 @@ extern "C" int gpudb_batch_run(gpudb_ctx* ctx, gpudb_request* reqs, uint32_t n, 
     }
     if (rc != GPUDB_OK) set_failed(i, rc);
   }
+  for (const std::vector<uint32_t>& part : q3_parts) {
+    const int rc = q3_batch_run(ctx, reqs, part, &aex);
+    if (rc != GPUDB_OK)
+      for (uint32_t i : part) set_failed(i, rc);
+  }
+  flush_scans(1);
+  if (!host_scans.empty()) run_host_scans(ctx, reqs, host_scans, async ? t : nullptr, &aex);
   if (async) return GPUDB_OK;
   if (te1) cudaEventRecord(te1, bs);
   gpudb_sync(ctx);   // per-request outcomes are in each status

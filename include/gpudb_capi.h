@@ -474,16 +474,20 @@ int gpudb_radix_join_pairs(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n
 /* ---- batched execution (no reference counterpart: the reference runs one query per
  *      command buffer, src/q1.cpp:59-106) ---------------------------------------------
  * One call runs many requests, each with its own exact result and status:
- *  - Q6/Q1 requests over device-resident tables are grouped by (table, row range) and
- *    evaluated in shared passes that read the rows once (up to 8 Q6 per pass; up to 2 Q1
- *    per pass, with 4 Q6 riding along); all passes are persistent launches that pull row
- *    tiles from a device queue, so many small requests cost a few launches in total;
+ *  - Q6/Q1 requests over device-resident tables are grouped by (table, row range): one Q1
+ *    request with up to 4 Q6 requests runs as one Q1 scan that evaluates the Q6 requests on
+ *    the rows it reads; one or two Q1 (up to three Q6) requests alone run their own scans;
+ *    more share passes that read the rows once (up to 8 Q6 per pass; up to 2 Q1 per pass,
+ *    with 4 Q6 riding along), persistent launches that pull row tiles from a device queue;
+ *  - Q6/Q1 requests over the same host-resident table share one chunked copy of it;
  *  - Q3 requests (global mode) over the same tables run in groups of up to 8 that share
  *    every stage's launch and one probe pass over the fact table;
  *  - in a synchronous call, identical Q3/Q9 requests run once and the others get copies;
  *  - a lone request runs through its own pipeline, exactly as the single-request call.
- * Everything is enqueued on one stream; a synchronous call finishes the requests in issue
- * order and times the whole batch in `t`. */
+ * Everything is enqueued on one stream, cheapest work per request first (scans of tables of
+ * at most 2^24 rows, the joins that run alone, the Q3 groups, scans of larger tables, scans
+ * of host-resident tables), and each request completes when its own work has finished; a
+ * synchronous call times the whole batch in `t`. */
 enum { GPUDB_PIPE_Q6 = 1, GPUDB_PIPE_Q1 = 2, GPUDB_PIPE_Q3 = 3, GPUDB_PIPE_Q9 = 4 };
 
 typedef struct gpudb_q3_tables { gpudb_customer cu; gpudb_orders od; gpudb_lineitem li; } gpudb_q3_tables;
