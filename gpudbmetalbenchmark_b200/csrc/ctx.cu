@@ -545,7 +545,7 @@ int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value) {
       ctx->radix_bits = (int)value;
       return GPUDB_OK;
     case GPUDB_OPT_RADIX_SHAPE:
-      if (value < 0 || value > 5) return fail(ctx, GPUDB_E_INVALID, "radix shape must be 0..5");
+      if (value < 0 || value > 7) return fail(ctx, GPUDB_E_INVALID, "radix shape must be 0..7");
       ctx->radix_shape = (int)value;
       return GPUDB_OK;
     case GPUDB_OPT_Q3_AUTO_MODE:

@@ -389,11 +389,13 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
   const int passes = bits <= kRxPassBits ? 1 : 2;
   const int d0 = passes == 1 ? bits : (bits + 1) / 2;
   auto k0 = rx_scatter_kernel<Src, P, PAY, T, I, STG, STABLE>;
-  auto k1 = rx_scatter_kernel<ColumnSource<P>, P, PAY, T, I, STG, STABLE>;
+  // the second pass is always stable: it must keep the first pass's order inside each of its
+  // digits, or the rows of one final partition would not be contiguous
+  auto k1 = rx_scatter_kernel<ColumnSource<P>, P, PAY, T, I, STG, true>;
   const size_t smem0 = rx_scatter_smem<Src, P, PAY, T, I, STG, STABLE>(1u << d0);
   GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k0, smem0));
   if (passes > 1)
-    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k1, rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, STABLE>(1u << (bits - d0))));
+    GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)k1, rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, true>(1u << (bits - d0))));
   const int per_sm = kernel_occupancy(ctx, (const void*)k0, T, smem0);
   const uint64_t sub = (std::max<uint64_t>(n_max, 1) + TILE - 1) / TILE;
   const uint32_t G = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sub, (uint64_t)ctx->sm_count * std::max(per_sm, 1)));
@@ -414,7 +416,7 @@ int rx_partition_shaped(Call& call, const Src& src, uint64_t n_max, int bits, in
     int32_t* ko = pass == passes - 1 ? kout : ktmp;
     P* po = pass == passes - 1 ? pout : ptmp;
     const size_t sm0 = rx_scatter_smem<Src, P, PAY, T, I, STG, STABLE>(F);
-    const size_t sm1 = rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, STABLE>(F);
+    const size_t sm1 = rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, true>(F);
     GPUDB_CUDA(ctx, cudaMemsetAsync(hist, 0, hf * sizeof(uint32_t), s));
     if (pass == 0 && passes > 1) GPUDB_CUDA(ctx, cudaMemsetAsync(full, 0, parts * sizeof(uint32_t), s));
     uint32_t* fullp = (pass == 0 && passes > 1) ? full : nullptr;
@@ -456,17 +458,20 @@ template <class Src, class P, bool PAY, int T, int I, int STG, bool STABLE>
 constexpr bool rx_shape_fits(int bits) {
   const int d0 = bits <= kRxPassBits ? bits : (bits + 1) / 2;
   return rx_scatter_smem<Src, P, PAY, T, I, STG, STABLE>(1u << d0) <= kRxSmemLimit &&
-         rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, STABLE>(1u << (bits - d0 > 0 ? bits - d0 : 0)) <= kRxSmemLimit;
+         rx_scatter_smem<ColumnSource<P>, P, PAY, T, I, STG, true>(1u << (bits - d0 > 0 ? bits - d0 : 0)) <= kRxSmemLimit;
 }
 
 // The scatter block shape of the context (GPUDB_OPT_RADIX_SHAPE): 1 512 threads x 16 rows,
-// 2 256 x 8 (both with direct loads), 3 512 x 8, 4 256 x 8, 5 512 x 16 (each with a
-// two-stage bulk-copy ring); 0 (default) picks 5. A shape whose shared memory does not fit
-// falls back to 3, then 4, then 2. STABLE: rows keep their input order inside a partition.
+// 2 256 x 8 (both with direct loads), 3 512 x 8, 4 256 x 8, 5 512 x 16, 7 256 x 16 (each
+// with a two-stage bulk-copy ring), 6 512 x 16 with a one-stage ring (more blocks per SM);
+// 0 (default) picks 5. A shape whose shared memory does not fit falls back to 3, then 4,
+// then 2. STABLE: rows keep their input order inside a partition.
 template <class Src, class P, bool PAY, bool STABLE>
 int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* kout, P* pout, uint32_t* offsets,
                  int32_t* ktmp, P* ptmp) {
   int shape = call.ctx()->radix_shape ? call.ctx()->radix_shape : 5;
+  if (shape == 6 && !rx_shape_fits<Src, P, PAY, 512, 16, 1, STABLE>(bits)) shape = 3;
+  if (shape == 7 && !rx_shape_fits<Src, P, PAY, 256, 16, 2, STABLE>(bits)) shape = 4;
   if (shape == 5 && !rx_shape_fits<Src, P, PAY, 512, 16, 2, STABLE>(bits)) shape = 3;
   if (shape == 3 && !rx_shape_fits<Src, P, PAY, 512, 8, 2, STABLE>(bits)) shape = 4;
   if (shape == 4 && !rx_shape_fits<Src, P, PAY, 256, 8, 2, STABLE>(bits)) shape = 2;
@@ -479,6 +484,10 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
       return rx_partition_shaped<Src, P, PAY, 256, 8, 2, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
     case 5:
       return rx_partition_shaped<Src, P, PAY, 512, 16, 2, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    case 6:
+      return rx_partition_shaped<Src, P, PAY, 512, 16, 1, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
+    case 7:
+      return rx_partition_shaped<Src, P, PAY, 256, 16, 2, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
     default:
       return rx_partition_shaped<Src, P, PAY, 256, 8, 0, STABLE>(call, src, n_max, bits, kout, pout, offsets, ktmp, ptmp);
   }
@@ -486,7 +495,8 @@ int rx_partition(Call& call, const Src& src, uint64_t n_max, int bits, int32_t* 
 
 // Plain columns (payload = row id when pay is null); the row count may be on the device.
 // STABLE (the C ABI's partitioning) keeps the input order inside each partition; the joins,
-// whose results do not depend on it, take the unstable form.
+// whose results do not depend on it, take the unstable form (for the first pass; a second
+// pass is always stable).
 template <class P, bool STABLE>
 int radix_partition_run(Call& call, const int32_t* keys, const P* pay, uint64_t n_max, const uint32_t* n_dev, int bits,
                         int32_t* keys_out, P* pay_out, uint32_t* offsets, int32_t* keys_tmp, P* pay_tmp) {

@@ -111,9 +111,10 @@ enum {
                                     stream is captured into a CUDA graph once per (tables, parameters)
                                     and replayed after; 0: its kernels are launched one by one */,
   GPUDB_OPT_RADIX_SHAPE = 10,    /* radix scatter block shape: 1 512 threads x 16 rows, 2 256 x 8 (both
-                                    loading rows directly), 3 512 x 8, 4 256 x 8, 5 512 x 16 (each with
-                                    a two-stage bulk-copy ring of sub-tiles); 0 (default) = 5. A shape
-                                    whose shared memory does not fit falls back to 3, 4, then 2 */
+                                    loading rows directly), 3 512 x 8, 4 256 x 8, 5 512 x 16, 7 256 x 16
+                                    (each with a two-stage bulk-copy ring of sub-tiles), 6 512 x 16 with
+                                    a one-stage ring; 0 (default) = 5. A shape whose shared memory does
+                                    not fit falls back to 3, 4, then 2 */
   GPUDB_OPT_Q3_AUTO_MODE = 9     /* what a Q3 call with join_mode GPUDB_JOIN_AUTO runs: -1 (default) the
                                     30% rule (direct map when it fits, else the global table), or
                                     GPUDB_JOIN_GLOBAL / _RADIX / _DIRECT (the autotuner's choice) */

@@ -108,7 +108,7 @@ def test_radix_partition_large_inputs(engine, orc, bits, n):
             engine.device_free(x)
 
 
-@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, 6, 7])
 def test_radix_partition_every_block_shape(engine, orc, shape):
     """Every scatter block shape (GPUDB_OPT_RADIX_SHAPE) gives the oracle's stable partition,
     in one pass (10 bits) and in two (13 bits), and the same join count; columns that start
@@ -193,6 +193,39 @@ def test_radix_join_count_multi_chunk_partition(engine, orc):
     db, dp = engine.to_device(b), engine.to_device(p)
     try:
         assert engine.hash_join_count(db, len(b), dp, len(p), capi.JOIN_RADIX) == orc.join_count(b, p)
+    finally:
+        for x in (db, dp):
+            engine.device_free(x)
+
+
+def test_radix_join_pairs_in_two_passes(engine, orc):
+    """2.1M build rows need 11 partition bits (two passes): every pair is found once."""
+    rng = np.random.default_rng(41)
+    b = (rng.permutation(2_100_000) * 3).astype(np.int32)
+    p = rng.integers(0, 7_000_000, 2_500_000).astype(np.int32)
+    want = np.sort(p[(p % 3 == 0) & (p < 6_300_000)])
+    db, dp = engine.to_device(b), engine.to_device(p)
+    ob, op = engine.device_array(len(want) * 4 + 4), engine.device_array(len(want) * 4 + 4)
+    try:
+        n = engine.radix_join_pairs(db, len(b), dp, len(p), ob, op, len(want))
+        assert n == len(want)
+        bk = b[engine.to_host(ob, n, np.int32)]
+        pk = p[engine.to_host(op, n, np.int32)]
+        assert np.array_equal(bk, pk)                 # each pair joins equal keys
+        assert np.array_equal(np.sort(pk), want)      # and every matching probe row once
+    finally:
+        for x in (db, dp, ob, op):
+            engine.device_free(x)
+
+
+def test_radix_join_count_in_two_passes(engine):
+    """16M distinct build keys need 11 partition bits in the count (two passes)."""
+    b = (np.arange(16_000_000, dtype=np.int64) * 2).astype(np.int32)
+    p = np.random.default_rng(43).integers(0, 40_000_000, 20_000_000).astype(np.int32)
+    want = int(((p % 2 == 0) & (p < 32_000_000)).sum())
+    db, dp = engine.to_device(b), engine.to_device(p)
+    try:
+        assert engine.hash_join_count(db, len(b), dp, len(p), capi.JOIN_RADIX) == want
     finally:
         for x in (db, dp):
             engine.device_free(x)

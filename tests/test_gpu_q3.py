@@ -194,3 +194,11 @@ def test_q3_10x_configuration(engine, orc, mode):
     """Config 2 at 10x rows: 1.5M customers, 15M orders, 60M lineitem rows."""
     cu, od, li = orc.q3_tables(1_500_000, 15_000_000, 60_000_000, 42)
     assert run(engine, cu, od, li, mode) == orc.q3(cu, od, li)
+
+
+@pytest.mark.parametrize("bits", [11, 12, 13])
+def test_q3_radix_in_two_passes(engine, orc, bits):
+    """More than 1024 partitions take two partitioning passes (the second stable, so each
+    final partition stays contiguous): the result equals the oracle's."""
+    cu, od, li = orc.q3_tables(3000, 20000, 80000, 5)
+    assert run(engine, cu, od, li, capi.JOIN_RADIX, radix_bits=bits) == orc.q3(cu, od, li)
