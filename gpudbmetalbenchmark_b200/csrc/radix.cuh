@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kRxThreads) rx_hist_kernel(Src src, uint32_t G
 template <class Src, class P, bool PAY, int T, int I, int STG, bool STABLE>
 __host__ __device__ constexpr size_t rx_scatter_smem(uint32_t F) {
   return (size_t)STG * Src::template stage_bytes<PAY>(T * I) + (PAY ? sizeof(P) * T * I : 0) +
-         (sizeof(int32_t) + sizeof(uint16_t)) * T * I +
+         (sizeof(int32_t) + sizeof(uint32_t)) * T * I +
          (STABLE ? sizeof(uint16_t) * (T / 32) * F : 2 * sizeof(uint32_t) * F) + sizeof(uint32_t) * F;
 }
 
@@ -199,8 +199,8 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
   unsigned char* ring = rx_smem;
   P* spay = reinterpret_cast<P*>(rx_smem + STG * SB);
   int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + STG * SB + (PAY ? sizeof(P) * TILE : 0));
-  uint16_t* sdig = reinterpret_cast<uint16_t*>(skey + TILE);            // digit of each staged row
-  uint16_t* wcnt = sdig + TILE;                                         // stable: [warp][digit]
+  uint32_t* sout = reinterpret_cast<uint32_t*>(skey + TILE);            // output row of each staged row
+  uint16_t* wcnt = reinterpret_cast<uint16_t*>(sout + TILE);            // stable: [warp][digit]
   uint32_t* cnt = reinterpret_cast<uint32_t*>(wcnt);                    // unstable: [digit] counts
   uint32_t* start = cnt + F;                                            // unstable: [digit] staged starts
   uint32_t* cur = STABLE ? reinterpret_cast<uint32_t*>(wcnt + W * F) : start + F;   // next output row per digit
@@ -323,24 +323,29 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
       if (threadIdx.x == T - 1) s_total = inc;
     }
     __syncthreads();
+    // stage digit-sorted, with each row's output row (its digit's cursor plus its rank
+    // among the sub-tile's rows of that digit)
 #pragma unroll
     for (int j = 0; j < I; j++)
       if (dr[j] != ~0u) {
-        const uint32_t d = dr[j] >> 16;
-        const uint32_t pos = (STABLE ? (uint32_t)mine[d] : start[d]) + (dr[j] & 0xFFFFu);
+        const uint32_t d = dr[j] >> 16, rank = dr[j] & 0xFFFFu;
+        const uint32_t pos = (STABLE ? (uint32_t)mine[d] : start[d]) + rank;
         skey[pos] = key[j];
-        sdig[pos] = (uint16_t)d;
+        sout[pos] = cur[d] + (STABLE ? pos - (uint32_t)wcnt[d] : rank);
         if (PAY) spay[pos] = pay[j];
       }
     __syncthreads();
     // write out: consecutive threads take consecutive staged rows, i.e. consecutive output
-    // rows inside each digit's run
+    // rows inside each digit's run; the I rows of a thread are independent
     const uint32_t m = s_total;
-    for (uint32_t i = threadIdx.x; i < m; i += T) {
-      const uint32_t d = sdig[i];
-      const uint32_t o = cur[d] + (i - (STABLE ? (uint32_t)wcnt[d] : start[d]));
-      kout[o] = skey[i];
-      if (PAY) pout[o] = spay[i];
+#pragma unroll
+    for (int j = 0; j < I; j++) {
+      const uint32_t i = threadIdx.x + (uint32_t)j * T;
+      if (i < m) {
+        const uint32_t o = sout[i];
+        kout[o] = skey[i];
+        if (PAY) pout[o] = spay[i];
+      }
     }
     __syncthreads();
     if (STABLE) {
