@@ -87,16 +87,22 @@ __global__ void __launch_bounds__(kPJThreads) partition_pairs_kernel(
 // with a kPCCap-slot shared table (128 KB), so a partition of up to kPCChunk build keys is one
 // chunk and one 10-bit pass per side covers 15M build rows. Partitions whose build side needs
 // more than one chunk mark matches in `flags` (one byte per partitioned probe row) and count
-// them after the last chunk. Each thread keeps kPCRows probe keys in flight.
+// them after the last chunk. Each thread keeps kPCRows build or probe keys in flight (the
+// kernel waits on those loads otherwise). A key's slot comes from the bits of its partition
+// hash above the `pbits` partition bits, so it is independent of the partition.
 constexpr int kPCThreads = 1024;
 constexpr uint32_t kPCCap = 32768;
 constexpr uint32_t kPCChunk = kPCCap / 2;
 constexpr uint64_t kCountRowsPerPartition = 15360;   // average build keys per partition (<= kPCChunk with margin)
-constexpr int kPCRows = 4;
+constexpr int kPCRows = 16;
 
-__global__ void __launch_bounds__(kPCThreads) partition_count_kernel(
+__device__ __forceinline__ uint32_t pc_slot(int32_t key, int pbits) {
+  return (key_hash32(key) >> pbits) & (kPCCap - 1);
+}
+
+__global__ void __launch_bounds__(kPCThreads, 1) partition_count_kernel(
     const int32_t* __restrict__ bk, const uint32_t* __restrict__ boff, const int32_t* __restrict__ pk,
-    const uint32_t* __restrict__ poff, uint8_t* flags, unsigned long long* count) {
+    const uint32_t* __restrict__ poff, int pbits, uint8_t* flags, unsigned long long* count) {
   extern __shared__ __align__(16) int32_t pc_key[];
   const uint32_t part = blockIdx.x, mask = kPCCap - 1;
   const uint32_t b0 = boff[part], b1 = boff[part + 1], p0 = poff[part], p1 = poff[part + 1];
@@ -110,11 +116,20 @@ __global__ void __launch_bounds__(kPCThreads) partition_count_kernel(
       reinterpret_cast<int4*>(pc_key)[i] = make_int4(kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey);
     __syncthreads();
     // duplicates take their own slots; a chunk fills at most half the table
-    for (uint32_t i = c0 + threadIdx.x; i < c1; i += kPCThreads) {
-      const int32_t k = __ldg(bk + i);
-      uint32_t s = key_slot(k, mask);
-      for (uint32_t t = 0; t < kPCCap; t++, s = (s + 1) & mask)
-        if (atomicCAS(&pc_key[s], kEmptyKey, k) == kEmptyKey) break;
+    for (uint32_t i0 = c0 + threadIdx.x; i0 < c1; i0 += kPCRows * kPCThreads) {
+      int32_t k[kPCRows];
+#pragma unroll
+      for (int u = 0; u < kPCRows; u++) {
+        const uint32_t i = i0 + u * kPCThreads;
+        k[u] = i < c1 ? __ldcs(bk + i) : kEmptyKey;
+      }
+#pragma unroll
+      for (int u = 0; u < kPCRows; u++) {
+        if (k[u] == kEmptyKey) continue;   // (an INT32_MIN key marks an empty slot and never matches)
+        uint32_t s = pc_slot(k[u], pbits);
+        for (uint32_t t = 0; t < kPCCap; t++, s = (s + 1) & mask)
+          if (atomicCAS(&pc_key[s], kEmptyKey, k[u]) == kEmptyKey) break;
+      }
     }
     __syncthreads();
     for (uint32_t i0 = p0 + threadIdx.x; i0 < p1; i0 += kPCRows * kPCThreads) {
@@ -128,7 +143,7 @@ __global__ void __launch_bounds__(kPCThreads) partition_count_kernel(
       for (int u = 0; u < kPCRows; u++) {
         bool hit = false;
         if (k[u] != kEmptyKey)
-          for (uint32_t s = key_slot(k[u], mask), t = 0; t < kPCCap; t++, s = (s + 1) & mask) {
+          for (uint32_t s = pc_slot(k[u], pbits), t = 0; t < kPCCap; t++, s = (s + 1) & mask) {
             const int32_t h = pc_key[s];
             if (h == k[u]) { hit = true; break; }
             if (h == kEmptyKey) break;
@@ -197,7 +212,7 @@ int radix_join_count(Call& call, const int32_t* build_keys, uint64_t n_build, co
   const size_t smem = kPCCap * sizeof(int32_t);
   GPUDB_CUDA(call.ctx(), kernel_smem(call.ctx(), (const void*)partition_count_kernel, smem));
   GPUDB_LAUNCH(call, partition_count_kernel, 1u << bits, kPCThreads, smem, (const int32_t*)s.bk, (const uint32_t*)s.boff,
-               (const int32_t*)s.pk, (const uint32_t*)s.poff, (uint8_t*)flags, count);
+               (const int32_t*)s.pk, (const uint32_t*)s.poff, bits, (uint8_t*)flags, count);
   return GPUDB_OK;
 }
 

@@ -198,12 +198,12 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
   const uint32_t F = 1u << dbits, dmask = F - 1;
   unsigned char* ring = rx_smem;
   P* spay = reinterpret_cast<P*>(rx_smem + STG * SB);
-  int32_t* skey = reinterpret_cast<int32_t*>(rx_smem + STG * SB + (PAY ? sizeof(P) * TILE : 0));
-  uint32_t* sout = reinterpret_cast<uint32_t*>(skey + TILE);            // output row of each staged row
-  uint16_t* wcnt = reinterpret_cast<uint16_t*>(sout + TILE);            // stable: [warp][digit]
-  uint32_t* cnt = reinterpret_cast<uint32_t*>(wcnt);                    // unstable: [digit] counts
-  uint32_t* start = cnt + F;                                            // unstable: [digit] staged starts
-  uint32_t* cur = STABLE ? reinterpret_cast<uint32_t*>(wcnt + W * F) : start + F;   // next output row per digit
+  // staged rows as (key, output row) pairs, one 8-byte access each way
+  int2* sko = reinterpret_cast<int2*>(rx_smem + STG * SB + (PAY ? sizeof(P) * TILE : 0));
+  uint16_t* wcnt = reinterpret_cast<uint16_t*>(sko + TILE);             // stable: [warp][digit]
+  uint32_t* cur = reinterpret_cast<uint32_t*>(wcnt + W * F);            // stable: next output row per digit
+  uint2* sc = reinterpret_cast<uint2*>(sko + TILE);                     // unstable: [digit] {staged start, next output row}
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(sc + F);                  // unstable: [digit] counts
   __shared__ uint32_t wt[W];
   __shared__ uint32_t s_total;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -218,11 +218,15 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
     for (int q = 0; q < NS; q++) mbar_init(&full[q], 1);
     mbar_fence_init();
   }
-  for (uint32_t d = threadIdx.x; d < F; d += T) cur[d] = offs[(size_t)d * G + blockIdx.x];
-  if (STABLE)
+  if (STABLE) {
+    for (uint32_t d = threadIdx.x; d < F; d += T) cur[d] = offs[(size_t)d * G + blockIdx.x];
     for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
-  else
-    for (uint32_t d = threadIdx.x; d < F; d += T) cnt[d] = 0;
+  } else {
+    for (uint32_t d = threadIdx.x; d < F; d += T) {
+      sc[d] = make_uint2(0u, offs[(size_t)d * G + blockIdx.x]);
+      cnt[d] = 0;
+    }
+  }
   __syncthreads();
   if (STG > 0 && threadIdx.x == 0)
     for (uint64_t q = 0; q < nring && q < (uint64_t)NS; q++)
@@ -317,7 +321,7 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
       const uint32_t inc = rx_block_scan<T>(sum, wt);
       uint32_t run = inc - sum;
       for (uint32_t b = b0; b < b1; b++) {
-        start[b] = run;
+        sc[b].x = run;
         run += cnt[b];
       }
       if (threadIdx.x == T - 1) s_total = inc;
@@ -329,9 +333,16 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
     for (int j = 0; j < I; j++)
       if (dr[j] != ~0u) {
         const uint32_t d = dr[j] >> 16, rank = dr[j] & 0xFFFFu;
-        const uint32_t pos = (STABLE ? (uint32_t)mine[d] : start[d]) + rank;
-        skey[pos] = key[j];
-        sout[pos] = cur[d] + (STABLE ? pos - (uint32_t)wcnt[d] : rank);
+        uint32_t pos, o;
+        if (STABLE) {
+          pos = (uint32_t)mine[d] + rank;
+          o = cur[d] + pos - (uint32_t)wcnt[d];
+        } else {
+          const uint2 v = sc[d];
+          pos = v.x + rank;
+          o = v.y + rank;
+        }
+        sko[pos] = make_int2(key[j], (int32_t)o);
         if (PAY) spay[pos] = pay[j];
       }
     __syncthreads();
@@ -342,9 +353,9 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
     for (int j = 0; j < I; j++) {
       const uint32_t i = threadIdx.x + (uint32_t)j * T;
       if (i < m) {
-        const uint32_t o = sout[i];
-        kout[o] = skey[i];
-        if (PAY) pout[o] = spay[i];
+        const int2 v = sko[i];
+        kout[(uint32_t)v.y] = v.x;
+        if (PAY) pout[(uint32_t)v.y] = spay[i];
       }
     }
     __syncthreads();
@@ -357,7 +368,7 @@ __global__ void __launch_bounds__(T) rx_scatter_kernel(Src src, uint32_t G, int 
       for (uint32_t i = threadIdx.x; i < W * F; i += T) wcnt[i] = 0;
     } else {
       for (uint32_t d = threadIdx.x; d < F; d += T) {
-        cur[d] += cnt[d];
+        sc[d].y += cnt[d];
         cnt[d] = 0;
       }
     }
