@@ -575,6 +575,7 @@ __global__ void __launch_bounds__(kFactThreads) q3_fact_filter_kernel(
 
 constexpr uint32_t kQ3PartCap = 4096;               // shared slots per partition table
 constexpr uint32_t kQ3PartChunk = kQ3PartCap / 2;   // build rows per chunk
+constexpr int kQ3PartGroups = 4;                    // 32-row groups a warp loads at once in q3_partition_kernel
 
 constexpr size_t q3_partition_smem() { return (size_t)kQ3PartCap * (8 + 4 + 4 + 4); }
 
@@ -609,15 +610,28 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
       }
     }
     __syncthreads();
-    // the partition keeps the input order, so an order's rows are adjacent: whole warps take
-    // 32 rows at a time, runs of equal keys are summed across their lanes (segmented shuffle
-    // scan) and the last lane of a run probes and adds once for the run
+    // an order's fact rows arrive mostly adjacent (compacted in row order; the partitioning
+    // moves a sub-tile's rows of one digit together): whole warps take 32 rows at a time, runs
+    // of equal keys are summed across their lanes (segmented shuffle scan) and the last lane of
+    // a run probes and adds once for the run. A warp loads kQ3PartGroups groups of 32 rows
+    // before it works on the first, so their loads are in flight together.
     const int lane = threadIdx.x & 31;
-    for (uint32_t base = p0 + (threadIdx.x & ~31u); base < p1; base += kTopkThreads) {
-      const uint32_t i = base + lane;
+    for (uint32_t gbase = p0 + (threadIdx.x & ~31u) * kQ3PartGroups; gbase < p1;
+         gbase += kTopkThreads * kQ3PartGroups) {
+     int32_t gkey[kQ3PartGroups];
+     long long gval[kQ3PartGroups];
+#pragma unroll
+     for (int g = 0; g < kQ3PartGroups; g++) {
+       const uint32_t i = gbase + g * 32 + lane;
+       gkey[g] = i < p1 ? pk[i] : kEmptyKey;
+       gval[g] = i < p1 ? (long long)pval[i] : 0ll;
+     }
+#pragma unroll
+     for (int g = 0; g < kQ3PartGroups; g++) {
+      const uint32_t i = gbase + g * 32 + lane;
       const bool valid = i < p1;
-      const int32_t key = valid ? pk[i] : kEmptyKey;
-      long long v = valid ? (long long)pval[i] : 0ll;
+      const int32_t key = gkey[g];
+      long long v = gval[g];
       uint32_t c = valid ? 1u : 0u;
       const int32_t prev = __shfl_up_sync(FULL_MASK, key, 1);
       const uint32_t heads = __ballot_sync(FULL_MASK, lane == 0 || key != prev);
@@ -636,6 +650,7 @@ __global__ void __launch_bounds__(kTopkThreads) q3_partition_kernel(
         if (hk == key) { atomicAdd(&hrev[s], (unsigned long long)v); atomicAdd(&hhit[s], c); break; }
         if (hk == kEmptyKey) break;
       }
+     }
     }
     __syncthreads();
     // append the chunk's groups: thread t owns slots [t * kPerThread, (t + 1) * kPerThread)
