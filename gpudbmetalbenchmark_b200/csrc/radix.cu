@@ -123,20 +123,12 @@ __global__ void __launch_bounds__(kPCThreads, 1) partition_count_kernel(
         const uint32_t i = i0 + u * kPCThreads;
         k[u] = i < c1 ? __ldcs(bk + i) : kEmptyKey;
       }
-      // inserts in lockstep rounds too (an INT32_MIN key marks an empty slot and never matches)
-      uint32_t slot[kPCRows], open = 0;
 #pragma unroll
       for (int u = 0; u < kPCRows; u++) {
-        slot[u] = pc_slot(k[u], pbits);
-        open |= (uint32_t)(k[u] != kEmptyKey) << u;
-      }
-      for (uint32_t t = 0; open && t < kPCCap; t++) {
-#pragma unroll
-        for (int u = 0; u < kPCRows; u++) {
-          if (!((open >> u) & 1u)) continue;
-          if (atomicCAS(&pc_key[slot[u]], kEmptyKey, k[u]) == kEmptyKey) open &= ~(1u << u);
-          else slot[u] = (slot[u] + 1) & mask;
-        }
+        if (k[u] == kEmptyKey) continue;   // (an INT32_MIN key marks an empty slot and never matches)
+        uint32_t s = pc_slot(k[u], pbits);
+        for (uint32_t t = 0; t < kPCCap; t++, s = (s + 1) & mask)
+          if (atomicCAS(&pc_key[s], kEmptyKey, k[u]) == kEmptyKey) break;
       }
     }
     __syncthreads();
@@ -147,32 +139,19 @@ __global__ void __launch_bounds__(kPCThreads, 1) partition_count_kernel(
         const uint32_t i = i0 + u * kPCThreads;
         k[u] = i < p1 ? __ldcs(pk + i) : kEmptyKey;
       }
-      // linear probing of the kPCRows keys in lockstep rounds: one shared load per unresolved
-      // key per round, so the keys' loads overlap instead of forming kPCRows dependent chains
-      uint32_t slot[kPCRows], open = 0, hit = 0;
+      // (probing the kPCRows keys in lockstep rounds was slower: a warp then runs as many
+      // rounds as the longest probe chain among its 512 keys)
 #pragma unroll
       for (int u = 0; u < kPCRows; u++) {
-        slot[u] = pc_slot(k[u], pbits);
-        open |= (uint32_t)(k[u] != kEmptyKey) << u;
-      }
-      for (uint32_t t = 0; open && t < kPCCap; t++) {
-        int32_t h[kPCRows];
-#pragma unroll
-        for (int u = 0; u < kPCRows; u++) h[u] = ((open >> u) & 1u) ? pc_key[slot[u]] : kEmptyKey;
-#pragma unroll
-        for (int u = 0; u < kPCRows; u++) {
-          if (!((open >> u) & 1u)) continue;
-          if (h[u] == k[u]) { hit |= 1u << u; open &= ~(1u << u); }
-          else if (h[u] == kEmptyKey) open &= ~(1u << u);
-          else slot[u] = (slot[u] + 1) & mask;
-        }
-      }
-      if (multi) {
-#pragma unroll
-        for (int u = 0; u < kPCRows; u++)
-          if ((hit >> u) & 1u) flags[i0 + u * kPCThreads] = 1;
-      } else {
-        c += __popc(hit);
+        bool hit = false;
+        if (k[u] != kEmptyKey)
+          for (uint32_t s = pc_slot(k[u], pbits), t = 0; t < kPCCap; t++, s = (s + 1) & mask) {
+            const int32_t h = pc_key[s];
+            if (h == k[u]) { hit = true; break; }
+            if (h == kEmptyKey) break;
+          }
+        if (multi) { if (hit) flags[i0 + u * kPCThreads] = 1; }
+        else c += hit;
       }
     }
     __syncthreads();
