@@ -280,7 +280,7 @@ class Request(C.Structure):
 
 
 class ServeConfig(C.Structure):
-    _fields_ = [("device", C.c_int32), ("lanes", C.c_uint32), ("max_batch", C.c_uint32), ("reserved", C.c_uint32),
+    _fields_ = [("device", C.c_int32), ("lanes", C.c_uint32), ("max_batch", C.c_uint32), ("heavy_lanes", C.c_uint32),
                 ("memory_budget", C.c_uint64)]
 
 

@@ -29,7 +29,17 @@ struct Ticket {
   double t_submit = 0, t_done = 0;
   uint64_t footprint = 0;
   bool done = false;
+  bool heavy = false;   // a scan of a large table (the heavy lanes' class)
 };
+
+// A Q6/Q1 request over more than 2^24 rows: the scans that end a batch (about 0.3 ms for a
+// Q1 and a Q6 over 60M rows). With heavy lanes configured, only those lanes take them.
+constexpr uint64_t kHeavyRows = 1ull << 24;
+bool heavy_request(const gpudb_request* r) {
+  if ((r->pipeline != GPUDB_PIPE_Q6 && r->pipeline != GPUDB_PIPE_Q1) || !r->li) return false;
+  const uint64_t end = r->row_end ? std::min<uint64_t>(r->row_end, r->li->n_rows) : r->li->n_rows;
+  return end - std::min<uint64_t>(r->row_begin, end) > kHeavyRows;
+}
 
 }  // namespace
 
@@ -103,6 +113,20 @@ struct gpudb_server {
     cv_work.notify_all();
   }
 
+  // Whether `lane` takes ticket `id`: every lane takes everything unless heavy lanes are
+  // configured; then the last heavy_lanes lanes take the heavy requests, the others the rest.
+  bool takes(size_t lane, uint64_t id) {
+    const uint32_t h = cfg.heavy_lanes;
+    if (h == 0 || h >= lanes.size()) return true;
+    return tickets[id].heavy == (lane >= lanes.size() - h);
+  }
+  // The first queued request of the lane's class (queue.end() if none).
+  std::deque<uint64_t>::iterator first_of(size_t lane) {
+    auto it = queue.begin();
+    while (it != queue.end() && !takes(lane, *it)) ++it;
+    return it;
+  }
+
   void work(size_t lane) {
     gpudb_ctx* ctx = lanes[lane];
     std::vector<gpudb_request> batch;
@@ -112,19 +136,23 @@ struct gpudb_server {
     for (;;) {
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] {
-          return closing || (!warming && !queue.empty() && fits(tickets[queue.front()].footprint));
-        });
-        if (queue.empty() && closing) return;
-        if (warming || queue.empty() || !fits(tickets[queue.front()].footprint)) continue;
+        auto ready = [&] {
+          if (warming) return false;
+          auto it = first_of(lane);
+          return it != queue.end() && fits(tickets[*it].footprint);
+        };
+        cv_work.wait(lk, [&] { return closing || ready(); });
+        if (closing && first_of(lane) == queue.end()) return;
+        if (!ready()) continue;
         ids.clear();
         uint64_t bytes = 0;
-        while (!queue.empty() && ids.size() < cfg.max_batch) {
-          const uint64_t fp = tickets[queue.front()].footprint;
+        for (auto it = queue.begin(); it != queue.end() && ids.size() < cfg.max_batch;) {
+          if (!takes(lane, *it)) { ++it; continue; }
+          const uint64_t fp = tickets[*it].footprint;
           if (!ids.empty() && !fits(bytes + fp)) break;   // keep arrival order: stop at the first misfit
           bytes += fp;
-          ids.push_back(queue.front());
-          queue.pop_front();
+          ids.push_back(*it);
+          it = queue.erase(it);
         }
         admitted_bytes += bytes;
         stats.peak_admitted_bytes = std::max(stats.peak_admitted_bytes, admitted_bytes);
@@ -152,6 +180,7 @@ struct gpudb_server {
 
 extern "C" int gpudb_serve_open(const gpudb_serve_config* cfg, gpudb_server** out) {
   if (!cfg || !out || cfg->lanes < 1 || cfg->lanes > 16 || cfg->max_batch < 1) return GPUDB_E_INVALID;
+  if (cfg->heavy_lanes && cfg->heavy_lanes >= cfg->lanes) return GPUDB_E_INVALID;
   *out = nullptr;
   gpudb_server* s = new gpudb_server();
   s->cfg = *cfg;
@@ -226,11 +255,12 @@ extern "C" int gpudb_serve_submit(gpudb_server* s, gpudb_request* req, uint64_t*
     t.req = req;
     t.t_submit = now_ms();
     t.footprint = fp;
+    t.heavy = heavy_request(req);
     s->queue.push_back(id);
     s->stats.submitted++;
     *ticket = id;
   }
-  s->cv_work.notify_one();
+  s->cv_work.notify_all();   // (with heavy lanes, only a lane of the request's class can take it)
   return GPUDB_OK;
 }
 

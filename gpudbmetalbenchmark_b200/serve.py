@@ -26,9 +26,10 @@ from .engine import Engine, Q1_COLS
 
 
 class Server:
-    def __init__(self, device=0, lanes=2, max_batch=64, memory_budget=0):
+    def __init__(self, device=0, lanes=2, max_batch=64, memory_budget=0, heavy_lanes=0):
         self.lib = capi.load()
-        cfg = capi.ServeConfig(device=device, lanes=lanes, max_batch=max_batch, memory_budget=memory_budget)
+        cfg = capi.ServeConfig(device=device, lanes=lanes, max_batch=max_batch, memory_budget=memory_budget,
+                               heavy_lanes=heavy_lanes)
         h = C.c_void_p()
         rc = self.lib.gpudb_serve_open(C.byref(cfg), C.byref(h))
         if rc != capi.OK:
@@ -224,9 +225,9 @@ def open_loop(server, jobs, rate, seed):
     return lat, status, wall
 
 
-def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None):
+def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None, heavy_lanes=0):
     jobs = wl.jobs(n, seed)
-    srv = Server(lanes=lanes, max_batch=max_batch)
+    srv = Server(lanes=lanes, max_batch=max_batch, heavy_lanes=heavy_lanes if lanes > 1 else 0)
     try:
         # one batch of the largest size on every lane sizes the lanes' scratch before timing
         srv.warmup(wl.jobs(max(max_batch, 16), seed + 7))
@@ -238,7 +239,8 @@ def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None):
     exact = None
     if check is not None:
         exact = all(j.result() == w for j, w in zip(jobs, check))
-    return {"mode": name, "lanes": lanes, "max_batch": max_batch, "offered_qps": rate, "requests": n,
+    return {"mode": name, "lanes": lanes, "heavy_lanes": heavy_lanes if lanes > 1 else 0, "max_batch": max_batch,
+            "offered_qps": rate, "requests": n,
             "achieved_qps": n / wall, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mean_batch":
             st["completed"] / max(1, st["batches"]), "all_ok": ok, "bit_exact_vs_solo": exact,
             "by_class": latency_by_class(jobs, lat)}
@@ -248,9 +250,12 @@ def run_mode(engine, wl, name, lanes, max_batch, rate, n, seed, check=None):
 # 5.2/4.4/4.7/5-21/8.0 ms on one B200 (two lanes overlap two batches on the GPU; more lanes
 # contend for it, one leaves it idle between batches).
 DEFAULT_LANES = 2
+# Lanes of those that take only the scans of large tables (gpudb_serve_config.heavy_lanes).
+DEFAULT_HEAVY_LANES = 0
 
 
-def compare(eng, seconds=1.0, lanes=DEFAULT_LANES, max_batch=64, loads=(0.5, 0.85), factor=3.0, seed=11):
+def compare(eng, seconds=1.0, lanes=DEFAULT_LANES, max_batch=64, loads=(0.5, 0.85), factor=3.0, seed=11,
+            heavy_lanes=DEFAULT_HEAVY_LANES):
     """Served form against the plain one-query-per-launch form on the same mixed stream.
 
     1. plain saturation: requests submitted back to back (closed loop), queries/s;
@@ -262,7 +267,7 @@ def compare(eng, seconds=1.0, lanes=DEFAULT_LANES, max_batch=64, loads=(0.5, 0.8
     4. served saturation (closed loop).
     Every result of every run is compared with the same request run alone."""
     wl = Workload(eng)
-    out = {"lanes": lanes, "max_batch": max_batch, "seconds_per_rate": seconds,
+    out = {"lanes": lanes, "heavy_lanes": heavy_lanes, "max_batch": max_batch, "seconds_per_rate": seconds,
            "workload": "Q6/Q1 over lineitem at 1M/6M/60M rows, Q3 at config-2 1x, Q9 at 6M fact rows; "
                        "random pipeline and constants per request, Poisson arrivals"}
     solos = {}
@@ -270,7 +275,7 @@ def compare(eng, seconds=1.0, lanes=DEFAULT_LANES, max_batch=64, loads=(0.5, 0.8
     def run(name, ln, mb, rate, n, sd):
         if (n, sd) not in solos:
             solos[(n, sd)] = wl.solo_results(wl.jobs(n, sd))
-        return _run_checked(eng, wl, name, ln, mb, rate, n, sd, wl.jobs(n, sd), solos[(n, sd)])
+        return _run_checked(eng, wl, name, ln, mb, rate, n, sd, wl.jobs(n, sd), solos[(n, sd)], heavy_lanes)
 
     runs = []
     sat = run("plain", 1, 1, 1e9, 3000, seed)
@@ -300,8 +305,8 @@ def compare(eng, seconds=1.0, lanes=DEFAULT_LANES, max_batch=64, loads=(0.5, 0.8
     return out
 
 
-def _run_checked(eng, wl, name, lanes, max_batch, rate, n, seed, jobs, solo):
-    srv = Server(lanes=lanes, max_batch=max_batch)
+def _run_checked(eng, wl, name, lanes, max_batch, rate, n, seed, jobs, solo, heavy_lanes=0):
+    srv = Server(lanes=lanes, max_batch=max_batch, heavy_lanes=heavy_lanes if lanes > 1 else 0)
     try:
         srv.warmup(wl.jobs(max(max_batch, 16), seed + 7))
         lat, status, wall = open_loop(srv, jobs, rate, seed + 1)
@@ -320,6 +325,8 @@ def main(argv=None):
     ap.add_argument("--rates", type=float, nargs="*", default=[1000, 2000, 4000, 8000, 16000, 32000])
     ap.add_argument("--seconds", type=float, default=2.0)
     ap.add_argument("--lanes", type=int, default=DEFAULT_LANES)
+    ap.add_argument("--heavy-lanes", type=int, default=DEFAULT_HEAVY_LANES,
+                    help="lanes that take only the scans of tables over 2^24 rows (0: every lane takes all)")
     ap.add_argument("--max-batch", type=int, default=64)
     ap.add_argument("--modes", nargs="*", default=["plain", "served"], choices=["plain", "served"])
     ap.add_argument("--compare", action="store_true",
@@ -327,7 +334,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     eng = Engine(0)
     if a.compare:
-        print(json.dumps(compare(eng, seconds=a.seconds, lanes=a.lanes, max_batch=a.max_batch)), flush=True)
+        print(json.dumps(compare(eng, seconds=a.seconds, lanes=a.lanes, max_batch=a.max_batch,
+                                 heavy_lanes=a.heavy_lanes)), flush=True)
         eng.close()
         return 0
     wl = Workload(eng)
@@ -338,7 +346,7 @@ def main(argv=None):
         for name, lanes, mb in (("plain", 1, 1), ("served", a.lanes, a.max_batch)):
             if name not in a.modes:
                 continue
-            res = run_mode(eng, wl, name, lanes, mb, rate, n, seed, check=solo)
+            res = run_mode(eng, wl, name, lanes, mb, rate, n, seed, check=solo, heavy_lanes=a.heavy_lanes)
             print(json.dumps(res), flush=True)
     eng.close()
     return 0

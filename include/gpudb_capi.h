@@ -599,7 +599,10 @@ typedef struct gpudb_serve_config {
   int32_t device;
   uint32_t lanes;            /* worker lanes (contexts), 1..16 */
   uint32_t max_batch;        /* requests per batch, >= 1 */
-  uint32_t reserved;
+  uint32_t heavy_lanes;      /* 0: every lane takes every request; else the last heavy_lanes lanes
+                                take only Q6/Q1 requests over more than 2^24 rows and the others
+                                the rest (a long scan never holds up short requests); must be
+                                below `lanes` */
   uint64_t memory_budget;    /* bytes of predicted device footprint admitted at once; 0 = no limit */
 } gpudb_serve_config;
 typedef struct gpudb_serve_stats {

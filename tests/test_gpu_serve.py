@@ -249,3 +249,26 @@ def test_q6_requests_riding_on_one_q1_scan(engine, orc, n6):
     assert q1_to_dict(o1) == orc.q1(li, 1800)
     for p, o in zip(q6s, o6):
         assert (o.revenue, o.rows_matched) == orc.q6(li, *p), p
+
+
+def test_heavy_lane_takes_the_large_scans(engine):
+    """With a heavy lane, scans of a table over 2^24 rows go to it and everything else to the
+    other lanes; every result is the same as alone, and a config with no light lane is refused."""
+    wl = Workload(engine, scan_rows=(100_003, 20_000_000), q3=(3000, 30_000, 120_000),
+                  q9=(4000, 400, 20_000, 100_000))
+    jobs = wl.jobs(600, seed=29)
+    solo = wl.solo_results(jobs)
+    for j in jobs:
+        j.out.__init__()
+        j.req.q9_groups = 0
+    srv = Server(lanes=3, max_batch=32, heavy_lanes=1)
+    try:
+        lat, status, wall = open_loop(srv, jobs, 20000.0, seed=2)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert all(s == capi.OK for s in status)
+    assert [j.result() for j in jobs] == solo
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    with pytest.raises(capi.GpudbError):
+        Server(lanes=2, heavy_lanes=2)
