@@ -528,7 +528,7 @@ int gpudb_set_option(gpudb_ctx* ctx, int32_t option, int64_t value) {
       ctx->chunk_rows = (uint64_t)value;
       return GPUDB_OK;
     case GPUDB_OPT_SCAN_VARIANT:
-      if (value < 0 || value > 8) return fail(ctx, GPUDB_E_INVALID, "scan variant must be 0..8");
+      if (value < 0 || value > 10) return fail(ctx, GPUDB_E_INVALID, "scan variant must be 0..10");
       ctx->scan_variant = (int)value;
       return GPUDB_OK;
     case GPUDB_OPT_Q6_VARIANT:

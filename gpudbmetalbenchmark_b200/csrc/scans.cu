@@ -652,8 +652,9 @@ struct Q6Riders {
 
 // MINB: resident blocks per SM the registers are sized for (2: the default; 3: variant 8,
 // more loads in flight for tables that end in one short wave). NQ6: Q6 requests riding along
-// (register sums per request, added into their words at the end).
-template <int MINB, int NQ6>
+// (register sums per request, added into their words at the end). QPI: 16-byte quads per
+// thread per step (2 by default; 4: variant 9; 1 with four blocks per SM: variant 10).
+template <int MINB, int NQ6, int QPI = 2>
 __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const int4* __restrict__ ship4, const int4* __restrict__ qty4,
                                                                      const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
                                                                      const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
@@ -698,18 +699,25 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
   const uint64_t nq = n >> 2;
   const uint64_t S = (uint64_t)gridDim.x * T;
   uint64_t q = (uint64_t)blockIdx.x * T + t;
-  for (; q + S < nq; q += 2 * S) {
-    const uint64_t q2 = q + S;
-    const int4 s0 = ld_stream(ship4 + q), s1 = ld_stream(ship4 + q2);
-    const int4 k0 = ld_stream(qty4 + q), k1 = ld_stream(qty4 + q2);
-    const longlong2 a0 = ld_stream(ext2 + 2 * q), b0 = ld_stream(ext2 + 2 * q + 1);
-    const longlong2 a1 = ld_stream(ext2 + 2 * q2), b1 = ld_stream(ext2 + 2 * q2 + 1);
-    const int4 d0 = ld_stream(disc4 + q), d1 = ld_stream(disc4 + q2);
-    const int4 x0 = ld_stream(tax4 + q), x1 = ld_stream(tax4 + q2);
-    const uint32_t f0 = ld_stream(flag4 + q), f1 = ld_stream(flag4 + q2);
-    const uint32_t g0 = ld_stream(stat4 + q), g1 = ld_stream(stat4 + q2);
-    quad(s0, k0, a0, b0, d0, x0, f0, g0);
-    quad(s1, k1, a1, b1, d1, x1, f1, g1);
+  // QPI quads per thread per step, all their loads issued before the first is used
+  for (; q + (uint64_t)(QPI - 1) * S < nq; q += (uint64_t)QPI * S) {
+    int4 sv[QPI], kv[QPI], dv[QPI], xv[QPI];
+    longlong2 av[QPI], bv[QPI];
+    uint32_t fv[QPI], gv[QPI];
+#pragma unroll
+    for (int u = 0; u < QPI; u++) {
+      const uint64_t qq = q + (uint64_t)u * S;
+      sv[u] = ld_stream(ship4 + qq);
+      kv[u] = ld_stream(qty4 + qq);
+      av[u] = ld_stream(ext2 + 2 * qq);
+      bv[u] = ld_stream(ext2 + 2 * qq + 1);
+      dv[u] = ld_stream(disc4 + qq);
+      xv[u] = ld_stream(tax4 + qq);
+      fv[u] = ld_stream(flag4 + qq);
+      gv[u] = ld_stream(stat4 + qq);
+    }
+#pragma unroll
+    for (int u = 0; u < QPI; u++) quad(sv[u], kv[u], av[u], bv[u], dv[u], xv[u], fv[u], gv[u]);
   }
   for (; q < nq; q += S)
     quad(ld_stream(ship4 + q), ld_stream(qty4 + q), ld_stream(ext2 + 2 * q), ld_stream(ext2 + 2 * q + 1),
@@ -828,10 +836,14 @@ int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, voi
   // 4 TMA 4096-row tiles x 2 stages
   int variant = ctx->scan_variant;
   if (variant == 0) variant = vec ? 7 : 3;
-  if ((variant == 7 || variant == 8) && !vec) variant = 3;
-  if (variant == 7 || variant == 8)
-    return launch_q1_smem(call, c, p, out, status, variant == 8 ? q1_vec_smem_kernel<3, 0> : q1_vec_smem_kernel<2, 0>,
-                          Q6Riders{});
+  if (variant >= 7 && variant <= 10 && !vec) variant = 3;
+  if (variant >= 7 && variant <= 10) {
+    const Q1SmemKernel k = variant == 8  ? q1_vec_smem_kernel<3, 0, 2>
+                         : variant == 9  ? q1_vec_smem_kernel<2, 0, 4>
+                         : variant == 10 ? q1_vec_smem_kernel<4, 0, 1>
+                                         : q1_vec_smem_kernel<2, 0, 2>;
+    return launch_q1_smem(call, c, p, out, status, k, Q6Riders{});
+  }
   if ((variant == 1 || variant >= 4) && !tma_ok) variant = vec ? 2 : 3;
   if (variant == 2 && !vec) variant = 3;
   if (variant == 1 || variant >= 4) {

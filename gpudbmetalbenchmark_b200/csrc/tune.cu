@@ -134,7 +134,7 @@ extern "C" int gpudb_autotune(gpudb_ctx* ctx, const gpudb_request* req, uint32_t
   switch (q.pipeline) {
     case GPUDB_PIPE_Q1:
       def = {GPUDB_OPT_SCAN_VARIANT, 0, 0, 0};
-      for (int v = 1; v <= 8; v++) cands.push_back({GPUDB_OPT_SCAN_VARIANT, v, 0, 0});
+      for (int v = 1; v <= 10; v++) cands.push_back({GPUDB_OPT_SCAN_VARIANT, v, 0, 0});
       break;
     case GPUDB_PIPE_Q6:
       def = {GPUDB_OPT_Q6_VARIANT, 0, 0, 0};

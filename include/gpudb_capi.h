@@ -99,7 +99,9 @@ enum {
   GPUDB_OPT_SCAN_VARIANT = 2, /* Q1 scan kernel: 0 auto (7), 1 TMA 2048-row tiles x 4 stages, 2 128-bit loads,
                                  3 one row per thread, 4 TMA 4096-row tiles x 2 stages, 5 TMA ring,
                                  6 TMA ring + shared accumulators, 7 128-bit loads + shared accumulators,
-                                 8 as 7 with registers for three blocks per SM */
+                                 8 as 7 with registers for three blocks per SM, 9 as 7 with four
+                                 quads per thread per step, 10 as 7 with one quad per step and
+                                 four blocks per SM */
   GPUDB_OPT_Q6_VARIANT = 3,   /* Q6 scan kernel: 0 auto (1 below 2^24 rows, else 2), 1 one row per thread,
                                  2/3/4 128-bit loads with 1/2/4 quads (4/8/16 rows) per thread per step */
   GPUDB_OPT_HT_LOAD = 4,      /* largest load of the Q3/Q9 build hash tables, percent: 50 (default) or 25 */
@@ -561,7 +563,7 @@ int gpudb_selftest_bounded_wait(gpudb_ctx* ctx, uint32_t polls, int32_t arrive);
 /* ---- autotuner (no reference counterpart) --------------------------------------------
  * gpudb_autotune times the candidate settings of one request's pipeline on the request's
  * own tables (reps runs each, median device time) and sets the fastest on the context:
- *   Q1: GPUDB_OPT_SCAN_VARIANT 1..7 (block size, rows per thread, 128-bit loads, TMA
+ *   Q1: GPUDB_OPT_SCAN_VARIANT 1..10 (block size, rows per thread, 128-bit loads, TMA
  *       staging, shared-memory accumulators); Q6: GPUDB_OPT_Q6_VARIANT 1..4 (row kernel or
  *       128-bit loads with 1/2/4 quads per thread per step); Q3 global mode:
  *       GPUDB_OPT_HT_LOAD 50/25; Q3 radix mode: GPUDB_OPT_RADIX_BITS; Q3 AUTO mode:

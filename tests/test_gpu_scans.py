@@ -56,7 +56,7 @@ def test_q6_q1_small_sizes(engine, orc, n):
         engine.free(t)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("n", [2047, 2048, 2049, 3 * 4096 + 5, 1_000_003])
 def test_q1_every_kernel_variant(engine, orc, variant, n):
     """TMA-staged tiles (1), 128-bit loads (2) and one row per thread (3) agree exactly."""
