@@ -532,32 +532,16 @@ __global__ void __launch_bounds__(kFactThreads) q3_fact_filter_kernel(
   auto row_of = [&](uint64_t b, int j) {   // row j (quad j / 4, element j % 4) of this thread
     return b + 4 * ((uint64_t)(j >> 2) * kFactThreads + threadIdx.x) + (j & 3);
   };
-  // the next step's ship dates and keys load while this step tests the key set and gathers
-  const uint64_t stride = (uint64_t)gridDim.x * kStep;
-  int4 nsv[kFactQuads], nkv[kFactQuads];
-  auto prefetch = [&](uint64_t b) {
+  // whole blocks stay in the loop: block_reserve needs every thread of the block
+  for (uint64_t b = (uint64_t)blockIdx.x * kStep; b < n; b += (uint64_t)gridDim.x * kStep) {
+    int32_t k[R];
+    uint32_t on = 0;
     if (vec && b + kStep <= n) {
 #pragma unroll
       for (int q = 0; q < kFactQuads; q++) {
         const uint64_t r0 = row_of(b, 4 * q);
-        nsv[q] = ld_stream(reinterpret_cast<const int4*>(lship + r0));
-        nkv[q] = ld_stream(reinterpret_cast<const int4*>(lkey + r0));
-      }
-    }
-  };
-  prefetch((uint64_t)blockIdx.x * kStep);
-  // whole blocks stay in the loop: block_reserve needs every thread of the block
-  for (uint64_t b = (uint64_t)blockIdx.x * kStep; b < n; b += stride) {
-    int32_t k[R];
-    uint32_t on = 0;
-    if (vec && b + kStep <= n) {
-      int4 csv[kFactQuads], ckv[kFactQuads];
-#pragma unroll
-      for (int q = 0; q < kFactQuads; q++) { csv[q] = nsv[q]; ckv[q] = nkv[q]; }
-      prefetch(b + stride);
-#pragma unroll
-      for (int q = 0; q < kFactQuads; q++) {
-        const int4 sv = csv[q], kv = ckv[q];
+        const int4 sv = ld_stream(reinterpret_cast<const int4*>(lship + r0));
+        const int4 kv = ld_stream(reinterpret_cast<const int4*>(lkey + r0));
         k[4 * q] = kv.x; k[4 * q + 1] = kv.y; k[4 * q + 2] = kv.z; k[4 * q + 3] = kv.w;
         on |= ((uint32_t)(sv.x > ship_gt) | (uint32_t)(sv.y > ship_gt) << 1 | (uint32_t)(sv.z > ship_gt) << 2 |
                (uint32_t)(sv.w > ship_gt) << 3) << (4 * q);
@@ -570,7 +554,6 @@ __global__ void __launch_bounds__(kFactThreads) q3_fact_filter_kernel(
         k[j] = in ? ld_stream(lkey + r) : 0;
         on |= (uint32_t)(in && ld_stream(lship + r) > ship_gt) << j;
       }
-      prefetch(b + stride);
     }
     uint32_t take = 0;
 #pragma unroll
