@@ -203,7 +203,10 @@ int Call::begin(size_t result_bytes) {
     dslot_ = ctx_->d_slots + (size_t)slot_ * kSlotBytes;
     hslot_ = ctx_->h_slots + (size_t)slot_ * kSlotBytes;
   }
-  GPUDB_CUDA(ctx_, cudaMemsetAsync(dslot_, 0, kSlotHeader + result_bytes, s_));
+  if (want_direct_ && !big_ && !dwork_ && ctx_->h_slots_dev)
+    direct_ = ctx_->h_slots_dev + (size_t)slot_ * kSlotBytes;
+  else
+    GPUDB_CUDA(ctx_, cudaMemsetAsync(dslot_, 0, kSlotHeader + result_bytes, s_));
   if (t_) {
     // the timed region starts after the result slot is cleared: kernels (and copies) only
     e0_ = event_get(ctx_);
@@ -212,6 +215,11 @@ int Call::begin(size_t result_bytes) {
     GPUDB_CUDA(ctx_, cudaEventRecord(e0_, s_));
   }
   return GPUDB_OK;
+}
+
+int Call::begin_direct(size_t result_bytes) {
+  want_direct_ = true;
+  return begin(result_bytes);
 }
 
 int Call::check_launch(const char* name) {
@@ -249,7 +257,9 @@ int Call::finish(size_t result_bytes, std::function<int(const uint8_t*)> convert
   side_end();   // (a stage that failed on the side stream may have left it selected)
   if (t_) GPUDB_CUDA(ctx_, cudaEventRecord(e1_, s_));
   size_t bytes = kSlotHeader + result_bytes;
-  GPUDB_CUDA(ctx_, cudaMemcpyAsync(hslot_, dslot_, bytes, cudaMemcpyDeviceToHost, s_));
+  // (a direct result is already in hslot_ when the kernel completes; its bytes crossed the
+  // link all the same)
+  if (!direct_) GPUDB_CUDA(ctx_, cudaMemcpyAsync(hslot_, dslot_, bytes, cudaMemcpyDeviceToHost, s_));
   d2h_ += bytes;
   ctx_->h2d_total += h2d_;
   ctx_->d2h_total += d2h_;
@@ -452,7 +462,14 @@ int gpudb_create(int device, gpudb_ctx** out) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_slots, (size_t)kResultSlots * kSlotBytes);
-  if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_slots, (size_t)kResultSlots * kSlotBytes, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_slots, (size_t)kResultSlots * kSlotBytes, cudaHostAllocMapped);
+  if (e == cudaSuccess) {
+    // kernels that write a call's result straight into its host slot (Call::begin_direct)
+    // need the slots' device address; without one every call copies its slot back
+    void* dev = nullptr;
+    if (cudaHostGetDevicePointer(&dev, ctx->h_slots, 0) == cudaSuccess) ctx->h_slots_dev = static_cast<uint8_t*>(dev);
+    (void)cudaGetLastError();
+  }
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_big, (size_t)kBigSlots * kBigSlotBytes);
   if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_big, (size_t)kBigSlots * kBigSlotBytes, cudaHostAllocDefault);
   if (e != cudaSuccess) {

@@ -78,6 +78,7 @@ struct gpudb_ctx {
   std::vector<void*> retired;          // outgrown scratch, freed once the context is idle
   uint8_t* d_slots = nullptr;          // result slots (device)
   uint8_t* h_slots = nullptr;          // their pinned host mirror
+  uint8_t* h_slots_dev = nullptr;      // the mirror's address in the device's address space (mapped), or null
   bool slot_busy[gpudb::kResultSlots] = {};
   int next_slot = 0;
   uint8_t* d_big = nullptr;            // large result slots (device) and their pinned mirror
@@ -138,6 +139,14 @@ class Call {
   Call(gpudb_ctx* ctx, const gpudb_exec* ex, gpudb_timing* t);
   ~Call();
   int begin(size_t result_bytes);          // acquires a slot and zeroes header + payload
+  // Direct result: for a pipeline whose result comes from ONE kernel's last block. The slot
+  // is not cleared and nothing is copied back: that block writes the status word and every
+  // result byte (overwriting, not adding) straight into the call's pinned host slot, through
+  // the slot's mapped device address, which direct_slot() returns (header, then payload).
+  // Falls back to begin() when the slot cannot be written that way (large results, no
+  // mapping); direct_slot() is then null and the pipeline launches as for begin().
+  int begin_direct(size_t result_bytes);
+  uint8_t* direct_slot() const { return direct_; }
   cudaStream_t stream() const { return s_; }
   uint32_t* status() const { return reinterpret_cast<uint32_t*>(dwork_ ? dwork_ : dslot_); }
   template <class T> T* result() const { return reinterpret_cast<T*>((dwork_ ? dwork_ : dslot_) + kSlotHeader); }
@@ -179,6 +188,8 @@ class Call {
   uint8_t* dslot_ = nullptr;
   uint8_t* hslot_ = nullptr;
   uint8_t* dwork_ = nullptr;
+  uint8_t* direct_ = nullptr;     // device address of hslot_ when the kernel writes it directly
+  bool want_direct_ = false;
   uint32_t kernels_ = 0, chunks_ = 0;
   uint64_t h2d_ = 0, d2h_ = 0;
   bool handed_off_ = false;

@@ -10,7 +10,10 @@
 // accumulators live in registers; the block reduces them with warp shuffles, writes one
 // partial per block, and the last block to finish folds the partials (one launch, no
 // second-stage kernel, no atomics on the result, deterministic). Results accumulate into
-// the output (+=) so a streamed table is one launch per chunk on the same output.
+// the output (+=) so a streamed table is one launch per chunk on the same output; a
+// one-launch call on device-resident columns instead passes `hstatus` (its pinned host
+// slot's status word, mapped) and the last block overwrites the output there, so the call
+// needs no clear of its slot before the kernel and no copy back after it.
 #include <algorithm>
 #include <cstring>
 
@@ -37,7 +40,7 @@ struct Q6Out { int64_t revenue; uint64_t matched; };
 
 template <int T>
 __device__ __forceinline__ void block_fold_q6(int64_t rev, uint64_t cnt, int64_t* part_rev, uint64_t* part_cnt,
-                                              unsigned* ticket, Q6Out* out) {
+                                              unsigned* ticket, Q6Out* out, uint32_t* hstatus) {
   __shared__ uint64_t sr[T / 32], sc[T / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint64_t r = warp_sum_u64((uint64_t)rev), c = warp_sum_u64(cnt);
@@ -63,8 +66,14 @@ __device__ __forceinline__ void block_fold_q6(int64_t rev, uint64_t cnt, int64_t
   if (threadIdx.x == 0) {
     uint64_t ta = 0, tb = 0;
     for (int w = 0; w < T / 32; w++) { ta += sr[w]; tb += sc[w]; }
-    out->revenue += (int64_t)ta;
-    out->matched += tb;
+    if (hstatus) {   // one launch, the host slot: overwrite (the Q6 scan sets no status bits)
+      out->revenue = (int64_t)ta;
+      out->matched = tb;
+      *hstatus = 0u;
+    } else {
+      out->revenue += (int64_t)ta;
+      out->matched += tb;
+    }
   }
 }
 
@@ -72,7 +81,7 @@ template <int UNROLL>
 __global__ void __launch_bounds__(kThreads) q6_vec_kernel(const int4* __restrict__ ship4, const int4* __restrict__ disc4,
                                                           const int4* __restrict__ qty4, const int64_t* __restrict__ ext,
                                                           uint64_t n, Q6P p, int64_t* part_rev, uint64_t* part_cnt,
-                                                          unsigned* ticket, Q6Out* out) {
+                                                          unsigned* ticket, Q6Out* out, uint32_t* hstatus) {
   const uint64_t nq = n >> 2;
   const uint64_t T = (uint64_t)gridDim.x * kThreads;
   uint64_t q = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
@@ -112,19 +121,20 @@ __global__ void __launch_bounds__(kThreads) q6_vec_kernel(const int4* __restrict
     const int32_t* qty = reinterpret_cast<const int32_t*>(qty4);
     if (q6_pass(ship[r], disc[r], qty[r], p)) { rev += ext[r] * (int64_t)disc[r]; cnt++; }
   }
-  block_fold_q6<kThreads>(rev, cnt, part_rev, part_cnt, ticket, out);
+  block_fold_q6<kThreads>(rev, cnt, part_rev, part_cnt, ticket, out, hstatus);
 }
 
 // Any alignment: one row per thread per step.
 __global__ void __launch_bounds__(kThreads) q6_row_kernel(const int32_t* ship, const int32_t* disc, const int32_t* qty,
                                                           const int64_t* ext, uint64_t n, Q6P p, int64_t* part_rev,
-                                                          uint64_t* part_cnt, unsigned* ticket, Q6Out* out) {
+                                                          uint64_t* part_cnt, unsigned* ticket, Q6Out* out,
+                                                          uint32_t* hstatus) {
   const uint64_t T = (uint64_t)gridDim.x * kThreads;
   int64_t rev = 0;
   uint32_t cnt = 0;
   for (uint64_t r = (uint64_t)blockIdx.x * kThreads + threadIdx.x; r < n; r += T)
     if (q6_pass(ship[r], disc[r], qty[r], p)) { rev += ext[r] * (int64_t)disc[r]; cnt++; }
-  block_fold_q6<kThreads>(rev, cnt, part_rev, part_cnt, ticket, out);
+  block_fold_q6<kThreads>(rev, cnt, part_rev, part_cnt, ticket, out, hstatus);
 }
 
 // ------------------------------------------------------------------------------------
@@ -251,7 +261,7 @@ __device__ __forceinline__ void atomic_add_u128(u128* p, u128 v) {
 // for the next launch (it is zero when first allocated). No per-block partials are read back.
 template <int T>
 __device__ __forceinline__ void q1_smem_fold(const uint64_t* acc, uint32_t bad, u128* gacc, unsigned* ticket, u128* out,
-                                             uint32_t* status) {
+                                             uint32_t* status, uint32_t* hstatus) {
   constexpr int W = T / 32;
   static_assert(24 % W == 0, "whole columns per warp");
   __shared__ u128 tot[6 * kQ1Raw];
@@ -302,12 +312,27 @@ __device__ __forceinline__ void q1_smem_fold(const uint64_t* acc, uint32_t bad, 
     const u128 disc_price = (u128)100 * r[2] - r[3];
     const u128 charge = (u128)100 * disc_price + r[4];
     u128* o = out + g * kQ1Metrics;
-    o[0] += r[0];
-    o[1] += r[1];
-    o[2] += r[2];
-    o[3] += disc_price;
-    o[4] += charge;
-    o[5] += r[5];
+    if (hstatus) {   // one launch, the host slot: overwrite
+      o[0] = r[0];
+      o[1] = r[1];
+      o[2] = r[2];
+      o[3] = disc_price;
+      o[4] = charge;
+      o[5] = r[5];
+    } else {
+      o[0] += r[0];
+      o[1] += r[1];
+      o[2] += r[2];
+      o[3] += disc_price;
+      o[4] += charge;
+      o[5] += r[5];
+    }
+  }
+  // the host slot takes the status every block has OR-ed in (visible past the ticket), and
+  // the launch's own status word is left at zero for the next launch
+  if (hstatus && threadIdx.x == 0) {
+    *hstatus = __ldcg(status);
+    *status = 0u;
   }
 }
 
@@ -660,7 +685,7 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
                                                                      const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
                                                                      const uint32_t* __restrict__ stat4, uint64_t n, int32_t ship_le,
                                                                      u128* gacc, unsigned* ticket, u128* out, uint32_t* status,
-                                                                     Q6Riders riders) {
+                                                                     uint32_t* hstatus, Q6Riders riders) {
   constexpr int T = kQ1SmemThreads;
   extern __shared__ __align__(16) uint64_t q1_acc[];   // [4 metrics][6 groups][T]
   const int t = threadIdx.x;
@@ -737,7 +762,7 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
       if (c) atomicAdd(riders.out[r] + 1, c);
     }
   }
-  q1_smem_fold<T>(q1_acc, bad, gacc, ticket, out, status);
+  q1_smem_fold<T>(q1_acc, bad, gacc, ticket, out, status, hstatus);
 }
 
 bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
@@ -765,8 +790,9 @@ int scan_scratch(gpudb_ctx* ctx, const char* name, size_t partial_bytes, void** 
 
 }  // namespace
 
-// Enqueue one Q6 scan of device-resident columns, adding into `out` (device).
-int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, void* out) {
+// Enqueue one Q6 scan of device-resident columns, adding into `out` (device), or with
+// `hstatus` overwriting `out` in the call's mapped host slot (a direct result).
+int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, void* out, uint32_t* hstatus) {
   gpudb_ctx* ctx = call.ctx();
   if (c.n_rows == 0) return GPUDB_OK;
   const Q6P pp{p.ship_lo, p.ship_hi, p.disc_lo, p.disc_hi, p.qty_lt};
@@ -790,10 +816,10 @@ int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, voi
   if (variant != 1) {
     auto k = unroll == 1 ? q6_vec_kernel<1> : unroll == 4 ? q6_vec_kernel<4> : q6_vec_kernel<2>;
     GPUDB_LAUNCH(call, k, grid, kThreads, 0, (const int4*)c.ship_date, (const int4*)c.discount,
-                 (const int4*)c.quantity, c.ext_price, c.n_rows, pp, prev, pcnt, ticket, (Q6Out*)out);
+                 (const int4*)c.quantity, c.ext_price, c.n_rows, pp, prev, pcnt, ticket, (Q6Out*)out, hstatus);
   } else {
     GPUDB_LAUNCH(call, q6_row_kernel, grid, kThreads, 0, c.ship_date, c.discount, c.quantity, c.ext_price, c.n_rows,
-                 pp, prev, pcnt, ticket, (Q6Out*)out);
+                 pp, prev, pcnt, ticket, (Q6Out*)out, hstatus);
   }
   return GPUDB_OK;
 }
@@ -801,10 +827,14 @@ int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, voi
 // Enqueue one Q1 scan of device-resident columns, adding into `out` (device, 36 x u128).
 // The shared-memory Q1 kernel (16-byte aligned columns): a grid of SMs x occupancy blocks
 // (at most kQ1RowsPerThread rows a thread) over the 36 u128 accumulators of "q1.acc".
+// With `hstatus` (a direct result: `out` and `hstatus` in the call's mapped host slot) the
+// launch's status word is the one in the scratch header beside the ticket, which the last
+// block copies to the host slot and leaves at zero.
 using Q1SmemKernel = void (*)(const int4*, const int4*, const longlong2*, const int4*, const int4*, const uint32_t*,
-                              const uint32_t*, uint64_t, int32_t, u128*, unsigned*, u128*, uint32_t*, Q6Riders);
+                              const uint32_t*, uint64_t, int32_t, u128*, unsigned*, u128*, uint32_t*, uint32_t*,
+                              Q6Riders);
 static int launch_q1_smem(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status,
-                          Q1SmemKernel kern, const Q6Riders& riders) {
+                          Q1SmemKernel kern, const Q6Riders& riders, uint32_t* hstatus = nullptr) {
   gpudb_ctx* ctx = call.ctx();
   const size_t smem = kQ1AccBytes;
   GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)kern, smem));
@@ -819,33 +849,43 @@ static int launch_q1_smem(Call& call, const gpudb_lineitem& c, const gpudb_q1_pa
   unsigned* ticket = nullptr;
   int rc = scan_scratch(ctx, "q1.acc", (size_t)6 * kQ1Raw * sizeof(u128), &part, &ticket);
   if (rc) return rc;
+  if (hstatus) status = ticket + 1;
   GPUDB_LAUNCH(call, kern, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
                (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
-               (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status, riders);
+               (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status, hstatus,
+               riders);
   return GPUDB_OK;
+}
+
+// The Q1 variant a launch over `c` runs (the auto choice resolved, and the choices that the
+// columns' alignment rules out replaced): 7-10 are the one-launch shared-memory kernels.
+static int q1_variant(const gpudb_ctx* ctx, const gpudb_lineitem& c) {
+  const bool vec = aligned(c.ship_date, 16) && aligned(c.quantity, 16) && aligned(c.ext_price, 16) &&
+                   aligned(c.discount, 16) && aligned(c.tax, 16) && aligned(c.flag, 4) && aligned(c.status, 4);
+  const bool tma_ok = vec && aligned(c.flag, 16) && aligned(c.status, 16) && c.n_rows >= 4096;
+  int variant = ctx->scan_variant;
+  if (variant == 0) variant = vec ? 7 : 3;
+  if (variant >= 7 && variant <= 10) return vec ? variant : 3;
+  if ((variant == 1 || variant >= 4) && !tma_ok) variant = vec ? 2 : 3;
+  if (variant == 2 && !vec) variant = 3;
+  return variant;
+}
+
+static Q1SmemKernel q1_smem_kernel(int variant) {
+  return variant == 8  ? q1_vec_smem_kernel<3, 0, 2>
+       : variant == 9  ? q1_vec_smem_kernel<2, 0, 4>
+       : variant == 10 ? q1_vec_smem_kernel<4, 0, 1>
+                       : q1_vec_smem_kernel<2, 0, 2>;
 }
 
 int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status) {
   gpudb_ctx* ctx = call.ctx();
   if (!status) status = call.status();
   if (c.n_rows == 0) return GPUDB_OK;
-  const bool vec = aligned(c.ship_date, 16) && aligned(c.quantity, 16) && aligned(c.ext_price, 16) &&
-                   aligned(c.discount, 16) && aligned(c.tax, 16) && aligned(c.flag, 4) && aligned(c.status, 4);
-  const bool tma_ok = vec && aligned(c.flag, 16) && aligned(c.status, 16) && c.n_rows >= 4096;
   // 0 auto, 1 TMA 2048-row tiles x 4 stages, 2 vector loads, 3 one row per thread,
-  // 4 TMA 4096-row tiles x 2 stages
-  int variant = ctx->scan_variant;
-  if (variant == 0) variant = vec ? 7 : 3;
-  if (variant >= 7 && variant <= 10 && !vec) variant = 3;
-  if (variant >= 7 && variant <= 10) {
-    const Q1SmemKernel k = variant == 8  ? q1_vec_smem_kernel<3, 0, 2>
-                         : variant == 9  ? q1_vec_smem_kernel<2, 0, 4>
-                         : variant == 10 ? q1_vec_smem_kernel<4, 0, 1>
-                                         : q1_vec_smem_kernel<2, 0, 2>;
-    return launch_q1_smem(call, c, p, out, status, k, Q6Riders{});
-  }
-  if ((variant == 1 || variant >= 4) && !tma_ok) variant = vec ? 2 : 3;
-  if (variant == 2 && !vec) variant = 3;
+  // 4 TMA 4096-row tiles x 2 stages, 5/6 TMA rings, 7-10 shared-memory sums
+  const int variant = q1_variant(ctx, c);
+  if (variant >= 7 && variant <= 10) return launch_q1_smem(call, c, p, out, status, q1_smem_kernel(variant), Q6Riders{});
   if (variant == 1 || variant >= 4) {
     const uint32_t R = (variant == 1 || variant == 5) ? 2048u : variant == 6 ? 1024u : 4096u;
     const int threads = variant == 6 ? 256 : kQ1TmaThreads;
@@ -921,10 +961,16 @@ extern "C" int gpudb_q6_sum(gpudb_ctx* ctx, const gpudb_lineitem* li, const gpud
   int rc = lineitem_check(ctx, li, mask);
   if (rc) return rc;
   Call call(ctx, ex, t);
-  if ((rc = call.begin(sizeof(int64_t) * 2))) return rc;
+  // device-resident columns: one launch, whose last block writes the result into the host slot
+  const bool direct = li->location == GPUDB_MEM_DEVICE && li->n_rows > 0;
+  if ((rc = direct ? call.begin_direct(sizeof(int64_t) * 2) : call.begin(sizeof(int64_t) * 2))) return rc;
   const gpudb_q6_params pp = *p;
-  void* dout = call.result<void>();
-  rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) { return launch_q6(call, c, pp, dout); });
+  if (uint8_t* d = call.direct_slot()) {
+    rc = launch_q6(call, *li, pp, d + kSlotHeader, reinterpret_cast<uint32_t*>(d));
+  } else {
+    void* dout = call.result<void>();
+    rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) { return launch_q6(call, c, pp, dout); });
+  }
   if (rc) return rc;
   return call.finish(sizeof(int64_t) * 2, [out](const uint8_t* h) {
     std::memcpy(&out->revenue, h, 8);
@@ -943,10 +989,19 @@ extern "C" int gpudb_q1_group6(gpudb_ctx* ctx, const gpudb_lineitem* li, const g
   Call call(ctx, ex, t);
   const size_t bytes = kQ1ResultBytes;
   static_assert(kQ1ResultBytes == 6 * kQ1Metrics * sizeof(u128), "Q1 result layout");
-  if ((rc = call.begin(bytes))) return rc;
+  // device-resident columns and a one-launch kernel: its last block writes the result into
+  // the host slot
+  const int variant = li->location == GPUDB_MEM_DEVICE && li->n_rows > 0 ? q1_variant(ctx, *li) : 0;
+  const bool direct = variant >= 7 && variant <= 10;
+  if ((rc = direct ? call.begin_direct(bytes) : call.begin(bytes))) return rc;
   const gpudb_q1_params pp = *p;
-  void* dout = call.result<void>();
-  rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) { return launch_q1(call, c, pp, dout); });
+  if (uint8_t* d = call.direct_slot()) {
+    rc = launch_q1_smem(call, *li, pp, d + kSlotHeader, nullptr, q1_smem_kernel(variant), Q6Riders{},
+                        reinterpret_cast<uint32_t*>(d));
+  } else {
+    void* dout = call.result<void>();
+    rc = stream_lineitem(call, li, mask, 0, [&](const gpudb_lineitem& c) { return launch_q1(call, c, pp, dout); });
+  }
   if (rc) return rc;
   return call.finish(bytes, [out](const uint8_t* h) {
     q1_result_from(h, out);

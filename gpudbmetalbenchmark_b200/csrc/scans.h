@@ -10,7 +10,9 @@ constexpr size_t kQ1ResultBytes = 6 * 6 * 16;      // 6 groups x {count, qty, ba
 // Enqueue one scan of device-resident columns on the call's stream, adding into `out`
 // (device; kQ6ResultBytes / kQ1ResultBytes, zeroed before the first chunk). Q1 reports a
 // value outside its exact-arithmetic domain in `status` (the call's status word if null).
-int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, void* out);
+// Q6 with `hstatus` (the status word of the call's mapped host slot, Call::begin_direct)
+// overwrites `out` in that slot instead: one launch over the whole table.
+int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, void* out, uint32_t* hstatus = nullptr);
 int launch_q1(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status = nullptr);
 // One Q1 scan that also evaluates up to 4 Q6 requests on the rows it reads (one read of the
 // table for all of them); each Q6 request adds into its own kQ6ResultBytes words. Falls back

@@ -264,6 +264,56 @@ def test_async_calls_complete_at_sync(engine, orc):
         engine.free(t)
 
 
+def test_direct_results_over_reused_slots(engine, orc):
+    """Device-resident Q6/Q1 calls write their result straight into the pinned host slot from
+    the kernel's last block (no slot clear, no copy back). Over more async calls than there
+    are result slots (1024), every result must equal the oracle's, whatever an earlier call
+    left in the slot, and a call whose Q1 status reports a domain error must not leak that
+    status into the calls after it. The same calls on a host-resident table (streamed, with
+    the slot cleared and copied back) give the same words."""
+    from gpudbmetalbenchmark_b200.engine import q1_to_dict
+    n = 50_001
+    li = orc.lineitem(n, seed=44)
+    bad = {k: v.copy() for k, v in li.items()}
+    bad["discount"][7] = 101
+    bad["ship_date"][7] = 0
+    t, tb = upload_li(engine, li), upload_li(engine, bad)
+    th = engine.upload("lineitem", li, location=capi.MEM_HOST)
+    try:
+        q6p = [(i * 90, i * 90 + 500, i % 6, i % 6 + 4, 20 + i) for i in range(12)]
+        q1p = [i * 230 for i in range(12)]
+        want6 = [orc.q6(li, *p) for p in q6p]
+        want1 = [orc.q1(li, s) for s in q1p]
+        calls = 1100
+        o6 = [capi.Q6Result() for _ in range(calls)]
+        o1 = [capi.Q1Result() for _ in range(calls)]
+        failed = capi.Q1Result()
+        for i in range(calls):
+            engine.q6(t, *q6p[i % 12], async_=True, out=o6[i])
+            engine.q1(t, q1p[i % 12], async_=True, out=o1[i])
+            if i == calls - 20:   # after the last drain that a full set of slots forces
+                engine.q1(tb, async_=True, out=failed)
+        with pytest.raises(capi.GpudbError) as e:
+            engine.sync()
+        assert e.value.code == capi.E_INVALID
+        for i in range(calls):
+            assert (o6[i].revenue, o6[i].rows_matched) == want6[i % 12]
+            assert q1_to_dict(o1[i]) == want1[i % 12]
+        # synchronous calls: direct (device table) and copied back (host table) agree
+        for p, s in zip(q6p[:3], q1p[:3]):
+            tm_d, tm_h = capi.Timing(), capi.Timing()
+            assert engine.q6(t, *p, timing=tm_d) == engine.q6(th, *p, timing=tm_h) == orc.q6(li, *p)
+            assert tm_d.d2h_bytes == tm_h.d2h_bytes
+            r_d, r_h = capi.Q1Result(), capi.Q1Result()
+            engine.q1(t, s, out=r_d)
+            engine.q1(th, s, out=r_h)
+            assert bytes(r_d) == bytes(r_h)
+    finally:
+        engine.free(t)
+        engine.free(tb)
+        engine.free(th)
+
+
 def test_full_size_60m_bit_exact(engine, orc):
     """Config 1 at its full size: 60M rows generated on the device, both scans bit-exact
     against the oracle run on the same rows generated on the host."""
