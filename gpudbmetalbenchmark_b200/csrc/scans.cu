@@ -243,24 +243,31 @@ __device__ __forceinline__ void q1_fold(Q1Acc& a, u128* partials, unsigned* tick
   }
 }
 
-// Exact unsigned 128-bit add into global memory with two 64-bit atomics: the carry out of the
-// low word's add goes into the high word's add, so once every add has landed the 128-bit
-// value is the exact sum, whatever the order of the adds.
-__device__ __forceinline__ void atomic_add_u128(u128* p, u128 v) {
-  unsigned long long* w = reinterpret_cast<unsigned long long*>(p);
-  const unsigned long long lo = (unsigned long long)v, hi = (unsigned long long)(v >> 64);
-  const unsigned long long old = atomicAdd(w, lo);
-  const unsigned long long up = hi + (old + lo < old ? 1ull : 0ull);
-  if (up) atomicAdd(w + 1, up);
+// The shared-memory form's grid accumulators: kQ1AccCopies copies (block b adds into copy
+// b % kQ1AccCopies, so fewer blocks queue on one address when they all finish together) of
+// the 36 raw metrics, each held as three 64-bit words of 32-bit limbs. A block total v
+// (below 2^96) adds limb j = (v >> 32j) & (2^32 - 1) into word j: a limb is below 2^32, so a
+// word cannot overflow before 2^32 blocks, and the add needs no return value (no round trip,
+// unlike a carry-propagating 128-bit add). The value is sum_j word_j * 2^32j, exact.
+constexpr int kQ1AccCopies = 16;
+constexpr size_t kQ1GaccWords = (size_t)kQ1AccCopies * 6 * kQ1Raw * 3;
+
+__device__ __forceinline__ void red_add_limbs(unsigned long long* w, u128 v) {
+  const unsigned long long l0 = (unsigned long long)v & 0xFFFFFFFFull;
+  const unsigned long long l1 = (unsigned long long)(v >> 32) & 0xFFFFFFFFull;
+  const unsigned long long l2 = (unsigned long long)(v >> 64);
+  if (l0) atomicAdd(w, l0);
+  if (l1) atomicAdd(w + 1, l1);
+  if (l2) atomicAdd(w + 2, l2);
 }
 
 // Fold of the shared-memory form's per-thread sums acc[(metric * 6 + group) * T + thread]
 // (metrics P, E, ED, EDT): each warp sums three of the 24 columns (P unpacked into count,
-// quantity and discount sum) and adds the block's totals into the 36 u128 words of `gacc`
-// with exact 128-bit atomics; the last block turns them into the output and zeroes `gacc`
-// for the next launch (it is zero when first allocated). No per-block partials are read back.
+// quantity and discount sum) and adds the block's totals into its copy of the limb words of
+// `gacc` (kQ1GaccWords); the last block turns them into the output and zeroes `gacc` for the
+// next launch (it is zero when first allocated). No per-block partials are read back.
 template <int T>
-__device__ __forceinline__ void q1_smem_fold(const uint64_t* acc, uint32_t bad, u128* gacc, unsigned* ticket, u128* out,
+__device__ __forceinline__ void q1_smem_fold(const uint64_t* acc, uint32_t bad, unsigned long long* gacc, unsigned* ticket, u128* out,
                                              uint32_t* status, uint32_t* hstatus) {
   constexpr int W = T / 32;
   static_assert(24 % W == 0, "whole columns per warp");
@@ -288,22 +295,29 @@ __device__ __forceinline__ void q1_smem_fold(const uint64_t* acc, uint32_t bad, 
       s2 = warp_sum_u128(s2);
     }
     if (lane == 0) {
-      u128* o = gacc + g * kQ1Raw;   // raw metrics: count, qty, E, ED, EDT, dsum
+      // raw metrics: count, qty, E, ED, EDT, dsum
+      unsigned long long* o = gacc + ((size_t)(blockIdx.x % kQ1AccCopies) * 6 * kQ1Raw + g * kQ1Raw) * 3;
       if (metric == 0) {
-        atomic_add_u128(o + 0, s0);
-        atomic_add_u128(o + 1, s1);
-        atomic_add_u128(o + 5, s2);
+        red_add_limbs(o + 0 * 3, s0);
+        red_add_limbs(o + 1 * 3, s1);
+        red_add_limbs(o + 5 * 3, s2);
       } else {
-        atomic_add_u128(o + 1 + metric, s0);
+        red_add_limbs(o + (1 + metric) * 3, s0);
       }
     }
   }
   if (!grid_last_block(ticket)) return;
   if (threadIdx.x < 6 * kQ1Raw) {
-    unsigned long long* w = reinterpret_cast<unsigned long long*>(gacc + threadIdx.x);
-    tot[threadIdx.x] = ((u128)__ldcg(w + 1) << 64) | __ldcg(w);
-    w[0] = 0;
-    w[1] = 0;
+    u128 v = 0;
+#pragma unroll
+    for (int c = 0; c < kQ1AccCopies; c++) {
+      unsigned long long* w = gacc + ((size_t)c * 6 * kQ1Raw + threadIdx.x) * 3;
+      v += (u128)__ldcg(w) + ((u128)__ldcg(w + 1) << 32) + ((u128)__ldcg(w + 2) << 64);
+      w[0] = 0;
+      w[1] = 0;
+      w[2] = 0;
+    }
+    tot[threadIdx.x] = v;
   }
   __syncthreads();
   if (threadIdx.x < 6) {
@@ -684,7 +698,7 @@ __global__ void __launch_bounds__(kQ1SmemThreads, MINB) q1_vec_smem_kernel(const
                                                                      const longlong2* __restrict__ ext2, const int4* __restrict__ disc4,
                                                                      const int4* __restrict__ tax4, const uint32_t* __restrict__ flag4,
                                                                      const uint32_t* __restrict__ stat4, uint64_t n, int32_t ship_le,
-                                                                     u128* gacc, unsigned* ticket, u128* out, uint32_t* status,
+                                                                     unsigned long long* gacc, unsigned* ticket, u128* out, uint32_t* status,
                                                                      uint32_t* hstatus, Q6Riders riders) {
   constexpr int T = kQ1SmemThreads;
   extern __shared__ __align__(16) uint64_t q1_acc[];   // [4 metrics][6 groups][T]
@@ -826,13 +840,13 @@ int launch_q6(Call& call, const gpudb_lineitem& c, const gpudb_q6_params& p, voi
 
 // Enqueue one Q1 scan of device-resident columns, adding into `out` (device, 36 x u128).
 // The shared-memory Q1 kernel (16-byte aligned columns): a grid of SMs x occupancy blocks
-// (at most kQ1RowsPerThread rows a thread) over the 36 u128 accumulators of "q1.acc".
+// (at most kQ1RowsPerThread rows a thread) over the limb accumulators of "q1.acc".
 // With `hstatus` (a direct result: `out` and `hstatus` in the call's mapped host slot) the
 // launch's status word is the one in the scratch header beside the ticket, which the last
 // block copies to the host slot and leaves at zero.
 using Q1SmemKernel = void (*)(const int4*, const int4*, const longlong2*, const int4*, const int4*, const uint32_t*,
-                              const uint32_t*, uint64_t, int32_t, u128*, unsigned*, u128*, uint32_t*, uint32_t*,
-                              Q6Riders);
+                              const uint32_t*, uint64_t, int32_t, unsigned long long*, unsigned*, u128*, uint32_t*,
+                              uint32_t*, Q6Riders);
 static int launch_q1_smem(Call& call, const gpudb_lineitem& c, const gpudb_q1_params& p, void* out, uint32_t* status,
                           Q1SmemKernel kern, const Q6Riders& riders, uint32_t* hstatus = nullptr) {
   gpudb_ctx* ctx = call.ctx();
@@ -844,15 +858,16 @@ static int launch_q1_smem(Call& call, const gpudb_lineitem& c, const gpudb_q1_pa
   const uint64_t want = (c.n_rows / 4 + kQ1SmemThreads - 1) / kQ1SmemThreads;
   const int grid = (int)std::max<uint64_t>(
       1, std::max(min_blocks, std::min<uint64_t>(want, (uint64_t)ctx->sm_count * std::max(per_sm, 1))));
-  // 36 u128 accumulators and a ticket, both left at zero by every launch's last block
+  // the limb accumulators and a ticket, both left at zero by every launch's last block
   void* part = nullptr;
   unsigned* ticket = nullptr;
-  int rc = scan_scratch(ctx, "q1.acc", (size_t)6 * kQ1Raw * sizeof(u128), &part, &ticket);
+  int rc = scan_scratch(ctx, "q1.acc", kQ1GaccWords * sizeof(unsigned long long), &part, &ticket);
   if (rc) return rc;
   if (hstatus) status = ticket + 1;
   GPUDB_LAUNCH(call, kern, grid, kQ1SmemThreads, smem, (const int4*)c.ship_date, (const int4*)c.quantity,
                (const longlong2*)c.ext_price, (const int4*)c.discount, (const int4*)c.tax, (const uint32_t*)c.flag,
-               (const uint32_t*)c.status, c.n_rows, p.ship_le, (u128*)part, ticket, (u128*)out, status, hstatus,
+               (const uint32_t*)c.status, c.n_rows, p.ship_le, (unsigned long long*)part, ticket, (u128*)out, status,
+               hstatus,
                riders);
   return GPUDB_OK;
 }

@@ -39,46 +39,49 @@ std::string device_name(gpudb_ctx* ctx) {
   return n;
 }
 
-// One run of the request through its single-request pipeline: device ms and a digest of the
-// result (the bytes of the result struct), or a negative status.
-int run_once(gpudb_ctx* ctx, const gpudb_request& q, double* ms, std::string* digest) {
+// The result of one run of a request, kept until the run completes (an async run writes it
+// at gpudb_sync).
+struct Outs {
+  gpudb_q6_result q6{};
+  gpudb_q1_result q1{};
+  gpudb_q3_result q3{};
+  std::vector<gpudb_q9_group> q9 = std::vector<gpudb_q9_group>(256);
+  uint32_t n9 = 0;
   gpudb_timing t{};
-  int rc = GPUDB_OK;
+};
+
+// Enqueues one run of the request through its single-request pipeline (synchronous when
+// `ex` is null), writing into `o`.
+int run(gpudb_ctx* ctx, const gpudb_request& q, Outs& o, const gpudb_exec* ex) {
   switch (q.pipeline) {
-    case GPUDB_PIPE_Q6: {
-      gpudb_q6_result o{};
-      rc = gpudb_q6_sum(ctx, q.li, &q.q6, &o, &t, nullptr);
-      digest->assign(reinterpret_cast<const char*>(&o), sizeof o);
-      break;
-    }
-    case GPUDB_PIPE_Q1: {
-      gpudb_q1_result o{};
-      rc = gpudb_q1_group6(ctx, q.li, &q.q1, &o, &t, nullptr);
-      digest->assign(reinterpret_cast<const char*>(&o), sizeof o);
-      break;
-    }
-    case GPUDB_PIPE_Q3: {
-      gpudb_q3_result o{};
-      rc = gpudb_q3_join_topk(ctx, &q.q3->cu, &q.q3->od, &q.q3->li, &q.q3p, &o, &t, nullptr);
-      o.join_mode = 0;   // the mode that ran differs between candidates; the answer must not
-      digest->assign(reinterpret_cast<const char*>(&o), sizeof o);
-      break;
-    }
-    case GPUDB_PIPE_Q9: {
-      std::vector<gpudb_q9_group> o(256);
-      uint32_t n = 0;
-      rc = gpudb_q9_star(ctx, &q.q9->pa, &q.q9->su, &q.q9->ps, &q.q9->od, &q.q9->li, &q.q9p, o.data(), 256, &n, &t,
-                         nullptr);
-      o.resize(std::min<uint32_t>(n, 256));
-      digest->assign(reinterpret_cast<const char*>(o.data()), o.size() * sizeof(gpudb_q9_group));
-      digest->append(reinterpret_cast<const char*>(&n), sizeof n);
-      break;
-    }
+    case GPUDB_PIPE_Q6: return gpudb_q6_sum(ctx, q.li, &q.q6, &o.q6, &o.t, ex);
+    case GPUDB_PIPE_Q1: return gpudb_q1_group6(ctx, q.li, &q.q1, &o.q1, &o.t, ex);
+    case GPUDB_PIPE_Q3:
+      return gpudb_q3_join_topk(ctx, &q.q3->cu, &q.q3->od, &q.q3->li, &q.q3p, &o.q3, &o.t, ex);
+    case GPUDB_PIPE_Q9:
+      return gpudb_q9_star(ctx, &q.q9->pa, &q.q9->su, &q.q9->ps, &q.q9->od, &q.q9->li, &q.q9p, o.q9.data(), 256,
+                           &o.n9, &o.t, ex);
     default:
       return fail(ctx, GPUDB_E_INVALID, "autotune: unknown pipeline %d", q.pipeline);
   }
-  *ms = t.gpu_ms;
-  return rc;
+}
+
+// A digest of a completed run's result (the bytes of the result struct).
+std::string digest_of(const gpudb_request& q, Outs& o) {
+  switch (q.pipeline) {
+    case GPUDB_PIPE_Q6: return std::string(reinterpret_cast<const char*>(&o.q6), sizeof o.q6);
+    case GPUDB_PIPE_Q1: return std::string(reinterpret_cast<const char*>(&o.q1), sizeof o.q1);
+    case GPUDB_PIPE_Q3: {
+      gpudb_q3_result r = o.q3;
+      r.join_mode = 0;   // the mode that ran differs between candidates; the answer must not
+      return std::string(reinterpret_cast<const char*>(&r), sizeof r);
+    }
+    default: {
+      std::string d(reinterpret_cast<const char*>(o.q9.data()), std::min<uint32_t>(o.n9, 256) * sizeof(gpudb_q9_group));
+      d.append(reinterpret_cast<const char*>(&o.n9), sizeof o.n9);
+      return d;
+    }
+  }
 }
 
 int apply(gpudb_ctx* ctx, const Candidate& c) {
@@ -87,21 +90,29 @@ int apply(gpudb_ctx* ctx, const Candidate& c) {
   return rc;
 }
 
-// Median device time of `reps` runs (after one untimed run that sizes scratch).
+// Median device time of `reps` runs issued back to back on the context's stream (as calls
+// run when a batch or a served stream keeps the GPU busy; an isolated call after idle time
+// measures a microsecond or two more), after one synchronous run that sizes scratch and
+// gives the digest. Every timed run's result must equal that digest.
 int measure(gpudb_ctx* ctx, const gpudb_request& q, uint32_t reps, double* median, std::string* digest) {
-  double ms;
-  int rc = run_once(ctx, q, &ms, digest);
+  Outs first;
+  int rc = run(ctx, q, first, nullptr);
   if (rc) return rc;
+  *digest = digest_of(q, first);
+  std::vector<Outs> outs(reps);
+  gpudb_exec ex{};
+  ex.async = 1;
+  for (uint32_t i = 0; i < reps && !rc; i++) rc = run(ctx, q, outs[i], &ex);
+  const int rs = gpudb_sync(ctx);   // also when an enqueue failed: no run is left in flight
+  if (rc) return rc;
+  if (rs) return rs;
   std::vector<double> v;
   for (uint32_t i = 0; i < reps; i++) {
-    std::string d;
-    rc = run_once(ctx, q, &ms, &d);
-    if (rc) return rc;
-    if (d != *digest) return fail(ctx, GPUDB_E_CUDA, "autotune: a configuration is not deterministic");
-    v.push_back(ms);
+    if (digest_of(q, outs[i]) != *digest) return fail(ctx, GPUDB_E_CUDA, "autotune: a configuration is not deterministic");
+    v.push_back(outs[i].t.gpu_ms);
   }
   std::sort(v.begin(), v.end());
-  *median = v.empty() ? ms : v[v.size() / 2];
+  *median = v.empty() ? first.t.gpu_ms : v[v.size() / 2];
   return GPUDB_OK;
 }
 

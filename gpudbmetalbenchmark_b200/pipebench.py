@@ -78,16 +78,31 @@ def q3_case(eng, n_cu, n_or, n_li, reps, label, out=emit):
 
 
 def scan_case(eng, rows, reps, out=emit):
-    """Q6 and Q1 over a device-resident lineitem table of `rows` rows: (q6, q1) records."""
+    """Q6 and Q1 over a device-resident lineitem table of `rows` rows: (q6, q1) records.
+    `ms` is the median over calls issued back to back; `sync_ms` the median over synchronous
+    calls, each starting on an idle GPU."""
     t = eng.generate("lineitem", rows, seed=42, columns=Q1_COLS)
-    ms6, _ = timed(lambda tm: eng.q6(t, timing=tm), reps)
-    r6 = out("q6_sum", "config %s" % ("1a" if rows > 6e6 else "1a at 6M"), rows, ms6, 20 * rows,
-             {"note": "6M rows = 120 MB, inside L2" if rows == 6_000_000 else ""})
-    ms1, t1 = timed(lambda tm: eng.q1(t, timing=tm), reps)
-    r1 = out("q1_group6", "config %s" % ("1b" if rows > 6e6 else "0"), rows, ms1, 26 * rows,
-             {"note": "6M rows = 156 MB" if rows == 6_000_000 else "", "kernels": t1.kernels})
+    recs = []
+    for name, fn, mk, bpr in (("q6_sum", eng.q6, capi.Q6Result, 20), ("q1_group6", eng.q1, capi.Q1Result, 26)):
+        sync_ms, tl = timed(lambda tm: fn(t, timing=tm), reps)
+        fn(t)
+        ts = [capi.Timing() for _ in range(reps)]
+        outs = [mk() for _ in range(reps)]
+        for tm, o in zip(ts, outs):
+            fn(t, timing=tm, async_=True, out=o)
+        eng.sync()
+        assert all(bytes(o) == bytes(outs[0]) for o in outs)
+        ms = statistics.median(x.gpu_ms for x in ts)
+        if name == "q6_sum":
+            cfg = "1a" if rows > 6e6 else "1a at 6M"
+            extra = {"note": "6M rows = 120 MB, inside L2" if rows == 6_000_000 else ""}
+        else:
+            cfg = "1b" if rows > 6e6 else "0"
+            extra = {"note": "6M rows = 156 MB" if rows == 6_000_000 else "", "kernels": tl.kernels}
+        extra.update({"sync_ms": round(sync_ms, 4), "timed": "calls back to back"})
+        recs.append(out(name, "config %s" % cfg, rows, ms, bpr * rows, extra))
     eng.free(t)
-    return r6, r1
+    return recs[0], recs[1]
 
 
 def q9_case(eng, reps, stream600m=False, out=emit):
