@@ -171,7 +171,7 @@ struct Q9Maps {
 constexpr int kQ9Threads = 256;
 
 constexpr int kLiThreads = 1024;
-constexpr int kLiQuads = 4;                  // 16-byte loads per thread per block step
+constexpr int kLiQuads = 4;                  // 128-row groups per warp per block step
 constexpr int kLiRows = 4 * kLiQuads;        // fact rows per thread per block step of li_filter_kernel
 constexpr uint64_t kQ9Piece = 64ull << 20;   // fact rows per filter + resolve pair (bounds the pair buffer)
 
@@ -182,66 +182,73 @@ enum : int {
 };
 
 // Fact rows whose part passes the filter -> bit (r & 31) of passbits[r >> 5] (rows of the
-// piece). The part filter (`mode`): the exact bitmap in shared memory, or a blocked Bloom
-// filter in shared memory whose hits are not confirmed here. A block step covers kLiThreads * 16 rows;
-// load q of thread t is the 16-byte quad q * kLiThreads + t of the step (coalesced), and the
-// next step's quads load while this one is tested. The four rows of a quad are four bits of
-// one word that eight lanes share: an OR across the eight lanes and one store per word, so
-// warps never wait for each other (no block barrier, no atomic) and the bitmask is dense
-// (one bit per row, 1/32 of the column read).
+// piece). A block step covers kLiThreads * 16 rows in 128-row groups, four per warp; lane L
+// tests rows 32k + L of a group (k = 0..3), loaded by four coalesced 4-byte loads (128 bytes
+// a warp each, any alignment), so the vote (__ballot_sync) of the lanes' row-32k tests is the
+// bitmask word k itself: one instruction a word, no shuffles, and lane 0 stores the group's
+// four words as one 16-byte store. The next step's keys load while this one is tested.
+// MODE: kPartExact tests the exact bitmap in shared memory (keys outside [0, part_max] fail);
+// kPartBloom a blocked Bloom filter in shared memory, whose word index is in range for any
+// key and whose hits (false positives, and keys outside the part range) the resolve
+// confirms against the exact bitmap.
+template <int MODE>
 __global__ void __launch_bounds__(kLiThreads) li_filter_kernel(const int32_t* __restrict__ part, uint64_t n,
-                                                               const uint32_t* __restrict__ bits, int32_t part_max,
-                                                               const uint32_t* __restrict__ filt, uint32_t filt_words,
-                                                               int mode, uint32_t* __restrict__ passbits) {
+                                                               int32_t part_max, const uint32_t* __restrict__ filt,
+                                                               uint32_t filt_words, uint32_t* __restrict__ passbits) {
   extern __shared__ uint32_t sfilt[];
   smem_filter_load(filt, filt_words, sfilt);
-  const bool vec = (reinterpret_cast<uintptr_t>(part) & 15u) == 0;
   const int lane = threadIdx.x & 31;
   constexpr uint64_t kStepRows = (uint64_t)kLiThreads * kLiRows;
   const uint64_t step = (uint64_t)gridDim.x * kStepRows;
-  // row of element (q, k) of this thread in the step at b
-  auto row_of = [&](uint64_t b, int q, int k) { return b + 4 * ((uint64_t)q * kLiThreads + threadIdx.x) + k; };
-  int4 nv[kLiQuads];
+  // first row of group g (0..kLiQuads-1) of this warp in the step at b
+  auto group_of = [&](uint64_t b, int g) { return b + 128 * ((uint64_t)g * (kLiThreads / 32) + (threadIdx.x >> 5)); };
+  int32_t nv[kLiRows];
   auto prefetch = [&](uint64_t b) {
-    if (vec && b + kStepRows <= n) {
+    if (b + kStepRows <= n) {
 #pragma unroll
-      for (int q = 0; q < kLiQuads; q++) nv[q] = ld_stream(reinterpret_cast<const int4*>(part + row_of(b, q, 0)));
+      for (int g = 0; g < kLiQuads; g++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) nv[4 * g + k] = ld_stream(part + group_of(b, g) + 32 * k + lane);
     }
   };
   uint64_t b = (uint64_t)blockIdx.x * kStepRows;
   prefetch(b);
-  for (; b < n; b += step) {
+  for (; b < n; b += step) {   // b is the same for the whole block: every lane votes
     int32_t p[kLiRows];
-    if (vec && b + kStepRows <= n) {
+    const bool full = b + kStepRows <= n;
+    if (full) {
 #pragma unroll
-      for (int q = 0; q < kLiQuads; q++) {
-        p[4 * q] = nv[q].x; p[4 * q + 1] = nv[q].y; p[4 * q + 2] = nv[q].z; p[4 * q + 3] = nv[q].w;
-      }
+      for (int j = 0; j < kLiRows; j++) p[j] = nv[j];
     } else {
 #pragma unroll
-      for (int q = 0; q < kLiQuads; q++)
+      for (int g = 0; g < kLiQuads; g++)
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          const uint64_t r = row_of(b, q, k);
-          p[4 * q + k] = r < n ? ld_stream(part + r) : -1;
+          const uint64_t r = group_of(b, g) + 32 * k + lane;
+          p[4 * g + k] = r < n ? ld_stream(part + r) : 0;
         }
     }
     prefetch(b + step);
-    uint32_t ok = 0;
 #pragma unroll
-    for (int j = 0; j < kLiRows; j++) ok |= (uint32_t)(p[j] >= 0 && p[j] <= part_max) << j;
-    // Bloom-form hits are not confirmed here: the resolve tests the exact bitmap after it has
-    // gathered the part key, before the other columns
-    const uint32_t take = smem_filter_mask<kLiRows, false>(sfilt, mode == kPartExact, bits, p, ok);
+    for (int g = 0; g < kLiQuads; g++) {
+      const uint64_t r0 = group_of(b, g);
+      uint32_t w[4];
 #pragma unroll
-    for (int q = 0; q < kLiQuads; q++) {
-      // rows 4*lane .. 4*lane+3 of this quad's 128 rows: bits 4*(lane & 7) .. of word lane / 8
-      uint32_t v = ((take >> (4 * q)) & 0xFu) << (4 * (lane & 7));
-      v |= __shfl_xor_sync(FULL_MASK, v, 1);
-      v |= __shfl_xor_sync(FULL_MASK, v, 2);
-      v |= __shfl_xor_sync(FULL_MASK, v, 4);
-      const uint64_t r0 = row_of(b, q, 0);
-      if ((lane & 7) == 0 && r0 < n) passbits[r0 >> 5] = v;
+      for (int k = 0; k < 4; k++) {
+        const int32_t key = p[4 * g + k];
+        bool hit;
+        if (MODE == kPartExact) {
+          const bool in = (uint32_t)key <= (uint32_t)part_max;
+          const uint32_t x = in ? (uint32_t)key : 0u;
+          hit = in && ((sfilt[x >> 5] >> (x & 31u)) & 1u);
+        } else {
+          const uint32_t h = smem_filter_mix(key), m = smem_filter_bits(h);
+          hit = (sfilt[smem_filter_word(h)] & m) == m;
+        }
+        if (!full) hit = hit && r0 + 32 * k + lane < n;
+        w[k] = __ballot_sync(FULL_MASK, hit);
+      }
+      if (lane == 0 && r0 < n) *reinterpret_cast<uint4*>(passbits + (r0 >> 5)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
 }
@@ -305,9 +312,12 @@ __global__ void __launch_bounds__(kQ9Threads) q9_resolve_kernel(const uint32_t* 
       if (j >= total) continue;
       const uint64_t r = ((g * 32 + src) << 5) + nth_set_bit(sw, j - sx);
       const int32_t pk = ld_stream(part + r);
-      // a Bloom filter's false positive (about 1% of the other parts) stops after one gather
-      // and one test of the exact bitmap (L2-resident); the fact filter checked the range
-      if (m.part_bits && !((__ldg(m.part_bits + ((uint32_t)pk >> 5)) >> ((uint32_t)pk & 31u)) & 1u)) continue;
+      // a Bloom filter's false positive (about 1% of the other parts, or a key outside the
+      // part range) stops after one gather and one test of the exact bitmap (L2-resident); the
+      // exact filter has tested the range and the bit itself
+      if (m.part_bits && ((uint32_t)pk > (uint32_t)m.part_max ||
+                          !((__ldg(m.part_bits + ((uint32_t)pk >> 5)) >> ((uint32_t)pk & 31u)) & 1u)))
+        continue;
       const int32_t sk = ld_stream(supp + r), o = ld_stream(order + r);
       const int64_t e = ld_stream(ext + r);
       const int32_t d = ld_stream(disc + r), q = ld_stream(qty + r);
@@ -451,6 +461,7 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   const uint64_t piece =
       std::max<uint64_t>(1, std::min<uint64_t>(pp.chunk_rows ? (uint64_t)pp.chunk_rows : li->n_rows, kQ9Piece));
   void* passbits = nullptr;
+  // (the filter writes whole 128-row groups: up to three words past (piece + 31) / 32)
   if (!rc) rc = scratch(ctx, "q9.passbits", ((piece + 31) / 32 + 32) * 4, &passbits);
   if (rc) return rc;
   uint32_t* cnt = static_cast<uint32_t*>(count);
@@ -461,8 +472,10 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
   // dynamic + static shared memory may pass the 48 KB default: always opt in (before any capture)
   GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q9_resolve_kernel, probe_smem));
   const size_t filt_smem = (size_t)filt_words * 4;
-  GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)li_filter_kernel, filt_smem));
-  const int filter_per_sm = kernel_occupancy(ctx, (const void*)li_filter_kernel, kLiThreads, filt_smem);
+  const void* li_kernel = filt_mode == kPartExact ? (const void*)li_filter_kernel<kPartExact>
+                                                   : (const void*)li_filter_kernel<kPartBloom>;
+  GPUDB_CUDA(ctx, kernel_smem(ctx, li_kernel, filt_smem));
+  const int filter_per_sm = kernel_occupancy(ctx, li_kernel, kLiThreads, filt_smem);
   const int resolve_per_sm = kernel_occupancy(ctx, (const void*)q9_resolve_kernel, kQ9Threads, probe_smem);
   GPUDB_CUDA(ctx, kernel_smem(ctx, (const void*)q9_sort_kernel, sort_smem));
   const int sms = ctx->sm_count;
@@ -514,9 +527,13 @@ extern "C" int gpudb_q9_star(gpudb_ctx* ctx, const gpudb_part* pa, const gpudb_s
         const unsigned fg = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((n + kLiThreads * kLiRows - 1) / (kLiThreads * kLiRows),
                                   (uint64_t)sms * std::max(1, filter_per_sm)));
-        GPUDB_LAUNCH(call, li_filter_kernel, fg, kLiThreads, filt_smem, c.part_key + off, n, (const uint32_t*)bits,
-                     part_max, (const uint32_t*)(filt_exact ? bits : hfilt), filt_words, filt_mode,
-                     (uint32_t*)passbits);
+        const uint32_t* fsrc = (const uint32_t*)(filt_exact ? bits : hfilt);
+        if (filt_mode == kPartExact)
+          GPUDB_LAUNCH(call, li_filter_kernel<kPartExact>, fg, kLiThreads, filt_smem, c.part_key + off, n, part_max,
+                       fsrc, filt_words, (uint32_t*)passbits);
+        else
+          GPUDB_LAUNCH(call, li_filter_kernel<kPartBloom>, fg, kLiThreads, filt_smem, c.part_key + off, n, part_max,
+                       fsrc, filt_words, (uint32_t*)passbits);
         if (!joined) {
           const int jr = call.side_join();
           if (jr) return jr;

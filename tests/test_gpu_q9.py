@@ -63,6 +63,27 @@ def test_q9_part_filter_past_shared_memory(engine, orc, n_parts):
         free_all(engine, ts)
 
 
+@pytest.mark.parametrize("piece", [0, 65_537])
+def test_q9_fact_part_keys_outside_the_part_range(engine, orc, piece):
+    """Fact rows whose part key is negative or above the part table's largest key match no
+    part. In the Bloom form (more parts than the shared-memory bitmap holds) the filter does
+    not test the range; such a key that passes the Bloom filter is turned away by the
+    resolve before it reads the exact bitmap."""
+    tabs = orc.q9_tables(1_700_000, 2_000, 200_000, 800_003, 23)
+    li = tabs[4]
+    part_max = int(tabs[0]["part_key"].max())
+    rng = np.random.default_rng(5)
+    rows = rng.choice(len(li["part_key"]), 40_000, replace=False)
+    bad = np.array([-7, -1, part_max + 1, part_max + 1_000_003, 2**31 - 1, -2**31], np.int32)
+    li["part_key"][rows] = bad[np.arange(len(rows)) % len(bad)]
+    ts = upload_all(engine, tabs)
+    try:
+        kw = {"chunk_rows": piece} if piece else {}
+        assert engine.q9(*ts, **kw) == orc.q9(*tabs)
+    finally:
+        free_all(engine, ts)
+
+
 @pytest.mark.parametrize("piece", [40_000, 30_001])
 def test_q9_fact_table_in_pieces(engine, orc, piece):
     """A device-resident fact table goes through the filter + resolve kernels in pieces of
