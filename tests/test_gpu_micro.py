@@ -141,6 +141,26 @@ def test_radix_partition_every_block_shape(engine, orc, shape):
             engine.device_free(x)
 
 
+@pytest.mark.parametrize("shape", [5, 3])
+def test_radix_join_count_through_the_ring(engine, orc, shape):
+    """Tables large enough that every scatter block walks several sub-tiles through its
+    bulk-copy ring: the join count over 10-bit partitions (unstable, keys only) equals the
+    oracle's, also for a probe side whose length is not a whole number of sub-tiles and
+    starts off a 16-byte boundary (direct loads, no ring)."""
+    nb, npr = 3_000_001, 12_000_017
+    b = orc.gen(8, nb, seed=41, n_orders=nb // 2, order_mode=2)
+    p = orc.gen(8, npr, seed=42, n_orders=nb // 2, order_mode=1)
+    db, dp = engine.to_device(b), engine.to_device(p)
+    try:
+        engine.set_option(capi.OPT_RADIX_SHAPE, shape)
+        assert engine.hash_join_count(db, nb, dp, npr, capi.JOIN_RADIX) == orc.join_count(b, p)
+        assert engine.hash_join_count(db, nb, dp + 4, npr - 1, capi.JOIN_RADIX) == orc.join_count(b, p[1:])
+    finally:
+        engine.set_option(capi.OPT_RADIX_SHAPE, 0)
+        engine.device_free(db)
+        engine.device_free(dp)
+
+
 def test_radix_partition_bad_bits(engine):
     with pytest.raises(capi.GpudbError) as e:
         engine.radix_partition(None, None, 0, 17, 1, 1, 1)
