@@ -562,7 +562,8 @@ int gpudb_selftest_bounded_wait(gpudb_ctx* ctx, uint32_t polls, int32_t arrive);
 
 /* ---- autotuner (no reference counterpart) --------------------------------------------
  * gpudb_autotune times the candidate settings of one request's pipeline on the request's
- * own tables (reps runs each, median device time) and sets the fastest on the context:
+ * own tables (one synchronous run, then reps runs issued back to back on the context's
+ * stream: median device time) and sets the fastest on the context:
  *   Q1: GPUDB_OPT_SCAN_VARIANT 1..10 (block size, rows per thread, 128-bit loads, TMA
  *       staging, shared-memory accumulators); Q6: GPUDB_OPT_Q6_VARIANT 1..4 (row kernel or
  *       128-bit loads with 1/2/4 quads per thread per step); Q3 global mode:
