@@ -228,25 +228,30 @@ def test_admission_by_footprint(engine, small):
     assert st["peak_admitted_bytes"] <= big
 
 
-@pytest.mark.parametrize("n6", [1, 2, 4, 5])
-def test_q6_requests_riding_on_one_q1_scan(engine, orc, n6):
-    """One Q1 request and n6 Q6 requests over the same rows: up to four Q6 requests are
-    evaluated by the Q1 kernel on the rows it reads, five go their own way; every result
-    equals the oracle's."""
+@pytest.mark.parametrize("n1,n6", [(1, 1), (1, 2), (1, 4), (1, 5), (2, 1), (2, 2), (2, 6), (3, 4), (4, 9)])
+def test_q6_requests_riding_on_a_q1_scan(engine, orc, n1, n6):
+    """n1 Q1 requests and n6 Q6 requests over the same rows: a lone Q1 request's kernel also
+    evaluates up to four Q6 requests on the rows it reads; other mixes go their own way
+    (single-request kernels, or shared passes for more requests); every result equals the
+    oracle's."""
     li = orc.lineitem(300_007, seed=31)
     s = engine.upload("lineitem", li).lineitem()
     q6s = [(100 + 300 * i, 900 + 300 * i, i % 5, i % 5 + 4, 20 + 5 * i) for i in range(n6)]
     q6s[-1] = (2000, 1000, 0, 10, 50)   # an empty ship range: nothing matches
-    reqs = (capi.Request * (1 + n6))()
-    o1 = capi.Q1Result()
-    reqs[0].pipeline, reqs[0].li, reqs[0].q1, reqs[0].q1_out = capi.PIPE_Q1, C.pointer(s), capi.Q1Params(1800, 0), C.pointer(o1)
+    q1s = [1800 - 250 * i for i in range(n1)]
+    reqs = (capi.Request * (n1 + n6))()
+    o1 = [capi.Q1Result() for _ in q1s]
+    for i, le in enumerate(q1s):
+        r = reqs[i]
+        r.pipeline, r.li, r.q1, r.q1_out = capi.PIPE_Q1, C.pointer(s), capi.Q1Params(le, 0), C.pointer(o1[i])
     o6 = [capi.Q6Result() for _ in q6s]
     for i, p in enumerate(q6s):
-        r = reqs[1 + i]
+        r = reqs[n1 + i]
         r.pipeline, r.li, r.q6, r.q6_out = capi.PIPE_Q6, C.pointer(s), capi.Q6Params(*p), C.pointer(o6[i])
     engine._check(engine.lib.gpudb_batch_run(engine.ctx, reqs, len(reqs), None, None))
     assert all(r.status == capi.OK for r in reqs)
-    assert q1_to_dict(o1) == orc.q1(li, 1800)
+    for le, o in zip(q1s, o1):
+        assert q1_to_dict(o) == orc.q1(li, le), le
     for p, o in zip(q6s, o6):
         assert (o.revenue, o.rows_matched) == orc.q6(li, *p), p
 
