@@ -4,9 +4,10 @@
 // hash_join_build/probe (kernels/microbenchmarks.metal:160-294).
 //
 // B200 design:
-//  - selection: one ballot per 32 rows gives a 32-bit word of the row bitmask directly
-//    (the reference writes one 32-bit 0/1 word per row); row ids are compacted in input
-//    order with per-tile counts, a device scan and a second pass;
+//  - selection: 32-bit words of the row bitmask (the reference writes one 32-bit 0/1 word
+//    per row). Bitmask and count alone: one kernel over SMs x occupancy blocks, 128-bit
+//    loads a tile ahead, one atomic add per block. With row ids: per-tile counts, a device
+//    scan, and a second pass that compacts the ids in input order (one ballot per 32 rows);
 //  - sum: 128-bit loads, int64 per thread, warp shuffle + last-block fold (one launch);
 //  - join count: build keys go into an open-addressing set (atomicCAS, power of two,
 //    <= 50% load); probe rows count once per row at the first match (semi-join count,
@@ -63,6 +64,66 @@ __global__ void __launch_bounds__(kThreads) select_count_kernel(const int32_t* _
     uint32_t t = 0;
     for (int w = 0; w < kThreads / 32; w++) t += wc[w];
     tile_counts[blockIdx.x] = t;
+  }
+}
+
+// Bitmask (when given) and count, no row ids, so no per-tile counts: a grid of SMs x occupancy
+// blocks walks the tiles; a lane's four 128-row steps of a tile are loaded together, one
+// tile ahead of the one being tested, the words are assembled as in select_count_kernel,
+// and each block adds its count to *total once.
+__global__ void __launch_bounds__(kThreads) select_bits_kernel(const int32_t* __restrict__ col, uint64_t n,
+                                                               int32_t value, uint32_t* bits,
+                                                               unsigned long long* total) {
+  constexpr int kSteps = kSelTile / 128 / (kThreads / 32);   // 128-row steps of a warp per tile
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool vec = (reinterpret_cast<uintptr_t>(col) & 15u) == 0;
+  const uint64_t tiles = (n + kSelTile - 1) / kSelTile;
+  uint32_t c = 0;
+  int4 nv[kSteps];   // the block's next tile, loading while this one is tested
+  auto prefetch = [&](uint64_t tile) {
+    if (vec && tile < tiles && (tile + 1) * kSelTile <= n) {
+#pragma unroll
+      for (int k = 0; k < kSteps; k++)
+        nv[k] = ld_stream(reinterpret_cast<const int4*>(col + tile * kSelTile +
+                                                        (uint64_t)(warp + k * (kThreads / 32)) * 128 + 4 * lane));
+    }
+  };
+  prefetch(blockIdx.x);
+  for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint64_t base = tile * kSelTile;
+    const bool full = vec && base + kSelTile <= n;
+    int4 v[kSteps];
+#pragma unroll
+    for (int k = 0; k < kSteps; k++) v[k] = nv[k];
+    prefetch(tile + gridDim.x);
+#pragma unroll
+    for (int k = 0; k < kSteps; k++) {
+      const uint64_t r = base + (uint64_t)(warp + k * (kThreads / 32)) * 128 + 4 * lane;
+      uint32_t nib = 0;
+      if (full) {
+        nib = (uint32_t)(v[k].x < value) | ((uint32_t)(v[k].y < value) << 1) | ((uint32_t)(v[k].z < value) << 2) |
+              ((uint32_t)(v[k].w < value) << 3);
+      } else {
+        for (int i = 0; i < 4; i++)
+          if (r + i < n && col[r + i] < value) nib |= 1u << i;
+      }
+      c += __popc(nib);
+      uint32_t word = nib << (4 * (lane & 7));
+      word |= __shfl_xor_sync(FULL_MASK, word, 1);
+      word |= __shfl_xor_sync(FULL_MASK, word, 2);
+      word |= __shfl_xor_sync(FULL_MASK, word, 4);
+      const uint64_t wr = r - 4 * (lane & 7);   // first row of this word
+      if (bits && (lane & 7) == 0 && wr < n) bits[wr >> 5] = word;
+    }
+  }
+  c = __reduce_add_sync(FULL_MASK, c);
+  __shared__ uint32_t wc[kThreads / 32];
+  if (lane == 0) wc[warp] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kThreads / 32; w++) t += wc[w];
+    if (t) atomicAdd(total, (unsigned long long)t);
   }
 }
 
@@ -231,7 +292,11 @@ extern "C" int gpudb_select_lt(gpudb_ctx* ctx, const int32_t* col, uint64_t n, i
   uint64_t* tile_off = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(tmp) + ((tiles + 1) * 4 + 15) / 16 * 16);
   uint64_t* scan_tmp = tile_off + tiles + 2;
   uint64_t* total = call.result<uint64_t>();
-  if (n) {
+  if (n && !out_rows) {
+    // (the result slot is zero: Call::begin clears it)
+    GPUDB_LAUNCH(call, select_bits_kernel, grid_of(ctx, tiles * kThreads, 8), kThreads, 0, col, n, value, out_bits,
+                 reinterpret_cast<unsigned long long*>(total));
+  } else if (n) {
     GPUDB_LAUNCH(call, select_count_kernel, (unsigned)tiles, kThreads, 0, col, n, value, out_bits, tile_counts);
     rc = exclusive_scan<uint32_t, uint64_t>(call, tile_counts, tiles, tile_off, scan_tmp, total);
     if (rc) return rc;

@@ -24,6 +24,18 @@ def test_select_lt(engine, orc, n, value):
         assert np.array_equal(engine.to_host(bits, (n + 31) // 32, np.uint32), wbits)
         assert np.array_equal(engine.to_host(rows, c, np.uint32), wrows)
         assert engine.select_lt(dcol, n, value) == wc   # count only
+        # bitmask only (one kernel, no per-tile counts): every word written, on a buffer of ones
+        words = (n + 31) // 32
+        ones = engine.to_device(np.full(words + 1, 0xFFFFFFFF, np.uint32))
+        try:
+            assert engine.select_lt(dcol, n, value, ones) == wc
+            assert np.array_equal(engine.to_host(ones, words, np.uint32), wbits)
+            if n > 1:   # the column 4 bytes past a 16-byte boundary
+                wc1, wbits1, _ = orc.select_lt(col[1:], value)
+                assert engine.select_lt(dcol + 4, n - 1, value, ones) == wc1
+                assert np.array_equal(engine.to_host(ones, (n + 30) // 32, np.uint32), wbits1)
+        finally:
+            engine.device_free(ones)
     finally:
         for p in (dcol, bits, rows):
             if p:
