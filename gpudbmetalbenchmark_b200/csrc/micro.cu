@@ -11,7 +11,9 @@
 //  - sum: 128-bit loads, int64 per thread, warp shuffle + last-block fold (one launch);
 //  - join count: build keys go into an open-addressing set (atomicCAS, power of two,
 //    <= 50% load); probe rows count once per row at the first match (semi-join count,
-//    as hash_join_probe does). Radix mode lives in radix.cu.
+//    as hash_join_probe does). Radix mode lives in radix.cu. Direct mode: the build keys'
+//    [min, max] found on the device, one bit per key of that span (order keys of 15M
+//    orders: 7.5 MB, L2-resident), and the probe streams its keys against the bits.
 #include <algorithm>
 #include <cstring>
 
@@ -251,6 +253,90 @@ __global__ void __launch_bounds__(kThreads) set_probe_count_kernel(const int32_t
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
 
+// ---- direct mode: one bit per key of the build keys' span [lo, hi] -----------------------
+constexpr uint64_t kDirectMaxSpan = 1ull << 30;   // keys the bitmap may span (128 MB of bits)
+
+// span = {lo, hi} of the build keys. It starts as {0x7F7F7F7F, 0x80808080} (byte memsets),
+// which can only widen the span of keys that lie beyond those values; no keys leave hi < lo.
+__global__ void __launch_bounds__(kThreads) key_span_kernel(const int32_t* __restrict__ keys, uint64_t n,
+                                                            int32_t* span) {
+  int32_t lo = INT32_MAX, hi = INT32_MIN;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = __ldg(keys + i);   // cached: the bit-setting pass reads the keys again
+    lo = min(lo, k);
+    hi = max(hi, k);
+  }
+  lo = __reduce_min_sync(FULL_MASK, lo);
+  hi = __reduce_max_sync(FULL_MASK, hi);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(span, lo);
+    atomicMax(span + 1, hi);
+  }
+}
+
+// Whether the span is usable: not empty and at most kDirectMaxSpan keys.
+__device__ __forceinline__ bool span_usable(const int32_t* span, int64_t* lo, uint32_t* range) {
+  const int64_t l = span[0], h = span[1];
+  *lo = l;
+  *range = (uint32_t)(h - l);
+  return h >= l && (uint64_t)(h - l) < kDirectMaxSpan;
+}
+
+// Clears the span's bitmap words; a span over kDirectMaxSpan keys sets ST_KEY_RANGE instead.
+__global__ void __launch_bounds__(kThreads) span_clear_kernel(const int32_t* span, uint32_t* bm, uint32_t* status) {
+  int64_t lo;
+  uint32_t range;
+  if (!span_usable(span, &lo, &range)) {
+    if (span[1] >= span[0] && blockIdx.x == 0 && threadIdx.x == 0) set_status(status, ST_KEY_RANGE);
+    return;
+  }
+  const uint64_t words = ((uint64_t)range >> 5) + 1, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) bm[i] = 0u;
+}
+
+__global__ void __launch_bounds__(kThreads) span_set_kernel(const int32_t* __restrict__ keys, uint64_t n,
+                                                            const int32_t* span, uint32_t* bm) {
+  int64_t lo;
+  uint32_t range;
+  if (!span_usable(span, &lo, &range)) return;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t x = (uint32_t)((int64_t)__ldg(keys + i) - lo);   // in [0, range]: lo <= key <= hi
+    atomicOr(bm + (x >> 5), 1u << (x & 31u));
+  }
+}
+
+__device__ __forceinline__ uint32_t span_hit(const uint32_t* bm, int64_t lo, uint32_t range, int32_t k) {
+  const int64_t d = (int64_t)k - lo;   // 64-bit: no key outside the span can alias into it
+  return d >= 0 && d <= (int64_t)range ? (__ldg(bm + ((uint64_t)d >> 5)) >> ((uint32_t)d & 31u)) & 1u : 0u;
+}
+
+// Probe rows whose key's bit is set: 128-bit loads of the keys where the column allows.
+__global__ void __launch_bounds__(kThreads) span_probe_kernel(const int32_t* __restrict__ keys, uint64_t n,
+                                                              const int32_t* span, const uint32_t* __restrict__ bm,
+                                                              unsigned long long* count) {
+  int64_t lo;
+  uint32_t range;
+  if (!span_usable(span, &lo, &range)) return;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x, tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t c = 0;
+  if ((reinterpret_cast<uintptr_t>(keys) & 15u) == 0) {
+    const uint64_t nq = n >> 2;
+    for (uint64_t q = tid; q < nq; q += stride) {
+      const int4 v = ld_stream(reinterpret_cast<const int4*>(keys) + q);
+      c += span_hit(bm, lo, range, v.x) + span_hit(bm, lo, range, v.y) + span_hit(bm, lo, range, v.z) +
+           span_hit(bm, lo, range, v.w);
+    }
+    const uint64_t r = (nq << 2) + tid;
+    if (r < n) c += span_hit(bm, lo, range, keys[r]);
+  } else {
+    for (uint64_t i = tid; i < n; i += stride) c += span_hit(bm, lo, range, ld_stream(keys + i));
+  }
+  c = __reduce_add_sync(FULL_MASK, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
 unsigned grid_of(gpudb_ctx* ctx, uint64_t items, int per_sm) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + kThreads - 1) / kThreads, (uint64_t)ctx->sm_count * per_sm));
 }
@@ -338,7 +424,8 @@ extern "C" int gpudb_hash_join_count(gpudb_ctx* ctx, const int32_t* build_keys, 
   if (!ctx) return GPUDB_E_INVALID;
   if (!matches || (n_build && !build_keys) || (n_probe && !probe_keys))
     return fail(ctx, GPUDB_E_INVALID, "join: keys and matches are required");
-  if (mode != GPUDB_JOIN_GLOBAL && mode != GPUDB_JOIN_RADIX) return fail(ctx, GPUDB_E_INVALID, "join: unknown mode");
+  if (mode != GPUDB_JOIN_GLOBAL && mode != GPUDB_JOIN_RADIX && mode != GPUDB_JOIN_DIRECT)
+    return fail(ctx, GPUDB_E_INVALID, "join: unknown mode");
   if (n_build > (1ull << 30)) return fail(ctx, GPUDB_E_INVALID, "join: build side larger than 2^30 rows");
   Call call(ctx, ex, t);
   int rc = call.begin(16);
@@ -352,6 +439,25 @@ extern "C" int gpudb_hash_join_count(gpudb_ctx* ctx, const int32_t* build_keys, 
     if (n_probe)
       GPUDB_LAUNCH(call, set_probe_count_kernel, grid_of(ctx, n_probe, 8), kThreads, 0, probe_keys, n_probe,
                    (const int32_t*)set, cap, cnt);
+  } else if (mode == GPUDB_JOIN_DIRECT) {
+    // a bitmap over the build keys' span, found on the device (no host round trip)
+    void* sp = nullptr;
+    void* bm = nullptr;
+    rc = scratch(ctx, "join.span", 256, &sp);
+    if (!rc) rc = scratch(ctx, "join.bitmap", kDirectMaxSpan / 8, &bm);
+    if (rc) return rc;
+    int32_t* span = static_cast<int32_t*>(sp);
+    GPUDB_CUDA(ctx, cudaMemsetAsync(span, 0x7F, 4, call.stream()));
+    GPUDB_CUDA(ctx, cudaMemsetAsync(span + 1, 0x80, 4, call.stream()));
+    if (n_build) GPUDB_LAUNCH(call, key_span_kernel, grid_of(ctx, n_build, 8), kThreads, 0, build_keys, n_build, span);
+    GPUDB_LAUNCH(call, span_clear_kernel, grid_of(ctx, kDirectMaxSpan / 32, 8), kThreads, 0, (const int32_t*)span,
+                 (uint32_t*)bm, call.status());
+    if (n_build)
+      GPUDB_LAUNCH(call, span_set_kernel, grid_of(ctx, n_build, 8), kThreads, 0, build_keys, n_build,
+                   (const int32_t*)span, (uint32_t*)bm);
+    if (n_probe)
+      GPUDB_LAUNCH(call, span_probe_kernel, grid_of(ctx, n_probe / 4 + 1, 8), kThreads, 0, probe_keys, n_probe,
+                   (const int32_t*)span, (const uint32_t*)bm, cnt);
   } else {
     rc = radix_join_count(call, build_keys, n_build, probe_keys, n_probe, cnt);
     if (rc) return rc;

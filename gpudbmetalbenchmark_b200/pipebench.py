@@ -132,16 +132,20 @@ def q9_case(eng, reps, stream600m=False, out=emit):
 
 
 def join_count_case(eng, reps, out=emit):
-    """Join microbenchmark: 15M-key build x 60M-key probe, global table and radix partitions."""
+    """Join microbenchmark: 15M-key build x 60M-key probe, global table, radix partitions and
+    the direct bitmap over the build keys' span; every mode's count must agree."""
     b = eng.generate("orders", 15_000_000, seed=42, columns=("order_key",))
     p = eng.generate("lineitem", 60_000_000, seed=42, columns=("order_key",), n_orders=15_000_000,
                      order_mode=capi.ORDERS_CLUSTERED)
     res = {}
-    for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix")):
+    counts = set()
+    for mode, mname in ((capi.JOIN_GLOBAL, "global"), (capi.JOIN_RADIX, "radix"), (capi.JOIN_DIRECT, "direct")):
         ms, t = timed(lambda tm: eng.hash_join_count(b.ptr("order_key"), 15_000_000, p.ptr("order_key"),
                                                      60_000_000, mode, timing=tm), reps)
+        counts.add(eng.hash_join_count(b.ptr("order_key"), 15_000_000, p.ptr("order_key"), 60_000_000, mode))
         res[mname] = out("hash_join_count", "15M build x 60M probe, %s" % mname, 60_000_000, ms, 75_000_000 * 4,
                          {"kernels": t.kernels})
+    assert len(counts) == 1, counts
     eng.free(b)
     eng.free(p)
     return res

@@ -452,7 +452,10 @@ int gpudb_select_lt(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int32_t valu
 int gpudb_sum_i32(gpudb_ctx* ctx, const int32_t* col, uint64_t n, int64_t* sum,
                   gpudb_timing* t, const gpudb_exec* ex);
 /* Number of probe rows whose key occurs among the build keys (hash_join_probe counts a
- * probe row once, at its first match). mode: GPUDB_JOIN_GLOBAL or GPUDB_JOIN_RADIX. */
+ * probe row once, at its first match). mode: GPUDB_JOIN_GLOBAL (one hash set), GPUDB_JOIN_RADIX
+ * (radix partitions, a shared-memory set per partition) or GPUDB_JOIN_DIRECT (one bit per key
+ * of the build keys' span [min, max], found on the device; a span of 2^30 keys or more
+ * returns GPUDB_E_KEY_RANGE; the context keeps 128 MB of scratch for the bits). */
 int gpudb_hash_join_count(gpudb_ctx* ctx, const int32_t* build_keys, uint64_t n_build,
                           const int32_t* probe_keys, uint64_t n_probe, int32_t mode,
                           uint64_t* matches, gpudb_timing* t, const gpudb_exec* ex);

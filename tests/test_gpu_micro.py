@@ -64,7 +64,7 @@ def test_sum_i32_extreme_values(engine, orc):
         engine.device_free(d)
 
 
-@pytest.mark.parametrize("mode", [capi.JOIN_GLOBAL, capi.JOIN_RADIX])
+@pytest.mark.parametrize("mode", [capi.JOIN_GLOBAL, capi.JOIN_RADIX, capi.JOIN_DIRECT])
 @pytest.mark.parametrize("nb,np_,orders", [(1_500_000, 6_000_000, 1_500_000), (1000, 5000, 700), (1, 1, 1),
                                            (0, 100, 10), (100, 0, 10), (200_000, 300_000, 50_000)])
 def test_hash_join_count(engine, orc, mode, nb, np_, orders):
@@ -171,6 +171,41 @@ def test_radix_join_count_through_the_ring(engine, orc, shape):
         engine.set_option(capi.OPT_RADIX_SHAPE, 0)
         engine.device_free(db)
         engine.device_free(dp)
+
+
+def test_join_count_direct_edges(engine, orc):
+    """Direct mode: a bitmap over the build keys' span [min, max]. Negative keys, the int32
+    extremes among the probe keys (outside the span: no match, whatever their distance), a
+    probe column off a 16-byte boundary, a span of one key, and a span of 2^30 keys or more
+    (refused with GPUDB_E_KEY_RANGE, the context still usable)."""
+    rng = np.random.default_rng(9)
+    b = rng.integers(-500_000, 2_000_000, 300_000, dtype=np.int64).astype(np.int32)
+    p = np.concatenate([rng.integers(-800_000, 2_500_000, 1_000_003, dtype=np.int64).astype(np.int32),
+                        np.array([-2**31, 2**31 - 1, -500_001, 2_000_000, b.min(), b.max()], np.int32)])
+    db, dp = engine.to_device(b), engine.to_device(p)
+    try:
+        assert engine.hash_join_count(db, len(b), dp, len(p), capi.JOIN_DIRECT) == orc.join_count(b, p)
+        assert engine.hash_join_count(db, len(b), dp + 4, len(p) - 1, capi.JOIN_DIRECT) == orc.join_count(b, p[1:])
+        assert engine.hash_join_count(db, 1, dp, len(p), capi.JOIN_DIRECT) == orc.join_count(b[:1], p)
+    finally:
+        engine.device_free(db)
+        engine.device_free(dp)
+    wide = np.array([5, 5 + 2**30, 17], np.int32)
+    dw, dq = engine.to_device(wide), engine.to_device(np.array([5, 17, 6], np.int32))
+    try:
+        with pytest.raises(capi.GpudbError) as e:
+            engine.hash_join_count(dw, 3, dq, 3, capi.JOIN_DIRECT)
+        assert e.value.code == capi.E_KEY_RANGE
+        assert engine.hash_join_count(dw, 3, dq, 3, capi.JOIN_GLOBAL) == 2
+        narrow = np.array([5, 4 + 2**30, 17], np.int32)   # a span of exactly 2^30 keys is refused, 2^30 - 1 is not
+        dn = engine.to_device(narrow)
+        try:
+            assert engine.hash_join_count(dn, 3, dq, 3, capi.JOIN_DIRECT) == 2
+        finally:
+            engine.device_free(dn)
+    finally:
+        engine.device_free(dw)
+        engine.device_free(dq)
 
 
 def test_radix_partition_bad_bits(engine):
