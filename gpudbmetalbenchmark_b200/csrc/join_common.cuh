@@ -107,9 +107,9 @@ __device__ __forceinline__ void smem_filter_load(const uint32_t* __restrict__ sr
 }
 
 // Filter of N keys (ok[j]: key j is in [0, key_max]) -> bit j set where key j passes: the
-// shared-memory tests first, then (Bloom form, CONFIRM) every confirming load of `bits`
-// issued before any is used, so a thread waits for one memory latency, not N.
-template <int N, bool CONFIRM = true>
+// shared-memory tests first, then (Bloom form) every confirming load of `bits` issued before
+// any is used, so a thread waits for one memory latency, not N.
+template <int N>
 __device__ __forceinline__ uint32_t smem_filter_mask(const uint32_t* sfilt, bool exact, const uint32_t* bits,
                                                      const int32_t (&key)[N], uint32_t ok) {
   uint32_t hit = 0;
@@ -127,7 +127,7 @@ __device__ __forceinline__ uint32_t smem_filter_mask(const uint32_t* sfilt, bool
     const uint32_t h = smem_filter_mix(key[j]), m = smem_filter_bits(h);
     hit |= (uint32_t)(((ok >> j) & 1u) && (sfilt[smem_filter_word(h)] & m) == m) << j;
   }
-  if (!CONFIRM || !hit) return hit;
+  if (!hit) return hit;
   uint32_t w[N];
 #pragma unroll
   for (int j = 0; j < N; j++) w[j] = ((hit >> j) & 1u) ? __ldg(bits + ((uint32_t)key[j] >> 5)) : 0u;
