@@ -5,7 +5,9 @@ one step = one pass of each pipeline over the table.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0). value = lineitem rows scanned per second by the whole job
-(2 x rows x N per step); e2e = the same metric through the C ABI with the table in pinned
+(2 x rows x N per step), device-timed over K steps of async calls on the engine's stream;
+`roofline` is the Q1 kernel's, its launch time from CUDA events around the calls of every
+16th step of that timed region; e2e = the same metric through the C ABI with the table in pinned
 host memory (chunked host->HBM streaming inside the timed region), one call per pipeline;
 e2e_batched = the same two requests as one gpudb_batch_run call, which copies each chunk
 once for both scans. For N > 1 (torchrun) every rank scans its own 60M-row shard of one
