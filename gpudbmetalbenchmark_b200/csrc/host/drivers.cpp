@@ -741,13 +741,15 @@ void runJoinBenchmark(gpudb_ctx* ctx, const RunOptions& o) {
     probe = generate(ctx, ps, GPUDB_COL_LI_ORDER_KEY, GPUDB_MEM_DEVICE);
   }
   std::printf("Loaded %" PRIu64 " rows for build phase, %" PRIu64 " rows for probe phase.\n", bs.n_rows, ps.n_rows);
-  for (int mode : {GPUDB_JOIN_GLOBAL, GPUDB_JOIN_RADIX}) {
+  for (int mode : {GPUDB_JOIN_GLOBAL, GPUDB_JOIN_RADIX, GPUDB_JOIN_DIRECT}) {
     uint64_t m = 0;
     gpudb_timing t{};
     for (int i = 0; i < o.reps; i++)
       check(ctx, gpudb_hash_join_count(ctx, build.as<int32_t>(), bs.n_rows, probe.as<int32_t>(), ps.n_rows, mode, &m, &t, nullptr),
             "gpudb_hash_join_count");
-    std::printf("Join (%s) complete. Found %" PRIu64 " total matches.\n", mode == GPUDB_JOIN_GLOBAL ? "global table" : "radix partitioned", m);
+    const char* name = mode == GPUDB_JOIN_GLOBAL ? "global table" : mode == GPUDB_JOIN_RADIX ? "radix partitioned"
+                                                                                          : "direct bitmap";
+    std::printf("Join (%s) complete. Found %" PRIu64 " total matches.\n", name, m);
     std::printf("Total Join GPU time: %.4f ms\n\n", t.gpu_ms);
   }
 }

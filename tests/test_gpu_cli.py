@@ -154,7 +154,8 @@ def test_cli_microbenchmarks(orc):
     out = run("sf1", "join", "--scale", "0.01")
     b = orc.gen(30, 15000, 42)
     p = orc.gen(8, 60000, 42, n_orders=15000, order_mode=1)
-    assert [int(x) for x in re.findall(r"Found (\d+) total matches", out)] == [orc.join_count(b, p)] * 2
+    assert [int(x) for x in re.findall(r"Found (\d+) total matches", out)] == [orc.join_count(b, p)] * 3
+    assert re.findall(r"Join \(([a-z ]+)\) complete", out) == ["global table", "radix partitioned", "direct bitmap"]
 
 
 def test_cli_sf100_streams_the_fact_table(orc):
@@ -210,7 +211,7 @@ def test_cli_reads_tbl_files(orc, tmp_path):
     assert [(int(a), int(bb), scaled(c, 4)) for a, bb, c in rows] == want9[:15]
     out = run("join", "--data", d)
     assert [int(x) for x in re.findall(r"Found (\d+) total matches", out)] == [orc.join_count(od["order_key"],
-                                                                                                li["order_key"])] * 2
+                                                                                                li["order_key"])] * 3
     out = run("q4", "--data", d)
     assert q4_rows(out) == orc.q4(od, li)
     out = run("q12", "--data", d)
